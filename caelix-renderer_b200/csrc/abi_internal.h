@@ -1,0 +1,32 @@
+// Internal declarations shared by the translation units behind the C ABI.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "../../include/caelix_b200.h"
+
+namespace cx {
+
+void log(CaelixLogLevel level, const char* fmt, ...);
+CaelixResult cuda_result(cudaError_t e, const char* what);
+CaelixResult status_result(uint32_t status, const char* what);
+
+// Device memory grown on demand (never shrunk); freed by release().
+struct GrowBuffer
+{
+    void* ptr = nullptr;
+    uint64_t bytes = 0;
+    CaelixResult reserve(uint64_t want, const char* what);
+    void release();
+};
+
+}  // namespace cx
+
+struct CaelixDevice
+{
+    int ordinal = 0;
+    uint32_t sm_count = 148;
+    cx::GrowBuffer sort_scratch;  // caelix_radix_sort_pairs
+    uint32_t* status = nullptr;   // device word the asynchronous entry points OR their failures into
+};

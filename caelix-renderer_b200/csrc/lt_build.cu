@@ -1,0 +1,597 @@
+// Kernels and host sequence of the light BVH build (lt_build.cuh describes the pipeline).
+#include <cuda/atomic>
+
+#include "cx_device.cuh"
+#include "lt_build.cuh"
+#include "radix_sort.cuh"
+
+namespace cx {
+
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ float power6(const float f[6])
+{
+    return f[0] + f[1] + f[2] + f[3] + f[4] + f[5];
+}
+
+__device__ __forceinline__ float hmin(float a, float b) { return b < a ? b : a; }
+__device__ __forceinline__ float hmax(float a, float b) { return b > a ? b : a; }
+
+__device__ __forceinline__ LightSummary load_summary(const LightSummary* p)
+{
+    const float4 a = __ldg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldg(reinterpret_cast<const float4*>(p) + 1);
+    const float4 c = __ldg(reinterpret_cast<const float4*>(p) + 2);
+    LightSummary s;
+    s.face[0] = a.x; s.face[1] = a.y; s.face[2] = a.z; s.face[3] = a.w;
+    s.face[4] = b.x; s.face[5] = b.y; s.lo[0] = b.z; s.lo[1] = b.w;
+    s.lo[2] = c.x; s.hi[0] = c.y; s.hi[1] = c.z; s.hi[2] = c.w;
+    return s;
+}
+
+// A summary written by another thread of the same kernel: read through L2 (not the
+// non-coherent read-only path).
+__device__ __forceinline__ LightSummary load_summary_cg(const LightSummary* p)
+{
+    const float4 a = __ldcg(reinterpret_cast<const float4*>(p));
+    const float4 b = __ldcg(reinterpret_cast<const float4*>(p) + 1);
+    const float4 c = __ldcg(reinterpret_cast<const float4*>(p) + 2);
+    LightSummary s;
+    s.face[0] = a.x; s.face[1] = a.y; s.face[2] = a.z; s.face[3] = a.w;
+    s.face[4] = b.x; s.face[5] = b.y; s.lo[0] = b.z; s.lo[1] = b.w;
+    s.lo[2] = c.x; s.hi[0] = c.y; s.hi[1] = c.z; s.hi[2] = c.w;
+    return s;
+}
+
+__device__ __forceinline__ void store_summary(LightSummary* p, const LightSummary& s)
+{
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(s.face[0], s.face[1], s.face[2], s.face[3]);
+    q[1] = make_float4(s.face[4], s.face[5], s.lo[0], s.lo[1]);
+    q[2] = make_float4(s.lo[2], s.hi[0], s.hi[1], s.hi[2]);
+}
+
+// LtUnion (caelix_light_tree_layout.hlsl:315-334): a summary of power 0 is skipped.
+__device__ __forceinline__ LightSummary lt_union(const LightSummary& a, const LightSummary& b)
+{
+    if (power6(a.face) <= 0.0f) return b;
+    if (power6(b.face) <= 0.0f) return a;
+    LightSummary s;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) s.face[f] = a.face[f] + b.face[f];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        s.lo[k] = hmin(a.lo[k], b.lo[k]);
+        s.hi[k] = hmax(a.hi[k], b.hi[k]);
+    }
+    return s;
+}
+
+__device__ __forceinline__ uint32_t part1by2(uint32_t v)
+{
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t morton30(uint32_t x, uint32_t y, uint32_t z)
+{
+    return part1by2(x) | (part1by2(y) << 1) | (part1by2(z) << 2);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Gather emit + centre bounds. One thread per record.
+__global__ void __launch_bounds__(kThreads)
+    lt_emit_kernel(const BrickLightRecord* __restrict__ records, uint32_t n,
+                   const uint32_t* __restrict__ record_group, const uint32_t* __restrict__ record_entry,
+                   const GroupFrame* __restrict__ frames, LightBvhLeaf* __restrict__ leaves,
+                   BuildControl* __restrict__ control)
+{
+    uint32_t lo_code[3] = {0, 0, 0};  // ~order(centre), max-reduced
+    uint32_t hi_code[3] = {0, 0, 0};  // order(centre), max-reduced
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4* rp = reinterpret_cast<const uint4*>(records + i);
+        const uint4 w0 = __ldg(rp);
+        const uint4 w1 = __ldg(rp + 1);
+        const uint4 w2 = __ldg(rp + 2);
+        LightSummary local;
+        local.face[0] = __uint_as_float(w0.x);
+        local.face[1] = __uint_as_float(w0.y);
+        local.face[2] = __uint_as_float(w0.z);
+        local.face[3] = __uint_as_float(w0.w);
+        local.face[4] = __uint_as_float(w1.x);
+        local.face[5] = __uint_as_float(w1.y);
+        const uint32_t box_lo = w1.z;
+        const uint32_t box_hi = w1.w;
+        (void)w2;
+        const uint32_t g = record_group ? __ldg(record_group + i) : 0u;
+        float origin[3] = {0.0f, 0.0f, 0.0f};
+        float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        float t[3] = {0.0f, 0.0f, 0.0f};
+        if (frames) {
+            const GroupFrame* f = frames + g;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                origin[k] = __ldg(&f->origin[k]);
+                t[k] = __ldg(&f->trans[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 9; ++k) r[k] = __ldg(&f->rot[k]);
+        }
+        local.lo[0] = origin[0] + (float)(box_lo & kVoxelMask);
+        local.lo[1] = origin[1] + (float)((box_lo >> kVoxelBits) & kVoxelMask);
+        local.lo[2] = origin[2] + (float)((box_lo >> (2 * kVoxelBits)) & kVoxelMask);
+        local.hi[0] = origin[0] + (float)(box_hi & kVoxelMask);
+        local.hi[1] = origin[1] + (float)((box_hi >> kVoxelBits) & kVoxelMask);
+        local.hi[2] = origin[2] + (float)((box_hi >> (2 * kVoxelBits)) & kVoxelMask);
+
+        // LtWorldSummary (caelix_light_gather_emit.hlsl:11-34).
+        float centre[3], half[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            centre[k] = 0.5f * (local.lo[k] + local.hi[k]);
+            half[k] = 0.5f * (local.hi[k] - local.lo[k]);
+        }
+        LightSummary w;
+#pragma unroll
+        for (int row = 0; row < 3; ++row) {
+            const float wc = r[3 * row] * centre[0] + r[3 * row + 1] * centre[1] + r[3 * row + 2] * centre[2] +
+                             t[row];
+            const float wh = fabsf(r[3 * row]) * half[0] + fabsf(r[3 * row + 1]) * half[1] +
+                             fabsf(r[3 * row + 2]) * half[2];
+            w.lo[row] = wc - wh;
+            w.hi[row] = wc + wh;
+        }
+#pragma unroll
+        for (int f = 0; f < 6; ++f) w.face[f] = 0.0f;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            const int axis = f >> 1;
+            const float sign = (f & 1) ? -1.0f : 1.0f;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) {
+                const float d = sign * r[3 * b + axis];
+                w.face[2 * b] += local.face[f] * hmax(0.0f, d);
+                w.face[2 * b + 1] += local.face[f] * hmax(0.0f, -d);
+            }
+        }
+        LightBvhLeaf* leaf = leaves + i;
+        store_summary(&leaf->summary, w);
+        const uint32_t e = record_entry ? __ldg(record_entry + i) : i;
+        *reinterpret_cast<uint4*>(&leaf->group) = make_uint4(g, e, 0u, kNone);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float c = 0.5f * (w.lo[k] + w.hi[k]);
+            const uint32_t code = float_order(c);
+            lo_code[k] = max(lo_code[k], ~code);
+            hi_code[k] = max(hi_code[k], code);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo_code[k] = __reduce_max_sync(0xFFFFFFFFu, lo_code[k]);
+        hi_code[k] = __reduce_max_sync(0xFFFFFFFFu, hi_code[k]);
+    }
+    if ((threadIdx.x & 31u) == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (lo_code[k]) atomicMax(&control->bounds_code[k], lo_code[k]);
+            if (hi_code[k]) atomicMax(&control->bounds_code[3 + k], hi_code[k]);
+        }
+    }
+}
+
+// The centre bounds of the build from the reduced codes (3e38 / -3e38 without leaves, as the
+// reference's one-workgroup reduction starts).
+__device__ __forceinline__ void decode_bounds(const BuildControl* control, float lo[3], float hi[3])
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const uint32_t l = control->bounds_code[k];
+        const uint32_t h = control->bounds_code[3 + k];
+        lo[k] = l ? float_unorder(~l) : 3.0e38f;
+        hi[k] = h ? float_unorder(h) : -3.0e38f;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Morton codes (value = leaf index) + the four digit histograms + clearing the arrival counters.
+__global__ void __launch_bounds__(kThreads)
+    lt_morton_kernel(const LightBvhLeaf* __restrict__ leaves, uint32_t n, const BuildControl* __restrict__ control,
+                     uint32_t* __restrict__ keys, uint32_t* __restrict__ counter, uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t s_hist[4][kRadix];
+    for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+    float lo[3], hi[3];
+    decode_bounds(control, lo, hi);
+    float extent[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) extent[k] = hmax(hi[k] - lo[k], 1e-6f);
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const float4* lp = reinterpret_cast<const float4*>(leaves + i);
+        const float4 b = __ldg(lp + 1);  // face4, face5, lo.x, lo.y
+        const float4 c = __ldg(lp + 2);  // lo.z, hi.x, hi.y, hi.z
+        const float box_lo[3] = {b.z, b.w, c.x};
+        const float box_hi[3] = {c.y, c.z, c.w};
+        uint32_t cell[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float centre = 0.5f * (box_lo[k] + box_hi[k]);
+            const float q = hmin(hmax((centre - lo[k]) / extent[k] * 1024.0f, 0.0f), 1023.0f);
+            cell[k] = (uint32_t)q;
+        }
+        const uint32_t key = morton30(cell[0], cell[1], cell[2]);
+        keys[i] = key;
+        counter[i] = 0;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) atomicAdd(&s_hist[p][(key >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) {
+        const uint32_t v = (&s_hist[0][0])[i];
+        if (v) atomicAdd(&hist[i], v);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Karras 2012 binary radix tree over the sorted keys; ties broken by sorted position.
+__device__ __forceinline__ int lt_delta(const uint32_t* __restrict__ keys, int i, int j, int n, uint32_t key_i)
+{
+    if (j < 0 || j >= n) return -1;
+    const uint32_t key_j = __ldg(keys + j);
+    if (key_i == key_j) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+    return __clz(key_i ^ key_j);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    lt_karras_kernel(const uint32_t* __restrict__ keys, int n, uint32_t* __restrict__ left,
+                     uint32_t* __restrict__ right, uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    if (i == 0) parent[0] = kNone;
+    const uint32_t key_i = __ldg(keys + i);
+    const int d = lt_delta(keys, i, i + 1, n, key_i) - lt_delta(keys, i, i - 1, n, key_i) >= 0 ? 1 : -1;
+    const int delta_min = lt_delta(keys, i, i - d, n, key_i);
+    int length_max = 2;
+    while (lt_delta(keys, i, i + length_max * d, n, key_i) > delta_min) length_max *= 2;
+    int length = 0;
+    for (int step = length_max / 2; step >= 1; step /= 2)
+        if (lt_delta(keys, i, i + (length + step) * d, n, key_i) > delta_min) length += step;
+    const int j = i + length * d;
+    const int delta_node = lt_delta(keys, i, j, n, key_i);
+    int split = 0;
+    int divisor = 2;
+    int step2 = (length + divisor - 1) / divisor;
+    for (;;) {
+        if (lt_delta(keys, i, i + (split + step2) * d, n, key_i) > delta_node) split += step2;
+        if (step2 == 1) break;
+        divisor *= 2;
+        step2 = (length + divisor - 1) / divisor;
+    }
+    const int gamma = i + split * d + min(d, 0);
+    const uint32_t l = min(i, j) == gamma ? (kChildLeafBit | (uint32_t)gamma) : (uint32_t)gamma;
+    const uint32_t r = max(i, j) == gamma + 1 ? (kChildLeafBit | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
+    left[i] = l;
+    right[i] = r;
+    if (l & kChildLeafBit) leaf_parent[l & ~kChildLeafBit] = (uint32_t)i;
+    else parent[l] = (uint32_t)i;
+    if (r & kChildLeafBit) leaf_parent[r & ~kChildLeafBit] = (uint32_t)i;
+    else parent[r] = (uint32_t)i;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
+// computes its summary from both children and goes on (acq_rel arrival counter).
+__device__ __forceinline__ LightSummary child_summary(uint32_t child, const uint32_t* __restrict__ values,
+                                                     const LightBvhLeaf* __restrict__ leaves,
+                                                     const LightSummary* aggregates)
+{
+    if (child & kChildLeafBit) return load_summary(&leaves[__ldg(values + (child & ~kChildLeafBit))].summary);
+    return load_summary_cg(aggregates + child);
+}
+
+__global__ void __launch_bounds__(kThreads)
+    lt_aggregate_kernel(uint32_t n, const uint32_t* __restrict__ values, const LightBvhLeaf* __restrict__ leaves,
+                        const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                        const uint32_t* __restrict__ parent, const uint32_t* __restrict__ leaf_parent,
+                        uint32_t* counter, LightSummary* aggregates, BuildControl* control)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    uint32_t node = __ldg(leaf_parent + j);
+    uint32_t depth = 0;
+    for (; depth < 128 && node != kNone; ++depth) {
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+        if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+        const LightSummary a = child_summary(__ldg(left + node), values, leaves, aggregates);
+        const LightSummary b = child_summary(__ldg(right + node), values, leaves, aggregates);
+        store_summary(aggregates + node, lt_union(a, b));
+        node = __ldg(parent + node);
+    }
+    if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Depth of every binary node (walk to the root) and the exclusive scan of the even-depth flags
+// (the 4-wide node index), single pass with a decoupled look-back over tiles of 256 nodes.
+__global__ void __launch_bounds__(kScanThreads)
+    lt_depth_scan_kernel(uint32_t n, const uint32_t* __restrict__ parent, uint32_t* __restrict__ depth_out,
+                         uint32_t* __restrict__ wide, uint32_t* scan_states, BuildControl* control)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[kScanThreads / 32];
+    __shared__ uint32_t s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(&control->scan_tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t i = tile * kScanThreads + threadIdx.x;
+    uint32_t flag = 0;
+    if (i + 1 < n) {
+        uint32_t d = 0;
+        uint32_t node = __ldg(parent + i);
+        for (uint32_t guard = 0; guard < 128 && node != kNone; ++guard) {
+            ++d;
+            node = __ldg(parent + node);
+        }
+        if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
+        depth_out[i] = d;
+        flag = (d & 1u) == 0 ? 1u : 0u;
+    }
+    uint32_t total;
+    const uint32_t local = block_exclusive_sum<kScanThreads>(flag, s_scan, total);
+    if (threadIdx.x == 0) {
+        uint32_t exclusive = 0;
+        uint32_t* state = scan_states + tile;
+        if (tile == 0) {
+            st_relaxed(state, kTileFlagPrefix | total);
+        } else {
+            st_relaxed(state, kTileFlagAggregate | total);
+            int64_t j = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                const uint32_t s = ld_relaxed(scan_states + j);
+                if ((s & ~kTileValueMask) == 0) {
+                    if (!spin_wait(spins)) {
+                        atomicOr(&control->status, kStatusLookbackTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                exclusive += s & kTileValueMask;
+                if (s & kTileFlagPrefix) break;
+                --j;
+            }
+            st_relaxed(state, kTileFlagPrefix | (exclusive + total));
+        }
+        s_prefix = exclusive;
+        if (tile == gridDim.x - 1) control->node_count = exclusive + total;
+    }
+    __syncthreads();
+    if (i + 1 < n) wide[i] = s_prefix + local;
+}
+
+// ---------------------------------------------------------------------------------------------
+// 4-wide collapse: one thread per binary node at even depth.
+__global__ void __launch_bounds__(kThreads)
+    lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
+                   const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                   const uint32_t* __restrict__ depth, const uint32_t* __restrict__ wide,
+                   const LightSummary* __restrict__ aggregates, LightBvhLeaf* leaves, LightBvhNode* nodes)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i + 1 >= n || (__ldg(depth + i) & 1u) != 0) return;
+    const uint32_t w = __ldg(wide + i);
+    if (w >= node_capacity) return;
+    uint32_t slots[4] = {kNone, kNone, kNone, kNone};
+    uint32_t count = 0;
+    const uint32_t children[2] = {__ldg(left + i), __ldg(right + i)};
+#pragma unroll
+    for (int c = 0; c < 2; ++c) {
+        const uint32_t child = children[c];
+        if (child & kChildLeafBit) {
+            slots[count++] = child;
+        } else {
+            slots[count++] = __ldg(left + child);
+            slots[count++] = __ldg(right + child);
+        }
+    }
+    LightBvhNode* node = nodes + w;
+    uint32_t words[4] = {kNone, kNone, kNone, kNone};
+    float faces[24];
+    float bounds[24];  // lo[4][3], then hi[4][3]
+#pragma unroll
+    for (uint32_t s = 0; s < 4; ++s) {
+        LightSummary sm;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) sm.face[f] = 0.0f;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sm.lo[k] = sm.hi[k] = 0.0f;
+        if (s < count) {
+            const uint32_t slot = slots[s];
+            if (slot & kChildLeafBit) {
+                const uint32_t leaf = __ldg(values + (slot & ~kChildLeafBit));
+                sm = load_summary(&leaves[leaf].summary);
+                words[s] = kChildLeafBit | leaf;
+                leaves[leaf].parent = (w << kParentSlotBits) | s;
+            } else {
+                sm = load_summary(aggregates + slot);
+                const uint32_t child_node = __ldg(wide + slot);
+                words[s] = child_node;
+                if (child_node < node_capacity)
+                    *reinterpret_cast<uint2*>(&nodes[child_node].parent) = make_uint2(w, s);
+            }
+        }
+#pragma unroll
+        for (int f = 0; f < 6; ++f) faces[6 * s + f] = sm.face[f];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            bounds[3 * s + k] = sm.lo[k];
+            bounds[12 + 3 * s + k] = sm.hi[k];
+        }
+    }
+    float4* q = reinterpret_cast<float4*>(node);
+#pragma unroll
+    for (int v = 0; v < 6; ++v) {
+        q[v] = make_float4(faces[4 * v], faces[4 * v + 1], faces[4 * v + 2], faces[4 * v + 3]);
+        q[6 + v] = make_float4(bounds[4 * v], bounds[4 * v + 1], bounds[4 * v + 2], bounds[4 * v + 3]);
+    }
+    *reinterpret_cast<uint4*>(node->child) = make_uint4(words[0], words[1], words[2], words[3]);
+    if (i == 0) *reinterpret_cast<uint2*>(&node->parent) = make_uint2(kNone, 0u);
+}
+
+// ---------------------------------------------------------------------------------------------
+// The header (one thread): root summary, counts, overflow; the one-leaf tree's single node.
+__global__ void lt_finish_kernel(uint32_t n, uint32_t found, uint32_t node_capacity, LightBvhLeaf* leaves,
+                                 LightBvhNode* nodes, const LightSummary* aggregates, LightTreeHeader* header,
+                                 LightTreeState* state, const BuildControl* control)
+{
+    LightSummary root;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) root.face[f] = 0.0f;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) root.lo[k] = root.hi[k] = 0.0f;
+    uint32_t root_index = kNone, node_count = 0, overflow = 0;
+    if (n == 1) {
+        root = load_summary_cg(&leaves[0].summary);
+        LightBvhNode* node = nodes;
+        float4* q = reinterpret_cast<float4*>(node);
+        for (int v = 0; v < 12; ++v) q[v] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (int f = 0; f < 6; ++f) node->child_face[0][f] = root.face[f];
+        for (int k = 0; k < 3; ++k) {
+            node->child_lo[0][k] = root.lo[k];
+            node->child_hi[0][k] = root.hi[k];
+        }
+        *reinterpret_cast<uint4*>(node->child) = make_uint4(kChildLeafBit, kNone, kNone, kNone);
+        *reinterpret_cast<uint2*>(&node->parent) = make_uint2(kNone, 0u);
+        leaves[0].parent = 0;
+        root_index = 0;
+        node_count = 1;
+    } else if (n >= 2) {
+        node_count = control->node_count;
+        if (node_count > node_capacity) {
+            overflow = 1;
+        } else {
+            root = load_summary_cg(aggregates);
+            root_index = 0;
+        }
+    }
+    store_summary(&header->summary, root);
+    *reinterpret_cast<uint4*>(&header->root) = make_uint4(root_index, overflow ? 0u : n, node_count, 0u);
+    float lo[3], hi[3];
+    decode_bounds(control, lo, hi);
+    state->building = 0;
+    state->leaves_found = found;
+    state->leaves_dropped = found - n;
+    state->builds += 1;
+    state->node_overflow = overflow;
+    state->status = control->status | (overflow ? kStatusNodeOverflow : 0u);
+    for (int k = 0; k < 3; ++k) {
+        state->bounds[k] = lo[k];
+        state->bounds[3 + k] = hi[k];
+    }
+}
+
+uint32_t grid_for(uint32_t n, uint32_t per_block, uint32_t cap)
+{
+    uint32_t g = (n + per_block - 1) / per_block;
+    if (g == 0) g = 1;
+    return g < cap ? g : cap;
+}
+
+uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t{255}; }
+
+}  // namespace
+
+uint64_t lt_buffer_bytes(uint32_t cap)
+{
+    const uint64_t c = cap < 2 ? 2 : cap;
+    uint64_t b = 0;
+    b += align256(c * sizeof(LightBvhLeaf));
+    b += align256(c * sizeof(LightBvhNode));  // node capacity = leaf capacity (>= n - 1 nodes)
+    b += align256(128);                       // header + state
+    b += 11 * align256(c * 4);                // keys, values, alt x2, left, right, parent, leaf_parent, counter, depth, wide
+    b += align256(c * sizeof(LightSummary));
+    b += align256(sizeof(BuildControl) + sort_scratch_words((uint32_t)c) * 4 + scan_tiles((uint32_t)c) * 4);
+    return b;
+}
+
+LightBvhBuffers lt_carve(void* base, uint32_t cap)
+{
+    const uint64_t c = cap < 2 ? 2 : cap;
+    LightBvhBuffers b;
+    b.leaf_capacity = cap;
+    b.node_capacity = (uint32_t)c;
+    char* p = static_cast<char*>(base);
+    auto take = [&](uint64_t bytes) {
+        char* q = p;
+        p += align256(bytes);
+        return q;
+    };
+    b.leaves = reinterpret_cast<LightBvhLeaf*>(take(c * sizeof(LightBvhLeaf)));
+    b.nodes = reinterpret_cast<LightBvhNode*>(take(c * sizeof(LightBvhNode)));
+    char* hs = take(128);
+    b.header = reinterpret_cast<LightTreeHeader*>(hs);
+    b.state = reinterpret_cast<LightTreeState*>(hs + 64);
+    b.keys = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.values = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.keys_alt = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.values_alt = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.left = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.right = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.parent = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.leaf_parent = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.counter = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.depth = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.wide = reinterpret_cast<uint32_t*>(take(c * 4));
+    b.aggregates = reinterpret_cast<LightSummary*>(take(c * sizeof(LightSummary)));
+    const uint64_t zero = sizeof(BuildControl) + sort_scratch_words((uint32_t)c) * 4 + scan_tiles((uint32_t)c) * 4;
+    char* z = take(zero);
+    b.control = reinterpret_cast<BuildControl*>(z);
+    b.sort_scratch = reinterpret_cast<uint32_t*>(z + sizeof(BuildControl));
+    b.zero_bytes = zero;
+    return b;
+}
+
+cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream)
+{
+    const uint32_t found = in.count;
+    const uint32_t n = found < b.leaf_capacity ? found : b.leaf_capacity;
+    // The scan states follow the sort scratch sized for this build's n.
+    const uint64_t sort_words = sort_scratch_words(n);
+    uint32_t* scan_states = b.sort_scratch + sort_words;
+    const uint64_t zero = sizeof(BuildControl) + sort_words * 4 + (uint64_t)scan_tiles(n) * 4;
+    cudaError_t e = cudaMemsetAsync(b.control, 0, zero, stream);
+    if (e != cudaSuccess) return e;
+    const uint32_t sms = 148;
+    if (n > 0) {
+        lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
+            in.records, n, in.record_group, in.record_entry, in.group_frames, b.leaves, b.control);
+        lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
+            b.leaves, n, b.control, b.keys, b.counter, b.sort_scratch);
+        onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
+                      stream);
+    }
+    if (n >= 2) {
+        const uint32_t nodes = n - 1;
+        lt_karras_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
+            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent);
+        lt_aggregate_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(
+            n, b.values, b.leaves, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.control);
+        lt_depth_scan_kernel<<<scan_tiles(nodes), kScanThreads, 0, stream>>>(n, b.parent, b.depth, b.wide,
+                                                                             scan_states, b.control);
+        lt_wide_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
+            n, b.node_capacity, b.values, b.left, b.right, b.depth, b.wide, b.aggregates, b.leaves, b.nodes);
+    }
+    lt_finish_kernel<<<1, 1, 0, stream>>>(n, found, b.node_capacity, b.leaves, b.nodes, b.aggregates, b.header,
+                                          b.state, b.control);
+    return cudaGetLastError();
+}
+
+}  // namespace cx

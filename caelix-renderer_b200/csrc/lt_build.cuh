@@ -1,0 +1,109 @@
+// The light BVH build on the GPU: brick light records -> world leaves -> Morton codes -> onesweep
+// radix sort -> Karras binary radix tree -> bottom-up aggregation -> depth parity + scan -> 4-wide
+// collapse -> header.
+//
+// Replaces the reference's per-tree dispatch sequence LightTree::RecordTree
+// (lib/src/light/light_tree_record.cpp:230-309, about 35 dependent dispatches with a barrier after
+// each) with 10 kernels and one memset, all on one stream (capturable in a CUDA graph):
+//   lt_emit_kernel        gather emit (caelix_light_gather_emit.hlsl:11-86) fused with the centre
+//                         bounds (caelix_light_bvh_bounds.hlsl:10-53): warp max-reductions of
+//                         order-preserving codes instead of a one-workgroup reduction
+//   lt_morton_kernel      Morton codes (caelix_light_bvh_morton.hlsl:6-28) fused with the digit
+//                         histograms of all four sort passes and the clear of the arrival counters
+//   onesweep_pass_kernel  x4 (radix_sort.cuh)
+//   lt_karras_kernel      caelix_light_bvh_karras.hlsl:8-96
+//   lt_aggregate_kernel   caelix_light_bvh_aggregate.hlsl:30-55 (acq_rel arrival counters)
+//   lt_depth_scan_kernel  caelix_light_bvh_depth.hlsl:7-30 fused with the scan of the even-depth
+//                         flags (decoupled look-back instead of a one-workgroup scan)
+//   lt_wide_kernel        caelix_light_bvh_wide.hlsl:10-100
+//   lt_finish_kernel      caelix_light_bvh_finish.hlsl:8-63
+// Every float operation is a single IEEE fp32 operation in the order of the HLSL source (the
+// library is compiled with --fmad=false), so the tree is bit-identical to the oracle's.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "cx_layout.h"
+
+namespace cx {
+
+// Per-tree build state, persistent across builds (LightTreeState, light_tree_layout.h:123-148).
+struct alignas(16) LightTreeState
+{
+    uint32_t building;
+    uint32_t leaves_found;
+    uint32_t leaves_dropped;
+    uint32_t builds;
+    uint32_t node_overflow;
+    uint32_t status;  // cx::kStatus* bits of the newest build
+    uint32_t pad0[2];
+    float bounds[6];  // centre bounds lo[3], hi[3]
+    uint32_t pad1[2];
+};
+static_assert(sizeof(LightTreeState) == 64);
+
+// The control words a build zeroes before its first kernel.
+struct BuildControl
+{
+    uint32_t bounds_code[6];  // [0..2] ~order(min centre), [3..5] order(max centre): atomicMax from 0
+    uint32_t status;
+    uint32_t node_count;         // the scan total of the even-depth flags
+    uint32_t scan_tile_counter;  // dynamic tile ids of lt_depth_scan_kernel
+    uint32_t pad[7];
+};
+static_assert(sizeof(BuildControl) == 64);
+
+// Device arrays of one tree and its build scratch (the kLtScratch* arrays of
+// light_tree_layout.h:392-423, here separate arrays).
+struct LightBvhBuffers
+{
+    uint32_t leaf_capacity = 0;
+    uint32_t node_capacity = 0;
+    LightBvhLeaf* leaves = nullptr;
+    LightBvhNode* nodes = nullptr;
+    LightTreeHeader* header = nullptr;  // header then LightTreeState, 128 bytes
+    LightTreeState* state = nullptr;
+    uint32_t* keys = nullptr;  // sorted Morton codes after the build
+    uint32_t* values = nullptr;
+    uint32_t* keys_alt = nullptr;
+    uint32_t* values_alt = nullptr;
+    uint32_t* left = nullptr;
+    uint32_t* right = nullptr;
+    uint32_t* parent = nullptr;
+    uint32_t* leaf_parent = nullptr;
+    uint32_t* counter = nullptr;
+    uint32_t* depth = nullptr;
+    uint32_t* wide = nullptr;
+    LightSummary* aggregates = nullptr;
+    BuildControl* control = nullptr;  // followed by the sort scratch, then the scan states
+    uint32_t* sort_scratch = nullptr;
+    uint32_t* scan_states = nullptr;
+    uint64_t zero_bytes = 0;  // bytes from `control` that a build clears
+};
+
+// Input of one build: `count` records (device), optional per-record group and entry words and
+// per-group frames (device; null: group 0, entry = record index, identity frame at origin 0).
+struct LightBvhInput
+{
+    const BrickLightRecord* records;
+    uint32_t count;
+    const uint32_t* record_group;
+    const uint32_t* record_entry;
+    const GroupFrame* group_frames;
+};
+
+constexpr int kScanThreads = 256;
+__host__ __device__ constexpr uint32_t scan_tiles(uint32_t n)
+{
+    return (n + kScanThreads - 1) / kScanThreads;
+}
+
+// Bytes of device memory for a leaf capacity (one allocation, carved by lt_carve).
+uint64_t lt_buffer_bytes(uint32_t leaf_capacity);
+// Carves the arrays of `leaf_capacity` leaves out of `base` (lt_buffer_bytes bytes, 256-aligned).
+LightBvhBuffers lt_carve(void* base, uint32_t leaf_capacity);
+// Records the build into `stream`. Returns the first CUDA launch error.
+cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream);
+
+}  // namespace cx

@@ -1,0 +1,192 @@
+// Kernels of the onesweep radix sort (radix_sort.cuh describes the algorithm).
+#include "cx_device.cuh"
+#include "radix_sort.cuh"
+
+namespace cx {
+
+struct SortPass
+{
+    const uint32_t* keys_in;
+    const uint32_t* values_in;  // nullptr: the value of element i is i
+    uint32_t* keys_out;
+    uint32_t* values_out;
+    uint32_t n;
+    uint32_t shift;
+    const uint32_t* counts;  // the 256 global digit counts of this pass
+    uint32_t* tile_counter;
+    uint32_t* tile_states;  // tiles * 256 words, zero
+    uint32_t* status;
+};
+
+namespace {
+
+__global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __restrict__ keys, uint32_t n,
+                                                              uint32_t* __restrict__ hist)
+{
+    __shared__ uint32_t s_hist[4][kRadix];
+    for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
+    __syncthreads();
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint32_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) atomicAdd(&s_hist[p][(k >> (8 * p)) & 255u], 1u);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) {
+        const uint32_t c = (&s_hist[0][0])[i];
+        if (c) atomicAdd(&hist[i], c);
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortPass a)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp_counts[kSortWarps][kRadix];  // counts, then exclusive offsets per warp
+    __shared__ uint32_t s_local[kRadix];                    // tile-local exclusive offset of each digit
+    __shared__ uint32_t s_dest[kRadix];                     // global destination base minus s_local
+    __shared__ uint32_t s_scan[kSortWarps];
+    __shared__ uint32_t s_keys[kSortTile];
+    __shared__ uint32_t s_values[kSortTile];
+
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    if (tid == 0) s_tile = atomicAdd(a.tile_counter, 1u);
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) s_warp_counts[w][tid] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t base = tile * kSortTile;
+    const uint32_t warp_base = base + warp * 32u * kSortKeysPerThread;
+
+    uint32_t key[kSortKeysPerThread];
+    uint32_t value[kSortKeysPerThread];
+    uint32_t rank[kSortKeysPerThread];
+#pragma unroll
+    for (int k = 0; k < kSortKeysPerThread; ++k) {
+        const uint32_t i = warp_base + k * 32u + lane;
+        const bool valid = i < a.n;
+        key[k] = valid ? __ldg(a.keys_in + i) : 0u;
+        value[k] = valid ? (a.values_in ? __ldg(a.values_in + i) : i) : 0u;
+    }
+    // Stable rank inside the warp: element (k, lane) precedes (k, lane + 1) and (k + 1, *).
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < kSortKeysPerThread; ++k) {
+        const uint32_t i = warp_base + k * 32u + lane;
+        const uint32_t digit = i < a.n ? (key[k] >> a.shift) & 255u : 256u + lane;  // invalid: alone
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
+        const uint32_t before = __popc(peers & lt);
+        uint32_t running = 0;
+        if (digit < 256u) running = s_warp_counts[warp][digit];
+        rank[k] = running + before;
+        __syncwarp();
+        if (digit < 256u && before == 0) s_warp_counts[warp][digit] = running + __popc(peers);
+        __syncwarp();
+    }
+    __syncthreads();
+
+    // Thread d owns digit d: per-warp exclusive offsets, the tile total, the look-back.
+    const uint32_t d = tid;
+    uint32_t total = 0;
+#pragma unroll
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = s_warp_counts[w][d];
+        s_warp_counts[w][d] = total;
+        total += c;
+    }
+    uint32_t* state = a.tile_states + (uint64_t)tile * kRadix + d;
+    uint32_t exclusive = 0;
+    if (tile == 0) {
+        st_relaxed(state, kTileFlagPrefix | total);
+    } else {
+        st_relaxed(state, kTileFlagAggregate | total);
+        int64_t j = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (j >= 0) {
+            const uint32_t s = ld_relaxed(a.tile_states + (uint64_t)j * kRadix + d);
+            if ((s & ~kTileValueMask) == 0) {
+                if (!spin_wait(spins)) {
+                    atomicOr(a.status, kStatusLookbackTimeout);
+                    break;
+                }
+                continue;
+            }
+            exclusive += s & kTileValueMask;
+            if (s & kTileFlagPrefix) break;
+            --j;
+        }
+        st_relaxed(state, kTileFlagPrefix | (exclusive + total));
+    }
+    uint32_t digit_total;
+    const uint32_t global_base = block_exclusive_sum<kSortThreads>(a.counts[d], s_scan, digit_total);
+    uint32_t tile_total;
+    const uint32_t local = block_exclusive_sum<kSortThreads>(total, s_scan, tile_total);
+    s_local[d] = local;
+    s_dest[d] = global_base + exclusive - local;
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < kSortKeysPerThread; ++k) {
+        const uint32_t i = warp_base + k * 32u + lane;
+        if (i < a.n) {
+            const uint32_t digit = (key[k] >> a.shift) & 255u;
+            const uint32_t at = s_local[digit] + s_warp_counts[warp][digit] + rank[k];
+            s_keys[at] = key[k];
+            s_values[at] = value[k];
+        }
+    }
+    __syncthreads();
+    const uint32_t count = a.n - base < (uint32_t)kSortTile ? a.n - base : (uint32_t)kSortTile;
+    for (uint32_t j = tid; j < count; j += kSortThreads) {
+        const uint32_t k = s_keys[j];
+        const uint32_t dest = s_dest[(k >> a.shift) & 255u] + j;
+        a.keys_out[dest] = k;
+        a.values_out[dest] = s_values[j];
+    }
+}
+
+}  // namespace
+
+void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream)
+{
+    if (n == 0) return;
+    radix_histogram_kernel<<<grid, 256, 0, stream>>>(keys, n, hist);
+}
+
+void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b,
+                          uint32_t n, bool identity_values, uint32_t* scratch, uint32_t* status,
+                          cudaStream_t stream)
+{
+    if (n == 0) return;
+    const uint32_t tiles = sort_tiles(n);
+    uint32_t* hist = scratch;
+    uint32_t* counters = scratch + 4 * kRadix;
+    uint32_t* states = counters + 4;
+    uint32_t* kin = keys_a;
+    uint32_t* vin = values_a;
+    uint32_t* kout = keys_b;
+    uint32_t* vout = values_b;
+    for (uint32_t pass = 0; pass < 4; ++pass) {
+        SortPass p;
+        p.keys_in = kin;
+        p.values_in = (pass == 0 && identity_values) ? nullptr : vin;
+        p.keys_out = kout;
+        p.values_out = vout;
+        p.n = n;
+        p.shift = 8 * pass;
+        p.counts = hist + kRadix * pass;
+        p.tile_counter = counters + pass;
+        p.tile_states = states + (uint64_t)pass * tiles * kRadix;
+        p.status = status;
+        onesweep_pass_kernel<<<tiles, kSortThreads, 0, stream>>>(p);
+        uint32_t* t = kin;
+        kin = kout;
+        kout = t;
+        t = vin;
+        vin = vout;
+        vout = t;
+    }
+}
+
+}  // namespace cx

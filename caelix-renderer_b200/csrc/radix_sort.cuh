@@ -1,0 +1,61 @@
+// Onesweep LSD radix sort of (u32 key, u32 value) pairs: 8-bit digits, 4 passes over 32-bit keys.
+//
+// Replaces the reference's sort (shaders/light/bvh/caelix_light_bvh_sort.hlsl,
+// caelix_light_bvh_sort_histogram.hlsl:8-38, caelix_light_bvh_sort_scatter.hlsl:10-78, driven by
+// lib/src/light/light_tree_record.cpp:282-302: 4-bit digits, 8 passes of histogram + one-workgroup
+// scan + scatter). Both are stable LSD sorts of the same keys, so the permutation is the same.
+//
+// One pass is one kernel (no separate histogram or scan launch):
+//   * the digit counts of all four passes come from one upsweep (the caller's key producer, or
+//     radix_histogram_kernel), so a pass only needs its own 256 global counts;
+//   * a CTA takes the next tile id from an atomic counter, loads 4096 keys warp-striped
+//     (coalesced 128-byte rows), ranks them stably inside each warp with __match_any_sync peers,
+//     and publishes its per-digit counts in the tile status words;
+//   * the per-digit exclusive prefix over earlier tiles comes from a decoupled look-back over
+//     those status words (one thread per digit, bounded spin: a timeout sets a status bit instead
+//     of hanging);
+//   * the tile is staged in shared memory in digit order and written out in runs per digit.
+#pragma once
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "cx_layout.h"
+
+namespace cx {
+
+constexpr int kSortThreads = 256;
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kSortKeysPerThread = 16;
+constexpr int kSortTile = kSortThreads * kSortKeysPerThread;  // 4096
+constexpr int kRadix = 256;
+constexpr uint32_t kTileFlagAggregate = 1u << 30;
+constexpr uint32_t kTileFlagPrefix = 2u << 30;
+constexpr uint32_t kTileValueMask = (1u << 30) - 1u;
+
+__host__ __device__ constexpr uint32_t sort_tiles(uint32_t n)
+{
+    return (n + kSortTile - 1) / kSortTile;
+}
+
+// Scratch words one sort of n elements needs (all of them zero before the first pass):
+//   histogram  4 * 256 digit counts
+//   counters   4 tile-id counters (one per pass)
+//   states     4 * tiles * 256 look-back status words
+__host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n)
+{
+    return 4ull * kRadix + 4ull + 4ull * sort_tiles(n) * kRadix;
+}
+
+// Accumulates the 256-bin histograms of all four digits of keys[0 .. n) into hist[4][256].
+void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream);
+
+// Launches the four passes: keys_a/values_a hold the input and, after the even number of passes,
+// the output; keys_b/values_b are the ping-pong buffers. `identity_values`: the input values are
+// 0 .. n-1 and are not read (values_a is still written). `scratch` holds sort_scratch_words(n)
+// words, already zero, with the histograms of all four digits in its first 1024 words
+// (radix_histogram or a fused producer).
+void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
+                   bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream);
+
+}  // namespace cx

@@ -1,0 +1,120 @@
+/* CPU oracle of the scene-flush and trace hot path of the Caelix voxel renderer.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is a scalar C restatement of the reference's HLSL kernels, used
+ * as the checker by the parity tests, by the smoke check and as the timed CPU baseline of the
+ * benchmark. The product library never links, loads or calls it.
+ *
+ * Layouts restate lib/src/light/light_tree_layout.h of the reference byte for byte (the structs
+ * below carry the same offsets; tests/test_layout.py compares them with the reference header
+ * compiled by oracle/ref_layout.mk). Arithmetic is IEEE fp32 without contraction (built with
+ * -ffp-contract=off), in the operation order of the HLSL source.
+ */
+#ifndef CAELIX_ORACLE_H
+#define CAELIX_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OC_NONE 0xFFFFFFFFu
+#define OC_CHILD_LEAF_BIT 0x80000000u
+
+/* LightSummary (light_tree_layout.h:89-102): 48 bytes. */
+typedef struct oc_summary {
+    float face[6];
+    float lo[3];
+    float hi[3];
+} oc_summary;
+
+/* BrickLightRecordHeader (light_tree_layout.h:298-323): 48 bytes. */
+typedef struct oc_record {
+    float face[6];
+    uint32_t box_lo; /* packed group-local voxel x | y << 10 | z << 20, inclusive */
+    uint32_t box_hi; /* exclusive */
+    uint32_t pos;
+    uint32_t entry_count;
+    uint32_t counts_lo;
+    uint32_t counts_hi;
+} oc_record;
+
+/* LightBvhLeaf (light_tree_layout.h:338-354): 64 bytes. */
+typedef struct oc_leaf {
+    oc_summary s;
+    uint32_t group;
+    uint32_t entry;
+    uint32_t pad;
+    uint32_t parent; /* node << 2 | slot */
+} oc_leaf;
+
+/* LightBvhNode (light_tree_layout.h:359-389): 224 bytes. */
+typedef struct oc_node {
+    float child_face[4][6];
+    float child_lo[4][3];
+    float child_hi[4][3];
+    uint32_t child[4];
+    uint32_t parent;
+    uint32_t parent_slot;
+    uint32_t pad[2];
+} oc_node;
+
+/* LightTreeHeader (light_tree_layout.h:105-121): 64 bytes. */
+typedef struct oc_header {
+    oc_summary s;
+    uint32_t root;
+    uint32_t leaf_count;
+    uint32_t node_count;
+    uint32_t pad;
+} oc_header;
+
+/* The frame a record's group-local box is moved to world space with (the group's voxel origin
+ * and its entity's object-to-world rows, caelix_light_tree_layout.hlsl:409-433). */
+typedef struct oc_frame {
+    float origin[3];
+    float rot[9]; /* row-major rows */
+    float trans[3];
+} oc_frame;
+
+/* Every array the build writes, each of leaf_capacity elements unless stated. The build
+ * scratch arrays of light_tree_layout.h:392-423. */
+typedef struct oc_build_out {
+    oc_leaf* leaves;         /* [leaf_capacity] */
+    oc_node* nodes;          /* [node_capacity] */
+    oc_header* header;       /* [1] */
+    uint32_t* keys;          /* sorted Morton codes */
+    uint32_t* values;        /* sorted leaf indices */
+    uint32_t* left;          /* binary node children (OC_CHILD_LEAF_BIT: sorted leaf position) */
+    uint32_t* right;
+    uint32_t* parent;        /* binary node parent, OC_NONE = root */
+    uint32_t* leaf_parent;   /* binary parent of the leaf at each sorted position */
+    uint32_t* depth;         /* binary node depth */
+    uint32_t* wide;          /* 4-wide node index of an even-depth binary node (the scan) */
+    oc_summary* aggregates;  /* binary node summaries */
+    float* bounds;           /* [6] centre bounds lo[3], hi[3] */
+    uint32_t* node_overflow; /* [1] */
+} oc_build_out;
+
+/* 30-bit Morton code of a cell (caelix_light_tree_layout.hlsl:247-261). */
+uint32_t oc_morton(uint32_t x, uint32_t y, uint32_t z);
+
+/* Stable LSD radix sort of (key, value) pairs by the 32-bit key, 8-bit digits, 4 passes. */
+void oc_radix_sort_pairs(uint32_t* keys, uint32_t* values, uint32_t n);
+
+/* The light BVH build of one tree over `n` brick light records (leaf i = record i):
+ * gather emit, centre bounds, Morton codes, radix sort, Karras, aggregation, depth, wide
+ * collapse, finish. rec_group / rec_entry give each leaf's (group, entry) words and
+ * group_frames the frame of every group (rec_group NULL: group 0, entry i, identity frame at
+ * origin 0). Returns 0, or -1 when a depth guard was exceeded. */
+int oc_lt_build(const oc_record* records, uint32_t n, const uint32_t* rec_group,
+                const uint32_t* rec_entry, const oc_frame* group_frames, uint32_t leaf_capacity,
+                uint32_t node_capacity, const oc_build_out* out);
+
+/* The importance of a summary for a point receiver x with unit normal n (0: no surface),
+ * caelix_light_tree.hlsl:114-160. */
+float oc_importance(const float x[3], const float n[3], const float lo[3], const float hi[3],
+                    const float face[6]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
