@@ -57,7 +57,7 @@ class CaelixLightBvhInput(C.Structure):
     _fields_ = [
         ("records", C.c_uint64),
         ("count", C.c_uint32),
-        ("reserved", C.c_uint32),
+        ("group_count", C.c_uint32),
         ("record_group", C.c_uint64),
         ("record_entry", C.c_uint64),
         ("group_frames", C.c_uint64),
@@ -223,8 +223,12 @@ class LightBvh:
         except Exception:
             pass
 
-    def build(self, records, count: int, record_group=None, record_entry=None, group_frames=None, stream: int = 0):
-        inp = CaelixLightBvhInput(_ptr(records), count, 0, _ptr(record_group), _ptr(record_entry), _ptr(group_frames))
+    def build(self, records, count: int, record_group=None, record_entry=None, group_frames=None, group_count=None,
+              stream: int = 0):
+        if group_frames is not None and group_count is None:
+            raise ValueError("group_count is required with group_frames")
+        inp = CaelixLightBvhInput(_ptr(records), count, group_count or 0, _ptr(record_group), _ptr(record_entry),
+                                  _ptr(group_frames))
         self.L.check(self.L.lib.caelix_light_bvh_build(self.handle, C.byref(inp), stream), "caelix_light_bvh_build")
 
     def view(self) -> CaelixLightBvhView:

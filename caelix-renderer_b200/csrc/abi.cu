@@ -217,7 +217,7 @@ CAELIX_API void caelix_light_bvh_destroy(CaelixLightBvh* bvh)
 CAELIX_API CaelixResult caelix_light_bvh_build(CaelixLightBvh* bvh, const CaelixLightBvhInput* input, uint64_t stream)
 {
     CAELIX_GUARD_BEGIN
-    if (!bvh || !input || input->reserved != 0 || (input->count > 0 && !input->records))
+    if (!bvh || !input || (input->count > 0 && !input->records) || (input->group_count > 0) != (input->group_frames != nullptr))
         return CAELIX_ERROR_INVALID_ARGUMENT;
     if ((reinterpret_cast<uintptr_t>(input->records) & 15u) != 0) {
         log(CAELIX_LOG_ERROR, "caelix_light_bvh_build: records must be 16-byte aligned");
@@ -235,6 +235,7 @@ CAELIX_API CaelixResult caelix_light_bvh_build(CaelixLightBvh* bvh, const Caelix
     in.record_group = input->record_group;
     in.record_entry = input->record_entry;
     in.group_frames = reinterpret_cast<const cx::GroupFrame*>(input->group_frames);
+    in.group_count = input->group_count;
     cudaEventRecord(bvh->start, s);
     const cudaError_t e = cx::lt_build(bvh->buffers, in, s);
     cudaEventRecord(bvh->stop, s);

@@ -89,7 +89,7 @@ __device__ __forceinline__ uint32_t morton30(uint32_t x, uint32_t y, uint32_t z)
 __global__ void __launch_bounds__(kThreads)
     lt_emit_kernel(const BrickLightRecord* __restrict__ records, uint32_t n,
                    const uint32_t* __restrict__ record_group, const uint32_t* __restrict__ record_entry,
-                   const GroupFrame* __restrict__ frames, LightBvhLeaf* __restrict__ leaves,
+                   const GroupFrame* __restrict__ frames, uint32_t frame_count, LightBvhLeaf* __restrict__ leaves,
                    BuildControl* __restrict__ control)
 {
     uint32_t lo_code[3] = {0, 0, 0};  // ~order(centre), max-reduced
@@ -113,7 +113,8 @@ __global__ void __launch_bounds__(kThreads)
         float origin[3] = {0.0f, 0.0f, 0.0f};
         float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
         float t[3] = {0.0f, 0.0f, 0.0f};
-        if (frames) {
+        if (frames && g >= frame_count) atomicOr(&control->status, kStatusBadGroup);
+        if (frames && g < frame_count) {
             const GroupFrame* f = frames + g;
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
@@ -572,7 +573,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     const uint32_t sms = 148;
     if (n > 0) {
         lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
-            in.records, n, in.record_group, in.record_entry, in.group_frames, b.leaves, b.control);
+            in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves, b.control);
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
             b.leaves, n, b.control, b.keys, b.counter, b.sort_scratch);
         onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,

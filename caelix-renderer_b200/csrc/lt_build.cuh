@@ -83,7 +83,8 @@ struct LightBvhBuffers
 };
 
 // Input of one build: `count` records (device), optional per-record group and entry words and
-// per-group frames (device; null: group 0, entry = record index, identity frame at origin 0).
+// group_count per-group frames (device; null: group 0, entry = record index, identity frame at
+// origin 0).
 struct LightBvhInput
 {
     const BrickLightRecord* records;
@@ -91,6 +92,7 @@ struct LightBvhInput
     const uint32_t* record_group;
     const uint32_t* record_entry;
     const GroupFrame* group_frames;
+    uint32_t group_count;
 };
 
 constexpr int kScanThreads = 256;

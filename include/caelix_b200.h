@@ -124,13 +124,14 @@ typedef struct CaelixGroupFrame
 
 /* One build's input (device pointers). Leaf i is record i (the reference's gather order,
    caelix_light_gather_emit.hlsl:66-85). record_group / record_entry: the (group, entry) words
-   of each leaf; group_frames: one frame per group. All three NULL: group 0, entry i, identity
-   frame at origin 0. */
+   of each leaf; group_frames: group_count frames, one per group (a record whose group is not
+   below group_count is emitted with the identity frame at origin 0 and sets a device status
+   bit). All three NULL: group 0, entry i, identity frame at origin 0. */
 typedef struct CaelixLightBvhInput
 {
     const CaelixBrickLightRecord* records;
     uint32_t count;
-    uint32_t reserved; /* must be 0 */
+    uint32_t group_count; /* frames in group_frames; 0 when it is NULL */
     const uint32_t* record_group;
     const uint32_t* record_entry;
     const CaelixGroupFrame* group_frames;

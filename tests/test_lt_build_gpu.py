@@ -26,7 +26,8 @@ def gpu_build(dev, rec, group=None, frames=None, capacity=None):
     d_rec = gpu_util.to_device(rec)
     d_group = gpu_util.to_device(group) if group is not None else None
     d_frames = gpu_util.to_device(frames) if frames is not None else None
-    bvh.build(d_rec, n, record_group=d_group, group_frames=d_frames)
+    bvh.build(d_rec, n, record_group=d_group, group_frames=d_frames,
+              group_count=len(frames) if frames is not None else None)
     stats = bvh.stats()
     v = bvh.view()
     m = min(n, v.leaf_capacity)
