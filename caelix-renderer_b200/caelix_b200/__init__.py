@@ -86,6 +86,8 @@ class CaelixLightBvhStats(C.Structure):
         ("status", C.c_uint32),
         ("bounds", C.c_float * 6),
         ("gpu_ms", C.c_float),
+        ("kernel_launches", C.c_uint32),
+        ("stage_ms", C.c_float * 7),
         ("pad", C.c_uint32),
     ]
 
@@ -133,11 +135,12 @@ class Library:
         L.caelix_light_bvh_build.argtypes = [vp, C.POINTER(CaelixLightBvhInput), C.c_uint64]
         L.caelix_light_bvh_get_view.argtypes = [vp, C.POINTER(CaelixLightBvhView)]
         L.caelix_light_bvh_get_stats.argtypes = [vp, C.POINTER(CaelixLightBvhStats)]
+        L.caelix_light_bvh_set_profiling.argtypes = [vp, C.c_uint32]
         L.caelix_radix_sort_pairs.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64]
         for name in (
             "caelix_device_create", "caelix_device_check", "caelix_light_bvh_create",
             "caelix_light_bvh_build", "caelix_light_bvh_get_view", "caelix_light_bvh_get_stats",
-            "caelix_radix_sort_pairs",
+            "caelix_radix_sort_pairs", "caelix_light_bvh_set_profiling",
         ):
             getattr(L, name).restype = C.c_int
         L.caelix_set_log_callback(self._callback, None)
@@ -230,6 +233,10 @@ class LightBvh:
         inp = CaelixLightBvhInput(_ptr(records), count, group_count or 0, _ptr(record_group), _ptr(record_entry),
                                   _ptr(group_frames))
         self.L.check(self.L.lib.caelix_light_bvh_build(self.handle, C.byref(inp), stream), "caelix_light_bvh_build")
+
+    def set_profiling(self, enabled: bool):
+        self.L.check(self.L.lib.caelix_light_bvh_set_profiling(self.handle, 1 if enabled else 0),
+                     "caelix_light_bvh_set_profiling")
 
     def view(self) -> CaelixLightBvhView:
         v = CaelixLightBvhView()

@@ -91,7 +91,11 @@ struct CaelixLightBvh
     cudaStream_t last_stream = nullptr;
     cudaEvent_t start = nullptr;
     cudaEvent_t stop = nullptr;
+    cudaEvent_t stage[cx::kBuildStages + 1] = {};
+    bool profiling = false;
     bool built = false;
+    bool profiled = false;
+    uint32_t launches = 0;
 };
 
 using cx::log;
@@ -210,6 +214,8 @@ CAELIX_API void caelix_light_bvh_destroy(CaelixLightBvh* bvh)
     cudaSetDevice(bvh->device->ordinal);
     if (bvh->start) cudaEventDestroy(bvh->start);
     if (bvh->stop) cudaEventDestroy(bvh->stop);
+    for (cudaEvent_t ev : bvh->stage)
+        if (ev) cudaEventDestroy(ev);
     cudaFree(bvh->memory);
     delete bvh;
 }
@@ -237,11 +243,29 @@ CAELIX_API CaelixResult caelix_light_bvh_build(CaelixLightBvh* bvh, const Caelix
     in.group_frames = reinterpret_cast<const cx::GroupFrame*>(input->group_frames);
     in.group_count = input->group_count;
     cudaEventRecord(bvh->start, s);
-    const cudaError_t e = cx::lt_build(bvh->buffers, in, s);
+    const cudaError_t e = cx::lt_build(bvh->buffers, in, s, bvh->profiling ? bvh->stage : nullptr);
     cudaEventRecord(bvh->stop, s);
     bvh->last_stream = s;
     bvh->built = true;
+    bvh->profiled = bvh->profiling;
+    bvh->launches = cx::lt_kernel_launches(std::min(input->count, bvh->buffers.leaf_capacity));
     return cx::cuda_result(e, "caelix_light_bvh_build");
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_light_bvh_set_profiling(CaelixLightBvh* bvh, uint32_t enabled)
+{
+    CAELIX_GUARD_BEGIN
+    if (!bvh || enabled > 1) return CAELIX_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(bvh->device->ordinal);
+    if (enabled && !bvh->stage[0]) {
+        for (cudaEvent_t& ev : bvh->stage) {
+            const cudaError_t e = cudaEventCreate(&ev);
+            if (e != cudaSuccess) return cx::cuda_result(e, "caelix_light_bvh_set_profiling");
+        }
+    }
+    bvh->profiling = enabled != 0;
+    return CAELIX_OK;
     CAELIX_GUARD_END
 }
 
@@ -293,6 +317,11 @@ CAELIX_API CaelixResult caelix_light_bvh_get_stats(CaelixLightBvh* bvh, CaelixLi
     std::memcpy(out->bounds, st.bounds, sizeof(out->bounds));
     float ms = 0.0f;
     if (cudaEventElapsedTime(&ms, bvh->start, bvh->stop) == cudaSuccess) out->gpu_ms = ms;
+    out->kernel_launches = bvh->launches;
+    if (bvh->profiled) {
+        for (int k = 0; k < cx::kBuildStages; ++k)
+            if (cudaEventElapsedTime(&ms, bvh->stage[k], bvh->stage[k + 1]) == cudaSuccess) out->stage_ms[k] = ms;
+    }
     return cx::status_result(st.status & ~cx::kStatusNodeOverflow, "caelix_light_bvh_build");
     CAELIX_GUARD_END
 }

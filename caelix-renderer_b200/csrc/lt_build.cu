@@ -560,10 +560,14 @@ LightBvhBuffers lt_carve(void* base, uint32_t cap)
     return b;
 }
 
-cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream)
+cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream, cudaEvent_t* stage)
 {
     const uint32_t found = in.count;
     const uint32_t n = found < b.leaf_capacity ? found : b.leaf_capacity;
+    auto mark = [&](int k) {
+        if (stage) cudaEventRecord(stage[k], stream);
+    };
+    mark(0);
     // The scan states follow the sort scratch sized for this build's n.
     const uint64_t sort_words = sort_scratch_words(n);
     uint32_t* scan_states = b.sort_scratch + sort_words;
@@ -574,25 +578,47 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     if (n > 0) {
         lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
             in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves, b.control);
+        mark(1);
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
             b.leaves, n, b.control, b.keys, b.counter, b.sort_scratch);
+        mark(2);
         onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
                       stream);
+        mark(3);
+    } else {
+        mark(1);
+        mark(2);
+        mark(3);
     }
     if (n >= 2) {
         const uint32_t nodes = n - 1;
         lt_karras_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
             b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent);
+        mark(4);
         lt_aggregate_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(
             n, b.values, b.leaves, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.control);
+        mark(5);
         lt_depth_scan_kernel<<<scan_tiles(nodes), kScanThreads, 0, stream>>>(n, b.parent, b.depth, b.wide,
                                                                              scan_states, b.control);
+        mark(6);
         lt_wide_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
             n, b.node_capacity, b.values, b.left, b.right, b.depth, b.wide, b.aggregates, b.leaves, b.nodes);
+    } else {
+        mark(4);
+        mark(5);
+        mark(6);
     }
     lt_finish_kernel<<<1, 1, 0, stream>>>(n, found, b.node_capacity, b.leaves, b.nodes, b.aggregates, b.header,
                                           b.state, b.control);
+    mark(7);
     return cudaGetLastError();
+}
+
+uint32_t lt_kernel_launches(uint32_t n)
+{
+    if (n == 0) return 1;
+    if (n == 1) return 7;
+    return 11;
 }
 
 }  // namespace cx

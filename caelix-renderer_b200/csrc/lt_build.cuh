@@ -105,7 +105,14 @@ __host__ __device__ constexpr uint32_t scan_tiles(uint32_t n)
 uint64_t lt_buffer_bytes(uint32_t leaf_capacity);
 // Carves the arrays of `leaf_capacity` leaves out of `base` (lt_buffer_bytes bytes, 256-aligned).
 LightBvhBuffers lt_carve(void* base, uint32_t leaf_capacity);
-// Records the build into `stream`. Returns the first CUDA launch error.
-cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream);
+// Stages of a build that lt_build can bracket with events: stage[k] is recorded after stage k - 1
+// (stage[0] before the first command): emit+bounds, morton+histograms, sort (4 passes), karras,
+// aggregate, depth+scan, wide+finish.
+constexpr int kBuildStages = 7;
+// Records the build into `stream`; `stage` (null, or kBuildStages + 1 events) brackets its stages.
+// Returns the first CUDA launch error.
+cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStream_t stream, cudaEvent_t* stage);
+// Kernels one build of n leaves launches.
+uint32_t lt_kernel_launches(uint32_t n);
 
 }  // namespace cx

@@ -188,8 +188,17 @@ typedef struct CaelixLightBvhStats
     uint32_t status;         /* device status bits of the build (0 = none) */
     float bounds[6];         /* leaf centre bounds lo[3], hi[3] */
     float gpu_ms;            /* device time of the newest build (events around it) */
+    uint32_t kernel_launches; /* kernels the newest build launched */
+    float stage_ms[7];       /* with profiling on (caelix_light_bvh_set_profiling): device time of the
+                                stages emit+bounds, morton+histograms, radix sort (4 passes), karras,
+                                aggregate, depth+scan, wide+finish; 0 otherwise */
     uint32_t pad;
 } CaelixLightBvhStats;
+
+/* Turns per-stage device timing of the following builds on (1) or off (0, the default): events
+   between the stages, reported in CaelixLightBvhStats::stage_ms. Replaces the per-pass GpuTimer
+   queries of the reference (lib/src/rhi/gpu_timer.h:9-82). */
+CAELIX_API CaelixResult caelix_light_bvh_set_profiling(CaelixLightBvh* bvh, uint32_t enabled);
 
 /* Synchronizes the stream of the newest build and fills *out. Returns CAELIX_ERROR_DEVICE_STATUS
    when the build's status word is not 0 (a bounded look-back gave up, a depth guard was hit, or the
