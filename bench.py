@@ -218,7 +218,7 @@ def run_build(args, world, rank, local):
     stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
 
-    rec, group, frames = workloads.brick_light_records(N_LEAVES, grid_bricks=1024, group_shift=4)
+    rec, group, frames = workloads.brick_light_records(args.records, grid_bricks=1024, group_shift=4)
     n = len(rec)
     d_rec = torch.from_numpy(rec.view(np.uint8)).cuda()
     d_group = torch.from_numpy(group.view(np.int32)).cuda()
@@ -389,6 +389,7 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["build"], default="build")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

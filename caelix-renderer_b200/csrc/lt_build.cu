@@ -201,10 +201,12 @@ __device__ __forceinline__ void decode_bounds(const BuildControl* control, float
 }
 
 // ---------------------------------------------------------------------------------------------
-// Morton codes (value = leaf index) + the four digit histograms + clearing the arrival counters.
+// Morton codes (value = leaf index) + the four digit histograms + clearing the arrival counters
+// and the range-count differences.
 __global__ void __launch_bounds__(kThreads)
     lt_morton_kernel(const LightBvhLeaf* __restrict__ leaves, uint32_t n, const BuildControl* __restrict__ control,
-                     uint32_t* __restrict__ keys, uint32_t* __restrict__ counter, uint32_t* __restrict__ hist)
+                     uint32_t* __restrict__ keys, uint32_t* __restrict__ counter, uint32_t* __restrict__ cover,
+                     uint32_t* __restrict__ hist)
 {
     __shared__ uint32_t s_hist[4][kRadix];
     for (int i = threadIdx.x; i < 4 * kRadix; i += blockDim.x) (&s_hist[0][0])[i] = 0;
@@ -230,6 +232,7 @@ __global__ void __launch_bounds__(kThreads)
         const uint32_t key = morton30(cell[0], cell[1], cell[2]);
         keys[i] = key;
         counter[i] = 0;
+        cover[i] = 0;
 #pragma unroll
         for (int p = 0; p < 4; ++p) atomicAdd(&s_hist[p][(key >> (8 * p)) & 255u], 1u);
     }
@@ -241,7 +244,9 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Karras 2012 binary radix tree over the sorted keys; ties broken by sorted position.
+// Karras 2012 binary radix tree over the sorted keys; ties broken by sorted position. Also the
+// range-count differences: node i covers the leaf boundaries [a, b) of its range [a, b], so
+// cover[a] += 1, cover[b] -= 1 (their prefix sum counts the nodes over every boundary).
 __device__ __forceinline__ int lt_delta(const uint32_t* __restrict__ keys, int i, int j, int n, uint32_t key_i)
 {
     if (j < 0 || j >= n) return -1;
@@ -252,7 +257,8 @@ __device__ __forceinline__ int lt_delta(const uint32_t* __restrict__ keys, int i
 
 __global__ void __launch_bounds__(kThreads)
     lt_karras_kernel(const uint32_t* __restrict__ keys, int n, uint32_t* __restrict__ left,
-                     uint32_t* __restrict__ right, uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent)
+                     uint32_t* __restrict__ right, uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent,
+                     uint32_t* __restrict__ cover)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -277,180 +283,288 @@ __global__ void __launch_bounds__(kThreads)
         step2 = (length + divisor - 1) / divisor;
     }
     const int gamma = i + split * d + min(d, 0);
-    const uint32_t l = min(i, j) == gamma ? (kChildLeafBit | (uint32_t)gamma) : (uint32_t)gamma;
-    const uint32_t r = max(i, j) == gamma + 1 ? (kChildLeafBit | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
+    const int a = min(i, j);
+    const int b = max(i, j);
+    const uint32_t l = a == gamma ? (kChildLeafBit | (uint32_t)gamma) : (uint32_t)gamma;
+    const uint32_t r = b == gamma + 1 ? (kChildLeafBit | (uint32_t)(gamma + 1)) : (uint32_t)(gamma + 1);
     left[i] = l;
     right[i] = r;
     if (l & kChildLeafBit) leaf_parent[l & ~kChildLeafBit] = (uint32_t)i;
     else parent[l] = (uint32_t)i;
     if (r & kChildLeafBit) leaf_parent[r & ~kChildLeafBit] = (uint32_t)i;
     else parent[r] = (uint32_t)i;
+    atomicAdd(cover + a, 1u);
+    atomicAdd(cover + b, 0xFFFFFFFFu);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
-// computes its summary from both children and goes on (acq_rel arrival counter).
-__device__ __forceinline__ LightSummary child_summary(uint32_t child, const uint32_t* __restrict__ values,
-                                                     const LightBvhLeaf* __restrict__ leaves,
-                                                     const LightSummary* aggregates)
+// computes its summary from both children and goes on (acq_rel arrival counter). Leaf summaries
+// come from the sorted copy (coalesced), node summaries are 64-byte slots (full-sector writes).
+__device__ __forceinline__ LightSummary child_summary(uint32_t child, const LightSummary* __restrict__ sorted,
+                                                     const AggregateSlot* aggregates)
 {
-    if (child & kChildLeafBit) return load_summary(&leaves[__ldg(values + (child & ~kChildLeafBit))].summary);
-    return load_summary_cg(aggregates + child);
+    if (child & kChildLeafBit) return load_summary(sorted + (child & ~kChildLeafBit));
+    return load_summary_cg(&aggregates[child].summary);
+}
+
+__device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
+{
+    float4* q = reinterpret_cast<float4*>(p);
+    q[0] = make_float4(s.face[0], s.face[1], s.face[2], s.face[3]);
+    q[1] = make_float4(s.face[4], s.face[5], s.lo[0], s.lo[1]);
+    q[2] = make_float4(s.lo[2], s.hi[0], s.hi[1], s.hi[2]);
+    q[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
 __global__ void __launch_bounds__(kThreads)
-    lt_aggregate_kernel(uint32_t n, const uint32_t* __restrict__ values, const LightBvhLeaf* __restrict__ leaves,
-                        const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                        const uint32_t* __restrict__ parent, const uint32_t* __restrict__ leaf_parent,
-                        uint32_t* counter, LightSummary* aggregates, BuildControl* control)
+    lt_aggregate_kernel(uint32_t n, const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
+                        const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
+                        const uint32_t* __restrict__ leaf_parent, uint32_t* counter, AggregateSlot* aggregates,
+                        BuildControl* control)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
     uint32_t node = __ldg(leaf_parent + j);
     uint32_t depth = 0;
     for (; depth < 128 && node != kNone; ++depth) {
+        const uint32_t l = __ldg(left + node);
+        const uint32_t r = __ldg(right + node);
+        const uint32_t up = __ldg(parent + node);
         cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
         if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-        const LightSummary a = child_summary(__ldg(left + node), values, leaves, aggregates);
-        const LightSummary b = child_summary(__ldg(right + node), values, leaves, aggregates);
-        store_summary(aggregates + node, lt_union(a, b));
-        node = __ldg(parent + node);
+        const LightSummary a = child_summary(l, sorted, aggregates);
+        const LightSummary b = child_summary(r, sorted, aggregates);
+        store_slot(aggregates + node, lt_union(a, b));
+        node = up;
     }
     if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
 }
 
 // ---------------------------------------------------------------------------------------------
-// Depth of every binary node (walk to the root) and the exclusive scan of the even-depth flags
-// (the 4-wide node index), single pass with a decoupled look-back over tiles of 256 nodes.
+// Single-pass exclusive scan (decoupled look-back over tiles of kScanItems per thread). `op`
+// picks the element: the range-count prefix (inclusive, in place) or the even-depth flags.
+constexpr int kScanItems = 4;
+constexpr uint32_t kScanTile = kScanThreads * kScanItems;
+
+__device__ __forceinline__ uint32_t scan_lookback(uint32_t* states, uint32_t tile, uint32_t total,
+                                                  BuildControl* control)
+{
+    uint32_t* state = states + tile;
+    if (tile == 0) {
+        st_relaxed(state, kTileFlagPrefix | total);
+        return 0;
+    }
+    st_relaxed(state, kTileFlagAggregate | total);
+    uint32_t exclusive = 0;
+    int64_t j = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (j >= 0) {
+        const uint32_t s = ld_relaxed(states + j);
+        if ((s & ~kTileValueMask) == 0) {
+            if (!spin_wait(spins)) {
+                atomicOr(&control->status, kStatusLookbackTimeout);
+                break;
+            }
+            continue;
+        }
+        exclusive += s & kTileValueMask;
+        if (s & kTileFlagPrefix) break;
+        --j;
+    }
+    st_relaxed(state, kTileFlagPrefix | ((exclusive + total) & kTileValueMask));
+    return exclusive;
+}
+
+// cover[g] for g < count becomes the number of binary nodes over leaf boundary g (inclusive prefix
+// sum of the differences). The u32 differences wrap; the prefix is exact.
 __global__ void __launch_bounds__(kScanThreads)
-    lt_depth_scan_kernel(uint32_t n, const uint32_t* __restrict__ parent, uint32_t* __restrict__ depth_out,
-                         uint32_t* __restrict__ wide, uint32_t* scan_states, BuildControl* control)
+    lt_cover_scan_kernel(uint32_t count, uint32_t* cover, uint32_t* states, uint32_t* tile_counter,
+                         BuildControl* control)
 {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[kScanThreads / 32];
     __shared__ uint32_t s_prefix;
-    if (threadIdx.x == 0) s_tile = atomicAdd(&control->scan_tile_counter, 1u);
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
     __syncthreads();
     const uint32_t tile = s_tile;
-    const uint32_t i = tile * kScanThreads + threadIdx.x;
-    uint32_t flag = 0;
-    if (i + 1 < n) {
-        uint32_t d = 0;
-        uint32_t node = __ldg(parent + i);
-        for (uint32_t guard = 0; guard < 128 && node != kNone; ++guard) {
-            ++d;
-            node = __ldg(parent + node);
-        }
-        if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
-        depth_out[i] = d;
-        flag = (d & 1u) == 0 ? 1u : 0u;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < count ? cover[base + k] : 0u;
+        sum += v[k];
     }
     uint32_t total;
-    const uint32_t local = block_exclusive_sum<kScanThreads>(flag, s_scan, total);
-    if (threadIdx.x == 0) {
-        uint32_t exclusive = 0;
-        uint32_t* state = scan_states + tile;
-        if (tile == 0) {
-            st_relaxed(state, kTileFlagPrefix | total);
-        } else {
-            st_relaxed(state, kTileFlagAggregate | total);
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t s = ld_relaxed(scan_states + j);
-                if ((s & ~kTileValueMask) == 0) {
-                    if (!spin_wait(spins)) {
-                        atomicOr(&control->status, kStatusLookbackTimeout);
-                        break;
-                    }
-                    continue;
-                }
-                exclusive += s & kTileValueMask;
-                if (s & kTileFlagPrefix) break;
-                --j;
-            }
-            st_relaxed(state, kTileFlagPrefix | (exclusive + total));
+    const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
+    // The look-back values are 30-bit: the range counts (at most the tree depth) never need more,
+    // but a tile's sum of differences can be "negative"; carry it as its low 30 bits.
+    if (threadIdx.x == 0) s_prefix = scan_lookback(states, tile, total & kTileValueMask, control);
+    __syncthreads();
+    uint32_t run = s_prefix + local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        run += v[k];
+        if (base + k < count) cover[base + k] = run & kTileValueMask;
+    }
+}
+
+// The depth of binary node i is the number of nodes over its split boundary minus one (the nodes
+// over boundary gamma are node i and its ancestors); even depths are flagged and scanned into the
+// 4-wide node index. The last tile writes the node count.
+__global__ void __launch_bounds__(kScanThreads)
+    lt_flags_scan_kernel(uint32_t nodes, const uint32_t* __restrict__ left, const uint32_t* __restrict__ cover,
+                         uint32_t* __restrict__ depth_out, uint32_t* __restrict__ wide, uint32_t* states,
+                         uint32_t* tile_counter, BuildControl* control)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_scan[kScanThreads / 32];
+    __shared__ uint32_t s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t flag[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        flag[k] = 0;
+        if (base + k < nodes) {
+            const uint32_t gamma = __ldg(left + base + k) & ~kChildLeafBit;
+            const uint32_t d = __ldg(cover + gamma) - 1u;
+            if (d >= 128u) atomicOr(&control->status, kStatusDepthGuard);
+            depth_out[base + k] = d;
+            flag[k] = (d & 1u) == 0 ? 1u : 0u;
         }
-        s_prefix = exclusive;
-        if (tile == gridDim.x - 1) control->node_count = exclusive + total;
+        sum += flag[k];
+    }
+    uint32_t total;
+    const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
+    if (threadIdx.x == 0) {
+        s_prefix = scan_lookback(states, tile, total, control);
+        if (tile == gridDim.x - 1) control->node_count = s_prefix + total;
     }
     __syncthreads();
-    if (i + 1 < n) wide[i] = s_prefix + local;
+    uint32_t run = s_prefix + local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < nodes) wide[base + k] = run;
+        run += flag[k];
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
-// 4-wide collapse: one thread per binary node at even depth.
+// 4-wide collapse: one thread per binary node at even depth writes its whole node (224 bytes,
+// its own parent link included: the 4-wide parent is the binary grandparent) and the parent words
+// of its leaf slots by sorted position.
 __global__ void __launch_bounds__(kThreads)
     lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                   const uint32_t* __restrict__ depth, const uint32_t* __restrict__ wide,
-                   const LightSummary* __restrict__ aggregates, LightBvhLeaf* leaves, LightBvhNode* nodes)
+                   const uint32_t* __restrict__ parent, const uint32_t* __restrict__ depth,
+                   const uint32_t* __restrict__ wide, const LightSummary* __restrict__ sorted,
+                   const AggregateSlot* __restrict__ aggregates, uint32_t* __restrict__ leaf_word,
+                   LightBvhNode* __restrict__ nodes)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i + 1 >= n || (__ldg(depth + i) & 1u) != 0) return;
     const uint32_t w = __ldg(wide + i);
     if (w >= node_capacity) return;
-    uint32_t slots[4] = {kNone, kNone, kNone, kNone};
-    uint32_t count = 0;
-    const uint32_t children[2] = {__ldg(left + i), __ldg(right + i)};
-#pragma unroll
-    for (int c = 0; c < 2; ++c) {
-        const uint32_t child = children[c];
-        if (child & kChildLeafBit) {
-            slots[count++] = child;
-        } else {
-            slots[count++] = __ldg(left + child);
-            slots[count++] = __ldg(right + child);
+    const uint32_t l = __ldg(left + i);
+    const uint32_t r = __ldg(right + i);
+    uint32_t slots[4];
+    uint32_t count;
+    {
+        const bool l_leaf = (l & kChildLeafBit) != 0;
+        const bool r_leaf = (r & kChildLeafBit) != 0;
+        const uint32_t ll = l_leaf ? l : __ldg(left + l);
+        const uint32_t lr = l_leaf ? kNone : __ldg(right + l);
+        const uint32_t rl = r_leaf ? r : __ldg(left + r);
+        const uint32_t rr = r_leaf ? kNone : __ldg(right + r);
+        slots[0] = ll;
+        slots[1] = l_leaf ? rl : lr;
+        slots[2] = l_leaf ? rr : rl;
+        slots[3] = l_leaf ? kNone : rr;
+        count = (l_leaf ? 1u : 2u) + (r_leaf ? 1u : 2u);
+        if (l_leaf && r_leaf) slots[2] = kNone;
+    }
+    // The node's own parent link.
+    uint32_t up_node = kNone, up_slot = 0;
+    if (i != 0) {
+        // An even-depth node below the root has a binary grandparent; the guard keeps a broken
+        // tree (a failed earlier stage) from reading outside the arrays.
+        const uint32_t p = __ldg(parent + i);
+        const uint32_t g = p + 1 < n ? __ldg(parent + p) : kNone;
+        if (g + 1 < n) {
+            const uint32_t gl = __ldg(left + g);
+            const uint32_t base = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
+            up_slot = base + (__ldg(right + p) == i ? 1u : 0u);
+            up_node = __ldg(wide + g);
         }
     }
-    LightBvhNode* node = nodes + w;
-    uint32_t words[4] = {kNone, kNone, kNone, kNone};
-    float faces[24];
-    float bounds[24];  // lo[4][3], then hi[4][3]
+    LightSummary sm[4];
+    uint32_t words[4];
 #pragma unroll
     for (uint32_t s = 0; s < 4; ++s) {
-        LightSummary sm;
+        words[s] = kNone;
 #pragma unroll
-        for (int f = 0; f < 6; ++f) sm.face[f] = 0.0f;
+        for (int f = 0; f < 6; ++f) sm[s].face[f] = 0.0f;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) sm.lo[k] = sm.hi[k] = 0.0f;
+        for (int k = 0; k < 3; ++k) sm[s].lo[k] = sm[s].hi[k] = 0.0f;
         if (s < count) {
             const uint32_t slot = slots[s];
             if (slot & kChildLeafBit) {
-                const uint32_t leaf = __ldg(values + (slot & ~kChildLeafBit));
-                sm = load_summary(&leaves[leaf].summary);
-                words[s] = kChildLeafBit | leaf;
-                leaves[leaf].parent = (w << kParentSlotBits) | s;
+                const uint32_t p = slot & ~kChildLeafBit;
+                sm[s] = load_summary(sorted + p);
+                words[s] = kChildLeafBit | __ldg(values + p);
             } else {
-                sm = load_summary(aggregates + slot);
-                const uint32_t child_node = __ldg(wide + slot);
-                words[s] = child_node;
-                if (child_node < node_capacity)
-                    *reinterpret_cast<uint2*>(&nodes[child_node].parent) = make_uint2(w, s);
+                sm[s] = load_summary(&aggregates[slot].summary);
+                words[s] = __ldg(wide + slot);
             }
         }
-#pragma unroll
-        for (int f = 0; f < 6; ++f) faces[6 * s + f] = sm.face[f];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            bounds[3 * s + k] = sm.lo[k];
-            bounds[12 + 3 * s + k] = sm.hi[k];
-        }
     }
-    float4* q = reinterpret_cast<float4*>(node);
 #pragma unroll
-    for (int v = 0; v < 6; ++v) {
-        q[v] = make_float4(faces[4 * v], faces[4 * v + 1], faces[4 * v + 2], faces[4 * v + 3]);
-        q[6 + v] = make_float4(bounds[4 * v], bounds[4 * v + 1], bounds[4 * v + 2], bounds[4 * v + 3]);
-    }
-    *reinterpret_cast<uint4*>(node->child) = make_uint4(words[0], words[1], words[2], words[3]);
-    if (i == 0) *reinterpret_cast<uint2*>(&node->parent) = make_uint2(kNone, 0u);
+    for (uint32_t s = 0; s < 4; ++s)
+        if (s < count && (slots[s] & kChildLeafBit)) leaf_word[slots[s] & ~kChildLeafBit] = (w << kParentSlotBits) | s;
+    float4* q = reinterpret_cast<float4*>(nodes + w);
+    q[0] = make_float4(sm[0].face[0], sm[0].face[1], sm[0].face[2], sm[0].face[3]);
+    q[1] = make_float4(sm[0].face[4], sm[0].face[5], sm[1].face[0], sm[1].face[1]);
+    q[2] = make_float4(sm[1].face[2], sm[1].face[3], sm[1].face[4], sm[1].face[5]);
+    q[3] = make_float4(sm[2].face[0], sm[2].face[1], sm[2].face[2], sm[2].face[3]);
+    q[4] = make_float4(sm[2].face[4], sm[2].face[5], sm[3].face[0], sm[3].face[1]);
+    q[5] = make_float4(sm[3].face[2], sm[3].face[3], sm[3].face[4], sm[3].face[5]);
+    q[6] = make_float4(sm[0].lo[0], sm[0].lo[1], sm[0].lo[2], sm[1].lo[0]);
+    q[7] = make_float4(sm[1].lo[1], sm[1].lo[2], sm[2].lo[0], sm[2].lo[1]);
+    q[8] = make_float4(sm[2].lo[2], sm[3].lo[0], sm[3].lo[1], sm[3].lo[2]);
+    q[9] = make_float4(sm[0].hi[0], sm[0].hi[1], sm[0].hi[2], sm[1].hi[0]);
+    q[10] = make_float4(sm[1].hi[1], sm[1].hi[2], sm[2].hi[0], sm[2].hi[1]);
+    q[11] = make_float4(sm[2].hi[2], sm[3].hi[0], sm[3].hi[1], sm[3].hi[2]);
+    uint4* u = reinterpret_cast<uint4*>(nodes + w);
+    u[12] = make_uint4(words[0], words[1], words[2], words[3]);
+    u[13] = make_uint4(up_node, up_slot, 0u, 0u);
+}
+
+// The parent words of the leaves in leaf (record) order: the second 32-byte sector of every leaf
+// is rewritten whole (lo.z, hi, group, entry, pad, parent), so no partial sector is written.
+__global__ void __launch_bounds__(kThreads)
+    lt_leaf_parent_kernel(uint32_t n, const uint32_t* __restrict__ inverse, const uint32_t* __restrict__ leaf_word,
+                          LightBvhLeaf* __restrict__ leaves)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t word = __ldg(leaf_word + __ldg(inverse + i));
+    uint4* sector = reinterpret_cast<uint4*>(leaves + i) + 2;
+    const uint4 a = sector[0];
+    uint4 b = sector[1];
+    b.w = word;
+    sector[0] = a;
+    sector[1] = b;
 }
 
 // ---------------------------------------------------------------------------------------------
 // The header (one thread): root summary, counts, overflow; the one-leaf tree's single node.
 __global__ void lt_finish_kernel(uint32_t n, uint32_t found, uint32_t node_capacity, LightBvhLeaf* leaves,
-                                 LightBvhNode* nodes, const LightSummary* aggregates, LightTreeHeader* header,
+                                 LightBvhNode* nodes, const AggregateSlot* aggregates, LightTreeHeader* header,
                                  LightTreeState* state, const BuildControl* control)
 {
     LightSummary root;
@@ -470,7 +584,7 @@ __global__ void lt_finish_kernel(uint32_t n, uint32_t found, uint32_t node_capac
             node->child_hi[0][k] = root.hi[k];
         }
         *reinterpret_cast<uint4*>(node->child) = make_uint4(kChildLeafBit, kNone, kNone, kNone);
-        *reinterpret_cast<uint2*>(&node->parent) = make_uint2(kNone, 0u);
+        *reinterpret_cast<uint4*>(&node->parent) = make_uint4(kNone, 0u, 0u, 0u);
         leaves[0].parent = 0;
         root_index = 0;
         node_count = 1;
@@ -479,7 +593,7 @@ __global__ void lt_finish_kernel(uint32_t n, uint32_t found, uint32_t node_capac
         if (node_count > node_capacity) {
             overflow = 1;
         } else {
-            root = load_summary_cg(aggregates);
+            root = load_summary_cg(&aggregates[0].summary);
             root_index = 0;
         }
     }
@@ -508,6 +622,12 @@ uint32_t grid_for(uint32_t n, uint32_t per_block, uint32_t cap)
 
 uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t{255}; }
 
+uint64_t zero_words(uint32_t n)
+{
+    // control words, the sort scratch, then two scan states and their tile counters
+    return sizeof(BuildControl) / 4 + sort_scratch_words(n) + 2ull * ((n + kScanTile - 1) / kScanTile) + 2;
+}
+
 }  // namespace
 
 uint64_t lt_buffer_bytes(uint32_t cap)
@@ -517,9 +637,10 @@ uint64_t lt_buffer_bytes(uint32_t cap)
     b += align256(c * sizeof(LightBvhLeaf));
     b += align256(c * sizeof(LightBvhNode));  // node capacity = leaf capacity (>= n - 1 nodes)
     b += align256(128);                       // header + state
-    b += 11 * align256(c * 4);                // keys, values, alt x2, left, right, parent, leaf_parent, counter, depth, wide
+    b += 14 * align256(c * 4);                // u32 arrays
+    b += align256(c * sizeof(AggregateSlot));
     b += align256(c * sizeof(LightSummary));
-    b += align256(sizeof(BuildControl) + sort_scratch_words((uint32_t)c) * 4 + scan_tiles((uint32_t)c) * 4);
+    b += align256(zero_words((uint32_t)c) * 4);
     return b;
 }
 
@@ -535,28 +656,31 @@ LightBvhBuffers lt_carve(void* base, uint32_t cap)
         p += align256(bytes);
         return q;
     };
+    auto u32 = [&]() { return reinterpret_cast<uint32_t*>(take(c * 4)); };
     b.leaves = reinterpret_cast<LightBvhLeaf*>(take(c * sizeof(LightBvhLeaf)));
     b.nodes = reinterpret_cast<LightBvhNode*>(take(c * sizeof(LightBvhNode)));
     char* hs = take(128);
     b.header = reinterpret_cast<LightTreeHeader*>(hs);
     b.state = reinterpret_cast<LightTreeState*>(hs + 64);
-    b.keys = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.values = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.keys_alt = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.values_alt = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.left = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.right = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.parent = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.leaf_parent = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.counter = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.depth = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.wide = reinterpret_cast<uint32_t*>(take(c * 4));
-    b.aggregates = reinterpret_cast<LightSummary*>(take(c * sizeof(LightSummary)));
-    const uint64_t zero = sizeof(BuildControl) + sort_scratch_words((uint32_t)c) * 4 + scan_tiles((uint32_t)c) * 4;
-    char* z = take(zero);
+    b.keys = u32();
+    b.values = u32();
+    b.keys_alt = u32();
+    b.values_alt = u32();
+    b.left = u32();
+    b.right = u32();
+    b.parent = u32();
+    b.leaf_parent = u32();
+    b.counter = u32();
+    b.depth = u32();
+    b.wide = u32();
+    b.cover = u32();
+    b.inverse = u32();
+    b.leaf_word = u32();
+    b.aggregates = reinterpret_cast<AggregateSlot*>(take(c * sizeof(AggregateSlot)));
+    b.sorted = reinterpret_cast<LightSummary*>(take(c * sizeof(LightSummary)));
+    char* z = take(zero_words((uint32_t)c) * 4);
     b.control = reinterpret_cast<BuildControl*>(z);
     b.sort_scratch = reinterpret_cast<uint32_t*>(z + sizeof(BuildControl));
-    b.zero_bytes = zero;
     return b;
 }
 
@@ -568,11 +692,13 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         if (stage) cudaEventRecord(stage[k], stream);
     };
     mark(0);
-    // The scan states follow the sort scratch sized for this build's n.
-    const uint64_t sort_words = sort_scratch_words(n);
-    uint32_t* scan_states = b.sort_scratch + sort_words;
-    const uint64_t zero = sizeof(BuildControl) + sort_words * 4 + (uint64_t)scan_tiles(n) * 4;
-    cudaError_t e = cudaMemsetAsync(b.control, 0, zero, stream);
+    // Zeroed words of this build: control, the sort scratch sized for n, two scan state arrays and
+    // their tile counters.
+    const uint32_t scan_tiles_n = (n + kScanTile - 1) / kScanTile;
+    uint32_t* cover_states = b.sort_scratch + sort_scratch_words(n);
+    uint32_t* flag_states = cover_states + scan_tiles_n;
+    uint32_t* scan_counters = flag_states + scan_tiles_n;
+    cudaError_t e = cudaMemsetAsync(b.control, 0, zero_words(n) * 4, stream);
     if (e != cudaSuccess) return e;
     const uint32_t sms = 148;
     if (n > 0) {
@@ -580,10 +706,15 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
             in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves, b.control);
         mark(1);
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
-            b.leaves, n, b.control, b.keys, b.counter, b.sort_scratch);
+            b.leaves, n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
         mark(2);
+        SortGather gather;
+        gather.rows_in = reinterpret_cast<const uint4*>(b.leaves);
+        gather.rows_in_stride = sizeof(LightBvhLeaf) / sizeof(uint4);
+        gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
+        gather.inverse = b.inverse;
         onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
-                      stream);
+                      stream, &gather);
         mark(3);
     } else {
         mark(1);
@@ -593,16 +724,22 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     if (n >= 2) {
         const uint32_t nodes = n - 1;
         lt_karras_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent);
+            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover);
         mark(4);
         lt_aggregate_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            n, b.values, b.leaves, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.control);
+            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.control);
         mark(5);
-        lt_depth_scan_kernel<<<scan_tiles(nodes), kScanThreads, 0, stream>>>(n, b.parent, b.depth, b.wide,
-                                                                             scan_states, b.control);
+        const uint32_t tiles = (nodes + kScanTile - 1) / kScanTile;
+        lt_cover_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.cover, cover_states, scan_counters,
+                                                                  b.control);
+        lt_flags_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.left, b.cover, b.depth, b.wide,
+                                                                  flag_states, scan_counters + 1, b.control);
         mark(6);
         lt_wide_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            n, b.node_capacity, b.values, b.left, b.right, b.depth, b.wide, b.aggregates, b.leaves, b.nodes);
+            n, b.node_capacity, b.values, b.left, b.right, b.parent, b.depth, b.wide, b.sorted, b.aggregates,
+            b.leaf_word, b.nodes);
+        lt_leaf_parent_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.inverse, b.leaf_word,
+                                                                                        b.leaves);
     } else {
         mark(4);
         mark(5);
@@ -618,7 +755,7 @@ uint32_t lt_kernel_launches(uint32_t n)
 {
     if (n == 0) return 1;
     if (n == 1) return 7;
-    return 11;
+    return 13;
 }
 
 }  // namespace cx

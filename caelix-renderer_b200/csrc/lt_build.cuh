@@ -4,18 +4,25 @@
 //
 // Replaces the reference's per-tree dispatch sequence LightTree::RecordTree
 // (lib/src/light/light_tree_record.cpp:230-309, about 35 dependent dispatches with a barrier after
-// each) with 10 kernels and one memset, all on one stream (capturable in a CUDA graph):
+// each) with 13 kernels and one memset, all on one stream (capturable in a CUDA graph):
 //   lt_emit_kernel        gather emit (caelix_light_gather_emit.hlsl:11-86) fused with the centre
 //                         bounds (caelix_light_bvh_bounds.hlsl:10-53): warp max-reductions of
 //                         order-preserving codes instead of a one-workgroup reduction
 //   lt_morton_kernel      Morton codes (caelix_light_bvh_morton.hlsl:6-28) fused with the digit
 //                         histograms of all four sort passes and the clear of the arrival counters
-//   onesweep_pass_kernel  x4 (radix_sort.cuh)
-//   lt_karras_kernel      caelix_light_bvh_karras.hlsl:8-96
+//   onesweep_pass_kernel  x4 (radix_sort.cuh); the last pass also gathers the leaf summaries into
+//                         sorted order and the inverse permutation, so every later kernel reads
+//                         leaves by sorted position (coalesced) instead of through the permutation
+//   lt_karras_kernel      caelix_light_bvh_karras.hlsl:8-96, plus the range-count differences
 //   lt_aggregate_kernel   caelix_light_bvh_aggregate.hlsl:30-55 (acq_rel arrival counters)
-//   lt_depth_scan_kernel  caelix_light_bvh_depth.hlsl:7-30 fused with the scan of the even-depth
-//                         flags (decoupled look-back instead of a one-workgroup scan)
-//   lt_wide_kernel        caelix_light_bvh_wide.hlsl:10-100
+//   lt_cover_scan_kernel  the depths (caelix_light_bvh_depth.hlsl:7-30) without walking to the
+//   lt_flags_scan_kernel  root: depth(i) + 1 = the number of binary nodes whose range spans node i's
+//                         split boundary (node i and its ancestors), a prefix sum of +1/-1 range
+//                         ends; then the even-depth flags scanned into 4-wide indices (single-pass
+//                         decoupled look-back scans instead of the one-workgroup scan)
+//   lt_wide_kernel        caelix_light_bvh_wide.hlsl:10-100; every thread writes its whole node,
+//                         its own parent link included (full 32-byte sectors)
+//   lt_leaf_parent_kernel the leaves' parent words in leaf order (whole-sector rewrites)
 //   lt_finish_kernel      caelix_light_bvh_finish.hlsl:8-63
 // Every float operation is a single IEEE fp32 operation in the order of the HLSL source (the
 // library is compiled with --fmad=false), so the tree is bit-identical to the oracle's.
@@ -54,6 +61,15 @@ struct BuildControl
 };
 static_assert(sizeof(BuildControl) == 64);
 
+// A binary node's summary padded to 64 bytes, so that every aggregate write covers two whole
+// 32-byte sectors.
+struct alignas(16) AggregateSlot
+{
+    LightSummary summary;
+    uint32_t pad[4];
+};
+static_assert(sizeof(AggregateSlot) == 64);
+
 // Device arrays of one tree and its build scratch (the kLtScratch* arrays of
 // light_tree_layout.h:392-423, here separate arrays).
 struct LightBvhBuffers
@@ -75,11 +91,13 @@ struct LightBvhBuffers
     uint32_t* counter = nullptr;
     uint32_t* depth = nullptr;
     uint32_t* wide = nullptr;
-    LightSummary* aggregates = nullptr;
+    uint32_t* cover = nullptr;      // range-count differences, then the nodes over each leaf boundary
+    uint32_t* inverse = nullptr;    // sorted position of every leaf
+    uint32_t* leaf_word = nullptr;  // parent word of the leaf at every sorted position
+    AggregateSlot* aggregates = nullptr;
+    LightSummary* sorted = nullptr;  // leaf summaries in sorted order
     BuildControl* control = nullptr;  // followed by the sort scratch, then the scan states
     uint32_t* sort_scratch = nullptr;
-    uint32_t* scan_states = nullptr;
-    uint64_t zero_bytes = 0;  // bytes from `control` that a build clears
 };
 
 // Input of one build: `count` records (device), optional per-record group and entry words and
@@ -96,10 +114,6 @@ struct LightBvhInput
 };
 
 constexpr int kScanThreads = 256;
-__host__ __device__ constexpr uint32_t scan_tiles(uint32_t n)
-{
-    return (n + kScanThreads - 1) / kScanThreads;
-}
 
 // Bytes of device memory for a leaf capacity (one allocation, carved by lt_carve).
 uint64_t lt_buffer_bytes(uint32_t leaf_capacity);

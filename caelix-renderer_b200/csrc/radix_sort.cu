@@ -16,6 +16,10 @@ struct SortPass
     uint32_t* tile_counter;
     uint32_t* tile_states;  // tiles * 256 words, zero
     uint32_t* status;
+    const uint4* rows_in;  // gathering pass: 48-byte rows by value (stride rows_in_stride uint4), else nullptr
+    uint32_t rows_in_stride;
+    uint4* rows_out;       // 48-byte rows by destination
+    uint32_t* inverse;     // inverse[value] = destination
 };
 
 namespace {
@@ -38,7 +42,15 @@ __global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __
     }
 }
 
-__global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortPass a)
+// One onesweep pass over a tile of kSortTile elements. Phases:
+//   1. keys (warp-striped, coalesced) -> digits -> stable rank inside the warp (__match_any_sync);
+//   2. per-digit warp offsets and tile counts; the tile's counts are published at once (the
+//      look-back of later tiles can proceed), then the keys go to the shared staging area in
+//      tile-sorted order (their key registers are free from here on);
+//   3. decoupled look-back per digit (one thread per digit, bounded spin);
+//   4. values (and, on the gathering pass, the 48-byte rows) are staged by the same positions and
+//      the tile is written out in runs per digit.
+__global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const SortPass a)
 {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp_counts[kSortWarps][kRadix];  // counts, then exclusive offsets per warp
@@ -59,17 +71,14 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortP
     const uint32_t base = tile * kSortTile;
     const uint32_t warp_base = base + warp * 32u * kSortKeysPerThread;
 
+    // Phase 1.
     uint32_t key[kSortKeysPerThread];
-    uint32_t value[kSortKeysPerThread];
-    uint32_t rank[kSortKeysPerThread];
+    uint32_t pos[kSortKeysPerThread];  // rank in the warp, then position in the tile
 #pragma unroll
     for (int k = 0; k < kSortKeysPerThread; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
-        const bool valid = i < a.n;
-        key[k] = valid ? __ldg(a.keys_in + i) : 0u;
-        value[k] = valid ? (a.values_in ? __ldg(a.values_in + i) : i) : 0u;
+        key[k] = i < a.n ? __ldg(a.keys_in + i) : 0u;
     }
-    // Stable rank inside the warp: element (k, lane) precedes (k, lane + 1) and (k + 1, *).
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int k = 0; k < kSortKeysPerThread; ++k) {
@@ -79,14 +88,14 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortP
         const uint32_t before = __popc(peers & lt);
         uint32_t running = 0;
         if (digit < 256u) running = s_warp_counts[warp][digit];
-        rank[k] = running + before;
+        pos[k] = running + before;
         __syncwarp();
         if (digit < 256u && before == 0) s_warp_counts[warp][digit] = running + __popc(peers);
         __syncwarp();
     }
     __syncthreads();
 
-    // Thread d owns digit d: per-warp exclusive offsets, the tile total, the look-back.
+    // Phase 2: thread d owns digit d.
     const uint32_t d = tid;
     uint32_t total = 0;
 #pragma unroll
@@ -96,11 +105,24 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortP
         total += c;
     }
     uint32_t* state = a.tile_states + (uint64_t)tile * kRadix + d;
+    st_relaxed(state, (tile == 0 ? kTileFlagPrefix : kTileFlagAggregate) | total);
+    uint32_t tile_total;
+    const uint32_t local = block_exclusive_sum<kSortThreads>(total, s_scan, tile_total);
+    s_local[d] = local;
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kSortKeysPerThread; ++k) {
+        const uint32_t i = warp_base + k * 32u + lane;
+        if (i < a.n) {
+            const uint32_t digit = (key[k] >> a.shift) & 255u;
+            pos[k] += s_local[digit] + s_warp_counts[warp][digit];
+            s_keys[pos[k]] = key[k];
+        }
+    }
+
+    // Phase 3: the exclusive prefix of digit d over the earlier tiles.
     uint32_t exclusive = 0;
-    if (tile == 0) {
-        st_relaxed(state, kTileFlagPrefix | total);
-    } else {
-        st_relaxed(state, kTileFlagAggregate | total);
+    if (tile != 0) {
         int64_t j = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (j >= 0) {
@@ -120,29 +142,33 @@ __global__ void __launch_bounds__(kSortThreads) onesweep_pass_kernel(const SortP
     }
     uint32_t digit_total;
     const uint32_t global_base = block_exclusive_sum<kSortThreads>(a.counts[d], s_scan, digit_total);
-    uint32_t tile_total;
-    const uint32_t local = block_exclusive_sum<kSortThreads>(total, s_scan, tile_total);
-    s_local[d] = local;
     s_dest[d] = global_base + exclusive - local;
-    __syncthreads();
 
+    // Phase 4.
 #pragma unroll
     for (int k = 0; k < kSortKeysPerThread; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
-        if (i < a.n) {
-            const uint32_t digit = (key[k] >> a.shift) & 255u;
-            const uint32_t at = s_local[digit] + s_warp_counts[warp][digit] + rank[k];
-            s_keys[at] = key[k];
-            s_values[at] = value[k];
-        }
+        if (i < a.n) s_values[pos[k]] = a.values_in ? __ldg(a.values_in + i) : i;
     }
     __syncthreads();
     const uint32_t count = a.n - base < (uint32_t)kSortTile ? a.n - base : (uint32_t)kSortTile;
     for (uint32_t j = tid; j < count; j += kSortThreads) {
         const uint32_t k = s_keys[j];
+        const uint32_t v = s_values[j];
         const uint32_t dest = s_dest[(k >> a.shift) & 255u] + j;
         a.keys_out[dest] = k;
-        a.values_out[dest] = s_values[j];
+        a.values_out[dest] = v;
+        if (a.rows_in) {
+            const uint4* src = a.rows_in + (uint64_t)a.rows_in_stride * v;
+            uint4* dst = a.rows_out + 3ull * dest;
+            const uint4 r0 = __ldg(src);
+            const uint4 r1 = __ldg(src + 1);
+            const uint4 r2 = __ldg(src + 2);
+            dst[0] = r0;
+            dst[1] = r1;
+            dst[2] = r2;
+            a.inverse[v] = dest;
+        }
     }
 }
 
@@ -154,9 +180,9 @@ void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t 
     radix_histogram_kernel<<<grid, 256, 0, stream>>>(keys, n, hist);
 }
 
-void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b,
-                          uint32_t n, bool identity_values, uint32_t* scratch, uint32_t* status,
-                          cudaStream_t stream)
+void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
+                   bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
+                   const SortGather* gather)
 {
     if (n == 0) return;
     const uint32_t tiles = sort_tiles(n);
@@ -179,6 +205,11 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         p.tile_counter = counters + pass;
         p.tile_states = states + (uint64_t)pass * tiles * kRadix;
         p.status = status;
+        const bool last = pass == 3;
+        p.rows_in = (last && gather) ? gather->rows_in : nullptr;
+        p.rows_in_stride = gather ? gather->rows_in_stride : 0;
+        p.rows_out = (last && gather) ? gather->rows_out : nullptr;
+        p.inverse = (last && gather) ? gather->inverse : nullptr;
         onesweep_pass_kernel<<<tiles, kSortThreads, 0, stream>>>(p);
         uint32_t* t = kin;
         kin = kout;

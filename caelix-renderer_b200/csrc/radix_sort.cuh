@@ -50,12 +50,24 @@ __host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n)
 // Accumulates the 256-bin histograms of all four digits of keys[0 .. n) into hist[4][256].
 void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream);
 
+// An optional gather fused into the last pass: the 48-byte row at rows_in + rows_in_stride * value
+// (in uint4 units) of every element is copied to rows_out[destination] (48-byte rows), and
+// inverse[value] = destination.
+struct SortGather
+{
+    const uint4* rows_in;
+    uint32_t rows_in_stride;
+    uint4* rows_out;
+    uint32_t* inverse;
+};
+
 // Launches the four passes: keys_a/values_a hold the input and, after the even number of passes,
 // the output; keys_b/values_b are the ping-pong buffers. `identity_values`: the input values are
 // 0 .. n-1 and are not read (values_a is still written). `scratch` holds sort_scratch_words(n)
 // words, already zero, with the histograms of all four digits in its first 1024 words
 // (radix_histogram or a fused producer).
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
-                   bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream);
+                   bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
+                   const SortGather* gather = nullptr);
 
 }  // namespace cx

@@ -153,7 +153,7 @@ typedef struct CaelixLightBvhView
     uint64_t leaf_parent; /* u32 binary parent of each sorted leaf */
     uint64_t depth;       /* u32 binary node depths */
     uint64_t wide;        /* u32 4-wide index of each even-depth binary node */
-    uint64_t aggregates;  /* LightSummary per binary node, 48 bytes each */
+    uint64_t aggregates;  /* LightSummary per binary node, in 64-byte slots (16 bytes of padding) */
     uint32_t leaf_capacity;
     uint32_t node_capacity;
 } CaelixLightBvhView;

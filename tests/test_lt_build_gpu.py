@@ -16,6 +16,7 @@ pytestmark = pytest.mark.gpu
 
 REPO = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 GOLDEN = np.load(os.path.join(REPO, "tests", "golden", "sort_mt19937_3.npz"))
+AGG_SLOT_DTYPE = np.dtype([("s", oracle_lib.SUMMARY_DTYPE), ("pad", "<u4", (4,))])
 
 
 def gpu_build(dev, rec, group=None, frames=None, capacity=None):
@@ -43,7 +44,7 @@ def gpu_build(dev, rec, group=None, frames=None, capacity=None):
         "leaf_parent": gpu_util.from_device(v.leaf_parent, np.uint32, m if m >= 2 else 0),
         "depth": gpu_util.from_device(v.depth, np.uint32, max(m - 1, 0)),
         "wide": gpu_util.from_device(v.wide, np.uint32, max(m - 1, 0)),
-        "aggregates": gpu_util.from_device(v.aggregates, oracle_lib.SUMMARY_DTYPE, max(m - 1, 0)),
+        "aggregates": gpu_util.from_device(v.aggregates, AGG_SLOT_DTYPE, max(m - 1, 0))["s"].copy(),
     }
     nc = int(out["header"][0]["node_count"])
     out["nodes"] = gpu_util.from_device(v.nodes, oracle_lib.NODE_DTYPE, nc)
