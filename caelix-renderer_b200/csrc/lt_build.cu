@@ -258,7 +258,7 @@ __device__ __forceinline__ int lt_delta(const uint32_t* __restrict__ keys, int i
 __global__ void __launch_bounds__(kThreads)
     lt_karras_kernel(const uint32_t* __restrict__ keys, int n, uint32_t* __restrict__ left,
                      uint32_t* __restrict__ right, uint32_t* __restrict__ parent, uint32_t* __restrict__ leaf_parent,
-                     uint32_t* __restrict__ cover)
+                     uint32_t* __restrict__ cover, uint32_t* __restrict__ range_end)
 {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n - 1) return;
@@ -293,20 +293,20 @@ __global__ void __launch_bounds__(kThreads)
     else parent[l] = (uint32_t)i;
     if (r & kChildLeafBit) leaf_parent[r & ~kChildLeafBit] = (uint32_t)i;
     else parent[r] = (uint32_t)i;
+    range_end[i] = (uint32_t)j;
     atomicAdd(cover + a, 1u);
     atomicAdd(cover + b, 0xFFFFFFFFu);
 }
 
 // ---------------------------------------------------------------------------------------------
 // Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
-// computes its summary from both children and goes on (acq_rel arrival counter). Leaf summaries
-// come from the sorted copy (coalesced), node summaries are 64-byte slots (full-sector writes).
-__device__ __forceinline__ LightSummary child_summary(uint32_t child, const LightSummary* __restrict__ sorted,
-                                                     const AggregateSlot* aggregates)
-{
-    if (child & kChildLeafBit) return load_summary(sorted + (child & ~kChildLeafBit));
-    return load_summary_cg(&aggregates[child].summary);
-}
+// computes its summary from both children and goes on. A CTA owns a tile of kAggTile consecutive
+// sorted leaves: a node whose range lies inside the tile is reached only by the tile's threads,
+// so its arrival counter and summary live in shared memory (block-scope acq_rel); only nodes whose
+// range crosses a tile boundary use device-scope counters. A thread carries the summary of the
+// child it comes from and loads only the sibling. Every node's summary is also stored to its
+// 64-byte global slot (full-sector writes) for the collapse.
+constexpr uint32_t kAggTile = 256;
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
 {
@@ -317,25 +317,49 @@ __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary&
     q[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kAggTile)
     lt_aggregate_kernel(uint32_t n, const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
                         const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
-                        const uint32_t* __restrict__ leaf_parent, uint32_t* counter, AggregateSlot* aggregates,
-                        BuildControl* control)
+                        const uint32_t* __restrict__ leaf_parent, const uint32_t* __restrict__ range_end,
+                        uint32_t* counter, AggregateSlot* aggregates, BuildControl* control)
 {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ uint32_t s_count[kAggTile];
+    __shared__ LightSummary s_sum[kAggTile];
+    const uint32_t lo = blockIdx.x * kAggTile;
+    const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
+    s_count[threadIdx.x] = 0;
+    __syncthreads();
+    const uint32_t j = lo + threadIdx.x;
     if (j >= n) return;
+    LightSummary cur = load_summary(sorted + j);
+    uint32_t from = kChildLeafBit | j;
     uint32_t node = __ldg(leaf_parent + j);
     uint32_t depth = 0;
     for (; depth < 128 && node != kNone; ++depth) {
         const uint32_t l = __ldg(left + node);
         const uint32_t r = __ldg(right + node);
         const uint32_t up = __ldg(parent + node);
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
-        if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-        const LightSummary a = child_summary(l, sorted, aggregates);
-        const LightSummary b = child_summary(r, sorted, aggregates);
-        store_slot(aggregates + node, lt_union(a, b));
+        const uint32_t end = __ldg(range_end + node);
+        const uint32_t a = min(node, end);
+        const uint32_t b = max(node, end);
+        const bool inside = a >= lo && b <= hi;
+        const uint32_t sibling = l == from ? r : l;
+        LightSummary sib;
+        if (inside) {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrival(s_count[node - lo]);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
+            else sib = s_sum[sibling - lo];
+        } else {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
+            else sib = load_summary_cg(&aggregates[sibling].summary);
+        }
+        cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
+        if (inside) s_sum[node - lo] = cur;
+        store_slot(aggregates + node, cur);
+        from = node;
         node = up;
     }
     if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
@@ -724,10 +748,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     if (n >= 2) {
         const uint32_t nodes = n - 1;
         lt_karras_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover);
+            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover, b.depth);
         mark(4);
-        lt_aggregate_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.control);
+        // `depth` holds each node's range end until the flags scan writes the depths.
+        lt_aggregate_kernel<<<(n + kAggTile - 1) / kAggTile, kAggTile, 0, stream>>>(
+            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.depth, b.counter, b.aggregates, b.control);
         mark(5);
         const uint32_t tiles = (nodes + kScanTile - 1) / kScanTile;
         lt_cover_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.cover, cover_states, scan_counters,
