@@ -249,3 +249,263 @@ class LightBvh:
         if check:
             self.L.check(code, "caelix_light_bvh_get_stats")
         return s
+
+
+# ---------------------------------------------------------------------------------------------
+# Scene and renderer
+
+
+class CaelixSceneDesc(C.Structure):
+    _fields_ = [("group_shift", C.c_uint32), ("encoding", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+
+
+class CaelixBrickKey(C.Structure):
+    _fields_ = [("x", C.c_int32), ("y", C.c_int32), ("z", C.c_int32)]
+
+
+class CaelixMaterial(C.Structure):
+    _fields_ = [
+        ("albedo", C.c_float * 3), ("smoothness", C.c_float), ("emission", C.c_float * 3), ("metallic", C.c_float),
+        ("ior", C.c_float), ("extinction", C.c_float), ("sss_model", C.c_uint32), ("sss_probability", C.c_float),
+        ("sss_albedo", C.c_float * 3), ("sss_anisotropy", C.c_float), ("sss_steps", C.c_uint32),
+        ("sss_params", C.c_float * 8), ("texture_set", C.c_uint32), ("connect_group", C.c_uint32),
+        ("reserved", C.c_uint32),
+    ]
+
+
+assert C.sizeof(CaelixMaterial) == 112
+
+
+class CaelixLightOptions(C.Structure):
+    _fields_ = [("enabled", C.c_uint32), ("min_emission", C.c_float), ("heap_bytes", C.c_uint64)]
+
+
+class CaelixFrameDesc(C.Structure):
+    _fields_ = [("command_buffer", C.c_uint64), ("frame_number", C.c_uint64), ("safe_frame_number", C.c_uint64)]
+
+
+class CaelixLightStats(C.Structure):
+    _fields_ = [
+        ("enabled", C.c_uint32), ("light_groups", C.c_uint32), ("light_bricks", C.c_uint64),
+        ("light_faces", C.c_uint64), ("bricks_dropped", C.c_uint64), ("heap_bytes_used", C.c_uint64),
+        ("heap_bytes_capacity", C.c_uint64), ("passes", C.c_uint32), ("failed_passes", C.c_uint32),
+        ("records_recomputed", C.c_uint32), ("records_copied", C.c_uint32), ("gpu_ms", C.c_float),
+        ("pad", C.c_uint32), ("tree_leaves", C.c_uint32 * 2), ("tree_nodes", C.c_uint32 * 2),
+        ("tree_builds", C.c_uint32 * 2), ("tree_leaves_dropped", C.c_uint32 * 2),
+    ]
+
+
+assert C.sizeof(CaelixLightStats) == 104
+
+
+class CaelixSceneView(C.Structure):
+    _fields_ = [("grid", C.c_uint32 * 3), ("group_shift", C.c_uint32), ("groups", C.c_uint32 * 3),
+                ("brick_count", C.c_uint32), ("hash_capacity", C.c_uint32), ("hash_slot_count", C.c_uint32),
+                ("hash_max_probe", C.c_uint32), ("light_count", C.c_uint32), ("heap_words", C.c_uint32),
+                ("group_count", C.c_uint32)] + [(n, C.c_uint64) for n in (
+                    "keys", "records", "hash_slots", "bitmap", "heap", "group_rows", "light_headers", "light_group",
+                    "light_entry", "light_brick", "tree_header", "tree_nodes", "tree_leaves")]
+
+
+class CaelixCamera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("pad0", C.c_float), ("right", C.c_float * 3), ("pad1", C.c_float),
+                ("up", C.c_float * 3), ("pad2", C.c_float), ("forward", C.c_float * 3), ("pad3", C.c_float),
+                ("tan_half_fov_y", C.c_float), ("aspect", C.c_float), ("near_z", C.c_float), ("far_z", C.c_float),
+                ("projection", C.c_float * 16), ("jitter", C.c_float * 2)]
+
+
+class CaelixRenderTargets(C.Structure):
+    _fields_ = [("radiance", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32)]
+
+
+class CaelixRenderOptions(C.Structure):
+    _fields_ = [("mode", C.c_uint32), ("bounce_count", C.c_uint32), ("frame_seed", C.c_uint32), ("spp", C.c_uint32),
+                ("reserved", C.c_uint32 * 4)]
+
+
+class CaelixLightNeeOptions(C.Structure):
+    _fields_ = [("enabled", C.c_uint32), ("flags", C.c_uint32), ("hint_patch", C.c_uint32), ("reserved", C.c_uint32)]
+
+
+class CaelixGpuTimings(C.Structure):
+    _fields_ = [("trace_ms", C.c_float), ("flush_ms", C.c_float), ("frame_number", C.c_uint64),
+                ("composite_ms", C.c_float), ("denoise_ms", C.c_float), ("upscale_ms", C.c_float),
+                ("pad", C.c_float)]
+
+
+class CaelixRenderStats(C.Structure):
+    _fields_ = [("primary_rays", C.c_uint64), ("bounce_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("kernel_launches", C.c_uint32), ("pad", C.c_uint32)]
+
+
+def _bind_scene(L):
+    vp = C.c_void_p
+    proto = {
+        "caelix_scene_create": [vp, C.POINTER(CaelixSceneDesc), C.POINTER(vp)],
+        "caelix_scene_upload_bricks": [vp, C.c_uint32, C.c_uint32, vp, vp, C.POINTER(C.c_uint32)],
+        "caelix_scene_set_brick_power": [vp, C.c_uint32, C.c_uint32, vp, vp],
+        "caelix_scene_set_materials": [vp, vp, C.c_uint32],
+        "caelix_scene_set_light_options": [vp, C.POINTER(CaelixLightOptions)],
+        "caelix_scene_flush": [vp, C.POINTER(CaelixFrameDesc)],
+        "caelix_scene_get_view": [vp, C.POINTER(CaelixSceneView)],
+        "caelix_renderer_create": [vp, vp, C.POINTER(vp)],
+        "caelix_renderer_render": [vp, C.POINTER(CaelixFrameDesc), C.POINTER(CaelixRenderTargets),
+                                   C.POINTER(CaelixCamera), C.POINTER(CaelixRenderOptions)],
+        "caelix_renderer_set_light_nee_options": [vp, C.POINTER(CaelixLightNeeOptions)],
+        "caelix_renderer_get_stats": [vp, C.POINTER(CaelixRenderStats)],
+    }
+    for name, args in proto.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.caelix_scene_destroy.argtypes = [vp]
+    L.caelix_scene_destroy.restype = None
+    L.caelix_renderer_destroy.argtypes = [vp]
+    L.caelix_renderer_destroy.restype = None
+    L.caelix_scene_get_light_stats.argtypes = [vp, C.POINTER(CaelixLightStats)]
+    L.caelix_scene_get_light_stats.restype = None
+    L.caelix_scene_get_light_tree.argtypes = [vp]
+    L.caelix_scene_get_light_tree.restype = C.c_uint64
+    L.caelix_renderer_get_gpu_timings.argtypes = [vp, C.POINTER(CaelixGpuTimings)]
+    L.caelix_renderer_get_gpu_timings.restype = None
+
+
+class Scene:
+    """caelix_scene_*: bricks, brick power, materials, flush."""
+
+    def __init__(self, device: Device, group_shift: int = 4):
+        self.device = device
+        self.L = device.L
+        _bind_scene(self.L.lib)
+        handle = C.c_void_p()
+        desc = CaelixSceneDesc(group_shift, 1, (C.c_uint32 * 2)(0, 0))
+        self.L.check(self.L.lib.caelix_scene_create(device.handle, C.byref(desc), C.byref(handle)), "caelix_scene_create")
+        self.handle = handle
+        self.frame = 0
+
+    def close(self):
+        if self.handle:
+            self.L.lib.caelix_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload_bricks(self, keys, voxels):
+        import numpy as np
+
+        keys = np.ascontiguousarray(keys, np.int32)
+        voxels = np.ascontiguousarray(voxels, np.uint16)
+        consumed = C.c_uint32(0)
+        self.L.check(self.L.lib.caelix_scene_upload_bricks(self.handle, 0, len(keys), keys.ctypes.data,
+                                                           voxels.ctypes.data, C.byref(consumed)),
+                     "caelix_scene_upload_bricks")
+        return consumed.value
+
+    def set_brick_power(self, keys, power):
+        import numpy as np
+
+        keys = np.ascontiguousarray(keys, np.int32)
+        power = np.ascontiguousarray(power, np.float32)
+        self.L.check(self.L.lib.caelix_scene_set_brick_power(self.handle, 0, len(keys), keys.ctypes.data,
+                                                             power.ctypes.data), "caelix_scene_set_brick_power")
+
+    def set_albedo(self, albedo):
+        """Material table entries 0 .. len(albedo) - 1 with the given albedo (Lambertian)."""
+        entries = (CaelixMaterial * len(albedo))()
+        for i, a in enumerate(albedo):
+            entries[i].albedo[:] = [float(v) for v in a]
+            entries[i].ior = 1.5
+        self.L.check(self.L.lib.caelix_scene_set_materials(self.handle, entries, len(albedo)),
+                     "caelix_scene_set_materials")
+
+    def flush(self, stream: int = 0):
+        self.frame += 1
+        fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
+        self.L.check(self.L.lib.caelix_scene_flush(self.handle, C.byref(fd)), "caelix_scene_flush")
+
+    def view(self) -> CaelixSceneView:
+        v = CaelixSceneView()
+        self.L.check(self.L.lib.caelix_scene_get_view(self.handle, C.byref(v)), "caelix_scene_get_view")
+        return v
+
+    def light_stats(self) -> CaelixLightStats:
+        s = CaelixLightStats()
+        self.L.lib.caelix_scene_get_light_stats(self.handle, C.byref(s))
+        return s
+
+    @classmethod
+    def from_voxel_scene(cls, device: Device, vs):
+        """A device scene holding a workloads.VoxelScene (bricks, power, albedo), flushed."""
+        s = cls(device, vs.group_shift)
+        s.upload_bricks(vs.keys, vs.voxels)
+        emissive = vs.power > 0
+        if emissive.any():
+            s.set_brick_power(vs.keys[emissive], vs.power[emissive])
+        s.set_albedo(vs.albedo)
+        s.flush()
+        return s
+
+
+def camera_struct(cam) -> CaelixCamera:
+    c = CaelixCamera()
+    c.position[:] = [float(v) for v in cam["position"]]
+    c.right[:] = [float(v) for v in cam["right"]]
+    c.up[:] = [float(v) for v in cam["up"]]
+    c.forward[:] = [float(v) for v in cam["forward"]]
+    c.tan_half_fov_y = float(cam["tan_half_fov_y"])
+    c.aspect = float(cam["aspect"])
+    return c
+
+
+class Renderer:
+    """caelix_renderer_*: the trace of a scene into a device radiance buffer."""
+
+    def __init__(self, device: Device, scene: Scene):
+        self.device = device
+        self.scene = scene
+        self.L = device.L
+        handle = C.c_void_p()
+        self.L.check(self.L.lib.caelix_renderer_create(device.handle, scene.handle, C.byref(handle)),
+                     "caelix_renderer_create")
+        self.handle = handle
+        self.frame = 0
+
+    def close(self):
+        if self.handle:
+            self.L.lib.caelix_renderer_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_light_nee(self, enabled: bool):
+        o = CaelixLightNeeOptions(1 if enabled else 0, 0, 0, 0)
+        self.L.check(self.L.lib.caelix_renderer_set_light_nee_options(self.handle, C.byref(o)),
+                     "caelix_renderer_set_light_nee_options")
+
+    def render(self, radiance, width: int, height: int, camera, bounces: int = 4, seed: int = 1, spp: int = 1,
+               stream: int = 0):
+        self.frame += 1
+        fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
+        t = CaelixRenderTargets(_ptr(radiance), width, height)
+        cam = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
+        o = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+        self.L.check(self.L.lib.caelix_renderer_render(self.handle, C.byref(fd), C.byref(t), C.byref(cam), C.byref(o)),
+                     "caelix_renderer_render")
+
+    def stats(self) -> CaelixRenderStats:
+        s = CaelixRenderStats()
+        self.L.check(self.L.lib.caelix_renderer_get_stats(self.handle, C.byref(s)), "caelix_renderer_get_stats")
+        return s
+
+    def timings(self) -> CaelixGpuTimings:
+        t = CaelixGpuTimings()
+        self.L.lib.caelix_renderer_get_gpu_timings(self.handle, C.byref(t))
+        return t

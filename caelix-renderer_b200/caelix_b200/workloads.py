@@ -92,6 +92,117 @@ class Pcg32:
         return np.exp(mu + sigma * z).astype(np.float32)
 
 
+def pcg_hash(v: np.ndarray) -> np.ndarray:
+    """PcgHash of caelix_random.hlsl:18-23 (vectorised, uint32)."""
+    v = np.asarray(v, np.uint32)
+    with np.errstate(over="ignore"):
+        state = v * np.uint32(747796405) + np.uint32(2891336453)
+        word = ((state >> ((state >> np.uint32(28)) + np.uint32(4))) ^ state) * np.uint32(277803737)
+    return (word >> np.uint32(22)) ^ word
+
+
+def value_noise(p: np.ndarray, seed: int) -> np.ndarray:
+    """Seeded 3D value noise in [0, 1): lattice values from a PcgHash chain of the integer lattice
+    point and the seed, trilinear interpolation with smoothstep weights (float64)."""
+    p = np.asarray(p, np.float64)
+    i0 = np.floor(p).astype(np.int64)
+    f = p - i0
+    w = f * f * (3.0 - 2.0 * f)
+    s = pcg_hash(np.uint32(seed))
+
+    def lattice(ix, iy, iz):
+        h = pcg_hash(np.asarray(iz, np.int64).astype(np.uint32) ^ s)
+        h = pcg_hash(np.asarray(iy, np.int64).astype(np.uint32) ^ h)
+        h = pcg_hash(np.asarray(ix, np.int64).astype(np.uint32) ^ h)
+        return (h >> np.uint32(8)).astype(np.float64) / 16777216.0
+
+    out = np.zeros(p.shape[:-1])
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                v = lattice(i0[..., 0] + dx, i0[..., 1] + dy, i0[..., 2] + dz)
+                wx = w[..., 0] if dx else 1.0 - w[..., 0]
+                wy = w[..., 1] if dy else 1.0 - w[..., 1]
+                wz = w[..., 2] if dz else 1.0 - w[..., 2]
+                out += v * wx * wy * wz
+    return out
+
+
+class VoxelScene:
+    """A voxel world of 8^3-voxel bricks: brick keys (in increasing linear brick index), raw block
+    values (block-ID encoding: opaque = 0x8000 | material, 0 = air), per-brick emitter power,
+    the albedo table (indexed by the material id) and a camera."""
+
+    def __init__(self, grid, keys, voxels, power, albedo, camera, group_shift=4):
+        self.grid = tuple(int(g) for g in grid)
+        self.keys = np.ascontiguousarray(keys, np.int32)
+        self.voxels = np.ascontiguousarray(voxels, np.uint16)
+        self.power = np.ascontiguousarray(power, np.float32)
+        self.albedo = np.ascontiguousarray(albedo, np.float32)
+        self.camera = camera
+        self.group_shift = group_shift
+
+    @property
+    def brick_count(self):
+        return len(self.keys)
+
+
+def look_at(position, target, tan_half_fov_y=0.5, aspect=1.0):
+    """A camera (Unity convention: +X right, +Y up, +Z forward) at `position` looking at `target`."""
+    pos = np.asarray(position, np.float64)
+    fwd = np.asarray(target, np.float64) - pos
+    fwd /= np.linalg.norm(fwd)
+    right = np.cross(np.array([0.0, 1.0, 0.0]), fwd)
+    right /= np.linalg.norm(right)
+    up = np.cross(fwd, right)
+    return {
+        "position": pos.astype(np.float32),
+        "right": right.astype(np.float32),
+        "up": up.astype(np.float32),
+        "forward": fwd.astype(np.float32),
+        "tan_half_fov_y": np.float32(tan_half_fov_y),
+        "aspect": np.float32(aspect),
+    }
+
+
+def noise_world(grid_bricks=(16, 16, 16), brick_occupancy=0.30, voxel_fill=0.5, emissive_fraction=0.01,
+                seed=2, brick_scale=0.25, voxel_scale=0.25, camera=None) -> VoxelScene:
+    """The plain trace scene: a grid of bricks, the `brick_occupancy` fraction of them occupied
+    (the bricks with the highest value noise at brick scale), their voxels solid where the value
+    noise at voxel scale exceeds 1 - voxel_fill, materials uniform in [1, 64] (block-ID value
+    0x8000 | m), `emissive_fraction` of the occupied bricks emissive with power log-normal(0, 1),
+    albedo uniform in [0.1, 0.9] per material and channel. Seeded PCG32 streams of `seed`."""
+    gx, gy, gz = grid_bricks
+    total = gx * gy * gz
+    lin = np.arange(total, dtype=np.int64)
+    bx, by, bz = lin % gx, (lin // gx) % gy, lin // (gx * gy)
+    centres = np.stack([bx, by, bz], -1).astype(np.float64) + 0.5
+    nb = value_noise(centres * brick_scale, seed * 7919 + 1)
+    occupied_count = int(round(brick_occupancy * total))
+    order = np.lexsort((lin, -nb))  # highest noise first, ties by index
+    occupied = np.sort(order[:occupied_count])
+    keys = np.stack([bx[occupied], by[occupied], bz[occupied]], -1).astype(np.int32)
+    n = len(occupied)
+    v = np.arange(512)
+    vx, vy, vz = v % 8, (v // 8) % 8, v // 64
+    pos = (keys[:, None, :].astype(np.float64) * 8 + np.stack([vx, vy, vz], -1)[None, :, :] + 0.5)
+    nv = value_noise(pos * voxel_scale, seed * 7919 + 2)
+    solid = nv > (1.0 - voxel_fill)
+    mat = Pcg32(seed, 2).next_u32(n * 512).reshape(n, 512)
+    material = (np.uint32(1) + (mat >> np.uint32(26))).astype(np.uint16)
+    voxels = np.where(solid, np.uint16(0x8000) | material, np.uint16(0)).astype(np.uint16)
+    emitters = max(1, int(round(emissive_fraction * n)))
+    perm = np.lexsort((np.arange(n), Pcg32(seed, 3).next_u32(n)))
+    power = np.zeros(n, np.float32)
+    power[np.sort(perm[:emitters])] = Pcg32(seed, 4).lognormal(emitters)
+    albedo = np.zeros((128, 3), np.float32)
+    albedo[1:65] = (0.1 + 0.8 * Pcg32(seed, 5).next_doubles(64 * 3)).reshape(64, 3).astype(np.float32)
+    world = np.array([gx, gy, gz], np.float64) * 8
+    if camera is None:
+        camera = look_at(np.array([-0.25, 1.2, -0.35]) * world, world * np.array([0.5, 0.35, 0.5]))
+    return VoxelScene(grid_bricks, keys, voxels, power, albedo, camera)
+
+
 def pack_voxel(x, y, z) -> np.ndarray:
     return (np.asarray(x, np.uint32) | (np.asarray(y, np.uint32) << np.uint32(10)) |
             (np.asarray(z, np.uint32) << np.uint32(20))).astype(np.uint32)

@@ -1,0 +1,440 @@
+// The scene and renderer parts of the C ABI (include/caelix_b200.h): host-side brick staging,
+// the flush (scene_build) and the render call (trace_launch). Replaces the entry points of the
+// reference's lib/src/abi/caelix.cpp for the scene (:296-700) and the renderer (:700-953).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <new>
+#include <tuple>
+#include <vector>
+
+#include "../../include/caelix_b200.h"
+#include "abi_internal.h"
+#include "scene.cuh"
+#include "trace.cuh"
+
+using cx::log;
+
+namespace {
+
+using Key = std::tuple<int32_t, int32_t, int32_t>;
+
+constexpr int32_t kMaxKey = 1024;
+
+bool key_ok(const CaelixBrickKey& k)
+{
+    return k.x >= 0 && k.y >= 0 && k.z >= 0 && k.x < kMaxKey && k.y < kMaxKey && k.z < kMaxKey;
+}
+
+}  // namespace
+
+struct CaelixScene
+{
+    CaelixDevice* device = nullptr;
+    uint32_t group_shift = 4;
+    std::map<Key, std::vector<uint16_t>> bricks;
+    std::map<Key, float> power;
+    float albedo[cx::kMaterialSlots * 3];
+    CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
+    bool dirty = true;
+    uint64_t last_frame = 0;
+    cx::DeviceScene dev;
+    bool built = false;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t stop = nullptr;
+    float flush_ms = 0.0f;
+};
+
+struct CaelixRenderer
+{
+    CaelixDevice* device = nullptr;
+    CaelixScene* scene = nullptr;
+    CaelixLightNeeOptions nee{1, 0, 0, 0};
+    unsigned long long* counts = nullptr;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t stop = nullptr;
+    cudaStream_t last_stream = nullptr;
+    uint64_t frame_number = 0;
+    bool rendered = false;
+};
+
+#define CAELIX_GUARD_BEGIN try {
+#define CAELIX_GUARD_END                                             \
+    }                                                                \
+    catch (const std::bad_alloc&)                                    \
+    {                                                                \
+        log(CAELIX_LOG_ERROR, "%s: out of host memory", __func__);    \
+        return CAELIX_ERROR_OUT_OF_MEMORY;                           \
+    }                                                                \
+    catch (...)                                                      \
+    {                                                                \
+        log(CAELIX_LOG_ERROR, "%s: unexpected exception", __func__);  \
+        return CAELIX_ERROR_INVALID_ARGUMENT;                        \
+    }
+
+extern "C" {
+
+CAELIX_API CaelixResult caelix_scene_create(CaelixDevice* device, const CaelixSceneDesc* desc, CaelixScene** out_scene)
+{
+    CAELIX_GUARD_BEGIN
+    if (!device || !out_scene) return CAELIX_ERROR_INVALID_ARGUMENT;
+    *out_scene = nullptr;
+    uint32_t shift = 4;
+    if (desc) {
+        if (desc->reserved[0] || desc->reserved[1]) return CAELIX_ERROR_INVALID_ARGUMENT;
+        if (desc->encoding != 1) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_create: only the block-ID encoding (1) is implemented");
+            return desc->encoding == 0 ? CAELIX_ERROR_UNSUPPORTED : CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+        shift = desc->group_shift ? desc->group_shift : 4;
+        if (shift > 4) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_create: group_shift %u above 4 is not implemented", shift);
+            return CAELIX_ERROR_UNSUPPORTED;
+        }
+    }
+    cudaSetDevice(device->ordinal);
+    CaelixScene* s = new CaelixScene();
+    s->device = device;
+    s->group_shift = shift;
+    for (uint32_t i = 0; i < cx::kMaterialSlots * 3; ++i) s->albedo[i] = 0.5f;
+    cudaError_t e = cudaEventCreate(&s->start);
+    if (e == cudaSuccess) e = cudaEventCreate(&s->stop);
+    if (e != cudaSuccess) {
+        delete s;
+        return cx::cuda_result(e, "caelix_scene_create");
+    }
+    *out_scene = s;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
+{
+    if (!scene) return;
+    cudaSetDevice(scene->device->ordinal);
+    cx::scene_release(scene->dev);
+    if (scene->start) cudaEventDestroy(scene->start);
+    if (scene->stop) cudaEventDestroy(scene->stop);
+    delete scene;
+}
+
+CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                   const CaelixBrickKey* keys, const void* blocks, uint32_t* consumed)
+{
+    CAELIX_GUARD_BEGIN
+    if (consumed) *consumed = 0;
+    if (!scene || entity != 0 || (count && (!keys || !blocks))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!key_ok(keys[i])) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_upload_bricks: key (%d, %d, %d) outside [0, %d)", keys[i].x, keys[i].y,
+                keys[i].z, kMaxKey);
+            return CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    const uint16_t* b = static_cast<const uint16_t*>(blocks);
+    for (uint32_t i = 0; i < count; ++i) {
+        std::vector<uint16_t>& v = scene->bricks[Key(keys[i].x, keys[i].y, keys[i].z)];
+        v.assign(b + 512ull * i, b + 512ull * (i + 1));
+    }
+    scene->dirty = scene->dirty || count > 0;
+    if (consumed) *consumed = count;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                     const CaelixBrickKey* keys, const float* power)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || entity != 0 || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i)
+        if (!key_ok(keys[i]) || !std::isfinite(power[i]) || power[i] < 0.0f) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) scene->power[Key(keys[i].x, keys[i].y, keys[i].z)] = power[i];
+    scene->dirty = scene->dirty || count > 0;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_set_materials(CaelixScene* scene, const CaelixMaterial* entries, uint32_t count)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || (count && !entries) || count > cx::kMaterialSlots) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i)
+        for (int k = 0; k < 3; ++k)
+            if (!std::isfinite(entries[i].albedo[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < cx::kMaterialSlots; ++i)
+        for (int k = 0; k < 3; ++k) scene->albedo[3 * i + k] = i < count ? entries[i].albedo[k] : 0.5f;
+    scene->dirty = true;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const CaelixLightOptions* options)
+{
+    if (!scene || !options || options->enabled > 1 || !std::isfinite(options->min_emission) ||
+        options->min_emission < 0.0f || options->heap_bytes > (16ull << 32))
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    scene->light_options = *options;
+    scene->dirty = true;
+    return CAELIX_OK;
+}
+
+CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrameDesc* desc)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || !desc) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (desc->frame_number <= scene->last_frame || desc->safe_frame_number >= desc->frame_number) {
+        log(CAELIX_LOG_ERROR, "caelix_scene_flush: frame %llu after %llu (safe %llu) breaks the frame contract",
+            (unsigned long long)desc->frame_number, (unsigned long long)scene->last_frame,
+            (unsigned long long)desc->safe_frame_number);
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    }
+    scene->last_frame = desc->frame_number;
+    if (!scene->dirty) return CAELIX_OK;
+    cudaSetDevice(scene->device->ordinal);
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
+    // Bricks in increasing linear brick index of the grid spanned by the keys.
+    uint32_t grid[3] = {1, 1, 1};
+    for (const auto& kv : scene->bricks) {
+        grid[0] = std::max<uint32_t>(grid[0], std::get<0>(kv.first) + 1);
+        grid[1] = std::max<uint32_t>(grid[1], std::get<1>(kv.first) + 1);
+        grid[2] = std::max<uint32_t>(grid[2], std::get<2>(kv.first) + 1);
+    }
+    std::vector<std::pair<uint64_t, const std::pair<const Key, std::vector<uint16_t>>*>> order;
+    order.reserve(scene->bricks.size());
+    for (const auto& kv : scene->bricks) {
+        const uint64_t lin = (uint64_t)std::get<0>(kv.first) +
+                             grid[0] * ((uint64_t)std::get<1>(kv.first) + (uint64_t)grid[1] * std::get<2>(kv.first));
+        order.emplace_back(lin, &kv);
+    }
+    std::sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+    const uint32_t n = (uint32_t)order.size();
+    std::vector<int32_t> keys(3ull * n);
+    std::vector<uint16_t> voxels(512ull * n);
+    std::vector<float> power(n, 0.0f);
+    for (uint32_t i = 0; i < n; ++i) {
+        const Key& k = order[i].second->first;
+        keys[3 * i] = std::get<0>(k);
+        keys[3 * i + 1] = std::get<1>(k);
+        keys[3 * i + 2] = std::get<2>(k);
+        std::memcpy(voxels.data() + 512ull * i, order[i].second->second.data(), 1024);
+        const auto p = scene->power.find(k);
+        if (p != scene->power.end() && scene->light_options.enabled) power[i] = p->second;
+    }
+    uint32_t status = 0;
+    cudaEventRecord(scene->start, stream);
+    const cudaError_t e = cx::scene_build(scene->dev, grid, scene->group_shift, n, keys.data(), voxels.data(),
+                                          power.data(), scene->albedo, stream, &status);
+    cudaEventRecord(scene->stop, stream);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    cudaEventSynchronize(scene->stop);
+    cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
+    scene->dirty = false;
+    scene->built = true;
+    return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
+    CAELIX_GUARD_END
+}
+
+CAELIX_API void caelix_scene_get_light_stats(const CaelixScene* scene, CaelixLightStats* out)
+{
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    if (!scene || !scene->built || !scene->light_options.enabled) return;
+    const cx::DeviceScene& d = scene->dev;
+    unsigned char host[128];
+    cudaSetDevice(scene->device->ordinal);
+    if (cudaMemcpy(host, d.tree.header, 128, cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    cx::LightTreeHeader h;
+    cx::LightTreeState st;
+    std::memcpy(&h, host, 64);
+    std::memcpy(&st, host + 64, 64);
+    out->enabled = 1;
+    out->light_bricks = d.light_count;
+    out->heap_bytes_used = 4ull * d.heap_words;
+    out->heap_bytes_capacity = 4ull * d.heap_words;
+    out->passes = 1;
+    out->records_recomputed = d.light_count;
+    out->gpu_ms = scene->flush_ms;
+    out->tree_leaves[0] = h.leaf_count;
+    out->tree_nodes[0] = h.node_count;
+    out->tree_builds[0] = st.builds;
+    out->tree_leaves_dropped[0] = st.leaves_dropped;
+    std::vector<uint32_t> rows(8ull * d.group_count);
+    if (d.group_count &&
+        cudaMemcpy(rows.data(), d.group_rows, 32ull * d.group_count, cudaMemcpyDeviceToHost) == cudaSuccess) {
+        for (uint32_t g = 0; g < d.group_count; ++g) out->light_groups += rows[8ull * g + 5] ? 1u : 0u;
+    }
+    if (d.light_count) {
+        std::vector<cx::BrickLightRecord> hdr(d.light_count);
+        if (cudaMemcpy(hdr.data(), d.light_headers, sizeof(cx::BrickLightRecord) * d.light_count,
+                       cudaMemcpyDeviceToHost) == cudaSuccess)
+            for (const auto& r : hdr) out->light_faces += r.entry_count;
+    }
+}
+
+CAELIX_API CaelixResult caelix_scene_get_view(const CaelixScene* scene, CaelixSceneView* out)
+{
+    if (!scene || !out) return CAELIX_ERROR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    if (!scene->built) return CAELIX_OK;
+    const cx::DeviceScene& d = scene->dev;
+    for (int k = 0; k < 3; ++k) {
+        out->grid[k] = d.grid[k];
+        out->groups[k] = d.groups[k];
+    }
+    out->group_shift = d.group_shift;
+    out->brick_count = d.brick_count;
+    out->hash_capacity = d.hash_capacity;
+    out->hash_slot_count = d.hash_slot_count;
+    out->hash_max_probe = d.hash_max_probe;
+    out->light_count = d.light_count;
+    out->heap_words = d.heap_words;
+    out->group_count = d.group_count;
+    out->keys = reinterpret_cast<uint64_t>(d.keys);
+    out->records = reinterpret_cast<uint64_t>(d.records);
+    out->hash_slots = reinterpret_cast<uint64_t>(d.hash_slots);
+    out->bitmap = reinterpret_cast<uint64_t>(d.bitmap);
+    out->heap = reinterpret_cast<uint64_t>(d.heap);
+    out->group_rows = reinterpret_cast<uint64_t>(d.group_rows);
+    out->light_headers = reinterpret_cast<uint64_t>(d.light_headers);
+    out->light_group = reinterpret_cast<uint64_t>(d.light_group);
+    out->light_entry = reinterpret_cast<uint64_t>(d.light_entry);
+    out->light_brick = reinterpret_cast<uint64_t>(d.light_brick);
+    out->tree_header = reinterpret_cast<uint64_t>(d.tree.header);
+    out->tree_nodes = reinterpret_cast<uint64_t>(d.tree.nodes);
+    out->tree_leaves = reinterpret_cast<uint64_t>(d.tree.leaves);
+    return CAELIX_OK;
+}
+
+CAELIX_API uint64_t caelix_scene_get_light_tree(const CaelixScene* scene)
+{
+    if (!scene || !scene->built || !scene->light_options.enabled) return 0;
+    return reinterpret_cast<uint64_t>(scene->dev.tree.header);
+}
+
+CAELIX_API CaelixResult caelix_renderer_create(CaelixDevice* device, CaelixScene* scene, CaelixRenderer** out_renderer)
+{
+    CAELIX_GUARD_BEGIN
+    if (!device || !scene || !out_renderer || scene->device != device) return CAELIX_ERROR_INVALID_ARGUMENT;
+    *out_renderer = nullptr;
+    cudaSetDevice(device->ordinal);
+    CaelixRenderer* r = new CaelixRenderer();
+    r->device = device;
+    r->scene = scene;
+    cudaError_t e = cudaMalloc(&r->counts, 64);
+    if (e == cudaSuccess) e = cudaEventCreate(&r->start);
+    if (e == cudaSuccess) e = cudaEventCreate(&r->stop);
+    if (e != cudaSuccess) {
+        if (r->counts) cudaFree(r->counts);
+        delete r;
+        return cx::cuda_result(e, "caelix_renderer_create");
+    }
+    *out_renderer = r;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API void caelix_renderer_destroy(CaelixRenderer* renderer)
+{
+    if (!renderer) return;
+    cudaSetDevice(renderer->device->ordinal);
+    if (renderer->counts) cudaFree(renderer->counts);
+    if (renderer->start) cudaEventDestroy(renderer->start);
+    if (renderer->stop) cudaEventDestroy(renderer->stop);
+    delete renderer;
+}
+
+CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const CaelixFrameDesc* frame,
+                                               const CaelixRenderTargets* targets, const CaelixCamera* camera,
+                                               const CaelixRenderOptions* options)
+{
+    CAELIX_GUARD_BEGIN
+    if (!renderer || !frame || !targets || !camera || !options) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!targets->radiance || targets->width == 0 || targets->height == 0 || options->mode != 1 ||
+        options->bounce_count > 14 || camera->jitter[0] != 0.0f || camera->jitter[1] != 0.0f)
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t r : options->reserved)
+        if (r) return CAELIX_ERROR_INVALID_ARGUMENT;
+    CaelixScene* scene = renderer->scene;
+    if (!scene->built) {
+        log(CAELIX_LOG_ERROR, "caelix_renderer_render: the scene has not been flushed");
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    }
+    cudaSetDevice(renderer->device->ordinal);
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
+    cx::TraceParams p;
+    for (int k = 0; k < 3; ++k) {
+        p.position[k] = camera->position[k];
+        p.right[k] = camera->right[k];
+        p.up[k] = camera->up[k];
+        p.forward[k] = camera->forward[k];
+    }
+    p.tan_half_fov_y = camera->tan_half_fov_y;
+    p.aspect = camera->aspect;
+    p.width = targets->width;
+    p.height = targets->height;
+    p.spp = options->spp ? options->spp : 1;
+    p.bounce_count = options->bounce_count;
+    p.frame_seed = options->frame_seed;
+    p.light_nee = (renderer->nee.enabled && scene->light_options.enabled && scene->dev.light_count) ? 1u : 0u;
+    cudaError_t e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_render");
+    cudaEventRecord(renderer->start, stream);
+    e = cx::trace_launch(cx::scene_view(scene->dev), p, reinterpret_cast<float*>(targets->radiance), renderer->counts,
+                         stream);
+    cudaEventRecord(renderer->stop, stream);
+    renderer->last_stream = stream;
+    renderer->frame_number = frame->frame_number;
+    renderer->rendered = true;
+    return cx::cuda_result(e, "caelix_renderer_render");
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_renderer_set_light_nee_options(CaelixRenderer* renderer, const CaelixLightNeeOptions* options)
+{
+    if (!renderer || !options || options->enabled > 1 || options->flags != 0 || options->reserved != 0 ||
+        (options->hint_patch != 0 && options->hint_patch != 1 && options->hint_patch != 2 && options->hint_patch != 4)) {
+        log(CAELIX_LOG_ERROR, "caelix_renderer_set_light_nee_options: invalid options");
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    }
+    renderer->nee = *options;
+    return CAELIX_OK;
+}
+
+CAELIX_API void caelix_renderer_get_gpu_timings(const CaelixRenderer* renderer, CaelixGpuTimings* out)
+{
+    if (!out) return;
+    std::memset(out, 0, sizeof(*out));
+    if (!renderer) return;
+    cudaSetDevice(renderer->device->ordinal);
+    out->flush_ms = renderer->scene->flush_ms;
+    if (!renderer->rendered) return;
+    cudaEventSynchronize(renderer->stop);
+    float ms = 0.0f;
+    if (cudaEventElapsedTime(&ms, renderer->start, renderer->stop) == cudaSuccess) out->trace_ms = ms;
+    out->frame_number = renderer->frame_number;
+}
+
+CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, CaelixRenderStats* out)
+{
+    CAELIX_GUARD_BEGIN
+    if (!renderer || !out) return CAELIX_ERROR_INVALID_ARGUMENT;
+    std::memset(out, 0, sizeof(*out));
+    if (!renderer->rendered) return CAELIX_OK;
+    cudaSetDevice(renderer->device->ordinal);
+    cudaError_t e = cudaStreamSynchronize(renderer->last_stream);
+    unsigned long long c[3] = {0, 0, 0};
+    if (e == cudaSuccess) e = cudaMemcpy(c, renderer->counts, 24, cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_get_stats");
+    out->primary_rays = c[0];
+    out->bounce_rays = c[1];
+    out->shadow_rays = c[2];
+    out->kernel_launches = 1;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+}  // extern "C"

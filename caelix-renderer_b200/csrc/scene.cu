@@ -1,0 +1,767 @@
+// The scene build (scene.cuh): brick records (finalize), the canonical brick hash table, the
+// brick occupancy bitmap, the light records in group light blocks, and the light tree.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "cx_device.cuh"
+#include "radix_sort.cuh"
+#include "scene.cuh"
+#include "scene_device.cuh"
+
+namespace cx {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanItems = 4;
+constexpr uint32_t kScanTile = kThreads * kScanItems;
+
+__host__ __device__ __forceinline__ uint32_t part1by2(uint32_t v)
+{
+    v &= 0x3FFu;
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__host__ __device__ __forceinline__ uint32_t morton30(uint32_t x, uint32_t y, uint32_t z)
+{
+    return part1by2(x) | (part1by2(y) << 1) | (part1by2(z) << 2);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Single-pass scan with a decoupled look-back over tiles of kScanTile u32 values (30-bit
+// results). kMax: inclusive running maximum; else exclusive sum (the last tile writes the total).
+template <bool kMax>
+__global__ void __launch_bounds__(kThreads)
+    lookback_scan_kernel(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t count,
+                         uint32_t* states, uint32_t* tile_counter, uint32_t* total, uint32_t* status)
+{
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_warp[kThreads / 32];
+    __shared__ uint32_t s_prefix;
+    if (threadIdx.x == 0) s_tile = atomicAdd(tile_counter, 1u);
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t agg = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < count ? in[base + k] : 0u;
+        agg = kMax ? max(agg, v[k]) : agg + v[k];
+    }
+    // Block-level exclusive scan of the per-thread aggregates.
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint32_t inc = agg;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, inc, d);
+        if (lane >= d) inc = kMax ? max(inc, o) : inc + o;
+    }
+    if (lane == 31) s_warp[warp] = inc;
+    __syncthreads();
+    uint32_t before = 0, tile_agg = 0;
+#pragma unroll
+    for (int w = 0; w < kThreads / 32; ++w) {
+        const uint32_t s = s_warp[w];
+        if ((uint32_t)w < warp) before = kMax ? max(before, s) : before + s;
+        tile_agg = kMax ? max(tile_agg, s) : tile_agg + s;
+    }
+    uint32_t excl_in_warp = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
+    if (lane == 0) excl_in_warp = 0;
+    const uint32_t local = kMax ? max(before, excl_in_warp) : before + excl_in_warp;
+    if (threadIdx.x == 0) {
+        uint32_t prefix = 0;
+        uint32_t* state = states + tile;
+        if (tile == 0) {
+            st_relaxed(state, kTileFlagPrefix | (tile_agg & kTileValueMask));
+        } else {
+            st_relaxed(state, kTileFlagAggregate | (tile_agg & kTileValueMask));
+            int64_t j = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                const uint32_t s = ld_relaxed(states + j);
+                if ((s & ~kTileValueMask) == 0) {
+                    if (!spin_wait(spins)) {
+                        atomicOr(status, kStatusLookbackTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                prefix = kMax ? max(prefix, s & kTileValueMask) : prefix + (s & kTileValueMask);
+                if (s & kTileFlagPrefix) break;
+                --j;
+            }
+            const uint32_t incl = kMax ? max(prefix, tile_agg) : prefix + tile_agg;
+            st_relaxed(state, kTileFlagPrefix | (incl & kTileValueMask));
+        }
+        s_prefix = prefix;
+        if (!kMax && tile == gridDim.x - 1 && total) *total = prefix + tile_agg;
+    }
+    __syncthreads();
+    uint32_t run = kMax ? max(s_prefix, local) : s_prefix + local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (kMax) {
+            run = max(run, v[k]);
+            if (base + k < count) out[base + k] = run;
+        } else {
+            if (base + k < count) out[base + k] = run;
+            run += v[k];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Hash table.
+
+__global__ void hash_home_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t capacity,
+                                 uint32_t* __restrict__ lo, uint32_t* __restrict__ hi, uint32_t* __restrict__ home)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t l, h;
+    hash_fingerprint(keys[3 * i], keys[3 * i + 1], keys[3 * i + 2], l, h);
+    lo[i] = l;
+    hi[i] = h;
+    home[i] = hash_home(l, capacity);
+}
+
+// v_k = home_k - k + n over the homes in sorted order (the input of the running maximum).
+__global__ void hash_shift_kernel(const uint32_t* __restrict__ home_sorted, uint32_t n, uint32_t* __restrict__ v)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k < n) v[k] = home_sorted[k] + n - k;
+}
+
+// pos_k = k + max_{j <= k} v_j - n: the first free slot at or after the home in (home, brick) order.
+__global__ void hash_place_kernel(const uint32_t* __restrict__ running_max, const uint32_t* __restrict__ home_sorted,
+                                  const uint32_t* __restrict__ order, const uint32_t* __restrict__ lo,
+                                  const uint32_t* __restrict__ hi, uint32_t n, uint4* __restrict__ slots,
+                                  uint32_t* max_probe)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t pos = k + running_max[k] - n;
+    const uint32_t b = order[k];
+    slots[pos] = make_uint4(lo[b], hi[b], b, 0u);
+    atomicMax(max_probe, pos - home_sorted[k]);
+}
+
+__global__ void bitmap_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t gx, uint32_t gy,
+                              uint32_t* __restrict__ bitmap)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint64_t c = (uint64_t)keys[3 * i] + gx * ((uint64_t)keys[3 * i + 1] + (uint64_t)gy * keys[3 * i + 2]);
+    atomicOr(bitmap + (c >> 5), 1u << (c & 31));
+}
+
+// ---------------------------------------------------------------------------------------------
+// Finalize (caelix_finalize.hlsl:110-340): one CTA of 64 threads per brick, thread t owns the
+// voxel row y = t & 7, z = t >> 3.
+
+struct FinalizeArgs
+{
+    const int32_t* keys;
+    const uint16_t* voxels;
+    uint32_t n;
+    uint32_t group_shift;
+    const uint4* slots;
+    uint32_t capacity;
+    uint32_t max_probe;
+    uint32_t* records;
+};
+
+__global__ void __launch_bounds__(64) finalize_kernel(const FinalizeArgs a)
+{
+    __shared__ uint32_t s_nbr[6];
+    __shared__ uint16_t s_vox[512];
+    __shared__ uint32_t s_occ[16];
+    __shared__ int s_min[3], s_max[3];
+    const uint32_t b = blockIdx.x;
+    const uint32_t t = threadIdx.x;
+    const uint32_t y = t & 7, z = t >> 3;
+    const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
+    if (t < 6) {
+        const int dx = t == 0 ? 1 : (t == 1 ? -1 : 0);
+        const int dy = t == 2 ? 1 : (t == 3 ? -1 : 0);
+        const int dz = t == 4 ? 1 : (t == 5 ? -1 : 0);
+        s_nbr[t] = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
+    }
+    if (t < 16) s_occ[t] = 0;
+    if (t < 3) {
+        s_min[t] = 8;
+        s_max[t] = -1;
+    }
+    const uint16_t* own = a.voxels + 512ull * b;
+    for (uint32_t i = t; i < 512; i += 64) s_vox[i] = own[i];
+    __syncthreads();
+    auto nbr_voxel = [&](int d, uint32_t vx, uint32_t vy, uint32_t vz) -> uint32_t {
+        const uint32_t r = s_nbr[d];
+        return r == 0xFFFFFFFFu ? 0u : (uint32_t)a.voxels[512ull * r + vx + 8 * vy + 64 * vz];
+    };
+    uint32_t out_words[4] = {0, 0, 0, 0};
+    uint32_t occupied = 0;
+#pragma unroll
+    for (uint32_t x = 0; x < 8; ++x) {
+        const uint32_t raw = s_vox[x + 8 * y + 64 * z];
+        const uint32_t v = (raw & kOpaqueBit) ? raw : (raw & 0x1FFu);
+        uint32_t nb[6];
+        nb[0] = x < 7 ? s_vox[(x + 1) + 8 * y + 64 * z] : nbr_voxel(0, 0, y, z);
+        nb[1] = x > 0 ? s_vox[(x - 1) + 8 * y + 64 * z] : nbr_voxel(1, 7, y, z);
+        nb[2] = y < 7 ? s_vox[x + 8 * (y + 1) + 64 * z] : nbr_voxel(2, x, 0, z);
+        nb[3] = y > 0 ? s_vox[x + 8 * (y - 1) + 64 * z] : nbr_voxel(3, x, 7, z);
+        nb[4] = z < 7 ? s_vox[x + 8 * y + 64 * (z + 1)] : nbr_voxel(4, x, y, 0);
+        nb[5] = z > 0 ? s_vox[x + 8 * y + 64 * (z - 1)] : nbr_voxel(5, x, y, 7);
+        uint32_t opaque_count = 0, faces = 0;
+#pragma unroll
+        for (int d = 0; d < 6; ++d) {
+            const bool nop = (nb[d] & kOpaqueBit) != 0;
+            opaque_count += nop ? 1u : 0u;
+            if (!nop && (nb[d] & 0x1FFu) != v) faces |= 1u << d;
+        }
+        const bool alive = opaque_count < 6;
+        const uint32_t result = (v & kOpaqueBit) ? v : (v | (faces << 9));
+        const bool iface = (v & kOpaqueBit) != 0 || faces != 0;
+        if (alive && result != 0 && iface) occupied |= 1u << x;
+        out_words[x >> 1] |= (x & 1) ? (result << 16) : result;
+    }
+    uint32_t* rec = a.records + (uint64_t)b * kRecordWords;
+#pragma unroll
+    for (int w = 0; w < 4; ++w) rec[kRecordPayloadWord + 4 * y + 32 * z + w] = out_words[w];
+    if (occupied) {
+        const uint32_t micro_base = ((y & 3) << 2) | ((z & 3) << 4);
+        const uint32_t coarse_yz = ((y >> 2) << 1) | ((z >> 2) << 2);
+        const uint32_t word = micro_base >> 5, bit = micro_base & 31;
+        const uint32_t low = occupied & 0xFu, high = occupied >> 4;
+        if (low) atomicOr(&s_occ[coarse_yz * 2 + word], low << bit);
+        if (high) atomicOr(&s_occ[(coarse_yz | 1u) * 2 + word], high << bit);
+        atomicMin(&s_min[0], __ffs(occupied) - 1);
+        atomicMax(&s_max[0], 31 - __clz(occupied));
+        atomicMin(&s_min[1], (int)y);
+        atomicMax(&s_max[1], (int)y);
+        atomicMin(&s_min[2], (int)z);
+        atomicMax(&s_max[2], (int)z);
+    }
+    __syncthreads();
+    if (t < 16) rec[2 + t] = s_occ[t];
+    if (t == 0) {
+        uint32_t coarse = 0;
+        for (int c = 0; c < 8; ++c)
+            if (s_occ[2 * c] | s_occ[2 * c + 1]) coarse |= 1u << c;
+        uint32_t bounds = 0;
+        if (s_max[0] >= 0)
+            bounds = (uint32_t)s_min[0] | ((uint32_t)s_min[1] << 3) | ((uint32_t)s_min[2] << 6) |
+                     ((uint32_t)s_max[0] << 9) | ((uint32_t)s_max[1] << 12) | ((uint32_t)s_max[2] << 15);
+        const uint32_t gm = (1u << a.group_shift) - 1u;
+        const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << a.group_shift) |
+                             (((uint32_t)bz & gm) << (2 * a.group_shift));
+        rec[0] = (pos & 0xFFFFu) | (coarse << 16);
+        rec[1] = bounds;
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Light records (caelix_light_tree_build.hlsl:93-285): light voxel = opaque voxel of a brick with
+// emitter power; its open faces are the entries.
+
+struct LightArgs
+{
+    const int32_t* keys;
+    const uint16_t* voxels;
+    const float* power;
+    uint32_t n;
+    uint32_t group_shift;
+    uint32_t groups[3];
+    const uint4* slots;
+    uint32_t capacity;
+    uint32_t max_probe;
+};
+
+__global__ void light_collect_kernel(const LightArgs a, uint32_t* counter, uint32_t* lkeys, uint32_t* lbricks)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n || !(a.power[i] > 0.0f)) return;
+    const uint32_t gs = a.group_shift, gm = (1u << gs) - 1u;
+    const uint32_t bx = (uint32_t)a.keys[3 * i], by = (uint32_t)a.keys[3 * i + 1], bz = (uint32_t)a.keys[3 * i + 2];
+    const uint32_t g = (bx >> gs) + a.groups[0] * ((by >> gs) + a.groups[1] * (bz >> gs));
+    const uint32_t slot = atomicAdd(counter, 1u);
+    lkeys[slot] = (g << (3 * gs)) | morton30(bx & gm, by & gm, bz & gm);
+    lbricks[slot] = i;
+}
+
+// The open faces of the 16 voxels of lane `lane` of brick b: open[v] bit f, and the voxel values.
+__device__ __forceinline__ void lane_open_faces(const LightArgs& a, uint32_t b, uint32_t lane, uint32_t open[16],
+                                                uint32_t value[16])
+{
+    const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
+    uint32_t my_nbr = 0xFFFFFFFFu;
+    if (lane < 6) {
+        const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
+        const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
+        const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
+        my_nbr = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
+    }
+    uint32_t nbr[6];
+#pragma unroll
+    for (int d = 0; d < 6; ++d) nbr[d] = __shfl_sync(0xFFFFFFFFu, my_nbr, d);
+    const uint16_t* own = a.voxels + 512ull * b;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const uint32_t vi = lane * 16 + k;
+        const int x = vi & 7, y = (vi >> 3) & 7, z = vi >> 6;
+        const uint32_t v = own[vi];
+        value[k] = v;
+        open[k] = 0;
+        if (!(v & kOpaqueBit)) continue;
+        const int dx[6] = {1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, 1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, 1, -1};
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            int nx = x + dx[f], ny = y + dy[f], nz = z + dz[f];
+            uint32_t nv;
+            if (nx >= 0 && nx < 8 && ny >= 0 && ny < 8 && nz >= 0 && nz < 8) {
+                nv = own[nx + 8 * ny + 64 * nz];
+            } else {
+                const uint32_t r = nbr[f];
+                nx &= 7;
+                ny &= 7;
+                nz &= 7;
+                nv = r == 0xFFFFFFFFu ? 0u : (uint32_t)a.voxels[512ull * r + nx + 8 * ny + 64 * nz];
+            }
+            if (!(nv & kOpaqueBit)) open[k] |= 1u << f;
+        }
+    }
+}
+
+// Warp per light brick (sorted order): the family counts and the record's units.
+__global__ void __launch_bounds__(128) light_measure_kernel(const LightArgs a, const uint32_t* __restrict__ lbricks,
+                                                            uint32_t m, uint32_t* __restrict__ counts6,
+                                                            uint32_t* __restrict__ units)
+{
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (k >= m) return;
+    uint32_t open[16], value[16];
+    lane_open_faces(a, lbricks[k], lane, open, value);
+    uint32_t total = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        uint32_t c = 0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) c += (open[q] >> f) & 1u;
+        c = __reduce_add_sync(0xFFFFFFFFu, c);
+        if (lane == 0) counts6[6 * k + f] = c;
+        total += c;
+    }
+    if (lane == 0) units[k] = 3 + (4 * total + 15) / 16;
+}
+
+// Per light: its block's extra units (header + index entries) when it starts its group.
+__global__ void light_group_kernel(const uint32_t* __restrict__ lkeys, uint32_t m, uint32_t gshift,
+                                   const uint32_t* __restrict__ units, uint32_t* __restrict__ total_units,
+                                   uint32_t* __restrict__ group_start)
+{
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= m) return;
+    const uint32_t g = lkeys[k] >> (3 * gshift);
+    // The group's first light (binary search for the first key of group g).
+    uint32_t lo = 0, hi = k;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((lkeys[mid] >> (3 * gshift)) < g) lo = mid + 1;
+        else hi = mid;
+    }
+    const uint32_t start = lo;
+    group_start[k] = start;
+    uint32_t extra = 0;
+    if (k == start) {
+        uint32_t a = k, b = m;
+        while (a < b) {
+            const uint32_t mid = (a + b) >> 1;
+            if ((lkeys[mid] >> (3 * gshift)) <= g) a = mid + 1;
+            else b = mid;
+        }
+        extra = 1 + (a - k);
+    }
+    total_units[k] = units[k] + extra;
+}
+
+struct LightWriteArgs
+{
+    LightArgs a;
+    const uint32_t* lkeys;
+    const uint32_t* lbricks;
+    uint32_t m;
+    const uint32_t* counts6;
+    const uint32_t* units;
+    const uint32_t* offsets;  // exclusive scan of the total units
+    const uint32_t* group_start;
+    uint32_t total;  // all units
+    uint32_t* heap;
+    uint32_t* group_rows;
+    BrickLightRecord* headers;
+    uint32_t* light_group;
+    uint32_t* light_entry;
+    uint32_t* light_brick;
+};
+
+__global__ void __launch_bounds__(128) light_write_kernel(const LightWriteArgs w)
+{
+    const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
+    if (k >= w.m) return;
+    const LightArgs& a = w.a;
+    const uint32_t b = w.lbricks[k];
+    const uint32_t gs = a.group_shift;
+    const uint32_t g = w.lkeys[k] >> (3 * gs);
+    const uint32_t s = w.group_start[k];
+    // The group's light count: the next group's start, or the end.
+    const uint32_t block = 1 + w.offsets[s];
+    uint32_t count;
+    {
+        uint32_t lo = s, hi = w.m;
+        while (lo < hi) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if ((w.lkeys[mid] >> (3 * gs)) <= g) lo = mid + 1;
+            else hi = mid;
+        }
+        count = lo - s;
+    }
+    const uint32_t rec_unit = 1 + w.offsets[k] + (k == s ? 1 + count : 0);
+    uint32_t* rec = w.heap + 4ull * rec_unit;
+    uint32_t open[16], value[16];
+    lane_open_faces(a, b, lane, open, value);
+    const float P = a.power[b];
+    const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f;
+    uint32_t fam_count[6], fam_base[6], cursor[6];
+    uint32_t written = 0;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        fam_count[f] = w.counts6[6 * k + f];
+        fam_base[f] = written;
+        written += fam_count[f];
+        uint32_t c = 0;
+#pragma unroll
+        for (int q = 0; q < 16; ++q) c += (open[q] >> f) & 1u;
+        const uint32_t inc = warp_inclusive_sum(c);
+        cursor[f] = inc - c;
+    }
+    float sums[6] = {0, 0, 0, 0, 0, 0};
+    uint32_t lo[3] = {8, 8, 8}, hi[3] = {0, 0, 0};
+#pragma unroll
+    for (int q = 0; q < 16; ++q) {
+        if (!open[q]) continue;
+        const uint32_t vi = lane * 16 + q;
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if ((open[q] >> f) & 1u) {
+                rec[12 + fam_base[f] + cursor[f]] = vi | (value[q] << 16);
+                ++cursor[f];
+                sums[f] += weight;
+            }
+        }
+        const uint32_t p[3] = {vi & 7u, (vi >> 3) & 7u, vi >> 6};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            lo[c] = min(lo[c], p[c]);
+            hi[c] = max(hi[c], p[c] + 1);
+        }
+    }
+#pragma unroll
+    for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+        for (int f = 0; f < 6; ++f) sums[f] += __shfl_down_sync(0xFFFFFFFFu, sums[f], off);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        lo[c] = __reduce_min_sync(0xFFFFFFFFu, lo[c]);
+        hi[c] = __reduce_max_sync(0xFFFFFFFFu, hi[c]);
+    }
+    // Zero padding of the record's last unit.
+    const uint32_t padded = (w.units[k] - 3) * 4;
+    for (uint32_t e = written + lane; e < padded; e += 32) rec[12 + e] = 0u;
+    if (lane == 0) {
+        const uint32_t gm = (1u << gs) - 1u;
+        const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
+        const uint32_t org[3] = {((uint32_t)bx & gm) * 8, ((uint32_t)by & gm) * 8, ((uint32_t)bz & gm) * 8};
+        if (written == 0) {
+            lo[0] = lo[1] = lo[2] = 0;
+            hi[0] = hi[1] = hi[2] = 0;
+        }
+        const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << gs) | (((uint32_t)bz & gm) << (2 * gs));
+        BrickLightRecord h;
+        for (int f = 0; f < 6; ++f) h.face[f] = sums[f];
+        h.box_lo = (org[0] + lo[0]) | ((org[1] + lo[1]) << 10) | ((org[2] + lo[2]) << 20);
+        h.box_hi = (org[0] + hi[0]) | ((org[1] + hi[1]) << 10) | ((org[2] + hi[2]) << 20);
+        h.pos = pos;
+        h.entry_count = written;
+        h.counts_lo = fam_count[0] | (fam_count[1] << 10) | (fam_count[2] << 20);
+        h.counts_hi = fam_count[3] | (fam_count[4] << 10) | (fam_count[5] << 20);
+        const uint4* hp = reinterpret_cast<const uint4*>(&h);
+        uint4* r4 = reinterpret_cast<uint4*>(rec);
+        r4[0] = hp[0];
+        r4[1] = hp[1];
+        r4[2] = hp[2];
+        w.headers[k] = h;
+        const uint32_t entry = k - s;
+        uint32_t* ie = w.heap + 4ull * (block + 1 + entry);
+        ie[0] = pos;
+        ie[1] = b;
+        ie[2] = rec_unit - block;
+        ie[3] = k;
+        w.light_group[k] = g;
+        w.light_entry[k] = entry;
+        w.light_brick[k] = b;
+        atomicAdd(w.group_rows + 8ull * g + 6, written);  // the group's light faces
+        if (k == s) {
+            uint32_t* bh = w.heap + 4ull * block;
+            bh[0] = count;
+            bh[1] = bh[2] = bh[3] = 0;
+            const uint32_t end = count + s < w.m ? w.offsets[s + count] : w.total;
+            uint32_t* row = w.group_rows + 8ull * g;
+            row[0] = block;
+            row[1] = end - w.offsets[s];
+            row[2] = 0;
+            row[3] = 0;
+            row[4] = 0;
+            row[5] = count;
+            row[7] = 0;
+        }
+    }
+}
+
+uint32_t blocks_for(uint64_t n, uint32_t per) { return (uint32_t)std::max<uint64_t>(1, (n + per - 1) / per); }
+
+template <typename T>
+cudaError_t alloc(T*& p, uint64_t count)
+{
+    if (p) cudaFree(p);
+    p = nullptr;
+    return cudaMalloc(&p, std::max<uint64_t>(count, 1) * sizeof(T));
+}
+
+#define CX_TRY(x)                              \
+    do {                                       \
+        const cudaError_t e_ = (x);            \
+        if (e_ != cudaSuccess) return e_;      \
+    } while (0)
+
+cudaError_t run_scan(bool max_op, const uint32_t* in, uint32_t* out, uint32_t count, uint32_t* scratch,
+                     uint32_t* total, uint32_t* status, cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    const uint32_t tiles = blocks_for(count, kScanTile);
+    uint32_t* counter = scratch;
+    uint32_t* states = scratch + 1;
+    CX_TRY(cudaMemsetAsync(scratch, 0, (1 + (uint64_t)tiles) * 4, stream));
+    if (max_op)
+        lookback_scan_kernel<true><<<tiles, kThreads, 0, stream>>>(in, out, count, states, counter, total, status);
+    else
+        lookback_scan_kernel<false><<<tiles, kThreads, 0, stream>>>(in, out, count, states, counter, total, status);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+SceneView scene_view(const DeviceScene& s)
+{
+    SceneView v;
+    for (int k = 0; k < 3; ++k) {
+        v.grid[k] = s.grid[k];
+        v.groups[k] = s.groups[k];
+    }
+    v.group_shift = s.group_shift;
+    v.brick_count = s.brick_count;
+    v.records = s.records;
+    v.hash_slots = s.hash_slots;
+    v.hash_capacity = s.hash_capacity;
+    v.hash_max_probe = s.hash_max_probe;
+    v.bitmap = s.bitmap;
+    v.power = s.power;
+    v.albedo = s.albedo;
+    v.heap = s.heap;
+    v.group_rows = s.group_rows;
+    v.frames = s.frames;
+    v.leaves = s.tree.leaves;
+    v.nodes = s.tree.nodes;
+    v.header = s.tree.header;
+    v.light_count = s.light_count;
+    v.group_count = s.group_count;
+    return v;
+}
+
+void scene_release(DeviceScene& s)
+{
+    void* ptrs[] = {s.keys, s.voxels, s.power, s.records, s.hash_slots, s.bitmap, s.albedo, s.heap, s.group_rows,
+                    s.frames, s.light_headers, s.light_group, s.light_entry, s.light_brick, s.scratch,
+                    s.tree_memory, s.status};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    s = DeviceScene();
+}
+
+cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t n, const int32_t* keys,
+                        const uint16_t* voxels, const float* power, const float* albedo, cudaStream_t stream,
+                        uint32_t* device_status_out)
+{
+    for (int k = 0; k < 3; ++k) s.grid[k] = grid[k];
+    s.group_shift = group_shift;
+    const uint32_t gm = (1u << group_shift) - 1u;
+    for (int k = 0; k < 3; ++k) s.groups[k] = (grid[k] + gm) >> group_shift;
+    s.group_count = s.groups[0] * s.groups[1] * s.groups[2];
+    s.brick_count = n;
+    if (!s.status) CX_TRY(cudaMalloc(&s.status, 64));
+    CX_TRY(cudaMemsetAsync(s.status, 0, 64, stream));
+
+    // Inputs.
+    CX_TRY(alloc(s.keys, 3ull * n));
+    CX_TRY(alloc(s.voxels, 512ull * n));
+    CX_TRY(alloc(s.power, n));
+    CX_TRY(alloc(s.albedo, kMaterialSlots * 3));
+    CX_TRY(cudaMemcpyAsync(s.keys, keys, 12ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.voxels, voxels, 1024ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.power, power, 4ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.albedo, albedo, 12ull * kMaterialSlots, cudaMemcpyHostToDevice, stream));
+
+    // Scratch: 8 arrays of n words, 6 n words of family counts, the sort scratch, scan states.
+    const uint64_t sort_words = sort_scratch_words(std::max(n, 1u));
+    const uint64_t need = 14ull * std::max(n, 1u) + sort_words + 2 + blocks_for(std::max(n, 1u), kScanTile) + 64;
+    if (need > s.scratch_words) {
+        CX_TRY(alloc(s.scratch, need));
+        s.scratch_words = need;
+    }
+    uint32_t* w = s.scratch;
+    uint32_t* lo = w;
+    uint32_t* hi = w + n;
+    uint32_t* home = w + 2ull * n;
+    uint32_t* order = w + 3ull * n;
+    uint32_t* home_alt = w + 4ull * n;
+    uint32_t* order_alt = w + 5ull * n;
+    uint32_t* tmp = w + 6ull * n;
+    uint32_t* tmp2 = w + 7ull * n;
+    uint32_t* counts6 = w + 8ull * n;
+    uint32_t* sortw = w + 14ull * n;
+    uint32_t* small = sortw + sort_words;  // scan scratch and counters
+
+    // Hash table.
+    s.hash_capacity = std::max(2u * n, 2u);
+    s.hash_slot_count = s.hash_capacity + n + 1;
+    CX_TRY(alloc(s.hash_slots, s.hash_slot_count));
+    CX_TRY(cudaMemsetAsync(s.hash_slots, 0, 16ull * s.hash_slot_count, stream));
+    uint32_t* d_max_probe = s.status + 4;
+    if (n > 0) {
+        hash_home_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, s.hash_capacity, lo, hi, home);
+        CX_TRY(cudaMemsetAsync(sortw, 0, sort_words * 4, stream));
+        radix_histogram(home, n, sortw, std::min<uint32_t>(blocks_for(n, 2048), 148 * 4), stream);
+        onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream);
+        hash_shift_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(home, n, tmp);
+        CX_TRY(run_scan(true, tmp, tmp2, n, small, nullptr, s.status, stream));
+        hash_place_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(tmp2, home, order, lo, hi, n, s.hash_slots,
+                                                                            d_max_probe);
+    }
+    // Bitmap.
+    const uint64_t cells = (uint64_t)grid[0] * grid[1] * grid[2];
+    CX_TRY(alloc(s.bitmap, (cells + 31) / 32));
+    CX_TRY(cudaMemsetAsync(s.bitmap, 0, 4 * ((cells + 31) / 32), stream));
+    if (n > 0) bitmap_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, grid[0], grid[1], s.bitmap);
+    CX_TRY(cudaMemcpyAsync(&s.hash_max_probe, d_max_probe, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaStreamSynchronize(stream));
+
+    // Records.
+    CX_TRY(alloc(s.records, (uint64_t)kRecordWords * n));
+    CX_TRY(cudaMemsetAsync(s.records, 0, 4ull * kRecordWords * n, stream));
+    if (n > 0) {
+        FinalizeArgs fa{s.keys, s.voxels, n, group_shift, s.hash_slots, s.hash_capacity, s.hash_max_probe, s.records};
+        finalize_kernel<<<n, 64, 0, stream>>>(fa);
+    }
+
+    // Light records.
+    LightArgs la{s.keys, s.voxels, s.power, n, group_shift, {s.groups[0], s.groups[1], s.groups[2]},
+                 s.hash_slots, s.hash_capacity, s.hash_max_probe};
+    uint32_t* d_light_count = s.status + 5;
+    uint32_t* lkeys = lo;  // reuse the hash scratch
+    uint32_t* lbricks = hi;
+    uint32_t* lkeys_alt = home_alt;
+    uint32_t* lbricks_alt = order_alt;
+    if (n > 0) light_collect_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+    uint32_t m = 0;
+    CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaStreamSynchronize(stream));
+    s.light_count = m;
+    CX_TRY(alloc(s.group_rows, 8ull * s.group_count));
+    CX_TRY(cudaMemsetAsync(s.group_rows, 0, 32ull * s.group_count, stream));
+    CX_TRY(alloc(s.light_headers, m));
+    CX_TRY(alloc(s.light_group, m));
+    CX_TRY(alloc(s.light_entry, m));
+    CX_TRY(alloc(s.light_brick, m));
+    std::vector<GroupFrame> frames(s.group_count);
+    for (uint32_t g = 0; g < s.group_count; ++g) {
+        const uint32_t gx = g % s.groups[0], gy = (g / s.groups[0]) % s.groups[1], gz = g / (s.groups[0] * s.groups[1]);
+        GroupFrame f;
+        std::memset(&f, 0, sizeof(f));
+        f.origin[0] = (float)(gx * (8u << group_shift));
+        f.origin[1] = (float)(gy * (8u << group_shift));
+        f.origin[2] = (float)(gz * (8u << group_shift));
+        f.rot[0] = f.rot[4] = f.rot[8] = 1.0f;
+        frames[g] = f;
+    }
+    CX_TRY(alloc(s.frames, s.group_count));
+    CX_TRY(cudaMemcpyAsync(s.frames, frames.data(), sizeof(GroupFrame) * s.group_count, cudaMemcpyHostToDevice, stream));
+    uint32_t total_units = 0;
+    if (m > 0) {
+        CX_TRY(cudaMemsetAsync(sortw, 0, sort_scratch_words(m) * 4, stream));
+        radix_histogram(lkeys, m, sortw, std::min<uint32_t>(blocks_for(m, 2048), 148 * 4), stream);
+        onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream);
+        uint32_t* units = home;    // m words
+        uint32_t* totals = order;  // m words
+        uint32_t* group_start = tmp;
+        uint32_t* offsets = tmp2;
+        light_measure_kernel<<<blocks_for(32ull * m, 128), 128, 0, stream>>>(la, lbricks, m, counts6, units);
+        light_group_kernel<<<blocks_for(m, kThreads), kThreads, 0, stream>>>(lkeys, m, group_shift, units, totals,
+                                                                             group_start);
+        uint32_t* d_total = s.status + 6;
+        CX_TRY(run_scan(false, totals, offsets, m, small, d_total, s.status, stream));
+        CX_TRY(cudaMemcpyAsync(&total_units, d_total, 4, cudaMemcpyDeviceToHost, stream));
+        CX_TRY(cudaStreamSynchronize(stream));
+        s.heap_words = 4 * (1 + total_units);
+        CX_TRY(alloc(s.heap, s.heap_words));
+        CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
+        LightWriteArgs wa{la, lkeys, lbricks, m, counts6, units, offsets, group_start, total_units, s.heap,
+                          s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick};
+        light_write_kernel<<<blocks_for(32ull * m, 128), 128, 0, stream>>>(wa);
+    } else {
+        s.heap_words = 4;
+        CX_TRY(alloc(s.heap, 4));
+        CX_TRY(cudaMemsetAsync(s.heap, 0, 16, stream));
+    }
+
+    // The light tree over the light records (leaf = gather order).
+    const uint32_t cap = std::max(m, 1u);
+    if (cap > s.tree_capacity) {
+        if (s.tree_memory) cudaFree(s.tree_memory);
+        s.tree_memory = nullptr;
+        CX_TRY(cudaMalloc(&s.tree_memory, lt_buffer_bytes(cap)));
+        s.tree = lt_carve(s.tree_memory, cap);
+        s.tree_capacity = cap;
+        CX_TRY(cudaMemsetAsync(s.tree.header, 0, 128, stream));
+    }
+    LightBvhInput in;
+    in.records = s.light_headers;
+    in.count = m;
+    in.record_group = s.light_group;
+    in.record_entry = s.light_entry;
+    in.group_frames = s.frames;
+    in.group_count = s.group_count;
+    CX_TRY(lt_build(s.tree, in, stream, nullptr));
+    uint32_t status[2] = {0, 0};
+    CX_TRY(cudaMemcpyAsync(status, s.status, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaMemcpyAsync(status + 1, &s.tree.state->status, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaStreamSynchronize(stream));
+    if (device_status_out) *device_status_out = status[0] | status[1];
+    return cudaGetLastError();
+}
+
+}  // namespace cx

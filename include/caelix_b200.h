@@ -219,6 +219,258 @@ CAELIX_API CaelixResult caelix_light_bvh_get_stats(CaelixLightBvh* bvh, CaelixLi
 CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* keys, uint32_t* values,
                                                 uint32_t count, uint32_t identity_values, uint64_t stream);
 
+/* ---------------------------------------------------------------------------
+ * Scene: voxel bricks on the device
+ *
+ * Bricks are 8x8x8 blocks of 16-bit values, block-ID encoding (opaque = bit 15 set; a value
+ * without bit 15 is transparent, id = value & 0x1FF, id 0 = air), voxel index x + 8y + 64z, as in
+ * the reference (include/caelix/caelix.h:240-290). A brick key is the brick coordinate; this
+ * version takes keys in [0, 1024) per axis (the world grid is the bounding box of the keys) and
+ * one entity with the identity transform. caelix_scene_flush builds, on the device: the brick
+ * records (the finalize rules of the reference), the brick hash table, the brick occupancy bitmap,
+ * the brick light records and the light tree.
+ * ------------------------------------------------------------------------- */
+
+typedef struct CaelixScene CaelixScene;
+
+typedef struct CaelixSceneDesc
+{
+    uint32_t group_shift; /* render group edge in bricks = 1 << group_shift; 0 = 4; 1..4 */
+    uint32_t encoding;    /* 1 = block-ID (the only encoding of this version; 0 is rejected) */
+    uint32_t reserved[2]; /* must be 0 */
+} CaelixSceneDesc;
+
+/* Replaces caelix_scene_create / caelix_scene_destroy (include/caelix/caelix.h:296-300). */
+CAELIX_API CaelixResult caelix_scene_create(CaelixDevice* device, const CaelixSceneDesc* desc,
+                                            CaelixScene** out_scene);
+CAELIX_API void caelix_scene_destroy(CaelixScene* scene);
+
+typedef struct CaelixBrickKey
+{
+    int32_t x, y, z;
+} CaelixBrickKey;
+
+/* Replaces caelix_scene_upload_bricks (include/caelix/caelix.h:340-352): count raw bricks of 512
+   uint16_t values each (host memory, borrowed for the call); a brick with the same key is
+   replaced. entity must be 0. Every key is checked first: one out of range returns
+   CAELIX_ERROR_INVALID_ARGUMENT and accepts nothing. *consumed (may be NULL) = count. */
+CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                   const CaelixBrickKey* keys, const void* blocks,
+                                                   uint32_t* consumed);
+
+/* New (no reference counterpart): the emitter power of bricks (host arrays). An opaque voxel of a
+   brick with power P > 0 emits radiance (P, P, P) and is a light voxel of the light tree (the
+   reference derives light voxels from emissive material codes, include/caelix/caelix.h:600-630;
+   the benchmark scenes give each emissive brick its own power). Keys without an uploaded brick are
+   kept and apply when it arrives. */
+CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                     const CaelixBrickKey* keys, const float* power);
+
+/* Replaces CaelixMaterial (include/caelix/caelix.h:533-565): the same 112-byte entry. This version
+   shades opaque codes with a Lambertian lobe of `albedo`; the other fields are validated and
+   stored. */
+typedef struct CaelixMaterial
+{
+    float albedo[3];
+    float smoothness;
+    float emission[3];
+    float metallic;
+    float ior;
+    float extinction;
+    uint32_t sss_model;
+    float sss_probability;
+    float sss_albedo[3];
+    float sss_anisotropy;
+    uint32_t sss_steps;
+    float sss_params[8];
+    uint32_t texture_set;
+    uint32_t connect_group;
+    uint32_t reserved;
+} CaelixMaterial;
+
+/* Replaces caelix_scene_set_materials (include/caelix/caelix.h:567): entries [0, count) are the
+   material table entries of codes 0x8000 | i (the opaque block-ID codes of material id i,
+   i < 128); the rest keep albedo 0.5. Every float must be finite. */
+CAELIX_API CaelixResult caelix_scene_set_materials(CaelixScene* scene, const CaelixMaterial* entries,
+                                                   uint32_t count);
+
+/* Replaces CaelixLightOptions / caelix_scene_set_light_options (include/caelix/caelix.h:632-646). */
+typedef struct CaelixLightOptions
+{
+    uint32_t enabled;    /* 0 = no light tree, 1 = build it (the default of this version) */
+    float min_emission;  /* stored; light voxels come from the brick power */
+    uint64_t heap_bytes; /* stored; the heap is sized exactly at every flush */
+} CaelixLightOptions;
+CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const CaelixLightOptions* options);
+
+/* Replaces CaelixFrameDesc (include/caelix/caelix.h:358-364): command_buffer is a cudaStream_t. */
+typedef struct CaelixFrameDesc
+{
+    uint64_t command_buffer;
+    uint64_t frame_number;      /* strictly increasing across flushes, > safe_frame_number */
+    uint64_t safe_frame_number;
+} CaelixFrameDesc;
+
+/* Replaces caelix_scene_flush (include/caelix/caelix.h:379; lib/src/scene/scene_flush.cpp:567):
+   builds the device scene from everything uploaded so far when it changed (records, hash table,
+   bitmap, light records, light tree) on the frame's stream and waits for it (the build reads
+   back its sizes). The frame contract is checked as in the reference. */
+CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrameDesc* desc);
+
+/* Replaces CaelixLightStats (include/caelix/caelix.h:650-677, 104 bytes); tree index 1 (dynamic
+   entities) stays 0 in this version. */
+typedef struct CaelixLightStats
+{
+    uint32_t enabled;
+    uint32_t light_groups;
+    uint64_t light_bricks;
+    uint64_t light_faces;
+    uint64_t bricks_dropped;
+    uint64_t heap_bytes_used;
+    uint64_t heap_bytes_capacity;
+    uint32_t passes;
+    uint32_t failed_passes;
+    uint32_t records_recomputed;
+    uint32_t records_copied;
+    float gpu_ms;
+    uint32_t pad;
+    uint32_t tree_leaves[2];
+    uint32_t tree_nodes[2];
+    uint32_t tree_builds[2];
+    uint32_t tree_leaves_dropped[2];
+} CaelixLightStats;
+/* Replaces caelix_scene_get_light_stats (include/caelix/caelix.h:681). NULL arguments are ignored. */
+CAELIX_API void caelix_scene_get_light_stats(const CaelixScene* scene, CaelixLightStats* out);
+
+/* Device pointers and sizes of the built scene, for tests and hosts (replaces the descriptor of
+   caelix_scene_get_light_tree, include/caelix/caelix.h:688, and the scene tables the reference's
+   tests read back). Valid until the next flush that rebuilds or the scene's destruction. */
+typedef struct CaelixSceneView
+{
+    uint32_t grid[3];
+    uint32_t group_shift;
+    uint32_t groups[3];
+    uint32_t brick_count;
+    uint32_t hash_capacity;
+    uint32_t hash_slot_count;
+    uint32_t hash_max_probe;
+    uint32_t light_count;
+    uint32_t heap_words;
+    uint32_t group_count;
+    uint64_t keys;          /* int32 [brick_count][3], increasing linear brick index */
+    uint64_t records;       /* u32 [brick_count][274] */
+    uint64_t hash_slots;    /* u32 [hash_slot_count][4]: key_lo, key_hi, record, 0 */
+    uint64_t bitmap;        /* u32 brick occupancy by linear brick index */
+    uint64_t heap;          /* u32 group light blocks */
+    uint64_t group_rows;    /* u32 [group_count][8] */
+    uint64_t light_headers; /* CaelixBrickLightRecord [light_count], leaf order */
+    uint64_t light_group;   /* u32 [light_count] */
+    uint64_t light_entry;   /* u32 [light_count] */
+    uint64_t light_brick;   /* u32 [light_count] */
+    uint64_t tree_header;   /* LightTreeHeader + LightTreeState */
+    uint64_t tree_nodes;
+    uint64_t tree_leaves;
+} CaelixSceneView;
+CAELIX_API CaelixResult caelix_scene_get_view(const CaelixScene* scene, CaelixSceneView* out);
+
+/* Replaces caelix_scene_get_light_tree (include/caelix/caelix.h:688): the device address of the
+   light tree header (LightTreeHeader, then LightTreeState); 0 without a tree. */
+CAELIX_API uint64_t caelix_scene_get_light_tree(const CaelixScene* scene);
+
+/* ---------------------------------------------------------------------------
+ * Renderer: path-traces a scene into a headless device radiance buffer
+ * ------------------------------------------------------------------------- */
+
+typedef struct CaelixRenderer CaelixRenderer;
+
+/* Replaces caelix_renderer_create / destroy (include/caelix/caelix.h:800-805). */
+CAELIX_API CaelixResult caelix_renderer_create(CaelixDevice* device, CaelixScene* scene,
+                                               CaelixRenderer** out_renderer);
+CAELIX_API void caelix_renderer_destroy(CaelixRenderer* renderer);
+
+/* Replaces CaelixCamera (include/caelix/caelix.h:814-844), the same layout and pinhole mapping
+   (common/caelix_frame.hlsl:164-171); jitter must be 0 in this version, projection is unused. */
+typedef struct CaelixCamera
+{
+    float position[3];
+    float pad0;
+    float right[3];
+    float pad1;
+    float up[3];
+    float pad2;
+    float forward[3];
+    float pad3;
+    float tan_half_fov_y;
+    float aspect;
+    float near_z, far_z;
+    float projection[16];
+    float jitter[2];
+} CaelixCamera;
+
+/* Replaces CaelixRenderTargets (include/caelix/caelix.h:1130-1200): one headless target, the fp32
+   RGB radiance of every pixel (row 0 = the top row), deterministic + albedo * stochastic as the
+   reference's composite forms it (shaders/render/caelix_composite.hlsl:7). */
+typedef struct CaelixRenderTargets
+{
+    uint64_t radiance; /* device float[height][width][3] */
+    uint32_t width;
+    uint32_t height;
+} CaelixRenderTargets;
+
+/* Replaces CaelixRenderOptions (include/caelix/caelix.h:1043-1126): the fields of the path-traced
+   mode that this version implements, under the reference's names. */
+typedef struct CaelixRenderOptions
+{
+    uint32_t mode;         /* 1 = CAELIX_MODE_PATH_TRACE (the only mode of this version) */
+    uint32_t bounce_count; /* stochastic bounces after the primary hit, 0 .. 14 */
+    uint32_t frame_seed;   /* per-pixel random streams depend on the pixel and this value only */
+    uint32_t spp;          /* new: samples per pixel (frame seeds frame_seed .. + spp - 1, averaged); 0 = 1 */
+    uint32_t reserved[4];  /* must be 0 */
+} CaelixRenderOptions;
+
+/* Replaces caelix_renderer_render (include/caelix/caelix.h:1257): records the trace of one frame
+   into the frame's stream (asynchronous). */
+CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const CaelixFrameDesc* frame,
+                                               const CaelixRenderTargets* targets, const CaelixCamera* camera,
+                                               const CaelixRenderOptions* options);
+
+/* Replaces CaelixLightNeeOptions / caelix_renderer_set_light_nee_options
+   (include/caelix/caelix.h:1283-1297). flags must be 0 (MIS on, no visibility hint). */
+typedef struct CaelixLightNeeOptions
+{
+    uint32_t enabled;
+    uint32_t flags;
+    uint32_t hint_patch;
+    uint32_t reserved;
+} CaelixLightNeeOptions;
+CAELIX_API CaelixResult caelix_renderer_set_light_nee_options(CaelixRenderer* renderer,
+                                                              const CaelixLightNeeOptions* options);
+
+/* Replaces CaelixGpuTimings / caelix_renderer_get_gpu_timings (include/caelix/caelix.h:1324-1339):
+   events around the newest render and flush, read after waiting for them. */
+typedef struct CaelixGpuTimings
+{
+    float trace_ms;
+    float flush_ms;
+    uint64_t frame_number;
+    float composite_ms;
+    float denoise_ms;
+    float upscale_ms;
+    float pad;
+} CaelixGpuTimings;
+CAELIX_API void caelix_renderer_get_gpu_timings(const CaelixRenderer* renderer, CaelixGpuTimings* out);
+
+/* New: rays traced by the newest render call, by kind (read after waiting for it). */
+typedef struct CaelixRenderStats
+{
+    uint64_t primary_rays;
+    uint64_t bounce_rays;
+    uint64_t shadow_rays;
+    uint32_t kernel_launches;
+    uint32_t pad;
+} CaelixRenderStats;
+CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, CaelixRenderStats* out);
+
 #ifdef __cplusplus
 }
 #endif

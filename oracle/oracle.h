@@ -114,6 +114,108 @@ int oc_lt_build(const oc_record* records, uint32_t n, const uint32_t* rec_group,
 float oc_importance(const float x[3], const float n[3], const float lo[3], const float hi[3],
                     const float face[6]);
 
+/* ---- scene (oracle/scene.c) ---- */
+
+#define OC_RECORD_WORDS 274
+
+/* A voxel world of bricks: keys[i] = brick coordinate (x, y, z) of brick i (every coordinate in
+ * [0, grid)), voxels[512 i + x + 8 y + 64 z] = raw block value (block-ID encoding: opaque =
+ * 0x8000 | material, 0 = air), power[i] = the brick's emitter power (0: not emissive). */
+typedef struct oc_scene_desc {
+    uint32_t grid[3];
+    uint32_t group_shift;
+    uint32_t brick_count;
+    uint32_t pad;
+    const int32_t* keys;
+    const uint16_t* voxels;
+    const float* power;
+} oc_scene_desc;
+
+typedef struct oc_scene {
+    uint32_t grid[3];
+    uint32_t group_shift;
+    uint32_t brick_count;
+    uint32_t hash_capacity;   /* home slots (load factor 0.5) */
+    uint32_t hash_slot_count; /* slots including the tail */
+    uint32_t hash_max_probe;
+    uint32_t bitmap_words;
+    uint32_t light_count;
+    uint32_t heap_words;
+    uint32_t group_count;
+    uint32_t groups[3];
+    uint32_t pad;
+    uint32_t* records;     /* [brick_count][274] */
+    uint32_t* hash_slots;  /* [hash_slot_count][4]: key_lo, key_hi, record, 0 */
+    uint32_t* bitmap;      /* brick occupancy by linear brick index */
+    oc_record* light_headers; /* [light_count] in leaf (gather) order */
+    uint32_t* light_group;
+    uint32_t* light_entry;
+    uint32_t* light_brick; /* scene record of every light brick */
+    uint32_t* heap;        /* group light blocks (16-byte units) */
+    uint32_t* group_rows;  /* [group_count][8] GroupLightRow */
+    oc_frame* group_frames;
+} oc_scene;
+
+int oc_scene_build(const oc_scene_desc* d, oc_scene* s);
+void oc_scene_free(oc_scene* s);
+void oc_hash_fingerprint(int32_t x, int32_t y, int32_t z, uint32_t* key_lo, uint32_t* key_hi);
+uint32_t oc_hash_home(uint32_t key_lo, uint32_t capacity);
+uint32_t oc_hash_lookup(const oc_scene* s, int32_t x, int32_t y, int32_t z);
+
+/* ---- trace (oracle/trace.c) ---- */
+
+typedef struct oc_camera {
+    float position[3];
+    float right[3];
+    float up[3];
+    float forward[3];
+    float tan_half_fov_y;
+    float aspect;
+} oc_camera;
+
+typedef struct oc_render_desc {
+    uint32_t width;
+    uint32_t height;
+    uint32_t spp;
+    uint32_t bounce_count;
+    uint32_t frame_seed;
+    uint32_t light_nee; /* 1: light-tree NEE with MIS */
+    uint32_t x0, y0, x1, y1; /* pixel window rendered (the rest is left untouched) */
+} oc_render_desc;
+
+/* A built light tree (the build's output) for the trace. */
+typedef struct oc_light_tree {
+    const oc_leaf* leaves;
+    const oc_node* nodes;
+    const oc_header* header;
+} oc_light_tree;
+
+typedef struct oc_hit {
+    uint32_t hit;
+    float t;
+    uint32_t attrib;
+    uint32_t record;
+    uint32_t group;
+    float normal[3];
+    float object_hit[3];
+} oc_hit;
+
+/* Closest hit of a ray (unit direction) over the bricks, t in [tmin, tmax). */
+oc_hit oc_trace_ray(const oc_scene* s, const float origin[3], const float dir[3], float tmin, float tmax);
+
+/* Renders the pixel window; radiance[3 * (y * width + x)] (fp32 RGB, averaged over spp);
+ * rays[3]: primary, bounce, shadow rays traced. Threads > 1 splits rows across threads. */
+void oc_render(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
+               const oc_camera* cam, const oc_render_desc* r, float* radiance, uint64_t* rays, int threads);
+
+/* Light tree draw for a point receiver (caelix_light_tree.hlsl:749-767): returns 1 and fills
+ * out[0..2] position, out[3..5] normal, out[6] pdf, words[0..4] block, voxel, face, group, entry. */
+int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t rng,
+                    float out[7], uint32_t words[5]);
+/* The light tree pdf of a light face point (caelix_light_tree.hlsl:936-949). */
+float oc_light_point_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
+                         uint32_t group, const uint32_t voxel_in_group[3], uint32_t face, uint32_t block);
+
 #ifdef __cplusplus
 }
 #endif

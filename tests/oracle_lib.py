@@ -77,3 +77,142 @@ def lt_build(lib, records, record_group=None, record_entry=None, group_frames=No
     out["status"] = status
     out["n"] = n
     return out
+
+
+# ---------------------------------------------------------------------------------------------
+# Scene and trace
+
+
+class SceneDesc(C.Structure):
+    _fields_ = [("grid", C.c_uint32 * 3), ("group_shift", C.c_uint32), ("brick_count", C.c_uint32),
+                ("pad", C.c_uint32), ("keys", C.c_void_p), ("voxels", C.c_void_p), ("power", C.c_void_p)]
+
+
+class Scene(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "grid0", "grid1", "grid2", "group_shift", "brick_count", "hash_capacity", "hash_slot_count",
+        "hash_max_probe", "bitmap_words", "light_count", "heap_words", "group_count", "groups0", "groups1",
+        "groups2", "pad")] + [(n, C.c_void_p) for n in (
+        "records", "hash_slots", "bitmap", "light_headers", "light_group", "light_entry", "light_brick",
+        "heap", "group_rows", "group_frames")]
+
+
+class Camera(C.Structure):
+    _fields_ = [("position", C.c_float * 3), ("right", C.c_float * 3), ("up", C.c_float * 3),
+                ("forward", C.c_float * 3), ("tan_half_fov_y", C.c_float), ("aspect", C.c_float)]
+
+
+class RenderDesc(C.Structure):
+    _fields_ = [(n, C.c_uint32) for n in (
+        "width", "height", "spp", "bounce_count", "frame_seed", "light_nee", "x0", "y0", "x1", "y1")]
+
+
+class LightTree(C.Structure):
+    _fields_ = [("leaves", C.c_void_p), ("nodes", C.c_void_p), ("header", C.c_void_p)]
+
+
+class Hit(C.Structure):
+    _fields_ = [("hit", C.c_uint32), ("t", C.c_float), ("attrib", C.c_uint32), ("record", C.c_uint32),
+                ("group", C.c_uint32), ("normal", C.c_float * 3), ("object_hit", C.c_float * 3)]
+
+
+def _bind_scene(lib):
+    if getattr(lib, "_scene_bound", False):
+        return
+    lib.oc_scene_build.argtypes = [C.POINTER(SceneDesc), C.POINTER(Scene)]
+    lib.oc_scene_build.restype = C.c_int
+    lib.oc_scene_free.argtypes = [C.POINTER(Scene)]
+    lib.oc_scene_free.restype = None
+    lib.oc_hash_lookup.argtypes = [C.POINTER(Scene), C.c_int32, C.c_int32, C.c_int32]
+    lib.oc_hash_lookup.restype = C.c_uint32
+    lib.oc_trace_ray.argtypes = [C.POINTER(Scene), C.c_void_p, C.c_void_p, C.c_float, C.c_float]
+    lib.oc_trace_ray.restype = Hit
+    lib.oc_render.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                              C.POINTER(RenderDesc), C.c_void_p, C.c_void_p, C.c_int]
+    lib.oc_render.restype = None
+    lib.oc_light_sample.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
+                                    C.c_void_p, C.c_void_p]
+    lib.oc_light_sample.restype = C.c_int
+    lib.oc_light_point_pdf.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
+                                       C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.oc_light_point_pdf.restype = C.c_float
+    lib.oc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+    lib.oc_sincos.restype = None
+    lib._scene_bound = True
+
+
+class OracleScene:
+    """The oracle's scene (records, hash table, light blocks) and light tree for a VoxelScene."""
+
+    def __init__(self, lib, scene):
+        _bind_scene(lib)
+        self.lib = lib
+        self.src = scene
+        self.desc = SceneDesc((C.c_uint32 * 3)(*scene.grid), scene.group_shift, scene.brick_count, 0,
+                              scene.keys.ctypes.data, scene.voxels.ctypes.data, scene.power.ctypes.data)
+        self.s = Scene()
+        lib.oc_scene_build(C.byref(self.desc), C.byref(self.s))
+        s = self.s
+        n = scene.brick_count
+        self.records = np.ctypeslib.as_array(C.cast(s.records, C.POINTER(C.c_uint32)), (max(n, 1) * 274,))[: n * 274].reshape(n, 274).copy()
+        self.hash_slots = np.ctypeslib.as_array(C.cast(s.hash_slots, C.POINTER(C.c_uint32)), (s.hash_slot_count * 4,)).reshape(-1, 4).copy()
+        m = s.light_count
+        self.light_count = m
+        if m:
+            hdr = np.ctypeslib.as_array(C.cast(s.light_headers, C.POINTER(C.c_uint8)), (m * 48,))
+            from caelix_b200 import workloads
+
+            self.light_headers = hdr.view(workloads.RECORD_DTYPE).copy()
+            self.light_group = np.ctypeslib.as_array(C.cast(s.light_group, C.POINTER(C.c_uint32)), (m,)).copy()
+            self.light_entry = np.ctypeslib.as_array(C.cast(s.light_entry, C.POINTER(C.c_uint32)), (m,)).copy()
+            self.light_brick = np.ctypeslib.as_array(C.cast(s.light_brick, C.POINTER(C.c_uint32)), (m,)).copy()
+        self.heap = np.ctypeslib.as_array(C.cast(s.heap, C.POINTER(C.c_uint32)), (max(s.heap_words, 1),))[: s.heap_words].copy()
+        self.group_rows = np.ctypeslib.as_array(C.cast(s.group_rows, C.POINTER(C.c_uint32)), (s.group_count * 8,)).reshape(-1, 8).copy()
+        from caelix_b200 import workloads
+
+        fr = np.ctypeslib.as_array(C.cast(s.group_frames, C.POINTER(C.c_uint8)), (s.group_count * 60,))
+        self.group_frames = fr.view(workloads.FRAME_DTYPE).copy()
+        # The light tree over the light records (leaf = gather order).
+        if m:
+            self.tree = lt_build(lib, self.light_headers, record_group=self.light_group, record_entry=self.light_entry,
+                                 group_frames=self.group_frames)
+        else:
+            self.tree = lt_build(lib, np.zeros(0, RECORD_DTYPE_LOCAL()), leaf_capacity=1)
+        self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
+                            self.tree["header"].ctypes.data)
+
+    def close(self):
+        if self.s.records:
+            self.lib.oc_scene_free(C.byref(self.s))
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def lookup(self, x, y, z):
+        return self.lib.oc_hash_lookup(C.byref(self.s), x, y, z)
+
+    def trace(self, origin, direction, tmin=0.0, tmax=1e30):
+        o = np.asarray(origin, np.float32)
+        d = np.asarray(direction, np.float32)
+        return self.lib.oc_trace_ray(C.byref(self.s), o.ctypes.data, d.ctypes.data, tmin, tmax)
+
+    def render(self, width, height, spp=1, bounces=4, seed=1, light_nee=True, window=None, threads=1):
+        cam = self.src.camera
+        c = Camera((C.c_float * 3)(*cam["position"]), (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]),
+                   (C.c_float * 3)(*cam["forward"]), float(cam["tan_half_fov_y"]), float(cam["aspect"]))
+        x0, y0, x1, y1 = window or (0, 0, width, height)
+        r = RenderDesc(width, height, spp, bounces, seed, 1 if light_nee else 0, x0, y0, x1, y1)
+        out = np.zeros((height, width, 3), np.float32)
+        rays = np.zeros(3, np.uint64)
+        self.lib.oc_render(C.byref(self.s), C.byref(self.lt), self.src.albedo.ctypes.data, self.src.power.ctypes.data,
+                           C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data, threads)
+        return out, rays
+
+
+def RECORD_DTYPE_LOCAL():
+    from caelix_b200 import workloads
+
+    return workloads.RECORD_DTYPE
