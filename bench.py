@@ -1,19 +1,27 @@
 #!/usr/bin/env python3
 """Benchmark of the scene-flush / trace hot path on B200 (one JSON line on stdout, rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload NAME]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload trace|build]
 
 Workloads (seeded synthetic inputs with the shapes of the benchmark configurations; no dataset):
-  build   the light-tree build over N_LEAVES brick light records (brick coords uniform in a
-          1024^3-brick grid, render groups of 16^3 bricks with identity frames, power
-          log-normal(0, 1) split over the faces): gather emit, centre bounds, Morton codes, onesweep
-          radix sort, Karras, aggregation, depth + scan, 4-wide collapse. value = Mleaves/s.
-          The 4,096-record plain build is timed beside it (config1_ms).
+  trace   (default, the headline) the plain brick-DDA trace: a 128^3-voxel world of 16^3 bricks,
+          30 % of the bricks occupied by thresholded value noise, voxel materials uniform in
+          [1, 64], 1 % of the occupied bricks emissive (power log-normal(0, 1)), brick keys in the
+          device hash table at load factor 0.5; 512 x 512 pinhole camera, 1 spp, 4 bounces,
+          light-tree NEE with MIS; fp32 radiance. A step is one render call; value = Mrays/s with
+          the rays counted on the device (primary + bounce + shadow).
+  build   the light-tree build over 4,194,304 brick light records (brick coords uniform in a
+          1024^3-brick grid, 16^3-brick render groups, power log-normal(0, 1) split over the faces);
+          value = Mleaves/s.
+Both lines carry the other measurement: the trace line has a `build` object (the 4M-record build
+with its roofline and stage times, and the 4,096-record plain build in ms).
 
-A step is one pass of the hot path over one batch of inputs already resident in HBM (`value`);
-`e2e` times the same step through the C ABI with the inputs copied from pinned host memory and the
-tree header read back, every step. Multi-GPU: replicas (the build does not shard); every rank runs
-the same workload, value = the work of all ranks / the max time over ranks.
+`value` times the step with its inputs resident in HBM (CUDA events on the launching stream, L2
+flushed by a 256 MiB write between timed steps). `e2e` times the same step through the C ABI with
+host buffers (trace: the radiance read back into pinned memory every step; build: the records
+copied in from pinned memory and the tree header read back). Multi-GPU: replicas (neither the
+build nor a 512^2 frame is sharded); every rank runs the same workload, value = the work of all
+ranks / the max time over ranks.
 """
 from __future__ import annotations
 
@@ -30,10 +38,13 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(REPO, "caelix-renderer_b200"))
 
 N_LEAVES = 1 << 22
+TRACE_W = TRACE_H = 512
+TRACE_BOUNCES = 4
 L2_FLUSH_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 BUILD_BYTES_PER_LEAF = 492  # emit 112 + Morton 32 + sort 68 + Karras 20 + aggregate 100 + wide 160
 SORT_PASS_BYTES_PER_PAIR = 60.0 / 4  # pass 0 reads keys only (12 B), passes 1-3 read and write pairs (16 B)
+TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record sector per ray
 
 
 def measured_peaks():
@@ -135,14 +146,68 @@ def barrier(world: int):
     torch.cuda.synchronize()
 
 
+def base_line(args, world, metric, value, unit, ms_per_step, config, higher=True):
+    return {
+        "metric": metric,
+        "value": value,
+        "unit": unit,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": ms_per_step,
+        "higher_is_better": higher,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": config,
+    }
+
+
+TRACE_METRIC = "trace throughput, Mrays/s (primary + bounce + shadow rays counted on the device)"
+TRACE_CONFIG = {
+    "workload": "plain brick-DDA trace: 128^3-voxel world (16^3 bricks, 30% occupied, value noise seed 2), "
+                "512x512 pinhole, 1 spp, 4 bounces, light-tree NEE with MIS, fp32 radiance",
+    "bricks": 1229,
+    "emissive_bricks": 12,
+    "width": TRACE_W,
+    "height": TRACE_H,
+    "spp": 1,
+    "bounces": TRACE_BOUNCES,
+    "l2": "flushed between timed steps (256 MiB write)",
+}
+
 # ---------------------------------------------------------------------------------------------
-# CPU baseline / reference arm: the oracle (the reference's build restated in C; the reference's
-# GPU code is HLSL for Vulkan and cannot run here)
+# CPU baseline / reference arm: the oracle (the reference's shader logic restated in C; the
+# reference's own GPU code is HLSL for Vulkan and has no CPU build)
+
+
+_ORACLE_SCENE = None
+
+
+def oracle_trace(seconds: float, threads: int, first_seed: int = 1):
+    """Renders whole frames of the trace workload with the oracle (seeds first_seed, +1, ...) on
+    `threads` threads for about `seconds`; returns (rays, seconds, frames)."""
+    global _ORACLE_SCENE
+    sys.path.insert(0, os.path.join(REPO, "tests"))
+    import oracle_lib
+    from caelix_b200 import workloads
+
+    if _ORACLE_SCENE is None:
+        _ORACLE_SCENE = oracle_lib.OracleScene(oracle_lib.load(), workloads.noise_world())
+    rays = 0
+    frames = 0
+    t0 = time.perf_counter()
+    while frames == 0 or time.perf_counter() - t0 < seconds:
+        _, r = _ORACLE_SCENE.render(TRACE_W, TRACE_H, spp=1, bounces=TRACE_BOUNCES, seed=first_seed + frames,
+                                    threads=threads)
+        rays += int(r.sum())
+        frames += 1
+    return rays, time.perf_counter() - t0, frames
 
 
 def oracle_build_throughput(n: int, seconds: float, threads: int):
-    """Runs independent oracle builds of an n-record sample on `threads` host threads for about
-    `seconds`; returns (Mleaves/s, builds, wall seconds)."""
+    """Independent oracle builds of an n-record sample on `threads` host threads for about `seconds`."""
     sys.path.insert(0, os.path.join(REPO, "tests"))
     import oracle_lib
     from caelix_b200 import workloads
@@ -164,41 +229,39 @@ def oracle_build_throughput(n: int, seconds: float, threads: int):
     for t in ts:
         t.join()
     wall = time.perf_counter() - t0
-    builds = sum(counts)
-    return builds * n / wall / 1e6, builds, wall
+    return sum(counts) * n / wall / 1e6, sum(counts), wall
 
 
 def run_reference(args, world, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    n = 1 << 18
-    values = []
-    for _ in range(args.warmup):
-        oracle_build_throughput(n, 0.5, threads)
-    for _ in range(args.steps):
-        v, builds, wall = oracle_build_throughput(n, 4.0, threads)
-        values.append(v)
-    value = statistics.mean(values)
-    line = {
-        "impl": "reference",
-        "metric": "light-tree build throughput (Mleaves/s)",
-        "value": value,
-        "unit": "Mleaves/s",
-        "n_gpus": args.gpus,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic",
-        "config": {"workload": f"light-tree build, {N_LEAVES} brick light records (sampled at {n} per build)",
-                   "records": N_LEAVES},
-        "cpu_baseline": {"value": value, "unit": "Mleaves/s", "cores": threads, "kind": "port",
-                         "sample": f"independent oracle builds of {n} records on {threads} threads, ~4 s per step"},
-        "e2e": {"value": value, "unit": "Mleaves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-    }
+    if args.workload == "build":
+        n = 1 << 18
+        for _ in range(args.warmup):
+            oracle_build_throughput(n, 0.5, threads)
+        values = [oracle_build_throughput(n, 4.0, threads)[0] for _ in range(args.steps)]
+        value = statistics.mean(values)
+        line = base_line(args, args.gpus, "light-tree build throughput (Mleaves/s)", value, "Mleaves/s", None,
+                         {"workload": f"light-tree build, {N_LEAVES} brick light records (sampled at {n} per build)"})
+        sample = f"independent oracle builds of {n} records on {threads} threads, ~4 s per step"
+    else:
+        for _ in range(min(args.warmup, 1)):
+            oracle_trace(0.0, threads, 5000)
+        rays = 0
+        secs = 0.0
+        frames = 0
+        for k in range(args.steps):
+            r, s, f = oracle_trace(2.0, threads, 1 + 100 * k)
+            rays += r
+            secs += s
+            frames += f
+        value = rays / secs / 1e6
+        line = base_line(args, args.gpus, TRACE_METRIC, value, "Mrays/s", 1e3 * secs / frames, TRACE_CONFIG)
+        sample = f"{frames} oracle renders of the whole 512x512 frame on {threads} threads (~2 s per step)"
+    line["impl"] = "reference"
+    line["cpu_baseline"] = {"value": value, "unit": line["unit"], "cores": threads, "kind": "port", "sample": sample}
+    line["e2e"] = {"value": value, "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
 
 
@@ -206,57 +269,42 @@ def run_reference(args, world, rank):
 # Our arm
 
 
-def run_build(args, world, rank, local):
+def measure_build(args, world, local, dev, stream, flush, records):
     import numpy as np
     import torch
 
     import caelix_b200
     from caelix_b200 import workloads
 
-    torch.cuda.set_device(local)
-    dev = caelix_b200.Device(local)
-    stream = torch.cuda.Stream()
     sptr = stream.cuda_stream
-
-    rec, group, frames = workloads.brick_light_records(args.records, grid_bricks=1024, group_shift=4)
+    rec, group, frames = workloads.brick_light_records(records, grid_bricks=1024, group_shift=4)
     n = len(rec)
     d_rec = torch.from_numpy(rec.view(np.uint8)).cuda()
     d_group = torch.from_numpy(group.view(np.int32)).cuda()
     d_frames = torch.from_numpy(frames.view(np.uint8)).cuda()
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     bvh = caelix_b200.LightBvh(dev, n)
 
     def build():
         bvh.build(d_rec, n, record_group=d_group, group_frames=d_frames, group_count=len(frames), stream=sptr)
 
-    # Warm-up.
     with torch.cuda.stream(stream):
         for _ in range(args.warmup):
             build()
     stream.synchronize()
     bvh.stats()
-
-    # Timed region: K builds, L2 flushed between them (outside the events), events on the stream.
     starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     stops = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
     barrier(world)
-    with ClockSampler(local) as clocks:
-        with torch.cuda.stream(stream):
-            for k in range(args.steps):
-                flush.zero_()
-                starts[k].record(stream)
-                build()
-                stops[k].record(stream)
-        stream.synchronize()
+    with torch.cuda.stream(stream):
+        for k in range(args.steps):
+            flush.zero_()
+            starts[k].record(stream)
+            build()
+            stops[k].record(stream)
+    stream.synchronize()
     barrier(world)
-    step_ms = [a.elapsed_time(b) for a, b in zip(starts, stops)]
-    total_ms = max_over_ranks(sum(step_ms), world)
-    ms_per_step = total_ms / args.steps
-    value = world * n / (ms_per_step / 1e3) / 1e6
-    stats = bvh.stats()
-    launches = stats.kernel_launches * args.steps
-
-    # Per-stage timing of one build (profiling events) for the roofline of the dominant kernel.
+    ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in zip(starts, stops)), world) / args.steps
+    launches = bvh.stats().kernel_launches * args.steps
     bvh.set_profiling(True)
     stage_ms = np.zeros(7)
     reps = 5
@@ -267,12 +315,11 @@ def run_build(args, world, rank, local):
             stage_ms += np.array(bvh.stats().stage_ms[:])
     stage_ms /= reps
     bvh.set_profiling(False)
-    sort_pass_ms = stage_ms[2] / 4
     peak, peak_kind = measured_peaks()
-    sort_achieved = SORT_PASS_BYTES_PER_PAIR * n / (sort_pass_ms / 1e3) / 1e9
-    build_achieved = BUILD_BYTES_PER_LEAF * n / (ms_per_step / 1e3) / 1e9
+    sort_achieved = SORT_PASS_BYTES_PER_PAIR * n / (stage_ms[2] / 4 / 1e3) / 1e9
+    build_achieved = BUILD_BYTES_PER_LEAF * n / (ms / 1e3) / 1e9
 
-    # The plain 4,096-record build (config 1), L2 flushed between builds.
+    # The 4,096-record plain build, L2 flushed between builds.
     rec1, _, _ = workloads.brick_light_records(4096)
     d_rec1 = torch.from_numpy(rec1.view(np.uint8)).cuda()
     bvh1 = caelix_b200.LightBvh(dev, 4096)
@@ -290,22 +337,18 @@ def run_build(args, world, rank, local):
     stream.synchronize()
     config1_ms = max_over_ranks(statistics.mean(a.elapsed_time(b) for a, b in c1), world)
 
-    # End to end through the C ABI: pinned host records -> device, build, tree header and state read
-    # back by caelix_light_bvh_get_stats (which waits for the build), every step; host clock per step.
+    # End to end through the C ABI: records from pinned memory, build, header and state read back.
     h_rec = torch.from_numpy(rec.view(np.uint8)).pin_memory()
     h_group = torch.from_numpy(group.view(np.int32)).pin_memory()
     h_frames = torch.from_numpy(frames.view(np.uint8)).pin_memory()
-    e2e_dev_rec = torch.empty_like(d_rec)
-    e2e_dev_group = torch.empty_like(d_group)
-    e2e_dev_frames = torch.empty_like(d_frames)
+    e_rec, e_group, e_frames = torch.empty_like(d_rec), torch.empty_like(d_group), torch.empty_like(d_frames)
 
     def e2e_step():
         with torch.cuda.stream(stream):
-            e2e_dev_rec.copy_(h_rec, non_blocking=True)
-            e2e_dev_group.copy_(h_group, non_blocking=True)
-            e2e_dev_frames.copy_(h_frames, non_blocking=True)
-            bvh.build(e2e_dev_rec, n, record_group=e2e_dev_group, group_frames=e2e_dev_frames,
-                      group_count=len(frames), stream=sptr)
+            e_rec.copy_(h_rec, non_blocking=True)
+            e_group.copy_(h_group, non_blocking=True)
+            e_frames.copy_(h_frames, non_blocking=True)
+            bvh.build(e_rec, n, record_group=e_group, group_frames=e_frames, group_count=len(frames), stream=sptr)
         return bvh.stats()
 
     for _ in range(args.warmup):
@@ -319,65 +362,143 @@ def run_build(args, world, rank, local):
         e2e_step()
         e2e_s += time.perf_counter() - t0
     e2e_ms = max_over_ranks(e2e_s * 1e3, world) / args.steps
-    e2e_value = world * n / (e2e_ms / 1e3) / 1e6
-    h2d = rec.nbytes + group.nbytes + frames.nbytes
-
-    line = {
-        "metric": "light-tree build throughput (Mleaves/s)",
-        "value": value,
-        "unit": "Mleaves/s",
-        "n_gpus": world,
-        "steps": args.steps,
-        "warmup": args.warmup,
-        "ms_per_step": ms_per_step,
-        "higher_is_better": True,
-        "scaling": "weak",
-        "vs_baseline": None,
-        "dtype": "f32",
-        "data": "synthetic",
-        "config": {
-            "workload": f"light-tree build, {n} brick light records in a 1024^3-brick grid (16^3-brick groups)",
-            "records": n,
-            "l2": "flushed between timed steps (256 MiB write) and inputs larger than L2",
-            "parallelism": f"replicas x{world}",
-        },
-        "build_ms": ms_per_step,
+    bvh.close()
+    bvh1.close()
+    return {
+        "workload": f"light-tree build, {n} brick light records in a 1024^3-brick grid (16^3-brick groups)",
+        "records": n,
+        "build_ms": ms,
+        "mleaves_per_s": world * n / (ms / 1e3) / 1e6,
         "config1_ms": config1_ms,
         "stage_ms": {name: float(v) for name, v in zip(
             ["emit_bounds", "morton_hist", "sort_4_passes", "karras", "aggregate", "depth_scan", "wide_finish"],
             stage_ms)},
-        "roofline": {
-            "kernel": "onesweep_pass_kernel",
-            "bound": "hbm",
-            "achieved": sort_achieved,
-            "peak": peak,
-            "unit": "GB/s",
-            "frac": sort_achieved / peak,
-            "peak_kind": peak_kind,
-            "traffic": None,
-            "algorithmic_bytes_per_launch": SORT_PASS_BYTES_PER_PAIR * n,
-        },
-        "roofline_build": {
-            "bound": "hbm",
-            "achieved": build_achieved,
-            "peak": peak,
-            "unit": "GB/s",
-            "frac": build_achieved / peak,
-            "bytes_per_leaf": BUILD_BYTES_PER_LEAF,
-        },
-        "e2e": {"value": e2e_value, "unit": "Mleaves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": 128,
+        "roofline": {"kernel": "onesweep_pass_kernel", "bound": "hbm", "achieved": sort_achieved, "peak": peak,
+                     "unit": "GB/s", "frac": sort_achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "algorithmic_bytes_per_launch": SORT_PASS_BYTES_PER_PAIR * n},
+        "roofline_build": {"bound": "hbm", "achieved": build_achieved, "peak": peak, "unit": "GB/s",
+                           "frac": build_achieved / peak, "bytes_per_leaf": BUILD_BYTES_PER_LEAF},
+        "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mleaves/s",
+                "h2d_bytes_per_step": rec.nbytes + group.nbytes + frames.nbytes, "d2h_bytes_per_step": 128,
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
+    }
+
+
+def measure_trace(args, world, local, dev, stream, flush):
+    import torch
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    sptr = stream.cuda_stream
+    vs = workloads.noise_world()
+    scene = caelix_b200.Scene.from_voxel_scene(dev, vs)
+    renderer = caelix_b200.Renderer(dev, scene)
+    out = torch.zeros(TRACE_W * TRACE_H * 3, dtype=torch.float32, device="cuda")
+
+    def render(seed):
+        renderer.render(out, TRACE_W, TRACE_H, vs.camera, bounces=TRACE_BOUNCES, seed=seed, spp=1, stream=sptr)
+
+    with torch.cuda.stream(stream):
+        for k in range(args.warmup):
+            render(1000 + k)
+    stream.synchronize()
+    rays = 0
+    total_ms = 0.0
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        for k in range(args.steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                render(1 + k)
+                b.record(stream)
+            st = renderer.stats()  # waits for the step; outside its events
+            rays += st.primary_rays + st.bounce_rays + st.shadow_rays
+            total_ms += a.elapsed_time(b)
+    barrier(world)
+    ms = max_over_ranks(total_ms, world) / args.steps
+    rays_per_step = rays / args.steps
+    value = world * rays_per_step / (ms / 1e3) / 1e6
+
+    # End to end through the C ABI: render, radiance read back into pinned host memory, per step.
+    host = torch.empty(TRACE_W * TRACE_H * 3, dtype=torch.float32).pin_memory()
+    for k in range(args.warmup):
+        with torch.cuda.stream(stream):
+            render(2000 + k)
+            host.copy_(out, non_blocking=True)
+        stream.synchronize()
+    barrier(world)
+    e2e_s = 0.0
+    for k in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        with torch.cuda.stream(stream):
+            render(1 + k)
+            host.copy_(out, non_blocking=True)
+        stream.synchronize()
+        e2e_s += time.perf_counter() - t0
+    e2e_ms = max_over_ranks(e2e_s * 1e3, world) / args.steps
+    peak, peak_kind = measured_peaks()
+    achieved = TRACE_BYTES_PER_RAY * rays_per_step / (ms / 1e3) / 1e9
+    result = {
+        "value": value,
+        "ms_per_step": ms,
+        "rays_per_step": rays_per_step,
+        "roofline": {"kernel": "trace_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "bytes_per_ray": TRACE_BYTES_PER_RAY,
+                     "note": "latency-bound ray traversal; the bytes are a per-ray lower bound"},
+        "e2e": {"value": world * rays_per_step / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
+                "h2d_bytes_per_step": 208 + 32, "d2h_bytes_per_step": TRACE_W * TRACE_H * 12, "ms_per_step": e2e_ms},
+        "gpu_launches": args.steps,
         "clocks": clocks.summary(),
     }
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        v, builds, wall = oracle_build_throughput(1 << 20, 10.0, 1)
-        line["cpu_baseline"] = {"value": v, "unit": "Mleaves/s", "cores": 1, "kind": "port",
-                                "sample": f"{builds} oracle builds of 1048576 records, 1 thread, {wall:.1f} s"}
+    renderer.close()
+    scene.close()
+    return result
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import caelix_b200
+
+    torch.cuda.set_device(local)
+    dev = caelix_b200.Device(local)
+    stream = torch.cuda.Stream()
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    build = measure_build(args, world, local, dev, stream, flush, args.records)
+    if args.workload == "build":
+        line = base_line(args, world, "light-tree build throughput (Mleaves/s)", build["mleaves_per_s"], "Mleaves/s",
+                         build["build_ms"], {"workload": build["workload"], "records": build["records"],
+                                             "l2": "flushed between timed steps (256 MiB write)",
+                                             "parallelism": f"replicas x{world}"})
+        line.update({k: build[k] for k in ("roofline", "roofline_build", "e2e", "gpu_launches", "stage_ms",
+                                           "config1_ms")})
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            v, builds, wall = oracle_build_throughput(1 << 20, 10.0, 1)
+            line["cpu_baseline"] = {"value": v, "unit": "Mleaves/s", "cores": 1, "kind": "port",
+                                    "sample": f"{builds} oracle builds of 1048576 records, 1 thread, {wall:.1f} s"}
+    else:
+        trace = measure_trace(args, world, local, dev, stream, flush)
+        config = dict(TRACE_CONFIG)
+        config["parallelism"] = f"replicas x{world}"
+        line = base_line(args, world, TRACE_METRIC, trace["value"], "Mrays/s", trace["ms_per_step"], config)
+        line.update({k: trace[k] for k in ("roofline", "e2e", "gpu_launches", "clocks", "rays_per_step")})
+        line["build"] = {k: build[k] for k in ("workload", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
+                                               "roofline", "roofline_build", "e2e")}
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            rays, secs, frames = oracle_trace(10.0, 1)
+            line["cpu_baseline"] = {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": 1, "kind": "port",
+                                    "sample": f"{frames} oracle renders of the whole 512x512 frame, 1 thread, "
+                                              f"{secs:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
-    bvh.close()
-    bvh1.close()
     dev.close()
 
 
@@ -387,7 +508,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["build"], default="build")
+    ap.add_argument("--workload", choices=["trace", "build"], default="trace")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
     args = ap.parse_args()
@@ -396,7 +517,7 @@ def main():
         if args.impl == "reference":
             run_reference(args, world, rank)
         else:
-            run_build(args, world, rank, local)
+            run_ours(args, world, rank, local)
     finally:
         if world > 1:
             import torch.distributed as dist
