@@ -219,6 +219,20 @@ CAELIX_API CaelixResult caelix_light_bvh_get_stats(CaelixLightBvh* bvh, CaelixLi
 CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* keys, uint32_t* values,
                                                 uint32_t count, uint32_t identity_values, uint64_t stream);
 
+/* No counterpart in the reference. The same sort for callers that cannot allocate device memory
+   while they record work (an engine render thread inside a frame capture, a host with a fixed
+   memory budget, code inside a CUDA graph capture): it allocates nothing. Its scratch is an array
+   compiled into the library, about 2.4 MB reserved on every GPU that loads it until the process
+   exits, so one call sorts at most 262144 pairs (more returns CAELIX_ERROR_INVALID_ARGUMENT).
+   Runs on the current CUDA device. The first call on a device looks up the array's device address
+   (cudaGetSymbolAddress); make that first call before any stream capture. Every call shares the
+   array and clears what must start at zero; calls whose work overlaps on the GPU (other streams,
+   other host threads) race on it and must be serialized by the caller. `status` (a device word,
+   may be NULL) receives device-side failures OR-ed in (a look-back that gave up). Asynchronous on
+   `stream`. */
+CAELIX_API CaelixResult caelix_radix_sort_pairs_static(uint32_t* keys, uint32_t* values, uint32_t count,
+                                                       uint32_t identity_values, uint32_t* status, uint64_t stream);
+
 /* ---------------------------------------------------------------------------
  * Scene: voxel bricks on the device
  *
