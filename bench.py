@@ -472,7 +472,7 @@ def run_ours(args, world, rank, local):
     dev = caelix_b200.Device(local)
     stream = torch.cuda.Stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
-    build = measure_build(args, world, local, dev, stream, flush, args.records)
+    build = None if args.no_build else measure_build(args, world, local, dev, stream, flush, args.records)
     if args.workload == "build":
         line = base_line(args, world, "light-tree build throughput (Mleaves/s)", build["mleaves_per_s"], "Mleaves/s",
                          build["build_ms"], {"workload": build["workload"], "records": build["records"],
@@ -490,8 +490,9 @@ def run_ours(args, world, rank, local):
         config["parallelism"] = f"replicas x{world}"
         line = base_line(args, world, TRACE_METRIC, trace["value"], "Mrays/s", trace["ms_per_step"], config)
         line.update({k: trace[k] for k in ("roofline", "e2e", "gpu_launches", "clocks", "rays_per_step")})
-        line["build"] = {k: build[k] for k in ("workload", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
-                                               "roofline", "roofline_build", "e2e")}
+        if build is not None:
+            line["build"] = {k: build[k] for k in ("workload", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
+                                                   "roofline", "roofline_build", "e2e")}
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             rays, secs, frames = oracle_trace(10.0, 1)
             line["cpu_baseline"] = {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": 1, "kind": "port",
@@ -511,6 +512,7 @@ def main():
     ap.add_argument("--workload", choices=["trace", "build"], default="trace")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
+    ap.add_argument("--no-build", action="store_true", help="trace workload only: skip the build section")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

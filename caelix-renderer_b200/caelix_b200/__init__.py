@@ -110,7 +110,8 @@ def _ptr(x) -> int:
 class Library:
     """The loaded libcaelix_b200.so with its prototypes and a log sink."""
 
-    def __init__(self, path: str = LIB_PATH):
+    def __init__(self, path: str | None = None):
+        path = path or os.environ.get("CAELIX_B200_LIB", LIB_PATH)
         if not os.path.exists(path):
             raise OSError(f"libcaelix_b200.so not built: {path} (run make -C caelix-renderer_b200)")
         self.path = path

@@ -223,7 +223,7 @@ struct Hit
 };
 
 // Closest hit over the bricks (front-to-back DDA over the brick grid).
-__device__ Hit trace_ray(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+__device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
 {
     Hit h;
     h.hit = false;
@@ -309,7 +309,7 @@ __device__ __forceinline__ void emitter_cosines(const float dlo[3], const float 
     }
 }
 
-__device__ float importance(const float x[3], const float n[3], const float lo[3], const float hi[3], const float face[6])
+__device__ __noinline__ float importance(const float x[3], const float n[3], const float lo[3], const float hi[3], const float face[6])
 {
     float dlo[3], dhi[3], c[6];
 #pragma unroll
@@ -468,7 +468,7 @@ __device__ float slot_probability(const LightBvhNode* nd, const float x[3], cons
     return pick_probability(sum_i, sum_p, imp_t, pow_t);
 }
 
-__device__ float leaf_probability(const SceneView& s, uint32_t leaf, const float x[3], const float n[3])
+__device__ __noinline__ float leaf_probability(const SceneView& s, uint32_t leaf, const float x[3], const float n[3])
 {
     if (__ldg(&s.header->root) == kNone) return 0.0f;
     const uint32_t parent = __ldg(&s.leaves[leaf].parent);
@@ -545,7 +545,7 @@ struct LightPoint
     uint32_t entry;
 };
 
-__device__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
+__device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
 {
     float pdf_brick = 1.0f;
     // The tree (two draws, one per tree).
@@ -654,7 +654,7 @@ __device__ bool light_sample(const SceneView& s, const float x[3], const float n
 }
 
 // LightTreeFindLightFace: a light voxel is an opaque voxel of a brick with a light record.
-__device__ bool find_light_face(const SceneView& s, const float x[3], uint32_t group, const uint32_t v[3], uint32_t face,
+__device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3], uint32_t group, const uint32_t v[3], uint32_t face,
                                 uint32_t block_value, uint32_t& entry_out, uint32_t& leaf_out, float& in_brick)
 {
     entry_out = kNone;
@@ -754,7 +754,7 @@ struct Counters
     uint32_t primary, bounce, shadow;
 };
 
-__device__ void next_event(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng, float out[3],
+__device__ __noinline__ void next_event(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng, float out[3],
                            Counters& rays)
 {
     out[0] = out[1] = out[2] = 0.0f;
@@ -791,7 +791,7 @@ __device__ void next_event(const SceneView& s, const float x[3], const float n[3
     }
 }
 
-__device__ float lamp_hit_weight(const SceneView& s, uint32_t segment_light, const Hit& h, const float origin[3],
+__device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segment_light, const Hit& h, const float origin[3],
                                  const float dir[3], const float seg_n[3])
 {
     if (segment_light == 0u || h.t < kNearField) return 1.0f;
@@ -917,8 +917,10 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
     }
 }
 
-// One thread per pixel; blocks of 128 threads cover 16 x 8 pixel tiles.
-__global__ void __launch_bounds__(128) trace_kernel(const SceneView s, const TraceParams P, float* __restrict__ radiance,
+// One thread per pixel; blocks of 128 threads cover 16 x 8 pixel tiles. The traversal, the light-tree
+// walks and the NEE are out-of-line functions (one copy each: the megakernel's instruction footprint
+// was its bound), and 8 blocks per SM cap the registers at 64.
+__global__ void __launch_bounds__(128, 8) trace_kernel(const SceneView s, const TraceParams P, float* __restrict__ radiance,
                                                     unsigned long long* __restrict__ ray_counts)
 {
     const uint32_t tiles_x = (P.width + 15) / 16;
