@@ -463,6 +463,74 @@ def measure_trace(args, world, local, dev, stream, flush):
     return result
 
 
+def measure_large(args, world, local, dev, stream, flush):
+    """The large scene: 2048 x 2048 x 512 voxels (256 x 256 x 64 bricks), ~2M occupied bricks (12 %
+    voxel occupancy overall), ~100k emissive bricks; the flush (records, hash table, light records,
+    a full light-tree rebuild) and 1920 x 1080 frames at 4 spp, 6 bounces, light-tree NEE."""
+    import torch
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    t0 = time.perf_counter()
+    vs = workloads.noise_world_large()
+    gen_s = time.perf_counter() - t0
+    scene = caelix_b200.Scene(dev, vs.group_shift)
+    t0 = time.perf_counter()
+    scene.upload_bricks(vs.keys, vs.voxels)
+    em = vs.power > 0
+    scene.set_brick_power(vs.keys[em], vs.power[em])
+    scene.set_albedo(vs.albedo)
+    upload_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    scene.flush(stream.cuda_stream)
+    flush_wall_s = time.perf_counter() - t0
+    ls = scene.light_stats()
+    renderer = caelix_b200.Renderer(dev, scene)
+    w, h, spp, bounces = 1920, 1080, 4, 6
+    out = torch.zeros(w * h * 3, dtype=torch.float32, device="cuda")
+    sptr = stream.cuda_stream
+    with torch.cuda.stream(stream):
+        renderer.render(out, w, h, vs.camera, bounces=bounces, seed=999, spp=spp, stream=sptr)
+    stream.synchronize()
+    steps = max(1, min(args.steps, 3))
+    rays = 0
+    total_ms = 0.0
+    for k in range(steps):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            renderer.render(out, w, h, vs.camera, bounces=bounces, seed=1 + 4 * k, spp=spp, stream=sptr)
+            b.record(stream)
+        st = renderer.stats()
+        rays += st.primary_rays + st.bounce_rays + st.shadow_rays
+        total_ms += a.elapsed_time(b)
+    ms = max_over_ranks(total_ms, world) / steps
+    t = renderer.timings()
+    result = {
+        "workload": "2048x2048x512-voxel world (256x256x64 bricks), value noise seed 3, 1920x1080, 4 spp, "
+                    "6 bounces, light-tree NEE with MIS",
+        "bricks": int(vs.brick_count),
+        "brick_occupancy": float(vs.brick_count) / (256 * 256 * 64),
+        "voxel_occupancy": float((vs.voxels != 0).sum()) / (2048 * 2048 * 512),
+        "emissive_bricks": int(em.sum()),
+        "light_tree_leaves": int(ls.tree_leaves[0]),
+        "light_tree_nodes": int(ls.tree_nodes[0]),
+        "flush_ms": float(t.flush_ms),
+        "flush_wall_s": flush_wall_s,
+        "generate_s": gen_s,
+        "upload_s": upload_s,
+        "frame_ms": ms,
+        "rays_per_frame": rays / steps,
+        "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6,
+    }
+    renderer.close()
+    scene.close()
+    return result
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -493,6 +561,8 @@ def run_ours(args, world, rank, local):
         if build is not None:
             line["build"] = {k: build[k] for k in ("workload", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
                                                    "roofline", "roofline_build", "e2e")}
+        if args.large:
+            line["large"] = measure_large(args, world, local, dev, stream, flush)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             rays, secs, frames = oracle_trace(10.0, 1)
             line["cpu_baseline"] = {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": 1, "kind": "port",
@@ -513,6 +583,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
     ap.add_argument("--no-build", action="store_true", help="trace workload only: skip the build section")
+    ap.add_argument("--large", action=argparse.BooleanOptionalAction, default=True,
+                    help="add the large-scene section (2M bricks, 1080p, 4 spp, 6 bounces)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

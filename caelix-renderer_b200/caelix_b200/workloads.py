@@ -203,6 +203,92 @@ def noise_world(grid_bricks=(16, 16, 16), brick_occupancy=0.30, voxel_fill=0.5, 
     return VoxelScene(grid_bricks, keys, voxels, power, albedo, camera)
 
 
+def _torch_pcg_hash(v):
+    import torch
+
+    v = v & 0xFFFFFFFF
+    state = (v * 747796405 + 2891336453) & 0xFFFFFFFF
+    word = (((state >> ((state >> 28) + 4)) ^ state) * 277803737) & 0xFFFFFFFF
+    return ((word >> 22) ^ word) & 0xFFFFFFFF
+
+
+def _torch_value_noise(p, seed: int):
+    """value_noise on a torch int64/float64 device tensor p[..., 3] (the same lattice hash)."""
+    import torch
+
+    i0 = torch.floor(p).to(torch.int64)
+    f = p - i0.to(torch.float64)
+    w = f * f * (3.0 - 2.0 * f)
+    s = int(pcg_hash(np.uint32(seed)))
+    out = torch.zeros(p.shape[:-1], dtype=torch.float64, device=p.device)
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                h = _torch_pcg_hash((i0[..., 2] + dz) ^ s)
+                h = _torch_pcg_hash((i0[..., 1] + dy) ^ h)
+                h = _torch_pcg_hash((i0[..., 0] + dx) ^ h)
+                v = (h >> 8).to(torch.float64) / 16777216.0
+                wx = w[..., 0] if dx else 1.0 - w[..., 0]
+                wy = w[..., 1] if dy else 1.0 - w[..., 1]
+                wz = w[..., 2] if dz else 1.0 - w[..., 2]
+                out += v * wx * wy * wz
+    return out
+
+
+def noise_world_large(grid_bricks=(256, 256, 64), occupied_bricks=2_000_000, voxel_fill=0.25, emissive_bricks=100_000,
+                      seed=3, brick_scale=1.0 / 16, voxel_scale=0.125, chunk=1 << 16, camera=None) -> VoxelScene:
+    """The large trace scene, generated on the GPU (torch): a grid of bricks, `occupied_bricks` of
+    them occupied (highest value noise at brick scale), their voxels solid where the voxel-scale
+    value noise exceeds 1 - voxel_fill, materials uniform in [1, 64] (PcgHash of the voxel's global
+    index, so no host stream of a billion draws is needed), `emissive_bricks` of the
+    occupied bricks emissive with power log-normal(0, 1) (PCG32 streams of `seed`). Returns host
+    arrays (the oracle and the C ABI take host memory)."""
+    import torch
+
+    gx, gy, gz = grid_bricks
+    total = gx * gy * gz
+    dev = "cuda"
+    lin = torch.arange(total, dtype=torch.int64, device=dev)
+    b = torch.stack([lin % gx, (lin // gx) % gy, lin // (gx * gy)], -1)
+    nb = _torch_value_noise((b.to(torch.float64) + 0.5) * brick_scale, seed * 7919 + 1)
+    # Highest noise first, ties by index: a stable sort of -noise.
+    order = torch.sort(-nb, stable=True).indices
+    occupied = torch.sort(order[:occupied_bricks]).values
+    keys = b[occupied].to(torch.int32)
+    n = keys.shape[0]
+    v = torch.arange(512, dtype=torch.int64, device=dev)
+    local = torch.stack([v % 8, (v // 8) % 8, v // 64], -1).to(torch.float64)
+    mat_seed = int(pcg_hash(np.uint32(seed * 7919 + 3)))
+    voxels = torch.empty((n, 512), dtype=torch.int32, device=dev)
+    # The solid threshold: the (1 - voxel_fill) quantile of the voxel noise over the first bricks,
+    # so that voxel_fill of the voxels of occupied bricks are solid.
+    probe = min(n, 4096)
+    pos = keys[:probe, None, :].to(torch.float64) * 8 + local[None] + 0.5
+    sample = _torch_value_noise(pos * voxel_scale, seed * 7919 + 2).reshape(-1)
+    threshold = float(torch.kthvalue(sample.cpu(), max(1, int((1.0 - voxel_fill) * sample.numel()))).values)
+    for start in range(0, n, chunk):
+        end = min(n, start + chunk)
+        pos = keys[start:end, None, :].to(torch.float64) * 8 + local[None] + 0.5
+        nv = _torch_value_noise(pos * voxel_scale, seed * 7919 + 2)
+        index = torch.arange(start * 512, end * 512, dtype=torch.int64, device=dev).view(end - start, 512)
+        material = 1 + (_torch_pcg_hash(index ^ mat_seed) >> 26)  # uniform in [1, 64]
+        voxels[start:end] = torch.where(nv > threshold, (0x8000 | material).to(torch.int32),
+                                        torch.zeros_like(material, dtype=torch.int32))
+    keys_h = keys.cpu().numpy()
+    vox_h = voxels.cpu().numpy().astype(np.uint16)
+    emitters = min(emissive_bricks, n)
+    perm = np.lexsort((np.arange(n), Pcg32(seed, 3).next_u32(n)))
+    power = np.zeros(n, np.float32)
+    power[np.sort(perm[:emitters])] = Pcg32(seed, 4).lognormal(emitters)
+    albedo = np.zeros((128, 3), np.float32)
+    albedo[1:65] = (0.1 + 0.8 * Pcg32(seed, 5).next_doubles(64 * 3)).reshape(64, 3).astype(np.float32)
+    world = np.array([gx, gy, gz], np.float64) * 8
+    if camera is None:
+        camera = look_at(world * np.array([-0.05, 1.0, -0.05]) + np.array([0.0, 200.0, 0.0]),
+                         world * np.array([0.45, 0.3, 0.45]), tan_half_fov_y=0.5, aspect=16.0 / 9.0)
+    return VoxelScene(grid_bricks, keys_h, vox_h, power, albedo, camera)
+
+
 def pack_voxel(x, y, z) -> np.ndarray:
     return (np.asarray(x, np.uint32) | (np.asarray(y, np.uint32) << np.uint32(10)) |
             (np.asarray(z, np.uint32) << np.uint32(20))).astype(np.uint32)

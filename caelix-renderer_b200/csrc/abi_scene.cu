@@ -6,9 +6,8 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
-#include <map>
+#include <unordered_map>
 #include <new>
-#include <tuple>
 #include <vector>
 
 #include "../../include/caelix_b200.h"
@@ -20,13 +19,16 @@ using cx::log;
 
 namespace {
 
-using Key = std::tuple<int32_t, int32_t, int32_t>;
-
 constexpr int32_t kMaxKey = 1024;
 
 bool key_ok(const CaelixBrickKey& k)
 {
     return k.x >= 0 && k.y >= 0 && k.z >= 0 && k.x < kMaxKey && k.y < kMaxKey && k.z < kMaxKey;
+}
+
+uint64_t pack_key(const CaelixBrickKey& k)
+{
+    return (uint64_t)(uint32_t)k.x | ((uint64_t)(uint32_t)k.y << 20) | ((uint64_t)(uint32_t)k.z << 40);
 }
 
 }  // namespace
@@ -35,8 +37,11 @@ struct CaelixScene
 {
     CaelixDevice* device = nullptr;
     uint32_t group_shift = 4;
-    std::map<Key, std::vector<uint16_t>> bricks;
-    std::map<Key, float> power;
+    // Host staging of the uploaded bricks: slot s holds keys[3s .. 3s+2] and voxels[512s ..].
+    std::unordered_map<uint64_t, uint32_t> slot_of;
+    std::vector<int32_t> keys;
+    std::vector<uint16_t> voxels;
+    std::unordered_map<uint64_t, float> power;
     float albedo[cx::kMaterialSlots * 3];
     CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
     bool dirty = true;
@@ -136,8 +141,20 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     }
     const uint16_t* b = static_cast<const uint16_t*>(blocks);
     for (uint32_t i = 0; i < count; ++i) {
-        std::vector<uint16_t>& v = scene->bricks[Key(keys[i].x, keys[i].y, keys[i].z)];
-        v.assign(b + 512ull * i, b + 512ull * (i + 1));
+        const uint64_t packed = pack_key(keys[i]);
+        auto it = scene->slot_of.find(packed);
+        uint32_t slot;
+        if (it == scene->slot_of.end()) {
+            slot = (uint32_t)(scene->keys.size() / 3);
+            scene->slot_of.emplace(packed, slot);
+            scene->keys.push_back(keys[i].x);
+            scene->keys.push_back(keys[i].y);
+            scene->keys.push_back(keys[i].z);
+            scene->voxels.resize(scene->voxels.size() + 512);
+        } else {
+            slot = it->second;
+        }
+        std::memcpy(scene->voxels.data() + 512ull * slot, b + 512ull * i, 1024);
     }
     scene->dirty = scene->dirty || count > 0;
     if (consumed) *consumed = count;
@@ -152,7 +169,7 @@ CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_
     if (!scene || entity != 0 || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
     for (uint32_t i = 0; i < count; ++i)
         if (!key_ok(keys[i]) || !std::isfinite(power[i]) || power[i] < 0.0f) return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (uint32_t i = 0; i < count; ++i) scene->power[Key(keys[i].x, keys[i].y, keys[i].z)] = power[i];
+    for (uint32_t i = 0; i < count; ++i) scene->power[pack_key(keys[i])] = power[i];
     scene->dirty = scene->dirty || count > 0;
     return CAELIX_OK;
     CAELIX_GUARD_END
@@ -197,31 +214,26 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     cudaSetDevice(scene->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
     // Bricks in increasing linear brick index of the grid spanned by the keys.
+    const uint32_t n = (uint32_t)(scene->keys.size() / 3);
+    const int32_t* sk = scene->keys.data();
     uint32_t grid[3] = {1, 1, 1};
-    for (const auto& kv : scene->bricks) {
-        grid[0] = std::max<uint32_t>(grid[0], std::get<0>(kv.first) + 1);
-        grid[1] = std::max<uint32_t>(grid[1], std::get<1>(kv.first) + 1);
-        grid[2] = std::max<uint32_t>(grid[2], std::get<2>(kv.first) + 1);
-    }
-    std::vector<std::pair<uint64_t, const std::pair<const Key, std::vector<uint16_t>>*>> order;
-    order.reserve(scene->bricks.size());
-    for (const auto& kv : scene->bricks) {
-        const uint64_t lin = (uint64_t)std::get<0>(kv.first) +
-                             grid[0] * ((uint64_t)std::get<1>(kv.first) + (uint64_t)grid[1] * std::get<2>(kv.first));
-        order.emplace_back(lin, &kv);
-    }
-    std::sort(order.begin(), order.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
-    const uint32_t n = (uint32_t)order.size();
+    for (uint32_t s = 0; s < n; ++s)
+        for (int k = 0; k < 3; ++k) grid[k] = std::max<uint32_t>(grid[k], (uint32_t)sk[3 * s + k] + 1);
+    std::vector<std::pair<uint64_t, uint32_t>> order(n);
+    for (uint32_t s = 0; s < n; ++s)
+        order[s] = {(uint64_t)sk[3 * s] + grid[0] * ((uint64_t)sk[3 * s + 1] + (uint64_t)grid[1] * sk[3 * s + 2]), s};
+    std::sort(order.begin(), order.end());
     std::vector<int32_t> keys(3ull * n);
     std::vector<uint16_t> voxels(512ull * n);
     std::vector<float> power(n, 0.0f);
     for (uint32_t i = 0; i < n; ++i) {
-        const Key& k = order[i].second->first;
-        keys[3 * i] = std::get<0>(k);
-        keys[3 * i + 1] = std::get<1>(k);
-        keys[3 * i + 2] = std::get<2>(k);
-        std::memcpy(voxels.data() + 512ull * i, order[i].second->second.data(), 1024);
-        const auto p = scene->power.find(k);
+        const uint32_t s = order[i].second;
+        keys[3 * i] = sk[3 * s];
+        keys[3 * i + 1] = sk[3 * s + 1];
+        keys[3 * i + 2] = sk[3 * s + 2];
+        std::memcpy(voxels.data() + 512ull * i, scene->voxels.data() + 512ull * s, 1024);
+        const CaelixBrickKey key{sk[3 * s], sk[3 * s + 1], sk[3 * s + 2]};
+        const auto p = scene->power.find(pack_key(key));
         if (p != scene->power.end() && scene->light_options.enabled) power[i] = p->second;
     }
     uint32_t status = 0;
