@@ -428,6 +428,13 @@ class Scene:
         fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
         self.L.check(self.L.lib.caelix_scene_flush(self.handle, C.byref(fd)), "caelix_scene_flush")
 
+    def set_light_options(self, enabled: bool = True, min_emission: float = 20.0, heap_bytes: int = 16 << 20):
+        """caelix_scene_set_light_options; with the tree already on, the next flush rebuilds only the
+        light tree."""
+        o = CaelixLightOptions(1 if enabled else 0, float(min_emission), int(heap_bytes))
+        self.L.check(self.L.lib.caelix_scene_set_light_options(self.handle, C.byref(o)),
+                     "caelix_scene_set_light_options")
+
     def view(self) -> CaelixSceneView:
         v = CaelixSceneView()
         self.L.check(self.L.lib.caelix_scene_get_view(self.handle, C.byref(v)), "caelix_scene_get_view")
@@ -510,3 +517,118 @@ class Renderer:
         t = CaelixGpuTimings()
         self.L.lib.caelix_renderer_get_gpu_timings(self.handle, C.byref(t))
         return t
+
+
+class CaelixBatchView(C.Structure):
+    _fields_ = [("renderer", C.c_void_p), ("camera", CaelixCamera), ("target", CaelixRenderTargets),
+                ("options", CaelixRenderOptions)]
+
+
+class CaelixBatchDesc(C.Structure):
+    _fields_ = [("view_count", C.c_uint32), ("rebuild_light_trees", C.c_uint32),
+                ("views", C.POINTER(CaelixBatchView)), ("reserved", C.c_uint32 * 4)]
+
+
+class CaelixBatchTuning(C.Structure):
+    _fields_ = [("min_blocks", C.c_uint32), ("wavefront", C.c_uint32), ("block_width", C.c_uint32),
+                ("refill_min", C.c_uint32), ("sort_keys_per_thread", C.c_uint32), ("order", C.c_uint32),
+                ("reserved", C.c_uint32 * 2)]
+
+    def as_dict(self) -> dict:
+        return {n: int(getattr(self, n)) for n, _ in self._fields_ if n != "reserved"}
+
+
+class CaelixBatchStats(C.Structure):
+    _fields_ = [("primary_rays", C.c_uint64), ("bounce_rays", C.c_uint64), ("shadow_rays", C.c_uint64),
+                ("gpu_ms", C.c_float), ("kernel_launches", C.c_uint32), ("light_tree_builds", C.c_uint32),
+                ("wavefront", C.c_uint32), ("graph_captures", C.c_uint32), ("pad", C.c_uint32)]
+
+
+def _bind_batch(L):
+    vp = C.c_void_p
+    proto = {
+        "caelix_batch_create": [vp, C.POINTER(CaelixBatchDesc), C.POINTER(vp)],
+        "caelix_batch_run": [vp, C.POINTER(CaelixFrameDesc)],
+        "caelix_batch_set_tuning": [vp, C.POINTER(CaelixBatchTuning)],
+        "caelix_batch_get_tuning": [vp, C.POINTER(CaelixBatchTuning)],
+        "caelix_batch_autotune": [vp, C.POINTER(CaelixFrameDesc), C.c_char_p, C.c_uint32,
+                                  C.POINTER(CaelixBatchTuning)],
+        "caelix_batch_get_stats": [vp, C.POINTER(CaelixBatchStats)],
+        "caelix_batch_get_view_stats": [vp, C.c_uint32, C.POINTER(CaelixRenderStats)],
+    }
+    for name, args in proto.items():
+        f = getattr(L, name)
+        f.argtypes = args
+        f.restype = C.c_int
+    L.caelix_batch_destroy.argtypes = [vp]
+    L.caelix_batch_destroy.restype = None
+
+
+class Batch:
+    """caelix_batch_*: many views (renderer, target, camera, options) in one CUDA graph launch per run.
+    `views`: (renderer, radiance buffer, width, height, camera, bounces, seed, spp) tuples."""
+
+    def __init__(self, device: Device, views, rebuild_light_trees: bool = True):
+        self.device = device
+        self.L = device.L
+        _bind_scene(self.L.lib)
+        _bind_batch(self.L.lib)
+        self.renderers = [v[0] for v in views]  # kept alive with the batch
+        arr = (CaelixBatchView * len(views))()
+        for i, (renderer, radiance, width, height, camera, bounces, seed, spp) in enumerate(views):
+            arr[i].renderer = renderer.handle
+            arr[i].camera = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
+            arr[i].target = CaelixRenderTargets(_ptr(radiance), width, height)
+            arr[i].options = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+        desc = CaelixBatchDesc(len(views), 1 if rebuild_light_trees else 0, arr, (C.c_uint32 * 4)(0, 0, 0, 0))
+        handle = C.c_void_p()
+        self.L.check(self.L.lib.caelix_batch_create(device.handle, C.byref(desc), C.byref(handle)),
+                     "caelix_batch_create")
+        self.handle = handle
+        self.frame = 0
+
+    def close(self):
+        if self.handle:
+            self.L.lib.caelix_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def run(self, stream: int = 0):
+        self.frame += 1
+        fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
+        self.L.check(self.L.lib.caelix_batch_run(self.handle, C.byref(fd)), "caelix_batch_run")
+
+    def tuning(self) -> CaelixBatchTuning:
+        t = CaelixBatchTuning()
+        self.L.check(self.L.lib.caelix_batch_get_tuning(self.handle, C.byref(t)), "caelix_batch_get_tuning")
+        return t
+
+    def set_tuning(self, **fields):
+        t = self.tuning()
+        for k, v in fields.items():
+            setattr(t, k, int(v))
+        self.L.check(self.L.lib.caelix_batch_set_tuning(self.handle, C.byref(t)), "caelix_batch_set_tuning")
+
+    def autotune(self, cache_path: str | None = None, repeats: int = 2, stream: int = 0) -> CaelixBatchTuning:
+        fd = CaelixFrameDesc(stream, self.frame + 1, self.frame)
+        t = CaelixBatchTuning()
+        path = cache_path.encode() if cache_path else None
+        self.L.check(self.L.lib.caelix_batch_autotune(self.handle, C.byref(fd), path, repeats, C.byref(t)),
+                     "caelix_batch_autotune")
+        return t
+
+    def stats(self) -> CaelixBatchStats:
+        s = CaelixBatchStats()
+        self.L.check(self.L.lib.caelix_batch_get_stats(self.handle, C.byref(s)), "caelix_batch_get_stats")
+        return s
+
+    def view_stats(self, index: int) -> CaelixRenderStats:
+        s = CaelixRenderStats()
+        self.L.check(self.L.lib.caelix_batch_get_view_stats(self.handle, index, C.byref(s)),
+                     "caelix_batch_get_view_stats")
+        return s

@@ -334,3 +334,29 @@ def brick_light_records(n: int, grid_bricks: int = 32, seed: int = 1, stream: in
     frames["origin"][:, 2] = (g // (groups_per_axis * groups_per_axis)) * edge
     frames["rotation"][:] = np.array([1, 0, 0, 0, 1, 0, 0, 0, 1], np.float32)
     return rec, group, frames
+
+
+BATCH_VIEWPORTS = (256, 512, 1024)
+
+
+def batch_plan(count: int = 64, min_bricks: int = 1000, max_bricks: int = 500_000, seed: int = 4):
+    """The batched workload's scene list: `count` scenes with brick counts log-uniform in
+    [min_bricks, max_bricks] and square viewports uniform among BATCH_VIEWPORTS (PCG32 streams of
+    `seed`). Returns [(brick_count, side)]."""
+    u = Pcg32(seed, 11).next_doubles(count)
+    bricks = np.rint(np.exp(np.log(min_bricks) + u * (np.log(max_bricks) - np.log(min_bricks)))).astype(np.int64)
+    sides = np.array(BATCH_VIEWPORTS)[Pcg32(seed, 12).next_u32(count) % np.uint32(len(BATCH_VIEWPORTS))]
+    return [(int(b), int(s)) for b, s in zip(bricks, sides)]
+
+
+def batch_scene(bricks: int, seed: int, occupancy: float = 0.30, emissive_fraction: float = 0.01) -> VoxelScene:
+    """One scene of the batched workload: the plain scene's generator (value noise, `occupancy` of
+    the bricks of a cubic grid occupied, half the voxels of an occupied brick solid, materials
+    uniform in [1, 64], `emissive_fraction` of the bricks emissive with log-normal(0, 1) power)
+    at `bricks` occupied bricks, on the GPU; the camera of the plain scene, aspect 1."""
+    side = int(np.ceil(np.cbrt(bricks / occupancy)))
+    world = np.array([side, side, side], np.float64) * 8
+    camera = look_at(np.array([-0.25, 1.2, -0.35]) * world, world * np.array([0.5, 0.35, 0.5]))
+    return noise_world_large(grid_bricks=(side, side, side), occupied_bricks=bricks, voxel_fill=0.5,
+                             emissive_bricks=max(1, int(round(emissive_fraction * bricks))), seed=seed,
+                             brick_scale=0.25, voxel_scale=0.25, camera=camera)

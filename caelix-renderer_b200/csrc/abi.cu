@@ -100,20 +100,6 @@ struct CaelixLightBvh
 
 using cx::log;
 
-#define CAELIX_GUARD_BEGIN try {
-#define CAELIX_GUARD_END                                               \
-    }                                                                  \
-    catch (const std::bad_alloc&)                                      \
-    {                                                                  \
-        log(CAELIX_LOG_ERROR, "%s: out of host memory", __func__);      \
-        return CAELIX_ERROR_OUT_OF_MEMORY;                             \
-    }                                                                  \
-    catch (...)                                                        \
-    {                                                                  \
-        log(CAELIX_LOG_ERROR, "%s: unexpected exception", __func__);    \
-        return CAELIX_ERROR_INVALID_ARGUMENT;                          \
-    }
-
 extern "C" {
 
 CAELIX_API void caelix_get_version(CaelixVersion* out)

@@ -3,8 +3,25 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <new>
 
 #include "../../include/caelix_b200.h"
+
+// Exceptions never cross the C ABI: the body of every entry point that may allocate on the host
+// runs inside CAELIX_GUARD_BEGIN / CAELIX_GUARD_END.
+#define CAELIX_GUARD_BEGIN try {
+#define CAELIX_GUARD_END                                                \
+    }                                                                   \
+    catch (const std::bad_alloc&)                                       \
+    {                                                                   \
+        cx::log(CAELIX_LOG_ERROR, "%s: out of host memory", __func__);   \
+        return CAELIX_ERROR_OUT_OF_MEMORY;                              \
+    }                                                                   \
+    catch (...)                                                         \
+    {                                                                   \
+        cx::log(CAELIX_LOG_ERROR, "%s: unexpected exception", __func__); \
+        return CAELIX_ERROR_INVALID_ARGUMENT;                           \
+    }
 
 namespace cx {
 

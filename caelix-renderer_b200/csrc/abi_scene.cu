@@ -12,6 +12,7 @@
 
 #include "../../include/caelix_b200.h"
 #include "abi_internal.h"
+#include "abi_scene_internal.h"
 #include "scene.cuh"
 #include "trace.cuh"
 
@@ -33,52 +34,38 @@ uint64_t pack_key(const CaelixBrickKey& k)
 
 }  // namespace
 
-struct CaelixScene
+CaelixResult render_params(const CaelixRenderer* renderer, const CaelixRenderTargets* targets,
+                           const CaelixCamera* camera, const CaelixRenderOptions* options, const char* what,
+                           cx::TraceParams* out)
 {
-    CaelixDevice* device = nullptr;
-    uint32_t group_shift = 4;
-    // Host staging of the uploaded bricks: slot s holds keys[3s .. 3s+2] and voxels[512s ..].
-    std::unordered_map<uint64_t, uint32_t> slot_of;
-    std::vector<int32_t> keys;
-    std::vector<uint16_t> voxels;
-    std::unordered_map<uint64_t, float> power;
-    float albedo[cx::kMaterialSlots * 3];
-    CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
-    bool dirty = true;
-    uint64_t last_frame = 0;
-    cx::DeviceScene dev;
-    bool built = false;
-    cudaEvent_t start = nullptr;
-    cudaEvent_t stop = nullptr;
-    float flush_ms = 0.0f;
-};
-
-struct CaelixRenderer
-{
-    CaelixDevice* device = nullptr;
-    CaelixScene* scene = nullptr;
-    CaelixLightNeeOptions nee{1, 0, 0, 0};
-    unsigned long long* counts = nullptr;
-    cudaEvent_t start = nullptr;
-    cudaEvent_t stop = nullptr;
-    cudaStream_t last_stream = nullptr;
-    uint64_t frame_number = 0;
-    bool rendered = false;
-};
-
-#define CAELIX_GUARD_BEGIN try {
-#define CAELIX_GUARD_END                                             \
-    }                                                                \
-    catch (const std::bad_alloc&)                                    \
-    {                                                                \
-        log(CAELIX_LOG_ERROR, "%s: out of host memory", __func__);    \
-        return CAELIX_ERROR_OUT_OF_MEMORY;                           \
-    }                                                                \
-    catch (...)                                                      \
-    {                                                                \
-        log(CAELIX_LOG_ERROR, "%s: unexpected exception", __func__);  \
-        return CAELIX_ERROR_INVALID_ARGUMENT;                        \
+    if (!renderer || !targets || !camera || !options || !out) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!targets->radiance || targets->width == 0 || targets->height == 0 || options->mode != 1 ||
+        options->bounce_count > 14 || camera->jitter[0] != 0.0f || camera->jitter[1] != 0.0f)
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t r : options->reserved)
+        if (r) return CAELIX_ERROR_INVALID_ARGUMENT;
+    const CaelixScene* scene = renderer->scene;
+    if (!scene->built) {
+        log(CAELIX_LOG_ERROR, "%s: the scene has not been flushed", what);
+        return CAELIX_ERROR_INVALID_ARGUMENT;
     }
+    cx::TraceParams& p = *out;
+    for (int k = 0; k < 3; ++k) {
+        p.position[k] = camera->position[k];
+        p.right[k] = camera->right[k];
+        p.up[k] = camera->up[k];
+        p.forward[k] = camera->forward[k];
+    }
+    p.tan_half_fov_y = camera->tan_half_fov_y;
+    p.aspect = camera->aspect;
+    p.width = targets->width;
+    p.height = targets->height;
+    p.spp = options->spp ? options->spp : 1;
+    p.bounce_count = options->bounce_count;
+    p.frame_seed = options->frame_seed;
+    p.light_nee = (renderer->nee.enabled && scene->light_options.enabled && scene->dev.light_count) ? 1u : 0u;
+    return CAELIX_OK;
+}
 
 extern "C" {
 
@@ -194,8 +181,11 @@ CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const
     if (!scene || !options || options->enabled > 1 || !std::isfinite(options->min_emission) ||
         options->min_emission < 0.0f || options->heap_bytes > (16ull << 32))
         return CAELIX_ERROR_INVALID_ARGUMENT;
+    // Toggling the tree changes the light records (the power of every brick); any other change
+    // takes effect as a light-tree rebuild at the next flush, as in the reference.
+    if (options->enabled != scene->light_options.enabled || !scene->built) scene->dirty = true;
+    else scene->light_tree_dirty = true;
     scene->light_options = *options;
-    scene->dirty = true;
     return CAELIX_OK;
 }
 
@@ -210,9 +200,21 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         return CAELIX_ERROR_INVALID_ARGUMENT;
     }
     scene->last_frame = desc->frame_number;
-    if (!scene->dirty) return CAELIX_OK;
+    if (!scene->dirty && !scene->light_tree_dirty) return CAELIX_OK;
     cudaSetDevice(scene->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
+    if (!scene->dirty) {
+        // Light tree only: the build over the resident light records, then its status.
+        uint32_t status = 0;
+        cudaEventRecord(scene->start, stream);
+        cudaError_t e = cx::scene_build_light_tree(scene->dev, stream);
+        cudaEventRecord(scene->stop, stream);
+        if (e == cudaSuccess) e = cx::scene_read_status(scene->dev, stream, &status);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+        cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
+        scene->light_tree_dirty = false;
+        return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
+    }
     // Bricks in increasing linear brick index of the grid spanned by the keys.
     const uint32_t n = (uint32_t)(scene->keys.size() / 3);
     const int32_t* sk = scene->keys.data();
@@ -245,7 +247,9 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     cudaEventSynchronize(scene->stop);
     cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
     scene->dirty = false;
+    scene->light_tree_dirty = false;
     scene->built = true;
+    scene->generation += 1;
     return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
     CAELIX_GUARD_END
 }
@@ -364,34 +368,13 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
                                                const CaelixRenderOptions* options)
 {
     CAELIX_GUARD_BEGIN
-    if (!renderer || !frame || !targets || !camera || !options) return CAELIX_ERROR_INVALID_ARGUMENT;
-    if (!targets->radiance || targets->width == 0 || targets->height == 0 || options->mode != 1 ||
-        options->bounce_count > 14 || camera->jitter[0] != 0.0f || camera->jitter[1] != 0.0f)
-        return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (uint32_t r : options->reserved)
-        if (r) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!renderer || !frame) return CAELIX_ERROR_INVALID_ARGUMENT;
+    cx::TraceParams p;
+    const CaelixResult r = render_params(renderer, targets, camera, options, "caelix_renderer_render", &p);
+    if (r != CAELIX_OK) return r;
     CaelixScene* scene = renderer->scene;
-    if (!scene->built) {
-        log(CAELIX_LOG_ERROR, "caelix_renderer_render: the scene has not been flushed");
-        return CAELIX_ERROR_INVALID_ARGUMENT;
-    }
     cudaSetDevice(renderer->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
-    cx::TraceParams p;
-    for (int k = 0; k < 3; ++k) {
-        p.position[k] = camera->position[k];
-        p.right[k] = camera->right[k];
-        p.up[k] = camera->up[k];
-        p.forward[k] = camera->forward[k];
-    }
-    p.tan_half_fov_y = camera->tan_half_fov_y;
-    p.aspect = camera->aspect;
-    p.width = targets->width;
-    p.height = targets->height;
-    p.spp = options->spp ? options->spp : 1;
-    p.bounce_count = options->bounce_count;
-    p.frame_seed = options->frame_seed;
-    p.light_nee = (renderer->nee.enabled && scene->light_options.enabled && scene->dev.light_count) ? 1u : 0u;
     cudaError_t e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_render");
     cudaEventRecord(renderer->start, stream);

@@ -1,0 +1,54 @@
+// The scene and renderer objects behind the C ABI, shared by abi_scene.cu and abi_batch.cu.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <unordered_map>
+#include <vector>
+
+#include "../../include/caelix_b200.h"
+#include "abi_internal.h"
+#include "scene.cuh"
+#include "trace.cuh"
+
+struct CaelixScene
+{
+    CaelixDevice* device = nullptr;
+    uint32_t group_shift = 4;
+    // Host staging of the uploaded bricks: slot s holds keys[3s .. 3s+2] and voxels[512s ..].
+    std::unordered_map<uint64_t, uint32_t> slot_of;
+    std::vector<int32_t> keys;
+    std::vector<uint16_t> voxels;
+    std::unordered_map<uint64_t, float> power;
+    float albedo[cx::kMaterialSlots * 3];
+    CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
+    bool dirty = true;
+    bool light_tree_dirty = false;  // only the light tree is stale (a light-options change)
+    uint64_t last_frame = 0;
+    cx::DeviceScene dev;
+    bool built = false;
+    uint64_t generation = 0;  // full builds so far (the device tables move on each)
+    cudaEvent_t start = nullptr;
+    cudaEvent_t stop = nullptr;
+    float flush_ms = 0.0f;
+};
+
+struct CaelixRenderer
+{
+    CaelixDevice* device = nullptr;
+    CaelixScene* scene = nullptr;
+    CaelixLightNeeOptions nee{1, 0, 0, 0};
+    unsigned long long* counts = nullptr;
+    cudaEvent_t start = nullptr;
+    cudaEvent_t stop = nullptr;
+    cudaStream_t last_stream = nullptr;
+    uint64_t frame_number = 0;
+    bool rendered = false;
+};
+
+
+// The trace parameters of a render call (caelix_renderer_render's checks): INVALID_ARGUMENT for a
+// bad target, camera or options, or a scene that was never flushed.
+CaelixResult render_params(const CaelixRenderer* renderer, const CaelixRenderTargets* targets,
+                           const CaelixCamera* camera, const CaelixRenderOptions* options, const char* what,
+                           cx::TraceParams* out);

@@ -10,6 +10,13 @@
 #include <cstddef>
 #include <cstdint>
 
+// Returns the first failing CUDA call's error from a host function returning cudaError_t.
+#define CX_TRY(x)                         \
+    do {                                  \
+        const cudaError_t e_ = (x);       \
+        if (e_ != cudaSuccess) return e_; \
+    } while (0)
+
 namespace cx {
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;

@@ -646,10 +646,11 @@ uint32_t grid_for(uint32_t n, uint32_t per_block, uint32_t cap)
 
 uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t{255}; }
 
-uint64_t zero_words(uint32_t n)
+uint64_t zero_words(uint32_t n, uint32_t kpt)
 {
-    // control words, the sort scratch, then two scan states and their tile counters
-    return sizeof(BuildControl) / 4 + sort_scratch_words(n) + 2ull * ((n + kScanTile - 1) / kScanTile) + 2;
+    // control words, the sort scratch of tiles of 256 * kpt keys, then two scan states and their
+    // tile counters
+    return sizeof(BuildControl) / 4 + sort_scratch_words(n, kpt) + 2ull * ((n + kScanTile - 1) / kScanTile) + 2;
 }
 
 }  // namespace
@@ -664,7 +665,7 @@ uint64_t lt_buffer_bytes(uint32_t cap)
     b += 14 * align256(c * 4);                // u32 arrays
     b += align256(c * sizeof(AggregateSlot));
     b += align256(c * sizeof(LightSummary));
-    b += align256(zero_words((uint32_t)c) * 4);
+    b += align256(zero_words((uint32_t)c, kSortMinKeysPerThread) * 4);
     return b;
 }
 
@@ -702,7 +703,7 @@ LightBvhBuffers lt_carve(void* base, uint32_t cap)
     b.leaf_word = u32();
     b.aggregates = reinterpret_cast<AggregateSlot*>(take(c * sizeof(AggregateSlot)));
     b.sorted = reinterpret_cast<LightSummary*>(take(c * sizeof(LightSummary)));
-    char* z = take(zero_words((uint32_t)c) * 4);
+    char* z = take(zero_words((uint32_t)c, kSortMinKeysPerThread) * 4);
     b.control = reinterpret_cast<BuildControl*>(z);
     b.sort_scratch = reinterpret_cast<uint32_t*>(z + sizeof(BuildControl));
     return b;
@@ -718,11 +719,13 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     mark(0);
     // Zeroed words of this build: control, the sort scratch sized for n, two scan state arrays and
     // their tile counters.
+    const uint32_t kpt = sort_keys_per_thread_ok(in.sort_keys_per_thread) ? in.sort_keys_per_thread
+                                                                             : (uint32_t)kSortKeysPerThread;
     const uint32_t scan_tiles_n = (n + kScanTile - 1) / kScanTile;
-    uint32_t* cover_states = b.sort_scratch + sort_scratch_words(n);
+    uint32_t* cover_states = b.sort_scratch + sort_scratch_words(n, kpt);
     uint32_t* flag_states = cover_states + scan_tiles_n;
     uint32_t* scan_counters = flag_states + scan_tiles_n;
-    cudaError_t e = cudaMemsetAsync(b.control, 0, zero_words(n) * 4, stream);
+    cudaError_t e = cudaMemsetAsync(b.control, 0, zero_words(n, kpt) * 4, stream);
     if (e != cudaSuccess) return e;
     const uint32_t sms = 148;
     if (n > 0) {
@@ -738,7 +741,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
         gather.inverse = b.inverse;
         onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
-                      stream, &gather);
+                      stream, &gather, kpt);
         mark(3);
     } else {
         mark(1);

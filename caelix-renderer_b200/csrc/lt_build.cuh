@@ -32,6 +32,7 @@
 #include <cstdint>
 
 #include "cx_layout.h"
+#include "radix_sort.cuh"
 
 namespace cx {
 
@@ -111,6 +112,7 @@ struct LightBvhInput
     const uint32_t* record_entry;
     const GroupFrame* group_frames;
     uint32_t group_count;
+    uint32_t sort_keys_per_thread = kSortKeysPerThread;  // the radix sort's tile: 256 x 4, 8 or 16 keys
 };
 
 constexpr int kScanThreads = 256;

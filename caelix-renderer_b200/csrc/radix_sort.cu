@@ -42,7 +42,7 @@ __global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __
     }
 }
 
-// One onesweep pass over a tile of kSortTile elements. Phases:
+// One onesweep pass over a tile of 256 * KPT elements. Phases:
 //   1. keys (warp-striped, coalesced) -> digits -> stable rank inside the warp (__match_any_sync);
 //   2. per-digit warp offsets and tile counts; the tile's counts are published at once (the
 //      look-back of later tiles can proceed), then the keys go to the shared staging area in
@@ -50,15 +50,17 @@ __global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __
 //   3. decoupled look-back per digit (one thread per digit, bounded spin);
 //   4. values (and, on the gathering pass, the 48-byte rows) are staged by the same positions and
 //      the tile is written out in runs per digit.
+template <int KPT>
 __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const SortPass a)
 {
+    constexpr int kTile = kSortThreads * KPT;
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_warp_counts[kSortWarps][kRadix];  // counts, then exclusive offsets per warp
     __shared__ uint32_t s_local[kRadix];                    // tile-local exclusive offset of each digit
     __shared__ uint32_t s_dest[kRadix];                     // global destination base minus s_local
     __shared__ uint32_t s_scan[kSortWarps];
-    __shared__ uint32_t s_keys[kSortTile];
-    __shared__ uint32_t s_values[kSortTile];
+    __shared__ uint32_t s_keys[kTile];
+    __shared__ uint32_t s_values[kTile];
 
     const uint32_t tid = threadIdx.x;
     const uint32_t lane = tid & 31u;
@@ -68,20 +70,20 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
     for (int w = 0; w < kSortWarps; ++w) s_warp_counts[w][tid] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
-    const uint32_t base = tile * kSortTile;
-    const uint32_t warp_base = base + warp * 32u * kSortKeysPerThread;
+    const uint32_t base = tile * kTile;
+    const uint32_t warp_base = base + warp * 32u * KPT;
 
     // Phase 1.
-    uint32_t key[kSortKeysPerThread];
-    uint32_t pos[kSortKeysPerThread];  // rank in the warp, then position in the tile
+    uint32_t key[KPT];
+    uint32_t pos[KPT];  // rank in the warp, then position in the tile
 #pragma unroll
-    for (int k = 0; k < kSortKeysPerThread; ++k) {
+    for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
         key[k] = i < a.n ? __ldg(a.keys_in + i) : 0u;
     }
     const uint32_t lt = lanemask_lt();
 #pragma unroll
-    for (int k = 0; k < kSortKeysPerThread; ++k) {
+    for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
         const uint32_t digit = i < a.n ? (key[k] >> a.shift) & 255u : 256u + lane;  // invalid: alone
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
@@ -111,7 +113,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
     s_local[d] = local;
     __syncthreads();
 #pragma unroll
-    for (int k = 0; k < kSortKeysPerThread; ++k) {
+    for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
         if (i < a.n) {
             const uint32_t digit = (key[k] >> a.shift) & 255u;
@@ -146,12 +148,12 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
 
     // Phase 4.
 #pragma unroll
-    for (int k = 0; k < kSortKeysPerThread; ++k) {
+    for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
         if (i < a.n) s_values[pos[k]] = a.values_in ? __ldg(a.values_in + i) : i;
     }
     __syncthreads();
-    const uint32_t count = a.n - base < (uint32_t)kSortTile ? a.n - base : (uint32_t)kSortTile;
+    const uint32_t count = a.n - base < (uint32_t)kTile ? a.n - base : (uint32_t)kTile;
     for (uint32_t j = tid; j < count; j += kSortThreads) {
         const uint32_t k = s_keys[j];
         const uint32_t v = s_values[j];
@@ -182,10 +184,11 @@ void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t 
 
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
-                   const SortGather* gather)
+                   const SortGather* gather, uint32_t keys_per_thread)
 {
     if (n == 0) return;
-    const uint32_t tiles = sort_tiles(n);
+    if (!sort_keys_per_thread_ok(keys_per_thread)) keys_per_thread = kSortKeysPerThread;
+    const uint32_t tiles = sort_tiles(n, keys_per_thread);
     uint32_t* hist = scratch;
     uint32_t* counters = scratch + 4 * kRadix;
     uint32_t* states = counters + 4;
@@ -210,7 +213,9 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         p.rows_in_stride = gather ? gather->rows_in_stride : 0;
         p.rows_out = (last && gather) ? gather->rows_out : nullptr;
         p.inverse = (last && gather) ? gather->inverse : nullptr;
-        onesweep_pass_kernel<<<tiles, kSortThreads, 0, stream>>>(p);
+        if (keys_per_thread == 4) onesweep_pass_kernel<4><<<tiles, kSortThreads, 0, stream>>>(p);
+        else if (keys_per_thread == 8) onesweep_pass_kernel<8><<<tiles, kSortThreads, 0, stream>>>(p);
+        else onesweep_pass_kernel<16><<<tiles, kSortThreads, 0, stream>>>(p);
         uint32_t* t = kin;
         kin = kout;
         kout = t;

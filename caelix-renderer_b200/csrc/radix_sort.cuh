@@ -8,7 +8,7 @@
 // One pass is one kernel (no separate histogram or scan launch):
 //   * the digit counts of all four passes come from one upsweep (the caller's key producer, or
 //     radix_histogram_kernel), so a pass only needs its own 256 global counts;
-//   * a CTA takes the next tile id from an atomic counter, loads 4096 keys warp-striped
+//   * a CTA takes the next tile id from an atomic counter, loads a tile of keys warp-striped
 //     (coalesced 128-byte rows), ranks them stably inside each warp with __match_any_sync peers,
 //     and publishes its per-digit counts in the tile status words;
 //   * the per-digit exclusive prefix over earlier tiles comes from a decoupled look-back over
@@ -26,25 +26,33 @@ namespace cx {
 
 constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
-constexpr int kSortKeysPerThread = 16;
-constexpr int kSortTile = kSortThreads * kSortKeysPerThread;  // 4096
+constexpr int kSortKeysPerThread = 16;  // the default tile: 4096 keys
+constexpr int kSortMinKeysPerThread = 4;  // the smallest tile a caller may pick: 1024 keys
 constexpr int kRadix = 256;
 constexpr uint32_t kTileFlagAggregate = 1u << 30;
 constexpr uint32_t kTileFlagPrefix = 2u << 30;
 constexpr uint32_t kTileValueMask = (1u << 30) - 1u;
 
-__host__ __device__ constexpr uint32_t sort_tiles(uint32_t n)
+// The tile sizes a sort may use: 256 threads x 4, 8 or 16 keys.
+__host__ __device__ constexpr bool sort_keys_per_thread_ok(uint32_t kpt)
 {
-    return (n + kSortTile - 1) / kSortTile;
+    return kpt == 4 || kpt == 8 || kpt == 16;
 }
 
-// Scratch words one sort of n elements needs (all of them zero before the first pass):
+__host__ __device__ constexpr uint32_t sort_tiles(uint32_t n, uint32_t kpt = kSortKeysPerThread)
+{
+    return (n + kSortThreads * kpt - 1) / (kSortThreads * kpt);
+}
+
+// Scratch words one sort of n elements with tiles of 256 * kpt keys needs (all of them zero
+// before the first pass):
 //   histogram  4 * 256 digit counts
 //   counters   4 tile-id counters (one per pass)
 //   states     4 * tiles * 256 look-back status words
-__host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n)
+// sort_scratch_words(n, kSortMinKeysPerThread) covers every tile size.
+__host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n, uint32_t kpt = kSortKeysPerThread)
 {
-    return 4ull * kRadix + 4ull + 4ull * sort_tiles(n) * kRadix;
+    return 4ull * kRadix + 4ull + 4ull * sort_tiles(n, kpt) * kRadix;
 }
 
 // Accumulates the 256-bin histograms of all four digits of keys[0 .. n) into hist[4][256].
@@ -66,8 +74,10 @@ struct SortGather
 // 0 .. n-1 and are not read (values_a is still written). `scratch` holds sort_scratch_words(n)
 // words, already zero, with the histograms of all four digits in its first 1024 words
 // (radix_histogram or a fused producer).
+// `keys_per_thread` (4, 8 or 16) sets the tile (256 * keys_per_thread keys); `scratch` then holds
+// sort_scratch_words(n, keys_per_thread) words.
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
-                   const SortGather* gather = nullptr);
+                   const SortGather* gather = nullptr, uint32_t keys_per_thread = kSortKeysPerThread);
 
 }  // namespace cx

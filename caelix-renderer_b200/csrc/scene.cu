@@ -543,12 +543,6 @@ cudaError_t alloc(T*& p, uint64_t count)
     return cudaMalloc(&p, std::max<uint64_t>(count, 1) * sizeof(T));
 }
 
-#define CX_TRY(x)                              \
-    do {                                       \
-        const cudaError_t e_ = (x);            \
-        if (e_ != cudaSuccess) return e_;      \
-    } while (0)
-
 cudaError_t run_scan(bool max_op, const uint32_t* in, uint32_t* out, uint32_t count, uint32_t* scratch,
                      uint32_t* total, uint32_t* status, cudaStream_t stream)
 {
@@ -748,14 +742,26 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
         s.tree_capacity = cap;
         CX_TRY(cudaMemsetAsync(s.tree.header, 0, 128, stream));
     }
+    CX_TRY(scene_build_light_tree(s, stream));
+    return scene_read_status(s, stream, device_status_out);
+}
+
+cudaError_t scene_build_light_tree(const DeviceScene& s, cudaStream_t stream, uint32_t sort_keys_per_thread)
+{
+    if (s.tree_capacity < std::max(s.light_count, 1u)) return cudaErrorInvalidValue;
     LightBvhInput in;
     in.records = s.light_headers;
-    in.count = m;
+    in.count = s.light_count;
     in.record_group = s.light_group;
     in.record_entry = s.light_entry;
     in.group_frames = s.frames;
     in.group_count = s.group_count;
-    CX_TRY(lt_build(s.tree, in, stream, nullptr));
+    in.sort_keys_per_thread = sort_keys_per_thread;
+    return lt_build(s.tree, in, stream, nullptr);
+}
+
+cudaError_t scene_read_status(const DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out)
+{
     uint32_t status[2] = {0, 0};
     CX_TRY(cudaMemcpyAsync(status, s.status, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaMemcpyAsync(status + 1, &s.tree.state->status, 4, cudaMemcpyDeviceToHost, stream));

@@ -87,6 +87,13 @@ struct DeviceScene
 cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
                         const int32_t* keys, const uint16_t* voxels, const float* power, const float* albedo,
                         cudaStream_t stream, uint32_t* device_status_out);
+// Rebuilds the light tree of a built scene from its light records (asynchronous on `stream`, no
+// allocation: the tree buffers were sized by scene_build). The reference's per-flush light BVH
+// rebuild (lib/src/light/light_tree_record.cpp:230-302, RecordTree).
+cudaError_t scene_build_light_tree(const DeviceScene& s, cudaStream_t stream,
+                                   uint32_t sort_keys_per_thread = kSortKeysPerThread);
+// Reads the scene's and its light tree's device status words (synchronises `stream`).
+cudaError_t scene_read_status(const DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out);
 void scene_release(DeviceScene& s);
 SceneView scene_view(const DeviceScene& s);
 

@@ -1,843 +1,24 @@
-// The trace kernel: one thread per pixel runs the path tracer with light-tree NEE over the brick
-// scene (scene.cuh). Restates, as device code:
-//   brick DDA          shaders/render/caelix_brick_trace.hlsl:177-451
-//   scene traversal    shaders/render/caelix_scene_trace.hlsl:57-169, the TLAS replaced by a
-//                      front-to-back DDA over the brick grid: the occupancy bitmap, then the brick
-//                      hash table, then the brick DDA; the first brick in DDA order with a hit in
-//                      [tmin, tmax) is the closest hit
-//   light tree draw    shaders/light/caelix_light_tree.hlsl:65-767
-//   light tree pdf     caelix_light_tree.hlsl:514-608, 769-777, 853-949
-//   integrator         shaders/render/caelix_path_trace.hlsl:245-449, :737-978,
-//                      caelix_light_nee.hlsl:20-34, caelix_shading.hlsl:267-307,
-//                      caelix_random.hlsl, common/caelix_frame.hlsl:164-171
-// in the configuration of the benchmark scenes: opaque voxels with a Lambertian lobe (metallic 0,
-// smoothness 0), light-tree NEE with MIS, no sun, black sky, no fog, identity entity transform,
-// bounce NEE probability 1. Emission of an opaque voxel = its brick's emitter power on every
-// channel. Every float operation is one IEEE fp32 operation in the reference's order (the library
-// is built with --fmad=false); sin/cos of the unit-vector draw use this library's Cody-Waite +
-// Taylor polynomials, normalize is v * (1 / sqrt(dot(v, v))).
+// The per-frame trace kernel: one thread per pixel runs the path tracer (trace_device.cuh) with
+// light-tree NEE over the brick scene; the integrator loop restates
+// shaders/render/caelix_path_trace.hlsl:737-978 (primary hit, NEE, bounces, MIS, Russian roulette).
 #include <cstdint>
 
-#include "cx_device.cuh"
-#include "scene.cuh"
-#include "scene_device.cuh"
 #include "trace.cuh"
+#include "trace_device.cuh"
 
 namespace cx {
 
 namespace {
 
-constexpr float kRayTMax = 1e30f;
-constexpr float kBounceTMax = 1e4f;
-constexpr float kPushOff = 0.002f;
-constexpr float kNearField = 8.0f;
-constexpr float kPi = 3.1415926535f;
-constexpr float kTwoPi = 6.283185307f;
-
-__device__ __forceinline__ float hmin(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float hmax(float a, float b) { return b > a ? b : a; }
-__device__ __forceinline__ float dot3(const float a[3], const float b[3]) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
-
-// ---- random streams ----
-__device__ __forceinline__ uint32_t pcg_hash(uint32_t v)
-{
-    const uint32_t state = v * 747796405u + 2891336453u;
-    const uint32_t word = ((state >> ((state >> 28u) + 4u)) ^ state) * 277803737u;
-    return (word >> 22u) ^ word;
-}
-__device__ __forceinline__ uint32_t init_random(uint32_t px, uint32_t py, uint32_t seed)
-{
-    const uint32_t s = pcg_hash(px ^ (py << 16) ^ (seed * 0x9E3779B9u));
-    return s != 0u ? s : 0x9E3779B9u;
-}
-__device__ __forceinline__ uint32_t random_u32(uint32_t& s)
-{
-    s ^= s << 13;
-    s ^= s >> 17;
-    s ^= s << 5;
-    return s;
-}
-__device__ __forceinline__ float random01(uint32_t& s) { return (float)(random_u32(s) >> 8) * (1.0f / 16777216.0f); }
-__device__ __forceinline__ uint32_t lt_random(uint32_t& rng)
-{
-    rng = rng * 747796405u + 2891336453u;
-    const uint32_t word = ((rng >> ((rng >> 28) + 4u)) ^ rng) * 277803737u;
-    return (word >> 22) ^ word;
-}
-__device__ __forceinline__ float lt_random_float(uint32_t& rng) { return (float)(lt_random(rng) >> 8) * (1.0f / 16777216.0f); }
-
-// sin and cos of a in [0, 2 pi]: Cody-Waite reduction by pi/2, Taylor polynomials (Horner).
-__device__ __forceinline__ void sincos_cw(float a, float& s, float& c)
-{
-    const float k = floorf(a * 0.636619772f + 0.5f);
-    const float r = (a - k * 1.57079637f) - k * -4.37113883e-8f;
-    const float r2 = r * r;
-    const float sp =
-        r + r * r2 * (-0.166666667f + r2 * (0.00833333333f + r2 * (-0.000198412698f + r2 * 2.75573192e-6f)));
-    const float cp =
-        1.0f + r2 * (-0.5f + r2 * (0.0416666667f + r2 * (-0.00138888889f + r2 * (2.48015873e-5f + r2 * -2.75573192e-7f))));
-    const int q = ((int)k) & 3;
-    s = q == 0 ? sp : (q == 1 ? cp : (q == 2 ? -sp : -cp));
-    c = q == 0 ? cp : (q == 1 ? -sp : (q == 2 ? -cp : sp));
-}
-
-__device__ __forceinline__ void random_unit_vector(uint32_t& rng, float out[3])
-{
-    const float u = random01(rng);
-    const float v = random01(rng);
-    const float a = u * kTwoPi;
-    const float y = v * 2.0f - 1.0f;
-    const float sy = sqrtf(hmax(1.0f - y * y, 0.0f));
-    float sa, ca;
-    sincos_cw(a, sa, ca);
-    out[0] = sa * sy;
-    out[1] = y;
-    out[2] = ca * sy;
-}
-
-// ---- brick DDA ----
-__device__ __forceinline__ float safe_inv_axis(float d)
-{
-    if (fabsf(d) >= 1e-20f) return 1.0f / d;
-    return d < 0.0f ? -1.0f / 1e-20f : 1.0f / 1e-20f;
-}
-
-__device__ __forceinline__ void vrt_step(int cell[3], const float t_start[3], const float origin[3], const float dir[3],
-                                         const float inv[3])
-{
-    float side[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) side[k] = t_start[k] + (float)cell[k] * inv[k];
-    const float tmin = hmin(hmin(side[0], side[1]), side[2]) + 0.0001f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) cell[k] = (int)floorf(origin[k] + tmin * dir[k]);
-}
-
-__device__ __forceinline__ float brick_ray(const uint32_t* __restrict__ rec, const float entry[3], const float dir[3],
-                                           float entry_t, uint32_t entry_coarse, uint32_t& attrib)
-{
-    float inv[3], t_start[3], origin[3];
-    int cell[3], prev[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        inv[k] = safe_inv_axis(dir[k]);
-        t_start[k] = ((dir[k] >= 0.0f ? 1.0f : 0.0f) - entry[k]) * inv[k];
-        origin[k] = hmin(hmax(entry[k], 0.0f), 8.0f - 0.0001f);
-        cell[k] = (int)floorf(origin[k]);
-        prev[k] = cell[k];
-    }
-    for (uint32_t step = 0; step < 22; ++step) {
-        if ((uint32_t)cell[0] >= 8u || (uint32_t)cell[1] >= 8u || (uint32_t)cell[2] >= 8u) break;
-        const uint32_t cbit = (uint32_t)((cell[0] >> 2) | ((cell[1] >> 2) << 1) | ((cell[2] >> 2) << 2));
-        if ((entry_coarse & (1u << cbit)) == 0u) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                cell[k] = dir[k] < 0.0f ? (cell[k] & ~3) : (cell[k] | 3);
-                prev[k] = cell[k];
-            }
-            vrt_step(cell, t_start, origin, dir, inv);
-            continue;
-        }
-        const uint2 occ2 = __ldg(reinterpret_cast<const uint2*>(rec + 2 + 2 * cbit));
-        const uint32_t mbit = (uint32_t)((cell[0] & 3) | ((cell[1] & 3) << 2) | ((cell[2] & 3) << 4));
-        const uint32_t occ_word = mbit < 32 ? occ2.x : occ2.y;
-        if ((occ_word >> (mbit & 31)) & 1u) {
-            const uint32_t w = __ldg(rec + 18 + (cell[0] >> 1) + (cell[1] << 2) + (cell[2] << 5));
-            const uint32_t blk = (w >> ((cell[0] & 1) << 4)) & 0xFFFFu;
-            float T;
-            uint32_t nf;
-            if (step == 0u) {
-                T = 0.0f;
-                nf = entry_coarse >> 26;
-            } else {
-                float side[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) side[k] = t_start[k] + (float)prev[k] * inv[k];
-                T = hmin(hmin(side[0], side[1]), side[2]);
-                const bool mx = side[0] <= T + 0.0001f;
-                const bool my = side[1] <= T + 0.0001f;
-                const uint32_t x_use = mx ? 0xFFFFFFFFu : 0u;
-                const uint32_t y_use = (my ? 0xFFFFFFFFu : 0u) & ~x_use;
-                const uint32_t z_use = ~(x_use | y_use);
-                nf = ((dir[0] > 0.0f ? 2u : 1u) & x_use) | ((dir[1] > 0.0f ? 8u : 4u) & y_use) |
-                     ((dir[2] > 0.0f ? 32u : 16u) & z_use);
-            }
-            bool term = (blk & kOpaqueBit) != 0;
-            if (!term) term = (step == 0 && entry_t == 0.0f) ? false : ((((blk >> 9) & 63u) & nf) != 0);
-            if (term) {
-                attrib = (blk << 16) | (((uint32_t)cell[0] | ((uint32_t)cell[1] << 3) | ((uint32_t)cell[2] << 6)) << 6) | nf;
-                return entry_t + T;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) prev[k] = cell[k];
-        vrt_step(cell, t_start, origin, dir, inv);
-    }
-    attrib = 0u;
-    return 0.0f;
-}
-
-__device__ __forceinline__ float brick_primitive(const uint32_t* __restrict__ rec, const float o[3], const float d[3],
-                                                 float t_current, const float bo[3], uint32_t& attrib)
-{
-    const uint2 info = __ldg(reinterpret_cast<const uint2*>(rec));
-    const uint32_t tb = info.y;
-    const float tmin_v[3] = {(float)(tb & 7u), (float)((tb >> 3) & 7u), (float)((tb >> 6) & 7u)};
-    const float tmax_v[3] = {(float)((tb >> 9) & 7u) + 1.0f, (float)((tb >> 12) & 7u) + 1.0f,
-                             (float)((tb >> 15) & 7u) + 1.0f};
-    float tmin[3], tmax[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float inv = 1.0f / d[k];
-        const float t0 = (bo[k] + tmin_v[k] - o[k]) * inv;
-        const float t1 = (bo[k] + tmax_v[k] - o[k]) * inv;
-        tmin[k] = hmin(t0, t1);
-        tmax[k] = hmax(t0, t1);
-    }
-    const float largest = hmax(hmax(tmin[0], tmin[1]), tmin[2]);
-    const float smallest = hmin(hmin(tmax[0], tmax[1]), tmax[2]);
-    if (largest > smallest || smallest < 0.0f || largest > t_current) {
-        attrib = 0u;
-        return 0.0f;
-    }
-    const float t = hmax(0.0f, largest);
-    float entry[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) entry[k] = o[k] + d[k] * t - bo[k];
-    uint32_t nf;
-    if (largest == tmin[0]) nf = d[0] > 0.0f ? 2u : 1u;
-    else if (largest == tmin[1]) nf = d[1] > 0.0f ? 8u : 4u;
-    else nf = d[2] > 0.0f ? 32u : 16u;
-    return brick_ray(rec, entry, d, t, (nf << 26) | ((info.x >> 16) & 0xFFu), attrib);
-}
-
-struct Hit
-{
-    bool hit;
-    float t;
-    uint32_t attrib;
-    uint32_t record;
-    uint32_t group;
-    float normal[3];
-    float object_hit[3];
-};
-
-// Closest hit over the bricks (front-to-back DDA over the brick grid).
-__device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
-{
-    Hit h;
-    h.hit = false;
-    float inv[3], tnear = -3.0e38f, tfar = 3.0e38f;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        inv[k] = safe_inv_axis(d[k]);
-        const float t0 = (0.0f - o[k]) * inv[k];
-        const float t1 = ((float)(8u * s.grid[k]) - o[k]) * inv[k];
-        tnear = hmax(tnear, hmin(t0, t1));
-        tfar = hmin(tfar, hmax(t0, t1));
-    }
-    const float t_enter = hmax(tnear, tmin_ray);
-    const float t_exit = hmin(tfar, tmax_ray);
-    if (!(t_enter <= t_exit)) return h;
-    int cell[3], step[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float p = o[k] + d[k] * t_enter;
-        int c = (int)floorf(p * 0.125f);
-        c = c < 0 ? 0 : c;
-        c = c > (int)s.grid[k] - 1 ? (int)s.grid[k] - 1 : c;
-        cell[k] = c;
-        step[k] = d[k] >= 0.0f ? 1 : -1;
-    }
-    const uint32_t limit = s.grid[0] + s.grid[1] + s.grid[2] + 3;
-    for (uint32_t it = 0; it < limit; ++it) {
-        const uint64_t lin = (uint64_t)cell[0] + s.grid[0] * ((uint64_t)cell[1] + (uint64_t)s.grid[1] * cell[2]);
-        if ((__ldg(s.bitmap + (lin >> 5)) >> (lin & 31)) & 1u) {
-            const uint32_t r = hash_lookup(s.hash_slots, s.hash_capacity, s.hash_max_probe, cell[0], cell[1], cell[2]);
-            if (r != 0xFFFFFFFFu) {
-                const float bo[3] = {(float)(cell[0] * 8), (float)(cell[1] * 8), (float)(cell[2] * 8)};
-                uint32_t attrib;
-                const float t = brick_primitive(s.records + (uint64_t)r * kRecordWords, o, d, tmax_ray, bo, attrib);
-                if (attrib != 0u && t >= tmin_ray && t < tmax_ray) {
-                    h.hit = true;
-                    h.t = t;
-                    h.attrib = attrib;
-                    h.record = r;
-                    const uint32_t gs = s.group_shift;
-                    h.group = ((uint32_t)cell[0] >> gs) +
-                              s.groups[0] * (((uint32_t)cell[1] >> gs) + s.groups[1] * ((uint32_t)cell[2] >> gs));
-                    const uint32_t f = (uint32_t)(__ffs(attrib & 0x3Fu) - 1);
-                    h.normal[0] = f == 0 ? 1.0f : (f == 1 ? -1.0f : 0.0f);
-                    h.normal[1] = f == 2 ? 1.0f : (f == 3 ? -1.0f : 0.0f);
-                    h.normal[2] = f == 4 ? 1.0f : (f == 5 ? -1.0f : 0.0f);
-#pragma unroll
-                    for (int k = 0; k < 3; ++k) h.object_hit[k] = o[k] + d[k] * t;
-                    return h;
-                }
-            }
-        }
-        float tn[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) tn[k] = ((float)((cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
-        int axis = 0;
-        if (tn[1] < tn[axis]) axis = 1;
-        if (tn[2] < tn[axis]) axis = 2;
-        if (tn[axis] > t_exit) break;
-        cell[axis] += step[axis];
-        if (cell[axis] < 0 || cell[axis] >= (int)s.grid[axis]) break;
-    }
-    return h;
-}
-
-// ---- light tree ----
-__device__ __forceinline__ float power6(const float f[6]) { return f[0] + f[1] + f[2] + f[3] + f[4] + f[5]; }
-
-__device__ __forceinline__ void emitter_cosines(const float dlo[3], const float dhi[3], float c[6])
-{
-    float c2[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float cl = hmin(hmax(0.0f, dlo[k]), dhi[k]);
-        c2[k] = cl * cl;
-    }
-    const float all2 = c2[0] + c2[1] + c2[2];
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float others = all2 - c2[a];
-        c[2 * a] = dhi[a] > 0.0f ? dhi[a] / sqrtf(dhi[a] * dhi[a] + others) : 0.0f;
-        c[2 * a + 1] = dlo[a] < 0.0f ? -dlo[a] / sqrtf(dlo[a] * dlo[a] + others) : 0.0f;
-    }
-}
-
-__device__ __noinline__ float importance(const float x[3], const float n[3], const float lo[3], const float hi[3], const float face[6])
-{
-    float dlo[3], dhi[3], c[6];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        dlo[k] = x[k] - hi[k];
-        dhi[k] = x[k] - lo[k];
-    }
-    emitter_cosines(dlo, dhi, c);
-    float e = 0.0f;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) e += face[f] * c[f];
-    if (e <= 0.0f) return 0.0f;
-    float centre[3], half[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        centre[k] = 0.5f * (lo[k] + hi[k]);
-        half[k] = 0.5f * (hi[k] - lo[k]);
-    }
-    float cr = 1.0f;
-    if (n[0] != 0.0f || n[1] != 0.0f || n[2] != 0.0f) {
-        const float cx[3] = {centre[0] - x[0], centre[1] - x[1], centre[2] - x[2]};
-        const float an[3] = {fabsf(n[0]), fabsf(n[1]), fabsf(n[2])};
-        const float m = dot3(n, cx) + dot3(an, half);
-        if (m <= 0.0f) return 0.0f;
-        float q[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = hmax(hmax(lo[k] - x[k], x[k] - hi[k]), 0.0f);
-        const float dmin = sqrtf(dot3(q, q));
-        cr = dmin > 0.0f ? hmin(1.0f, m / dmin) : 1.0f;
-    }
-    const float tc[3] = {x[0] - centre[0], x[1] - centre[1], x[2] - centre[2]};
-    const float extent2 = dot3(half, half);
-    const float d2 = hmax(dot3(tc, tc), hmax(1.0f, extent2));
-    return e * cr / d2;
-}
-
-struct Pick
-{
-    float sum_i, sum_p, weight_i, weight_p;
-    uint32_t index_i, index_p;
-};
-__device__ __forceinline__ void pick_add(Pick& p, float imp, float pw, uint32_t index, float u)
-{
-    if (imp > 0.0f) {
-        p.sum_i += imp;
-        if (u * p.sum_i < imp) {
-            p.weight_i = imp;
-            p.index_i = index;
-        }
-    }
-    if (pw > 0.0f) {
-        p.sum_p += pw;
-        if (u * p.sum_p < pw) {
-            p.weight_p = pw;
-            p.index_p = index;
-        }
-    }
-}
-__device__ __forceinline__ uint32_t pick_end(const Pick& p, float& prob)
-{
-    if (p.sum_i > 0.0f) {
-        prob = p.weight_i / p.sum_i;
-        return p.index_i;
-    }
-    prob = p.sum_p > 0.0f ? p.weight_p / p.sum_p : 0.0f;
-    return p.sum_p > 0.0f ? p.index_p : kNone;
-}
-__device__ __forceinline__ float pick_probability(float sum_i, float sum_p, float imp, float pw)
-{
-    if (sum_i > 0.0f) return imp / sum_i;
-    return sum_p > 0.0f ? pw / sum_p : 0.0f;
-}
-
-struct Summary
-{
-    float face[6], lo[3], hi[3];
-};
-
-__device__ __forceinline__ void node_slot(const LightBvhNode* nd, uint32_t s, Summary& out)
-{
-#pragma unroll
-    for (int f = 0; f < 6; ++f) out.face[f] = __ldg(&nd->child_face[s][f]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        out.lo[k] = __ldg(&nd->child_lo[s][k]);
-        out.hi[k] = __ldg(&nd->child_hi[s][k]);
-    }
-}
-
-// Tree 0 is the built tree; tree 1 (dynamic entities) is empty.
-__device__ __forceinline__ void tree_summary(const SceneView& s, uint32_t k, Summary& out, uint32_t& root)
-{
-#pragma unroll
-    for (int f = 0; f < 6; ++f) out.face[f] = 0.0f;
-#pragma unroll
-    for (int q = 0; q < 3; ++q) out.lo[q] = out.hi[q] = 0.0f;
-    root = kNone;
-    if (k == 0) {
-        const uint32_t r = __ldg(&s.header->root);
-        if (r != kNone) {
-            root = r;
-#pragma unroll
-            for (int f = 0; f < 6; ++f) out.face[f] = __ldg(&s.header->summary.face[f]);
-#pragma unroll
-            for (int q = 0; q < 3; ++q) {
-                out.lo[q] = __ldg(&s.header->summary.lo[q]);
-                out.hi[q] = __ldg(&s.header->summary.hi[q]);
-            }
-        }
-    }
-}
-
-__device__ __forceinline__ uint32_t child_count(const uint4 c)
-{
-    return (c.x != kNone) + (c.y != kNone) + (c.z != kNone) + (c.w != kNone);
-}
-
-__device__ float tree_probability(const SceneView& s, const float x[3], const float n[3], uint32_t target)
-{
-    float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
-    for (uint32_t k = 0; k < 2; ++k) {
-        Summary sm;
-        uint32_t root;
-        tree_summary(s, k, sm, root);
-        const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
-        const float pw = power6(sm.face);
-        sum_i += imp > 0.0f ? imp : 0.0f;
-        sum_p += pw > 0.0f ? pw : 0.0f;
-        if (k == target) {
-            imp_t = imp;
-            pow_t = pw;
-        }
-    }
-    return pick_probability(sum_i, sum_p, imp_t, pow_t);
-}
-
-__device__ float slot_probability(const LightBvhNode* nd, const float x[3], const float n[3], uint32_t slot)
-{
-    const uint4 ch = __ldg(reinterpret_cast<const uint4*>(nd->child));
-    if (child_count(ch) == 1) return 1.0f;
-    const uint32_t cw[4] = {ch.x, ch.y, ch.z, ch.w};
-    float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
-    for (uint32_t q = 0; q < 4; ++q) {
-        if (cw[q] == kNone) continue;
-        Summary sm;
-        node_slot(nd, q, sm);
-        const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
-        const float pw = power6(sm.face);
-        sum_i += imp > 0.0f ? imp : 0.0f;
-        sum_p += pw > 0.0f ? pw : 0.0f;
-        if (q == slot) {
-            imp_t = imp;
-            pow_t = pw;
-        }
-    }
-    return pick_probability(sum_i, sum_p, imp_t, pow_t);
-}
-
-__device__ __noinline__ float leaf_probability(const SceneView& s, uint32_t leaf, const float x[3], const float n[3])
-{
-    if (__ldg(&s.header->root) == kNone) return 0.0f;
-    const uint32_t parent = __ldg(&s.leaves[leaf].parent);
-    if (parent == kNone) return 0.0f;
-    uint32_t node = parent >> kParentSlotBits, slot = parent & kParentSlotMask;
-    float probability = 1.0f;
-    for (uint32_t depth = 0; depth < 64; ++depth) {
-        const LightBvhNode* nd = s.nodes + node;
-        probability *= slot_probability(nd, x, n, slot);
-        const uint2 up = __ldg(reinterpret_cast<const uint2*>(&nd->parent));
-        if (up.x == kNone) return probability * tree_probability(s, x, n, 0);
-        node = up.x;
-        slot = up.y;
-    }
-    return 0.0f;
-}
-
-__device__ __forceinline__ uint32_t family_count(const uint32_t* rec, uint32_t f)
-{
-    const uint32_t word = f < 3 ? __ldg(rec + 10) : __ldg(rec + 11);
-    return (word >> (10 * (f % 3))) & 0x3FFu;
-}
-
-__device__ float family_weights(const SceneView& s, uint32_t group, const uint32_t* rec, const float x[3], float w[6])
-{
-    const GroupFrame* fr = s.frames + group;
-    float v[3], xg[3], R[9], org[3];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) R[k] = __ldg(&fr->rot[k]);
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        v[k] = x[k] - __ldg(&fr->trans[k]);
-        org[k] = __ldg(&fr->origin[k]);
-    }
-#pragma unroll
-    for (int j = 0; j < 3; ++j) xg[j] = v[0] * R[0 * 3 + j] + v[1] * R[1 * 3 + j] + v[2] * R[2 * 3 + j] - org[j];
-    const uint32_t blo = __ldg(rec + 6), bhi = __ldg(rec + 7);
-    const float lo[3] = {(float)(blo & 0x3FFu), (float)((blo >> 10) & 0x3FFu), (float)((blo >> 20) & 0x3FFu)};
-    const float hi[3] = {(float)(bhi & 0x3FFu), (float)((bhi >> 10) & 0x3FFu), (float)((bhi >> 20) & 0x3FFu)};
-    float dlo[3], dhi[3], c[6];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        dlo[k] = xg[k] - hi[k];
-        dhi[k] = xg[k] - lo[k];
-    }
-    emitter_cosines(dlo, dhi, c);
-    float face[6];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) face[f] = __uint_as_float(__ldg(rec + f));
-    float sum = 0.0f;
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        w[f] = face[f] * c[f];
-        sum += w[f];
-    }
-    if (sum <= 0.0f) {
-        sum = 0.0f;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            w[f] = face[f];
-            sum += w[f];
-        }
-    }
-    return sum;
-}
-
-struct LightPoint
-{
-    float position[3];
-    float normal[3];
-    float pdf;
-    uint32_t block;
-    uint32_t group;
-    uint32_t entry;
-};
-
-__device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
-{
-    float pdf_brick = 1.0f;
-    // The tree (two draws, one per tree).
-    uint32_t root;
-    {
-        Pick pk = {0, 0, 0, 0, kNone, kNone};
-        uint32_t roots[2];
-        for (uint32_t k = 0; k < 2; ++k) {
-            Summary sm;
-            tree_summary(s, k, sm, roots[k]);
-            pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), k, lt_random_float(rng));
-        }
-        float prob;
-        const uint32_t k = pick_end(pk, prob);
-        if (k == kNone) return false;
-        root = roots[k];
-        pdf_brick *= prob;
-    }
-    // Down the 4-wide nodes.
-    uint32_t leaf = kNone;
-    uint32_t node = root;
-    for (uint32_t depth = 0; depth < 64; ++depth) {
-        const LightBvhNode* nd = s.nodes + node;
-        const uint4 ch = __ldg(reinterpret_cast<const uint4*>(nd->child));
-        const uint32_t cw[4] = {ch.x, ch.y, ch.z, ch.w};
-        uint32_t chosen;
-        if (child_count(ch) == 1) {
-            chosen = ch.x;
-        } else {
-            Pick pk = {0, 0, 0, 0, kNone, kNone};
-            for (uint32_t q = 0; q < 4; ++q) {
-                if (cw[q] == kNone) continue;
-                Summary sm;
-                node_slot(nd, q, sm);
-                pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), q, lt_random_float(rng));
-            }
-            float prob;
-            const uint32_t q = pick_end(pk, prob);
-            if (q == kNone) return false;
-            pdf_brick *= prob;
-            chosen = cw[q];
-        }
-        if (chosen & kChildLeafBit) {
-            leaf = chosen & ~kChildLeafBit;
-            break;
-        }
-        node = chosen;
-    }
-    if (leaf == kNone) return false;
-    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&s.leaves[leaf].group));
-    const uint32_t group = owner.x, entry = owner.y;
-    p.group = group;
-    p.entry = entry;
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
-    if (row.y == 0) return false;
-    const uint32_t* block = s.heap + 4ull * row.x;
-    const uint32_t* rec = block + 4ull * __ldg(block + 4 + 4 * entry + 2);
-    float w[6];
-    const float sum = family_weights(s, group, rec, x, w);
-    if (sum <= 0.0f) return false;
-    const float u = lt_random_float(rng) * sum;
-    uint32_t f = kNone, last = 0;
-    float cumulative = 0.0f;
-#pragma unroll
-    for (uint32_t g = 0; g < 6; ++g) {
-        if (w[g] > 0.0f) {
-            last = g;
-            cumulative += w[g];
-            if (f == kNone && u < cumulative) f = g;
-        }
-    }
-    f = f == kNone ? last : f;
-    uint32_t first = 0;
-    for (uint32_t h = 0; h < f; ++h) first += family_count(rec, h);
-    const uint32_t count = family_count(rec, f);
-    if (count == 0 || w[f] <= 0.0f) return false;
-    uint32_t ei = (uint32_t)(lt_random_float(rng) * (float)count);
-    ei = ei > count - 1u ? count - 1u : ei;
-    const uint32_t ent = __ldg(rec + 12 + first + ei);
-    const uint32_t vi = ent & 0x1FFu;
-    const uint32_t gs = s.group_shift, gm = (1u << gs) - 1u;
-    const uint32_t pos = __ldg(rec + 8);
-    const uint32_t voxel[3] = {(pos & gm) * 8 + (vi & 7u), ((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u),
-                               ((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)};
-    const GroupFrame* fr = s.frames + group;
-    const uint32_t axis = f >> 1;
-    float local[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) local[q] = __ldg(&fr->origin[q]) + (float)voxel[q];
-    const float a = lt_random_float(rng);
-    const float b = lt_random_float(rng);
-    local[axis] += (f & 1) ? 0.0f : 1.0f;
-    local[(axis + 1) % 3] += a;
-    local[(axis + 2) % 3] += b;
-    const float dn[3] = {f == 0 ? 1.0f : (f == 1 ? -1.0f : 0.0f), f == 2 ? 1.0f : (f == 3 ? -1.0f : 0.0f),
-                         f == 4 ? 1.0f : (f == 5 ? -1.0f : 0.0f)};
-#pragma unroll
-    for (int r = 0; r < 3; ++r) {
-        const float R0 = __ldg(&fr->rot[3 * r]), R1 = __ldg(&fr->rot[3 * r + 1]), R2 = __ldg(&fr->rot[3 * r + 2]);
-        p.position[r] = R0 * local[0] + R1 * local[1] + R2 * local[2] + __ldg(&fr->trans[r]);
-        p.normal[r] = R0 * dn[0] + R1 * dn[1] + R2 * dn[2];
-    }
-    p.pdf = w[f] / sum / (float)count * pdf_brick;
-    p.block = ent >> 16;
-    return true;
-}
-
-// LightTreeFindLightFace: a light voxel is an opaque voxel of a brick with a light record.
-__device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3], uint32_t group, const uint32_t v[3], uint32_t face,
-                                uint32_t block_value, uint32_t& entry_out, uint32_t& leaf_out, float& in_brick)
-{
-    entry_out = kNone;
-    leaf_out = kNone;
-    in_brick = 0.0f;
-    if (!(block_value & kOpaqueBit) || face > 5) return false;
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
-    if (row.y == 0) return false;
-    const uint32_t* block = s.heap + 4ull * row.x;
-    const uint32_t count_r = __ldg(block);
-    const uint32_t gs = s.group_shift, gm = (1u << gs) - 1u;
-    auto morton = [](uint32_t a, uint32_t b, uint32_t c) {
-        auto part = [](uint32_t q) {
-            q &= 0x3FFu;
-            q = (q | (q << 16)) & 0x030000FFu;
-            q = (q | (q << 8)) & 0x0300F00Fu;
-            q = (q | (q << 4)) & 0x030C30C3u;
-            q = (q | (q << 2)) & 0x09249249u;
-            return q;
-        };
-        return part(a) | (part(b) << 1) | (part(c) << 2);
-    };
-    const uint32_t key = morton(v[0] / 8, v[1] / 8, v[2] / 8);
-    uint32_t lo = 0, hi = count_r, entry = kNone;
-    while (lo < hi) {
-        const uint32_t mid = (lo + hi) >> 1;
-        const uint32_t pos = __ldg(block + 4 + 4 * mid);
-        const uint32_t mk = morton(pos & gm, (pos >> gs) & gm, (pos >> (2 * gs)) & gm);
-        if (mk == key) {
-            entry = mid;
-            break;
-        }
-        if (mk < key) lo = mid + 1;
-        else hi = mid;
-    }
-    if (entry == kNone) return false;
-    entry_out = entry;
-    const uint32_t* rec = block + 4ull * __ldg(block + 4 + 4 * entry + 2);
-    float w[6];
-    const float sum = family_weights(s, group, rec, x, w);
-    const uint32_t count = family_count(rec, face);
-    if (sum <= 0.0f || w[face] <= 0.0f || count == 0) return false;
-    uint32_t first = 0;
-    for (uint32_t g = 0; g < face; ++g) first += family_count(rec, g);
-    const uint32_t vi = (v[0] % 8) | ((v[1] % 8) << 3) | ((v[2] % 8) << 6);
-    uint32_t a = 0, b = count;
-    bool found = false;
-    while (a < b) {
-        const uint32_t mid = (a + b) >> 1;
-        const uint32_t ev = __ldg(rec + 12 + first + mid) & 0x1FFu;
-        if (ev == vi) {
-            found = true;
-            break;
-        }
-        if (ev < vi) a = mid + 1;
-        else b = mid;
-    }
-    if (!found) return false;
-    in_brick = (w[face] / sum) / (float)count;
-    const uint32_t bvh_leaf = __ldg(block + 4 + 4 * entry + 3);
-    if (bvh_leaf != kNone) {
-        const uint32_t leaf = bvh_leaf & 0x7FFFFFFFu;
-        const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&s.leaves[leaf].group));
-        if (owner.x == group && owner.y == entry) leaf_out = bvh_leaf;
-    }
-    return true;
-}
-
-__device__ float brick_pdf(const SceneView& s, const float x[3], const float n[3], uint32_t group, uint32_t entry)
-{
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
-    if (row.y == 0) return 0.0f;
-    const uint32_t* block = s.heap + 4ull * row.x;
-    if (entry >= __ldg(block)) return 0.0f;
-    const uint32_t bvh_leaf = __ldg(block + 4 + 4 * entry + 3);
-    if (bvh_leaf == kNone) return 0.0f;
-    const uint32_t leaf = bvh_leaf & 0x7FFFFFFFu;
-    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&s.leaves[leaf].group));
-    if (owner.x != group || owner.y != entry) return 0.0f;
-    return leaf_probability(s, leaf, x, n);
-}
-
-// ---- integrator ----
-__device__ __forceinline__ float mis_weight(float p_area, const float n_r[3], const float w[3], float d, float cos_l,
-                                            bool nee_side)
-{
-    const float p_sa = cos_l > 0.0f ? p_area * (d * d) / cos_l : 0.0f;
-    const float p_bsdf = hmax(0.0f, dot3(n_r, w)) * (1.0f / 3.1415926535f);
-    if (!(cos_l > 0.0f) || !(p_sa <= 3.0e38f)) return nee_side ? 1.0f : 0.0f;
-    const float sum = p_sa + p_bsdf;
-    if (!(sum > 0.0f)) return nee_side ? 0.0f : 1.0f;
-    return (nee_side ? p_sa : p_bsdf) / sum;
-}
-
-struct Counters
-{
-    uint32_t primary, bounce, shadow;
-};
-
-__device__ __noinline__ void next_event(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng, float out[3],
-                           Counters& rays)
+__device__ __noinline__ void next_event(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng,
+                                        float out[3], Counters& rays)
 {
     out[0] = out[1] = out[2] = 0.0f;
-    const uint32_t point_seed = random_u32(light_rng);
-    LightPoint p;
-    if (!light_sample(s, x, n, point_seed, p) || !(p.pdf > 0.0f)) return;
-    const float d[3] = {p.position[0] - x[0], p.position[1] - x[1], p.position[2] - x[2]};
-    const float d2 = dot3(d, d);
-    const float dist = sqrtf(d2);
-    if (!(dist >= kNearField)) return;
-    const float w[3] = {d[0] / dist, d[1] / dist, d[2] / dist};
-    const float cos_r = dot3(n, w);
-    const float cos_l = -dot3(p.normal, w);
-    if (!(cos_r > 0.0f) || !(cos_l > 0.0f)) return;
-    float scale = (cos_r * (1.0f / kPi)) * (cos_l / d2) / p.pdf;
-    scale *= mis_weight(p.pdf, n, w, dist, cos_l, true);
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * p.group));
-    const uint32_t brick = __ldg(s.heap + 4ull * row.x + 4 + 4 * p.entry + 1);
-    const float e = (p.block & kOpaqueBit) ? __ldg(s.power + brick) : 0.0f;
-    const float contribution[3] = {e * scale, e * scale, e * scale};
-    const float lum = contribution[0] * 0.2126f + contribution[1] * 0.7152f + contribution[2] * 0.0722f;
-    const float w_lamp = lum * hmax(0.05f, 1.0f);
-    const float w_sum = 0.0f + w_lamp;
-    if (!(w_sum > 0.0f)) return;
-    const float t_max = dist - 2.0f * kPushOff;
-    if (t_max > 0.0f) {
-        ++rays.shadow;
-        const Hit h = trace_ray(s, x, w, 0.0f, t_max);
-        if (!h.hit) {
-            const float k = w_sum / w_lamp;
-#pragma unroll
-            for (int q = 0; q < 3; ++q) out[q] = contribution[q] * k;
-        }
-    }
-}
-
-__device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segment_light, const Hit& h, const float origin[3],
-                                 const float dir[3], const float seg_n[3])
-{
-    if (segment_light == 0u || h.t < kNearField) return 1.0f;
-    const GroupFrame* fr = s.frames + h.group;
-    uint32_t vig[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const int32_t voxel = (int32_t)floorf(h.object_hit[k] - 0.25f * h.normal[k]);
-        vig[k] = (uint32_t)(voxel - (int32_t)__ldg(&fr->origin[k]));
-    }
-    const uint32_t face = (uint32_t)(__ffs(h.attrib & 0x3Fu) - 1);
-    const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-    uint32_t entry, leaf;
-    float in_brick;
-    if (!find_light_face(s, origin, h.group, vig, face, block, entry, leaf, in_brick) || leaf == kNone) return 1.0f;
-    const float cos_l = -dot3(h.normal, dir);
-    const float p_area = brick_pdf(s, origin, seg_n, h.group, entry) * in_brick;
-    return mis_weight(p_area, seg_n, dir, h.t, cos_l, false);
-}
-
-__device__ __forceinline__ void shade(const SceneView& s, const Hit& h, const float ray_o[3], const float ray_d[3],
-                                      uint32_t& rng, float albedo[3], float& emission, float origin[3], float dir[3])
-{
-    const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-    emission = (block & kOpaqueBit) ? __ldg(s.power + h.record) : 0.0f;
-    const float* a = s.albedo + 3 * (block & (kMaterialSlots - 1));
-    albedo[0] = __ldg(a);
-    albedo[1] = __ldg(a + 1);
-    albedo[2] = __ldg(a + 2);
-    (void)random01(rng);  // the lobe draw (specular chance 0)
-    float u[3];
-    random_unit_vector(rng, u);
-    const float v[3] = {h.normal[0] + u[0], h.normal[1] + u[1], h.normal[2] + u[2]};
-    const float dp3 = hmax(1.175494351e-38f, dot3(v, v));
-    const float inv = 1.0f / sqrtf(dp3);
-    float dd[3] = {v[0] * inv, v[1] * inv, v[2] * inv};
-    if (!(dot3(dd, dd) > 0.0f)) {
-        dd[0] = h.normal[0];
-        dd[1] = h.normal[1];
-        dd[2] = h.normal[2];
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        dir[k] = dd[k];
-        origin[k] = (ray_o[k] + ray_d[k] * h.t) + kPushOff * h.normal[k];
-    }
+    ShadowRay r;
+    if (!nee_prepare(s, x, n, light_rng, r)) return;
+    ++rays.shadow;
+    const Hit h = trace_ray(s, x, r.dir, 0.0f, r.t_max);
+    if (!h.hit) out[0] = out[1] = out[2] = r.value;
 }
 
 __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t px, uint32_t py, uint32_t seed,

@@ -485,6 +485,99 @@ typedef struct CaelixRenderStats
 } CaelixRenderStats;
 CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, CaelixRenderStats* out);
 
+/* ---------------------------------------------------------------------------
+ * Batch: many scenes and viewports in one CUDA graph launch
+ *
+ * No counterpart in the reference (it renders one scene per renderer call). A batch holds up to
+ * 256 views (a renderer, hence its scene and NEE options, plus a camera, a target and render
+ * options each). One run is one CUDA graph launch: the light tree of every distinct scene is
+ * rebuilt (as caelix_scene_flush does after caelix_scene_set_light_options), the builds of
+ * different scenes running as parallel branches, then one persistent kernel traces every view,
+ * its resident threads taking pixels of all views from one work counter. Each view's radiance is
+ * bit-identical to caelix_renderer_render of the same renderer, target, camera and options.
+ *
+ * The scenes must be flushed before the batch is created. A full re-flush of a scene (bricks,
+ * powers or materials changed) moves its device tables: the next run notices it and captures
+ * the graph again. Calls on a batch and on its scenes and renderers are externally synchronized.
+ * ------------------------------------------------------------------------- */
+
+typedef struct CaelixBatch CaelixBatch;
+
+typedef struct CaelixBatchView
+{
+    CaelixRenderer* renderer;
+    CaelixCamera camera;
+    CaelixRenderTargets target;
+    CaelixRenderOptions options;
+} CaelixBatchView;
+
+typedef struct CaelixBatchDesc
+{
+    uint32_t view_count; /* 1 .. 256 */
+    uint32_t rebuild_light_trees; /* 1: every run rebuilds the light trees first; 0: trace only */
+    const CaelixBatchView* views; /* copied */
+    uint32_t reserved[4]; /* must be 0 */
+} CaelixBatchDesc;
+
+/* The launch parameters of a run, chosen by caelix_batch_autotune or set by hand. */
+typedef struct CaelixBatchTuning
+{
+    uint32_t min_blocks;           /* register cap of the persistent kernel: 4, 6 or 8 CTAs of 128
+                                      threads resident per SM (128, 80 or 64 registers) */
+    uint32_t wavefront;            /* paths in flight = persistent threads, rounded down to whole
+                                      CTAs; 0 = every resident thread */
+    uint32_t block_width;          /* pixel block of 32 consecutive work items: 8 (8x4), 16 (16x2)
+                                      or 32 (32x1) */
+    uint32_t refill_min;           /* a warp takes new pixels once this many lanes are idle, 1..32 */
+    uint32_t sort_keys_per_thread; /* the light-tree radix sort's tile: 256 x 4, 8 or 16 keys */
+    uint32_t order;                /* 0 = views in the given order, 1 = the most pixel samples first */
+    uint32_t reserved[2];          /* must be 0 */
+} CaelixBatchTuning;
+
+/* Creates a batch (device buffers, no GPU work). Fails with INVALID_ARGUMENT on a bad view (NULL
+   renderer, scene not flushed, target not a device buffer of the right size, options as
+   caelix_renderer_render rejects them). */
+CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBatchDesc* desc,
+                                            CaelixBatch** out_batch);
+CAELIX_API void caelix_batch_destroy(CaelixBatch* batch);
+
+/* Launches one run on frame->command_buffer (asynchronous). The first run, and the first after a
+   change of tuning or a scene re-flush, captures the graph first (waiting for the previous run).
+   Runs of one batch share its device buffers: two runs must not overlap (same stream, or the
+   host waits in between). */
+CAELIX_API CaelixResult caelix_batch_run(CaelixBatch* batch, const CaelixFrameDesc* frame);
+
+CAELIX_API CaelixResult caelix_batch_set_tuning(CaelixBatch* batch, const CaelixBatchTuning* tuning);
+CAELIX_API CaelixResult caelix_batch_get_tuning(const CaelixBatch* batch, CaelixBatchTuning* out);
+
+/* Picks the tuning of this batch on this GPU. With a cache file (JSON, NULL = none) whose entry
+   for this GPU and workload exists, takes it without running anything; else times candidate
+   tunings on frame->command_buffer (coordinate descent: the sort tile on the light-tree builds
+   alone, then the trace parameters on the trace alone, each candidate timed by CUDA events over
+   `repeats` runs after one warm-up run; 0 = 2), applies the best and, with a cache file, stores
+   it there. Synchronous. */
+CAELIX_API CaelixResult caelix_batch_autotune(CaelixBatch* batch, const CaelixFrameDesc* frame,
+                                              const char* cache_path, uint32_t repeats,
+                                              CaelixBatchTuning* out);
+
+/* Rays and GPU time of the newest run (read after waiting for it); the status words of the run's
+   builds and trace are checked (CAELIX_ERROR_DEVICE_STATUS on a device-side failure). */
+typedef struct CaelixBatchStats
+{
+    uint64_t primary_rays;
+    uint64_t bounce_rays;
+    uint64_t shadow_rays;
+    float gpu_ms;             /* the whole graph launch */
+    uint32_t kernel_launches; /* kernel nodes of the graph */
+    uint32_t light_tree_builds;
+    uint32_t wavefront;       /* persistent threads of the trace */
+    uint32_t graph_captures;  /* captures so far */
+    uint32_t pad;
+} CaelixBatchStats;
+CAELIX_API CaelixResult caelix_batch_get_stats(CaelixBatch* batch, CaelixBatchStats* out);
+/* Rays of one view in the newest run (kernel_launches = 1: the shared persistent launch). */
+CAELIX_API CaelixResult caelix_batch_get_view_stats(CaelixBatch* batch, uint32_t view, CaelixRenderStats* out);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,3 +45,33 @@ def test_header_is_c99(tmp_path):
     src.write_text('#include "caelix_b200.h"\nint main(void) { CaelixVersion v; caelix_get_version(&v); return 0; }\n')
     subprocess.run(["gcc", "-std=c99", "-pedantic", "-Wall", "-Werror", "-I", os.path.join(REPO, "include"), "-c",
                     str(src), "-o", str(tmp_path / "abi.o")], check=True)
+
+
+@pytest.mark.skipif(shutil.which("gcc") is None, reason="gcc not available")
+def test_python_structs_match_the_header(tmp_path):
+    """Every ctypes struct of the Python mirror has the C header's size and field offsets."""
+    import caelix_b200
+
+    structs = [v for k, v in vars(caelix_b200).items()
+               if k.startswith("Caelix") and isinstance(v, type) and issubclass(v, ctypes.Structure)]
+    assert any(s.__name__ == "CaelixBatchView" for s in structs)
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "caelix_b200.h"', "int main(void) {"]
+    for s in structs:
+        lines.append(f'printf("{s.__name__} sizeof %zu\\n", sizeof({s.__name__}));')
+        for name, _ in s._fields_:
+            lines.append(f'printf("{s.__name__} {name} %zu\\n", offsetof({s.__name__}, {name}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-I", os.path.join(REPO, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            struct, field, value = line.split()
+            got[(struct, field)] = int(value)
+    for s in structs:
+        assert got[(s.__name__, "sizeof")] == ctypes.sizeof(s), s.__name__
+        for name, _ in s._fields_:
+            assert got[(s.__name__, name)] == getattr(s, name).offset, (s.__name__, name)
