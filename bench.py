@@ -531,6 +531,137 @@ def measure_large(args, world, local, dev, stream, flush):
     return result
 
 
+BATCH_SPP = 2
+BATCH_BOUNCES = 4
+TUNE_CACHE = os.path.join(REPO, "caelix-renderer_b200", "tuning", "batch_tuning.json")
+
+
+def measure_batch(args, world, local, dev, stream):
+    """The batched workload: `--batch-scenes` scenes (brick counts log-uniform in [1k, 500k], 1 %
+    emissive, the plain scene's generator), square viewports uniform among 256, 512, 1024, 2 spp,
+    4 bounces, light-tree NEE. One step = every scene's light-tree rebuild and the trace of every
+    view. Timed three ways on the same scenes, renderers and targets (CUDA events around a step):
+      batched     caelix_batch_run: one CUDA graph launch (parallel light-tree builds, then one
+                  persistent trace launch over all views), launch parameters from the autotuner;
+      sequential  one scene at a time through the plain C ABI: caelix_scene_set_light_options +
+                  caelix_scene_flush (the light-tree rebuild and its status read-back) +
+                  caelix_renderer_render, 64 times;
+      per-view    the batched graph of one view, 64 times (separates the kernel from the batching).
+    The scenes (~10 GB on the device) are larger than L2, so no flush is needed between steps."""
+    import torch
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    sptr = stream.cuda_stream
+    plan = workloads.batch_plan(args.batch_scenes)
+    t0 = time.perf_counter()
+    scenes, renderers, views = [], [], []
+    bricks = lights = 0
+    for i, (count, side) in enumerate(plan):
+        vs = workloads.batch_scene(count, seed=100 + i)
+        scene = caelix_b200.Scene.from_voxel_scene(dev, vs)
+        renderer = caelix_b200.Renderer(dev, scene)
+        out = torch.zeros(side * side * 3, dtype=torch.float32, device="cuda")
+        views.append((renderer, out, side, side, vs.camera, BATCH_BOUNCES, 1 + i, BATCH_SPP))
+        scenes.append(scene)
+        renderers.append(renderer)
+        bricks += vs.brick_count
+        lights += scene.view().light_count
+        del vs
+    setup_s = time.perf_counter() - t0
+    torch.cuda.synchronize()
+
+    def timed(step, steps):
+        total_ms = 0.0
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                step(k)
+                b.record(stream)
+            b.synchronize()
+            total_ms += a.elapsed_time(b)
+        return total_ms / steps
+
+    steps = max(1, min(args.steps, 5))
+    batch = caelix_b200.Batch(dev, views, rebuild_light_trees=True)
+    t0 = time.perf_counter()
+    if args.tuning:
+        batch.set_tuning(**{k: int(v) for k, v in (kv.split("=") for kv in args.tuning.split(","))})
+        tuning = batch.tuning()
+    else:
+        tuning = batch.autotune(args.tune_cache, repeats=2, stream=sptr)
+    tune_s = time.perf_counter() - t0
+    for _ in range(args.warmup):
+        batch.run(sptr)
+    stream.synchronize()
+    barrier(world)
+    with ClockSampler(local) as clocks:
+        batched_ms = timed(lambda k: batch.run(sptr), steps)
+    barrier(world)
+    batched_ms = max_over_ranks(batched_ms, world)
+    st = batch.stats()
+    rays = st.primary_rays + st.bounce_rays + st.shadow_rays
+
+    def sequential(k):
+        for scene, (renderer, out, w, h, cam, bounces, seed, spp) in zip(scenes, views):
+            scene.set_light_options(True)
+            scene.flush(sptr)
+            renderer.render(out, w, h, cam, bounces=bounces, seed=seed, spp=spp, stream=sptr)
+
+    for _ in range(max(1, args.warmup // 2)):
+        sequential(0)
+    stream.synchronize()
+    sequential_ms = max_over_ranks(timed(sequential, steps), world)
+    seq_rays = 0
+    for r in renderers:
+        rs = r.stats()
+        seq_rays += rs.primary_rays + rs.bounce_rays + rs.shadow_rays
+
+    singles = []
+    for v in views:
+        b1 = caelix_b200.Batch(dev, [v], rebuild_light_trees=True)
+        b1.set_tuning(**{k: val for k, val in tuning.as_dict().items()})
+        b1.run(sptr)
+        singles.append(b1)
+    stream.synchronize()
+    per_view_ms = max_over_ranks(timed(lambda k: [b1.run(sptr) for b1 in singles], steps), world)
+    for b1 in singles:
+        b1.close()
+
+    result = {
+        "workload": f"{len(plan)} scenes, brick counts log-uniform in [1k, 500k] (1% emissive), square viewports "
+                    f"uniform among 256/512/1024, {BATCH_SPP} spp, {BATCH_BOUNCES} bounces, light-tree rebuild + "
+                    "trace per scene per step",
+        "scenes": len(plan),
+        "bricks": int(bricks),
+        "light_tree_leaves": int(lights),
+        "pixels": int(sum(v[2] * v[3] for v in views)),
+        "setup_s": setup_s,
+        "autotune_s": tune_s,
+        "tuning": tuning.as_dict(),
+        "graph_kernel_nodes": int(st.kernel_launches),
+        "wavefront": int(st.wavefront),
+        "rays_per_step": int(rays),
+        "sequential_rays_per_step": int(seq_rays),
+        "batched_ms": batched_ms,
+        "sequential_ms": sequential_ms,
+        "per_view_batched_ms": per_view_ms,
+        "speedup_vs_sequential": sequential_ms / batched_ms,
+        "batched_mrays_per_s": world * rays / (batched_ms / 1e3) / 1e6,
+        "sequential_mrays_per_s": world * seq_rays / (sequential_ms / 1e3) / 1e6,
+        "clocks": clocks.summary(),
+    }
+    batch.close()
+    for r in renderers:
+        r.close()
+    for s in scenes:
+        s.close()
+    return result
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -540,6 +671,20 @@ def run_ours(args, world, rank, local):
     dev = caelix_b200.Device(local)
     stream = torch.cuda.Stream()
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    if args.workload == "batch":
+        batch = measure_batch(args, world, local, dev, stream)
+        line = base_line(args, world, "batched trace throughput, Mrays/s (light-tree rebuild + trace of every scene "
+                         "per step)", batch["batched_mrays_per_s"], "Mrays/s", batch["batched_ms"],
+                         {"workload": batch["workload"], "scenes": batch["scenes"], "spp": BATCH_SPP,
+                          "bounces": BATCH_BOUNCES, "l2": "inputs larger than L2 (~10 GB of scenes)",
+                          "parallelism": f"replicas x{world}"})
+        line["batch"] = batch
+        line["gpu_launches"] = args.steps * batch["graph_kernel_nodes"]
+        line["clocks"] = batch["clocks"]
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dev.close()
+        return
     build = None if args.no_build else measure_build(args, world, local, dev, stream, flush, args.records)
     if args.workload == "build":
         line = base_line(args, world, "light-tree build throughput (Mleaves/s)", build["mleaves_per_s"], "Mleaves/s",
@@ -563,6 +708,8 @@ def run_ours(args, world, rank, local):
                                                    "roofline", "roofline_build", "e2e")}
         if args.large:
             line["large"] = measure_large(args, world, local, dev, stream, flush)
+        if args.batch:
+            line["batch"] = measure_batch(args, world, local, dev, stream)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             rays, secs, frames = oracle_trace(10.0, 1)
             line["cpu_baseline"] = {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": 1, "kind": "port",
@@ -579,12 +726,18 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["trace", "build"], default="trace")
+    ap.add_argument("--workload", choices=["trace", "build", "batch"], default="trace")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
     ap.add_argument("--no-build", action="store_true", help="trace workload only: skip the build section")
     ap.add_argument("--large", action=argparse.BooleanOptionalAction, default=True,
                     help="add the large-scene section (2M bricks, 1080p, 4 spp, 6 bounces)")
+    ap.add_argument("--batch", action=argparse.BooleanOptionalAction, default=True,
+                    help="add the batched section (64 scenes: batched graph vs one scene at a time)")
+    ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--tune-cache", default=TUNE_CACHE, help="the autotuner's JSON cache (read, and written on a miss)")
+    ap.add_argument("--tuning", default="", help="fixed batch tuning instead of the autotuner, e.g. "
+                    "min_blocks=8,block_width=8,refill_min=4")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     try:

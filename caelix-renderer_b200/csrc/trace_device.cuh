@@ -281,12 +281,27 @@ __device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], cons
         float tn[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) tn[k] = ((float)((cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
+        // The axis of the nearest boundary (the first of equals), stepped with selects.
         int axis = 0;
-        if (tn[1] < tn[axis]) axis = 1;
-        if (tn[2] < tn[axis]) axis = 2;
-        if (tn[axis] > t_exit) break;
-        cell[axis] += step[axis];
-        if (cell[axis] < 0 || cell[axis] >= (int)s.grid[axis]) break;
+        float t_next = tn[0];
+        if (tn[1] < t_next) {
+            axis = 1;
+            t_next = tn[1];
+        }
+        if (tn[2] < t_next) {
+            axis = 2;
+            t_next = tn[2];
+        }
+        if (t_next > t_exit) break;
+        bool out = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (axis == k) {
+                cell[k] += step[k];
+                out = cell[k] < 0 || cell[k] >= (int)s.grid[k];
+            }
+        }
+        if (out) break;
     }
     return h;
 }
@@ -306,12 +321,20 @@ __device__ __forceinline__ void emitter_cosines(const float dlo[3], const float 
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const float others = all2 - c2[a];
-        c[2 * a] = dhi[a] > 0.0f ? dhi[a] / sqrtf(dhi[a] * dhi[a] + others) : 0.0f;
-        c[2 * a + 1] = dlo[a] < 0.0f ? -dlo[a] / sqrtf(dlo[a] * dlo[a] + others) : 0.0f;
+        // Both quotients for every lane, then the selects (no divergent branch around them).
+        const float ch = dhi[a] / sqrtf(dhi[a] * dhi[a] + others);
+        const float cl = -dlo[a] / sqrtf(dlo[a] * dlo[a] + others);
+        c[2 * a] = dhi[a] > 0.0f ? ch : 0.0f;
+        c[2 * a + 1] = dlo[a] < 0.0f ? cl : 0.0f;
     }
 }
 
-__device__ __noinline__ float importance(const float x[3], const float n[3], const float lo[3], const float hi[3], const float face[6])
+// The importance of a light box for the shading point x with normal n (LtImportance,
+// caelix_light_tree.hlsl:85-155). Branch-free: every operation of the reference's order is
+// computed for every lane and the early exits become selects, so that the lanes of a warp walking
+// the tree stay converged (an early-exit branch would leave the others idle while it runs).
+__device__ __forceinline__ float importance(const float x[3], const float n[3], const float lo[3], const float hi[3],
+                                            const float face[6])
 {
     float dlo[3], dhi[3], c[6];
 #pragma unroll
@@ -323,29 +346,27 @@ __device__ __noinline__ float importance(const float x[3], const float n[3], con
     float e = 0.0f;
 #pragma unroll
     for (int f = 0; f < 6; ++f) e += face[f] * c[f];
-    if (e <= 0.0f) return 0.0f;
     float centre[3], half[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         centre[k] = 0.5f * (lo[k] + hi[k]);
         half[k] = 0.5f * (hi[k] - lo[k]);
     }
-    float cr = 1.0f;
-    if (n[0] != 0.0f || n[1] != 0.0f || n[2] != 0.0f) {
-        const float cx[3] = {centre[0] - x[0], centre[1] - x[1], centre[2] - x[2]};
-        const float an[3] = {fabsf(n[0]), fabsf(n[1]), fabsf(n[2])};
-        const float m = dot3(n, cx) + dot3(an, half);
-        if (m <= 0.0f) return 0.0f;
-        float q[3];
+    const bool has_n = n[0] != 0.0f || n[1] != 0.0f || n[2] != 0.0f;
+    const float cx[3] = {centre[0] - x[0], centre[1] - x[1], centre[2] - x[2]};
+    const float an[3] = {fabsf(n[0]), fabsf(n[1]), fabsf(n[2])};
+    const float m = dot3(n, cx) + dot3(an, half);
+    float q[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) q[k] = hmax(hmax(lo[k] - x[k], x[k] - hi[k]), 0.0f);
-        const float dmin = sqrtf(dot3(q, q));
-        cr = dmin > 0.0f ? hmin(1.0f, m / dmin) : 1.0f;
-    }
+    for (int k = 0; k < 3; ++k) q[k] = hmax(hmax(lo[k] - x[k], x[k] - hi[k]), 0.0f);
+    const float dmin = sqrtf(dot3(q, q));
+    const float ratio = m / dmin;
+    const float cr = has_n ? (dmin > 0.0f ? hmin(1.0f, ratio) : 1.0f) : 1.0f;
     const float tc[3] = {x[0] - centre[0], x[1] - centre[1], x[2] - centre[2]};
     const float extent2 = dot3(half, half);
     const float d2 = hmax(dot3(tc, tc), hmax(1.0f, extent2));
-    return e * cr / d2;
+    const float value = e * cr / d2;
+    return e <= 0.0f ? 0.0f : ((has_n && m <= 0.0f) ? 0.0f : value);
 }
 
 struct Pick
@@ -429,39 +450,35 @@ __device__ __forceinline__ uint32_t child_count(const uint4 c)
     return (c.x != kNone) + (c.y != kNone) + (c.z != kNone) + (c.w != kNone);
 }
 
-__device__ float tree_probability(const SceneView& s, const float x[3], const float n[3], uint32_t target)
+// The probability of picking tree 0 (LtTreeProbability). Tree 1 (dynamic entities) is empty:
+// its box and faces are zero, so its importance and power are never positive and it adds nothing
+// to either sum.
+__device__ float tree_probability(const SceneView& s, const float x[3], const float n[3])
 {
-    float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
-    for (uint32_t k = 0; k < 2; ++k) {
-        Summary sm;
-        uint32_t root;
-        tree_summary(s, k, sm, root);
-        const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
-        const float pw = power6(sm.face);
-        sum_i += imp > 0.0f ? imp : 0.0f;
-        sum_p += pw > 0.0f ? pw : 0.0f;
-        if (k == target) {
-            imp_t = imp;
-            pow_t = pw;
-        }
-    }
-    return pick_probability(sum_i, sum_p, imp_t, pow_t);
+    Summary sm;
+    uint32_t root;
+    tree_summary(s, 0, sm, root);
+    const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
+    const float pw = power6(sm.face);
+    const float sum_i = imp > 0.0f ? imp : 0.0f;
+    const float sum_p = pw > 0.0f ? pw : 0.0f;
+    return pick_probability(sum_i, sum_p, imp, pw);
 }
 
 __device__ float slot_probability(const LightBvhNode* nd, const float x[3], const float n[3], uint32_t slot)
 {
     const uint4 ch = __ldg(reinterpret_cast<const uint4*>(nd->child));
     if (child_count(ch) == 1) return 1.0f;
-    const uint32_t cw[4] = {ch.x, ch.y, ch.z, ch.w};
     float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
     for (uint32_t q = 0; q < 4; ++q) {
-        if (cw[q] == kNone) continue;
         Summary sm;
         node_slot(nd, q, sm);
         const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
         const float pw = power6(sm.face);
-        sum_i += imp > 0.0f ? imp : 0.0f;
-        sum_p += pw > 0.0f ? pw : 0.0f;
+        if (__ldg(&nd->child[q]) != kNone) {
+            sum_i += imp > 0.0f ? imp : 0.0f;
+            sum_p += pw > 0.0f ? pw : 0.0f;
+        }
         if (q == slot) {
             imp_t = imp;
             pow_t = pw;
@@ -481,17 +498,11 @@ __device__ __noinline__ float leaf_probability(const SceneView& s, uint32_t leaf
         const LightBvhNode* nd = s.nodes + node;
         probability *= slot_probability(nd, x, n, slot);
         const uint2 up = __ldg(reinterpret_cast<const uint2*>(&nd->parent));
-        if (up.x == kNone) return probability * tree_probability(s, x, n, 0);
+        if (up.x == kNone) return probability * tree_probability(s, x, n);
         node = up.x;
         slot = up.y;
     }
     return 0.0f;
-}
-
-__device__ __forceinline__ uint32_t family_count(const uint32_t* rec, uint32_t f)
-{
-    const uint32_t word = f < 3 ? __ldg(rec + 10) : __ldg(rec + 11);
-    return (word >> (10 * (f % 3))) & 0x3FFu;
 }
 
 __device__ float family_weights(const SceneView& s, uint32_t group, const uint32_t* rec, const float x[3], float w[6])
@@ -550,45 +561,43 @@ struct LightPoint
 __device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
 {
     float pdf_brick = 1.0f;
-    // The tree (two draws, one per tree).
+    // The tree (one draw per tree; tree 1, dynamic entities, is empty: its importance and power
+    // are never positive, so it only consumes its draw).
     uint32_t root;
     {
         Pick pk = {0, 0, 0, 0, kNone, kNone};
-        uint32_t roots[2];
-        for (uint32_t k = 0; k < 2; ++k) {
-            Summary sm;
-            tree_summary(s, k, sm, roots[k]);
-            pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), k, lt_random_float(rng));
-        }
+        Summary sm;
+        tree_summary(s, 0, sm, root);
+        pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), 0, lt_random_float(rng));
+        (void)lt_random_float(rng);
         float prob;
         const uint32_t k = pick_end(pk, prob);
         if (k == kNone) return false;
-        root = roots[k];
         pdf_brick *= prob;
     }
-    // Down the 4-wide nodes.
+    // Down the 4-wide nodes. Every slot's importance is computed by every lane (empty slots
+    // hold zero summaries and are skipped by the pick), so the lanes stay converged.
     uint32_t leaf = kNone;
     uint32_t node = root;
     for (uint32_t depth = 0; depth < 64; ++depth) {
         const LightBvhNode* nd = s.nodes + node;
         const uint4 ch = __ldg(reinterpret_cast<const uint4*>(nd->child));
-        const uint32_t cw[4] = {ch.x, ch.y, ch.z, ch.w};
         uint32_t chosen;
         if (child_count(ch) == 1) {
             chosen = ch.x;
         } else {
             Pick pk = {0, 0, 0, 0, kNone, kNone};
             for (uint32_t q = 0; q < 4; ++q) {
-                if (cw[q] == kNone) continue;
                 Summary sm;
                 node_slot(nd, q, sm);
-                pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), q, lt_random_float(rng));
+                const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
+                if (__ldg(&nd->child[q]) != kNone) pick_add(pk, imp, power6(sm.face), q, lt_random_float(rng));
             }
             float prob;
             const uint32_t q = pick_end(pk, prob);
             if (q == kNone) return false;
             pdf_brick *= prob;
-            chosen = cw[q];
+            chosen = __ldg(&nd->child[q]);
         }
         if (chosen & kChildLeafBit) {
             leaf = chosen & ~kChildLeafBit;
@@ -620,10 +629,20 @@ __device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], 
         }
     }
     f = f == kNone ? last : f;
-    uint32_t first = 0;
-    for (uint32_t h = 0; h < f; ++h) first += family_count(rec, h);
-    const uint32_t count = family_count(rec, f);
-    if (count == 0 || w[f] <= 0.0f) return false;
+    // The entries of families before f, the count and weight of f (selects, no local array).
+    const uint32_t counts_lo = __ldg(rec + 10), counts_hi = __ldg(rec + 11);
+    uint32_t first = 0, count = 0;
+    float wf = 0.0f;
+#pragma unroll
+    for (uint32_t g = 0; g < 6; ++g) {
+        const uint32_t c = ((g < 3 ? counts_lo : counts_hi) >> (10 * (g % 3))) & 0x3FFu;
+        if (g < f) first += c;
+        if (g == f) {
+            count = c;
+            wf = w[g];
+        }
+    }
+    if (count == 0 || wf <= 0.0f) return false;
     uint32_t ei = (uint32_t)(lt_random_float(rng) * (float)count);
     ei = ei > count - 1u ? count - 1u : ei;
     const uint32_t ent = __ldg(rec + 12 + first + ei);
@@ -634,14 +653,16 @@ __device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], 
                                ((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)};
     const GroupFrame* fr = s.frames + group;
     const uint32_t axis = f >> 1;
-    float local[3];
-#pragma unroll
-    for (int q = 0; q < 3; ++q) local[q] = __ldg(&fr->origin[q]) + (float)voxel[q];
     const float a = lt_random_float(rng);
     const float b = lt_random_float(rng);
-    local[axis] += (f & 1) ? 0.0f : 1.0f;
-    local[(axis + 1) % 3] += a;
-    local[(axis + 2) % 3] += b;
+    // The face's own axis gets the face offset, the next axis a, the one after b.
+    const float off = (f & 1) ? 0.0f : 1.0f;
+    float local[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+        const uint32_t rel = ((uint32_t)q + 3u - axis) % 3u;
+        local[q] = (__ldg(&fr->origin[q]) + (float)voxel[q]) + (rel == 0 ? off : (rel == 1 ? a : b));
+    }
     const float dn[3] = {f == 0 ? 1.0f : (f == 1 ? -1.0f : 0.0f), f == 2 ? 1.0f : (f == 3 ? -1.0f : 0.0f),
                          f == 4 ? 1.0f : (f == 5 ? -1.0f : 0.0f)};
 #pragma unroll
@@ -650,7 +671,7 @@ __device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], 
         p.position[r] = R0 * local[0] + R1 * local[1] + R2 * local[2] + __ldg(&fr->trans[r]);
         p.normal[r] = R0 * dn[0] + R1 * dn[1] + R2 * dn[2];
     }
-    p.pdf = w[f] / sum / (float)count * pdf_brick;
+    p.pdf = wf / sum / (float)count * pdf_brick;
     p.block = ent >> 16;
     return true;
 }
@@ -697,10 +718,19 @@ __device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3
     const uint32_t* rec = block + 4ull * __ldg(block + 4 + 4 * entry + 2);
     float w[6];
     const float sum = family_weights(s, group, rec, x, w);
-    const uint32_t count = family_count(rec, face);
-    if (sum <= 0.0f || w[face] <= 0.0f || count == 0) return false;
-    uint32_t first = 0;
-    for (uint32_t g = 0; g < face; ++g) first += family_count(rec, g);
+    const uint32_t counts_lo = __ldg(rec + 10), counts_hi = __ldg(rec + 11);
+    uint32_t first = 0, count = 0;
+    float wf = 0.0f;
+#pragma unroll
+    for (uint32_t g = 0; g < 6; ++g) {
+        const uint32_t c = ((g < 3 ? counts_lo : counts_hi) >> (10 * (g % 3))) & 0x3FFu;
+        if (g < face) first += c;
+        if (g == face) {
+            count = c;
+            wf = w[g];
+        }
+    }
+    if (sum <= 0.0f || wf <= 0.0f || count == 0) return false;
     const uint32_t vi = (v[0] % 8) | ((v[1] % 8) << 3) | ((v[2] % 8) << 6);
     uint32_t a = 0, b = count;
     bool found = false;
@@ -715,7 +745,7 @@ __device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3
         else b = mid;
     }
     if (!found) return false;
-    in_brick = (w[face] / sum) / (float)count;
+    in_brick = (wf / sum) / (float)count;
     const uint32_t bvh_leaf = __ldg(block + 4 + 4 * entry + 3);
     if (bvh_leaf != kNone) {
         const uint32_t leaf = bvh_leaf & 0x7FFFFFFFu;
