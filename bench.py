@@ -531,6 +531,102 @@ def measure_large(args, world, local, dev, stream, flush):
     return result
 
 
+ADJ_W = ADJ_H = 256
+ADJ_SPP = 8
+ADJ_BOUNCES = 3
+
+
+def measure_adjoint(args, world, local, dev, stream, flush, rank):
+    """The differentiation workload: the solid-brick world of the plain light-tree build (4096 brick
+    records, 32^3 brick grid), 256 x 256, 8 spp, 3 bounces; L2 loss against a target rendered with
+    albedo and power perturbed by up to 10 %. Times caelix_renderer_render (forward) and
+    caelix_renderer_backward (dL/dalbedo 128 x 3 and dL/dpower per brick, path replay) with CUDA
+    events, L2 flushed before each; the CPU baseline is the double-precision adjoint reference
+    (the oracle, all host threads)."""
+    import torch
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    sptr = stream.cuda_stream
+    vs = workloads.solid_brick_scene()
+    scene = caelix_b200.Scene.from_voxel_scene(dev, vs)
+    tscene = caelix_b200.Scene.from_voxel_scene(dev, workloads.perturbed(vs))
+    r = caelix_b200.Renderer(dev, scene)
+    tr = caelix_b200.Renderer(dev, tscene)
+    img = torch.zeros(ADJ_W * ADJ_H * 3, device="cuda")
+    tgt = torch.zeros_like(img)
+    d_alb = torch.zeros(128 * 3, device="cuda")
+    d_pow = torch.zeros(vs.brick_count, device="cuda")
+
+    def forward():
+        r.render(img, ADJ_W, ADJ_H, vs.camera, bounces=ADJ_BOUNCES, seed=1, spp=ADJ_SPP, stream=sptr)
+
+    def backward():
+        r.backward(d_rad, ADJ_W, ADJ_H, vs.camera, d_alb, d_pow, bounces=ADJ_BOUNCES, seed=1, spp=ADJ_SPP,
+                   stream=sptr)
+
+    with torch.cuda.stream(stream):
+        tr.render(tgt, ADJ_W, ADJ_H, vs.camera, bounces=ADJ_BOUNCES, seed=1, spp=ADJ_SPP, stream=sptr)
+        forward()
+        d_rad = 2.0 * (img - tgt)
+    stream.synchronize()
+
+    def timed(fn, steps):
+        total = 0.0
+        for _ in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                fn()
+                b.record(stream)
+            b.synchronize()
+            total += a.elapsed_time(b)
+        return total / steps
+
+    for _ in range(args.warmup):
+        forward()
+        backward()
+    stream.synchronize()
+    steps = max(1, min(args.steps, 10))
+    fwd_ms = max_over_ranks(timed(forward, steps), world)
+    st = r.stats()
+    fwd_rays = st.primary_rays + st.bounce_rays + st.shadow_rays
+    bwd_ms = max_over_ranks(timed(backward, steps), world)
+    result = {
+        "workload": f"solid-brick world of the 4096-record build (32^3 bricks), {ADJ_W}x{ADJ_H}, {ADJ_SPP} spp, "
+                    f"{ADJ_BOUNCES} bounces, L2 loss vs a target with albedo/power perturbed by up to 10%; "
+                    "gradients w.r.t. 64x3 material albedo and per-brick power (path replay, sampling held fixed)",
+        "bricks": int(vs.brick_count),
+        "forward_ms": fwd_ms,
+        "backward_ms": bwd_ms,
+        "adjoint_over_forward": bwd_ms / fwd_ms,
+        "forward_mrays_per_s": fwd_rays / (fwd_ms / 1e3) / 1e6,
+        "parity": "tests/test_adjoint_gpu.py: vs the double-precision reference and central differences (1e-3)",
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        import oracle_lib
+
+        osc = oracle_lib.OracleScene(oracle_lib.load(), vs)
+        threads = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        osc.adjoint(ADJ_W, ADJ_H, spp=ADJ_SPP, bounces=ADJ_BOUNCES, seed=1, d_radiance=d_rad.cpu().numpy(),
+                    threads=threads)
+        cpu_s = time.perf_counter() - t0
+        osc.close()
+        result["cpu_baseline"] = {"value": cpu_s * 1e3, "unit": "ms", "cores": threads, "kind": "port",
+                                  "sample": "one double-precision adjoint of the whole frame (oracle oc_adjoint), "
+                                            f"{threads} threads"}
+    r.close()
+    tr.close()
+    scene.close()
+    tscene.close()
+    return result
+
+
 BATCH_SPP = 2
 BATCH_BOUNCES = 4
 TUNE_CACHE = os.path.join(REPO, "caelix-renderer_b200", "tuning", "batch_tuning.json")
@@ -708,6 +804,8 @@ def run_ours(args, world, rank, local):
                                                    "roofline", "roofline_build", "e2e")}
         if args.large:
             line["large"] = measure_large(args, world, local, dev, stream, flush)
+        if args.adjoint:
+            line["adjoint"] = measure_adjoint(args, world, local, dev, stream, flush, rank)
         if args.batch:
             line["batch"] = measure_batch(args, world, local, dev, stream)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -735,6 +833,8 @@ def main():
     ap.add_argument("--batch", action=argparse.BooleanOptionalAction, default=True,
                     help="add the batched section (64 scenes: batched graph vs one scene at a time)")
     ap.add_argument("--batch-scenes", type=int, default=64)
+    ap.add_argument("--adjoint", action=argparse.BooleanOptionalAction, default=True,
+                    help="add the differentiation section (forward vs backward time)")
     ap.add_argument("--tune-cache", default=TUNE_CACHE, help="the autotuner's JSON cache (read, and written on a miss)")
     ap.add_argument("--tuning", default="", help="fixed batch tuning instead of the autotuner, e.g. "
                     "min_blocks=8,block_width=8,refill_min=4")

@@ -354,6 +354,9 @@ def _bind_scene(L):
                                    C.POINTER(CaelixCamera), C.POINTER(CaelixRenderOptions)],
         "caelix_renderer_set_light_nee_options": [vp, C.POINTER(CaelixLightNeeOptions)],
         "caelix_renderer_get_stats": [vp, C.POINTER(CaelixRenderStats)],
+        "caelix_renderer_backward": [vp, C.POINTER(CaelixFrameDesc), C.POINTER(CaelixRenderTargets),
+                                     C.POINTER(CaelixCamera), C.POINTER(CaelixRenderOptions), C.c_uint64, C.c_uint64,
+                                     C.c_uint64],
     }
     for name, args in proto.items():
         f = getattr(L, name)
@@ -507,6 +510,20 @@ class Renderer:
         o = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
         self.L.check(self.L.lib.caelix_renderer_render(self.handle, C.byref(fd), C.byref(t), C.byref(cam), C.byref(o)),
                      "caelix_renderer_render")
+
+    def backward(self, d_radiance, width: int, height: int, camera, d_albedo, d_power, bounces: int = 4,
+                 seed: int = 1, spp: int = 1, image=None, stream: int = 0):
+        """caelix_renderer_backward: d_radiance = dL/d(radiance) (device, height x width x 3); writes
+        dL/dalbedo into d_albedo (device, 128 x 3) and dL/dpower into d_power (device, one per brick
+        in the scene's order); image (device, optional) receives the forward radiance."""
+        self.frame += 1
+        fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
+        t = CaelixRenderTargets(_ptr(image) if image is not None else 0, width, height)
+        cam = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
+        o = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+        self.L.check(self.L.lib.caelix_renderer_backward(self.handle, C.byref(fd), C.byref(t), C.byref(cam),
+                                                         C.byref(o), _ptr(d_radiance), _ptr(d_albedo),
+                                                         _ptr(d_power)), "caelix_renderer_backward")
 
     def stats(self) -> CaelixRenderStats:
         s = CaelixRenderStats()

@@ -360,3 +360,39 @@ def batch_scene(bricks: int, seed: int, occupancy: float = 0.30, emissive_fracti
     return noise_world_large(grid_bricks=(side, side, side), occupied_bricks=bricks, voxel_fill=0.5,
                              emissive_bricks=max(1, int(round(emissive_fraction * bricks))), seed=seed,
                              brick_scale=0.25, voxel_scale=0.25, camera=camera)
+
+
+def solid_brick_scene(n: int = 4096, grid_bricks: int = 32, seed: int = 1, stream: int = 1) -> VoxelScene:
+    """The plain light-tree build's bricks as a voxel world (the differentiation scene): brick
+    coordinates and powers from brick_light_records' PCG32 stream (uniform in [0, grid_bricks)^3,
+    power log-normal(0, 1); a repeated coordinate keeps its first draw), every brick solid (AABB =
+    the brick), voxel materials uniform in [1, 64] (PCG32 stream 2), every brick emissive, albedo
+    uniform in [0.1, 0.9] per material and channel (stream 5); bricks in increasing linear index;
+    a camera looking into the grid, aspect 1."""
+    rng = Pcg32(seed, stream)
+    bits = int(grid_bricks).bit_length() - 1
+    assert 1 << bits == grid_bricks, "grid_bricks must be a power of two"
+    coords = (rng.next_u32(3 * n).reshape(n, 3) >> np.uint32(32 - bits)).astype(np.int64)
+    power = rng.lognormal(n)
+    lin = coords[:, 0] + grid_bricks * (coords[:, 1] + grid_bricks * coords[:, 2])
+    _, first = np.unique(lin, return_index=True)  # sorted by linear index, first occurrence of each
+    keys = coords[first].astype(np.int32)
+    power = power[first].astype(np.float32)
+    m = len(keys)
+    mat = Pcg32(seed, 2).next_u32(m * 512).reshape(m, 512)
+    voxels = (np.uint16(0x8000) | (np.uint32(1) + (mat >> np.uint32(26))).astype(np.uint16)).astype(np.uint16)
+    albedo = np.zeros((128, 3), np.float32)
+    albedo[1:65] = (0.1 + 0.8 * Pcg32(seed, 5).next_doubles(64 * 3)).reshape(64, 3).astype(np.float32)
+    world = np.array([grid_bricks] * 3, np.float64) * 8
+    camera = look_at(np.array([-0.25, 1.2, -0.35]) * world, world * np.array([0.5, 0.35, 0.5]))
+    return VoxelScene((grid_bricks,) * 3, keys, voxels, power, albedo, camera)
+
+
+def perturbed(vs: VoxelScene, seed: int = 7, amount: float = 0.10) -> VoxelScene:
+    """The same world with albedo and power each scaled by (1 + amount * u), u uniform in [-1, 1]
+    (PCG32 streams 21 and 22 of `seed`): the target of the differentiation workload."""
+    ua = 2.0 * Pcg32(seed, 21).next_doubles(vs.albedo.size).reshape(vs.albedo.shape) - 1.0
+    up = 2.0 * Pcg32(seed, 22).next_doubles(len(vs.power)) - 1.0
+    albedo = (vs.albedo * (1.0 + amount * ua)).astype(np.float32)
+    power = (vs.power * (1.0 + amount * up)).astype(np.float32)
+    return VoxelScene(vs.grid, vs.keys, vs.voxels, power, albedo, vs.camera, vs.group_shift)

@@ -388,6 +388,39 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
     CAELIX_GUARD_END
 }
 
+CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const CaelixFrameDesc* frame,
+                                                 const CaelixRenderTargets* targets, const CaelixCamera* camera,
+                                                 const CaelixRenderOptions* options, const float* d_radiance,
+                                                 float* d_albedo, float* d_power)
+{
+    CAELIX_GUARD_BEGIN
+    if (!renderer || !frame || !d_radiance || !d_albedo || !d_power) return CAELIX_ERROR_INVALID_ARGUMENT;
+    cx::TraceParams p;
+    // The forward image is optional here: a zero radiance pointer passes the target checks with a
+    // stand-in and is not written.
+    CaelixRenderTargets t = targets ? *targets : CaelixRenderTargets{0, 0, 0};
+    const uint64_t image = t.radiance;
+    if (!t.radiance) t.radiance = 1;
+    const CaelixResult r = render_params(renderer, &t, camera, options, "caelix_renderer_backward", &p);
+    if (r != CAELIX_OK) return r;
+    CaelixScene* scene = renderer->scene;
+    cudaSetDevice(renderer->device->ordinal);
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
+    cudaError_t e = cudaMemsetAsync(d_albedo, 0, sizeof(float) * cx::kMaterialSlots * 3, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d_power, 0, sizeof(float) * std::max(scene->dev.brick_count, 1u), stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_backward");
+    cudaEventRecord(renderer->start, stream);
+    e = cx::adjoint_launch(cx::scene_view(scene->dev), p, d_radiance, reinterpret_cast<float*>(image), d_albedo,
+                           d_power, renderer->counts, stream);
+    cudaEventRecord(renderer->stop, stream);
+    renderer->last_stream = stream;
+    renderer->frame_number = frame->frame_number;
+    renderer->rendered = true;
+    return cx::cuda_result(e, "caelix_renderer_backward");
+    CAELIX_GUARD_END
+}
+
 CAELIX_API CaelixResult caelix_renderer_set_light_nee_options(CaelixRenderer* renderer, const CaelixLightNeeOptions* options)
 {
     if (!renderer || !options || options->enabled > 1 || options->flags != 0 || options->reserved != 0 ||

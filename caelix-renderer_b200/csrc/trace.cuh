@@ -31,6 +31,12 @@ struct TraceParams
 cudaError_t trace_launch(const SceneView& s, const TraceParams& p, float* radiance, unsigned long long* ray_counts,
                          cudaStream_t stream);
 
+// The adjoint of trace_launch (backward.cu): d_radiance = dL/d(radiance), width * height RGB;
+// d_albedo (kMaterialSlots x 3) and d_power (one per brick, the scene's order) are accumulated
+// into (zero them first); image (may be null) receives the forward radiance.
+cudaError_t adjoint_launch(const SceneView& s, const TraceParams& p, const float* d_radiance, float* image,
+                           float* d_albedo, float* d_power, unsigned long long* ray_counts, cudaStream_t stream);
+
 // ---- the batched persistent trace (trace_batch.cu) ----
 
 constexpr uint32_t kMaxBatchViews = 256;  // views of one persistent launch

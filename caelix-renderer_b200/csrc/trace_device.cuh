@@ -794,7 +794,9 @@ struct ShadowRay
 {
     float dir[3];
     float t_max;
-    float value;  // the contribution on every channel if the ray is unoccluded
+    float value;       // the contribution on every channel if the ray is unoccluded
+    float dvalue_de;   // d value / d (the lamp brick's power), the sampling factors held fixed
+    uint32_t brick;    // the lamp brick (kNone when its emission is not its power)
 };
 
 __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng,
@@ -827,7 +829,10 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
     r.dir[1] = w[1];
     r.dir[2] = w[2];
     r.t_max = t_max;
-    r.value = contribution * (w_sum / w_lamp);
+    const float k = w_sum / w_lamp;
+    r.value = contribution * k;
+    r.dvalue_de = scale * k;
+    r.brick = (p.block & kOpaqueBit) ? brick : kNone;
     return true;
 }
 

@@ -485,6 +485,22 @@ typedef struct CaelixRenderStats
 } CaelixRenderStats;
 CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, CaelixRenderStats* out);
 
+/* New (no reference counterpart): the adjoint of caelix_renderer_render for an image loss L.
+   d_radiance: device float[height][width][3], dL/d(radiance) of the frame the same renderer,
+   target size, camera and options render. Writes (after zeroing them) the gradients of L with
+   respect to the albedo of every material, d_albedo: device float[128][3] (row = material id,
+   value & 0x7F), and to the emitter power of every brick, d_power: device float[brick_count] in
+   the scene's brick order (the keys of caelix_scene_get_view: increasing linear brick index).
+   Sampling quantities (pdfs, MIS weights, Russian-roulette probabilities, discrete decisions) are
+   held fixed; each path is traced again (path replay), nothing of it is stored. When
+   targets->radiance is not 0 it also receives the forward radiance (bit-identical to
+   caelix_renderer_render). Asynchronous on frame->command_buffer; rays and timings through
+   caelix_renderer_get_stats / caelix_renderer_get_gpu_timings. */
+CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const CaelixFrameDesc* frame,
+                                                 const CaelixRenderTargets* targets, const CaelixCamera* camera,
+                                                 const CaelixRenderOptions* options, const float* d_radiance,
+                                                 float* d_albedo, float* d_power);
+
 /* ---------------------------------------------------------------------------
  * Batch: many scenes and viewports in one CUDA graph launch
  *

@@ -208,6 +208,14 @@ oc_hit oc_trace_ray(const oc_scene* s, const float origin[3], const float dir[3]
 void oc_render(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
                const oc_camera* cam, const oc_render_desc* r, float* radiance, uint64_t* rays, int threads);
 
+/* The adjoint reference (double precision): the estimator with the sampling quantities of the
+ * fp32 render at (albedo, power) held fixed, evaluated at (A, P) (double; NULL = the fp32
+ * parameters). image (may be NULL): the double image. d_radiance (may be NULL): dL/d(pixel);
+ * then d_albedo [128][3] and d_power [brick_count] receive dL/dA and dL/dP at (A, P). */
+void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
+                const oc_camera* cam, const oc_render_desc* r, const double* A, const double* P,
+                const float* d_radiance, double* image, double* d_albedo, double* d_power, int threads);
+
 /* Light tree draw for a point receiver (caelix_light_tree.hlsl:749-767): returns 1 and fills
  * out[0..2] position, out[3..5] normal, out[6] pdf, words[0..4] block, voxel, face, group, entry. */
 int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t rng,

@@ -728,9 +728,12 @@ static void emission_of(const ctx* c, uint32_t record, uint32_t block, float e[3
 }
 
 /* NextEventAtVertex without the sun: the lamp candidate and its shadow ray. */
-static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* light_rng, float out[3])
+static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* light_rng, float out[3],
+                       uint32_t* lamp_brick, float* dvalue)
 {
     out[0] = out[1] = out[2] = 0.0f;
+    *lamp_brick = OC_NONE;
+    *dvalue = 0.0f;
     const uint32_t point_seed = random_u32(light_rng);
     float p[7];
     uint32_t words[5];
@@ -766,6 +769,11 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
     if (t_max > 0.0f && !occluded) {
         const float k = w_sum / w_lamp;
         for (int q = 0; q < 3; ++q) out[q] = contribution[q] * k;
+        /* For the adjoint: the contribution is the lamp brick's power times scale * k. */
+        if (words[0] & OPAQUE) {
+            *lamp_brick = brick;
+            *dvalue = scale * k;
+        }
     }
 }
 
@@ -810,8 +818,45 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
     for (int k = 0; k < 3; ++k) origin[k] = (ray_o[k] + ray_d[k] * h->t) + PUSH_OFF * h->normal[k];
 }
 
-static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float rgb[3])
+/* ---- the path record of the adjoint reference ----
+ * The events of one path sample in order, as the estimator gathers them: an emitter hit adds
+ * power[brick] * factor * throughput, an NEE lamp adds power[brick] * factor * throughput, a
+ * bounce vertex multiplies the throughput by the albedo of its material, a Russian-roulette
+ * survival by factor (1 / cp). The factors are the sampling quantities of the fp32 forward pass
+ * (MIS weights, geometry / pdf terms, RR probabilities), held fixed by the adjoint. */
+enum { EV_EMIT = 0, EV_ALBEDO = 1, EV_NEE = 2, EV_RR = 3 };
+#define MAX_EVENTS 64
+
+typedef struct path_event {
+    uint32_t kind;
+    uint32_t index; /* brick (EMIT, NEE) or material (ALBEDO) */
+    float factor;
+} path_event;
+
+typedef struct path_rec {
+    int hit;
+    int emits0;         /* the primary emission is power[record0] */
+    uint32_t material0; /* the primary albedo row */
+    uint32_t record0;
+    int bad;            /* the fp32 radiance was not finite (the sample's radiance part is 0) */
+    float radiance[3];  /* the fp32 radiance of the sample */
+    uint32_t n;
+    path_event ev[MAX_EVENTS];
+} path_rec;
+
+static void rec_event(path_rec* rec, uint32_t kind, uint32_t index, float factor)
 {
+    if (rec && rec->n < MAX_EVENTS) {
+        rec->ev[rec->n].kind = kind;
+        rec->ev[rec->n].index = index;
+        rec->ev[rec->n].factor = factor;
+        rec->n++;
+    }
+}
+
+static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float rgb[3], path_rec* rec)
+{
+    if (rec) memset(rec, 0, sizeof(*rec));
     const oc_camera* cam = c->cam;
     const oc_render_desc* r = c->r;
     rgb[0] = rgb[1] = rgb[2] = 0.0f;
@@ -832,15 +877,24 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     uint32_t light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
     float a0[3], e0[3], org[3], dir[3];
     shade(c, &primary, cam->position, d, &rng, a0, e0, org, dir);
+    if (rec) {
+        const uint32_t block0 = (primary.attrib >> 16) & 0xFFFFu;
+        rec->hit = 1;
+        rec->emits0 = (block0 & OPAQUE) != 0;
+        rec->material0 = block0 & 0x7Fu;
+        rec->record0 = primary.record;
+    }
     float seg_n[3];
     memcpy(seg_n, primary.normal, sizeof(seg_n));
     float radiance[3] = {0, 0, 0};
     float throughput[3] = {1.0f / hmax(0.001f, 1.0f), 1.0f / hmax(0.001f, 1.0f), 1.0f / hmax(0.001f, 1.0f)};
     uint32_t segment_light = 0;
     if (r->light_nee && r->bounce_count >= 1) {
-        float nee[3];
-        next_event(c, org, primary.normal, &light_rng, nee);
+        float nee[3], dv;
+        uint32_t lamp;
+        next_event(c, org, primary.normal, &light_rng, nee, &lamp, &dv);
         for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * throughput[k];
+        if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, dv);
         segment_light = 3u; /* lamp NEE with MIS */
     }
     uint32_t bounce_index = 1;
@@ -855,16 +909,22 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
         if (segment_light != 0u && (em[0] > 0.0f || em[1] > 0.0f || em[2] > 0.0f))
             ew = lamp_hit_weight(c, segment_light, &h, org, dir, seg_n);
         for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
+        const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
+        if (block & OPAQUE) rec_event(rec, EV_EMIT, h.record, ew);
+        rec_event(rec, EV_ALBEDO, block & 0x7Fu, 0.0f);
         for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
         segment_light = 0u;
         if (r->light_nee && bounce_index <= r->bounce_count) {
             segment_light = 3u;
-            float nee[3];
-            next_event(c, o2, h.normal, &light_rng, nee);
+            float nee[3], dv;
+            uint32_t lamp;
+            next_event(c, o2, h.normal, &light_rng, nee, &lamp, &dv);
             for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * (throughput[k] * (1.0f / 1.0f));
+            if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, dv);
         }
         const float cp = hmax(throughput[0], hmax(throughput[1], throughput[2]));
         if (cp <= 0.0f || cp < random01(&rng)) break;
+        rec_event(rec, EV_RR, 0, 1.0f / cp);
         for (int k = 0; k < 3; ++k) throughput[k] *= 1.0f / cp;
         memcpy(org, o2, sizeof(org));
         memcpy(dir, d2, sizeof(dir));
@@ -876,6 +936,10 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     for (int k = 0; k < 3; ++k) {
         const float sr = hmin(bad ? 0.0f : radiance[k], 65504.0f);
         rgb[k] = e0[k] + a0[k] * sr;
+    }
+    if (rec) {
+        rec->bad = bad;
+        memcpy(rec->radiance, radiance, sizeof(radiance));
     }
 }
 
@@ -896,7 +960,7 @@ static void* run_rows(void* arg)
             float acc[3] = {0, 0, 0};
             for (uint32_t s = 0; s < r->spp; ++s) {
                 float rgb[3];
-                trace_pixel(&local, x, y, r->frame_seed + s, rgb);
+                trace_pixel(&local, x, y, r->frame_seed + s, rgb, NULL);
                 for (int k = 0; k < 3; ++k) acc[k] += rgb[k];
             }
             float* out = local.radiance + 3ull * ((uint64_t)y * r->width + x);
@@ -928,4 +992,167 @@ void oc_render(const oc_scene* s, const oc_light_tree* t, const float* albedo, c
     }
     free(jobs);
     free(tids);
+}
+
+/* ---- the adjoint reference (double precision) ----
+ * The adjoint of the estimator with its sampling quantities held fixed (the factors of the path
+ * record): a sample is then a polynomial in the albedo table A and the brick powers P,
+ *   rgb = E0 + A0 * sanitize(R),  R = sum over the emission events of P[brick] * factor * T,
+ * T the product of the albedo and RR factors before the event. The fp32 forward pass (the
+ * oracle's trace_pixel, bit-exact with the CUDA path) fixes the path and its factors; the sample
+ * is then evaluated and differentiated in double: forward over the events for the throughputs,
+ * backward over them for dL/dT (reverse accumulation, no difference of partial sums). sanitize
+ * keeps the fp32 decisions: a non-finite fp32 radiance gives 0, a channel above 65504 gives the
+ * constant 65504. */
+
+typedef struct adj_job {
+    const ctx* c;
+    uint32_t y_begin, y_end;
+    const double* A;        /* evaluation albedo [128][3] */
+    const double* P;        /* evaluation power [brick_count] */
+    const float* d_radiance; /* dL/d(pixel) (gradient mode) */
+    double* image;          /* evaluation mode: the double image */
+    double* dA;             /* gradient mode: this job's albedo gradient [128][3] */
+    double* dP;             /* gradient mode: this job's power gradient [brick_count] */
+} adj_job;
+
+static void eval_sample(const path_rec* rec, const double* A, const double* P, double rgb[3], double T_before[][3],
+                        double R[3])
+{
+    double T[3] = {1.0, 1.0, 1.0};
+    R[0] = R[1] = R[2] = 0.0;
+    for (uint32_t i = 0; i < rec->n; ++i) {
+        const path_event* e = &rec->ev[i];
+        for (int k = 0; k < 3; ++k) T_before[i][k] = T[k];
+        if (e->kind == EV_EMIT || e->kind == EV_NEE) {
+            for (int k = 0; k < 3; ++k) R[k] += P[e->index] * (double)e->factor * T[k];
+        } else if (e->kind == EV_ALBEDO) {
+            for (int k = 0; k < 3; ++k) T[k] *= A[3 * e->index + k];
+        } else {
+            for (int k = 0; k < 3; ++k) T[k] *= (double)e->factor;
+        }
+    }
+    const double e0 = rec->emits0 ? P[rec->record0] : 0.0;
+    for (int k = 0; k < 3; ++k) {
+        const double sr = rec->bad ? 0.0 : (rec->radiance[k] > 65504.0f ? 65504.0 : R[k]);
+        rgb[k] = e0 + A[3 * rec->material0 + k] * sr;
+    }
+}
+
+static void* run_adjoint_rows(void* arg)
+{
+    adj_job* j = (adj_job*)arg;
+    ctx local = *j->c;
+    const oc_render_desc* r = local.r;
+    path_rec* rec = (path_rec*)malloc(sizeof(path_rec));
+    double (*T_before)[3] = (double (*)[3])malloc(sizeof(double) * 3 * MAX_EVENTS);
+    for (uint32_t y = j->y_begin; y < j->y_end; ++y)
+        for (uint32_t x = r->x0; x < r->x1; ++x) {
+            const uint64_t pix = (uint64_t)y * r->width + x;
+            double acc[3] = {0, 0, 0};
+            for (uint32_t s = 0; s < r->spp; ++s) {
+                float rgb32[3];
+                trace_pixel(&local, x, y, r->frame_seed + s, rgb32, rec);
+                if (!rec->hit) continue;
+                double rgb[3], R[3];
+                eval_sample(rec, j->A, j->P, rgb, T_before, R);
+                for (int k = 0; k < 3; ++k) acc[k] += rgb[k];
+                if (!j->dA) continue;
+                double g[3], G[3];
+                for (int k = 0; k < 3; ++k) g[k] = (double)j->d_radiance[3 * pix + k] / (double)r->spp;
+                const double* a0 = j->A + 3 * rec->material0;
+                for (int k = 0; k < 3; ++k) {
+                    const int pass = !rec->bad && !(rec->radiance[k] > 65504.0f);
+                    const double sr = rec->bad ? 0.0 : (pass ? R[k] : 65504.0);
+                    j->dA[3 * rec->material0 + k] += g[k] * sr;
+                    G[k] = pass ? g[k] * a0[k] : 0.0;
+                }
+                if (rec->emits0) j->dP[rec->record0] += g[0] + g[1] + g[2];
+                /* Backward over the events: lambda = dL/dT after the event. */
+                double lambda[3] = {0, 0, 0};
+                for (int32_t i = (int32_t)rec->n - 1; i >= 0; --i) {
+                    const path_event* e = &rec->ev[i];
+                    const double* T = T_before[i];
+                    if (e->kind == EV_EMIT || e->kind == EV_NEE) {
+                        const double f = (double)e->factor;
+                        j->dP[e->index] += (G[0] * T[0] + G[1] * T[1] + G[2] * T[2]) * f;
+                        for (int k = 0; k < 3; ++k) lambda[k] += G[k] * j->P[e->index] * f;
+                    } else if (e->kind == EV_ALBEDO) {
+                        for (int k = 0; k < 3; ++k) {
+                            j->dA[3 * e->index + k] += lambda[k] * T[k];
+                            lambda[k] *= j->A[3 * e->index + k];
+                        }
+                    } else {
+                        for (int k = 0; k < 3; ++k) lambda[k] *= (double)e->factor;
+                    }
+                }
+            }
+            if (j->image)
+                for (int k = 0; k < 3; ++k) j->image[3 * pix + k] = acc[k] / (double)r->spp;
+        }
+    free(rec);
+    free(T_before);
+    return NULL;
+}
+
+/* The frozen estimator (image, double) and/or its gradient. The paths and their sampling
+ * quantities are those of the fp32 render at (albedo, power); the estimator is evaluated at
+ * (A, P) (double; NULL = the fp32 parameters). d_radiance (may be NULL) = dL/d(pixel): then
+ * d_albedo [128][3] and d_power [brick_count] receive dL/dA and dL/dP at (A, P). image (may be
+ * NULL) receives the image at (A, P). Per-thread partial gradients are summed in thread order. */
+void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
+                const oc_camera* cam, const oc_render_desc* r, const double* A, const double* P,
+                const float* d_radiance, double* image, double* d_albedo, double* d_power, int threads)
+{
+    ctx c = {s, t, albedo, power, cam, r, NULL, {0, 0, 0}};
+    double* a_own = NULL;
+    double* p_own = NULL;
+    if (!A) {
+        a_own = (double*)malloc(sizeof(double) * 128 * 3);
+        for (int i = 0; i < 128 * 3; ++i) a_own[i] = albedo[i];
+        A = a_own;
+    }
+    if (!P) {
+        p_own = (double*)malloc(sizeof(double) * (s->brick_count ? s->brick_count : 1));
+        for (uint32_t i = 0; i < s->brick_count; ++i) p_own[i] = power[i];
+        P = p_own;
+    }
+    if (threads < 1) threads = 1;
+    const uint32_t rows = r->y1 - r->y0;
+    if ((uint32_t)threads > rows) threads = (int)(rows ? rows : 1);
+    adj_job* jobs = (adj_job*)calloc((size_t)threads, sizeof(adj_job));
+    pthread_t* tids = (pthread_t*)calloc((size_t)threads, sizeof(pthread_t));
+    const size_t nb = s->brick_count ? s->brick_count : 1;
+    for (int i = 0; i < threads; ++i) {
+        jobs[i].c = &c;
+        jobs[i].y_begin = r->y0 + (uint32_t)((uint64_t)rows * i / threads);
+        jobs[i].y_end = r->y0 + (uint32_t)((uint64_t)rows * (i + 1) / threads);
+        jobs[i].A = A;
+        jobs[i].P = P;
+        jobs[i].d_radiance = d_radiance;
+        jobs[i].image = image;
+        if (d_radiance) {
+            jobs[i].dA = (double*)calloc(128 * 3, sizeof(double));
+            jobs[i].dP = (double*)calloc(nb, sizeof(double));
+        }
+        if (threads == 1) run_adjoint_rows(&jobs[i]);
+        else pthread_create(&tids[i], NULL, run_adjoint_rows, &jobs[i]);
+    }
+    if (d_radiance) {
+        memset(d_albedo, 0, sizeof(double) * 128 * 3);
+        memset(d_power, 0, sizeof(double) * nb);
+    }
+    for (int i = 0; i < threads; ++i) {
+        if (threads > 1) pthread_join(tids[i], NULL);
+        if (d_radiance) {
+            for (int q = 0; q < 128 * 3; ++q) d_albedo[q] += jobs[i].dA[q];
+            for (size_t q = 0; q < nb; ++q) d_power[q] += jobs[i].dP[q];
+            free(jobs[i].dA);
+            free(jobs[i].dP);
+        }
+    }
+    free(jobs);
+    free(tids);
+    free(a_own);
+    free(p_own);
 }

@@ -130,6 +130,10 @@ def _bind_scene(lib):
     lib.oc_render.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.POINTER(Camera),
                               C.POINTER(RenderDesc), C.c_void_p, C.c_void_p, C.c_int]
     lib.oc_render.restype = None
+    lib.oc_adjoint.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.POINTER(Camera),
+                               C.POINTER(RenderDesc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                               C.c_void_p, C.c_int]
+    lib.oc_adjoint.restype = None
     lib.oc_light_sample.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
                                     C.c_void_p, C.c_void_p]
     lib.oc_light_sample.restype = C.c_int
@@ -210,6 +214,35 @@ class OracleScene:
         self.lib.oc_render(C.byref(self.s), C.byref(self.lt), self.src.albedo.ctypes.data, self.src.power.ctypes.data,
                            C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data, threads)
         return out, rays
+
+
+    def adjoint(self, width, height, spp=1, bounces=4, seed=1, d_radiance=None, A=None, P=None, threads=8):
+        """The double-precision adjoint reference (oc_adjoint): the frozen estimator's image at
+        (A, P) (None: the scene's own fp32 parameters) and, with d_radiance = dL/d(pixel), the
+        gradients dL/dalbedo [128][3] and dL/dpower [brick_count]."""
+        cam = self.src.camera
+        c = Camera((C.c_float * 3)(*cam["position"]), (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]),
+                   (C.c_float * 3)(*cam["forward"]), float(cam["tan_half_fov_y"]), float(cam["aspect"]))
+        r = RenderDesc(width, height, spp, bounces, seed, 1, 0, 0, width, height)
+        nb = max(self.s.brick_count, 1)
+        image = np.zeros((height, width, 3), np.float64)
+        dA = np.zeros((128, 3), np.float64)
+        dP = np.zeros(nb, np.float64)
+        a_ptr = p_ptr = None
+        if A is not None:
+            A = np.ascontiguousarray(A, np.float64)
+            a_ptr = A.ctypes.data
+        if P is not None:
+            P = np.ascontiguousarray(P, np.float64)
+            p_ptr = P.ctypes.data
+        g_ptr = None
+        if d_radiance is not None:
+            d_radiance = np.ascontiguousarray(d_radiance, np.float32)
+            g_ptr = d_radiance.ctypes.data
+        self.lib.oc_adjoint(C.byref(self.s), C.byref(self.lt), self.src.albedo.ctypes.data, self.src.power.ctypes.data,
+                            C.byref(c), C.byref(r), a_ptr, p_ptr, g_ptr, image.ctypes.data, dA.ctypes.data,
+                            dP.ctypes.data, threads)
+        return image, dA, dP[: self.s.brick_count]
 
 
 def RECORD_DTYPE_LOCAL():
