@@ -354,6 +354,7 @@ def _bind_scene(L):
                                    C.POINTER(CaelixCamera), C.POINTER(CaelixRenderOptions)],
         "caelix_renderer_set_light_nee_options": [vp, C.POINTER(CaelixLightNeeOptions)],
         "caelix_renderer_get_stats": [vp, C.POINTER(CaelixRenderStats)],
+        "caelix_renderer_set_trace_mode": [vp, C.c_uint32, C.c_uint32],
         "caelix_renderer_backward": [vp, C.POINTER(CaelixFrameDesc), C.POINTER(CaelixRenderTargets),
                                      C.POINTER(CaelixCamera), C.POINTER(CaelixRenderOptions), C.c_uint64, C.c_uint64,
                                      C.c_uint64],
@@ -496,6 +497,15 @@ class Renderer:
         except Exception:
             pass
 
+    TRACE_WAVEFRONT = 0
+    TRACE_MEGAKERNEL = 1
+
+    def set_trace_mode(self, mode: int, wave_capacity: int = 0):
+        """caelix_renderer_set_trace_mode: TRACE_WAVEFRONT (default; wave_capacity bounds the paths in
+        flight, 0 = one per pixel) or TRACE_MEGAKERNEL."""
+        self.L.check(self.L.lib.caelix_renderer_set_trace_mode(self.handle, mode, wave_capacity),
+                     "caelix_renderer_set_trace_mode")
+
     def set_light_nee(self, enabled: bool):
         o = CaelixLightNeeOptions(1 if enabled else 0, 0, 0, 0)
         self.L.check(self.L.lib.caelix_renderer_set_light_nee_options(self.handle, C.byref(o)),
@@ -549,7 +559,7 @@ class CaelixBatchDesc(C.Structure):
 class CaelixBatchTuning(C.Structure):
     _fields_ = [("min_blocks", C.c_uint32), ("wavefront", C.c_uint32), ("block_width", C.c_uint32),
                 ("refill_min", C.c_uint32), ("sort_keys_per_thread", C.c_uint32), ("order", C.c_uint32),
-                ("reserved", C.c_uint32 * 2)]
+                ("kernel", C.c_uint32), ("reserved", C.c_uint32)]
 
     def as_dict(self) -> dict:
         return {n: int(getattr(self, n)) for n, _ in self._fields_ if n != "reserved"}

@@ -1,6 +1,7 @@
 // The batch part of the C ABI (include/caelix_b200.h): many views of many scenes in one CUDA graph
-// launch (per-scene light-tree rebuilds as parallel graph branches, then the persistent trace
-// kernel of trace_batch.cu), and the autotuner of its launch parameters with a JSON cache.
+// launch (per-scene light-tree rebuilds as parallel graph branches, then the trace of every view:
+// the persistent kernel of trace_batch.cu or the wavefront kernels of wave.cu), and the autotuner
+// of its launch parameters with a JSON cache.
 // No counterpart in the reference, which renders one scene per renderer call
 // (lib/src/abi/caelix.cpp:700-953).
 #include <cuda_runtime.h>
@@ -42,12 +43,16 @@ CaelixBatchTuning default_tuning()
     return t;
 }
 
+constexpr uint32_t kDefaultWaveSlots = 1u << 22;
+
 bool tuning_ok(const CaelixBatchTuning& t)
 {
     return cx::trace_batch_variant_ok(t.min_blocks) &&
            (t.block_width == 8 || t.block_width == 16 || t.block_width == 32) && t.refill_min >= 1 &&
            t.refill_min <= 32 && cx::sort_keys_per_thread_ok(t.sort_keys_per_thread) && t.order <= 1 &&
-           t.reserved[0] == 0 && t.reserved[1] == 0;
+           t.kernel <= CAELIX_BATCH_WAVEFRONT && (t.kernel != CAELIX_BATCH_WAVEFRONT || t.wavefront == 0 ||
+                                                   t.wavefront >= 32) &&
+           t.reserved == 0;
 }
 
 bool same_tuning(const CaelixBatchTuning& a, const CaelixBatchTuning& b)
@@ -66,6 +71,11 @@ struct CaelixBatch
     std::vector<uint64_t> generations;      // of the scenes when the graph was captured
     CaelixBatchTuning tuning = default_tuning();
     cx::BatchView* d_views = nullptr;
+    cx::WaveView* d_wave_views = nullptr;
+    cx::GrowBuffer wave_table;               // the wave plan's view tables
+    cx::GrowBuffer wave_memory;              // path state and queues of the wavefront kernels
+    cx::WavePlan plan;                       // of the uploaded view order
+    std::vector<cx::WaveView> wave_views;    // host copy, in the uploaded order
     unsigned long long* d_counts = nullptr;  // [view][3]
     uint32_t* d_next = nullptr;
     cudaStream_t capture = nullptr;
@@ -89,6 +99,9 @@ void release(CaelixBatch* b)
 {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->d_views) cudaFree(b->d_views);
+    if (b->d_wave_views) cudaFree(b->d_wave_views);
+    b->wave_table.release();
+    b->wave_memory.release();
     if (b->d_counts) cudaFree(b->d_counts);
     if (b->d_next) cudaFree(b->d_next);
     if (b->capture) cudaStreamDestroy(b->capture);
@@ -118,6 +131,7 @@ cudaError_t upload_views(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t* i
     const uint32_t bw = t.block_width;
     const uint32_t bh = 32u / bw;
     std::vector<cx::BatchView> host(n);
+    b->wave_views.assign(n, cx::WaveView{});
     uint64_t items = 0;
     for (uint32_t j = 0; j < n; ++j) {
         const uint32_t i = order[j];
@@ -131,13 +145,40 @@ cudaError_t upload_views(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t* i
         h.ray_counts = b->d_counts + 3ull * i;
         h.item_base = (uint32_t)items;
         h.blocks_x = (v.target.width + bw - 1) / bw;
+        cx::WaveView& wv = b->wave_views[j];
+        std::memset(&wv, 0, sizeof(wv));
+        wv.scene = h.scene;
+        wv.params = h.params;
+        wv.radiance = h.radiance;
+        wv.ray_counts = h.ray_counts;
+        wv.blocks_x = h.blocks_x;
         const uint64_t blocks_y = (v.target.height + bh - 1) / bh;
         items += 32ull * h.blocks_x * blocks_y;
         // The work counter runs past the last item by at most 32 per warp: keep clear of 2^32.
         if (items >= (1ull << 32) - (1ull << 24)) return cudaErrorInvalidValue;
     }
     *item_count = (uint32_t)items;
-    return cudaMemcpy(b->d_views, host.data(), sizeof(cx::BatchView) * n, cudaMemcpyHostToDevice);
+    CX_TRY(cudaMemcpy(b->d_views, host.data(), sizeof(cx::BatchView) * n, cudaMemcpyHostToDevice));
+    if (t.kernel != CAELIX_BATCH_WAVEFRONT) return cudaSuccess;
+    // The wavefront organisation: its view table, wave plan and path state.
+    CX_TRY(cudaMemcpy(b->d_wave_views, b->wave_views.data(), sizeof(cx::WaveView) * n, cudaMemcpyHostToDevice));
+    b->plan = cx::wave_plan(b->wave_views.data(), n, bw);
+    if (b->wave_table.reserve(4ull * std::max<size_t>(b->plan.table.size(), 1), "caelix_batch_run") != CAELIX_OK)
+        return cudaErrorMemoryAllocation;
+    CX_TRY(cudaMemcpy(b->wave_table.ptr, b->plan.table.data(), 4 * b->plan.table.size(), cudaMemcpyHostToDevice));
+    uint32_t largest = 0;
+    for (uint32_t w : b->plan.items) largest = std::max(largest, w);
+    const uint32_t slots = std::min(largest, t.wavefront ? t.wavefront : kDefaultWaveSlots);
+    if (b->wave_memory.reserve(cx::wave_buffer_bytes(slots), "caelix_batch_run") != CAELIX_OK)
+        return cudaErrorMemoryAllocation;
+    return cudaSuccess;
+}
+
+uint32_t wave_slots(const CaelixBatch* b, const CaelixBatchTuning& t)
+{
+    uint32_t largest = 0;
+    for (uint32_t w : b->plan.items) largest = std::max(largest, w);
+    return std::max(32u, std::min(largest, t.wavefront ? t.wavefront : kDefaultWaveSlots));
 }
 
 uint32_t trace_grid(const CaelixBatch* b, const CaelixBatchTuning& t)
@@ -162,6 +203,13 @@ cudaError_t record(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t item_cou
             CX_TRY(cudaEventRecord(b->joins[j], b->branches[j]));
             CX_TRY(cudaStreamWaitEvent(s, b->joins[j], 0));
         }
+    }
+    if (trace && t.kernel == CAELIX_BATCH_WAVEFRONT) {
+        CX_TRY(cudaMemsetAsync(b->d_counts, 0, 24ull * b->views.size(), s));
+        const cx::WaveBuffers wb = cx::wave_carve(b->wave_memory.ptr, wave_slots(b, t));
+        return cx::wave_trace(b->wave_views.data(), b->d_wave_views, (uint32_t)b->views.size(), b->plan,
+                              static_cast<const uint32_t*>(b->wave_table.ptr), wb, t.block_width, b->device->sm_count,
+                              s, nullptr);
     }
     if (trace) {
         CX_TRY(cudaMemsetAsync(b->d_counts, 0, 24ull * b->views.size(), s));
@@ -233,7 +281,8 @@ cudaError_t ensure_graph(CaelixBatch* b)
     CX_TRY(capture_graph(b, b->tuning, true, true, &b->exec, &kernels));
     b->exec_tuning = b->tuning;
     b->kernel_nodes = kernels;
-    b->wavefront = trace_grid(b, b->tuning) * cx::kBatchThreads;
+    b->wavefront = b->tuning.kernel == CAELIX_BATCH_WAVEFRONT ? wave_slots(b, b->tuning)
+                                                               : trace_grid(b, b->tuning) * cx::kBatchThreads;
     for (size_t i = 0; i < b->scenes.size(); ++i) b->generations[i] = b->scenes[i]->generation;
     b->captures += 1;
     return cudaSuccess;
@@ -283,7 +332,7 @@ std::string tuning_key(const CaelixBatch* b)
 
 // The cache file: one JSON object, one entry per line:
 //   {"format": "caelix-batch-tuning/1", "entries": [
-//   {"key": "...", "min_blocks": 6, "wavefront": 0, "block_width": 16, "refill_min": 4, "sort_keys_per_thread": 16, "order": 1, "ms": 12.5},
+//   {"key": "...", "min_blocks": 6, "wavefront": 0, "block_width": 16, "refill_min": 4, "sort_keys_per_thread": 16, "order": 1, "kernel": 1, "ms": 12.5},
 //   ...
 //   ]}
 bool read_field(const std::string& line, const char* name, double* out)
@@ -320,11 +369,12 @@ bool cache_lookup(const char* path, const std::string& key, CaelixBatchTuning* t
         if (line.compare(0, tag.size(), tag) != 0) continue;
         CaelixBatchTuning c = default_tuning();
         double v;
-        const char* names[6] = {"min_blocks", "wavefront", "block_width", "refill_min", "sort_keys_per_thread", "order"};
-        uint32_t* fields[6] = {&c.min_blocks, &c.wavefront, &c.block_width, &c.refill_min, &c.sort_keys_per_thread,
-                               &c.order};
+        const char* names[7] = {"min_blocks", "wavefront",  "block_width", "refill_min", "sort_keys_per_thread",
+                                "order",      "kernel"};
+        uint32_t* fields[7] = {&c.min_blocks, &c.wavefront, &c.block_width, &c.refill_min, &c.sort_keys_per_thread,
+                               &c.order,      &c.kernel};
         bool ok = true;
-        for (int i = 0; i < 6; ++i) {
+        for (int i = 0; i < 7; ++i) {
             if (!read_field(line, names[i], &v) || v < 0 || v > 4294967295.0) {
                 ok = false;
                 break;
@@ -349,9 +399,9 @@ bool cache_store(const char* path, const std::string& key, const CaelixBatchTuni
     char buf[1024];
     std::snprintf(buf, sizeof(buf),
                   "{\"key\": \"%s\", \"min_blocks\": %u, \"wavefront\": %u, \"block_width\": %u, \"refill_min\": %u, "
-                  "\"sort_keys_per_thread\": %u, \"order\": %u, \"ms\": %.4f}",
+                  "\"sort_keys_per_thread\": %u, \"order\": %u, \"kernel\": %u, \"ms\": %.4f}",
                   key.c_str(), t.min_blocks, t.wavefront, t.block_width, t.refill_min, t.sort_keys_per_thread, t.order,
-                  (double)ms);
+                  t.kernel, (double)ms);
     entries.push_back(buf);
     const std::string tmp = std::string(path) + ".tmp";
     {
@@ -433,6 +483,7 @@ CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBa
     b->generations.assign(b->scenes.size(), ~0ull);
     const uint32_t n = desc->view_count;
     cudaError_t e = cudaMalloc(&b->d_views, sizeof(cx::BatchView) * n);
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_wave_views, sizeof(cx::WaveView) * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_counts, 24ull * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_next, 64);
     if (e == cudaSuccess) e = cudaMemset(b->d_counts, 0, 24ull * n);
@@ -530,38 +581,55 @@ CAELIX_API CaelixResult caelix_batch_autotune(CaelixBatch* batch, const CaelixFr
         }
         t.sort_keys_per_thread = best_kpt;
     }
-    // The trace parameters on the trace alone, one coordinate at a time.
-    float best = INFINITY;
-    e = time_part(batch, t, false, true, s, repeats, &best);
-    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_autotune");
-    const int per_sm_max = 8;
-    const uint32_t full = batch->device->sm_count * per_sm_max * cx::kBatchThreads;
+    // The trace parameters on the trace alone: for each kernel organisation a coordinate descent
+    // over its own parameters; the best of the two.
     struct Axis
     {
         uint32_t CaelixBatchTuning::*field;
         std::vector<uint32_t> values;
     };
-    const Axis axes[] = {
+    const uint32_t full = batch->device->sm_count * 8u * cx::kBatchThreads;
+    const std::vector<Axis> persistent_axes = {
         {&CaelixBatchTuning::min_blocks, {4u, 6u, 8u}},
         {&CaelixBatchTuning::block_width, {8u, 16u, 32u}},
         {&CaelixBatchTuning::refill_min, {1u, 4u, 16u}},
         {&CaelixBatchTuning::order, {0u, 1u}},
         {&CaelixBatchTuning::wavefront, {0u, full / 4u, full / 2u}},
     };
-    for (const Axis& axis : axes) {
-        for (uint32_t value : axis.values) {
-            if (t.*(axis.field) == value) continue;
-            CaelixBatchTuning c = t;
-            c.*(axis.field) = value;
-            float ms = 0.0f;
-            e = time_part(batch, c, false, true, s, repeats, &ms);
-            if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_autotune");
-            if (ms < best) {
-                best = ms;
-                t = c;
+    const std::vector<Axis> wave_axes = {
+        {&CaelixBatchTuning::block_width, {8u, 16u, 32u}},
+        {&CaelixBatchTuning::order, {0u, 1u}},
+        {&CaelixBatchTuning::wavefront, {0u, 1u << 20, 1u << 24}},
+    };
+    float best = INFINITY;
+    CaelixBatchTuning best_t = t;
+    for (uint32_t kernel : {CAELIX_BATCH_PERSISTENT, CAELIX_BATCH_WAVEFRONT}) {
+        CaelixBatchTuning k = t;
+        k.kernel = kernel;
+        k.wavefront = 0;
+        float k_best = 0.0f;
+        e = time_part(batch, k, false, true, s, repeats, &k_best);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_autotune");
+        for (const Axis& axis : kernel == CAELIX_BATCH_WAVEFRONT ? wave_axes : persistent_axes) {
+            for (uint32_t value : axis.values) {
+                if (k.*(axis.field) == value) continue;
+                CaelixBatchTuning c = k;
+                c.*(axis.field) = value;
+                float ms = 0.0f;
+                e = time_part(batch, c, false, true, s, repeats, &ms);
+                if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_autotune");
+                if (ms < k_best) {
+                    k_best = ms;
+                    k = c;
+                }
             }
         }
+        if (k_best < best) {
+            best = k_best;
+            best_t = k;
+        }
     }
+    t = best_t;
     batch->tuning = t;
     if (cache_path && !cache_store(cache_path, key, t, best))
         log(CAELIX_LOG_WARNING, "caelix_batch_autotune: could not write the cache %s", cache_path);

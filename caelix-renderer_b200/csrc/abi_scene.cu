@@ -357,9 +357,12 @@ CAELIX_API void caelix_renderer_destroy(CaelixRenderer* renderer)
 {
     if (!renderer) return;
     cudaSetDevice(renderer->device->ordinal);
+    if (renderer->rendered) cudaStreamSynchronize(renderer->last_stream);
     if (renderer->counts) cudaFree(renderer->counts);
     if (renderer->start) cudaEventDestroy(renderer->start);
     if (renderer->stop) cudaEventDestroy(renderer->stop);
+    renderer->wave_memory.release();
+    renderer->wave_views.release();
     delete renderer;
 }
 
@@ -377,10 +380,45 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
     cudaError_t e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_render");
-    cudaEventRecord(renderer->start, stream);
-    e = cx::trace_launch(cx::scene_view(scene->dev), p, reinterpret_cast<float*>(targets->radiance), renderer->counts,
-                         stream);
-    cudaEventRecord(renderer->stop, stream);
+    if (renderer->trace_mode == CAELIX_TRACE_MEGAKERNEL) {
+        cudaEventRecord(renderer->start, stream);
+        e = cx::trace_launch(cx::scene_view(scene->dev), p, reinterpret_cast<float*>(targets->radiance),
+                             renderer->counts, stream);
+        cudaEventRecord(renderer->stop, stream);
+        renderer->launches = 1;
+    } else {
+        // The wavefront trace of the one view: its path state sized for one sample of every pixel
+        // (or the set capacity), the view and its wave table uploaded ahead of the kernels.
+        cx::WaveView view;
+        std::memset(&view, 0, sizeof(view));
+        view.scene = cx::scene_view(scene->dev);
+        view.params = p;
+        view.radiance = reinterpret_cast<float*>(targets->radiance);
+        view.ray_counts = renderer->counts;
+        constexpr uint32_t kBlockWidth = 16;
+        view.blocks_x = (p.width + kBlockWidth - 1) / kBlockWidth;
+        const cx::WavePlan plan = cx::wave_plan(&view, 1, kBlockWidth);
+        const uint32_t items = plan.items.empty() ? 0 : plan.items[0];
+        const uint32_t capacity = renderer->wave_capacity ? std::min(renderer->wave_capacity, items) : items;
+        CaelixResult r2 = renderer->wave_memory.reserve(cx::wave_buffer_bytes(capacity), "caelix_renderer_render");
+        const uint64_t view_bytes = (sizeof(cx::WaveView) + 255) & ~uint64_t{255};
+        if (r2 == CAELIX_OK)
+            r2 = renderer->wave_views.reserve(view_bytes + 4ull * plan.table.size(), "caelix_renderer_render");
+        if (r2 != CAELIX_OK) return r2;
+        char* vbase = static_cast<char*>(renderer->wave_views.ptr);
+        cx::WaveView* d_view = reinterpret_cast<cx::WaveView*>(vbase);
+        uint32_t* d_table = reinterpret_cast<uint32_t*>(vbase + view_bytes);
+        e = cudaMemcpyAsync(d_view, &view, sizeof(view), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(d_table, plan.table.data(), 4 * plan.table.size(), cudaMemcpyHostToDevice, stream);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_render");
+        const cx::WaveBuffers wb = cx::wave_carve(renderer->wave_memory.ptr, capacity);
+        renderer->launches = 0;
+        cudaEventRecord(renderer->start, stream);
+        e = cx::wave_trace(&view, d_view, 1, plan, d_table, wb, kBlockWidth, renderer->device->sm_count, stream,
+                           &renderer->launches);
+        cudaEventRecord(renderer->stop, stream);
+    }
     renderer->last_stream = stream;
     renderer->frame_number = frame->frame_number;
     renderer->rendered = true;
@@ -419,6 +457,16 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     renderer->rendered = true;
     return cx::cuda_result(e, "caelix_renderer_backward");
     CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_renderer_set_trace_mode(CaelixRenderer* renderer, uint32_t mode, uint32_t wave_capacity)
+{
+    if (!renderer || (mode != CAELIX_TRACE_WAVEFRONT && mode != CAELIX_TRACE_MEGAKERNEL) ||
+        (wave_capacity != 0 && wave_capacity < 32))
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    renderer->trace_mode = mode;
+    renderer->wave_capacity = wave_capacity;
+    return CAELIX_OK;
 }
 
 CAELIX_API CaelixResult caelix_renderer_set_light_nee_options(CaelixRenderer* renderer, const CaelixLightNeeOptions* options)
@@ -460,7 +508,7 @@ CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, Cael
     out->primary_rays = c[0];
     out->bounce_rays = c[1];
     out->shadow_rays = c[2];
-    out->kernel_launches = 1;
+    out->kernel_launches = renderer->launches;
     return CAELIX_OK;
     CAELIX_GUARD_END
 }

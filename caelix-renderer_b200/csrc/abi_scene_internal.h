@@ -44,6 +44,11 @@ struct CaelixRenderer
     cudaStream_t last_stream = nullptr;
     uint64_t frame_number = 0;
     bool rendered = false;
+    uint32_t trace_mode = 0;        // CAELIX_TRACE_WAVEFRONT or CAELIX_TRACE_MEGAKERNEL
+    uint32_t wave_capacity = 0;     // 0 = every pixel of a sample in one wave
+    cx::GrowBuffer wave_memory;     // path state and queues of the wavefront trace
+    cx::GrowBuffer wave_views;      // the device copy of the view and its wave table
+    uint32_t launches = 0;          // kernels of the newest render
 };
 
 

@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <vector>
 
 #include "scene.cuh"
 
@@ -36,6 +37,71 @@ cudaError_t trace_launch(const SceneView& s, const TraceParams& p, float* radian
 // into (zero them first); image (may be null) receives the forward radiance.
 cudaError_t adjoint_launch(const SceneView& s, const TraceParams& p, const float* d_radiance, float* image,
                            float* d_albedo, float* d_power, unsigned long long* ray_counts, cudaStream_t stream);
+
+// ---- the wavefront trace (wave.cu) ----
+//
+// Paths live in HBM (structure of arrays, one slot per path); a wave is every pixel of one sample
+// index of the views that have it, split into sub-waves of at most `capacity` slots. Per bounce
+// two kernels run over compacted queues: wave_trace_kernel traces every queued ray (extension
+// and shadow rays alike, one DDA code path) and wave_shade_kernel advances every live path by
+// one vertex (shadow result, emission and MIS, albedo, light-tree NEE, Russian roulette),
+// queueing its next rays. Each kernel is small, and its warps start full.
+
+struct WaveView
+{
+    SceneView scene;
+    TraceParams params;
+    float* radiance;                 // width * height fp32 RGB (accumulated over the samples)
+    unsigned long long* ray_counts;  // u64 primary, bounce, shadow rays of this view
+    uint32_t blocks_x;               // pixel blocks per row (block_width x 32 / block_width pixels)
+    uint32_t pad;
+};
+
+struct WaveBuffers
+{
+    uint32_t capacity = 0;  // slots
+    uint32_t* item = nullptr;   // pixel index within the view (y * width + x)
+    uint32_t* vs = nullptr;     // view | sample << 16
+    uint32_t* flags = nullptr;
+    uint32_t* rng = nullptr;
+    uint32_t* light_rng = nullptr;
+    float4* org = nullptr;
+    float4* dir = nullptr;
+    float4* throughput = nullptr;
+    float4* radiance = nullptr;
+    float4* seg_n = nullptr;
+    float4* a0e0 = nullptr;  // primary albedo, primary emission
+    float4* sdir = nullptr;  // pending shadow ray: direction, t_max
+    float4* sadd = nullptr;  // pending shadow contribution
+    uint4* hit = nullptr;    // t bits, attrib (0 = miss), record, group
+    uint32_t* occluded = nullptr;
+    uint32_t* rayq[2] = {nullptr, nullptr};   // 2 * capacity entries: slot | kind << 30
+    uint32_t* pathq[2] = {nullptr, nullptr};  // capacity entries
+    uint32_t* counts = nullptr;               // [parity][2]: rays, paths
+};
+
+uint64_t wave_buffer_bytes(uint32_t capacity);
+WaveBuffers wave_carve(void* base, uint32_t capacity);
+
+// The wave plan of a set of views: for every sample index s below the largest spp, the views
+// with spp > s and their first item (pixel blocks x 32 per view) in that wave.
+struct WavePlan
+{
+    std::vector<uint32_t> table;     // per wave: view indices, then item bases (n_views each)
+    std::vector<uint32_t> offset;    // per wave: first word of its views in `table`
+    std::vector<uint32_t> views;     // per wave: number of views
+    std::vector<uint32_t> items;     // per wave: items
+    std::vector<uint32_t> bounces;   // per wave: the largest bounce count of its views
+};
+WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_width);
+
+// Records the trace of every sample of every view into `stream` (no host synchronisation):
+// d_views the device copy of `views`, d_table the device copy of plan.table. The views'
+// radiance buffers receive the averaged radiance (the per-frame kernel's result, bit for bit).
+// Kernel launches recorded are added to *launches (may be null).
+cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
+                       const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
+                       cudaStream_t stream, uint32_t* launches);
 
 // ---- the batched persistent trace (trace_batch.cu) ----
 

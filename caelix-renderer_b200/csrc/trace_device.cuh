@@ -225,7 +225,7 @@ struct Hit
 };
 
 // Closest hit over the bricks (front-to-back DDA over the brick grid).
-__device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+__device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
 {
     Hit h;
     h.hit = false;
@@ -304,6 +304,13 @@ __device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], cons
         if (out) break;
     }
     return h;
+}
+
+// The out-of-line copy for kernels that trace from several call sites (one copy of the DDA keeps
+// their instruction footprint small); a kernel with one call site inlines trace_ray_body.
+__device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+{
+    return trace_ray_body(s, o, d, tmin_ray, tmax_ray);
 }
 
 // ---- light tree ----
@@ -558,7 +565,7 @@ struct LightPoint
     uint32_t entry;
 };
 
-__device__ __noinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
+__device__ __forceinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
 {
     float pdf_brick = 1.0f;
     // The tree (one draw per tree; tree 1, dynamic entities, is empty: its importance and power

@@ -1,0 +1,453 @@
+// The wavefront trace (trace.cuh): path state in HBM, one kernel per stage over compacted queues.
+//
+// Stages of one sub-wave (a range of the pixels of one sample index):
+//   wave_generate_kernel  one slot per pixel: the camera ray (trace_pixel's), queued;
+//   then bounce_count + 1 times:
+//   wave_trace_kernel     every queued ray: the closest hit (extension rays) or occlusion (shadow
+//                         rays) through the brick-grid DDA, written to the slot;
+//   wave_shade_kernel     every live path: its shadow result, then its vertex (the per-frame
+//                         kernel's integrator step: emission with MIS, albedo, light-tree NEE,
+//                         Russian roulette), queueing its shadow ray and its next extension ray;
+//                         a finished path adds its sample to the pixel (the last sample divides).
+// A path's arithmetic is trace_pixel's in the same order (the shadow contribution of a vertex is
+// added before anything of the next vertex), so the radiance is the per-frame kernel's, bit for
+// bit. Queues are compacted with warp-aggregated atomics; every kernel reads its queue length on
+// the device, so a whole frame is recorded without a host synchronisation (graph-capturable).
+#include <algorithm>
+#include <cstdint>
+
+#include "trace.cuh"
+#include "trace_device.cuh"
+
+namespace cx {
+
+namespace {
+
+constexpr uint32_t kWaveThreads = 128;
+constexpr uint32_t kKindPrimary = 0, kKindBounce = 1, kKindShadow = 2;
+constexpr uint32_t kSlotMask = 0x3FFFFFFFu;
+constexpr uint32_t kFlagBounce = 0xFFu;       // bounce_index
+constexpr uint32_t kFlagSegLight = 1u << 8;   // segment_light = 3
+constexpr uint32_t kFlagShadow = 1u << 9;     // a shadow ray of the last vertex was queued
+constexpr uint32_t kFlagExt = 1u << 10;       // an extension ray was queued
+constexpr uint32_t kFlagPrimary = 1u << 11;   // that extension ray is the camera ray
+
+struct WaveGen
+{
+    const uint32_t* table;  // view indices, then item bases (n_views each)
+    uint32_t n_views;
+    uint32_t sample;
+    uint32_t first_item;
+    uint32_t count;
+    uint32_t block_width;
+};
+
+// Warp-aggregated append: returns this lane's first index in the queue. All lanes of the warp call.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, uint32_t n)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t incl = n;
+#pragma unroll
+    for (uint32_t d = 1; d < 32; d <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += t;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    uint32_t base = 0;
+    if (lane == 0 && total) base = atomicAdd(counter, total);
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    return base + incl - n;
+}
+
+__global__ void __launch_bounds__(kWaveThreads)
+    wave_generate_kernel(const WaveView* __restrict__ views, const WaveGen g, const WaveBuffers b)
+{
+    const uint32_t i = blockIdx.x * kWaveThreads + threadIdx.x;
+    const uint32_t bw = g.block_width, bh = 32u / bw;
+    bool valid = false;
+    if (i < g.count) {
+        const uint32_t item = g.first_item + i;
+        const uint32_t* bases = g.table + g.n_views;
+        uint32_t lo = 0, hi = g.n_views;
+        while (hi - lo > 1u) {
+            const uint32_t mid = (lo + hi) >> 1;
+            if (__ldg(bases + mid) <= item) lo = mid;
+            else hi = mid;
+        }
+        const uint32_t v = __ldg(g.table + lo);
+        const WaveView& V = views[v];
+        const TraceParams& P = V.params;
+        const uint32_t local = item - __ldg(bases + lo);
+        const uint32_t blk = local >> 5, in = local & 31u;
+        const uint32_t px = (blk % V.blocks_x) * bw + in % bw;
+        const uint32_t py = (blk / V.blocks_x) * bh + in / bw;
+        if (px < P.width && py < P.height) {
+            valid = true;
+            const float sx = (float)px + 0.5f + 0.0f;
+            const float sy = (float)py + 0.5f + 0.0f;
+            const float ndc_x = sx / (float)P.width * 2.0f - 1.0f;
+            const float ndc_y = 1.0f - sy / (float)P.height * 2.0f;
+            const float a = ndc_x * P.tan_half_fov_y * P.aspect;
+            const float bb = ndc_y * P.tan_half_fov_y;
+            float d[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) d[k] = P.right[k] * a + P.up[k] * bb + P.forward[k];
+            const float inv_len = 1.0f / sqrtf(dot3(d, d));
+#pragma unroll
+            for (int k = 0; k < 3; ++k) d[k] = d[k] * inv_len;
+            b.item[i] = py * P.width + px;
+            b.vs[i] = v | (g.sample << 16);
+            b.flags[i] = kFlagExt | kFlagPrimary;
+            b.org[i] = make_float4(P.position[0], P.position[1], P.position[2], 0.0f);
+            b.dir[i] = make_float4(d[0], d[1], d[2], 0.0f);
+        }
+    }
+    const uint32_t q = warp_append(&b.counts[1], valid ? 1u : 0u);
+    const uint32_t r = warp_append(&b.counts[0], valid ? 1u : 0u);
+    if (valid) {
+        b.pathq[0][q] = i;
+        b.rayq[0][r] = i | (kKindPrimary << 30);
+    }
+}
+
+__global__ void __launch_bounds__(kWaveThreads)
+    wave_trace_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
+{
+    const uint32_t n = *(volatile uint32_t*)&b.counts[2 * parity];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        b.counts[2 * (parity ^ 1u)] = 0;
+        b.counts[2 * (parity ^ 1u) + 1] = 0;
+    }
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * kWaveThreads;
+    for (uint32_t base = blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t i = base + lane;
+        uint32_t key = 0xFFFFFFFFu;
+        if (i < n) {
+            const uint32_t e = b.rayq[parity][i];
+            const uint32_t slot = e & kSlotMask, kind = e >> 30;
+            const uint32_t v = b.vs[slot] & 0xFFFFu;
+            const float4 o4 = b.org[slot];
+            const float4 d4 = kind == kKindShadow ? b.sdir[slot] : b.dir[slot];
+            const float o[3] = {o4.x, o4.y, o4.z};
+            const float d[3] = {d4.x, d4.y, d4.z};
+            const float t_max = kind == kKindShadow ? d4.w : (kind == kKindPrimary ? kRayTMax : kBounceTMax);
+            const Hit h = trace_ray_body(views[v].scene, o, d, 0.0f, t_max);
+            if (kind == kKindShadow) b.occluded[slot] = h.hit ? 1u : 0u;
+            else b.hit[slot] = h.hit ? make_uint4(__float_as_uint(h.t), h.attrib, h.record, h.group) : make_uint4(0, 0, 0, 0);
+            key = v * 4u + kind;
+        }
+        // Ray counters: one atomic per (view, kind) group of the warp.
+        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
+        if (key != 0xFFFFFFFFu && lane == (uint32_t)__ffs(peers) - 1u)
+            atomicAdd(views[key >> 2].ray_counts + (key & 3u), (unsigned long long)__popc(peers));
+    }
+}
+
+__global__ void __launch_bounds__(kWaveThreads, 8)
+    wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
+{
+    const uint32_t n = *(volatile uint32_t*)&b.counts[2 * parity + 1];
+    const uint32_t out = parity ^ 1u;
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t stride = gridDim.x * kWaveThreads;
+    for (uint32_t base = blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n; base += stride) {
+        const uint32_t i = base + lane;
+        uint32_t slot = 0, next_flags = 0;
+        bool live = false, shadow = false, ext = false;
+        if (i < n) {
+            slot = b.pathq[parity][i];
+            const uint32_t f = b.flags[slot];
+            const uint32_t vs = b.vs[slot];
+            const WaveView& V = views[vs & 0xFFFFu];
+            const SceneView& S = V.scene;
+            const TraceParams& P = V.params;
+            const uint32_t sp = vs >> 16;
+            const uint32_t item = b.item[slot];
+            const bool primary = (f & kFlagPrimary) != 0;
+            float rad[3] = {0.0f, 0.0f, 0.0f};
+            if (!primary) {
+                const float4 r4 = b.radiance[slot];
+                rad[0] = r4.x;
+                rad[1] = r4.y;
+                rad[2] = r4.z;
+            }
+            if ((f & kFlagShadow) && !b.occluded[slot]) {
+                const float4 s4 = b.sadd[slot];
+                rad[0] += s4.x;
+                rad[1] += s4.y;
+                rad[2] += s4.z;
+            }
+            bool finish = true, zero = false;
+            float e0 = 0.0f, a0[3] = {0.0f, 0.0f, 0.0f};
+            if (!primary) {
+                const float4 a4 = b.a0e0[slot];
+                a0[0] = a4.x;
+                a0[1] = a4.y;
+                a0[2] = a4.z;
+                e0 = a4.w;
+            }
+            if (f & kFlagExt) {
+                const uint4 hw = b.hit[slot];
+                const float4 o4 = b.org[slot];
+                const float4 d4 = b.dir[slot];
+                const float org[3] = {o4.x, o4.y, o4.z};
+                const float dir[3] = {d4.x, d4.y, d4.z};
+                if (hw.y == 0u) {
+                    zero = primary;  // a missed camera ray: the sample is 0
+                } else {
+                    Hit h;
+                    h.hit = true;
+                    h.t = __uint_as_float(hw.x);
+                    h.attrib = hw.y;
+                    h.record = hw.z;
+                    h.group = hw.w;
+                    const uint32_t fc = (uint32_t)(__ffs(h.attrib & 0x3Fu) - 1);
+                    h.normal[0] = fc == 0 ? 1.0f : (fc == 1 ? -1.0f : 0.0f);
+                    h.normal[1] = fc == 2 ? 1.0f : (fc == 3 ? -1.0f : 0.0f);
+                    h.normal[2] = fc == 4 ? 1.0f : (fc == 5 ? -1.0f : 0.0f);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) h.object_hit[k] = org[k] + dir[k] * h.t;
+                    const uint32_t px = item % P.width, py = item / P.width;
+                    const uint32_t seed = P.frame_seed + sp;
+                    uint32_t rng, light_rng;
+                    if (primary) {
+                        rng = init_random(px, py, seed);
+                        light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
+                    } else {
+                        rng = b.rng[slot];
+                        light_rng = b.light_rng[slot];
+                    }
+                    float tp[3], seg_n[3];
+                    uint32_t bounce_index, seg_light;
+                    float al[3], em, o2[3], d2[3];
+                    shade(S, h, org, dir, rng, al, em, o2, d2);
+                    bool nee_now;
+                    if (primary) {
+                        e0 = em;
+                        const float t0 = 1.0f / hmax(0.001f, 1.0f);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) {
+                            a0[k] = al[k];
+                            rad[k] = 0.0f;
+                            tp[k] = t0;
+                        }
+                        seg_light = 0;
+                        bounce_index = 1;
+                        nee_now = P.light_nee && P.bounce_count >= 1;
+                    } else {
+                        const float4 t4 = b.throughput[slot];
+                        const float4 n4 = b.seg_n[slot];
+                        tp[0] = t4.x;
+                        tp[1] = t4.y;
+                        tp[2] = t4.z;
+                        seg_n[0] = n4.x;
+                        seg_n[1] = n4.y;
+                        seg_n[2] = n4.z;
+                        seg_light = (f & kFlagSegLight) ? 3u : 0u;
+                        bounce_index = (f & kFlagBounce) + 1u;
+                        float ew = 1.0f;
+                        if (seg_light != 0u && em > 0.0f) ew = lamp_hit_weight(S, seg_light, h, org, dir, seg_n);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) rad[k] += em * (tp[k] * ew);
+#pragma unroll
+                        for (int k = 0; k < 3; ++k) tp[k] *= al[k] / hmax(0.001f, 1.0f);
+                        seg_light = 0u;
+                        nee_now = P.light_nee && bounce_index <= P.bounce_count;
+                    }
+                    ShadowRay r;
+                    float sadd[3] = {0.0f, 0.0f, 0.0f};
+                    if (nee_now) {
+                        seg_light = 3u;
+                        shadow = nee_prepare(S, o2, h.normal, light_rng, r);
+                        // Added to the radiance when unoccluded as nee * throughput (this vertex's
+                        // throughput, before Russian roulette rescales it).
+                        if (shadow) {
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) sadd[k] = r.value * (tp[k] * (1.0f / 1.0f));
+                        }
+                    }
+                    bool alive = true;
+                    if (!primary) {
+                        const float cp = hmax(tp[0], hmax(tp[1], tp[2]));
+                        alive = !(cp <= 0.0f || cp < random01(rng));
+                        if (alive) {
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) tp[k] *= 1.0f / cp;
+                        }
+                    }
+                    ext = alive && bounce_index <= P.bounce_count;
+                    if (shadow || ext) {
+                        finish = false;
+                        live = true;
+                        next_flags = bounce_index | (seg_light ? kFlagSegLight : 0u) | (shadow ? kFlagShadow : 0u) |
+                                     (ext ? kFlagExt : 0u);
+                        b.flags[slot] = next_flags;
+                        b.rng[slot] = rng;
+                        b.light_rng[slot] = light_rng;
+                        b.org[slot] = make_float4(o2[0], o2[1], o2[2], 0.0f);
+                        if (ext) {
+                            b.dir[slot] = make_float4(d2[0], d2[1], d2[2], 0.0f);
+                            b.seg_n[slot] = make_float4(h.normal[0], h.normal[1], h.normal[2], 0.0f);
+                            b.throughput[slot] = make_float4(tp[0], tp[1], tp[2], 0.0f);
+                        }
+                        if (shadow) {
+                            b.sdir[slot] = make_float4(r.dir[0], r.dir[1], r.dir[2], r.t_max);
+                            b.sadd[slot] = make_float4(sadd[0], sadd[1], sadd[2], 0.0f);
+                        }
+                        b.radiance[slot] = make_float4(rad[0], rad[1], rad[2], 0.0f);
+                        if (primary) b.a0e0[slot] = make_float4(a0[0], a0[1], a0[2], e0);
+                    }
+                }
+            }
+            if (finish) {
+                float rgb[3] = {0.0f, 0.0f, 0.0f};
+                if (!zero) {
+                    bool bad = false;
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) bad |= isnan(rad[k]) || isinf(rad[k]);
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) {
+                        const float sr = hmin(bad ? 0.0f : rad[k], 65504.0f);
+                        rgb[k] = e0 + a0[k] * sr;
+                    }
+                }
+                float* o = V.radiance + 3ull * item;
+                const bool last = sp + 1u == P.spp;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float acc = (sp == 0 ? 0.0f : o[k]) + rgb[k];
+                    o[k] = last ? acc / (float)P.spp : acc;
+                }
+            }
+        }
+        const uint32_t q = warp_append(&b.counts[2 * out + 1], live ? 1u : 0u);
+        const uint32_t nr = (shadow ? 1u : 0u) + (ext ? 1u : 0u);
+        const uint32_t r = warp_append(&b.counts[2 * out], nr);
+        if (live) {
+            b.pathq[out][q] = slot;
+            uint32_t k = r;
+            if (shadow) b.rayq[out][k++] = slot | (kKindShadow << 30);
+            if (ext) b.rayq[out][k] = slot | (kKindBounce << 30);
+        }
+    }
+}
+
+}  // namespace
+
+uint64_t wave_buffer_bytes(uint32_t capacity)
+{
+    const uint64_t c = std::max<uint32_t>(capacity, 32);
+    auto a = [](uint64_t x) { return (x + 255u) & ~uint64_t{255}; };
+    return 5 * a(4 * c) + 8 * a(16 * c) + a(16 * c) + a(4 * c) + 2 * a(8 * c) + 2 * a(4 * c) + a(64);
+}
+
+WaveBuffers wave_carve(void* base, uint32_t capacity)
+{
+    const uint64_t c = std::max<uint32_t>(capacity, 32);
+    char* p = static_cast<char*>(base);
+    auto take = [&](uint64_t bytes) {
+        char* q = p;
+        p += (bytes + 255u) & ~uint64_t{255};
+        return q;
+    };
+    WaveBuffers b;
+    b.capacity = capacity;
+    b.item = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.vs = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.flags = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.rng = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.light_rng = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.org = reinterpret_cast<float4*>(take(16 * c));
+    b.dir = reinterpret_cast<float4*>(take(16 * c));
+    b.throughput = reinterpret_cast<float4*>(take(16 * c));
+    b.radiance = reinterpret_cast<float4*>(take(16 * c));
+    b.seg_n = reinterpret_cast<float4*>(take(16 * c));
+    b.a0e0 = reinterpret_cast<float4*>(take(16 * c));
+    b.sdir = reinterpret_cast<float4*>(take(16 * c));
+    b.sadd = reinterpret_cast<float4*>(take(16 * c));
+    b.hit = reinterpret_cast<uint4*>(take(16 * c));
+    b.occluded = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.rayq[0] = reinterpret_cast<uint32_t*>(take(8 * c));
+    b.rayq[1] = reinterpret_cast<uint32_t*>(take(8 * c));
+    b.pathq[0] = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.pathq[1] = reinterpret_cast<uint32_t*>(take(4 * c));
+    b.counts = reinterpret_cast<uint32_t*>(take(64));
+    return b;
+}
+
+WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_width)
+{
+    WavePlan plan;
+    uint32_t max_spp = 0;
+    for (uint32_t v = 0; v < view_count; ++v) max_spp = std::max(max_spp, views[v].params.spp);
+    const uint32_t bh = 32u / block_width;
+    for (uint32_t s = 0; s < max_spp; ++s) {
+        std::vector<uint32_t> ids, bases;
+        uint64_t items = 0;
+        uint32_t bounces = 0;
+        for (uint32_t v = 0; v < view_count; ++v) {
+            const TraceParams& p = views[v].params;
+            if (p.spp <= s) continue;
+            ids.push_back(v);
+            bases.push_back((uint32_t)items);
+            const uint64_t bx = (p.width + block_width - 1) / block_width, by = (p.height + bh - 1) / bh;
+            items += 32ull * bx * by;
+            bounces = std::max(bounces, p.bounce_count);
+        }
+        plan.offset.push_back((uint32_t)plan.table.size());
+        plan.views.push_back((uint32_t)ids.size());
+        plan.items.push_back((uint32_t)std::min<uint64_t>(items, 0xFFFFFFFFull));
+        plan.bounces.push_back(bounces);
+        plan.table.insert(plan.table.end(), ids.begin(), ids.end());
+        plan.table.insert(plan.table.end(), bases.begin(), bases.end());
+    }
+    return plan;
+}
+
+cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
+                       const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
+                       cudaStream_t stream, uint32_t* launches)
+{
+    (void)views;
+    (void)view_count;
+    if (b.capacity == 0) return cudaErrorInvalidValue;
+    static int trace_blocks = 0, shade_blocks = 0;
+    if (trace_blocks == 0) {
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks, wave_trace_kernel, kWaveThreads, 0));
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel, kWaveThreads, 0));
+        trace_blocks = std::max(trace_blocks, 1);
+        shade_blocks = std::max(shade_blocks, 1);
+    }
+    uint32_t count = 0;
+    for (size_t s = 0; s < plan.items.size(); ++s) {
+        for (uint32_t first = 0; first < plan.items[s]; first += b.capacity) {
+            const uint32_t n = std::min(b.capacity, plan.items[s] - first);
+            WaveGen g;
+            g.table = d_table + plan.offset[s];
+            g.n_views = plan.views[s];
+            g.sample = (uint32_t)s;
+            g.first_item = first;
+            g.count = n;
+            g.block_width = block_width;
+            CX_TRY(cudaMemsetAsync(b.counts, 0, 16, stream));
+            wave_generate_kernel<<<(n + kWaveThreads - 1) / kWaveThreads, kWaveThreads, 0, stream>>>(d_views, g, b);
+            ++count;
+            const uint32_t ray_grid = std::min<uint32_t>((2 * n + kWaveThreads - 1) / kWaveThreads,
+                                                         sm_count * (uint32_t)trace_blocks);
+            const uint32_t shade_grid = std::min<uint32_t>((n + kWaveThreads - 1) / kWaveThreads,
+                                                           sm_count * (uint32_t)shade_blocks);
+            for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
+                const uint32_t parity = it & 1u;
+                wave_trace_kernel<<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                wave_shade_kernel<<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                count += 2;
+            }
+            CX_TRY(cudaGetLastError());
+        }
+    }
+    if (launches) *launches += count;
+    return cudaSuccess;
+}
+
+}  // namespace cx

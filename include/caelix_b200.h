@@ -448,6 +448,18 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
                                                const CaelixRenderTargets* targets, const CaelixCamera* camera,
                                                const CaelixRenderOptions* options);
 
+/* New (no reference counterpart; the reference traces with ray queries inside one compute
+   shader): the kernel organisation of caelix_renderer_render. Both give the same radiance, bit
+   for bit.
+     CAELIX_TRACE_WAVEFRONT (default): path state in device memory, one kernel per stage (trace,
+       shade) over compacted ray and path queues, every bounce; wave_capacity bounds the paths in
+       flight (0 = one per pixel; else at least 32), the rest of the pixels follow in later waves.
+     CAELIX_TRACE_MEGAKERNEL: one thread per pixel runs its whole path in one kernel. */
+#define CAELIX_TRACE_WAVEFRONT 0u
+#define CAELIX_TRACE_MEGAKERNEL 1u
+CAELIX_API CaelixResult caelix_renderer_set_trace_mode(CaelixRenderer* renderer, uint32_t mode,
+                                                       uint32_t wave_capacity);
+
 /* Replaces CaelixLightNeeOptions / caelix_renderer_set_light_nee_options
    (include/caelix/caelix.h:1283-1297). flags must be 0 (MIS on, no visibility hint). */
 typedef struct CaelixLightNeeOptions
@@ -508,9 +520,11 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
  * 256 views (a renderer, hence its scene and NEE options, plus a camera, a target and render
  * options each). One run is one CUDA graph launch: the light tree of every distinct scene is
  * rebuilt (as caelix_scene_flush does after caelix_scene_set_light_options), the builds of
- * different scenes running as parallel branches, then one persistent kernel traces every view,
- * its resident threads taking pixels of all views from one work counter. Each view's radiance is
- * bit-identical to caelix_renderer_render of the same renderer, target, camera and options.
+ * different scenes running as parallel branches, then every view is traced, either by one
+ * persistent kernel whose resident threads take pixels of all views from one work counter, or by
+ * the wavefront kernels over the paths of all views at once (CaelixBatchTuning::kernel). Each
+ * view's radiance is bit-identical to caelix_renderer_render of the same renderer, target, camera
+ * and options.
  *
  * The scenes must be flushed before the batch is created. A full re-flush of a scene (bricks,
  * powers or materials changed) moves its device tables: the next run notices it and captures
@@ -538,17 +552,24 @@ typedef struct CaelixBatchDesc
 /* The launch parameters of a run, chosen by caelix_batch_autotune or set by hand. */
 typedef struct CaelixBatchTuning
 {
-    uint32_t min_blocks;           /* register cap of the persistent kernel: 4, 6 or 8 CTAs of 128
+    uint32_t min_blocks;           /* persistent kernel: its register cap, 4, 6 or 8 CTAs of 128
                                       threads resident per SM (128, 80 or 64 registers) */
-    uint32_t wavefront;            /* paths in flight = persistent threads, rounded down to whole
-                                      CTAs; 0 = every resident thread */
+    uint32_t wavefront;            /* paths in flight. Persistent kernel: its threads, rounded down
+                                      to whole CTAs, 0 = every resident thread. Wavefront kernels:
+                                      the slots of one sub-wave (at least 32), 0 = 4M */
     uint32_t block_width;          /* pixel block of 32 consecutive work items: 8 (8x4), 16 (16x2)
                                       or 32 (32x1) */
-    uint32_t refill_min;           /* a warp takes new pixels once this many lanes are idle, 1..32 */
+    uint32_t refill_min;           /* persistent kernel: a warp takes new pixels once this many of its
+                                      lanes are idle, 1..32 */
     uint32_t sort_keys_per_thread; /* the light-tree radix sort's tile: 256 x 4, 8 or 16 keys */
     uint32_t order;                /* 0 = views in the given order, 1 = the most pixel samples first */
-    uint32_t reserved[2];          /* must be 0 */
+    uint32_t kernel;               /* CAELIX_BATCH_PERSISTENT: one persistent launch traces every
+                                      view; CAELIX_BATCH_WAVEFRONT: the wavefront kernels of
+                                      caelix_renderer_set_trace_mode over the paths of every view */
+    uint32_t reserved;             /* must be 0 */
 } CaelixBatchTuning;
+#define CAELIX_BATCH_PERSISTENT 0u
+#define CAELIX_BATCH_WAVEFRONT 1u
 
 /* Creates a batch (device buffers, no GPU work). Fails with INVALID_ARGUMENT on a bad view (NULL
    renderer, scene not flushed, target not a device buffer of the right size, options as
@@ -571,7 +592,8 @@ CAELIX_API CaelixResult caelix_batch_get_tuning(const CaelixBatch* batch, Caelix
    tunings on frame->command_buffer (coordinate descent: the sort tile on the light-tree builds
    alone, then the trace parameters on the trace alone, each candidate timed by CUDA events over
    `repeats` runs after one warm-up run; 0 = 2), applies the best and, with a cache file, stores
-   it there. Synchronous. */
+   it there. The kernel organisation is a coordinate too (each with its own parameters).
+   Synchronous. */
 CAELIX_API CaelixResult caelix_batch_autotune(CaelixBatch* batch, const CaelixFrameDesc* frame,
                                               const char* cache_path, uint32_t repeats,
                                               CaelixBatchTuning* out);

@@ -73,16 +73,18 @@ def check_views(batch, small_batch):
         assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == rays, f"view {i}"
 
 
-@pytest.mark.parametrize("min_blocks", [4, 6, 8])
+@pytest.mark.parametrize("min_blocks", [4, 6, 8, "wave"])
 def test_batch_matches_plain_renders(cuda_device, small_batch, min_blocks):
     import caelix_b200
 
     batch = caelix_b200.Batch(cuda_device, small_batch["views"], rebuild_light_trees=True)
+    wave = min_blocks == "wave"
     for block_width, refill_min, order in [(16, 4, 1), (8, 1, 0), (32, 16, 1)]:
         for v in small_batch["views"]:
             v[1].fill_(-1.0)
-        batch.set_tuning(min_blocks=min_blocks, block_width=block_width, refill_min=refill_min, order=order,
-                         sort_keys_per_thread=4 if order else 16)
+        batch.set_tuning(min_blocks=6 if wave else min_blocks, block_width=block_width, refill_min=refill_min,
+                         order=order, sort_keys_per_thread=4 if order else 16, kernel=1 if wave else 0,
+                         wavefront=(4096 if order else 0) if wave else 0)
         batch.run()
         st = batch.stats()
         check_views(batch, small_batch)

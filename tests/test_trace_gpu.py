@@ -138,3 +138,29 @@ def test_render_is_deterministic(cuda_device, oracle):
     assert torch.equal(a, b)
     r.close()
     scene.close()
+
+
+@pytest.mark.parametrize("capacity", [0, 4096, 777])
+def test_wavefront_equals_megakernel(cuda_device, capacity):
+    """The two kernel organisations give the same radiance bit for bit and the same ray counts,
+    whatever the wave capacity (small capacities split a sample into many sub-waves)."""
+    import torch
+
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(10, 8, 12), brick_occupancy=0.4, emissive_fraction=0.06, seed=13)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    r = caelix_b200.Renderer(cuda_device, scene)
+    w, h = 100, 70
+    outs, rays = [], []
+    for mode in (caelix_b200.Renderer.TRACE_MEGAKERNEL, caelix_b200.Renderer.TRACE_WAVEFRONT):
+        r.set_trace_mode(mode, capacity if mode == caelix_b200.Renderer.TRACE_WAVEFRONT else 0)
+        out = torch.full((w * h * 3,), -1.0, device="cuda")
+        r.render(out, w, h, vs.camera, bounces=5, seed=4, spp=3)
+        st = r.stats()
+        outs.append(out.cpu().numpy())
+        rays.append((st.primary_rays, st.bounce_rays, st.shadow_rays))
+    assert outs[0].view(np.uint32).tobytes() == outs[1].view(np.uint32).tobytes()
+    assert rays[0] == rays[1]
+    r.close()
+    scene.close()
