@@ -405,6 +405,7 @@ def measure_trace(args, world, local, dev, stream, flush):
             render(1000 + k)
     stream.synchronize()
     rays = 0
+    launches = 0
     total_ms = 0.0
     barrier(world)
     with ClockSampler(local) as clocks:
@@ -418,6 +419,7 @@ def measure_trace(args, world, local, dev, stream, flush):
                 b.record(stream)
             st = renderer.stats()  # waits for the step; outside its events
             rays += st.primary_rays + st.bounce_rays + st.shadow_rays
+            launches += st.kernel_launches
             total_ms += a.elapsed_time(b)
     barrier(world)
     ms = max_over_ranks(total_ms, world) / args.steps
@@ -449,13 +451,14 @@ def measure_trace(args, world, local, dev, stream, flush):
         "value": value,
         "ms_per_step": ms,
         "rays_per_step": rays_per_step,
-        "roofline": {"kernel": "trace_kernel", "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "roofline": {"kernel": "wave_trace_kernel + wave_shade_kernel (the frame)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                      "bytes_per_ray": TRACE_BYTES_PER_RAY,
                      "note": "latency-bound ray traversal; the bytes are a per-ray lower bound"},
         "e2e": {"value": world * rays_per_step / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
                 "h2d_bytes_per_step": 208 + 32, "d2h_bytes_per_step": TRACE_W * TRACE_H * 12, "ms_per_step": e2e_ms},
-        "gpu_launches": args.steps,
+        "gpu_launches": launches,
         "clocks": clocks.summary(),
     }
     renderer.close()
