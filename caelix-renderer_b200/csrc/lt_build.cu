@@ -482,7 +482,7 @@ __global__ void __launch_bounds__(kScanThreads)
 // 4-wide collapse: one thread per binary node at even depth writes its whole node (224 bytes,
 // its own parent link included: the 4-wide parent is the binary grandparent) and the parent words
 // of its leaf slots by sorted position.
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 4)
     lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                    const uint32_t* __restrict__ parent, const uint32_t* __restrict__ depth,
