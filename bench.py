@@ -45,6 +45,11 @@ FALLBACK_HBM_GBS = 6650.0
 BUILD_BYTES_PER_LEAF = 492  # emit 112 + Morton 32 + sort 68 + Karras 20 + aggregate 100 + wide 160
 SORT_PASS_BYTES_PER_PAIR = 60.0 / 4  # pass 0 reads keys only (12 B), passes 1-3 read and write pairs (16 B)
 TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record sector per ray
+# DRAM bytes (read + write) measured by ncu (one capture, cold cache; profiles/): a plain onesweep
+# pass at 4,194,304 pairs, scaled per pair; the wavefront frame of the 512 x 512 trace (trace and
+# shade kernels of its 5 bounce iterations).
+SORT_PASS_DRAM_BYTES_PER_PAIR = 35.1e6 / 4194304
+TRACE_FRAME_DRAM_BYTES = 156.8e6
 
 
 def measured_peaks():
@@ -374,7 +379,9 @@ def measure_build(args, world, local, dev, stream, flush, records):
             ["emit_bounds", "morton_hist", "sort_4_passes", "karras", "aggregate", "depth_scan", "wide_finish"],
             stage_ms)},
         "roofline": {"kernel": "onesweep_pass_kernel", "bound": "hbm", "achieved": sort_achieved, "peak": peak,
-                     "unit": "GB/s", "frac": sort_achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "unit": "GB/s", "frac": sort_achieved / peak, "peak_kind": peak_kind,
+                     "traffic": SORT_PASS_DRAM_BYTES_PER_PAIR * n,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4M-pair pass, per pair",
                      "algorithmic_bytes_per_launch": SORT_PASS_BYTES_PER_PAIR * n},
         "roofline_build": {"bound": "hbm", "achieved": build_achieved, "peak": peak, "unit": "GB/s",
                            "frac": build_achieved / peak, "bytes_per_leaf": BUILD_BYTES_PER_LEAF},
@@ -453,7 +460,8 @@ def measure_trace(args, world, local, dev, stream, flush):
         "rays_per_step": rays_per_step,
         "roofline": {"kernel": "wave_trace_kernel + wave_shade_kernel (the frame)", "bound": "hbm",
                      "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": TRACE_FRAME_DRAM_BYTES,
+                     "traffic_source": "ncu launch list: DRAM bytes of one frame's wave kernels (cold cache)",
                      "bytes_per_ray": TRACE_BYTES_PER_RAY,
                      "note": "latency-bound ray traversal; the bytes are a per-ray lower bound"},
         "e2e": {"value": world * rays_per_step / (e2e_ms / 1e3) / 1e6, "unit": "Mrays/s",
