@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark of the scene-flush / trace hot path on B200 (one JSON line on stdout, rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload trace|build]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload trace|build|batch]
 
 Workloads (seeded synthetic inputs with the shapes of the benchmark configurations; no dataset):
   trace   (default, the headline) the plain brick-DDA trace: a 128^3-voxel world of 16^3 bricks,
@@ -13,8 +13,14 @@ Workloads (seeded synthetic inputs with the shapes of the benchmark configuratio
   build   the light-tree build over 4,194,304 brick light records (brick coords uniform in a
           1024^3-brick grid, 16^3-brick render groups, power log-normal(0, 1) split over the faces);
           value = Mleaves/s.
-Both lines carry the other measurement: the trace line has a `build` object (the 4M-record build
-with its roofline and stage times, and the 4,096-record plain build in ms).
+  batch   64 scenes (brick counts log-uniform in [1k, 500k], square viewports 256/512/1024, 2 spp,
+          4 bounces): every scene's light-tree rebuild + the trace of every view as one CUDA graph
+          launch, against the same work one scene at a time through the plain C ABI.
+The trace line carries the other measurements as objects: `build` (the 4M-record build with its
+roofline and stage times, and the 4,096-record plain build in ms), `large` (the 2M-brick world at
+1920 x 1080, 4 spp, 6 bounces: flush and frame), `adjoint` (256 x 256, 8 spp, 3 bounces: forward
+vs backward time) and `batch` (the batched workload above); --no-large / --no-adjoint / --no-batch
+/ --no-build leave them out.
 
 `value` times the step with its inputs resident in HBM (CUDA events on the launching stream, L2
 flushed by a 256 MiB write between timed steps). `e2e` times the same step through the C ABI with
