@@ -448,9 +448,14 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     if (e == cudaSuccess) e = cudaMemsetAsync(d_power, 0, sizeof(float) * std::max(scene->dev.brick_count, 1u), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_backward");
+    const CaelixResult r2 =
+        renderer->wave_memory.reserve(cx::adjoint_bytes(p, renderer->wave_capacity), "caelix_renderer_backward");
+    if (r2 != CAELIX_OK) return r2;
+    renderer->launches = 0;
     cudaEventRecord(renderer->start, stream);
     e = cx::adjoint_launch(cx::scene_view(scene->dev), p, d_radiance, reinterpret_cast<float*>(image), d_albedo,
-                           d_power, renderer->counts, stream);
+                           d_power, renderer->counts, renderer->wave_memory.ptr, renderer->wave_capacity,
+                           renderer->device->sm_count, stream, &renderer->launches);
     cudaEventRecord(renderer->stop, stream);
     renderer->last_stream = stream;
     renderer->frame_number = frame->frame_number;

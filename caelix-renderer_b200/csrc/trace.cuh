@@ -32,11 +32,15 @@ struct TraceParams
 cudaError_t trace_launch(const SceneView& s, const TraceParams& p, float* radiance, unsigned long long* ray_counts,
                          cudaStream_t stream);
 
-// The adjoint of trace_launch (backward.cu): d_radiance = dL/d(radiance), width * height RGB;
+// The adjoint of a frame (backward.cu): d_radiance = dL/d(radiance), width * height RGB;
 // d_albedo (kMaterialSlots x 3) and d_power (one per brick, the scene's order) are accumulated
-// into (zero them first); image (may be null) receives the forward radiance.
+// into (zero them first); image (may be null) receives the forward radiance; ray_counts (may be
+// null) the rays of the recording pass. `memory`: adjoint_bytes(p, wave_capacity) bytes of device
+// memory, 256-aligned (wave_capacity 0 = one path per pixel).
+uint64_t adjoint_bytes(const TraceParams& p, uint32_t wave_capacity);
 cudaError_t adjoint_launch(const SceneView& s, const TraceParams& p, const float* d_radiance, float* image,
-                           float* d_albedo, float* d_power, unsigned long long* ray_counts, cudaStream_t stream);
+                           float* d_albedo, float* d_power, unsigned long long* ray_counts, void* memory,
+                           uint32_t wave_capacity, uint32_t sm_count, cudaStream_t stream, uint32_t* launches);
 
 // ---- the wavefront trace (wave.cu) ----
 //
@@ -77,7 +81,23 @@ struct WaveBuffers
     uint32_t* occluded = nullptr;
     uint32_t* rayq[2] = {nullptr, nullptr};   // 2 * capacity entries: slot | kind << 30
     uint32_t* pathq[2] = {nullptr, nullptr};  // capacity entries
-    uint32_t* counts = nullptr;               // [parity][2]: rays, paths
+    uint32_t* counts = nullptr;               // [parity][2]: rays, paths; then the trace fetch counters
+    // The adjoint's per-slot state (wave_adjoint): dL/dR of the sample, its radiance R, the power
+    // gradient of a pending NEE lamp (brick, value; applied if its shadow ray is unoccluded).
+    float4* adj_g = nullptr;
+    float4* adj_r = nullptr;
+    uint2* adj_nee = nullptr;
+};
+
+// The arrays of an adjoint (wave_adjoint, one view): dL/d(pixel), the radiance of every pixel
+// sample (spp x width x height x 3, written by the recording pass, read by the replay), and the
+// gradients (accumulated into).
+struct WaveAdjoint
+{
+    const float* d_radiance;
+    float* sample_radiance;
+    float* d_albedo;  // [kMaterialSlots][3]
+    float* d_power;   // [brick_count]
 };
 
 uint64_t wave_buffer_bytes(uint32_t capacity);
@@ -102,6 +122,15 @@ WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_wi
 cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
                        const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
                        cudaStream_t stream, uint32_t* launches);
+
+// The adjoint of wave_trace for one view (path replay, sampling held fixed; backward.cu states the
+// estimator and its derivative): a recording pass (the trace of d_record: radiance into its
+// radiance buffer when not null, every sample's R into adj.sample_radiance), then the replay of
+// every path (d_replay: the same view without radiance buffer or ray counters) gathering dL/dalbedo
+// and dL/dpower. Gradients are accumulated into (zero them first).
+cudaError_t wave_adjoint(const WaveView* d_record, const WaveView* d_replay, const WavePlan& plan,
+                         const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
+                         const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches);
 
 // ---- the batched persistent trace (trace_batch.cu) ----
 

@@ -139,14 +139,36 @@ __global__ void __launch_bounds__(kWaveThreads)
         }
         // Ray counters: one atomic per (view, kind) group of the warp.
         const uint32_t peers = __match_any_sync(0xFFFFFFFFu, key);
-        if (key != 0xFFFFFFFFu && lane == (uint32_t)__ffs(peers) - 1u)
-            atomicAdd(views[key >> 2].ray_counts + (key & 3u), (unsigned long long)__popc(peers));
+        if (key != 0xFFFFFFFFu && lane == (uint32_t)__ffs(peers) - 1u) {
+            unsigned long long* counts = views[key >> 2].ray_counts;
+            if (counts) atomicAdd(counts + (key & 3u), (unsigned long long)__popc(peers));
+        }
     }
 }
 
-__global__ void __launch_bounds__(kWaveThreads, 8)
-    wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
+// kMode: kShadeRender (the render), kShadeRecord (the adjoint's recording pass: also every
+// sample's radiance R), kShadeReplay (the adjoint's replay: the gradients, no image).
+enum : int
 {
+    kShadeRender = 0,
+    kShadeRecord = 1,
+    kShadeReplay = 2,
+};
+
+__device__ __forceinline__ float gsum3(const float G[3], const float t[3], float s)
+{
+    return G[0] * (t[0] * s) + G[1] * (t[1] * s) + G[2] * (t[2] * s);
+}
+
+template <int kMode>
+__global__ void __launch_bounds__(kWaveThreads, 8)
+    wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity, const WaveAdjoint adj)
+{
+    __shared__ float s_albedo[kMode == kShadeReplay ? kMaterialSlots * 3 : 1];
+    if (kMode == kShadeReplay) {
+        for (uint32_t i = threadIdx.x; i < kMaterialSlots * 3; i += kWaveThreads) s_albedo[i] = 0.0f;
+        __syncthreads();
+    }
     const uint32_t n = *(volatile uint32_t*)&b.counts[2 * parity + 1];
     const uint32_t out = parity ^ 1u;
     const uint32_t lane = threadIdx.x & 31u;
@@ -177,6 +199,21 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
                 rad[0] += s4.x;
                 rad[1] += s4.y;
                 rad[2] += s4.z;
+                if (kMode == kShadeReplay) {
+                    const uint2 pn = b.adj_nee[slot];  // the lamp's power gradient, now unoccluded
+                    if (pn.x != kNone) atomicAdd(adj.d_power + pn.x, __uint_as_float(pn.y));
+                }
+            }
+            float G[3] = {0.0f, 0.0f, 0.0f}, R[3] = {0.0f, 0.0f, 0.0f};
+            if (kMode == kShadeReplay && !primary) {
+                const float4 g4 = b.adj_g[slot];
+                const float4 r4 = b.adj_r[slot];
+                G[0] = g4.x;
+                G[1] = g4.y;
+                G[2] = g4.z;
+                R[0] = r4.x;
+                R[1] = r4.y;
+                R[2] = r4.z;
             }
             bool finish = true, zero = false;
             float e0 = 0.0f, a0[3] = {0.0f, 0.0f, 0.0f};
@@ -235,6 +272,30 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
                         seg_light = 0;
                         bounce_index = 1;
                         nee_now = P.light_nee && P.bounce_count >= 1;
+                        if (kMode == kShadeReplay) {
+                            // The sample's value e0 + a0 * sanitize(R), R from the recording pass.
+                            const float* rs = adj.sample_radiance + 3ull * ((uint64_t)sp * P.width * P.height + item);
+                            bool bad = false;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                R[k] = rs[k];
+                                bad |= isnan(R[k]) || isinf(R[k]);
+                            }
+                            const uint32_t block0 = (h.attrib >> 16) & 0xFFFFu;
+                            float* ga = s_albedo + 3 * (block0 & (kMaterialSlots - 1));
+                            float g[3];
+                            bool any = false;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) {
+                                g[k] = adj.d_radiance[3ull * item + k] / (float)P.spp;
+                                const float sr = hmin(bad ? 0.0f : R[k], 65504.0f);
+                                atomicAdd(ga + k, g[k] * sr);
+                                G[k] = (!bad && R[k] <= 65504.0f) ? g[k] * a0[k] : 0.0f;
+                                any |= G[k] != 0.0f;
+                            }
+                            if (block0 & kOpaqueBit) atomicAdd(adj.d_power + h.record, g[0] + g[1] + g[2]);
+                            if (!any) nee_now = false, bounce_index = P.bounce_count + 1u;  // nothing flows back
+                        }
                     } else {
                         const float4 t4 = b.throughput[slot];
                         const float4 n4 = b.seg_n[slot];
@@ -250,6 +311,15 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
                         if (seg_light != 0u && em > 0.0f) ew = lamp_hit_weight(S, seg_light, h, org, dir, seg_n);
 #pragma unroll
                         for (int k = 0; k < 3; ++k) rad[k] += em * (tp[k] * ew);
+                        if (kMode == kShadeReplay) {
+                            const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
+                            if (block & kOpaqueBit) atomicAdd(adj.d_power + h.record, gsum3(G, tp, ew));
+                            // Everything gathered from here on carries this vertex's albedo.
+                            float* ga = s_albedo + 3 * (block & (kMaterialSlots - 1));
+#pragma unroll
+                            for (int k = 0; k < 3; ++k)
+                                if (al[k] > 0.0f && G[k] != 0.0f) atomicAdd(ga + k, G[k] * (R[k] - rad[k]) / al[k]);
+                        }
 #pragma unroll
                         for (int k = 0; k < 3; ++k) tp[k] *= al[k] / hmax(0.001f, 1.0f);
                         seg_light = 0u;
@@ -267,6 +337,9 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
                             for (int k = 0; k < 3; ++k) sadd[k] = r.value * (tp[k] * (1.0f / 1.0f));
                         }
                     }
+                    uint2 pending = make_uint2(kNone, 0u);
+                    if (kMode == kShadeReplay && shadow && r.brick != kNone)
+                        pending = make_uint2(r.brick, __float_as_uint(gsum3(G, tp, r.dvalue_de)));
                     bool alive = true;
                     if (!primary) {
                         const float cp = hmax(tp[0], hmax(tp[1], tp[2]));
@@ -297,10 +370,22 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
                         }
                         b.radiance[slot] = make_float4(rad[0], rad[1], rad[2], 0.0f);
                         if (primary) b.a0e0[slot] = make_float4(a0[0], a0[1], a0[2], e0);
+                        if (kMode == kShadeReplay) {
+                            if (primary) {
+                                b.adj_g[slot] = make_float4(G[0], G[1], G[2], 0.0f);
+                                b.adj_r[slot] = make_float4(R[0], R[1], R[2], 0.0f);
+                            }
+                            if (shadow) b.adj_nee[slot] = pending;
+                        }
                     }
                 }
             }
-            if (finish) {
+            if (finish && kMode == kShadeRecord) {
+                float* rs = adj.sample_radiance + 3ull * ((uint64_t)sp * P.width * P.height + item);
+#pragma unroll
+                for (int k = 0; k < 3; ++k) rs[k] = zero ? 0.0f : rad[k];
+            }
+            if (finish && kMode != kShadeReplay && V.radiance) {
                 float rgb[3] = {0.0f, 0.0f, 0.0f};
                 if (!zero) {
                     bool bad = false;
@@ -331,6 +416,11 @@ __global__ void __launch_bounds__(kWaveThreads, 8)
             if (ext) b.rayq[out][k] = slot | (kKindBounce << 30);
         }
     }
+    if (kMode == kShadeReplay) {
+        __syncthreads();
+        for (uint32_t i = threadIdx.x; i < kMaterialSlots * 3; i += kWaveThreads)
+            if (s_albedo[i] != 0.0f) atomicAdd(adj.d_albedo + i, s_albedo[i]);
+    }
 }
 
 }  // namespace
@@ -339,7 +429,8 @@ uint64_t wave_buffer_bytes(uint32_t capacity)
 {
     const uint64_t c = std::max<uint32_t>(capacity, 32);
     auto a = [](uint64_t x) { return (x + 255u) & ~uint64_t{255}; };
-    return 5 * a(4 * c) + 8 * a(16 * c) + a(16 * c) + a(4 * c) + 2 * a(8 * c) + 2 * a(4 * c) + a(64);
+    return 5 * a(4 * c) + 8 * a(16 * c) + a(16 * c) + a(4 * c) + 2 * a(8 * c) + 2 * a(4 * c) + a(64) +
+           2 * a(16 * c) + a(8 * c);
 }
 
 WaveBuffers wave_carve(void* base, uint32_t capacity)
@@ -373,6 +464,9 @@ WaveBuffers wave_carve(void* base, uint32_t capacity)
     b.pathq[0] = reinterpret_cast<uint32_t*>(take(4 * c));
     b.pathq[1] = reinterpret_cast<uint32_t*>(take(4 * c));
     b.counts = reinterpret_cast<uint32_t*>(take(64));
+    b.adj_g = reinterpret_cast<float4*>(take(16 * c));
+    b.adj_r = reinterpret_cast<float4*>(take(16 * c));
+    b.adj_nee = reinterpret_cast<uint2*>(take(8 * c));
     return b;
 }
 
@@ -405,17 +499,20 @@ WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_wi
     return plan;
 }
 
-cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
-                       const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
-                       cudaStream_t stream, uint32_t* launches)
+namespace {
+
+// Every sub-wave of every wave of the plan, its shade kernels in mode kMode.
+template <int kMode>
+cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b,
+                     uint32_t block_width, uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream,
+                     uint32_t* launches)
 {
-    (void)views;
-    (void)view_count;
     if (b.capacity == 0) return cudaErrorInvalidValue;
     static int trace_blocks = 0, shade_blocks = 0;
     if (trace_blocks == 0) {
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks, wave_trace_kernel, kWaveThreads, 0));
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel, kWaveThreads, 0));
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel<kShadeRender>,
+                                                             kWaveThreads, 0));
         trace_blocks = std::max(trace_blocks, 1);
         shade_blocks = std::max(shade_blocks, 1);
     }
@@ -440,7 +537,7 @@ cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t 
             for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
                 const uint32_t parity = it & 1u;
                 wave_trace_kernel<<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
-                wave_shade_kernel<<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                wave_shade_kernel<kMode><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
                 count += 2;
             }
             CX_TRY(cudaGetLastError());
@@ -448,6 +545,26 @@ cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t 
     }
     if (launches) *launches += count;
     return cudaSuccess;
+}
+
+}  // namespace
+
+cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
+                       const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
+                       cudaStream_t stream, uint32_t* launches)
+{
+    (void)views;
+    (void)view_count;
+    const WaveAdjoint none{nullptr, nullptr, nullptr, nullptr};
+    return wave_run<kShadeRender>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
+}
+
+cudaError_t wave_adjoint(const WaveView* d_record, const WaveView* d_replay, const WavePlan& plan,
+                         const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
+                         const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches)
+{
+    CX_TRY(wave_run<kShadeRecord>(d_record, plan, d_table, b, block_width, sm_count, adj, stream, launches));
+    return wave_run<kShadeReplay>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
 }
 
 }  // namespace cx

@@ -504,7 +504,9 @@ CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, Cael
    value & 0x7F), and to the emitter power of every brick, d_power: device float[brick_count] in
    the scene's brick order (the keys of caelix_scene_get_view: increasing linear brick index).
    Sampling quantities (pdfs, MIS weights, Russian-roulette probabilities, discrete decisions) are
-   held fixed; each path is traced again (path replay), nothing of it is stored. When
+   held fixed. The frame is traced twice (path replay): once recording each sample's radiance (one
+   image per sample index, in device memory the renderer keeps), once more gathering the
+   gradients; nothing of the paths is stored. When
    targets->radiance is not 0 it also receives the forward radiance (bit-identical to
    caelix_renderer_render). Asynchronous on frame->command_buffer; rays and timings through
    caelix_renderer_get_stats / caelix_renderer_get_gpu_timings. */

@@ -86,3 +86,47 @@ def test_oracle_build_grouped_frames(oracle):
     # Leaves are the world-space brick boxes.
     lo = o["leaves"]["lo"][:20000]
     assert np.all(lo >= 0) and np.all(o["leaves"]["hi"][:20000] <= 256 * 8)
+
+
+def test_batch_plan_distribution():
+    """The batched workload's plan: brick counts within [1k, 500k], log-uniform (the median near
+    the geometric mean), square viewports among 256, 512, 1024, deterministic."""
+    import numpy as np
+
+    from caelix_b200 import workloads
+
+    plan = workloads.batch_plan()
+    assert len(plan) == 64 and plan == workloads.batch_plan()
+    bricks = np.array([b for b, _ in plan], np.float64)
+    assert bricks.min() >= 1000 and bricks.max() <= 500_000
+    assert 0.25 < np.median(bricks) / np.sqrt(1000 * 500_000) < 4
+    assert {s for _, s in plan} <= set(workloads.BATCH_VIEWPORTS)
+    assert len({s for _, s in plan}) == 3
+
+
+def test_solid_brick_scene_and_target():
+    """The differentiation world: the first draw of a repeated coordinate kept, bricks in
+    increasing linear index, every brick solid and emissive; the target perturbs albedo and power
+    by at most 10 %."""
+    import numpy as np
+
+    from caelix_b200 import workloads
+
+    vs = workloads.solid_brick_scene(n=600, grid_bricks=16, seed=3)
+    lin = vs.keys[:, 0] + 16 * (vs.keys[:, 1] + 16 * vs.keys[:, 2])
+    assert np.all(np.diff(lin) > 0)
+    rng = workloads.Pcg32(3, 1)
+    coords = (rng.next_u32(3 * 600).reshape(600, 3) >> np.uint32(28)).astype(np.int64)
+    power = rng.lognormal(600)
+    first = {}
+    for i, c in enumerate(map(tuple, coords)):
+        first.setdefault(c, i)
+    assert len(first) == vs.brick_count
+    for k, p in zip(map(tuple, vs.keys), vs.power):
+        assert np.float32(power[first[k]]) == p
+    assert np.all(vs.voxels & 0x8000) and np.all(vs.power > 0)
+    t = workloads.perturbed(vs)
+    ra = t.albedo[1:65] / vs.albedo[1:65]
+    rp = t.power / vs.power
+    assert np.all(np.abs(ra - 1) <= 0.1 + 1e-6) and np.all(np.abs(rp - 1) <= 0.1 + 1e-6)
+    assert np.array_equal(t.keys, vs.keys) and np.array_equal(t.voxels, vs.voxels)
