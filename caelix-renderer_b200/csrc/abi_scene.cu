@@ -395,7 +395,7 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
         view.params = p;
         view.radiance = reinterpret_cast<float*>(targets->radiance);
         view.ray_counts = renderer->counts;
-        constexpr uint32_t kBlockWidth = 16;
+        constexpr uint32_t kBlockWidth = 8;  // 8 x 4 pixel blocks per warp
         view.blocks_x = (p.width + kBlockWidth - 1) / kBlockWidth;
         const cx::WavePlan plan = cx::wave_plan(&view, 1, kBlockWidth);
         const uint32_t items = plan.items.empty() ? 0 : plan.items[0];

@@ -32,7 +32,7 @@ namespace cx {
 
 namespace {
 
-constexpr uint32_t kAdjointBlockWidth = 16;
+constexpr uint32_t kAdjointBlockWidth = 8;
 
 uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t{255}; }
 
