@@ -483,7 +483,9 @@ def measure_trace(args, world, local, dev, stream, flush):
 def measure_large(args, world, local, dev, stream, flush):
     """The large scene: 2048 x 2048 x 512 voxels (256 x 256 x 64 bricks), ~2M occupied bricks (12 %
     voxel occupancy overall), ~100k emissive bricks; the flush (records, hash table, light records,
-    a full light-tree rebuild) and 1920 x 1080 frames at 4 spp, 6 bounces, light-tree NEE."""
+    a full light-tree rebuild) and 1920 x 1080 frames at 4 spp, 6 bounces, light-tree NEE; then a
+    light-tree-only flush and the flush after re-uploading 1 % of the bricks."""
+    import numpy as np
     import torch
 
     import caelix_b200
@@ -526,6 +528,20 @@ def measure_large(args, world, local, dev, stream, flush):
         total_ms += a.elapsed_time(b)
     ms = max_over_ranks(total_ms, world) / steps
     t = renderer.timings()
+    # A light-options change: the next flush rebuilds only the light tree.
+    scene.set_light_options(min_emission=20.0)
+    scene.flush(sptr)
+    tree_flush_ms = float(renderer.timings().flush_ms)
+    # An edit: 1 % of the bricks uploaded again (to the device staging), then the full flush from
+    # the staged bricks (device sort and gather of all bricks, records, hash table, light records).
+    edit = np.random.default_rng(5).choice(vs.brick_count, size=vs.brick_count // 100, replace=False)
+    t0 = time.perf_counter()
+    scene.upload_bricks(vs.keys[edit], vs.voxels[edit])
+    edit_upload_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    scene.flush(sptr)
+    edit_flush_wall_s = time.perf_counter() - t0
+    edit_flush_ms = float(renderer.timings().flush_ms)
     result = {
         "workload": "2048x2048x512-voxel world (256x256x64 bricks), value noise seed 3, 1920x1080, 4 spp, "
                     "6 bounces, light-tree NEE with MIS",
@@ -537,6 +553,11 @@ def measure_large(args, world, local, dev, stream, flush):
         "light_tree_nodes": int(ls.tree_nodes[0]),
         "flush_ms": float(t.flush_ms),
         "flush_wall_s": flush_wall_s,
+        "light_tree_flush_ms": tree_flush_ms,
+        "edit_bricks": int(len(edit)),
+        "edit_upload_s": edit_upload_s,
+        "edit_flush_ms": edit_flush_ms,
+        "edit_flush_wall_s": edit_flush_wall_s,
         "generate_s": gen_s,
         "upload_s": upload_s,
         "frame_ms": ms,

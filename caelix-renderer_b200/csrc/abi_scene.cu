@@ -1,5 +1,5 @@
-// The scene and renderer parts of the C ABI (include/caelix_b200.h): host-side brick staging,
-// the flush (scene_build) and the render call (trace_launch). Replaces the entry points of the
+// The scene and renderer parts of the C ABI (include/caelix_b200.h): device-resident brick
+// staging, the flush (staging_gather + scene_build_device) and the render call. Replaces the entry points of the
 // reference's lib/src/abi/caelix.cpp for the scene (:296-700) and the renderer (:700-953).
 #include <cuda_runtime.h>
 
@@ -94,8 +94,9 @@ CAELIX_API CaelixResult caelix_scene_create(CaelixDevice* device, const CaelixSc
     for (uint32_t i = 0; i < cx::kMaterialSlots * 3; ++i) s->albedo[i] = 0.5f;
     cudaError_t e = cudaEventCreate(&s->start);
     if (e == cudaSuccess) e = cudaEventCreate(&s->stop);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) {
-        delete s;
+        caelix_scene_destroy(s);
         return cx::cuda_result(e, "caelix_scene_create");
     }
     *out_scene = s;
@@ -108,6 +109,12 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     if (!scene) return;
     cudaSetDevice(scene->device->ordinal);
     cx::scene_release(scene->dev);
+    if (scene->upload_stream) cudaStreamSynchronize(scene->upload_stream);
+    if (scene->stage_keys) cudaFree(scene->stage_keys);
+    if (scene->stage_voxels) cudaFree(scene->stage_voxels);
+    scene->upload.release();
+    scene->flush_scratch.release();
+    if (scene->upload_stream) cudaStreamDestroy(scene->upload_stream);
     if (scene->start) cudaEventDestroy(scene->start);
     if (scene->stop) cudaEventDestroy(scene->stop);
     delete scene;
@@ -126,24 +133,84 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
             return CAELIX_ERROR_INVALID_ARGUMENT;
         }
     }
-    const uint16_t* b = static_cast<const uint16_t*>(blocks);
+    if (count == 0) return CAELIX_OK;
+    cudaSetDevice(scene->device->ordinal);
+    cudaStream_t st = scene->upload_stream;
+    // Slots: new keys take the next slots (with any power set before their upload).
+    const uint32_t old_slots = (uint32_t)scene->slot_power.size();
+    std::vector<uint32_t> slot(count);
     for (uint32_t i = 0; i < count; ++i) {
         const uint64_t packed = pack_key(keys[i]);
-        auto it = scene->slot_of.find(packed);
-        uint32_t slot;
-        if (it == scene->slot_of.end()) {
-            slot = (uint32_t)(scene->keys.size() / 3);
-            scene->slot_of.emplace(packed, slot);
-            scene->keys.push_back(keys[i].x);
-            scene->keys.push_back(keys[i].y);
-            scene->keys.push_back(keys[i].z);
-            scene->voxels.resize(scene->voxels.size() + 512);
-        } else {
-            slot = it->second;
+        const auto ins = scene->slot_of.emplace(packed, (uint32_t)scene->slot_power.size());
+        slot[i] = ins.first->second;
+        if (ins.second) {
+            scene->keys.insert(scene->keys.end(), {keys[i].x, keys[i].y, keys[i].z});
+            scene->key_max[0] = std::max(scene->key_max[0], keys[i].x);
+            scene->key_max[1] = std::max(scene->key_max[1], keys[i].y);
+            scene->key_max[2] = std::max(scene->key_max[2], keys[i].z);
+            const auto p = scene->pending_power.find(packed);
+            scene->slot_power.push_back(p != scene->pending_power.end() ? p->second : 0.0f);
+            if (p != scene->pending_power.end()) scene->pending_power.erase(p);
         }
-        std::memcpy(scene->voxels.data() + 512ull * slot, b + 512ull * i, 1024);
     }
-    scene->dirty = scene->dirty || count > 0;
+    const uint32_t slots = (uint32_t)scene->slot_power.size();
+    // Staging growth (doubling), the resident slots carried over.
+    if (slots > scene->stage_capacity) {
+        const uint32_t cap = std::max<uint32_t>(slots, std::max<uint32_t>(2 * scene->stage_capacity, 1024));
+        int32_t* nk = nullptr;
+        uint16_t* nv = nullptr;
+        cudaError_t e = cudaMalloc(&nk, 12ull * cap);
+        if (e == cudaSuccess) e = cudaMalloc(&nv, 1024ull * cap);
+        if (e == cudaSuccess && old_slots) {
+            e = cudaMemcpyAsync(nk, scene->stage_keys, 12ull * old_slots, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(nv, scene->stage_voxels, 1024ull * old_slots, cudaMemcpyDeviceToDevice, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        }
+        if (e != cudaSuccess) {
+            if (nk) cudaFree(nk);
+            if (nv) cudaFree(nv);
+            return cx::cuda_result(e, "caelix_scene_upload_bricks");
+        }
+        if (scene->stage_keys) cudaFree(scene->stage_keys);
+        if (scene->stage_voxels) cudaFree(scene->stage_voxels);
+        scene->stage_keys = nk;
+        scene->stage_voxels = nv;
+        scene->stage_capacity = cap;
+    }
+    // One copy per slot: the last upload of a key in this call wins.
+    scene->upload_mark.resize(slots, 0);
+    if (++scene->upload_epoch == 0) {
+        std::fill(scene->upload_mark.begin(), scene->upload_mark.end(), 0u);
+        scene->upload_epoch = 1;
+    }
+    std::vector<uint32_t> lists;  // [src index][slot], `unique` entries each
+    lists.reserve(2ull * count);
+    std::vector<uint32_t> dst;
+    dst.reserve(count);
+    for (uint32_t i = count; i-- > 0;) {
+        if (scene->upload_mark[slot[i]] == scene->upload_epoch) continue;
+        scene->upload_mark[slot[i]] = scene->upload_epoch;
+        lists.push_back(i);
+        dst.push_back(slot[i]);
+    }
+    const uint32_t unique = (uint32_t)dst.size();
+    lists.insert(lists.end(), dst.begin(), dst.end());
+    CaelixResult r = scene->upload.reserve(1024ull * count + 4ull * lists.size(), "caelix_scene_upload_bricks");
+    if (r != CAELIX_OK) return r;
+    uint16_t* d_blocks = static_cast<uint16_t*>(scene->upload.ptr);
+    uint32_t* d_lists = reinterpret_cast<uint32_t*>(d_blocks + 512ull * count);
+    cudaError_t e = cudaMemcpyAsync(d_blocks, blocks, 1024ull * count, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d_lists, lists.data(), 4ull * lists.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess && slots > old_slots)
+        e = cudaMemcpyAsync(scene->stage_keys + 3ull * old_slots, scene->keys.data() + 3ull * old_slots,
+                            12ull * (slots - old_slots), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cx::staging_scatter(d_blocks, d_lists, d_lists + unique, unique, scene->stage_voxels, st);
+    // The caller may reuse its buffers on return, and the next flush reads the staging.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_upload_bricks");
+    scene->dirty = true;
     if (consumed) *consumed = count;
     return CAELIX_OK;
     CAELIX_GUARD_END
@@ -156,7 +223,12 @@ CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_
     if (!scene || entity != 0 || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
     for (uint32_t i = 0; i < count; ++i)
         if (!key_ok(keys[i]) || !std::isfinite(power[i]) || power[i] < 0.0f) return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (uint32_t i = 0; i < count; ++i) scene->power[pack_key(keys[i])] = power[i];
+    for (uint32_t i = 0; i < count; ++i) {
+        const uint64_t packed = pack_key(keys[i]);
+        const auto it = scene->slot_of.find(packed);
+        if (it != scene->slot_of.end()) scene->slot_power[it->second] = power[i];
+        else scene->pending_power[packed] = power[i];
+    }
     scene->dirty = scene->dirty || count > 0;
     return CAELIX_OK;
     CAELIX_GUARD_END
@@ -215,33 +287,31 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         scene->light_tree_dirty = false;
         return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
     }
-    // Bricks in increasing linear brick index of the grid spanned by the keys.
-    const uint32_t n = (uint32_t)(scene->keys.size() / 3);
-    const int32_t* sk = scene->keys.data();
-    uint32_t grid[3] = {1, 1, 1};
-    for (uint32_t s = 0; s < n; ++s)
-        for (int k = 0; k < 3; ++k) grid[k] = std::max<uint32_t>(grid[k], (uint32_t)sk[3 * s + k] + 1);
-    std::vector<std::pair<uint64_t, uint32_t>> order(n);
-    for (uint32_t s = 0; s < n; ++s)
-        order[s] = {(uint64_t)sk[3 * s] + grid[0] * ((uint64_t)sk[3 * s + 1] + (uint64_t)grid[1] * sk[3 * s + 2]), s};
-    std::sort(order.begin(), order.end());
-    std::vector<int32_t> keys(3ull * n);
-    std::vector<uint16_t> voxels(512ull * n);
-    std::vector<float> power(n, 0.0f);
-    for (uint32_t i = 0; i < n; ++i) {
-        const uint32_t s = order[i].second;
-        keys[3 * i] = sk[3 * s];
-        keys[3 * i + 1] = sk[3 * s + 1];
-        keys[3 * i + 2] = sk[3 * s + 2];
-        std::memcpy(voxels.data() + 512ull * i, scene->voxels.data() + 512ull * s, 1024);
-        const CaelixBrickKey key{sk[3 * s], sk[3 * s + 1], sk[3 * s + 2]};
-        const auto p = scene->power.find(pack_key(key));
-        if (p != scene->power.end() && scene->light_options.enabled) power[i] = p->second;
-    }
+    // The staged bricks in increasing linear brick index of the grid spanned by the keys, sorted
+    // and gathered on the device, then the build.
+    const uint32_t n = (uint32_t)scene->slot_power.size();
+    const uint32_t grid[3] = {(uint32_t)scene->key_max[0] + 1, (uint32_t)scene->key_max[1] + 1,
+                              (uint32_t)scene->key_max[2] + 1};
+    const bool lit = scene->light_options.enabled != 0;
+    CaelixResult r = scene->flush_scratch.reserve(4ull * n + 4 * cx::staging_sort_words(n), "caelix_scene_flush");
+    if (r != CAELIX_OK) return r;
+    float* d_power = static_cast<float*>(scene->flush_scratch.ptr);
+    uint32_t* sort_scratch = reinterpret_cast<uint32_t*>(d_power + n);
+    // The build rewrites the device tables in place: renders of the previous build, on any
+    // stream, finish first.
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     uint32_t status = 0;
     cudaEventRecord(scene->start, stream);
-    const cudaError_t e = cx::scene_build(scene->dev, grid, scene->group_shift, n, keys.data(), voxels.data(),
-                                          power.data(), scene->albedo, stream, &status);
+    e = cx::scene_alloc_inputs(scene->dev, n, stream);
+    if (e == cudaSuccess && lit && n)
+        e = cudaMemcpyAsync(d_power, scene->slot_power.data(), 4ull * n, cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scene->dev.albedo, scene->albedo, sizeof(scene->albedo), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cx::staging_gather(scene->stage_keys, scene->stage_voxels, lit ? d_power : nullptr, n, grid, sort_scratch,
+                               scene->dev.status, scene->dev.keys, scene->dev.voxels, scene->dev.power, stream);
+    if (e == cudaSuccess) e = cx::scene_build_device(scene->dev, grid, scene->group_shift, n, stream, &status);
     cudaEventRecord(scene->stop, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     cudaEventSynchronize(scene->stop);

@@ -15,11 +15,22 @@ struct CaelixScene
 {
     CaelixDevice* device = nullptr;
     uint32_t group_shift = 4;
-    // Host staging of the uploaded bricks: slot s holds keys[3s .. 3s+2] and voxels[512s ..].
+    // Brick staging. Slot s holds the brick keys[3s .. 3s+2]; its 512 block values stay on the
+    // device (stage_voxels[512s ..], copied there by the upload that wrote them), its key in
+    // stage_keys[3s ..] and its power in slot_power[s].
     std::unordered_map<uint64_t, uint32_t> slot_of;
     std::vector<int32_t> keys;
-    std::vector<uint16_t> voxels;
-    std::unordered_map<uint64_t, float> power;
+    std::vector<float> slot_power;
+    std::unordered_map<uint64_t, float> pending_power;  // power of keys not uploaded yet
+    int32_t key_max[3] = {0, 0, 0};
+    uint32_t stage_capacity = 0;  // slots
+    int32_t* stage_keys = nullptr;
+    uint16_t* stage_voxels = nullptr;
+    cudaStream_t upload_stream = nullptr;
+    cx::GrowBuffer upload;         // one upload's block values and slot lists
+    cx::GrowBuffer flush_scratch;  // slot powers, linear indices and the sort of a flush
+    std::vector<uint32_t> upload_mark;  // per slot: the last upload that wrote it
+    uint32_t upload_epoch = 0;
     float albedo[cx::kMaterialSlots * 3];
     CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
     bool dirty = true;

@@ -161,8 +161,13 @@ __global__ void bitmap_kernel(const int32_t* __restrict__ keys, uint32_t n, uint
 }
 
 // ---------------------------------------------------------------------------------------------
-// Finalize (caelix_finalize.hlsl:110-340): one CTA of 64 threads per brick, thread t owns the
-// voxel row y = t & 7, z = t >> 3.
+// Finalize (caelix_finalize.hlsl:110-340): one warp per brick, grid-stride. Lane l owns the 16
+// voxels vi = l + 32k (x = l & 7, y = (l >> 3) + 4 (k & 1), z = k >> 1), so that every in-brick
+// neighbour read (vi +- 1, 8, 64) is a conflict-free shared-memory read of consecutive values.
+// The brick and its six neighbour faces are staged in shared memory (coalesced 16-byte loads
+// where the face is contiguous); the record (274 words) is staged too and stored in 8-byte
+// units, every word of it written (no clear of the record array is needed). Bricks whose values
+// are all air or opaque take a bit-mask path (see the kernel).
 
 struct FinalizeArgs
 {
@@ -176,92 +181,211 @@ struct FinalizeArgs
     uint32_t* records;
 };
 
-__global__ void __launch_bounds__(64) finalize_kernel(const FinalizeArgs a)
+constexpr uint32_t kFinalizeWarps = 8;
+constexpr uint32_t kFinalizeStageWords = 256 + 6 * 32;  // the brick + six faces of 64 values
+constexpr uint32_t kFinalizeRecordWords = 276;           // kRecordWords rounded up to 16 bytes
+static_assert(kRecordWords <= kFinalizeRecordWords && kRecordWords % 2 == 0, "record staging");
+
+// The 16 bits of a coarse cell's 4 x 4 voxels (x = 4 cx .. 4 cx + 3, 4 rows) in one ballot of
+// lanes x + 8 (y & 3): bit (x & 3) + 4 (y & 3).
+__device__ __forceinline__ uint32_t coarse_rows(uint32_t ballot, uint32_t cx)
 {
-    __shared__ uint32_t s_nbr[6];
-    __shared__ uint16_t s_vox[512];
-    __shared__ uint32_t s_occ[16];
-    __shared__ int s_min[3], s_max[3];
-    const uint32_t b = blockIdx.x;
-    const uint32_t t = threadIdx.x;
-    const uint32_t y = t & 7, z = t >> 3;
-    const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
-    if (t < 6) {
-        const int dx = t == 0 ? 1 : (t == 1 ? -1 : 0);
-        const int dy = t == 2 ? 1 : (t == 3 ? -1 : 0);
-        const int dz = t == 4 ? 1 : (t == 5 ? -1 : 0);
-        s_nbr[t] = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
-    }
-    if (t < 16) s_occ[t] = 0;
-    if (t < 3) {
-        s_min[t] = 8;
-        s_max[t] = -1;
-    }
-    const uint16_t* own = a.voxels + 512ull * b;
-    for (uint32_t i = t; i < 512; i += 64) s_vox[i] = own[i];
-    __syncthreads();
-    auto nbr_voxel = [&](int d, uint32_t vx, uint32_t vy, uint32_t vz) -> uint32_t {
-        const uint32_t r = s_nbr[d];
-        return r == 0xFFFFFFFFu ? 0u : (uint32_t)a.voxels[512ull * r + vx + 8 * vy + 64 * vz];
-    };
-    uint32_t out_words[4] = {0, 0, 0, 0};
-    uint32_t occupied = 0;
+    const uint32_t b = ballot >> (4 * cx);
+    return (b & 0xFu) | ((b >> 4) & 0xF0u) | ((b >> 8) & 0xF00u) | ((b >> 12) & 0xF000u);
+}
+
+// Whether a pair of values (one u32) / a value holds a non-opaque value other than air.
+__device__ __forceinline__ bool impure(uint32_t w)
+{
+    const uint32_t clear = ~w & 0x80008000u;
+    const uint32_t nonzero = ((w & 0x7FFF7FFFu) + 0x7FFF7FFFu) & 0x80008000u;
+    return (clear & nonzero) != 0;
+}
+__device__ __forceinline__ bool impure(const uint4& v)
+{
+    return impure(v.x) || impure(v.y) || impure(v.z) || impure(v.w);
+}
+__device__ __forceinline__ bool impure16(uint32_t v) { return !(v & kOpaqueBit) && v != 0; }
+
+// The opaque bits of 8 values (bit j = value j).
+__device__ __forceinline__ uint32_t opaque_byte(const uint4& v)
+{
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    uint32_t b = 0;
 #pragma unroll
-    for (uint32_t x = 0; x < 8; ++x) {
-        const uint32_t raw = s_vox[x + 8 * y + 64 * z];
-        const uint32_t v = (raw & kOpaqueBit) ? raw : (raw & 0x1FFu);
-        uint32_t nb[6];
-        nb[0] = x < 7 ? s_vox[(x + 1) + 8 * y + 64 * z] : nbr_voxel(0, 0, y, z);
-        nb[1] = x > 0 ? s_vox[(x - 1) + 8 * y + 64 * z] : nbr_voxel(1, 7, y, z);
-        nb[2] = y < 7 ? s_vox[x + 8 * (y + 1) + 64 * z] : nbr_voxel(2, x, 0, z);
-        nb[3] = y > 0 ? s_vox[x + 8 * (y - 1) + 64 * z] : nbr_voxel(3, x, 7, z);
-        nb[4] = z < 7 ? s_vox[x + 8 * y + 64 * (z + 1)] : nbr_voxel(4, x, y, 0);
-        nb[5] = z > 0 ? s_vox[x + 8 * y + 64 * (z - 1)] : nbr_voxel(5, x, y, 7);
-        uint32_t opaque_count = 0, faces = 0;
-#pragma unroll
-        for (int d = 0; d < 6; ++d) {
-            const bool nop = (nb[d] & kOpaqueBit) != 0;
-            opaque_count += nop ? 1u : 0u;
-            if (!nop && (nb[d] & 0x1FFu) != v) faces |= 1u << d;
+    for (int i = 0; i < 4; ++i) b |= (((w[i] >> 15) & 1u) | ((w[i] >> 30) & 2u)) << (2 * i);
+    return b;
+}
+
+// Bits 0 .. 3 of n to bits 0, 8, 16, 24 (one per row of a mask word).
+__device__ __forceinline__ uint32_t spread_rows(uint32_t n)
+{
+    return (n & 1u) | ((n & 2u) << 7) | ((n & 4u) << 14) | ((n & 8u) << 21);
+}
+
+__global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const FinalizeArgs a)
+{
+    __shared__ __align__(16) uint32_t s_stage[kFinalizeWarps][kFinalizeStageWords];
+    __shared__ __align__(16) uint32_t s_record[kFinalizeWarps][kFinalizeRecordWords];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint16_t* vox = reinterpret_cast<uint16_t*>(s_stage[warp]);  // [512] then faces [6][64]
+    uint16_t* rec16 = reinterpret_cast<uint16_t*>(s_record[warp]);
+    const uint32_t x = lane & 7u, ylo = lane >> 3;
+    const uint32_t fj = lane & 7u, fg = lane >> 3;  // face loads: row fj of face 2 + fg
+    for (uint32_t b = blockIdx.x * kFinalizeWarps + warp; b < a.n; b += gridDim.x * kFinalizeWarps) {
+        const int32_t bx = __ldg(a.keys + 3ull * b), by = __ldg(a.keys + 3ull * b + 1), bz = __ldg(a.keys + 3ull * b + 2);
+        const uint4* own = reinterpret_cast<const uint4*>(a.voxels + 512ull * b);
+        const uint4 v0 = __ldg(own + lane), v1 = __ldg(own + 32 + lane);
+        uint32_t my_nbr = 0xFFFFFFFFu;
+        if (lane < 6) {
+            const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
+            const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
+            const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
+            my_nbr = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
         }
-        const bool alive = opaque_count < 6;
-        const uint32_t result = (v & kOpaqueBit) ? v : (v | (faces << 9));
-        const bool iface = (v & kOpaqueBit) != 0 || faces != 0;
-        if (alive && result != 0 && iface) occupied |= 1u << x;
-        out_words[x >> 1] |= (x & 1) ? (result << 16) : result;
-    }
-    uint32_t* rec = a.records + (uint64_t)b * kRecordWords;
+        const uint32_t nx_pos = __shfl_sync(0xFFFFFFFFu, my_nbr, 0);
+        const uint32_t nx_neg = __shfl_sync(0xFFFFFFFFu, my_nbr, 1);
+        const uint32_t nf = __shfl_sync(0xFFFFFFFFu, my_nbr, 2 + fg);
+        // +-y faces: rows (x, 0 / 7, z = fj); +-z faces: rows (x, y = fj, 0 / 7); 16 bytes each.
+        const uint32_t fq = fg == 0 ? 8 * fj : (fg == 1 ? 8 * fj + 7 : (fg == 2 ? fj : 56 + fj));
+        const uint4 fv = nf == 0xFFFFFFFFu ? make_uint4(0, 0, 0, 0)
+                                           : __ldg(reinterpret_cast<const uint4*>(a.voxels + 512ull * nf) + fq);
+        // +-x faces: (0 / 7, y, z), entry y + 8 z, two per lane.
+        uint16_t xf[4];
 #pragma unroll
-    for (int w = 0; w < 4; ++w) rec[kRecordPayloadWord + 4 * y + 32 * z + w] = out_words[w];
-    if (occupied) {
-        const uint32_t micro_base = ((y & 3) << 2) | ((z & 3) << 4);
-        const uint32_t coarse_yz = ((y >> 2) << 1) | ((z >> 2) << 2);
-        const uint32_t word = micro_base >> 5, bit = micro_base & 31;
-        const uint32_t low = occupied & 0xFu, high = occupied >> 4;
-        if (low) atomicOr(&s_occ[coarse_yz * 2 + word], low << bit);
-        if (high) atomicOr(&s_occ[(coarse_yz | 1u) * 2 + word], high << bit);
-        atomicMin(&s_min[0], __ffs(occupied) - 1);
-        atomicMax(&s_max[0], 31 - __clz(occupied));
-        atomicMin(&s_min[1], (int)y);
-        atomicMax(&s_max[1], (int)y);
-        atomicMin(&s_min[2], (int)z);
-        atomicMax(&s_max[2], (int)z);
-    }
-    __syncthreads();
-    if (t < 16) rec[2 + t] = s_occ[t];
-    if (t == 0) {
-        uint32_t coarse = 0;
-        for (int c = 0; c < 8; ++c)
-            if (s_occ[2 * c] | s_occ[2 * c + 1]) coarse |= 1u << c;
-        uint32_t bounds = 0;
-        if (s_max[0] >= 0)
-            bounds = (uint32_t)s_min[0] | ((uint32_t)s_min[1] << 3) | ((uint32_t)s_min[2] << 6) |
-                     ((uint32_t)s_max[0] << 9) | ((uint32_t)s_max[1] << 12) | ((uint32_t)s_max[2] << 15);
-        const uint32_t gm = (1u << a.group_shift) - 1u;
-        const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << a.group_shift) |
-                             (((uint32_t)bz & gm) << (2 * a.group_shift));
-        rec[0] = (pos & 0xFFFFu) | (coarse << 16);
-        rec[1] = bounds;
+        for (int h = 0; h < 2; ++h) {
+            const uint32_t i = lane + 32 * h;
+            xf[2 * h] = nx_pos == 0xFFFFFFFFu ? (uint16_t)0 : a.voxels[512ull * nx_pos + 8 * i];
+            xf[2 * h + 1] = nx_neg == 0xFFFFFFFFu ? (uint16_t)0 : a.voxels[512ull * nx_neg + 7 + 8 * i];
+        }
+        __syncwarp();  // the previous brick's reads of the staging are done
+        reinterpret_cast<uint4*>(vox)[lane] = v0;
+        reinterpret_cast<uint4*>(vox)[32 + lane] = v1;
+        reinterpret_cast<uint4*>(vox + 512 + 64 * (2 + fg))[fj] = fv;
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            vox[512 + lane + 32 * h] = xf[2 * h];
+            vox[512 + 64 + lane + 32 * h] = xf[2 * h + 1];
+        }
+        __syncwarp();
+        // A clean brick (every value of it and of its six neighbour faces air or opaque) keeps
+        // its raw values as the payload, and a voxel of it is occupied iff it is opaque and not
+        // all six of its neighbours are: shifted masks of the opaque voxels. Other bricks take
+        // the per-voxel rules.
+        const bool dirty = __any_sync(0xFFFFFFFFu, impure(v0) || impure(v1) || impure(fv) || impure16(xf[0]) ||
+                                                       impure16(xf[1]) || impure16(xf[2]) || impure16(xf[3]));
+        // Lane k < 16 ends with word k of the occupied voxels: bit x + 8 (y & 3) for the rows
+        // y = 4 (k & 1) + (0 .. 3) at z = k >> 1.
+        uint32_t my_occ = 0;
+        const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
+        if (!dirty) {
+            // Opaque voxels: lane l holds voxels 8l .. 8l + 7 (v0) and 256 + 8l .. (v1).
+            const uint32_t o0 = opaque_byte(v0), o1 = opaque_byte(v1);
+            uint32_t o = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                const uint32_t src = (4 * lane + i) & 31u;
+                const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, o0, src), t1 = __shfl_sync(0xFFFFFFFFu, o1, src);
+                o |= (lane < 8 ? t0 : t1) << (8 * i);
+            }
+            // Opaque voxels of the faces: x faces by entry y + 8 z; y and z faces one byte per
+            // row (the lane that loaded it).
+            const uint32_t fxp0 = __ballot_sync(0xFFFFFFFFu, xf[0] & kOpaqueBit);
+            const uint32_t fxn0 = __ballot_sync(0xFFFFFFFFu, xf[1] & kOpaqueBit);
+            const uint32_t fxp1 = __ballot_sync(0xFFFFFFFFu, xf[2] & kOpaqueBit);
+            const uint32_t fxn1 = __ballot_sync(0xFFFFFFFFu, xf[3] & kOpaqueBit);
+            const uint32_t fb = opaque_byte(fv);
+            const uint32_t fyp = __shfl_sync(0xFFFFFFFFu, fb, kz), fyn = __shfl_sync(0xFFFFFFFFu, fb, 8 + kz);
+            uint32_t fzp = 0, fzn = 0;
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i) {
+                fzp |= __shfl_sync(0xFFFFFFFFu, fb, 16 + 4 * kyh + i) << (8 * i);
+                fzn |= __shfl_sync(0xFFFFFFFFu, fb, 24 + 4 * kyh + i) << (8 * i);
+            }
+            const uint32_t o_next = __shfl_down_sync(0xFFFFFFFFu, o, 1), o_prev = __shfl_up_sync(0xFFFFFFFFu, o, 1);
+            const uint32_t o_up = __shfl_down_sync(0xFFFFFFFFu, o, 2), o_down = __shfl_up_sync(0xFFFFFFFFu, o, 2);
+            const uint32_t xs = (4 * lane) & 31u;
+            const uint32_t nib_p = ((lane < 8 ? fxp0 : fxp1) >> xs) & 0xFu;
+            const uint32_t nib_n = ((lane < 8 ? fxn0 : fxn1) >> xs) & 0xFu;
+            const uint32_t px = ((o >> 1) & 0x7F7F7F7Fu) | (spread_rows(nib_p) << 7);
+            const uint32_t nx = ((o << 1) & 0xFEFEFEFEu) | spread_rows(nib_n);
+            const uint32_t py = (o >> 8) | ((kyh == 0 ? (o_next & 0xFFu) : fyp) << 24);
+            const uint32_t ny = (o << 8) | (kyh == 1 ? (o_prev >> 24) : fyn);
+            const uint32_t pz = kz < 7 ? o_up : fzp;
+            const uint32_t nz = kz > 0 ? o_down : fzn;
+            my_occ = lane < 16 ? (o & ~(px & nx & py & ny & pz & nz)) : 0u;
+        } else {
+#pragma unroll 2
+            for (uint32_t k = 0; k < 16; ++k) {
+                const uint32_t y = ylo + 4 * (k & 1), z = k >> 1;
+                const uint32_t vi = lane + 32 * k;
+                const uint32_t raw = vox[vi];
+                const uint32_t v = (raw & kOpaqueBit) ? raw : (raw & 0x1FFu);
+                uint32_t nb[6];
+                nb[0] = vox[x < 7 ? vi + 1 : 512 + 0 * 64 + y + 8 * z];
+                nb[1] = vox[x > 0 ? vi - 1 : 512 + 1 * 64 + y + 8 * z];
+                nb[2] = vox[y < 7 ? vi + 8 : 512 + 2 * 64 + x + 8 * z];
+                nb[3] = vox[y > 0 ? vi - 8 : 512 + 3 * 64 + x + 8 * z];
+                nb[4] = vox[z < 7 ? vi + 64 : 512 + 4 * 64 + x + 8 * y];
+                nb[5] = vox[z > 0 ? vi - 64 : 512 + 5 * 64 + x + 8 * y];
+                uint32_t opaque_count = 0, faces = 0;
+#pragma unroll
+                for (int d = 0; d < 6; ++d) {
+                    const bool nop = (nb[d] & kOpaqueBit) != 0;
+                    opaque_count += nop ? 1u : 0u;
+                    if (!nop && (nb[d] & 0x1FFu) != v) faces |= 1u << d;
+                }
+                const uint32_t result = (v & kOpaqueBit) ? v : (v | (faces << 9));
+                const bool iface = (v & kOpaqueBit) != 0 || faces != 0;
+                rec16[2 * kRecordPayloadWord + vi] = (uint16_t)result;
+                const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, opaque_count < 6 && result != 0 && iface);
+                if (lane == k) my_occ = ballot;
+            }
+        }
+        // Occupancy word w = 2 cell + half of coarse cell c = (x >> 2) + 2 (y >> 2) + 4 (z >> 2),
+        // bit (x & 3) + 4 (y & 3) + 16 (z & 3) - 32 half: the lanes of even z join the next z.
+        const uint32_t c0 = coarse_rows(my_occ, 0), c1 = coarse_rows(my_occ, 1);
+        const uint32_t c0_next = __shfl_down_sync(0xFFFFFFFFu, c0, 2), c1_next = __shfl_down_sync(0xFFFFFFFFu, c1, 2);
+        const uint32_t cell_yz = 2 * kyh + 4 * (kz >> 2), half = (kz & 3) >> 1;
+        if (lane < 16 && (kz & 1) == 0) {
+            s_record[warp][2 + 2 * cell_yz + half] = c0 | (c0_next << 16);
+            s_record[warp][2 + 2 * (cell_yz + 1) + half] = c1 | (c1_next << 16);
+        }
+        const uint32_t row_any = ((my_occ & 0xFFu) ? 1u : 0u) | ((my_occ & 0xFF00u) ? 2u : 0u) |
+                                 ((my_occ & 0xFF0000u) ? 4u : 0u) | ((my_occ & 0xFF000000u) ? 8u : 0u);
+        const uint32_t xmask = __reduce_or_sync(0xFFFFFFFFu, (my_occ | (my_occ >> 8) | (my_occ >> 16) | (my_occ >> 24)) & 0xFFu);
+        const uint32_t ymask = __reduce_or_sync(0xFFFFFFFFu, row_any << (4 * kyh));
+        const uint32_t zmask = __reduce_or_sync(0xFFFFFFFFu, (my_occ ? 1u : 0u) << kz);
+        const uint32_t coarse = __reduce_or_sync(0xFFFFFFFFu, ((c0 ? 1u : 0u) << cell_yz) | ((c1 ? 1u : 0u) << (cell_yz + 1)));
+        if (lane == 0) {
+            uint32_t bounds = 0;
+            if (xmask) {
+                const uint32_t x0 = __ffs(xmask) - 1, y0 = __ffs(ymask) - 1, z0 = __ffs(zmask) - 1;
+                const uint32_t x1 = 31 - __clz(xmask), y1 = 31 - __clz(ymask), z1 = 31 - __clz(zmask);
+                bounds = x0 | (y0 << 3) | (z0 << 6) | (x1 << 9) | (y1 << 12) | (z1 << 15);
+            }
+            const uint32_t gm = (1u << a.group_shift) - 1u;
+            const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << a.group_shift) |
+                                 (((uint32_t)bz & gm) << (2 * a.group_shift));
+            s_record[warp][0] = (pos & 0xFFFFu) | (coarse << 16);
+            s_record[warp][1] = bounds;
+        }
+        __syncwarp();
+        // The record: header words (0 .. 17) from the staging; the payload from the staging, or
+        // the raw values of a clean brick.
+        uint2* dst = reinterpret_cast<uint2*>(a.records + (uint64_t)b * kRecordWords);
+        const uint2* src = reinterpret_cast<const uint2*>(s_record[warp]);
+        if (lane < kRecordPayloadWord / 2) dst[lane] = src[lane];
+        if (!dirty) {
+            dst[kRecordPayloadWord / 2 + 2 * lane] = make_uint2(v0.x, v0.y);
+            dst[kRecordPayloadWord / 2 + 2 * lane + 1] = make_uint2(v0.z, v0.w);
+            dst[kRecordPayloadWord / 2 + 64 + 2 * lane] = make_uint2(v1.x, v1.y);
+            dst[kRecordPayloadWord / 2 + 64 + 2 * lane + 1] = make_uint2(v1.z, v1.w);
+        } else {
+#pragma unroll
+            for (uint32_t i = 0; i < 4; ++i)
+                dst[kRecordPayloadWord / 2 + lane + 32 * i] = src[kRecordPayloadWord / 2 + lane + 32 * i];
+        }
     }
 }
 
@@ -535,12 +659,32 @@ __global__ void __launch_bounds__(128) light_write_kernel(const LightWriteArgs w
 
 uint32_t blocks_for(uint64_t n, uint32_t per) { return (uint32_t)std::max<uint64_t>(1, (n + per - 1) / per); }
 
-template <typename T>
-cudaError_t alloc(T*& p, uint64_t count)
+// Resident CTAs of finalize_kernel on every SM of the current device, at most one warp per brick.
+uint32_t finalize_grid(uint32_t n)
 {
+    static int per_sm = 0, sms = 0;
+    if (per_sm == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finalize_kernel, kFinalizeWarps * 32, 0);
+        per_sm = std::max(per_sm, 1);
+        sms = std::max(sms, 1);
+    }
+    return std::min<uint32_t>(blocks_for(n, kFinalizeWarps), (uint32_t)(per_sm * sms));
+}
+
+template <typename T>
+cudaError_t alloc(T*& p, uint64_t& capacity, uint64_t count)
+{
+    count = std::max<uint64_t>(count, 1);
+    if (p && count <= capacity) return cudaSuccess;
     if (p) cudaFree(p);
     p = nullptr;
-    return cudaMalloc(&p, std::max<uint64_t>(count, 1) * sizeof(T));
+    capacity = 0;
+    CX_TRY(cudaMalloc(&p, count * sizeof(T)));
+    capacity = count;
+    return cudaSuccess;
 }
 
 cudaError_t run_scan(bool max_op, const uint32_t* in, uint32_t* out, uint32_t count, uint32_t* scratch,
@@ -597,9 +741,31 @@ void scene_release(DeviceScene& s)
     s = DeviceScene();
 }
 
+cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream)
+{
+    if (!s.status) CX_TRY(cudaMalloc(&s.status, 64));
+    CX_TRY(cudaMemsetAsync(s.status, 0, 64, stream));
+    CX_TRY(alloc(s.keys, s.capacity.keys, 3ull * n));
+    CX_TRY(alloc(s.voxels, s.capacity.voxels, 512ull * n));
+    CX_TRY(alloc(s.power, s.capacity.power, n));
+    CX_TRY(alloc(s.albedo, s.capacity.albedo, kMaterialSlots * 3));
+    return cudaSuccess;
+}
+
 cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t n, const int32_t* keys,
                         const uint16_t* voxels, const float* power, const float* albedo, cudaStream_t stream,
                         uint32_t* device_status_out)
+{
+    CX_TRY(scene_alloc_inputs(s, n, stream));
+    CX_TRY(cudaMemcpyAsync(s.keys, keys, 12ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.voxels, voxels, 1024ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.power, power, 4ull * n, cudaMemcpyHostToDevice, stream));
+    CX_TRY(cudaMemcpyAsync(s.albedo, albedo, 12ull * kMaterialSlots, cudaMemcpyHostToDevice, stream));
+    return scene_build_device(s, grid, group_shift, n, stream, device_status_out);
+}
+
+cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t n,
+                               cudaStream_t stream, uint32_t* device_status_out)
 {
     for (int k = 0; k < 3; ++k) s.grid[k] = grid[k];
     s.group_shift = group_shift;
@@ -607,24 +773,12 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
     for (int k = 0; k < 3; ++k) s.groups[k] = (grid[k] + gm) >> group_shift;
     s.group_count = s.groups[0] * s.groups[1] * s.groups[2];
     s.brick_count = n;
-    if (!s.status) CX_TRY(cudaMalloc(&s.status, 64));
-    CX_TRY(cudaMemsetAsync(s.status, 0, 64, stream));
-
-    // Inputs.
-    CX_TRY(alloc(s.keys, 3ull * n));
-    CX_TRY(alloc(s.voxels, 512ull * n));
-    CX_TRY(alloc(s.power, n));
-    CX_TRY(alloc(s.albedo, kMaterialSlots * 3));
-    CX_TRY(cudaMemcpyAsync(s.keys, keys, 12ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.voxels, voxels, 1024ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.power, power, 4ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.albedo, albedo, 12ull * kMaterialSlots, cudaMemcpyHostToDevice, stream));
 
     // Scratch: 8 arrays of n words, 6 n words of family counts, the sort scratch, scan states.
     const uint64_t sort_words = sort_scratch_words(std::max(n, 1u));
     const uint64_t need = 14ull * std::max(n, 1u) + sort_words + 2 + blocks_for(std::max(n, 1u), kScanTile) + 64;
     if (need > s.scratch_words) {
-        CX_TRY(alloc(s.scratch, need));
+        CX_TRY(alloc(s.scratch, s.capacity.scratch, need));
         s.scratch_words = need;
     }
     uint32_t* w = s.scratch;
@@ -643,7 +797,7 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
     // Hash table.
     s.hash_capacity = std::max(2u * n, 2u);
     s.hash_slot_count = s.hash_capacity + n + 1;
-    CX_TRY(alloc(s.hash_slots, s.hash_slot_count));
+    CX_TRY(alloc(s.hash_slots, s.capacity.hash_slots, s.hash_slot_count));
     CX_TRY(cudaMemsetAsync(s.hash_slots, 0, 16ull * s.hash_slot_count, stream));
     uint32_t* d_max_probe = s.status + 4;
     if (n > 0) {
@@ -658,18 +812,17 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
     }
     // Bitmap.
     const uint64_t cells = (uint64_t)grid[0] * grid[1] * grid[2];
-    CX_TRY(alloc(s.bitmap, (cells + 31) / 32));
+    CX_TRY(alloc(s.bitmap, s.capacity.bitmap, (cells + 31) / 32));
     CX_TRY(cudaMemsetAsync(s.bitmap, 0, 4 * ((cells + 31) / 32), stream));
     if (n > 0) bitmap_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, grid[0], grid[1], s.bitmap);
     CX_TRY(cudaMemcpyAsync(&s.hash_max_probe, d_max_probe, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
 
     // Records.
-    CX_TRY(alloc(s.records, (uint64_t)kRecordWords * n));
-    CX_TRY(cudaMemsetAsync(s.records, 0, 4ull * kRecordWords * n, stream));
+    CX_TRY(alloc(s.records, s.capacity.records, (uint64_t)kRecordWords * n));
     if (n > 0) {
         FinalizeArgs fa{s.keys, s.voxels, n, group_shift, s.hash_slots, s.hash_capacity, s.hash_max_probe, s.records};
-        finalize_kernel<<<n, 64, 0, stream>>>(fa);
+        finalize_kernel<<<finalize_grid(n), kFinalizeWarps * 32, 0, stream>>>(fa);
     }
 
     // Light records.
@@ -685,12 +838,12 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
     CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
     s.light_count = m;
-    CX_TRY(alloc(s.group_rows, 8ull * s.group_count));
+    CX_TRY(alloc(s.group_rows, s.capacity.group_rows, 8ull * s.group_count));
     CX_TRY(cudaMemsetAsync(s.group_rows, 0, 32ull * s.group_count, stream));
-    CX_TRY(alloc(s.light_headers, m));
-    CX_TRY(alloc(s.light_group, m));
-    CX_TRY(alloc(s.light_entry, m));
-    CX_TRY(alloc(s.light_brick, m));
+    CX_TRY(alloc(s.light_headers, s.capacity.light_headers, m));
+    CX_TRY(alloc(s.light_group, s.capacity.light_group, m));
+    CX_TRY(alloc(s.light_entry, s.capacity.light_entry, m));
+    CX_TRY(alloc(s.light_brick, s.capacity.light_brick, m));
     std::vector<GroupFrame> frames(s.group_count);
     for (uint32_t g = 0; g < s.group_count; ++g) {
         const uint32_t gx = g % s.groups[0], gy = (g / s.groups[0]) % s.groups[1], gz = g / (s.groups[0] * s.groups[1]);
@@ -702,7 +855,7 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
         f.rot[0] = f.rot[4] = f.rot[8] = 1.0f;
         frames[g] = f;
     }
-    CX_TRY(alloc(s.frames, s.group_count));
+    CX_TRY(alloc(s.frames, s.capacity.frames, s.group_count));
     CX_TRY(cudaMemcpyAsync(s.frames, frames.data(), sizeof(GroupFrame) * s.group_count, cudaMemcpyHostToDevice, stream));
     uint32_t total_units = 0;
     if (m > 0) {
@@ -721,14 +874,14 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
         CX_TRY(cudaMemcpyAsync(&total_units, d_total, 4, cudaMemcpyDeviceToHost, stream));
         CX_TRY(cudaStreamSynchronize(stream));
         s.heap_words = 4 * (1 + total_units);
-        CX_TRY(alloc(s.heap, s.heap_words));
+        CX_TRY(alloc(s.heap, s.capacity.heap, s.heap_words));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
         LightWriteArgs wa{la, lkeys, lbricks, m, counts6, units, offsets, group_start, total_units, s.heap,
                           s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick};
         light_write_kernel<<<blocks_for(32ull * m, 128), 128, 0, stream>>>(wa);
     } else {
         s.heap_words = 4;
-        CX_TRY(alloc(s.heap, 4));
+        CX_TRY(alloc(s.heap, s.capacity.heap, 4));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 16, stream));
     }
 

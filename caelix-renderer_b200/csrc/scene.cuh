@@ -79,6 +79,12 @@ struct DeviceScene
     LightBvhBuffers tree;
     uint32_t tree_capacity = 0;
     uint32_t* status = nullptr;  // device status word of the build
+    // Element capacities of the buffers above: a rebuild reallocates a buffer only to grow it.
+    struct
+    {
+        uint64_t keys, voxels, power, albedo, scratch, hash_slots, bitmap, records, group_rows, light_headers,
+            light_group, light_entry, light_brick, frames, heap;
+    } capacity{};
 };
 
 // Builds the device scene from host bricks (keys in increasing linear brick index, every
@@ -87,6 +93,24 @@ struct DeviceScene
 cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
                         const int32_t* keys, const uint16_t* voxels, const float* power, const float* albedo,
                         cudaStream_t stream, uint32_t* device_status_out);
+// The two halves of scene_build for inputs produced on the device: scene_alloc_inputs sizes
+// s.keys, s.voxels, s.power, s.albedo for n bricks (and clears the status words); the caller fills
+// them (keys in increasing linear brick index); scene_build_device builds everything else.
+cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream);
+cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
+                               cudaStream_t stream, uint32_t* device_status_out);
+
+// ---- device-resident brick staging (staging.cu) ----
+// Copies brick src_index[j] of an upload (src, device, 512 values per brick) to staging slot
+// slots[j], j < count (the slots distinct).
+cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, const uint32_t* slots, uint32_t count,
+                            uint16_t* stage_voxels, cudaStream_t stream);
+// The staging slots in increasing linear brick index of `grid`, gathered into the scene's input
+// arrays (power zero when `power` is null). `scratch`: staging_sort_words(n) words.
+uint64_t staging_sort_words(uint32_t n);
+cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
+                           uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
+                           uint16_t* voxels, float* power, cudaStream_t stream);
 // Rebuilds the light tree of a built scene from its light records (asynchronous on `stream`, no
 // allocation: the tree buffers were sized by scene_build). The reference's per-flush light BVH
 // rebuild (lib/src/light/light_tree_record.cpp:230-302, RecordTree).

@@ -1,0 +1,90 @@
+// Device-resident brick staging: the bricks a host uploads stay on the device in upload slots, so
+// a flush sorts and gathers them on the device instead of re-sending every brick. Replaces, for
+// the path here, the reference's staging of uploaded records (lib/src/scene/scene_flush.cpp:797-857:
+// uploaded records copied to the record pages on the device).
+#include <algorithm>
+
+#include "radix_sort.cuh"
+#include "scene.cuh"
+
+namespace cx {
+
+namespace {
+
+constexpr uint32_t kStageThreads = 256;
+
+// One uint4 (8 voxels) per thread: brick src_index[j] of the upload to staging slot slots[j].
+__global__ void __launch_bounds__(kStageThreads)
+    staging_scatter_kernel(const uint4* __restrict__ src, const uint32_t* __restrict__ src_index,
+                           const uint32_t* __restrict__ slots, uint32_t count, uint4* __restrict__ stage)
+{
+    const uint64_t u = (uint64_t)blockIdx.x * kStageThreads + threadIdx.x;
+    if (u >= 64ull * count) return;
+    const uint32_t j = (uint32_t)(u >> 6), w = (uint32_t)(u & 63u);
+    stage[64ull * __ldg(slots + j) + w] = __ldg(src + 64ull * __ldg(src_index + j) + w);
+}
+
+__global__ void __launch_bounds__(kStageThreads)
+    staging_linear_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t gx, uint32_t gy,
+                          uint32_t* __restrict__ lin)
+{
+    const uint32_t s = blockIdx.x * kStageThreads + threadIdx.x;
+    if (s >= n) return;
+    lin[s] = (uint32_t)keys[3 * s] + gx * ((uint32_t)keys[3 * s + 1] + gy * (uint32_t)keys[3 * s + 2]);
+}
+
+__global__ void __launch_bounds__(kStageThreads)
+    staging_gather_kernel(const uint32_t* __restrict__ order, uint32_t n, const int32_t* __restrict__ stage_keys,
+                          const uint4* __restrict__ stage_voxels, const float* __restrict__ slot_power,
+                          int32_t* __restrict__ keys, uint4* __restrict__ voxels, float* __restrict__ power)
+{
+    const uint64_t u = (uint64_t)blockIdx.x * kStageThreads + threadIdx.x;
+    if (u >= 64ull * n) return;
+    const uint32_t i = (uint32_t)(u >> 6), w = (uint32_t)(u & 63u);
+    const uint32_t s = __ldg(order + i);
+    voxels[u] = __ldg(stage_voxels + 64ull * s + w);
+    if (w < 3) keys[3ull * i + w] = __ldg(stage_keys + 3ull * s + w);
+    if (w == 3) power[i] = slot_power ? __ldg(slot_power + s) : 0.0f;
+}
+
+uint32_t blocks(uint64_t items) { return (uint32_t)((items + kStageThreads - 1) / kStageThreads); }
+
+}  // namespace
+
+cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, const uint32_t* slots, uint32_t count,
+                            uint16_t* stage_voxels, cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    staging_scatter_kernel<<<blocks(64ull * count), kStageThreads, 0, stream>>>(
+        reinterpret_cast<const uint4*>(src), src_index, slots, count, reinterpret_cast<uint4*>(stage_voxels));
+    return cudaGetLastError();
+}
+
+uint64_t staging_sort_words(uint32_t n)
+{
+    const uint64_t c = std::max(n, 1u);
+    return 4 * c + sort_scratch_words((uint32_t)c);
+}
+
+cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
+                           uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
+                           uint16_t* voxels, float* power, cudaStream_t stream)
+{
+    if (n == 0) return cudaSuccess;
+    uint32_t* lin = scratch;
+    uint32_t* order = scratch + n;
+    uint32_t* lin_alt = scratch + 2ull * n;
+    uint32_t* order_alt = scratch + 3ull * n;
+    uint32_t* sortw = scratch + 4ull * n;
+    staging_linear_kernel<<<blocks(n), kStageThreads, 0, stream>>>(stage_keys, n, grid[0], grid[1], lin);
+    CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n), stream));
+    radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, 148 * 4), stream);
+    // A stable sort of the linear indices (unique: one slot per key), values = the slots.
+    onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream);
+    staging_gather_kernel<<<blocks(64ull * n), kStageThreads, 0, stream>>>(
+        order, n, stage_keys, reinterpret_cast<const uint4*>(stage_voxels), slot_power, keys,
+        reinterpret_cast<uint4*>(voxels), power);
+    return cudaGetLastError();
+}
+
+}  // namespace cx

@@ -802,7 +802,7 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
 {
     const uint32_t block = (h->attrib >> 16) & 0xFFFFu;
     emission_of(c, h->record, block, emission);
-    const float* a = c->albedo + 3 * (block & 0x7FFFu);
+    const float* a = c->albedo + 3 * (block & 0x7Fu); /* the material id of the 128-row table */
     albedo[0] = a[0];
     albedo[1] = a[1];
     albedo[2] = a[2];

@@ -1,0 +1,102 @@
+"""Device-resident brick staging: bricks uploaded in pieces, in any order, with overwrites and
+repeated keys inside one upload, give the same scene as one upload of the final bricks (bit-exact
+against the oracle), and a flush after edits rebuilds the edited scene."""
+import numpy as np
+import pytest
+
+import oracle_lib
+from caelix_b200 import workloads
+from test_trace_gpu import assert_scene_equal, assert_radiance_close, render_both
+
+pytestmark = pytest.mark.gpu
+
+
+def incremental_scene(cuda_device, vs, rng, pieces=5):
+    """The bricks of `vs` uploaded shuffled in `pieces` calls; a third of them first with other
+    voxels, some repeated inside a call (the last copy right); half the power set before the
+    upload of its brick, half after."""
+    import caelix_b200
+
+    s = caelix_b200.Scene(cuda_device, vs.group_shift)
+    n = vs.brick_count
+    emissive = np.nonzero(vs.power > 0)[0]
+    early = emissive[: len(emissive) // 2]
+    if len(early):
+        s.set_brick_power(vs.keys[early], vs.power[early])
+    junk = rng.choice(n, size=n // 3, replace=False)
+    s.upload_bricks(vs.keys[junk], rng.integers(0, 1 << 16, size=(len(junk), 512), dtype=np.uint16))
+    order = rng.permutation(n)
+    for part in np.array_split(order, pieces):
+        if len(part) == 0:
+            continue
+        rep = part[rng.random(len(part)) < 0.1]
+        keys = np.concatenate([vs.keys[rep], vs.keys[part]])
+        vox = np.concatenate([np.full((len(rep), 512), 0x8003, np.uint16), vs.voxels[part]])
+        s.upload_bricks(keys, vox)
+    late = emissive[len(emissive) // 2:]
+    if len(late):
+        s.set_brick_power(vs.keys[late], vs.power[late])
+    s.set_albedo(vs.albedo)
+    s.flush()
+    return s
+
+
+@pytest.mark.parametrize("seed", [2, 8])
+def test_incremental_uploads_equal_one_upload(cuda_device, oracle, seed):
+    vs = workloads.noise_world(grid_bricks=(8, 6, 10), brick_occupancy=0.45, emissive_fraction=0.08, seed=seed)
+    scene = incremental_scene(cuda_device, vs, np.random.default_rng(seed))
+    osc = oracle_lib.OracleScene(oracle, vs)
+    assert_scene_equal(scene, osc, vs)
+    gpu, ref, st, rays = render_both(cuda_device, scene, osc, vs, 96, 64, spp=2, bounces=4, seed=seed)
+    assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+    assert_radiance_close(gpu, ref)
+    scene.close()
+
+
+def test_config2_incremental_then_edit(cuda_device, oracle):
+    """The 4,096-brick scene uploaded in pieces, flushed, then a tenth of its bricks rewritten,
+    new bricks added (the grid grows) and a flush: both states equal the oracle's."""
+    vs = workloads.noise_world()
+    rng = np.random.default_rng(11)
+    scene = incremental_scene(cuda_device, vs, rng, pieces=7)
+    assert_scene_equal(scene, oracle_lib.OracleScene(oracle, vs), vs)
+
+    edit = rng.choice(vs.brick_count, size=vs.brick_count // 10, replace=False)
+    voxels = vs.voxels.copy()
+    voxels[edit] = np.where(rng.random((len(edit), 512)) < 0.5, 0x8002, 0).astype(np.uint16)
+    gx, gy, gz = vs.grid
+    extra = np.array([[gx, 0, 0], [gx + 1, gy, 2], [0, 0, gz + 3]], np.int32)
+    extra_vox = np.full((3, 512), 0x8001, np.uint16)
+    keys = np.concatenate([vs.keys, extra])
+    allvox = np.concatenate([voxels, extra_vox])
+    lin = keys[:, 0] + (gx + 2) * (keys[:, 1] + (gy + 1) * keys[:, 2].astype(np.int64))
+    o = np.argsort(lin, kind="stable")
+    power = np.concatenate([vs.power, np.zeros(3, np.float32)])
+    edited = workloads.VoxelScene((gx + 2, gy + 1, gz + 4), keys[o], allvox[o], power[o], vs.albedo, vs.camera,
+                                  vs.group_shift)
+    scene.upload_bricks(np.concatenate([vs.keys[edit], extra]), np.concatenate([voxels[edit], extra_vox]))
+    scene.flush()
+    assert_scene_equal(scene, oracle_lib.OracleScene(oracle, edited), edited)
+    scene.close()
+
+
+def test_empty_and_power_only_flushes(cuda_device, oracle):
+    """A scene flushed with no bricks; then bricks; then only a power change (a full rebuild of
+    the light records from the staged bricks)."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(6, 6, 6), brick_occupancy=0.5, emissive_fraction=0.1, seed=4)
+    s = caelix_b200.Scene(cuda_device, vs.group_shift)
+    s.flush()
+    assert s.view().brick_count == 0
+    s.upload_bricks(vs.keys, vs.voxels)
+    s.set_albedo(vs.albedo)
+    s.flush()
+    dark = workloads.VoxelScene(vs.grid, vs.keys, vs.voxels, np.zeros_like(vs.power), vs.albedo, vs.camera,
+                                vs.group_shift)
+    assert_scene_equal(s, oracle_lib.OracleScene(oracle, dark), dark)
+    emissive = vs.power > 0
+    s.set_brick_power(vs.keys[emissive], vs.power[emissive])
+    s.flush()
+    assert_scene_equal(s, oracle_lib.OracleScene(oracle, vs), vs)
+    s.close()

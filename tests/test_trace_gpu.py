@@ -123,6 +123,26 @@ def test_single_brick_and_edges(cuda_device, oracle):
     scene.close()
 
 
+def test_scene_with_non_opaque_values(cuda_device, oracle):
+    """Bricks holding non-opaque values other than air (finalize's per-voxel rules: face bits of
+    differing neighbours) next to bricks of air and opaque values only (its mask path)."""
+    vs = workloads.noise_world(grid_bricks=(8, 6, 10), brick_occupancy=0.45, emissive_fraction=0.08, seed=6)
+    rng = np.random.default_rng(6)
+    vox = vs.voxels.copy()
+    mixed = rng.random(vs.brick_count) < 0.3
+    cells = rng.random((vs.brick_count, 512)) < 0.2
+    values = rng.integers(1, 0x8000, size=(vs.brick_count, 512)).astype(np.uint16)
+    pick = mixed[:, None] & cells & (vox == 0)
+    vox[pick] = values[pick]
+    vs = workloads.VoxelScene(vs.grid, vs.keys, vox, vs.power, vs.albedo, vs.camera, vs.group_shift)
+    scene, osc = build_both(cuda_device, oracle, vs)
+    assert_scene_equal(scene, osc, vs)
+    gpu, ref, st, rays = render_both(cuda_device, scene, osc, vs, 96, 64, spp=2, bounces=4, seed=6)
+    assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+    assert_radiance_close(gpu, ref)
+    scene.close()
+
+
 def test_render_is_deterministic(cuda_device, oracle):
     import torch
 
