@@ -42,8 +42,19 @@ __global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __
     }
 }
 
+// Position p of tile element k, two 16-bit positions per register (a tile holds at most 4096).
+template <int KPT>
+struct TilePositions
+{
+    uint32_t w[KPT / 2];
+    __device__ __forceinline__ uint32_t get(int k) const { return (w[k >> 1] >> (16 * (k & 1))) & 0xFFFFu; }
+    __device__ __forceinline__ void add(int k, uint32_t v) { w[k >> 1] += v << (16 * (k & 1)); }
+};
+
 // One onesweep pass over a tile of 256 * KPT elements. Phases:
-//   1. keys (warp-striped, coalesced) -> digits -> stable rank inside the warp (__match_any_sync);
+//   1. keys (warp-striped, coalesced) -> digits -> stable rank inside the warp: the lanes of
+//      equal digits from eight ballots, the warp's running count of the digit from one shared
+//      atomic of the lowest such lane;
 //   2. per-digit warp offsets and tile counts; the tile's counts are published at once (the
 //      look-back of later tiles can proceed), then the keys go to the shared staging area in
 //      tile-sorted order (their key registers are free from here on);
@@ -51,7 +62,7 @@ __global__ void __launch_bounds__(256) radix_histogram_kernel(const uint32_t* __
 //   4. values (and, on the gathering pass, the 48-byte rows) are staged by the same positions and
 //      the tile is written out in runs per digit.
 template <int KPT>
-__global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const SortPass a)
+__global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const SortPass a)
 {
     constexpr int kTile = kSortThreads * KPT;
     __shared__ uint32_t s_tile;
@@ -75,7 +86,9 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
 
     // Phase 1.
     uint32_t key[KPT];
-    uint32_t pos[KPT];  // rank in the warp, then position in the tile
+    TilePositions<KPT> pos;  // rank in the warp, then position in the tile
+#pragma unroll
+    for (int k = 0; k < KPT / 2; ++k) pos.w[k] = 0;
 #pragma unroll
     for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
@@ -85,15 +98,19 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
 #pragma unroll
     for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
-        const uint32_t digit = i < a.n ? (key[k] >> a.shift) & 255u : 256u + lane;  // invalid: alone
-        const uint32_t peers = __match_any_sync(0xFFFFFFFFu, digit);
+        const bool valid = i < a.n;
+        const uint32_t digit = (key[k] >> a.shift) & 255u;
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);  // invalid lanes have no peers
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, (digit >> b) & 1u);
+            peers &= ((digit >> b) & 1u) ? m : ~m;
+        }
         const uint32_t before = __popc(peers & lt);
         uint32_t running = 0;
-        if (digit < 256u) running = s_warp_counts[warp][digit];
-        pos[k] = running + before;
-        __syncwarp();
-        if (digit < 256u && before == 0) s_warp_counts[warp][digit] = running + __popc(peers);
-        __syncwarp();
+        if (valid && before == 0) running = atomicAdd(&s_warp_counts[warp][digit], __popc(peers));
+        running = __shfl_sync(0xFFFFFFFFu, running, valid ? __ffs(peers) - 1 : lane);
+        pos.add(k, running + before);
     }
     __syncthreads();
 
@@ -117,8 +134,8 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
         const uint32_t i = warp_base + k * 32u + lane;
         if (i < a.n) {
             const uint32_t digit = (key[k] >> a.shift) & 255u;
-            pos[k] += s_local[digit] + s_warp_counts[warp][digit];
-            s_keys[pos[k]] = key[k];
+            pos.add(k, s_local[digit] + s_warp_counts[warp][digit]);
+            s_keys[pos.get(k)] = key[k];
         }
     }
 
@@ -150,7 +167,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) onesweep_pass_kernel(const So
 #pragma unroll
     for (int k = 0; k < KPT; ++k) {
         const uint32_t i = warp_base + k * 32u + lane;
-        if (i < a.n) s_values[pos[k]] = a.values_in ? __ldg(a.values_in + i) : i;
+        if (i < a.n) s_values[pos.get(k)] = a.values_in ? __ldg(a.values_in + i) : i;
     }
     __syncthreads();
     const uint32_t count = a.n - base < (uint32_t)kTile ? a.n - base : (uint32_t)kTile;

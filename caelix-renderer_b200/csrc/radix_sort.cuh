@@ -9,7 +9,8 @@
 //   * the digit counts of all four passes come from one upsweep (the caller's key producer, or
 //     radix_histogram_kernel), so a pass only needs its own 256 global counts;
 //   * a CTA takes the next tile id from an atomic counter, loads a tile of keys warp-striped
-//     (coalesced 128-byte rows), ranks them stably inside each warp with __match_any_sync peers,
+//     (coalesced 128-byte rows), ranks them stably inside each warp (the lanes of equal digits
+//     from eight ballots, the warp's running digit count from one shared atomic per digit group),
 //     and publishes its per-digit counts in the tile status words;
 //   * the per-digit exclusive prefix over earlier tiles comes from a decoupled look-back over
 //     those status words (one thread per digit, bounded spin: a timeout sets a status bit instead
