@@ -1,7 +1,7 @@
 #!/usr/bin/env python3
 """Benchmark of the scene-flush / trace hot path on B200 (one JSON line on stdout, rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload trace|build|batch]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--workload trace|build|batch|flush]
 
 Workloads (seeded synthetic inputs with the shapes of the benchmark configurations; no dataset):
   trace   (default, the headline) the plain brick-DDA trace: a 128^3-voxel world of 16^3 bricks,
@@ -16,6 +16,8 @@ Workloads (seeded synthetic inputs with the shapes of the benchmark configuratio
   batch   64 scenes (brick counts log-uniform in [1k, 500k], square viewports 256/512/1024, 2 spp,
           4 bounces): every scene's light-tree rebuild + the trace of every view as one CUDA graph
           launch, against the same work one scene at a time through the plain C ABI.
+  flush   the scene flush of the 2M-brick world: the incremental flush after re-uploading 1 % of
+          the bricks (value, ms), the first flush, a full rebuild and a light-tree-only flush.
 The trace line carries the other measurements as objects: `build` (the 4M-record build with its
 roofline and stage times, and the 4,096-record plain build in ms), `large` (the 2M-brick world at
 1920 x 1080, 4 spp, 6 bounces: flush and frame), `adjoint` (256 x 256, 8 spp, 3 bounces: forward
@@ -569,6 +571,81 @@ def measure_large(args, world, local, dev, stream, flush):
     return result
 
 
+# Algorithmic bytes per brick of a full flush: slot sort (12 + 4 + 68), gather (1040 read + 1040
+# write), hash build (~150), finalize (1024 + 6 x 128 faces read, 1096 written).
+FLUSH_BYTES_PER_BRICK = 84 + 2080 + 150 + 2888
+
+
+def measure_flush(args, world, local, dev, stream):
+    """The scene flush on the large world (`--flush-bricks` occupied bricks of the 256 x 256 x 64
+    brick grid, 5 % of them emissive): the first flush after the upload (a full build from the
+    device staging: slot sort and gather, hash table, bitmap, records, light records, light tree);
+    per step an edit of 1 % of the bricks (their values uploaded again) and its flush (incremental:
+    the edited bricks and their neighbours finalized again, light records and light tree rebuilt);
+    then a light-options change (the light tree alone) and a full rebuild (a new brick)."""
+    import numpy as np
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    nb = args.flush_bricks
+    vs = workloads.noise_world_large(occupied_bricks=nb, emissive_bricks=max(1, nb // 20))
+    scene = caelix_b200.Scene(dev, vs.group_shift)
+    renderer = caelix_b200.Renderer(dev, scene)
+    sptr = stream.cuda_stream
+    t0 = time.perf_counter()
+    scene.upload_bricks(vs.keys, vs.voxels)
+    upload_s = time.perf_counter() - t0
+    em = vs.power > 0
+    scene.set_brick_power(vs.keys[em], vs.power[em])
+    scene.set_albedo(vs.albedo)
+    scene.flush(sptr)
+    first_ms = float(renderer.timings().flush_ms)
+    rng = np.random.default_rng(5)
+    edit_ms, edit_upload_s = [], []
+    for k in range(args.warmup + args.steps):
+        edit = rng.choice(vs.brick_count, size=max(1, vs.brick_count // 100), replace=False)
+        t0 = time.perf_counter()
+        scene.upload_bricks(vs.keys[edit], vs.voxels[edit])
+        up = time.perf_counter() - t0
+        scene.flush(sptr)
+        if k >= args.warmup:
+            edit_ms.append(float(renderer.timings().flush_ms))
+            edit_upload_s.append(up)
+    scene.set_light_options(min_emission=20.0)
+    scene.flush(sptr)
+    tree_ms = float(renderer.timings().flush_ms)
+    # A brick at the first free cell of the grid: the key set changes, so the flush rebuilds all.
+    gx, gy, gz = vs.grid
+    lin = vs.keys[:, 0].astype(np.int64) + gx * (vs.keys[:, 1] + gy * vs.keys[:, 2].astype(np.int64))
+    free = np.setdiff1d(np.arange(min(gx * gy * gz, len(lin) + 1)), lin)[0]
+    key = np.array([[free % gx, (free // gx) % gy, free // (gx * gy)]], np.int32)
+    scene.upload_bricks(key, np.full((1, 512), 0x8001, np.uint16))
+    scene.flush(sptr)
+    full_ms = float(renderer.timings().flush_ms)
+    renderer.close()
+    scene.close()
+    ms = max_over_ranks(float(np.mean(edit_ms)), world)
+    full = max_over_ranks(full_ms, world)
+    achieved = vs.brick_count * FLUSH_BYTES_PER_BRICK / (full / 1e3) / 1e9
+    peak, peak_kind = measured_peaks()
+    return {
+        "workload": f"scene flush of the 256x256x64-brick world with {vs.brick_count} occupied bricks "
+                    f"({int(em.sum())} emissive): incremental flush after re-uploading 1% of the bricks",
+        "bricks": int(vs.brick_count),
+        "edit_bricks": int(max(1, vs.brick_count // 100)),
+        "edit_flush_ms": ms,
+        "edit_upload_s": float(np.mean(edit_upload_s)),
+        "first_flush_ms": first_ms,
+        "full_rebuild_ms": full,
+        "light_tree_flush_ms": tree_ms,
+        "upload_s": upload_s,
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
+                     "kernel": f"the full rebuild ({FLUSH_BYTES_PER_BRICK} algorithmic bytes per brick)"},
+    }
+
+
 ADJ_W = ADJ_H = 256
 ADJ_SPP = 8
 ADJ_BOUNCES = 3
@@ -819,6 +896,18 @@ def run_ours(args, world, rank, local):
             print(json.dumps(line), flush=True)
         dev.close()
         return
+    if args.workload == "flush":
+        fl = measure_flush(args, world, local, dev, stream)
+        line = base_line(args, world, "incremental scene flush time after a 1% edit (ms)", fl["edit_flush_ms"], "ms",
+                         fl["edit_flush_ms"], {"workload": fl["workload"], "bricks": fl["bricks"],
+                                               "l2": "inputs larger than L2 (2 GB of bricks)",
+                                               "parallelism": f"replicas x{world}"}, higher=False)
+        line["flush"] = fl
+        line["roofline"] = fl["roofline"]
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        dev.close()
+        return
     build = None if args.no_build else measure_build(args, world, local, dev, stream, flush, args.records)
     if args.workload == "build":
         line = base_line(args, world, "light-tree build throughput (Mleaves/s)", build["mleaves_per_s"], "Mleaves/s",
@@ -862,7 +951,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["trace", "build", "batch"], default="trace")
+    ap.add_argument("--workload", choices=["trace", "build", "batch", "flush"], default="trace")
+    ap.add_argument("--flush-bricks", type=int, default=2_000_000, help="occupied bricks of the flush workload")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--records", type=int, default=N_LEAVES, help="records of the build workload")
     ap.add_argument("--no-build", action="store_true", help="trace workload only: skip the build section")

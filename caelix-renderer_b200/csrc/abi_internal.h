@@ -35,6 +35,8 @@ struct GrowBuffer
     void* ptr = nullptr;
     uint64_t bytes = 0;
     CaelixResult reserve(uint64_t want, const char* what);
+    // reserve, growing by an extra eighth when it has to grow (buffers sized by a scene).
+    CaelixResult reserve_grow(uint64_t want, const char* what) { return want <= bytes ? CAELIX_OK : reserve(want + want / 8, what); }
     void release();
 };
 

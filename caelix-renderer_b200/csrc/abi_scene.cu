@@ -114,6 +114,9 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     if (scene->stage_voxels) cudaFree(scene->stage_voxels);
     scene->upload.release();
     scene->flush_scratch.release();
+    scene->record_of_slot.release();
+    scene->marks.release();
+    scene->update.release();
     if (scene->upload_stream) cudaStreamDestroy(scene->upload_stream);
     if (scene->start) cudaEventDestroy(scene->start);
     if (scene->stop) cudaEventDestroy(scene->stop);
@@ -196,6 +199,14 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     }
     const uint32_t unique = (uint32_t)dst.size();
     lists.insert(lists.end(), dst.begin(), dst.end());
+    if (slots > old_slots) scene->full_rebuild = true;
+    scene->slot_dirty.resize(slots, 0);
+    for (uint32_t s : dst) {
+        if (!scene->slot_dirty[s]) {
+            scene->slot_dirty[s] = 1;
+            scene->dirty_slots.push_back(s);
+        }
+    }
     CaelixResult r = scene->upload.reserve(1024ull * count + 4ull * lists.size(), "caelix_scene_upload_bricks");
     if (r != CAELIX_OK) return r;
     uint16_t* d_blocks = static_cast<uint16_t*>(scene->upload.ptr);
@@ -210,7 +221,6 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     // The caller may reuse its buffers on return, and the next flush reads the staging.
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_upload_bricks");
-    scene->dirty = true;
     if (consumed) *consumed = count;
     return CAELIX_OK;
     CAELIX_GUARD_END
@@ -226,10 +236,18 @@ CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_
     for (uint32_t i = 0; i < count; ++i) {
         const uint64_t packed = pack_key(keys[i]);
         const auto it = scene->slot_of.find(packed);
-        if (it != scene->slot_of.end()) scene->slot_power[it->second] = power[i];
-        else scene->pending_power[packed] = power[i];
+        if (it != scene->slot_of.end()) {
+            const uint32_t slot = it->second;
+            scene->slot_power[slot] = power[i];
+            scene->slot_dirty.resize(scene->slot_power.size(), 0);
+            if (!scene->slot_dirty[slot]) {
+                scene->slot_dirty[slot] = 1;
+                scene->dirty_slots.push_back(slot);
+            }
+        } else {
+            scene->pending_power[packed] = power[i];
+        }
     }
-    scene->dirty = scene->dirty || count > 0;
     return CAELIX_OK;
     CAELIX_GUARD_END
 }
@@ -243,7 +261,7 @@ CAELIX_API CaelixResult caelix_scene_set_materials(CaelixScene* scene, const Cae
             if (!std::isfinite(entries[i].albedo[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
     for (uint32_t i = 0; i < cx::kMaterialSlots; ++i)
         for (int k = 0; k < 3; ++k) scene->albedo[3 * i + k] = i < count ? entries[i].albedo[k] : 0.5f;
-    scene->dirty = true;
+    scene->albedo_dirty = true;
     return CAELIX_OK;
     CAELIX_GUARD_END
 }
@@ -255,7 +273,7 @@ CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const
         return CAELIX_ERROR_INVALID_ARGUMENT;
     // Toggling the tree changes the light records (the power of every brick); any other change
     // takes effect as a light-tree rebuild at the next flush, as in the reference.
-    if (options->enabled != scene->light_options.enabled || !scene->built) scene->dirty = true;
+    if (options->enabled != scene->light_options.enabled || !scene->built) scene->full_rebuild = true;
     else scene->light_tree_dirty = true;
     scene->light_options = *options;
     return CAELIX_OK;
@@ -272,51 +290,111 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         return CAELIX_ERROR_INVALID_ARGUMENT;
     }
     scene->last_frame = desc->frame_number;
-    if (!scene->dirty && !scene->light_tree_dirty) return CAELIX_OK;
+    if (!scene->built) scene->full_rebuild = true;
+    const bool edits = !scene->dirty_slots.empty();
+    if (!scene->full_rebuild && !edits && !scene->light_tree_dirty && !scene->albedo_dirty) return CAELIX_OK;
     cudaSetDevice(scene->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
-    if (!scene->dirty) {
-        // Light tree only: the build over the resident light records, then its status.
-        uint32_t status = 0;
+    const bool lit = scene->light_options.enabled != 0;
+    uint32_t status = 0;
+    cudaError_t e = cudaSuccess;
+    if (!scene->full_rebuild) {
+        // The brick set is unchanged: the tables stay; the edited bricks are copied into the
+        // scene and their records and their neighbours' finalized again, then the light records
+        // and the light tree are rebuilt. A light-options change alone rebuilds the light tree.
+        if (edits || scene->albedo_dirty) {
+            // Rewritten in place: renders of the scene, on any stream, finish first.
+            e = cudaDeviceSynchronize();
+            if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+        }
         cudaEventRecord(scene->start, stream);
-        cudaError_t e = cx::scene_build_light_tree(scene->dev, stream);
+        if (scene->albedo_dirty)
+            e = cudaMemcpyAsync(scene->dev.albedo, scene->albedo, sizeof(scene->albedo), cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess && edits) {
+            const uint32_t c = (uint32_t)scene->dirty_slots.size();
+            std::vector<uint32_t> host(2ull * c);
+            for (uint32_t i = 0; i < c; ++i) {
+                const uint32_t slot = scene->dirty_slots[i];
+                const float p = lit ? scene->slot_power[slot] : 0.0f;
+                host[i] = slot;
+                std::memcpy(&host[c + i], &p, 4);
+            }
+            CaelixResult r = scene->update.reserve(4ull * (9ull * c + 1), "caelix_scene_flush");
+            if (r != CAELIX_OK) return r;
+            uint32_t* d_slots = static_cast<uint32_t*>(scene->update.ptr);
+            const float* d_power = reinterpret_cast<const float*>(d_slots + c);
+            uint32_t* d_list = d_slots + 2ull * c;
+            uint32_t* d_count = d_list + 7ull * c;
+            if (++scene->mark_epoch == 0) {
+                e = cudaMemsetAsync(scene->marks.ptr, 0, 4ull * scene->dev.brick_count, stream);
+                scene->mark_epoch = 1;
+            }
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d_slots, host.data(), 8ull * c, cudaMemcpyHostToDevice, stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, 4, stream);
+            // The build's status words and counters start from zero, as in a full build.
+            if (e == cudaSuccess) e = cudaMemsetAsync(scene->dev.status, 0, 64, stream);
+            if (e == cudaSuccess)
+                e = cx::staging_update(scene->stage_voxels, d_slots, d_power, c,
+                                       static_cast<const uint32_t*>(scene->record_of_slot.ptr), scene->dev,
+                                       static_cast<uint32_t*>(scene->marks.ptr), scene->mark_epoch, d_list, d_count,
+                                       stream);
+            if (e == cudaSuccess) e = cx::scene_refinalize(scene->dev, d_list, d_count, 7 * c, stream);
+            if (e == cudaSuccess) e = cx::scene_build_lights(scene->dev, stream, &status);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(&scene->last_update_records, d_count, 4, cudaMemcpyDeviceToHost, stream);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        } else if (e == cudaSuccess && scene->light_tree_dirty) {
+            e = cx::scene_build_light_tree(scene->dev, stream);
+            if (e == cudaSuccess) e = cx::scene_read_status(scene->dev, stream, &status);
+        }
         cudaEventRecord(scene->stop, stream);
-        if (e == cudaSuccess) e = cx::scene_read_status(scene->dev, stream, &status);
         if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+        cudaEventSynchronize(scene->stop);
         cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
+        for (uint32_t slot : scene->dirty_slots) scene->slot_dirty[slot] = 0;
+        scene->dirty_slots.clear();
+        scene->albedo_dirty = false;
         scene->light_tree_dirty = false;
+        if (edits) scene->generation += 1;
         return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
     }
-    // The staged bricks in increasing linear brick index of the grid spanned by the keys, sorted
-    // and gathered on the device, then the build.
+    // A full rebuild: the staged bricks in increasing linear brick index of the grid spanned by
+    // the keys, sorted and gathered on the device, then the build.
     const uint32_t n = (uint32_t)scene->slot_power.size();
     const uint32_t grid[3] = {(uint32_t)scene->key_max[0] + 1, (uint32_t)scene->key_max[1] + 1,
                               (uint32_t)scene->key_max[2] + 1};
-    const bool lit = scene->light_options.enabled != 0;
-    CaelixResult r = scene->flush_scratch.reserve(4ull * n + 4 * cx::staging_sort_words(n), "caelix_scene_flush");
+    CaelixResult r = scene->flush_scratch.reserve_grow(4ull * n + 4 * cx::staging_sort_words(n), "caelix_scene_flush");
+    if (r == CAELIX_OK) r = scene->record_of_slot.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
+    if (r == CAELIX_OK) r = scene->marks.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
     if (r != CAELIX_OK) return r;
     float* d_power = static_cast<float*>(scene->flush_scratch.ptr);
     uint32_t* sort_scratch = reinterpret_cast<uint32_t*>(d_power + n);
     // The build rewrites the device tables in place: renders of the previous build, on any
     // stream, finish first.
-    cudaError_t e = cudaDeviceSynchronize();
+    e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
-    uint32_t status = 0;
     cudaEventRecord(scene->start, stream);
     e = cx::scene_alloc_inputs(scene->dev, n, stream);
     if (e == cudaSuccess && lit && n)
         e = cudaMemcpyAsync(d_power, scene->slot_power.data(), 4ull * n, cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(scene->dev.albedo, scene->albedo, sizeof(scene->albedo), cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(scene->marks.ptr, 0, 4ull * std::max(n, 1u), stream);
     if (e == cudaSuccess)
         e = cx::staging_gather(scene->stage_keys, scene->stage_voxels, lit ? d_power : nullptr, n, grid, sort_scratch,
-                               scene->dev.status, scene->dev.keys, scene->dev.voxels, scene->dev.power, stream);
+                               scene->dev.status, scene->dev.keys, scene->dev.voxels, scene->dev.power,
+                               static_cast<uint32_t*>(scene->record_of_slot.ptr), stream);
     if (e == cudaSuccess) e = cx::scene_build_device(scene->dev, grid, scene->group_shift, n, stream, &status);
     cudaEventRecord(scene->stop, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     cudaEventSynchronize(scene->stop);
     cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
-    scene->dirty = false;
+    for (uint32_t slot : scene->dirty_slots) scene->slot_dirty[slot] = 0;
+    scene->dirty_slots.clear();
+    scene->mark_epoch = 0;
+    scene->full_rebuild = false;
+    scene->albedo_dirty = false;
     scene->light_tree_dirty = false;
     scene->built = true;
     scene->generation += 1;

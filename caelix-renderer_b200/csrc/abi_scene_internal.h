@@ -31,10 +31,21 @@ struct CaelixScene
     cx::GrowBuffer flush_scratch;  // slot powers, linear indices and the sort of a flush
     std::vector<uint32_t> upload_mark;  // per slot: the last upload that wrote it
     uint32_t upload_epoch = 0;
+    // Edits since the last flush. A full rebuild follows a new key (or the first flush, or a
+    // light-tree toggle); otherwise only the edited slots are copied to their bricks and their
+    // records (and their neighbours') finalized again.
+    bool full_rebuild = true;
+    std::vector<uint32_t> dirty_slots;
+    std::vector<uint8_t> slot_dirty;
+    bool albedo_dirty = false;
+    cx::GrowBuffer record_of_slot;  // device: the brick index of every slot (the last full build)
+    cx::GrowBuffer marks;           // device: one word per brick (staging_update)
+    uint32_t mark_epoch = 0;
+    cx::GrowBuffer update;          // device: edited slots, their power, the refinalize list
+    uint32_t last_update_records = 0;  // records finalized again by the last incremental flush
     float albedo[cx::kMaterialSlots * 3];
     CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
-    bool dirty = true;
-    bool light_tree_dirty = false;  // only the light tree is stale (a light-options change)
+    bool light_tree_dirty = false;  // the light tree is stale (a light-options change)
     uint64_t last_frame = 0;
     cx::DeviceScene dev;
     bool built = false;

@@ -179,6 +179,8 @@ struct FinalizeArgs
     uint32_t capacity;
     uint32_t max_probe;
     uint32_t* records;
+    const uint32_t* list;        // nullptr: every brick; else the bricks list[0 .. *list_count)
+    const uint32_t* list_count;
 };
 
 constexpr uint32_t kFinalizeWarps = 8;
@@ -232,7 +234,9 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
     uint16_t* rec16 = reinterpret_cast<uint16_t*>(s_record[warp]);
     const uint32_t x = lane & 7u, ylo = lane >> 3;
     const uint32_t fj = lane & 7u, fg = lane >> 3;  // face loads: row fj of face 2 + fg
-    for (uint32_t b = blockIdx.x * kFinalizeWarps + warp; b < a.n; b += gridDim.x * kFinalizeWarps) {
+    const uint32_t items = a.list ? *a.list_count : a.n;
+    for (uint32_t item = blockIdx.x * kFinalizeWarps + warp; item < items; item += gridDim.x * kFinalizeWarps) {
+        const uint32_t b = a.list ? __ldg(a.list + item) : item;
         const int32_t bx = __ldg(a.keys + 3ull * b), by = __ldg(a.keys + 3ull * b + 1), bz = __ldg(a.keys + 3ull * b + 2);
         const uint4* own = reinterpret_cast<const uint4*>(a.voxels + 512ull * b);
         const uint4 v0 = __ldg(own + lane), v1 = __ldg(own + 32 + lane);
@@ -682,8 +686,10 @@ cudaError_t alloc(T*& p, uint64_t& capacity, uint64_t count)
     if (p) cudaFree(p);
     p = nullptr;
     capacity = 0;
-    CX_TRY(cudaMalloc(&p, count * sizeof(T)));
-    capacity = count;
+    // An eighth of headroom: a scene that grows by a few bricks keeps its buffers.
+    const uint64_t grown = count + count / 8;
+    CX_TRY(cudaMalloc(&p, grown * sizeof(T)));
+    capacity = grown;
     return cudaSuccess;
 }
 
@@ -731,6 +737,38 @@ SceneView scene_view(const DeviceScene& s)
     return v;
 }
 
+// The build scratch of a scene of s.brick_count bricks (sized by scene_build_device): 8 arrays of
+// n words, 6 n words of family counts, the sort scratch, scan states.
+struct BuildScratch
+{
+    uint32_t *lo, *hi, *home, *order, *home_alt, *order_alt, *tmp, *tmp2, *counts6, *sortw, *small;
+};
+
+static uint64_t build_scratch_words(uint32_t n)
+{
+    return 14ull * std::max(n, 1u) + sort_scratch_words(std::max(n, 1u)) + 2 +
+           blocks_for(std::max(n, 1u), kScanTile) + 64;
+}
+
+static BuildScratch build_scratch(const DeviceScene& s)
+{
+    const uint64_t n = s.brick_count;
+    uint32_t* w = s.scratch;
+    BuildScratch b;
+    b.lo = w;
+    b.hi = w + n;
+    b.home = w + 2 * n;
+    b.order = w + 3 * n;
+    b.home_alt = w + 4 * n;
+    b.order_alt = w + 5 * n;
+    b.tmp = w + 6 * n;
+    b.tmp2 = w + 7 * n;
+    b.counts6 = w + 8 * n;
+    b.sortw = w + 14 * n;
+    b.small = b.sortw + sort_scratch_words(std::max(s.brick_count, 1u));
+    return b;
+}
+
 void scene_release(DeviceScene& s)
 {
     void* ptrs[] = {s.keys, s.voxels, s.power, s.records, s.hash_slots, s.bitmap, s.albedo, s.heap, s.group_rows,
@@ -774,25 +812,23 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     s.group_count = s.groups[0] * s.groups[1] * s.groups[2];
     s.brick_count = n;
 
-    // Scratch: 8 arrays of n words, 6 n words of family counts, the sort scratch, scan states.
     const uint64_t sort_words = sort_scratch_words(std::max(n, 1u));
-    const uint64_t need = 14ull * std::max(n, 1u) + sort_words + 2 + blocks_for(std::max(n, 1u), kScanTile) + 64;
+    const uint64_t need = build_scratch_words(n);
     if (need > s.scratch_words) {
         CX_TRY(alloc(s.scratch, s.capacity.scratch, need));
         s.scratch_words = need;
     }
-    uint32_t* w = s.scratch;
-    uint32_t* lo = w;
-    uint32_t* hi = w + n;
-    uint32_t* home = w + 2ull * n;
-    uint32_t* order = w + 3ull * n;
-    uint32_t* home_alt = w + 4ull * n;
-    uint32_t* order_alt = w + 5ull * n;
-    uint32_t* tmp = w + 6ull * n;
-    uint32_t* tmp2 = w + 7ull * n;
-    uint32_t* counts6 = w + 8ull * n;
-    uint32_t* sortw = w + 14ull * n;
-    uint32_t* small = sortw + sort_words;  // scan scratch and counters
+    const BuildScratch bs = build_scratch(s);
+    uint32_t* lo = bs.lo;
+    uint32_t* hi = bs.hi;
+    uint32_t* home = bs.home;
+    uint32_t* order = bs.order;
+    uint32_t* home_alt = bs.home_alt;
+    uint32_t* order_alt = bs.order_alt;
+    uint32_t* tmp = bs.tmp;
+    uint32_t* tmp2 = bs.tmp2;
+    uint32_t* sortw = bs.sortw;
+    uint32_t* small = bs.small;
 
     // Hash table.
     s.hash_capacity = std::max(2u * n, 2u);
@@ -821,18 +857,44 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     // Records.
     CX_TRY(alloc(s.records, s.capacity.records, (uint64_t)kRecordWords * n));
     if (n > 0) {
-        FinalizeArgs fa{s.keys, s.voxels, n, group_shift, s.hash_slots, s.hash_capacity, s.hash_max_probe, s.records};
+        FinalizeArgs fa{s.keys,  s.voxels,          n,         group_shift, s.hash_slots, s.hash_capacity,
+                        s.hash_max_probe, s.records, nullptr, nullptr};
         finalize_kernel<<<finalize_grid(n), kFinalizeWarps * 32, 0, stream>>>(fa);
     }
+    return scene_build_lights(s, stream, device_status_out);
+}
+
+cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_t* list_count, uint32_t max_count,
+                             cudaStream_t stream)
+{
+    if (max_count == 0) return cudaSuccess;
+    FinalizeArgs fa{s.keys,  s.voxels,          s.brick_count, s.group_shift, s.hash_slots, s.hash_capacity,
+                    s.hash_max_probe, s.records, list,       list_count};
+    finalize_kernel<<<finalize_grid(max_count), kFinalizeWarps * 32, 0, stream>>>(fa);
+    return cudaGetLastError();
+}
+
+cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out)
+{
+    const uint32_t n = s.brick_count;
+    const uint32_t group_shift = s.group_shift;
+    const BuildScratch bs = build_scratch(s);
+    uint32_t* home = bs.home;
+    uint32_t* order = bs.order;
+    uint32_t* tmp = bs.tmp;
+    uint32_t* tmp2 = bs.tmp2;
+    uint32_t* counts6 = bs.counts6;
+    uint32_t* sortw = bs.sortw;
+    uint32_t* small = bs.small;
 
     // Light records.
     LightArgs la{s.keys, s.voxels, s.power, n, group_shift, {s.groups[0], s.groups[1], s.groups[2]},
                  s.hash_slots, s.hash_capacity, s.hash_max_probe};
     uint32_t* d_light_count = s.status + 5;
-    uint32_t* lkeys = lo;  // reuse the hash scratch
-    uint32_t* lbricks = hi;
-    uint32_t* lkeys_alt = home_alt;
-    uint32_t* lbricks_alt = order_alt;
+    uint32_t* lkeys = bs.lo;  // reuse the hash scratch
+    uint32_t* lbricks = bs.hi;
+    uint32_t* lkeys_alt = bs.home_alt;
+    uint32_t* lbricks_alt = bs.order_alt;
     if (n > 0) light_collect_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
     uint32_t m = 0;
     CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
@@ -890,9 +952,10 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     if (cap > s.tree_capacity) {
         if (s.tree_memory) cudaFree(s.tree_memory);
         s.tree_memory = nullptr;
-        CX_TRY(cudaMalloc(&s.tree_memory, lt_buffer_bytes(cap)));
-        s.tree = lt_carve(s.tree_memory, cap);
-        s.tree_capacity = cap;
+        const uint32_t grown = cap + cap / 8;
+        CX_TRY(cudaMalloc(&s.tree_memory, lt_buffer_bytes(grown)));
+        s.tree = lt_carve(s.tree_memory, grown);
+        s.tree_capacity = grown;
         CX_TRY(cudaMemsetAsync(s.tree.header, 0, 128, stream));
     }
     CX_TRY(scene_build_light_tree(s, stream));

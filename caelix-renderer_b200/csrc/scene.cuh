@@ -99,6 +99,12 @@ cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_s
 cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream);
 cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
                                cudaStream_t stream, uint32_t* device_status_out);
+// The parts of a rebuild whose brick set is unchanged (same keys, same order): the records of the
+// bricks list[0 .. *list_count) (device; at most max_count) finalized again from s.voxels, then
+// (scene_build_lights) the light records of every brick and the light tree. Synchronous.
+cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_t* list_count, uint32_t max_count,
+                             cudaStream_t stream);
+cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out);
 
 // ---- device-resident brick staging (staging.cu) ----
 // Copies brick src_index[j] of an upload (src, device, 512 values per brick) to staging slot
@@ -108,9 +114,18 @@ cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, cons
 // The staging slots in increasing linear brick index of `grid`, gathered into the scene's input
 // arrays (power zero when `power` is null). `scratch`: staging_sort_words(n) words.
 uint64_t staging_sort_words(uint32_t n);
+// Also writes record_of_slot[slot] = the slot's brick index in the scene.
 cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
                            uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
-                           uint16_t* voxels, float* power, cudaStream_t stream);
+                           uint16_t* voxels, float* power, uint32_t* record_of_slot, cudaStream_t stream);
+// An edit of a built scene that adds no brick: the `count` edited slots (slots[i], with power
+// power[i], both device) copied to their bricks in the scene (values and power), and the list of
+// the bricks whose records depend on them (each edited brick and its six neighbours, each once)
+// written to list[0 .. *list_count) (list: 7 * count words; `marks`: one word per brick, holding
+// `epoch` once listed, never equal to a new epoch before; *list_count zero on entry).
+cudaError_t staging_update(const uint16_t* stage_voxels, const uint32_t* slots, const float* power, uint32_t count,
+                           const uint32_t* record_of_slot, DeviceScene& s, uint32_t* marks, uint32_t epoch,
+                           uint32_t* list, uint32_t* list_count, cudaStream_t stream);
 // Rebuilds the light tree of a built scene from its light records (asynchronous on `stream`, no
 // allocation: the tree buffers were sized by scene_build). The reference's per-flush light BVH
 // rebuild (lib/src/light/light_tree_record.cpp:230-302, RecordTree).

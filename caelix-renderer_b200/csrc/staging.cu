@@ -6,6 +6,7 @@
 
 #include "radix_sort.cuh"
 #include "scene.cuh"
+#include "scene_device.cuh"
 
 namespace cx {
 
@@ -36,7 +37,8 @@ __global__ void __launch_bounds__(kStageThreads)
 __global__ void __launch_bounds__(kStageThreads)
     staging_gather_kernel(const uint32_t* __restrict__ order, uint32_t n, const int32_t* __restrict__ stage_keys,
                           const uint4* __restrict__ stage_voxels, const float* __restrict__ slot_power,
-                          int32_t* __restrict__ keys, uint4* __restrict__ voxels, float* __restrict__ power)
+                          int32_t* __restrict__ keys, uint4* __restrict__ voxels, float* __restrict__ power,
+                          uint32_t* __restrict__ record_of_slot)
 {
     const uint64_t u = (uint64_t)blockIdx.x * kStageThreads + threadIdx.x;
     if (u >= 64ull * n) return;
@@ -45,6 +47,39 @@ __global__ void __launch_bounds__(kStageThreads)
     voxels[u] = __ldg(stage_voxels + 64ull * s + w);
     if (w < 3) keys[3ull * i + w] = __ldg(stage_keys + 3ull * s + w);
     if (w == 3) power[i] = slot_power ? __ldg(slot_power + s) : 0.0f;
+    if (w == 4) record_of_slot[s] = i;
+}
+
+// One warp per edited slot: its values and power to its brick, then the brick and its six
+// neighbours listed once each (the first warp to stamp a brick with this epoch lists it).
+__global__ void __launch_bounds__(kStageThreads)
+    staging_update_kernel(const uint4* __restrict__ stage_voxels, const uint32_t* __restrict__ slots,
+                          const float* __restrict__ slot_power, uint32_t count,
+                          const uint32_t* __restrict__ record_of_slot, const int32_t* __restrict__ keys,
+                          uint4* __restrict__ voxels, float* __restrict__ power, const uint4* __restrict__ hash_slots,
+                          uint32_t hash_capacity, uint32_t hash_max_probe, uint32_t* __restrict__ marks,
+                          uint32_t epoch, uint32_t* __restrict__ list, uint32_t* __restrict__ list_count)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t j = (blockIdx.x * kStageThreads + threadIdx.x) >> 5;
+    if (j >= count) return;
+    const uint32_t s = __ldg(slots + j);
+    const uint32_t r = __ldg(record_of_slot + s);
+    voxels[64ull * r + lane] = __ldg(stage_voxels + 64ull * s + lane);
+    voxels[64ull * r + 32 + lane] = __ldg(stage_voxels + 64ull * s + 32 + lane);
+    if (lane == 0) power[r] = __ldg(slot_power + j);
+    uint32_t target = 0xFFFFFFFFu;
+    if (lane == 6) {
+        target = r;
+    } else if (lane < 6) {
+        const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
+        const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
+        const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
+        target = hash_lookup(hash_slots, hash_capacity, hash_max_probe, keys[3ull * r] + dx, keys[3ull * r + 1] + dy,
+                             keys[3ull * r + 2] + dz);
+    }
+    if (target != 0xFFFFFFFFu && atomicExch(marks + target, epoch) != epoch)
+        list[atomicAdd(list_count, 1u)] = target;
 }
 
 uint32_t blocks(uint64_t items) { return (uint32_t)((items + kStageThreads - 1) / kStageThreads); }
@@ -68,7 +103,7 @@ uint64_t staging_sort_words(uint32_t n)
 
 cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
                            uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
-                           uint16_t* voxels, float* power, cudaStream_t stream)
+                           uint16_t* voxels, float* power, uint32_t* record_of_slot, cudaStream_t stream)
 {
     if (n == 0) return cudaSuccess;
     uint32_t* lin = scratch;
@@ -83,7 +118,19 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
     onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream);
     staging_gather_kernel<<<blocks(64ull * n), kStageThreads, 0, stream>>>(
         order, n, stage_keys, reinterpret_cast<const uint4*>(stage_voxels), slot_power, keys,
-        reinterpret_cast<uint4*>(voxels), power);
+        reinterpret_cast<uint4*>(voxels), power, record_of_slot);
+    return cudaGetLastError();
+}
+
+cudaError_t staging_update(const uint16_t* stage_voxels, const uint32_t* slots, const float* power, uint32_t count,
+                           const uint32_t* record_of_slot, DeviceScene& s, uint32_t* marks, uint32_t epoch,
+                           uint32_t* list, uint32_t* list_count, cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    staging_update_kernel<<<blocks(32ull * count), kStageThreads, 0, stream>>>(
+        reinterpret_cast<const uint4*>(stage_voxels), slots, power, count, record_of_slot, s.keys,
+        reinterpret_cast<uint4*>(s.voxels), s.power, s.hash_slots, s.hash_capacity, s.hash_max_probe, marks, epoch,
+        list, list_count);
     return cudaGetLastError();
 }
 

@@ -81,8 +81,8 @@ def test_config2_incremental_then_edit(cuda_device, oracle):
 
 
 def test_empty_and_power_only_flushes(cuda_device, oracle):
-    """A scene flushed with no bricks; then bricks; then only a power change (a full rebuild of
-    the light records from the staged bricks)."""
+    """A scene flushed with no bricks; then bricks; then only a power change (the edited bricks'
+    records again, the light records and the light tree rebuilt)."""
     import caelix_b200
 
     vs = workloads.noise_world(grid_bricks=(6, 6, 6), brick_occupancy=0.5, emissive_fraction=0.1, seed=4)
@@ -100,3 +100,45 @@ def test_empty_and_power_only_flushes(cuda_device, oracle):
     s.flush()
     assert_scene_equal(s, oracle_lib.OracleScene(oracle, vs), vs)
     s.close()
+
+
+def test_edits_without_new_bricks(cuda_device, oracle):
+    """Edits that add no brick (rewritten values, bricks emptied, powers changed, a new albedo
+    table) take the incremental flush; each state equals the oracle's build of the edited scene,
+    and so does the render."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(10, 8, 12), brick_occupancy=0.45, emissive_fraction=0.08, seed=12)
+    rng = np.random.default_rng(12)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    voxels, power, albedo = vs.voxels.copy(), vs.power.copy(), vs.albedo.copy()
+    for step in range(3):
+        n = vs.brick_count
+        edit = rng.choice(n, size=n // 10, replace=False)
+        fresh = np.where(rng.random((len(edit), 512)) < 0.5,
+                         0x8000 | rng.integers(1, 65, size=(len(edit), 512)), 0).astype(np.uint16)
+        fresh[: len(edit) // 8] = 0  # emptied bricks stay in the scene
+        voxels[edit] = fresh
+        scene.upload_bricks(vs.keys[edit], fresh)
+        relit = rng.choice(n, size=max(1, n // 20), replace=False)
+        power[relit] = np.where(rng.random(len(relit)) < 0.5, 0.0, rng.lognormal(0.0, 1.0, len(relit))).astype(np.float32)
+        scene.set_brick_power(vs.keys[relit], power[relit])
+        if step == 1:
+            albedo = rng.uniform(0.1, 0.9, size=albedo.shape).astype(np.float32)
+            scene.set_albedo(albedo)
+        scene.flush()
+        cur = workloads.VoxelScene(vs.grid, vs.keys, voxels, power, albedo, vs.camera, vs.group_shift)
+        osc = oracle_lib.OracleScene(oracle, cur)
+        assert_scene_equal(scene, osc, cur)
+        gpu, ref, st, rays = render_both(cuda_device, scene, osc, cur, 64, 48, spp=2, bounces=3, seed=step + 1)
+        assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+        assert_radiance_close(gpu, ref)
+    # An albedo change alone: no rebuild, the render follows the new table.
+    albedo = rng.uniform(0.1, 0.9, size=albedo.shape).astype(np.float32)
+    scene.set_albedo(albedo)
+    scene.flush()
+    cur = workloads.VoxelScene(vs.grid, vs.keys, voxels, power, albedo, vs.camera, vs.group_shift)
+    osc = oracle_lib.OracleScene(oracle, cur)
+    gpu, ref, st, rays = render_both(cuda_device, scene, osc, cur, 64, 48, spp=2, bounces=3, seed=9)
+    assert_radiance_close(gpu, ref)
+    scene.close()
