@@ -225,6 +225,95 @@ __device__ __forceinline__ uint32_t spread_rows(uint32_t n)
     return (n & 1u) | ((n & 2u) << 7) | ((n & 4u) << 14) | ((n & 8u) << 21);
 }
 
+// A brick and its six neighbour faces in registers (one warp): lane l holds values 8l .. 8l + 7
+// (v0) and 256 + 8l .. (v1); the y and z faces one row of 8 values each (fv: row lane & 7 of face
+// 2 + (lane >> 3): rows (x, 0 / 7, z) of the +-y neighbours, rows (x, y, 0 / 7) of the +-z ones);
+// the x faces two values each (xf: (0, y, z) of the +x neighbour at y + 8 z = lane and lane + 32,
+// then (7, y, z) of the -x one). Absent neighbours read as air.
+struct BrickFaces
+{
+    uint4 v0, v1, fv;
+    uint32_t xf[4];  // +x lane, -x lane, +x lane + 32, -x lane + 32
+};
+
+__device__ __forceinline__ BrickFaces load_brick_faces(const int32_t* __restrict__ keys,
+                                                       const uint16_t* __restrict__ voxels, const uint4* slots,
+                                                       uint32_t capacity, uint32_t max_probe, uint32_t b, uint32_t lane)
+{
+    BrickFaces f;
+    const int32_t bx = __ldg(keys + 3ull * b), by = __ldg(keys + 3ull * b + 1), bz = __ldg(keys + 3ull * b + 2);
+    const uint4* own = reinterpret_cast<const uint4*>(voxels + 512ull * b);
+    f.v0 = __ldg(own + lane);
+    f.v1 = __ldg(own + 32 + lane);
+    uint32_t my_nbr = 0xFFFFFFFFu;
+    if (lane < 6) {
+        const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
+        const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
+        const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
+        my_nbr = hash_lookup(slots, capacity, max_probe, bx + dx, by + dy, bz + dz);
+    }
+    const uint32_t fj = lane & 7u, fg = lane >> 3;
+    const uint32_t nx_pos = __shfl_sync(0xFFFFFFFFu, my_nbr, 0);
+    const uint32_t nx_neg = __shfl_sync(0xFFFFFFFFu, my_nbr, 1);
+    const uint32_t nf = __shfl_sync(0xFFFFFFFFu, my_nbr, 2 + fg);
+    const uint32_t fq = fg == 0 ? 8 * fj : (fg == 1 ? 8 * fj + 7 : (fg == 2 ? fj : 56 + fj));
+    f.fv = nf == 0xFFFFFFFFu ? make_uint4(0, 0, 0, 0) : __ldg(reinterpret_cast<const uint4*>(voxels + 512ull * nf) + fq);
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const uint32_t i = lane + 32 * h;
+        f.xf[2 * h] = nx_pos == 0xFFFFFFFFu ? 0u : (uint32_t)voxels[512ull * nx_pos + 8 * i];
+        f.xf[2 * h + 1] = nx_neg == 0xFFFFFFFFu ? 0u : (uint32_t)voxels[512ull * nx_neg + 7 + 8 * i];
+    }
+    return f;
+}
+
+// Opaque masks of a brick and of its six neighbours of every voxel: lane k < 16 gets word k (bit
+// x + 8 (y & 3) for the rows y = 4 (k & 1) + 0 .. 3 at z = k >> 1) of the brick's opaque voxels
+// (o) and of the voxels whose neighbour in direction d is opaque (n[d]: +x, -x, +y, -y, +z, -z).
+struct OpaqueMasks
+{
+    uint32_t o, n[6];
+};
+
+__device__ __forceinline__ OpaqueMasks opaque_masks(const BrickFaces& f, uint32_t lane)
+{
+    const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
+    const uint32_t o0 = opaque_byte(f.v0), o1 = opaque_byte(f.v1);
+    uint32_t o = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 4; ++i) {
+        const uint32_t src = (4 * lane + i) & 31u;
+        const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, o0, src), t1 = __shfl_sync(0xFFFFFFFFu, o1, src);
+        o |= (lane < 8 ? t0 : t1) << (8 * i);
+    }
+    const uint32_t fxp0 = __ballot_sync(0xFFFFFFFFu, f.xf[0] & kOpaqueBit);
+    const uint32_t fxn0 = __ballot_sync(0xFFFFFFFFu, f.xf[1] & kOpaqueBit);
+    const uint32_t fxp1 = __ballot_sync(0xFFFFFFFFu, f.xf[2] & kOpaqueBit);
+    const uint32_t fxn1 = __ballot_sync(0xFFFFFFFFu, f.xf[3] & kOpaqueBit);
+    const uint32_t fb = opaque_byte(f.fv);
+    const uint32_t fyp = __shfl_sync(0xFFFFFFFFu, fb, kz), fyn = __shfl_sync(0xFFFFFFFFu, fb, 8 + kz);
+    uint32_t fzp = 0, fzn = 0;
+#pragma unroll
+    for (uint32_t i = 0; i < 4; ++i) {
+        fzp |= __shfl_sync(0xFFFFFFFFu, fb, 16 + 4 * kyh + i) << (8 * i);
+        fzn |= __shfl_sync(0xFFFFFFFFu, fb, 24 + 4 * kyh + i) << (8 * i);
+    }
+    const uint32_t o_next = __shfl_down_sync(0xFFFFFFFFu, o, 1), o_prev = __shfl_up_sync(0xFFFFFFFFu, o, 1);
+    const uint32_t o_up = __shfl_down_sync(0xFFFFFFFFu, o, 2), o_down = __shfl_up_sync(0xFFFFFFFFu, o, 2);
+    const uint32_t xs = (4 * lane) & 31u;
+    const uint32_t nib_p = ((lane < 8 ? fxp0 : fxp1) >> xs) & 0xFu;
+    const uint32_t nib_n = ((lane < 8 ? fxn0 : fxn1) >> xs) & 0xFu;
+    OpaqueMasks m;
+    m.o = lane < 16 ? o : 0u;
+    m.n[0] = ((o >> 1) & 0x7F7F7F7Fu) | (spread_rows(nib_p) << 7);
+    m.n[1] = ((o << 1) & 0xFEFEFEFEu) | spread_rows(nib_n);
+    m.n[2] = (o >> 8) | ((kyh == 0 ? (o_next & 0xFFu) : fyp) << 24);
+    m.n[3] = (o << 8) | (kyh == 1 ? (o_prev >> 24) : fyn);
+    m.n[4] = kz < 7 ? o_up : fzp;
+    m.n[5] = kz > 0 ? o_down : fzn;
+    return m;
+}
+
 __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const FinalizeArgs a)
 {
     __shared__ __align__(16) uint32_t s_stage[kFinalizeWarps][kFinalizeStageWords];
@@ -238,38 +327,17 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
     for (uint32_t item = blockIdx.x * kFinalizeWarps + warp; item < items; item += gridDim.x * kFinalizeWarps) {
         const uint32_t b = a.list ? __ldg(a.list + item) : item;
         const int32_t bx = __ldg(a.keys + 3ull * b), by = __ldg(a.keys + 3ull * b + 1), bz = __ldg(a.keys + 3ull * b + 2);
-        const uint4* own = reinterpret_cast<const uint4*>(a.voxels + 512ull * b);
-        const uint4 v0 = __ldg(own + lane), v1 = __ldg(own + 32 + lane);
-        uint32_t my_nbr = 0xFFFFFFFFu;
-        if (lane < 6) {
-            const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
-            const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
-            const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
-            my_nbr = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
-        }
-        const uint32_t nx_pos = __shfl_sync(0xFFFFFFFFu, my_nbr, 0);
-        const uint32_t nx_neg = __shfl_sync(0xFFFFFFFFu, my_nbr, 1);
-        const uint32_t nf = __shfl_sync(0xFFFFFFFFu, my_nbr, 2 + fg);
-        // +-y faces: rows (x, 0 / 7, z = fj); +-z faces: rows (x, y = fj, 0 / 7); 16 bytes each.
-        const uint32_t fq = fg == 0 ? 8 * fj : (fg == 1 ? 8 * fj + 7 : (fg == 2 ? fj : 56 + fj));
-        const uint4 fv = nf == 0xFFFFFFFFu ? make_uint4(0, 0, 0, 0)
-                                           : __ldg(reinterpret_cast<const uint4*>(a.voxels + 512ull * nf) + fq);
-        // +-x faces: (0 / 7, y, z), entry y + 8 z, two per lane.
-        uint16_t xf[4];
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const uint32_t i = lane + 32 * h;
-            xf[2 * h] = nx_pos == 0xFFFFFFFFu ? (uint16_t)0 : a.voxels[512ull * nx_pos + 8 * i];
-            xf[2 * h + 1] = nx_neg == 0xFFFFFFFFu ? (uint16_t)0 : a.voxels[512ull * nx_neg + 7 + 8 * i];
-        }
+        const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, b, lane);
+        const uint4 v0 = bf.v0, v1 = bf.v1, fv = bf.fv;
+        const uint32_t* xf = bf.xf;
         __syncwarp();  // the previous brick's reads of the staging are done
         reinterpret_cast<uint4*>(vox)[lane] = v0;
         reinterpret_cast<uint4*>(vox)[32 + lane] = v1;
         reinterpret_cast<uint4*>(vox + 512 + 64 * (2 + fg))[fj] = fv;
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
-            vox[512 + lane + 32 * h] = xf[2 * h];
-            vox[512 + 64 + lane + 32 * h] = xf[2 * h + 1];
+            vox[512 + lane + 32 * h] = (uint16_t)xf[2 * h];
+            vox[512 + 64 + lane + 32 * h] = (uint16_t)xf[2 * h + 1];
         }
         __syncwarp();
         // A clean brick (every value of it and of its six neighbour faces air or opaque) keeps
@@ -283,41 +351,8 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
         uint32_t my_occ = 0;
         const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
         if (!dirty) {
-            // Opaque voxels: lane l holds voxels 8l .. 8l + 7 (v0) and 256 + 8l .. (v1).
-            const uint32_t o0 = opaque_byte(v0), o1 = opaque_byte(v1);
-            uint32_t o = 0;
-#pragma unroll
-            for (uint32_t i = 0; i < 4; ++i) {
-                const uint32_t src = (4 * lane + i) & 31u;
-                const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, o0, src), t1 = __shfl_sync(0xFFFFFFFFu, o1, src);
-                o |= (lane < 8 ? t0 : t1) << (8 * i);
-            }
-            // Opaque voxels of the faces: x faces by entry y + 8 z; y and z faces one byte per
-            // row (the lane that loaded it).
-            const uint32_t fxp0 = __ballot_sync(0xFFFFFFFFu, xf[0] & kOpaqueBit);
-            const uint32_t fxn0 = __ballot_sync(0xFFFFFFFFu, xf[1] & kOpaqueBit);
-            const uint32_t fxp1 = __ballot_sync(0xFFFFFFFFu, xf[2] & kOpaqueBit);
-            const uint32_t fxn1 = __ballot_sync(0xFFFFFFFFu, xf[3] & kOpaqueBit);
-            const uint32_t fb = opaque_byte(fv);
-            const uint32_t fyp = __shfl_sync(0xFFFFFFFFu, fb, kz), fyn = __shfl_sync(0xFFFFFFFFu, fb, 8 + kz);
-            uint32_t fzp = 0, fzn = 0;
-#pragma unroll
-            for (uint32_t i = 0; i < 4; ++i) {
-                fzp |= __shfl_sync(0xFFFFFFFFu, fb, 16 + 4 * kyh + i) << (8 * i);
-                fzn |= __shfl_sync(0xFFFFFFFFu, fb, 24 + 4 * kyh + i) << (8 * i);
-            }
-            const uint32_t o_next = __shfl_down_sync(0xFFFFFFFFu, o, 1), o_prev = __shfl_up_sync(0xFFFFFFFFu, o, 1);
-            const uint32_t o_up = __shfl_down_sync(0xFFFFFFFFu, o, 2), o_down = __shfl_up_sync(0xFFFFFFFFu, o, 2);
-            const uint32_t xs = (4 * lane) & 31u;
-            const uint32_t nib_p = ((lane < 8 ? fxp0 : fxp1) >> xs) & 0xFu;
-            const uint32_t nib_n = ((lane < 8 ? fxn0 : fxn1) >> xs) & 0xFu;
-            const uint32_t px = ((o >> 1) & 0x7F7F7F7Fu) | (spread_rows(nib_p) << 7);
-            const uint32_t nx = ((o << 1) & 0xFEFEFEFEu) | spread_rows(nib_n);
-            const uint32_t py = (o >> 8) | ((kyh == 0 ? (o_next & 0xFFu) : fyp) << 24);
-            const uint32_t ny = (o << 8) | (kyh == 1 ? (o_prev >> 24) : fyn);
-            const uint32_t pz = kz < 7 ? o_up : fzp;
-            const uint32_t nz = kz > 0 ? o_down : fzn;
-            my_occ = lane < 16 ? (o & ~(px & nx & py & ny & pz & nz)) : 0u;
+            const OpaqueMasks m = opaque_masks(bf, lane);
+            my_occ = m.o & ~(m.n[0] & m.n[1] & m.n[2] & m.n[3] & m.n[4] & m.n[5]);
         } else {
 #pragma unroll 2
             for (uint32_t k = 0; k < 16; ++k) {
@@ -422,66 +457,34 @@ __global__ void light_collect_kernel(const LightArgs a, uint32_t* counter, uint3
     lbricks[slot] = i;
 }
 
-// The open faces of the 16 voxels of lane `lane` of brick b: open[v] bit f, and the voxel values.
-__device__ __forceinline__ void lane_open_faces(const LightArgs& a, uint32_t b, uint32_t lane, uint32_t open[16],
-                                                uint32_t value[16])
+// The open faces of the light voxels of light brick b (its opaque voxels; a face is open when the
+// neighbour across it is not opaque, an absent brick being air), per family f (+x, -x, +y, -y,
+// +z, -z) in the word layout of opaque_masks: lane k < 16 gets word k of each family.
+__device__ __forceinline__ void light_open_masks(const BrickFaces& f, uint32_t lane, uint32_t open[6])
 {
-    const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
-    uint32_t my_nbr = 0xFFFFFFFFu;
-    if (lane < 6) {
-        const int dx = lane == 0 ? 1 : (lane == 1 ? -1 : 0);
-        const int dy = lane == 2 ? 1 : (lane == 3 ? -1 : 0);
-        const int dz = lane == 4 ? 1 : (lane == 5 ? -1 : 0);
-        my_nbr = hash_lookup(a.slots, a.capacity, a.max_probe, bx + dx, by + dy, bz + dz);
-    }
-    uint32_t nbr[6];
+    const OpaqueMasks m = opaque_masks(f, lane);
 #pragma unroll
-    for (int d = 0; d < 6; ++d) nbr[d] = __shfl_sync(0xFFFFFFFFu, my_nbr, d);
-    const uint16_t* own = a.voxels + 512ull * b;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const uint32_t vi = lane * 16 + k;
-        const int x = vi & 7, y = (vi >> 3) & 7, z = vi >> 6;
-        const uint32_t v = own[vi];
-        value[k] = v;
-        open[k] = 0;
-        if (!(v & kOpaqueBit)) continue;
-        const int dx[6] = {1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, 1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, 1, -1};
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            int nx = x + dx[f], ny = y + dy[f], nz = z + dz[f];
-            uint32_t nv;
-            if (nx >= 0 && nx < 8 && ny >= 0 && ny < 8 && nz >= 0 && nz < 8) {
-                nv = own[nx + 8 * ny + 64 * nz];
-            } else {
-                const uint32_t r = nbr[f];
-                nx &= 7;
-                ny &= 7;
-                nz &= 7;
-                nv = r == 0xFFFFFFFFu ? 0u : (uint32_t)a.voxels[512ull * r + nx + 8 * ny + 64 * nz];
-            }
-            if (!(nv & kOpaqueBit)) open[k] |= 1u << f;
-        }
-    }
+    for (int d = 0; d < 6; ++d) open[d] = m.o & ~m.n[d];
 }
 
+constexpr uint32_t kLightWarps = 4;
+
 // Warp per light brick (sorted order): the family counts and the record's units.
-__global__ void __launch_bounds__(128) light_measure_kernel(const LightArgs a, const uint32_t* __restrict__ lbricks,
-                                                            uint32_t m, uint32_t* __restrict__ counts6,
-                                                            uint32_t* __restrict__ units)
+__global__ void __launch_bounds__(kLightWarps * 32) light_measure_kernel(const LightArgs a,
+                                                                        const uint32_t* __restrict__ lbricks,
+                                                                        uint32_t m, uint32_t* __restrict__ counts6,
+                                                                        uint32_t* __restrict__ units)
 {
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (k >= m) return;
-    uint32_t open[16], value[16];
-    lane_open_faces(a, lbricks[k], lane, open, value);
+    const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, lbricks[k], lane);
+    uint32_t open[6];
+    light_open_masks(bf, lane, open);
     uint32_t total = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        uint32_t c = 0;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) c += (open[q] >> f) & 1u;
-        c = __reduce_add_sync(0xFFFFFFFFu, c);
+        const uint32_t c = __reduce_add_sync(0xFFFFFFFFu, __popc(open[f]));
         if (lane == 0) counts6[6 * k + f] = c;
         total += c;
     }
@@ -537,10 +540,11 @@ struct LightWriteArgs
     uint32_t* light_brick;
 };
 
-__global__ void __launch_bounds__(128) light_write_kernel(const LightWriteArgs w)
+__global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const LightWriteArgs w)
 {
+    __shared__ __align__(16) uint4 s_vox[kLightWarps][64];
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     if (k >= w.m) return;
     const LightArgs& a = w.a;
     const uint32_t b = w.lbricks[k];
@@ -561,52 +565,62 @@ __global__ void __launch_bounds__(128) light_write_kernel(const LightWriteArgs w
     }
     const uint32_t rec_unit = 1 + w.offsets[k] + (k == s ? 1 + count : 0);
     uint32_t* rec = w.heap + 4ull * rec_unit;
-    uint32_t open[16], value[16];
-    lane_open_faces(a, b, lane, open, value);
+    const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, b, lane);
+    s_vox[warp][lane] = bf.v0;
+    s_vox[warp][32 + lane] = bf.v1;
+    __syncwarp();
+    const uint16_t* vox = reinterpret_cast<const uint16_t*>(s_vox[warp]);
+    uint32_t open[6];
+    light_open_masks(bf, lane, open);
     const float P = a.power[b];
     const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f;
-    uint32_t fam_count[6], fam_base[6], cursor[6];
+    // Entries per family in voxel order: lane k writes the voxels of word k (32k + bit) after the
+    // family's entries of the lanes before it.
+    uint32_t fam_count[6];
     uint32_t written = 0;
+    float sums[6];
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
-        fam_count[f] = w.counts6[6 * k + f];
-        fam_base[f] = written;
-        written += fam_count[f];
-        uint32_t c = 0;
-#pragma unroll
-        for (int q = 0; q < 16; ++q) c += (open[q] >> f) & 1u;
+        const uint32_t c = __popc(open[f]);
         const uint32_t inc = warp_inclusive_sum(c);
-        cursor[f] = inc - c;
-    }
-    float sums[6] = {0, 0, 0, 0, 0, 0};
-    uint32_t lo[3] = {8, 8, 8}, hi[3] = {0, 0, 0};
-#pragma unroll
-    for (int q = 0; q < 16; ++q) {
-        if (!open[q]) continue;
-        const uint32_t vi = lane * 16 + q;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            if ((open[q] >> f) & 1u) {
-                rec[12 + fam_base[f] + cursor[f]] = vi | (value[q] << 16);
-                ++cursor[f];
-                sums[f] += weight;
-            }
+        fam_count[f] = __shfl_sync(0xFFFFFFFFu, inc, 31);
+        uint32_t* out = rec + 12 + written + (inc - c);
+        uint32_t bits = open[f];
+        while (bits) {
+            const uint32_t bit = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const uint32_t vi = 32 * lane + bit;
+            *out++ = vi | ((uint32_t)vox[vi] << 16);
         }
-        const uint32_t p[3] = {vi & 7u, (vi >> 3) & 7u, vi >> 6};
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            lo[c] = min(lo[c], p[c]);
-            hi[c] = max(hi[c], p[c] + 1);
-        }
+        written += fam_count[f];
+        // The face sum as sixteen-voxel partial sums (voxels 16l .. 16l + 15 in lane l, the weight
+        // added once per open face), then a tree over the lanes.
+        const uint32_t word = __shfl_sync(0xFFFFFFFFu, open[f], lane >> 1);
+        const uint32_t n16 = __popc((word >> (16 * (lane & 1))) & 0xFFFFu);
+        float part = 0.0f;
+        for (uint32_t i = 0; i < n16; ++i) part += weight;
+        sums[f] = part;
     }
 #pragma unroll
     for (int off = 16; off >= 1; off >>= 1)
 #pragma unroll
         for (int f = 0; f < 6; ++f) sums[f] += __shfl_down_sync(0xFFFFFFFFu, sums[f], off);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        lo[c] = __reduce_min_sync(0xFFFFFFFFu, lo[c]);
-        hi[c] = __reduce_max_sync(0xFFFFFFFFu, hi[c]);
+    // The tight box of the voxels with an open face.
+    const uint32_t any = open[0] | open[1] | open[2] | open[3] | open[4] | open[5];
+    const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
+    const uint32_t rows = ((any & 0xFFu) ? 1u : 0u) | ((any & 0xFF00u) ? 2u : 0u) | ((any & 0xFF0000u) ? 4u : 0u) |
+                          ((any & 0xFF000000u) ? 8u : 0u);
+    const uint32_t xm = __reduce_or_sync(0xFFFFFFFFu, (any | (any >> 8) | (any >> 16) | (any >> 24)) & 0xFFu);
+    const uint32_t ym = __reduce_or_sync(0xFFFFFFFFu, rows << (4 * kyh));
+    const uint32_t zm = __reduce_or_sync(0xFFFFFFFFu, (any ? 1u : 0u) << kz);
+    uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+    if (xm) {
+        lo[0] = __ffs(xm) - 1;
+        lo[1] = __ffs(ym) - 1;
+        lo[2] = __ffs(zm) - 1;
+        hi[0] = 32 - __clz(xm);
+        hi[1] = 32 - __clz(ym);
+        hi[2] = 32 - __clz(zm);
     }
     // Zero padding of the record's last unit.
     const uint32_t padded = (w.units[k] - 3) * 4;
@@ -615,10 +629,6 @@ __global__ void __launch_bounds__(128) light_write_kernel(const LightWriteArgs w
         const uint32_t gm = (1u << gs) - 1u;
         const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
         const uint32_t org[3] = {((uint32_t)bx & gm) * 8, ((uint32_t)by & gm) * 8, ((uint32_t)bz & gm) * 8};
-        if (written == 0) {
-            lo[0] = lo[1] = lo[2] = 0;
-            hi[0] = hi[1] = hi[2] = 0;
-        }
         const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << gs) | (((uint32_t)bz & gm) << (2 * gs));
         BrickLightRecord h;
         for (int f = 0; f < 6; ++f) h.face[f] = sums[f];
@@ -928,7 +938,8 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         uint32_t* totals = order;  // m words
         uint32_t* group_start = tmp;
         uint32_t* offsets = tmp2;
-        light_measure_kernel<<<blocks_for(32ull * m, 128), 128, 0, stream>>>(la, lbricks, m, counts6, units);
+        light_measure_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(la, lbricks, m,
+                                                                                                  counts6, units);
         light_group_kernel<<<blocks_for(m, kThreads), kThreads, 0, stream>>>(lkeys, m, group_shift, units, totals,
                                                                              group_start);
         uint32_t* d_total = s.status + 6;
@@ -940,7 +951,7 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
         LightWriteArgs wa{la, lkeys, lbricks, m, counts6, units, offsets, group_start, total_units, s.heap,
                           s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick};
-        light_write_kernel<<<blocks_for(32ull * m, 128), 128, 0, stream>>>(wa);
+        light_write_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(wa);
     } else {
         s.heap_words = 4;
         CX_TRY(alloc(s.heap, s.capacity.heap, 4));
