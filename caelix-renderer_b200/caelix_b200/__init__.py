@@ -94,6 +94,22 @@ class CaelixLightBvhStats(C.Structure):
 
 LOG_CALLBACK = C.CFUNCTYPE(None, C.c_int, C.c_char_p, C.c_void_p)
 
+
+class CaelixWorldInfo(C.Structure):
+    _fields_ = [("version", C.c_uint16), ("has_player_pose", C.c_uint16), ("entity_count", C.c_uint32),
+                ("sector_count", C.c_uint64), ("player_position", C.c_float * 3), ("player_rotation", C.c_float * 4)]
+
+
+class CaelixWorldEntity(C.Structure):
+    _fields_ = [("guid", C.c_uint8 * 16), ("position", C.c_float * 3), ("rotation", C.c_float * 4),
+                ("velocity", C.c_float * 6), ("require_update_flags", C.c_uint16), ("flags", C.c_uint8),
+                ("is_protected", C.c_uint8), ("sector_count", C.c_uint32)]
+
+
+class CaelixWorldSector(C.Structure):
+    _fields_ = [("entity", C.c_uint32), ("coord", C.c_int32 * 3), ("region_offset", C.c_uint64),
+                ("region_size", C.c_uint32), ("pad", C.c_uint32)]
+
 # ---------------------------------------------------------------------------------------------
 # Library
 
@@ -138,7 +154,19 @@ class Library:
         L.caelix_light_bvh_get_stats.argtypes = [vp, C.POINTER(CaelixLightBvhStats)]
         L.caelix_light_bvh_set_profiling.argtypes = [vp, C.c_uint32]
         L.caelix_radix_sort_pairs.argtypes = [vp, C.c_uint64, C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint64]
+        L.caelix_world_open.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.caelix_world_close.argtypes = [vp]
+        L.caelix_world_close.restype = None
+        L.caelix_world_get_info.argtypes = [vp, C.POINTER(CaelixWorldInfo)]
+        L.caelix_world_get_entity.argtypes = [vp, C.c_uint32, C.POINTER(CaelixWorldEntity)]
+        L.caelix_world_get_sector.argtypes = [vp, C.c_uint64, C.POINTER(CaelixWorldSector)]
+        L.caelix_world_decode_sector.argtypes = [vp, C.c_uint64, C.c_uint32, vp, vp, vp, C.POINTER(C.c_uint32),
+                                                 C.POINTER(C.c_uint64)]
+        L.caelix_world_upload_entity.argtypes = [vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_int32),
+                                                 C.POINTER(C.c_uint64)]
         for name in (
+            "caelix_world_open", "caelix_world_get_info", "caelix_world_get_entity", "caelix_world_get_sector",
+            "caelix_world_decode_sector", "caelix_world_upload_entity",
             "caelix_device_create", "caelix_device_check", "caelix_light_bvh_create",
             "caelix_light_bvh_build", "caelix_light_bvh_get_view", "caelix_light_bvh_get_stats",
             "caelix_radix_sort_pairs", "caelix_light_bvh_set_profiling",
@@ -460,6 +488,72 @@ class Scene:
         s.set_albedo(vs.albedo)
         s.flush()
         return s
+
+
+class WorldFile:
+    """caelix_world_*: a .cxw world file (format version 8 and older) read on the host."""
+
+    def __init__(self, path: str):
+        self.L = library()
+        handle = C.c_void_p()
+        self.L.check(self.L.lib.caelix_world_open(os.fsencode(path), C.byref(handle)), "caelix_world_open")
+        self.handle = handle
+
+    def close(self):
+        if self.handle:
+            self.L.lib.caelix_world_close(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def info(self) -> CaelixWorldInfo:
+        out = CaelixWorldInfo()
+        self.L.check(self.L.lib.caelix_world_get_info(self.handle, C.byref(out)), "caelix_world_get_info")
+        return out
+
+    def entities(self) -> list:
+        out = []
+        for i in range(self.info().entity_count):
+            e = CaelixWorldEntity()
+            self.L.check(self.L.lib.caelix_world_get_entity(self.handle, i, C.byref(e)), "caelix_world_get_entity")
+            out.append(e)
+        return out
+
+    def sectors(self) -> list:
+        out = []
+        for i in range(self.info().sector_count):
+            s = CaelixWorldSector()
+            self.L.check(self.L.lib.caelix_world_get_sector(self.handle, i, C.byref(s)), "caelix_world_get_sector")
+            out.append(s)
+        return out
+
+    def decode(self, index: int):
+        """(keys int32 [n, 3], blocks uint16 [n, 512], summaries uint32 [n], non-zero value count)."""
+        import numpy as np
+
+        n = C.c_uint32(0)
+        voxels = C.c_uint64(0)
+        self.L.check(self.L.lib.caelix_world_decode_sector(self.handle, index, 0, None, None, None, C.byref(n),
+                                                           C.byref(voxels)), "caelix_world_decode_sector")
+        keys = np.zeros((n.value, 3), np.int32)
+        blocks = np.zeros((n.value, 512), np.uint16)
+        summaries = np.zeros(n.value, np.uint32)
+        self.L.check(self.L.lib.caelix_world_decode_sector(
+            self.handle, index, n.value, keys.ctypes.data, blocks.ctypes.data, summaries.ctypes.data, C.byref(n),
+            C.byref(voxels)), "caelix_world_decode_sector")
+        return keys, blocks, summaries, voxels.value
+
+    def upload_entity(self, entity: int, scene: "Scene", threads: int = 0):
+        """Decodes an entity's sectors and uploads its bricks to the scene; returns (origin, bricks)."""
+        origin = (C.c_int32 * 3)()
+        bricks = C.c_uint64(0)
+        self.L.check(self.L.lib.caelix_world_upload_entity(self.handle, entity, scene.handle, threads, origin,
+                                                           C.byref(bricks)), "caelix_world_upload_entity")
+        return tuple(origin), bricks.value
 
 
 def camera_struct(cam) -> CaelixCamera:

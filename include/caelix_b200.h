@@ -618,6 +618,78 @@ CAELIX_API CaelixResult caelix_batch_get_stats(CaelixBatch* batch, CaelixBatchSt
 /* Rays of one view in the newest run (kernel_launches = 1: the shared persistent launch). */
 CAELIX_API CaelixResult caelix_batch_get_view_stats(CaelixBatch* batch, uint32_t view, CaelixRenderStats* out);
 
+/* ---------------------------------------------------------------------------
+   World files (.cxw, format version 8 and older). Replaces the reference's reader crate
+   (host-rs/caelix-cxw/src/lib.rs: CxwFile::open :207-229, decode :243-248, decode_all :250-259,
+   the read rules of parse_index :339-452, region :455-493 and decode_payload :544-630) and the
+   world loader of its host (host-rs/caelix-app/src/world.rs, WorldLoader::open :93-170 and
+   upload :206-262), for the static world entity of this library's scenes.
+
+   Errors: a file that breaks a read rule returns CAELIX_ERROR_INVALID_ARGUMENT (a newer format
+   version: CAELIX_ERROR_UNSUPPORTED) and logs the reason in the words of the reference's error
+   (bad magic, truncated data at an offset, region size, duplicate sector, brick map counters,
+   inflate failure, payload structure). */
+typedef struct CaelixWorldFile CaelixWorldFile;
+
+typedef struct CaelixWorldInfo
+{
+    uint16_t version;
+    uint16_t has_player_pose; /* version 7+ world record with the pose flag */
+    uint32_t entity_count;
+    uint64_t sector_count;    /* all entities */
+    float player_position[3];
+    float player_rotation[4]; /* quaternion x, y, z, w */
+} CaelixWorldInfo;
+
+/* One entity record after the reader's version migrations (flags bit 0 HasBody, bit 1 Static;
+   before version 6 from the legacy body state; velocity zero before version 4). */
+typedef struct CaelixWorldEntity
+{
+    uint8_t guid[16];
+    float position[3];
+    float rotation[4];
+    float velocity[6]; /* linear xyz, angular xyz */
+    uint16_t require_update_flags;
+    uint8_t flags;
+    uint8_t is_protected;
+    uint32_t sector_count;
+} CaelixWorldEntity;
+
+typedef struct CaelixWorldSector
+{
+    uint32_t entity;
+    int32_t coord[3];
+    uint64_t region_offset;
+    uint32_t region_size;
+    uint32_t pad;
+} CaelixWorldSector;
+
+/* Reads the header, the world record, the entity table and every sector index, and checks every
+   region (CxwFile::open). The file is read into host memory; *out is owned by the caller. */
+CAELIX_API CaelixResult caelix_world_open(const char* path, CaelixWorldFile** out);
+CAELIX_API void caelix_world_close(CaelixWorldFile* file);
+CAELIX_API CaelixResult caelix_world_get_info(const CaelixWorldFile* file, CaelixWorldInfo* out);
+CAELIX_API CaelixResult caelix_world_get_entity(const CaelixWorldFile* file, uint32_t index,
+                                                CaelixWorldEntity* out);
+/* Sectors in entity order, then sector index order. */
+CAELIX_API CaelixResult caelix_world_get_sector(const CaelixWorldFile* file, uint64_t index,
+                                                CaelixWorldSector* out);
+/* Inflates and decodes one sector: its non-air bricks in ascending brick index (a brick whose 512
+   values are all 0 is dropped), entity-local keys (sector coord * 16 + brick in sector), the raw
+   values (voxel x + 8y + 64z), the preview word of each kept brick, and the count of non-zero
+   values. With keys == NULL only *brick_count (and *voxels) are written; otherwise the arrays
+   hold `capacity` bricks (fewer: CAELIX_ERROR_INVALID_ARGUMENT). */
+CAELIX_API CaelixResult caelix_world_decode_sector(const CaelixWorldFile* file, uint64_t index, uint32_t capacity,
+                                                   CaelixBrickKey* keys, uint16_t* blocks, uint32_t* summaries,
+                                                   uint32_t* brick_count, uint64_t* voxels);
+/* Decodes every sector of one entity on `threads` host threads (0 = all) and uploads its bricks
+   to the scene (caelix_scene_upload_bricks), keys moved by -origin, origin = the smallest key of
+   the entity per axis (written to `origin`, may be NULL), so that the world's lowest brick sits
+   at 0. Bricks outside the scene's key range after the move: CAELIX_ERROR_UNSUPPORTED, nothing
+   uploaded. *bricks (may be NULL) = bricks uploaded. */
+CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, uint32_t entity, CaelixScene* scene,
+                                                   uint32_t threads, int32_t origin[3], uint64_t* bricks);
+
 #ifdef __cplusplus
 }
 #endif
