@@ -340,7 +340,9 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
                                        static_cast<uint32_t*>(scene->marks.ptr), scene->mark_epoch, d_list, d_count,
                                        stream);
             if (e == cudaSuccess) e = cx::scene_refinalize(scene->dev, d_list, d_count, 7 * c, stream);
-            if (e == cudaSuccess) e = cx::scene_build_lights(scene->dev, stream, &status);
+            if (e == cudaSuccess)
+                e = cx::scene_build_lights(scene->dev, stream, &status, static_cast<const uint32_t*>(scene->marks.ptr),
+                                           scene->mark_epoch);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(&scene->last_update_records, d_count, 4, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);

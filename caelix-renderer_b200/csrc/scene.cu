@@ -469,15 +469,45 @@ __device__ __forceinline__ void light_open_masks(const BrickFaces& f, uint32_t l
 
 constexpr uint32_t kLightWarps = 4;
 
-// Warp per light brick (sorted order): the family counts and the record's units.
+// The previous build's light records, for a rebuild over the same bricks: a light brick that is
+// not marked with `epoch` (its values, its neighbours' and its power unchanged) keeps its record,
+// copied from the previous heap (prev_unit[b]: its first 16-byte unit there, kNone: none).
+struct LightReuse
+{
+    const uint32_t* prev_unit;  // nullptr: every record is recomputed
+    const uint32_t* prev_heap;
+    const uint32_t* marks;
+    uint32_t epoch;
+};
+
+__device__ __forceinline__ uint32_t reused_unit(const LightReuse& r, uint32_t b)
+{
+    if (!r.prev_unit) return kNone;
+    const uint32_t u = __ldg(r.prev_unit + b);
+    return (u != kNone && __ldg(r.marks + b) != r.epoch) ? u : kNone;
+}
+
+// Warp per light brick (sorted order): the family counts and the record's units (of a reused
+// record, from its header).
 __global__ void __launch_bounds__(kLightWarps * 32) light_measure_kernel(const LightArgs a,
                                                                         const uint32_t* __restrict__ lbricks,
                                                                         uint32_t m, uint32_t* __restrict__ counts6,
-                                                                        uint32_t* __restrict__ units)
+                                                                        uint32_t* __restrict__ units,
+                                                                        const LightReuse reuse)
 {
     const uint32_t k = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const uint32_t lane = threadIdx.x & 31u;
     if (k >= m) return;
+    const uint32_t pu = reused_unit(reuse, lbricks[k]);
+    if (pu != kNone) {
+        if (lane < 6) {
+            const uint32_t* hdr = reuse.prev_heap + 4ull * pu;
+            const uint32_t word = lane < 3 ? hdr[10] : hdr[11];
+            counts6[6 * k + lane] = (word >> (kFamilyCountBits * (lane % 3))) & kFamilyCountMask;
+            if (lane == 0) units[k] = 3 + (4 * hdr[9] + 15) / 16;
+        }
+        return;
+    }
     const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, lbricks[k], lane);
     uint32_t open[6];
     light_open_masks(bf, lane, open);
@@ -538,6 +568,8 @@ struct LightWriteArgs
     uint32_t* light_group;
     uint32_t* light_entry;
     uint32_t* light_brick;
+    LightReuse reuse;
+    uint32_t* unit_of_brick;  // out: the first unit of every light brick's record
 };
 
 __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const LightWriteArgs w)
@@ -565,95 +597,112 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
     }
     const uint32_t rec_unit = 1 + w.offsets[k] + (k == s ? 1 + count : 0);
     uint32_t* rec = w.heap + 4ull * rec_unit;
-    const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, b, lane);
-    s_vox[warp][lane] = bf.v0;
-    s_vox[warp][32 + lane] = bf.v1;
-    __syncwarp();
-    const uint16_t* vox = reinterpret_cast<const uint16_t*>(s_vox[warp]);
-    uint32_t open[6];
-    light_open_masks(bf, lane, open);
-    const float P = a.power[b];
-    const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f;
-    // Entries per family in voxel order: lane k writes the voxels of word k (32k + bit) after the
-    // family's entries of the lanes before it.
-    uint32_t fam_count[6];
-    uint32_t written = 0;
-    float sums[6];
-#pragma unroll
-    for (int f = 0; f < 6; ++f) {
-        const uint32_t c = __popc(open[f]);
-        const uint32_t inc = warp_inclusive_sum(c);
-        fam_count[f] = __shfl_sync(0xFFFFFFFFu, inc, 31);
-        uint32_t* out = rec + 12 + written + (inc - c);
-        uint32_t bits = open[f];
-        while (bits) {
-            const uint32_t bit = __ffs(bits) - 1;
-            bits &= bits - 1;
-            const uint32_t vi = 32 * lane + bit;
-            *out++ = vi | ((uint32_t)vox[vi] << 16);
+    BrickLightRecord h;
+    const uint32_t pu = reused_unit(w.reuse, b);
+    if (pu != kNone) {
+        // The previous build's record, copied whole (header, entries, padding of its last unit).
+        const uint4* src = reinterpret_cast<const uint4*>(w.reuse.prev_heap) + pu;
+        uint4* dst = reinterpret_cast<uint4*>(rec);
+        for (uint32_t i = lane; i < w.units[k]; i += 32) dst[i] = src[i];
+        if (lane == 0) {
+            uint4* hp = reinterpret_cast<uint4*>(&h);
+            hp[0] = src[0];
+            hp[1] = src[1];
+            hp[2] = src[2];
         }
-        written += fam_count[f];
-        // The face sum as sixteen-voxel partial sums (voxels 16l .. 16l + 15 in lane l, the weight
-        // added once per open face), then a tree over the lanes.
-        const uint32_t word = __shfl_sync(0xFFFFFFFFu, open[f], lane >> 1);
-        const uint32_t n16 = __popc((word >> (16 * (lane & 1))) & 0xFFFFu);
-        float part = 0.0f;
-        for (uint32_t i = 0; i < n16; ++i) part += weight;
-        sums[f] = part;
-    }
+    } else {
+        const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, b, lane);
+        s_vox[warp][lane] = bf.v0;
+        s_vox[warp][32 + lane] = bf.v1;
+        __syncwarp();
+        const uint16_t* vox = reinterpret_cast<const uint16_t*>(s_vox[warp]);
+        uint32_t open[6];
+        light_open_masks(bf, lane, open);
+        const float P = a.power[b];
+        const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f;
+        // Entries per family in voxel order: lane k writes the voxels of word k (32k + bit) after the
+        // family's entries of the lanes before it.
+        uint32_t fam_count[6];
+        uint32_t written = 0;
+        float sums[6];
 #pragma unroll
-    for (int off = 16; off >= 1; off >>= 1)
+        for (int f = 0; f < 6; ++f) {
+            const uint32_t c = __popc(open[f]);
+            const uint32_t inc = warp_inclusive_sum(c);
+            fam_count[f] = __shfl_sync(0xFFFFFFFFu, inc, 31);
+            uint32_t* out = rec + 12 + written + (inc - c);
+            uint32_t bits = open[f];
+            while (bits) {
+                const uint32_t bit = __ffs(bits) - 1;
+                bits &= bits - 1;
+                const uint32_t vi = 32 * lane + bit;
+                *out++ = vi | ((uint32_t)vox[vi] << 16);
+            }
+            written += fam_count[f];
+            // The face sum as sixteen-voxel partial sums (voxels 16l .. 16l + 15 in lane l, the weight
+            // added once per open face), then a tree over the lanes.
+            const uint32_t word = __shfl_sync(0xFFFFFFFFu, open[f], lane >> 1);
+            const uint32_t n16 = __popc((word >> (16 * (lane & 1))) & 0xFFFFu);
+            float part = 0.0f;
+            for (uint32_t i = 0; i < n16; ++i) part += weight;
+            sums[f] = part;
+        }
 #pragma unroll
-        for (int f = 0; f < 6; ++f) sums[f] += __shfl_down_sync(0xFFFFFFFFu, sums[f], off);
-    // The tight box of the voxels with an open face.
-    const uint32_t any = open[0] | open[1] | open[2] | open[3] | open[4] | open[5];
-    const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
-    const uint32_t rows = ((any & 0xFFu) ? 1u : 0u) | ((any & 0xFF00u) ? 2u : 0u) | ((any & 0xFF0000u) ? 4u : 0u) |
-                          ((any & 0xFF000000u) ? 8u : 0u);
-    const uint32_t xm = __reduce_or_sync(0xFFFFFFFFu, (any | (any >> 8) | (any >> 16) | (any >> 24)) & 0xFFu);
-    const uint32_t ym = __reduce_or_sync(0xFFFFFFFFu, rows << (4 * kyh));
-    const uint32_t zm = __reduce_or_sync(0xFFFFFFFFu, (any ? 1u : 0u) << kz);
-    uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
-    if (xm) {
-        lo[0] = __ffs(xm) - 1;
-        lo[1] = __ffs(ym) - 1;
-        lo[2] = __ffs(zm) - 1;
-        hi[0] = 32 - __clz(xm);
-        hi[1] = 32 - __clz(ym);
-        hi[2] = 32 - __clz(zm);
+        for (int off = 16; off >= 1; off >>= 1)
+#pragma unroll
+            for (int f = 0; f < 6; ++f) sums[f] += __shfl_down_sync(0xFFFFFFFFu, sums[f], off);
+        // The tight box of the voxels with an open face.
+        const uint32_t any = open[0] | open[1] | open[2] | open[3] | open[4] | open[5];
+        const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
+        const uint32_t rows = ((any & 0xFFu) ? 1u : 0u) | ((any & 0xFF00u) ? 2u : 0u) | ((any & 0xFF0000u) ? 4u : 0u) |
+                              ((any & 0xFF000000u) ? 8u : 0u);
+        const uint32_t xm = __reduce_or_sync(0xFFFFFFFFu, (any | (any >> 8) | (any >> 16) | (any >> 24)) & 0xFFu);
+        const uint32_t ym = __reduce_or_sync(0xFFFFFFFFu, rows << (4 * kyh));
+        const uint32_t zm = __reduce_or_sync(0xFFFFFFFFu, (any ? 1u : 0u) << kz);
+        uint32_t lo[3] = {0, 0, 0}, hi[3] = {0, 0, 0};
+        if (xm) {
+            lo[0] = __ffs(xm) - 1;
+            lo[1] = __ffs(ym) - 1;
+            lo[2] = __ffs(zm) - 1;
+            hi[0] = 32 - __clz(xm);
+            hi[1] = 32 - __clz(ym);
+            hi[2] = 32 - __clz(zm);
+        }
+        // Zero padding of the record's last unit.
+        const uint32_t padded = (w.units[k] - 3) * 4;
+        for (uint32_t e = written + lane; e < padded; e += 32) rec[12 + e] = 0u;
+        if (lane == 0) {
+            const uint32_t gm = (1u << gs) - 1u;
+            const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
+            const uint32_t org[3] = {((uint32_t)bx & gm) * 8, ((uint32_t)by & gm) * 8, ((uint32_t)bz & gm) * 8};
+            const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << gs) | (((uint32_t)bz & gm) << (2 * gs));
+            for (int f = 0; f < 6; ++f) h.face[f] = sums[f];
+            h.box_lo = (org[0] + lo[0]) | ((org[1] + lo[1]) << 10) | ((org[2] + lo[2]) << 20);
+            h.box_hi = (org[0] + hi[0]) | ((org[1] + hi[1]) << 10) | ((org[2] + hi[2]) << 20);
+            h.pos = pos;
+            h.entry_count = written;
+            h.counts_lo = fam_count[0] | (fam_count[1] << 10) | (fam_count[2] << 20);
+            h.counts_hi = fam_count[3] | (fam_count[4] << 10) | (fam_count[5] << 20);
+            const uint4* hp = reinterpret_cast<const uint4*>(&h);
+            uint4* r4 = reinterpret_cast<uint4*>(rec);
+            r4[0] = hp[0];
+            r4[1] = hp[1];
+            r4[2] = hp[2];
+        }
     }
-    // Zero padding of the record's last unit.
-    const uint32_t padded = (w.units[k] - 3) * 4;
-    for (uint32_t e = written + lane; e < padded; e += 32) rec[12 + e] = 0u;
     if (lane == 0) {
-        const uint32_t gm = (1u << gs) - 1u;
-        const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
-        const uint32_t org[3] = {((uint32_t)bx & gm) * 8, ((uint32_t)by & gm) * 8, ((uint32_t)bz & gm) * 8};
-        const uint32_t pos = ((uint32_t)bx & gm) | (((uint32_t)by & gm) << gs) | (((uint32_t)bz & gm) << (2 * gs));
-        BrickLightRecord h;
-        for (int f = 0; f < 6; ++f) h.face[f] = sums[f];
-        h.box_lo = (org[0] + lo[0]) | ((org[1] + lo[1]) << 10) | ((org[2] + lo[2]) << 20);
-        h.box_hi = (org[0] + hi[0]) | ((org[1] + hi[1]) << 10) | ((org[2] + hi[2]) << 20);
-        h.pos = pos;
-        h.entry_count = written;
-        h.counts_lo = fam_count[0] | (fam_count[1] << 10) | (fam_count[2] << 20);
-        h.counts_hi = fam_count[3] | (fam_count[4] << 10) | (fam_count[5] << 20);
-        const uint4* hp = reinterpret_cast<const uint4*>(&h);
-        uint4* r4 = reinterpret_cast<uint4*>(rec);
-        r4[0] = hp[0];
-        r4[1] = hp[1];
-        r4[2] = hp[2];
         w.headers[k] = h;
+        w.unit_of_brick[b] = rec_unit;
         const uint32_t entry = k - s;
         uint32_t* ie = w.heap + 4ull * (block + 1 + entry);
-        ie[0] = pos;
+        ie[0] = h.pos;
         ie[1] = b;
         ie[2] = rec_unit - block;
         ie[3] = k;
         w.light_group[k] = g;
         w.light_entry[k] = entry;
         w.light_brick[k] = b;
-        atomicAdd(w.group_rows + 8ull * g + 6, written);  // the group's light faces
+        atomicAdd(w.group_rows + 8ull * g + 6, h.entry_count);  // the group's light faces
         if (k == s) {
             uint32_t* bh = w.heap + 4ull * block;
             bh[0] = count;
@@ -781,9 +830,10 @@ static BuildScratch build_scratch(const DeviceScene& s)
 
 void scene_release(DeviceScene& s)
 {
-    void* ptrs[] = {s.keys, s.voxels, s.power, s.records, s.hash_slots, s.bitmap, s.albedo, s.heap, s.group_rows,
-                    s.frames, s.light_headers, s.light_group, s.light_entry, s.light_brick, s.scratch,
-                    s.tree_memory, s.status};
+    void* ptrs[] = {s.keys,          s.voxels,       s.power,        s.records,       s.hash_slots,
+                    s.bitmap,        s.albedo,       s.heap,         s.group_rows,    s.frames,
+                    s.light_headers, s.light_group,  s.light_entry,  s.light_brick,   s.scratch,
+                    s.tree_memory,   s.status,       s.heap_prev,    s.unit_of_brick, s.unit_of_brick_prev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     s = DeviceScene();
@@ -884,9 +934,21 @@ cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_
     return cudaGetLastError();
 }
 
-cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out)
+cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out,
+                               const uint32_t* marks, uint32_t epoch)
 {
     const uint32_t n = s.brick_count;
+    LightReuse reuse{nullptr, nullptr, nullptr, 0};
+    if (marks && s.unit_of_brick) {
+        // The previous build's heap and map become the source; the new ones take the other buffers.
+        std::swap(s.heap, s.heap_prev);
+        std::swap(s.capacity.heap, s.capacity.heap_prev);
+        std::swap(s.unit_of_brick, s.unit_of_brick_prev);
+        std::swap(s.capacity.unit_of_brick, s.capacity.unit_of_brick_prev);
+        reuse = LightReuse{s.unit_of_brick_prev, s.heap_prev, marks, epoch};
+    }
+    CX_TRY(alloc(s.unit_of_brick, s.capacity.unit_of_brick, std::max(n, 1u)));
+    CX_TRY(cudaMemsetAsync(s.unit_of_brick, 0xFF, 4ull * std::max(n, 1u), stream));
     const uint32_t group_shift = s.group_shift;
     const BuildScratch bs = build_scratch(s);
     uint32_t* home = bs.home;
@@ -938,8 +1000,8 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         uint32_t* totals = order;  // m words
         uint32_t* group_start = tmp;
         uint32_t* offsets = tmp2;
-        light_measure_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(la, lbricks, m,
-                                                                                                  counts6, units);
+        light_measure_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(
+            la, lbricks, m, counts6, units, reuse);
         light_group_kernel<<<blocks_for(m, kThreads), kThreads, 0, stream>>>(lkeys, m, group_shift, units, totals,
                                                                              group_start);
         uint32_t* d_total = s.status + 6;
@@ -949,8 +1011,10 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         s.heap_words = 4 * (1 + total_units);
         CX_TRY(alloc(s.heap, s.capacity.heap, s.heap_words));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
-        LightWriteArgs wa{la, lkeys, lbricks, m, counts6, units, offsets, group_start, total_units, s.heap,
-                          s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick};
+        LightWriteArgs wa{la,           lkeys,         lbricks,         m,           counts6,
+                          units,        offsets,       group_start,     total_units, s.heap,
+                          s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick,
+                          reuse,        s.unit_of_brick};
         light_write_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(wa);
     } else {
         s.heap_words = 4;

@@ -79,11 +79,17 @@ struct DeviceScene
     LightBvhBuffers tree;
     uint32_t tree_capacity = 0;
     uint32_t* status = nullptr;  // device status word of the build
+    // The light records kept for the next rebuild over the same bricks: the first unit of every
+    // brick's light record in `heap` (0xFFFFFFFF: none), and the previous heap and map (the
+    // buffers a rebuild over the same bricks copies unchanged records from, then swaps).
+    uint32_t* unit_of_brick = nullptr;
+    uint32_t* unit_of_brick_prev = nullptr;
+    uint32_t* heap_prev = nullptr;
     // Element capacities of the buffers above: a rebuild reallocates a buffer only to grow it.
     struct
     {
         uint64_t keys, voxels, power, albedo, scratch, hash_slots, bitmap, records, group_rows, light_headers,
-            light_group, light_entry, light_brick, frames, heap;
+            light_group, light_entry, light_brick, frames, heap, heap_prev, unit_of_brick, unit_of_brick_prev;
     } capacity{};
 };
 
@@ -101,10 +107,14 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
                                cudaStream_t stream, uint32_t* device_status_out);
 // The parts of a rebuild whose brick set is unchanged (same keys, same order): the records of the
 // bricks list[0 .. *list_count) (device; at most max_count) finalized again from s.voxels, then
-// (scene_build_lights) the light records of every brick and the light tree. Synchronous.
+// (scene_build_lights) the light records and the light tree. Synchronous.
 cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_t* list_count, uint32_t max_count,
                              cudaStream_t stream);
-cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out);
+// The light records of every light brick and the light tree. With `marks` (a rebuild over the
+// same bricks as the previous one), a light brick b with marks[b] != epoch keeps its previous
+// record (copied); the others are recomputed.
+cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out,
+                               const uint32_t* marks = nullptr, uint32_t epoch = 0);
 
 // ---- device-resident brick staging (staging.cu) ----
 // Copies brick src_index[j] of an upload (src, device, 512 values per brick) to staging slot
