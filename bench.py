@@ -582,31 +582,55 @@ def measure_flush(args, world, local, dev, stream):
     device staging: slot sort and gather, hash table, bitmap, records, light records, light tree);
     per step an edit of 1 % of the bricks (their values uploaded again) and its flush (incremental:
     the edited bricks and their neighbours finalized again, light records and light tree rebuilt);
-    then a light-options change (the light tree alone) and a full rebuild (a new brick)."""
+    then a light-options change (the light tree alone) and a full rebuild (a new brick). The bricks
+    are loaded from a .cxw world file written from the generated world (its read, decode and upload
+    timed as `world_file`)."""
     import numpy as np
 
     import caelix_b200
     from caelix_b200 import workloads
+
+    import tempfile
+
+    from caelix_b200 import cxw
 
     nb = args.flush_bricks
     vs = workloads.noise_world_large(occupied_bricks=nb, emissive_bricks=max(1, nb // 20))
     scene = caelix_b200.Scene(dev, vs.group_shift)
     renderer = caelix_b200.Renderer(dev, scene)
     sptr = stream.cuda_stream
-    t0 = time.perf_counter()
-    scene.upload_bricks(vs.keys, vs.voxels)
-    upload_s = time.perf_counter() - t0
-    em = vs.power > 0
-    scene.set_brick_power(vs.keys[em], vs.power[em])
+    # The bricks arrive from a .cxw world file: read, decoded on every host thread, uploaded.
+    with tempfile.TemporaryDirectory() as tmp:
+        path = os.path.join(tmp, "world.cxw")
+        t0 = time.perf_counter()
+        data = cxw.from_voxel_scene(vs)
+        with open(path, "wb") as fh:
+            fh.write(data)
+        write_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        wfile = caelix_b200.WorldFile(path)
+        open_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        origin, loaded = wfile.upload_entity(0, scene)
+        upload_s = time.perf_counter() - t0
+        wfile.close()
+    # The reader drops all-air bricks; the scene holds the others, moved to the returned origin.
+    keep = (vs.voxels != 0).any(axis=1)
+    assert loaded == int(keep.sum())
+    keys = vs.keys[keep] - np.array(origin, np.int32)
+    voxels, power = vs.voxels[keep], vs.power[keep]
+    threads = os.cpu_count() or 1
+    em = power > 0
+    scene.set_brick_power(keys[em], power[em])
     scene.set_albedo(vs.albedo)
     scene.flush(sptr)
     first_ms = float(renderer.timings().flush_ms)
     rng = np.random.default_rng(5)
     edit_ms, edit_upload_s = [], []
     for k in range(args.warmup + args.steps):
-        edit = rng.choice(vs.brick_count, size=max(1, vs.brick_count // 100), replace=False)
+        edit = rng.choice(len(keys), size=max(1, len(keys) // 100), replace=False)
         t0 = time.perf_counter()
-        scene.upload_bricks(vs.keys[edit], vs.voxels[edit])
+        scene.upload_bricks(keys[edit], voxels[edit])
         up = time.perf_counter() - t0
         scene.flush(sptr)
         if k >= args.warmup:
@@ -616,8 +640,8 @@ def measure_flush(args, world, local, dev, stream):
     scene.flush(sptr)
     tree_ms = float(renderer.timings().flush_ms)
     # A brick at the first free cell of the grid: the key set changes, so the flush rebuilds all.
-    gx, gy, gz = vs.grid
-    lin = vs.keys[:, 0].astype(np.int64) + gx * (vs.keys[:, 1] + gy * vs.keys[:, 2].astype(np.int64))
+    gx, gy, gz = (int(v) for v in keys.max(axis=0) + 1)
+    lin = keys[:, 0].astype(np.int64) + gx * (keys[:, 1] + gy * keys[:, 2].astype(np.int64))
     free = np.setdiff1d(np.arange(min(gx * gy * gz, len(lin) + 1)), lin)[0]
     key = np.array([[free % gx, (free // gx) % gy, free // (gx * gy)]], np.int32)
     scene.upload_bricks(key, np.full((1, 512), 0x8001, np.uint16))
@@ -627,19 +651,23 @@ def measure_flush(args, world, local, dev, stream):
     scene.close()
     ms = max_over_ranks(float(np.mean(edit_ms)), world)
     full = max_over_ranks(full_ms, world)
-    achieved = vs.brick_count * FLUSH_BYTES_PER_BRICK / (full / 1e3) / 1e9
+    achieved = len(keys) * FLUSH_BYTES_PER_BRICK / (full / 1e3) / 1e9
     peak, peak_kind = measured_peaks()
     return {
-        "workload": f"scene flush of the 256x256x64-brick world with {vs.brick_count} occupied bricks "
+        "workload": f"scene flush of the 256x256x64-brick world with {len(keys)} occupied bricks "
                     f"({int(em.sum())} emissive): incremental flush after re-uploading 1% of the bricks",
-        "bricks": int(vs.brick_count),
-        "edit_bricks": int(max(1, vs.brick_count // 100)),
+        "bricks": int(len(keys)),
+        "edit_bricks": int(max(1, len(keys) // 100)),
         "edit_flush_ms": ms,
         "edit_upload_s": float(np.mean(edit_upload_s)),
         "first_flush_ms": first_ms,
         "full_rebuild_ms": full,
         "light_tree_flush_ms": tree_ms,
-        "upload_s": upload_s,
+        "world_file": {"bytes": len(data), "write_s": write_s, "open_s": open_s,
+                       "decode_upload_s": upload_s, "bricks": int(loaded), "host_threads": threads,
+                       "mbricks_per_s": loaded / upload_s / 1e6,
+                       "note": "caelix_world_open + caelix_world_upload_entity (raw inflate and decode on every "
+                               "host thread, then caelix_scene_upload_bricks per sector)"},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "peak_kind": peak_kind, "traffic": None,
                      "kernel": f"the full rebuild ({FLUSH_BYTES_PER_BRICK} algorithmic bytes per brick)"},

@@ -1,4 +1,5 @@
-"""Writer of synthetic .cxw world files for the reader tests (test infrastructure).
+"""Writer of .cxw world files (format version 8 and older): synthetic worlds for the reader's tests
+and generated scenes saved as world files (`from_voxel_scene`).
 
 The layout follows the format's read rules (little-endian throughout):
   header (64 bytes): magic u32 ("CXLS", legacy "VXLS"), version u16, flags u16 (1 = Deflate),
@@ -20,7 +21,9 @@ from __future__ import annotations
 
 import struct
 import zlib
-from dataclasses import dataclass, field
+from dataclasses import dataclass
+
+import numpy as np
 
 FILE_MAGIC = 0x534C5843
 LEGACY_FILE_MAGIC = 0x534C5856
@@ -32,15 +35,15 @@ def deflate_raw(raw: bytes) -> bytes:
     return c.compress(raw) + c.flush()
 
 
-def preview_word(bi: int) -> int:
-    """A recognisable preview word per brick index."""
+def preview_word(bi):
+    """A recognisable preview word per brick index (an int or an array of them)."""
     return 0xA5A00000 | (bi << 8) | 0x0F
 
 
 @dataclass
 class Sector:
     coord: tuple
-    bricks: list  # (brick index in the sector 0..4095, 512 uint16 values)
+    bricks: object  # [(brick index 0..4095, 512 uint16 values)], or (indices [n], values [n, 512])
     free: int = 0  # free brick ids, below the used ones (so the used ids are remapped)
     physics_slot_first: bool = False  # a stride-1 slot record before the block slot
     payload_magic: int = PAYLOAD_MAGIC
@@ -48,6 +51,14 @@ class Sector:
     counts: tuple | None = None  # (capacity, count, free) written instead of the true ones
     block_stride: int = 2
     truncate_payload: int = 0  # bytes cut from the end of the raw payload
+
+    def arrays(self):
+        """(brick indices int64 [n], values uint16 [n, 512]) of the bricks, in list order."""
+        if isinstance(self.bricks, tuple):
+            return self.bricks
+        bi = np.array([b for b, _ in self.bricks], np.int64)
+        values = np.array([v for _, v in self.bricks], np.uint16).reshape(len(self.bricks), 512)
+        return bi, values
 
 
 @dataclass
@@ -74,26 +85,24 @@ class World:
 
 
 def payload(s: Sector) -> bytes:
-    n = len(s.bricks)
+    bis, values = s.arrays()
+    n = len(bis)
     capacity = n + s.free
-    indices = [-1] * 4096
-    for i, (bi, _) in enumerate(s.bricks):
-        indices[bi] = capacity - 1 - i  # used ids from the top down
+    indices = np.full(4096, -1, np.int16)
+    indices[bis] = capacity - 1 - np.arange(n)  # used ids from the top down
     cap, cnt, fr = s.counts if s.counts else (capacity, n, s.free)
     out = bytearray(struct.pack("<4I", s.payload_magic, cap, cnt, fr))
-    out += struct.pack("<4096h", *indices)
-    out += struct.pack(f"<{s.free}h", *range(s.free))
+    out += indices.astype("<i2").tobytes()
+    out += np.arange(s.free, dtype="<i2").tobytes()
     out += struct.pack("<H", 1) + bytes(4096 * 2)
     out += struct.pack("<I", 2 if s.physics_slot_first else 1)
     if s.physics_slot_first:
         out += struct.pack("<BH", 1, 1) + bytes([0x7E]) * (capacity * 512)
     out += struct.pack("<BH", 0, s.block_stride)
-    block = [0xFFFF] * (capacity * 512)  # free ids hold values that must never be read
-    for i, (_, values) in enumerate(s.bricks):
-        bid = capacity - 1 - i
-        block[bid * 512:(bid + 1) * 512] = [int(v) for v in values]
     if s.block_stride == 2:
-        out += struct.pack(f"<{capacity * 512}H", *block)
+        block = np.full((capacity, 512), 0xFFFF, "<u2")  # free ids hold values that must never be read
+        block[capacity - 1 - np.arange(n)] = values
+        out += block.tobytes()
     else:
         out += bytes(capacity * 512 * s.block_stride)
     if s.truncate_payload:
@@ -120,10 +129,10 @@ def build(w: World) -> bytes:
         for s in e.sectors:
             compressed = s.compressed if s.compressed is not None else deflate_raw(payload(s))
             region_offset = regions_start + len(regions)
-            preview = [0] * 4096
-            for bi, _ in s.bricks:
-                preview[bi] = preview_word(bi)
-            regions += struct.pack("<4096I", *preview)
+            preview = np.zeros(4096, "<u4")
+            bis = s.arrays()[0]
+            preview[bis] = preview_word(bis.astype(np.uint32))
+            regions += preview.tobytes()
             regions += struct.pack("<I", len(compressed)) + compressed
             index += struct.pack("<3iQI", *s.coord, region_offset, 16388 + len(compressed))
         body += index + regions
@@ -163,3 +172,20 @@ def expected_sector(s: Sector):
         blocks.append(list(values))
         summaries.append(preview_word(bi))
     return keys, blocks, summaries, voxels
+
+
+def from_voxel_scene(vs, shift=(0, 0, 0), version: int = 8) -> bytes:
+    """A .cxw file holding the bricks of a workloads.VoxelScene as one static entity, the brick
+    keys moved by `shift` bricks (sectors of 16^3 bricks; all-air bricks are written too, the
+    reader drops them)."""
+    keys = np.asarray(vs.keys, np.int64) + np.asarray(shift, np.int64)
+    coords = keys // 16
+    local = keys - coords * 16
+    bi = local[:, 0] + 16 * (local[:, 1] + 16 * local[:, 2])
+    order = np.lexsort((bi, coords[:, 0], coords[:, 1], coords[:, 2]))
+    c = coords[order]
+    starts = np.flatnonzero(np.r_[True, (c[1:] != c[:-1]).any(axis=1)])
+    ends = np.r_[starts[1:], len(order)]
+    voxels = np.asarray(vs.voxels, np.uint16)
+    sectors = [Sector(tuple(int(v) for v in c[a]), (bi[order[a:b]], voxels[order[a:b]])) for a, b in zip(starts, ends)]
+    return build(World(version, [Entity(sectors, flags_byte=2)]))

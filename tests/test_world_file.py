@@ -2,13 +2,13 @@
 (versions 2 to 8), payload details (free lists and remapped brick ids, all-air bricks, extra slot
 records, negative sector coordinates), and every read rule's error. The cases follow the
 reference reader's tests (host-rs/caelix-cxw/tests/synthetic.rs); the files come from
-tests/cxw_writer.py."""
+caelix_b200/cxw.py."""
 import struct
 
 import numpy as np
 import pytest
 
-import cxw_writer as W
+from caelix_b200 import cxw as W
 
 
 def open_world(tmp_path, data: bytes, name="w.cxw"):

@@ -4,23 +4,12 @@ flushed scene equals the oracle's build of the same bricks moved to the returned
 import numpy as np
 import pytest
 
-import cxw_writer as W
+from caelix_b200 import cxw as W
 import oracle_lib
 from caelix_b200 import workloads
 from test_trace_gpu import assert_scene_equal
 
 pytestmark = pytest.mark.gpu
-
-
-def world_of(vs, shift):
-    """The bricks of `vs` as one entity's sectors, keys moved by `shift` bricks."""
-    sectors = {}
-    for k, vox in zip(vs.keys, vs.voxels):
-        g = [int(k[a]) + shift[a] for a in range(3)]
-        coord = tuple(v // 16 for v in g)
-        bi = (g[0] % 16) + 16 * ((g[1] % 16) + 16 * (g[2] % 16))
-        sectors.setdefault(coord, []).append((bi, [int(v) for v in vox]))
-    return W.World(8, [W.Entity([W.Sector(c, b) for c, b in sorted(sectors.items())])])
 
 
 def test_world_file_into_scene(cuda_device, oracle, tmp_path):
@@ -29,7 +18,7 @@ def test_world_file_into_scene(cuda_device, oracle, tmp_path):
     vs = workloads.noise_world(grid_bricks=(20, 12, 18), brick_occupancy=0.4, emissive_fraction=0.05, seed=21)
     shift = (-37, 5, -16)
     path = tmp_path / "world.cxw"
-    path.write_bytes(W.build(world_of(vs, shift)))
+    path.write_bytes(W.from_voxel_scene(vs, shift))
     f = caelix_b200.WorldFile(str(path))
     scene = caelix_b200.Scene(cuda_device, vs.group_shift)
     origin, bricks = f.upload_entity(0, scene, threads=4)
