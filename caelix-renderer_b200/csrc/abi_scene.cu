@@ -139,8 +139,11 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     if (count == 0) return CAELIX_OK;
     cudaSetDevice(scene->device->ordinal);
     cudaStream_t st = scene->upload_stream;
-    // Slots: new keys take the next slots (with any power set before their upload).
+    // Slots: new keys take the next slots (with any power set before their upload). A failure
+    // below gives the new slots back, so the scene stays as it was before the call.
     const uint32_t old_slots = (uint32_t)scene->slot_power.size();
+    const int32_t old_max[3] = {scene->key_max[0], scene->key_max[1], scene->key_max[2]};
+    std::vector<std::pair<uint64_t, float>> taken_power;
     std::vector<uint32_t> slot(count);
     for (uint32_t i = 0; i < count; ++i) {
         const uint64_t packed = pack_key(keys[i]);
@@ -153,10 +156,24 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
             scene->key_max[2] = std::max(scene->key_max[2], keys[i].z);
             const auto p = scene->pending_power.find(packed);
             scene->slot_power.push_back(p != scene->pending_power.end() ? p->second : 0.0f);
-            if (p != scene->pending_power.end()) scene->pending_power.erase(p);
+            if (p != scene->pending_power.end()) {
+                taken_power.emplace_back(p->first, p->second);
+                scene->pending_power.erase(p);
+            }
         }
     }
     const uint32_t slots = (uint32_t)scene->slot_power.size();
+    auto give_back = [&](CaelixResult r) {
+        for (uint32_t s = old_slots; s < slots; ++s) {
+            const CaelixBrickKey k{scene->keys[3ull * s], scene->keys[3ull * s + 1], scene->keys[3ull * s + 2]};
+            scene->slot_of.erase(pack_key(k));
+        }
+        scene->keys.resize(3ull * old_slots);
+        scene->slot_power.resize(old_slots);
+        for (int a = 0; a < 3; ++a) scene->key_max[a] = old_max[a];
+        for (const auto& kv : taken_power) scene->pending_power.insert(kv);
+        return r;
+    };
     // Staging growth (doubling), the resident slots carried over.
     if (slots > scene->stage_capacity) {
         const uint32_t cap = std::max<uint32_t>(slots, std::max<uint32_t>(2 * scene->stage_capacity, 1024));
@@ -173,7 +190,7 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
         if (e != cudaSuccess) {
             if (nk) cudaFree(nk);
             if (nv) cudaFree(nv);
-            return cx::cuda_result(e, "caelix_scene_upload_bricks");
+            return give_back(cx::cuda_result(e, "caelix_scene_upload_bricks"));
         }
         if (scene->stage_keys) cudaFree(scene->stage_keys);
         if (scene->stage_voxels) cudaFree(scene->stage_voxels);
@@ -199,16 +216,8 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     }
     const uint32_t unique = (uint32_t)dst.size();
     lists.insert(lists.end(), dst.begin(), dst.end());
-    if (slots > old_slots) scene->full_rebuild = true;
-    scene->slot_dirty.resize(slots, 0);
-    for (uint32_t s : dst) {
-        if (!scene->slot_dirty[s]) {
-            scene->slot_dirty[s] = 1;
-            scene->dirty_slots.push_back(s);
-        }
-    }
     CaelixResult r = scene->upload.reserve(1024ull * count + 4ull * lists.size(), "caelix_scene_upload_bricks");
-    if (r != CAELIX_OK) return r;
+    if (r != CAELIX_OK) return give_back(r);
     uint16_t* d_blocks = static_cast<uint16_t*>(scene->upload.ptr);
     uint32_t* d_lists = reinterpret_cast<uint32_t*>(d_blocks + 512ull * count);
     cudaError_t e = cudaMemcpyAsync(d_blocks, blocks, 1024ull * count, cudaMemcpyHostToDevice, st);
@@ -220,7 +229,16 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
         e = cx::staging_scatter(d_blocks, d_lists, d_lists + unique, unique, scene->stage_voxels, st);
     // The caller may reuse its buffers on return, and the next flush reads the staging.
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_upload_bricks");
+    if (e != cudaSuccess) return give_back(cx::cuda_result(e, "caelix_scene_upload_bricks"));
+    // The call's slots are edits of the next flush (a new key: a full rebuild).
+    if (slots > old_slots) scene->full_rebuild = true;
+    scene->slot_dirty.resize(slots, 0);
+    for (uint32_t s : dst) {
+        if (!scene->slot_dirty[s]) {
+            scene->slot_dirty[s] = 1;
+            scene->dirty_slots.push_back(s);
+        }
+    }
     if (consumed) *consumed = count;
     return CAELIX_OK;
     CAELIX_GUARD_END
