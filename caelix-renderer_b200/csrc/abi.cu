@@ -96,7 +96,49 @@ struct CaelixLightBvh
     bool built = false;
     bool profiled = false;
     uint32_t launches = 0;
+    // The build as a CUDA graph, replayed while the inputs stay the same (one submission instead
+    // of a launch per kernel: a small build is bound by launch latency, not by its work).
+    cudaStream_t capture_stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cx::LightBvhInput graph_input{};
 };
+
+namespace {
+
+bool same_input(const cx::LightBvhInput& a, const cx::LightBvhInput& b)
+{
+    return a.records == b.records && a.count == b.count && a.record_group == b.record_group &&
+           a.record_entry == b.record_entry && a.group_frames == b.group_frames && a.group_count == b.group_count &&
+           a.sort_keys_per_thread == b.sort_keys_per_thread;
+}
+
+// The build of `in` as an instantiated graph (captured on the object's own stream).
+cudaError_t capture_build(CaelixLightBvh* bvh, const cx::LightBvhInput& in)
+{
+    if (bvh->graph) {
+        cudaGraphExecDestroy(bvh->graph);
+        bvh->graph = nullptr;
+    }
+    if (!bvh->capture_stream) CX_TRY(cudaStreamCreateWithFlags(&bvh->capture_stream, cudaStreamNonBlocking));
+    CX_TRY(cudaStreamBeginCapture(bvh->capture_stream, cudaStreamCaptureModeThreadLocal));
+    const cudaError_t built = cx::lt_build(bvh->buffers, in, bvh->capture_stream, nullptr);
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ended = cudaStreamEndCapture(bvh->capture_stream, &graph);
+    if (built != cudaSuccess || ended != cudaSuccess) {
+        if (graph) cudaGraphDestroy(graph);
+        return built != cudaSuccess ? built : ended;
+    }
+    const cudaError_t e = cudaGraphInstantiate(&bvh->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+        bvh->graph = nullptr;
+        return e;
+    }
+    bvh->graph_input = in;
+    return cudaSuccess;
+}
+
+}  // namespace
 
 using cx::log;
 
@@ -202,6 +244,9 @@ CAELIX_API void caelix_light_bvh_destroy(CaelixLightBvh* bvh)
     if (bvh->stop) cudaEventDestroy(bvh->stop);
     for (cudaEvent_t ev : bvh->stage)
         if (ev) cudaEventDestroy(ev);
+    if (bvh->last_stream) cudaStreamSynchronize(bvh->last_stream);
+    if (bvh->graph) cudaGraphExecDestroy(bvh->graph);
+    if (bvh->capture_stream) cudaStreamDestroy(bvh->capture_stream);
     cudaFree(bvh->memory);
     delete bvh;
 }
@@ -228,8 +273,15 @@ CAELIX_API CaelixResult caelix_light_bvh_build(CaelixLightBvh* bvh, const Caelix
     in.record_entry = input->record_entry;
     in.group_frames = reinterpret_cast<const cx::GroupFrame*>(input->group_frames);
     in.group_count = input->group_count;
+    // Profiled builds run kernel by kernel (their stage events sit between the launches); others
+    // replay the graph of the same inputs, captured on first use.
+    cudaError_t e = cudaSuccess;
+    if (!bvh->profiling && !(bvh->graph && same_input(bvh->graph_input, in))) e = capture_build(bvh, in);
     cudaEventRecord(bvh->start, s);
-    const cudaError_t e = cx::lt_build(bvh->buffers, in, s, bvh->profiling ? bvh->stage : nullptr);
+    if (e == cudaSuccess) {
+        if (bvh->profiling) e = cx::lt_build(bvh->buffers, in, s, bvh->stage);
+        else e = cudaGraphLaunch(bvh->graph, s);
+    }
     cudaEventRecord(bvh->stop, s);
     bvh->last_stream = s;
     bvh->built = true;
