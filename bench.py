@@ -536,14 +536,19 @@ def measure_large(args, world, local, dev, stream, flush):
     tree_flush_ms = float(renderer.timings().flush_ms)
     # An edit: 1 % of the bricks uploaded again (to the device staging), then the full flush from
     # the staged bricks (device sort and gather of all bricks, records, hash table, light records).
-    edit = np.random.default_rng(5).choice(vs.brick_count, size=vs.brick_count // 100, replace=False)
-    t0 = time.perf_counter()
-    scene.upload_bricks(vs.keys[edit], vs.voxels[edit])
-    edit_upload_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    scene.flush(sptr)
-    edit_flush_wall_s = time.perf_counter() - t0
-    edit_flush_ms = float(renderer.timings().flush_ms)
+    # The first such flush also allocates the second light heap and the edit buffers; the second
+    # one is the steady state.
+    edit_ms = []
+    for k in range(2):
+        edit = np.random.default_rng(5 + k).choice(vs.brick_count, size=vs.brick_count // 100, replace=False)
+        t0 = time.perf_counter()
+        scene.upload_bricks(vs.keys[edit], vs.voxels[edit])
+        edit_upload_s = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        scene.flush(sptr)
+        edit_flush_wall_s = time.perf_counter() - t0
+        edit_ms.append(float(renderer.timings().flush_ms))
+    first_edit_flush_ms, edit_flush_ms = edit_ms
     result = {
         "workload": "2048x2048x512-voxel world (256x256x64 bricks), value noise seed 3, 1920x1080, 4 spp, "
                     "6 bounces, light-tree NEE with MIS",
@@ -558,6 +563,7 @@ def measure_large(args, world, local, dev, stream, flush):
         "light_tree_flush_ms": tree_flush_ms,
         "edit_bricks": int(len(edit)),
         "edit_upload_s": edit_upload_s,
+        "first_edit_flush_ms": first_edit_flush_ms,
         "edit_flush_ms": edit_flush_ms,
         "edit_flush_wall_s": edit_flush_wall_s,
         "generate_s": gen_s,
