@@ -246,3 +246,25 @@ def test_upload_rejects_a_world_wider_than_the_scene(tmp_path):
     code = f.L.lib.caelix_world_upload_entity(f.handle, 0, fake_scene, 2, origin, ctypes.byref(bricks))
     assert code == 2 and "spans 1040 bricks on axis 0" in f.L.log[-1]
     assert bricks.value == 0
+
+
+def test_scene_round_trip(tmp_path):
+    """A generated scene written as a world file (caelix_b200.cxw.from_voxel_scene, keys moved to
+    negative sectors) decodes back to its non-air bricks, sector by sector."""
+    from caelix_b200 import workloads
+
+    vs = workloads.noise_world(grid_bricks=(20, 12, 18), brick_occupancy=0.4, emissive_fraction=0.05, seed=21)
+    vox = vs.voxels.copy()
+    vox[::7] = 0  # all-air bricks are written and dropped by the reader
+    vs = workloads.VoxelScene(vs.grid, vs.keys, vox, vs.power, vs.albedo, vs.camera, vs.group_shift)
+    shift = (-37, 5, -16)
+    f = open_world(tmp_path, W.from_voxel_scene(vs, shift))
+    got = {}
+    for i in range(f.info().sector_count):
+        keys, blocks, summaries, _ = f.decode(i)
+        for k, b in zip(keys, blocks):
+            got[tuple(int(v) for v in k)] = b
+    keep = (vs.voxels != 0).any(axis=1)
+    want = {tuple(int(v) + s for v, s in zip(k, shift)): b for k, b, kp in zip(vs.keys, vs.voxels, keep) if kp}
+    assert got.keys() == want.keys()
+    assert all(np.array_equal(got[k], want[k]) for k in want)
