@@ -51,6 +51,35 @@ struct TilePositions
     __device__ __forceinline__ void add(int k, uint32_t v) { w[k >> 1] += v << (16 * (k & 1)); }
 };
 
+// Stable ranks inside the warp of its KPT x 32 warp-striped keys (element k of lane l is tile
+// element warp_base + 32k + l; elements at or above n take no part): pos.add(k, the number of the
+// warp's earlier keys of the same digit), counts[digit] += the warp's keys of each digit. The lanes
+// of equal digits come from eight ballots; the lowest of them adds their count with one shared
+// atomic and broadcasts the old value.
+template <int KPT>
+__device__ __forceinline__ void warp_rank(const uint32_t (&key)[KPT], uint32_t warp_base, uint32_t n, uint32_t shift,
+                                          uint32_t* counts, TilePositions<KPT>& pos)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t lt = lanemask_lt();
+#pragma unroll
+    for (int k = 0; k < KPT; ++k) {
+        const bool valid = warp_base + k * 32u + lane < n;
+        const uint32_t digit = (key[k] >> shift) & 255u;
+        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);  // invalid lanes have no peers
+#pragma unroll
+        for (int b = 0; b < 8; ++b) {
+            const uint32_t m = __ballot_sync(0xFFFFFFFFu, (digit >> b) & 1u);
+            peers &= ((digit >> b) & 1u) ? m : ~m;
+        }
+        const uint32_t before = __popc(peers & lt);
+        uint32_t running = 0;
+        if (valid && before == 0) running = atomicAdd(&counts[digit], __popc(peers));
+        running = __shfl_sync(0xFFFFFFFFu, running, valid ? __ffs(peers) - 1 : lane);
+        pos.add(k, running + before);
+    }
+}
+
 // One onesweep pass over a tile of 256 * KPT elements. Phases:
 //   1. keys (warp-striped, coalesced) -> digits -> stable rank inside the warp: the lanes of
 //      equal digits from eight ballots, the warp's running count of the digit from one shared
@@ -94,24 +123,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
         const uint32_t i = warp_base + k * 32u + lane;
         key[k] = i < a.n ? __ldg(a.keys_in + i) : 0u;
     }
-    const uint32_t lt = lanemask_lt();
-#pragma unroll
-    for (int k = 0; k < KPT; ++k) {
-        const uint32_t i = warp_base + k * 32u + lane;
-        const bool valid = i < a.n;
-        const uint32_t digit = (key[k] >> a.shift) & 255u;
-        uint32_t peers = __ballot_sync(0xFFFFFFFFu, valid);  // invalid lanes have no peers
-#pragma unroll
-        for (int b = 0; b < 8; ++b) {
-            const uint32_t m = __ballot_sync(0xFFFFFFFFu, (digit >> b) & 1u);
-            peers &= ((digit >> b) & 1u) ? m : ~m;
-        }
-        const uint32_t before = __popc(peers & lt);
-        uint32_t running = 0;
-        if (valid && before == 0) running = atomicAdd(&s_warp_counts[warp][digit], __popc(peers));
-        running = __shfl_sync(0xFFFFFFFFu, running, valid ? __ffs(peers) - 1 : lane);
-        pos.add(k, running + before);
-    }
+    warp_rank<KPT>(key, warp_base, a.n, a.shift, s_warp_counts[warp], pos);
     __syncthreads();
 
     // Phase 2: thread d owns digit d.
@@ -191,6 +203,85 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
     }
 }
 
+// A whole sort of n <= kSmallSortKeys pairs by one CTA: the four passes of the onesweep ranking
+// over one tile held in shared memory (a stable LSD sort: the same permutation as the onesweep
+// passes), then the output with the optional row gather of the last pass. One launch instead of
+// four for the small sorts of small light trees.
+constexpr int kSmallSortKeysPerThread = 16;
+static_assert(kSmallSortKeys == kSortThreads * kSmallSortKeysPerThread, "one tile");
+
+template <bool kIdentity>
+__global__ void __launch_bounds__(kSortThreads) small_sort_kernel(uint32_t* __restrict__ keys,
+                                                                  uint32_t* __restrict__ values, uint32_t n,
+                                                                  const SortGather gather)
+{
+    constexpr int KPT = kSmallSortKeysPerThread;
+    __shared__ uint32_t s_warp_counts[kSortWarps][kRadix];
+    __shared__ uint32_t s_local[kRadix];
+    __shared__ uint32_t s_scan[kSortWarps];
+    __shared__ uint32_t s_keys[kSmallSortKeys];
+    __shared__ uint32_t s_values[kSmallSortKeys];
+    const uint32_t tid = threadIdx.x, lane = tid & 31u, warp = tid >> 5;
+    for (uint32_t i = tid; i < n; i += kSortThreads) {
+        s_keys[i] = keys[i];
+        s_values[i] = kIdentity ? i : values[i];
+    }
+    const uint32_t warp_base = warp * 32u * KPT;
+    for (uint32_t pass = 0; pass < 4; ++pass) {
+        const uint32_t shift = 8 * pass;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) s_warp_counts[w][tid] = 0;
+        __syncthreads();
+        uint32_t key[KPT], val[KPT];
+#pragma unroll
+        for (int k = 0; k < KPT; ++k) {
+            const uint32_t i = warp_base + k * 32u + lane;
+            key[k] = i < n ? s_keys[i] : 0u;
+            val[k] = i < n ? s_values[i] : 0u;
+        }
+        TilePositions<KPT> pos;
+#pragma unroll
+        for (int k = 0; k < KPT / 2; ++k) pos.w[k] = 0;
+        warp_rank<KPT>(key, warp_base, n, shift, s_warp_counts[warp], pos);
+        __syncthreads();
+        // Thread d owns digit d: the warps' exclusive offsets and the tile offset of the digit.
+        const uint32_t d = tid;
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = s_warp_counts[w][d];
+            s_warp_counts[w][d] = total;
+            total += c;
+        }
+        uint32_t tile_total;
+        s_local[d] = block_exclusive_sum<kSortThreads>(total, s_scan, tile_total);
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KPT; ++k) {
+            if (warp_base + k * 32u + lane < n) {
+                const uint32_t digit = (key[k] >> shift) & 255u;
+                const uint32_t p = pos.get(k) + s_local[digit] + s_warp_counts[warp][digit];
+                s_keys[p] = key[k];
+                s_values[p] = val[k];
+            }
+        }
+        __syncthreads();
+    }
+    for (uint32_t i = tid; i < n; i += kSortThreads) {
+        const uint32_t v = s_values[i];
+        keys[i] = s_keys[i];
+        values[i] = v;
+        if (gather.rows_in) {
+            const uint4* src = gather.rows_in + (uint64_t)gather.rows_in_stride * v;
+            uint4* dst = gather.rows_out + 3ull * i;
+            dst[0] = __ldg(src);
+            dst[1] = __ldg(src + 1);
+            dst[2] = __ldg(src + 2);
+            gather.inverse[v] = i;
+        }
+    }
+}
+
 }  // namespace
 
 void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream)
@@ -204,6 +295,12 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
                    const SortGather* gather, uint32_t keys_per_thread)
 {
     if (n == 0) return;
+    if (n <= kSmallSortKeys) {
+        const SortGather g = gather ? *gather : SortGather{nullptr, 0, nullptr, nullptr};
+        if (identity_values) small_sort_kernel<true><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
+        else small_sort_kernel<false><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
+        return;
+    }
     if (!sort_keys_per_thread_ok(keys_per_thread)) keys_per_thread = kSortKeysPerThread;
     const uint32_t tiles = sort_tiles(n, keys_per_thread);
     uint32_t* hist = scratch;

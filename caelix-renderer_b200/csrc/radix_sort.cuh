@@ -29,6 +29,7 @@ constexpr int kSortThreads = 256;
 constexpr int kSortWarps = kSortThreads / 32;
 constexpr int kSortKeysPerThread = 16;  // the default tile: 4096 keys
 constexpr int kSortMinKeysPerThread = 4;  // the smallest tile a caller may pick: 1024 keys
+constexpr uint32_t kSmallSortKeys = 4096;  // up to this many pairs, one CTA sorts in shared memory
 constexpr int kRadix = 256;
 constexpr uint32_t kTileFlagAggregate = 1u << 30;
 constexpr uint32_t kTileFlagPrefix = 2u << 30;
