@@ -77,7 +77,8 @@ struct SortGather
 // words, already zero, with the histograms of all four digits in its first 1024 words
 // (radix_histogram or a fused producer).
 // `keys_per_thread` (4, 8 or 16) sets the tile (256 * keys_per_thread keys); `scratch` then holds
-// sort_scratch_words(n, keys_per_thread) words.
+// sort_scratch_words(n, keys_per_thread) words. Up to kSmallSortKeys pairs one CTA does all four
+// passes in shared memory (one launch; the same permutation; scratch and histograms unused).
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
                    const SortGather* gather = nullptr, uint32_t keys_per_thread = kSortKeysPerThread);
