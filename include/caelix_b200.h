@@ -220,8 +220,8 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* 
                                                 uint32_t count, uint32_t identity_values, uint64_t stream);
 
 /* No counterpart in the reference. The same sort for callers that cannot allocate device memory
-   while they record work (an engine render thread inside a frame capture, a host with a fixed
-   memory budget, code inside a CUDA graph capture): it allocates nothing. Its scratch is an array
+   while they record work (an engine render thread that records a frame and must not stall it on
+   an allocation, a host whose device memory budget is fixed up front): it allocates nothing. Its scratch is an array
    compiled into the library, about 2.4 MB reserved on every GPU that loads it until the process
    exits, so one call sorts at most 262144 pairs (more returns CAELIX_ERROR_INVALID_ARGUMENT).
    Runs on the current CUDA device. The first call on a device looks up the array's device address

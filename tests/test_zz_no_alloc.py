@@ -1,6 +1,6 @@
 """caelix_radix_sort_pairs_static, the sort for callers that cannot allocate device memory while
-they record GPU work (an engine render thread inside a frame capture, a fixed memory budget, a CUDA
-graph capture): it uses a scratch array compiled into the library instead of cudaMalloc.
+they record GPU work (an engine render thread that must not stall a frame on an allocation, a host
+with a fixed memory budget): it uses a scratch array compiled into the library instead of cudaMalloc.
 
 Checked through the C ABI against caelix_radix_sort_pairs (the allocating entry point) on two calls
 in a row with different data (the second call must not see the first call's leftovers in the
