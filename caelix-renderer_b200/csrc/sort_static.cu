@@ -1,9 +1,8 @@
 // caelix_radix_sort_pairs_static: the radix sort for callers that cannot allocate device memory.
 //
 // Some hosts must not call cudaMalloc (or anything that may allocate) on the thread that records
-// their GPU work: a render thread of an engine plugin that records into a frame already being
-// captured, a host with a fixed memory budget set at start-up, or code running inside a CUDA graph
-// capture, where an allocation would fail or break the capture. caelix_radix_sort_pairs keeps a
+// their GPU work: a render thread of an engine plugin that must not stall the frame it records on
+// an allocation, or a host with a fixed device memory budget set at start-up. caelix_radix_sort_pairs keeps a
 // scratch buffer that it grows with cudaMalloc on demand; this variant instead uses a scratch
 // array compiled into the library (a file-scope __device__ array of a fixed size), so a call
 // allocates nothing. The price: the array is reserved on every GPU that loads the library, from
