@@ -178,6 +178,8 @@ def base_line(args, world, metric, value, unit, ms_per_step, config, higher=True
 
 
 TRACE_METRIC = "trace throughput, Mrays/s (primary + bounce + shadow rays counted on the device)"
+BATCH_METRIC = "batched trace throughput, Mrays/s (light-tree rebuild + trace of every scene per step)"
+FLUSH_METRIC = "incremental scene flush time after a 1% edit (ms)"
 TRACE_CONFIG = {
     "workload": "plain brick-DDA trace: 128^3-voxel world (16^3 bricks, 30% occupied, value noise seed 2), "
                 "512x512 pinhole, 1 spp, 4 bounces, light-tree NEE with MIS, fp32 radiance",
@@ -258,6 +260,64 @@ def run_reference(args, world, rank):
         line = base_line(args, args.gpus, "light-tree build throughput (Mleaves/s)", value, "Mleaves/s", None,
                          {"workload": f"light-tree build, {N_LEAVES} brick light records (sampled at {n} per build)"})
         sample = f"independent oracle builds of {n} records on {threads} threads, ~4 s per step"
+    elif args.workload == "flush":
+        # The oracle has no incremental path: every flush is a whole scene build (records, hash
+        # table, light records, light tree) on one thread, timed on a sample of the generator
+        # and scaled by brick count to the 2M-brick world.
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        import oracle_lib
+        from caelix_b200 import workloads
+
+        lib = oracle_lib.load()
+        vs = workloads.noise_world(grid_bricks=(48, 48, 24), brick_occupancy=0.476, voxel_fill=0.25,
+                                   emissive_fraction=0.05, seed=3)
+        for _ in range(min(args.warmup, 1)):
+            oracle_lib.OracleScene(lib, vs).close()
+        per_step = []
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            builds = 0
+            while builds == 0 or time.perf_counter() - t0 < 2.0:
+                oracle_lib.OracleScene(lib, vs).close()
+                builds += 1
+            per_step.append((time.perf_counter() - t0) / builds)
+        value = 1e3 * statistics.mean(per_step) * args.flush_bricks / vs.brick_count
+        line = base_line(args, args.gpus, FLUSH_METRIC, value, "ms", value,
+                         {"workload": f"scene flush of the 256x256x64-brick world with {args.flush_bricks} occupied "
+                                      "bricks (5% emissive)"}, higher=False)
+        threads = 1
+        sample = (f"whole oracle scene builds of a {vs.brick_count}-brick world of the same generator on one thread "
+                  f"(~2 s per step), scaled by brick count to {args.flush_bricks}")
+    elif args.workload == "batch":
+        # The oracle renders the smallest scene of the batch plan at its viewport, 2 spp, 4 bounces,
+        # on every host thread.
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        import oracle_lib
+        from caelix_b200 import workloads
+
+        plan = workloads.batch_plan(args.batch_scenes)
+        i = min(range(len(plan)), key=lambda j: plan[j][0])
+        bricks, side = plan[i]
+        osc = oracle_lib.OracleScene(oracle_lib.load(), workloads.batch_scene(bricks, seed=100 + i))
+        rays = 0
+        secs = 0.0
+        frames = 0
+        for k in range(args.steps):
+            t0 = time.perf_counter()
+            while True:
+                _, r = osc.render(side, side, spp=BATCH_SPP, bounces=BATCH_BOUNCES, seed=1 + k + frames,
+                                  threads=threads)
+                rays += int(r.sum())
+                frames += 1
+                if time.perf_counter() - t0 >= 2.0:
+                    break
+            secs += time.perf_counter() - t0
+        value = rays / secs / 1e6
+        line = base_line(args, args.gpus, BATCH_METRIC, value, "Mrays/s", 1e3 * secs / frames,
+                         {"workload": f"{args.batch_scenes} scenes, brick counts log-uniform in [1k, 500k], square "
+                                      f"viewports among 256/512/1024, {BATCH_SPP} spp, {BATCH_BOUNCES} bounces"})
+        sample = (f"{frames} oracle renders of the plan's smallest scene ({bricks} bricks, {side}x{side}) on "
+                  f"{threads} threads (~2 s per step)")
     else:
         for _ in range(min(args.warmup, 1)):
             oracle_trace(0.0, threads, 5000)
@@ -918,8 +978,7 @@ def run_ours(args, world, rank, local):
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     if args.workload == "batch":
         batch = measure_batch(args, world, local, dev, stream)
-        line = base_line(args, world, "batched trace throughput, Mrays/s (light-tree rebuild + trace of every scene "
-                         "per step)", batch["batched_mrays_per_s"], "Mrays/s", batch["batched_ms"],
+        line = base_line(args, world, BATCH_METRIC, batch["batched_mrays_per_s"], "Mrays/s", batch["batched_ms"],
                          {"workload": batch["workload"], "scenes": batch["scenes"], "spp": BATCH_SPP,
                           "bounces": BATCH_BOUNCES, "l2": "inputs larger than L2 (~10 GB of scenes)",
                           "parallelism": f"replicas x{world}"})
@@ -932,7 +991,7 @@ def run_ours(args, world, rank, local):
         return
     if args.workload == "flush":
         fl = measure_flush(args, world, local, dev, stream)
-        line = base_line(args, world, "incremental scene flush time after a 1% edit (ms)", fl["edit_flush_ms"], "ms",
+        line = base_line(args, world, FLUSH_METRIC, fl["edit_flush_ms"], "ms",
                          fl["edit_flush_ms"], {"workload": fl["workload"], "bricks": fl["bricks"],
                                                "l2": "inputs larger than L2 (2 GB of bricks)",
                                                "parallelism": f"replicas x{world}"}, higher=False)
