@@ -56,8 +56,8 @@ TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record secto
 # DRAM bytes (read + write) measured by ncu (one capture, cold cache; profiles/): a plain onesweep
 # pass at 4,194,304 pairs, scaled per pair; the wavefront frame of the 512 x 512 trace (trace and
 # shade kernels of its 5 bounce iterations).
-SORT_PASS_DRAM_BYTES_PER_PAIR = 35.1e6 / 4194304
-TRACE_FRAME_DRAM_BYTES = 156.8e6
+SORT_PASS_DRAM_BYTES_PER_PAIR = 34.5e6 / 4194304
+TRACE_FRAME_DRAM_BYTES = 154.3e6
 
 
 def measured_peaks():
