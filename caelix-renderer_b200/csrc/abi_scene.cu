@@ -387,6 +387,8 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     CaelixResult r = scene->flush_scratch.reserve_grow(4ull * n + 4 * cx::staging_sort_words(n), "caelix_scene_flush");
     if (r == CAELIX_OK) r = scene->record_of_slot.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
     if (r == CAELIX_OK) r = scene->marks.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
+    // The edit lists of later flushes, sized for edits of up to 1/32 of the bricks.
+    if (r == CAELIX_OK) r = scene->update.reserve_grow(4ull * (9ull * std::max(n / 32, 1024u) + 1), "caelix_scene_flush");
     if (r != CAELIX_OK) return r;
     float* d_power = static_cast<float*>(scene->flush_scratch.ptr);
     uint32_t* sort_scratch = reinterpret_cast<uint32_t*>(d_power + n);

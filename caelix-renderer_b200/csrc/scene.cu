@@ -1021,6 +1021,13 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         CX_TRY(alloc(s.heap, s.capacity.heap, 4));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 16, stream));
     }
+    if (!marks) {
+        // The buffers the next rebuild over the same bricks swaps in, sized now (a full build
+        // allocates anyway; the edit flushes that follow then allocate nothing while the heap
+        // keeps its size).
+        CX_TRY(alloc(s.heap_prev, s.capacity.heap_prev, s.heap_words));
+        CX_TRY(alloc(s.unit_of_brick_prev, s.capacity.unit_of_brick_prev, std::max(n, 1u)));
+    }
 
     // The light tree over the light records (leaf = gather order).
     const uint32_t cap = std::max(m, 1u);
