@@ -86,7 +86,8 @@ cudaError_t adjoint_launch(const SceneView& s, const TraceParams& p, const float
     adj.sample_radiance = samples;
     adj.d_albedo = d_albedo;
     adj.d_power = d_power;
-    return wave_adjoint(d_record, d_replay, plan, d_table, wb, kAdjointBlockWidth, sm_count, adj, stream, launches);
+    return wave_adjoint(s, d_record, d_replay, plan, d_table, wb, kAdjointBlockWidth, sm_count, adj, stream,
+                        launches);
 }
 
 }  // namespace cx

@@ -119,6 +119,9 @@ WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_wi
 // d_views the device copy of `views`, d_table the device copy of plan.table. The views'
 // radiance buffers receive the averaged radiance (the per-frame kernel's result, bit for bit).
 // Kernel launches recorded are added to *launches (may be null).
+// A single view of a scene of at most kWaveResidentBricks bricks (records about 72 MB: they stay
+// in the 126 MB L2) runs the shade kernels at 5 CTAs per SM, anything larger or a batch at 8.
+constexpr uint32_t kWaveResidentBricks = 65536;
 cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
                        const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
                        cudaStream_t stream, uint32_t* launches);
@@ -128,9 +131,9 @@ cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t 
 // radiance buffer when not null, every sample's R into adj.sample_radiance), then the replay of
 // every path (d_replay: the same view without radiance buffer or ray counters) gathering dL/dalbedo
 // and dL/dpower. Gradients are accumulated into (zero them first).
-cudaError_t wave_adjoint(const WaveView* d_record, const WaveView* d_replay, const WavePlan& plan,
-                         const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
-                         const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches);
+cudaError_t wave_adjoint(const SceneView& scene, const WaveView* d_record, const WaveView* d_replay,
+                         const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width,
+                         uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches);
 
 // ---- the batched persistent trace (trace_batch.cu) ----
 

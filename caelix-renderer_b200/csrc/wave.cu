@@ -160,8 +160,12 @@ __device__ __forceinline__ float gsum3(const float G[3], const float t[3], float
     return G[0] * (t[0] * s) + G[1] * (t[1] * s) + G[2] * (t[2] * s);
 }
 
-template <int kMode>
-__global__ void __launch_bounds__(kWaveThreads, 8)
+// kMinBlocks CTAs of 128 threads per SM: 5 (96 registers, few spills) for a scene whose records
+// stay in L2, 8 (64 registers) where the descent and the record loads go to HBM and more warps
+// in flight hide them (measured: 5 is the fastest of 3 .. 8 on the 128^3 world; 8 on the
+// 2 M-brick world and the 64-scene batch).
+template <int kMode, int kMinBlocks>
+__global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity, const WaveAdjoint adj)
 {
     __shared__ float s_albedo[kMode == kShadeReplay ? kMaterialSlots * 3 : 1];
@@ -501,8 +505,9 @@ WavePlan wave_plan(const WaveView* views, uint32_t view_count, uint32_t block_wi
 
 namespace {
 
-// Every sub-wave of every wave of the plan, its shade kernels in mode kMode.
-template <int kMode>
+// Every sub-wave of every wave of the plan, its shade kernels in mode kMode with kMinBlocks CTAs
+// per SM.
+template <int kMode, int kMinBlocks>
 cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b,
                      uint32_t block_width, uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream,
                      uint32_t* launches)
@@ -511,7 +516,7 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
     static int trace_blocks = 0, shade_blocks = 0;
     if (trace_blocks == 0) {
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks, wave_trace_kernel, kWaveThreads, 0));
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel<kShadeRender>,
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel<kMode, kMinBlocks>,
                                                              kWaveThreads, 0));
         trace_blocks = std::max(trace_blocks, 1);
         shade_blocks = std::max(shade_blocks, 1);
@@ -537,7 +542,7 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
             for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
                 const uint32_t parity = it & 1u;
                 wave_trace_kernel<<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
-                wave_shade_kernel<kMode><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
+                wave_shade_kernel<kMode, kMinBlocks><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
                 count += 2;
             }
             CX_TRY(cudaGetLastError());
@@ -549,22 +554,30 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
 
 }  // namespace
 
+bool wave_resident_scene(const SceneView& s) { return s.brick_count <= kWaveResidentBricks; }
+
 cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t view_count, const WavePlan& plan,
                        const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
                        cudaStream_t stream, uint32_t* launches)
 {
-    (void)views;
-    (void)view_count;
     const WaveAdjoint none{nullptr, nullptr, nullptr, nullptr};
-    return wave_run<kShadeRender>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
+    if (view_count == 1 && wave_resident_scene(views[0].scene))
+        return wave_run<kShadeRender, 5>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
+    return wave_run<kShadeRender, 8>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
 }
 
-cudaError_t wave_adjoint(const WaveView* d_record, const WaveView* d_replay, const WavePlan& plan,
-                         const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width, uint32_t sm_count,
-                         const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches)
+cudaError_t wave_adjoint(const SceneView& scene, const WaveView* d_record, const WaveView* d_replay,
+                         const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width,
+                         uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches)
 {
-    CX_TRY(wave_run<kShadeRecord>(d_record, plan, d_table, b, block_width, sm_count, adj, stream, launches));
-    return wave_run<kShadeReplay>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
+    if (wave_resident_scene(scene)) {
+        CX_TRY((wave_run<kShadeRecord, 5>(d_record, plan, d_table, b, block_width, sm_count, adj, stream,
+                                              launches)));
+        return wave_run<kShadeReplay, 5>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
+    }
+    CX_TRY((wave_run<kShadeRecord, 8>(d_record, plan, d_table, b, block_width, sm_count, adj, stream,
+                                          launches)));
+    return wave_run<kShadeReplay, 8>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
 }
 
 }  // namespace cx
