@@ -220,6 +220,12 @@ void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, 
  * out[0..2] position, out[3..5] normal, out[6] pdf, words[0..4] block, voxel, face, group, entry. */
 int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t rng,
                     float out[7], uint32_t words[5]);
+/* count draws of oc_light_sample at one receiver (the reference probe's draw mode,
+ * tests/light_tree_test.cpp:961 CheckHistogram): per draw out[4 i ..] = group, voxel in group
+ * (x | y << 10 | z << 20), face, 1 (all zero for a failed draw). The draws' generator states come
+ * from an xorshift sequence started at seed. */
+void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t seed,
+                    uint32_t count, uint32_t* out);
 /* The light tree pdf of a light face point (caelix_light_tree.hlsl:936-949). */
 float oc_light_point_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
                          uint32_t group, const uint32_t voxel_in_group[3], uint32_t face, uint32_t block);

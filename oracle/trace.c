@@ -615,6 +615,27 @@ int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3],
     return 1;
 }
 
+void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t seed,
+                    uint32_t count, uint32_t* out)
+{
+    uint32_t state = seed != 0u ? seed : 0x9E3779B9u;
+    const uint32_t gs = s->group_shift, gm = (1u << gs) - 1u;
+    for (uint32_t i = 0; i < count; ++i) {
+        float p[7];
+        uint32_t words[5];
+        uint32_t* o = out + 4ull * i;
+        o[0] = o[1] = o[2] = o[3] = 0;
+        if (!oc_light_sample(s, t, x, n, random_u32(&state), p, words)) continue;
+        const uint32_t pos = entry_record(s, words[3], words[4], NULL)[8];
+        const uint32_t vi = words[1];
+        o[0] = words[3];
+        o[1] = ((pos & gm) * 8 + (vi & 7u)) | ((((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u)) << 10) |
+               ((((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)) << 20);
+        o[2] = words[2];
+        o[3] = 1;
+    }
+}
+
 /* LightTreeFindLightFace (caelix_light_tree.hlsl:853-934): with per-brick emitter power, a light
  * voxel is an opaque voxel of a brick that has a brick light record. */
 static int find_light_face(const oc_scene* s, const oc_light_tree* t, const float x[3], uint32_t group,

@@ -209,3 +209,93 @@ def test_oracle_render_properties(osc):
     assert rays[0] == 48 * 48
     img2, rays2 = osc.render(48, 48, spp=1, bounces=4, seed=3, threads=4)
     assert np.array_equal(img, img2) and np.array_equal(rays, rays2)
+
+
+def face_table(osc):
+    """The light faces keyed like the reference's RefFace index: (group, packed voxel in group, face)."""
+    faces = all_light_faces(osc)
+    keys = {}
+    for i, (g, v, f, blk) in enumerate(faces):
+        keys[(g, int(v[0]) | (int(v[1]) << 10) | (int(v[2]) << 20), f)] = i
+    assert len(keys) == len(faces)
+    return faces, keys
+
+
+def face_pdfs(osc, faces, x, n):
+    import ctypes as C
+
+    return np.array([osc.lib.oc_light_point_pdf(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data, g,
+                                                np.ascontiguousarray(v).ctypes.data, f, blk)
+                     for g, v, f, blk in faces], np.float32)
+
+
+@pytest.mark.parametrize("with_normal", [False, True])
+def test_light_sample_histogram(osc, small_scene, with_normal):
+    """2^21 draws at one receiver land on each light face in proportion to its pdf: every face with
+    at least 50 expected draws is within 5 sigma of pdf * draws, and a face of pdf 0 is never drawn
+    (the reference's CheckHistogram, tests/light_tree_test.cpp:961-993)."""
+    import ctypes as C
+
+    faces, keys = face_table(osc)
+    world = np.array(small_scene.grid, np.float32) * 8
+    x = np.ascontiguousarray(world * np.float32(0.45))
+    n = np.zeros(3, np.float32)
+    if with_normal:
+        n = np.array([0.3, 0.8, -0.52], np.float32)
+        n /= np.float32(np.linalg.norm(n))
+    pdfs = face_pdfs(osc, faces, x, n)
+    draws = 1 << 21
+    out = np.zeros((draws, 4), np.uint32)
+    osc.lib.oc_light_draws(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data, 777, draws,
+                           out.ctypes.data)
+    assert np.all(out[:, 3] == 1)
+    packed, inverse = np.unique(out[:, :3], axis=0, return_inverse=True)
+    counts = np.zeros(len(faces), np.int64)
+    per_key = np.bincount(inverse.reshape(-1), minlength=len(packed))
+    for row, c in zip(packed, per_key):
+        index = keys.get((int(row[0]), int(row[1]), int(row[2])))
+        assert index is not None, row
+        counts[index] += c
+    expected = pdfs.astype(np.float64) * draws
+    assert np.all(counts[pdfs == 0.0] == 0)
+    big = expected >= 50.0
+    assert big.sum() > 0
+    assert np.all(np.abs(counts[big] - expected[big]) <= 5.0 * np.sqrt(expected[big])), \
+        np.max(np.abs(counts[big] - expected[big]) / np.sqrt(expected[big]))
+
+
+def test_light_pdf_bound(osc):
+    """A receiver that sees a light face's centre with both cosines above 0.05 gets a positive pdf
+    for that face: the tree's importance bounds never cull a contributing light (the reference's
+    CheckBound, tests/light_tree_test.cpp:995-1064; receivers within 4 or 60 voxels of the centre,
+    every second one without a normal)."""
+    import ctypes as C
+
+    faces = all_light_faces(osc)
+    dirs = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]], np.float32)
+    rng = np.random.default_rng(1234)
+    checked = 0
+    for k in range(4096):
+        g, v, f, blk = faces[int(rng.integers(len(faces)))]
+        fr = osc.group_frames[g]
+        rot = fr["rotation"].reshape(3, 3)
+        centre = rot @ (fr["origin"] + v.astype(np.float32) + 0.5 + 0.5 * dirs[f]) + fr["translation"]
+        normal = rot @ dirs[f]
+        rng_range = 4.0 if k % 3 == 0 else 60.0
+        x = (centre + rng.uniform(-1.0, 1.0, 3) * rng_range).astype(np.float32)
+        m = rng.uniform(-1.0, 1.0, 3)
+        has_normal = k % 2 == 0
+        n = (m / np.linalg.norm(m)).astype(np.float32) if has_normal else np.zeros(3, np.float32)
+        d = x - centre
+        dist = float(np.linalg.norm(d))
+        if dist < 0.5:
+            continue
+        emitter = float(normal @ d) / dist
+        receiving = float(-(n @ d)) / dist if has_normal else 1.0
+        if emitter < 0.05 or receiving < 0.05:
+            continue
+        pdf = osc.lib.oc_light_point_pdf(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data, g,
+                                         np.ascontiguousarray(v).ctypes.data, f, blk)
+        assert pdf > 0.0, (k, g, v, f)
+        checked += 1
+    assert checked > 100
