@@ -226,6 +226,10 @@ int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3],
  * from an xorshift sequence started at seed. */
 void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t seed,
                     uint32_t count, uint32_t* out);
+/* The balance-heuristic MIS weight of one side (caelix_light_nee.hlsl:20-34): p_area is the
+ * light tree's area density of the lamp point, d its distance, cos_l the lamp-side cosine, n_r the
+ * receiver normal, w the unit direction to the lamp; nee_side selects the light-sampling side. */
+float oc_mis_weight(float p_area, const float n_r[3], const float w[3], float d, float cos_l, int nee_side);
 /* The light tree pdf of a light face point (caelix_light_tree.hlsl:936-949). */
 float oc_light_point_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
                          uint32_t group, const uint32_t voxel_in_group[3], uint32_t face, uint32_t block);

@@ -742,6 +742,11 @@ static float mis_weight(float p_area, const float n_r[3], const float w[3], floa
     return (nee_side ? p_sa : p_bsdf) / sum;
 }
 
+float oc_mis_weight(float p_area, const float n_r[3], const float w[3], float d, float cos_l, int nee_side)
+{
+    return mis_weight(p_area, n_r, w, d, cos_l, nee_side);
+}
+
 static void emission_of(const ctx* c, uint32_t record, uint32_t block, float e[3])
 {
     const float p = (block & OPAQUE) ? c->power[record] : 0.0f;

@@ -143,6 +143,8 @@ def _bind_scene(lib):
     lib.oc_light_draws.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
                                    C.c_uint32, C.c_void_p]
     lib.oc_light_draws.restype = None
+    lib.oc_mis_weight.argtypes = [C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_int]
+    lib.oc_mis_weight.restype = C.c_float
     lib.oc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.oc_sincos.restype = None
     lib._scene_bound = True
