@@ -131,9 +131,13 @@ def dist_setup():
     if world > 1:
         import datetime
 
+        import torch
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        # NCCL on the GPU box; gloo where no CUDA device is visible (the host-side tests of the
+        # multi-rank plumbing).
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return world, rank, local
 
 
@@ -143,7 +147,7 @@ def max_over_ranks(value: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    t = torch.tensor([value], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -151,12 +155,15 @@ def max_over_ranks(value: float, world: int) -> float:
 def barrier(world: int):
     import torch
 
-    torch.cuda.synchronize()
+    cuda = torch.cuda.is_available()
+    if cuda:
+        torch.cuda.synchronize()
     if world > 1:
         import torch.distributed as dist
 
         dist.barrier()
-    torch.cuda.synchronize()
+    if cuda:
+        torch.cuda.synchronize()
 
 
 def base_line(args, world, metric, value, unit, ms_per_step, config, higher=True):
