@@ -373,6 +373,7 @@ def _bind_scene(L):
         "caelix_scene_create": [vp, C.POINTER(CaelixSceneDesc), C.POINTER(vp)],
         "caelix_scene_upload_bricks": [vp, C.c_uint32, C.c_uint32, vp, vp, C.POINTER(C.c_uint32)],
         "caelix_scene_set_brick_power": [vp, C.c_uint32, C.c_uint32, vp, vp],
+        "caelix_scene_remove_bricks": [vp, C.c_uint32, C.c_uint32, vp],
         "caelix_scene_set_materials": [vp, vp, C.c_uint32],
         "caelix_scene_set_light_options": [vp, C.POINTER(CaelixLightOptions)],
         "caelix_scene_flush": [vp, C.POINTER(CaelixFrameDesc)],
@@ -437,6 +438,15 @@ class Scene:
                                                            voxels.ctypes.data, C.byref(consumed)),
                      "caelix_scene_upload_bricks")
         return consumed.value
+
+    def remove_bricks(self, keys):
+        """caelix_scene_remove_bricks: keys the scene does not have are ignored; the next flush
+        rebuilds the tables from the remaining bricks."""
+        import numpy as np
+
+        keys = np.ascontiguousarray(keys, np.int32).reshape(-1, 3)
+        self.L.check(self.L.lib.caelix_scene_remove_bricks(self.handle, 0, len(keys), keys.ctypes.data),
+                     "caelix_scene_remove_bricks")
 
     def set_brick_power(self, keys, power):
         import numpy as np

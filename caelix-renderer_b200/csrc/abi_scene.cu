@@ -244,6 +244,74 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     CAELIX_GUARD_END
 }
 
+CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                   const CaelixBrickKey* keys)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || entity != 0 || (count && !keys)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (count == 0) return CAELIX_OK;
+    // Room for the compaction's moves (one per removed key), taken before any state changes.
+    CaelixResult r = scene->upload.reserve(8ull * count, "caelix_scene_remove_bricks");
+    if (r != CAELIX_OK) return r;
+    // The slots stay dense: the last slot moves into the removed one. `source` maps a slot that
+    // took another brick to the slot that brick had before this call.
+    const uint32_t old_slots = (uint32_t)scene->slot_power.size();
+    uint32_t n = old_slots;
+    std::unordered_map<uint32_t, uint32_t> source;
+    for (uint32_t i = 0; i < count; ++i) {
+        if (!key_ok(keys[i])) continue;
+        const auto it = scene->slot_of.find(pack_key(keys[i]));
+        if (it == scene->slot_of.end()) continue;
+        const uint32_t s = it->second;
+        scene->slot_of.erase(it);
+        const uint32_t last = n - 1;
+        if (s != last) {
+            const CaelixBrickKey k{scene->keys[3ull * last], scene->keys[3ull * last + 1], scene->keys[3ull * last + 2]};
+            scene->slot_of[pack_key(k)] = s;
+            for (int a = 0; a < 3; ++a) scene->keys[3ull * s + a] = scene->keys[3ull * last + a];
+            scene->slot_power[s] = scene->slot_power[last];
+            const auto m = source.find(last);
+            const uint32_t from = m != source.end() ? m->second : last;
+            source[s] = from;
+        }
+        source.erase(last);
+        n = last;
+    }
+    if (n == old_slots) return CAELIX_OK;
+    scene->keys.resize(3ull * n);
+    scene->slot_power.resize(n);
+    scene->slot_dirty.assign(n, 0);
+    scene->dirty_slots.clear();
+    scene->upload_mark.resize(n, 0);
+    for (int a = 0; a < 3; ++a) scene->key_max[a] = 0;
+    for (uint32_t s = 0; s < n; ++s)
+        for (int a = 0; a < 3; ++a) scene->key_max[a] = std::max(scene->key_max[a], scene->keys[3ull * s + a]);
+    // The key set changed: the next flush rebuilds the tables from the remaining slots.
+    scene->full_rebuild = true;
+    // Every destination is a remaining slot and every source a slot past the end, so the device
+    // moves never overlap.
+    std::vector<uint32_t> moves;
+    moves.reserve(2 * source.size());
+    for (const auto& kv : source) {
+        if (kv.first >= n || kv.second < n || kv.second >= old_slots) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_remove_bricks: bad staging move %u <- %u", kv.first, kv.second);
+            return CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+        moves.push_back(kv.first);
+        moves.push_back(kv.second);
+    }
+    if (moves.empty()) return CAELIX_OK;
+    cudaSetDevice(scene->device->ordinal);
+    cudaStream_t st = scene->upload_stream;
+    uint32_t* d_moves = static_cast<uint32_t*>(scene->upload.ptr);
+    cudaError_t e = cudaMemcpyAsync(d_moves, moves.data(), 4ull * moves.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cx::staging_move(scene->stage_keys, scene->stage_voxels, d_moves, (uint32_t)(moves.size() / 2), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    return e == cudaSuccess ? CAELIX_OK : cx::cuda_result(e, "caelix_scene_remove_bricks");
+    CAELIX_GUARD_END
+}
+
 CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                      const CaelixBrickKey* keys, const float* power)
 {

@@ -121,6 +121,10 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
 // slots[j], j < count (the slots distinct).
 cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, const uint32_t* slots, uint32_t count,
                             uint16_t* stage_voxels, cudaStream_t stream);
+// Compaction of the staging after a removal: for j < count, slot moves[2j] takes the key and the
+// block values of slot moves[2j + 1] (moves: device, no destination also a source).
+cudaError_t staging_move(int32_t* stage_keys, uint16_t* stage_voxels, const uint32_t* moves, uint32_t count,
+                         cudaStream_t stream);
 // The staging slots in increasing linear brick index of `grid`, gathered into the scene's input
 // arrays (power zero when `power` is null). `scratch`: staging_sort_words(n) words.
 uint64_t staging_sort_words(uint32_t n);

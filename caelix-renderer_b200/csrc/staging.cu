@@ -25,6 +25,20 @@ __global__ void __launch_bounds__(kStageThreads)
     stage[64ull * __ldg(slots + j) + w] = __ldg(src + 64ull * __ldg(src_index + j) + w);
 }
 
+// Compaction after a removal: slot moves[2j] takes the key and the block values of slot
+// moves[2j + 1]. No destination is also a source, so the moves run in any order.
+__global__ void __launch_bounds__(kStageThreads)
+    staging_move_kernel(int32_t* __restrict__ keys, uint4* __restrict__ stage, const uint32_t* __restrict__ moves,
+                        uint32_t count)
+{
+    const uint64_t u = (uint64_t)blockIdx.x * kStageThreads + threadIdx.x;
+    if (u >= 64ull * count) return;
+    const uint32_t j = (uint32_t)(u >> 6), w = (uint32_t)(u & 63u);
+    const uint32_t dst = __ldg(moves + 2 * j), src = __ldg(moves + 2 * j + 1);
+    stage[64ull * dst + w] = stage[64ull * src + w];
+    if (w < 3) keys[3ull * dst + w] = keys[3ull * src + w];
+}
+
 __global__ void __launch_bounds__(kStageThreads)
     staging_linear_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t gx, uint32_t gy,
                           uint32_t* __restrict__ lin)
@@ -92,6 +106,15 @@ cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, cons
     if (count == 0) return cudaSuccess;
     staging_scatter_kernel<<<blocks(64ull * count), kStageThreads, 0, stream>>>(
         reinterpret_cast<const uint4*>(src), src_index, slots, count, reinterpret_cast<uint4*>(stage_voxels));
+    return cudaGetLastError();
+}
+
+cudaError_t staging_move(int32_t* stage_keys, uint16_t* stage_voxels, const uint32_t* moves, uint32_t count,
+                         cudaStream_t stream)
+{
+    if (count == 0) return cudaSuccess;
+    staging_move_kernel<<<blocks(64ull * count), kStageThreads, 0, stream>>>(
+        stage_keys, reinterpret_cast<uint4*>(stage_voxels), moves, count);
     return cudaGetLastError();
 }
 

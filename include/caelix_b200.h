@@ -272,6 +272,15 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
                                                    const CaelixBrickKey* keys, const void* blocks,
                                                    uint32_t* consumed);
 
+/* Replaces caelix_scene_remove_bricks (include/caelix/caelix.h:353-356): removes the bricks of the
+   given keys (host memory, borrowed for the call); keys the scene does not have, including keys
+   outside the range an upload accepts, are ignored, and a key repeated in the call is removed
+   once. entity must be 0. The next flush rebuilds the scene's tables from the remaining bricks
+   (their groups, and a group's light block, go with their last brick). A removed brick's power
+   goes with it: a later upload of the same key starts with power 0 unless the host sets it. */
+CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
+                                                   const CaelixBrickKey* keys);
+
 /* New (no reference counterpart): the emitter power of bricks (host arrays). An opaque voxel of a
    brick with power P > 0 emits radiance (P, P, P) and is a light voxel of the light tree (the
    reference derives light voxels from emissive material codes, include/caelix/caelix.h:600-630;

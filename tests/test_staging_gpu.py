@@ -142,3 +142,61 @@ def test_edits_without_new_bricks(cuda_device, oracle):
     gpu, ref, st, rays = render_both(cuda_device, scene, osc, cur, 64, 48, spp=2, bounces=3, seed=9)
     assert_radiance_close(gpu, ref)
     scene.close()
+
+
+def scene_of(keys, voxels, power, vs):
+    """A VoxelScene of the given bricks in increasing linear brick index of the grid their keys
+    span (the grid always holds brick 0, as the scene's)."""
+    grid = tuple(int(g) for g in np.maximum(keys.max(axis=0), 0) + 1) if len(keys) else (1, 1, 1)
+    lin = keys[:, 0] + grid[0] * (keys[:, 1] + grid[1] * keys[:, 2].astype(np.int64))
+    o = np.argsort(lin, kind="stable")
+    return workloads.VoxelScene(grid, keys[o], voxels[o], power[o], vs.albedo, vs.camera, vs.group_shift)
+
+
+def test_remove_bricks(cuda_device, oracle):
+    """caelix_scene_remove_bricks: a quarter of the bricks removed (every brick of the highest x
+    plane among them, so the grid shrinks; emissive bricks; repeated, absent and out-of-range keys
+    that are ignored), then some of them uploaded again (one emissive brick without its power: it
+    comes back dark), then every brick removed. Each flushed state equals the oracle's build of the
+    remaining bricks, and so does the render."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(9, 7, 8), brick_occupancy=0.5, emissive_fraction=0.08, seed=5)
+    rng = np.random.default_rng(5)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    n = vs.brick_count
+    top = np.nonzero(vs.keys[:, 0] == vs.keys[:, 0].max())[0]
+    gone = np.unique(np.concatenate([rng.choice(n, size=n // 4, replace=False), top,
+                                     np.nonzero(vs.power > 0)[0][:3]]))
+    extra = np.array([[vs.grid[0] + 5, 0, 0], [-1, 2, 2], [0, -3, 1]], np.int32)  # absent, out of range
+    scene.remove_bricks(np.concatenate([vs.keys[gone], vs.keys[gone[:10]], extra]))
+    scene.flush()
+    keep = np.setdiff1d(np.arange(n), gone)
+    cur = scene_of(vs.keys[keep], vs.voxels[keep], vs.power[keep], vs)
+    assert cur.grid[0] < vs.grid[0]
+    osc = oracle_lib.OracleScene(oracle, cur)
+    assert_scene_equal(scene, osc, cur)
+    gpu, ref, st, rays = render_both(cuda_device, scene, osc, cur, 64, 48, spp=2, bounces=3, seed=3)
+    assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+    assert_radiance_close(gpu, ref)
+
+    back = gone[rng.random(len(gone)) < 0.5]
+    lit_back = back[vs.power[back] > 0]
+    scene.upload_bricks(vs.keys[back], vs.voxels[back])
+    if len(lit_back) > 1:
+        scene.set_brick_power(vs.keys[lit_back[1:]], vs.power[lit_back[1:]])
+    scene.flush()
+    power = vs.power.copy()
+    if len(lit_back):
+        power[lit_back[0]] = 0.0
+    now = np.union1d(keep, back)
+    cur = scene_of(vs.keys[now], vs.voxels[now], power[now], vs)
+    osc = oracle_lib.OracleScene(oracle, cur)
+    assert_scene_equal(scene, osc, cur)
+    gpu, ref, st, rays = render_both(cuda_device, scene, osc, cur, 64, 48, spp=2, bounces=3, seed=4)
+    assert_radiance_close(gpu, ref)
+
+    scene.remove_bricks(vs.keys)
+    scene.flush()
+    assert scene.view().brick_count == 0
+    scene.close()
