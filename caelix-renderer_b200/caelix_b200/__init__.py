@@ -284,6 +284,10 @@ class LightBvh:
 # Scene and renderer
 
 
+class CaelixEntityDesc(C.Structure):
+    _fields_ = [("guid", C.c_uint8 * 16), ("position", C.c_float * 3), ("rotation", C.c_float * 4)]
+
+
 class CaelixSceneDesc(C.Structure):
     _fields_ = [("group_shift", C.c_uint32), ("encoding", C.c_uint32), ("reserved", C.c_uint32 * 2)]
 
@@ -374,6 +378,10 @@ def _bind_scene(L):
         "caelix_scene_upload_bricks": [vp, C.c_uint32, C.c_uint32, vp, vp, C.POINTER(C.c_uint32)],
         "caelix_scene_set_brick_power": [vp, C.c_uint32, C.c_uint32, vp, vp],
         "caelix_scene_remove_bricks": [vp, C.c_uint32, C.c_uint32, vp],
+        "caelix_scene_add_entity": [vp, C.POINTER(CaelixEntityDesc), C.POINTER(C.c_uint32)],
+        "caelix_scene_remove_entity": [vp, C.c_uint32],
+        "caelix_scene_set_entity_transform": [vp, C.c_uint32, vp, vp],
+        "caelix_scene_set_entity_motion": [vp, C.c_uint32, C.c_uint32],
         "caelix_scene_set_materials": [vp, vp, C.c_uint32],
         "caelix_scene_set_light_options": [vp, C.POINTER(CaelixLightOptions)],
         "caelix_scene_flush": [vp, C.POINTER(CaelixFrameDesc)],
@@ -428,32 +436,57 @@ class Scene:
         except Exception:
             pass
 
-    def upload_bricks(self, keys, voxels):
+    def upload_bricks(self, keys, voxels, entity: int = 0):
         import numpy as np
 
         keys = np.ascontiguousarray(keys, np.int32)
         voxels = np.ascontiguousarray(voxels, np.uint16)
         consumed = C.c_uint32(0)
-        self.L.check(self.L.lib.caelix_scene_upload_bricks(self.handle, 0, len(keys), keys.ctypes.data,
+        self.L.check(self.L.lib.caelix_scene_upload_bricks(self.handle, entity, len(keys), keys.ctypes.data,
                                                            voxels.ctypes.data, C.byref(consumed)),
                      "caelix_scene_upload_bricks")
         return consumed.value
 
-    def remove_bricks(self, keys):
+    def add_entity(self, position, rotation=(0.0, 0.0, 0.0, 1.0), guid=b""):
+        """caelix_scene_add_entity: an entity with no bricks at `position` with the unit quaternion
+        `rotation` (x, y, z, w); returns its id (1, 2, ...)."""
+        d = CaelixEntityDesc()
+        g = bytes(guid)[:16]
+        d.guid[: len(g)] = list(g)
+        d.position[:] = [float(v) for v in position]
+        d.rotation[:] = [float(v) for v in rotation]
+        out = C.c_uint32(0)
+        self.L.check(self.L.lib.caelix_scene_add_entity(self.handle, C.byref(d), C.byref(out)), "caelix_scene_add_entity")
+        return out.value
+
+    def remove_entity(self, entity: int):
+        self.L.check(self.L.lib.caelix_scene_remove_entity(self.handle, entity), "caelix_scene_remove_entity")
+
+    def set_entity_transform(self, entity: int, position, rotation):
+        p = (C.c_float * 3)(*[float(v) for v in position])
+        q = (C.c_float * 4)(*[float(v) for v in rotation])
+        self.L.check(self.L.lib.caelix_scene_set_entity_transform(self.handle, entity, p, q),
+                     "caelix_scene_set_entity_transform")
+
+    def set_entity_motion(self, entity: int, motion: int):
+        self.L.check(self.L.lib.caelix_scene_set_entity_motion(self.handle, entity, motion),
+                     "caelix_scene_set_entity_motion")
+
+    def remove_bricks(self, keys, entity: int = 0):
         """caelix_scene_remove_bricks: keys the scene does not have are ignored; the next flush
         rebuilds the tables from the remaining bricks."""
         import numpy as np
 
         keys = np.ascontiguousarray(keys, np.int32).reshape(-1, 3)
-        self.L.check(self.L.lib.caelix_scene_remove_bricks(self.handle, 0, len(keys), keys.ctypes.data),
+        self.L.check(self.L.lib.caelix_scene_remove_bricks(self.handle, entity, len(keys), keys.ctypes.data),
                      "caelix_scene_remove_bricks")
 
-    def set_brick_power(self, keys, power):
+    def set_brick_power(self, keys, power, entity: int = 0):
         import numpy as np
 
         keys = np.ascontiguousarray(keys, np.int32)
         power = np.ascontiguousarray(power, np.float32)
-        self.L.check(self.L.lib.caelix_scene_set_brick_power(self.handle, 0, len(keys), keys.ctypes.data,
+        self.L.check(self.L.lib.caelix_scene_set_brick_power(self.handle, entity, len(keys), keys.ctypes.data,
                                                              power.ctypes.data), "caelix_scene_set_brick_power")
 
     def set_albedo(self, albedo):

@@ -462,6 +462,10 @@ CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBa
         CaelixResult r = v.renderer ? CAELIX_OK : CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK && v.renderer->device != device) r = CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK) r = render_params(v.renderer, &v.target, &v.camera, &v.options, "caelix_batch_create", &p);
+        if (r == CAELIX_OK && (v.renderer->scene->entity_view_count || !v.renderer->scene->entities.empty())) {
+            log(CAELIX_LOG_ERROR, "caelix_batch_create: view %u: scenes with entities are not batched", i);
+            r = CAELIX_ERROR_UNSUPPORTED;
+        }
         if (r == CAELIX_OK) {
             cudaPointerAttributes attr;
             if (cudaPointerGetAttributes(&attr, reinterpret_cast<const void*>(v.target.radiance)) != cudaSuccess ||
@@ -518,6 +522,11 @@ CAELIX_API CaelixResult caelix_batch_run(CaelixBatch* batch, const CaelixFrameDe
 {
     CAELIX_GUARD_BEGIN
     if (!batch || !frame) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (const CaelixScene* sc : batch->scenes)
+        if (!sc->entities.empty()) {
+            log(CAELIX_LOG_ERROR, "caelix_batch_run: a scene of the batch has entities (not batched)");
+            return CAELIX_ERROR_UNSUPPORTED;
+        }
     cudaSetDevice(batch->device->ordinal);
     cudaError_t e = ensure_graph(batch);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_run");

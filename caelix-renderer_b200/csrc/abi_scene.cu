@@ -32,7 +32,71 @@ uint64_t pack_key(const CaelixBrickKey& k)
     return (uint64_t)(uint32_t)k.x | ((uint64_t)(uint32_t)k.y << 20) | ((uint64_t)(uint32_t)k.z << 40);
 }
 
+// Object-to-world rotation rows of a quaternion (x, y, z, w), normalised, in double, then rounded.
+bool entity_rows(const float q[4], float rot[9])
+{
+    for (int i = 0; i < 4; ++i)
+        if (!std::isfinite(q[i])) return false;
+    const double n = std::sqrt((double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2] + (double)q[3] * q[3]);
+    if (!(n > 0.0) || !std::isfinite(n)) return false;
+    const double x = q[0] / n, y = q[1] / n, z = q[2] / n, w = q[3] / n;
+    const double r[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                         2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                         2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
+    for (int i = 0; i < 9; ++i) rot[i] = (float)r[i];
+    return true;
+}
+
+// The scene holding the bricks of `entity` (0: the scene itself), or null for an unknown id.
+CaelixScene* entity_bricks(CaelixScene* scene, uint32_t entity)
+{
+    if (entity == 0) return scene;
+    if (entity > scene->entities.size()) return nullptr;
+    return scene->entities[entity - 1].bricks;
+}
+
+// Rewrites the device views of the live entities (after waiting for the device: renders may read
+// the old ones) and returns when they are in place. An entity whose bricks were never flushed has
+// no tables yet and joins at the flush that builds them.
+CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
+{
+    std::vector<cx::EntityView> views;
+    for (auto& e : scene->entities) {
+        if (!e.bricks || !e.bricks->built) continue;
+        cx::EntityView v;
+        v.scene = cx::scene_view(e.bricks->dev);
+        std::memcpy(v.rot, e.rot, sizeof(v.rot));
+        std::memcpy(v.pos, e.position, sizeof(v.pos));
+        views.push_back(v);
+        e.generation = e.bricks->generation;
+    }
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    scene->entity_view_count = 0;
+    if (!views.empty()) {
+        CaelixResult r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
+        if (r != CAELIX_OK) return r;
+        e = cudaMemcpyAsync(scene->entity_views.ptr, views.data(), sizeof(cx::EntityView) * views.size(),
+                            cudaMemcpyHostToDevice, stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    }
+    scene->entity_view_count = (uint32_t)views.size();
+    scene->entity_views_dirty = false;
+    return CAELIX_OK;
+}
+
 }  // namespace
+
+cx::SceneView render_view(const CaelixScene* scene)
+{
+    cx::SceneView v = cx::scene_view(scene->dev);
+    if (scene->entity_view_count) {
+        v.entities = static_cast<const cx::EntityView*>(scene->entity_views.ptr);
+        v.entity_count = scene->entity_view_count;
+    }
+    return v;
+}
 
 CaelixResult render_params(const CaelixRenderer* renderer, const CaelixRenderTargets* targets,
                            const CaelixCamera* camera, const CaelixRenderOptions* options, const char* what,
@@ -108,6 +172,9 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
 {
     if (!scene) return;
     cudaSetDevice(scene->device->ordinal);
+    for (auto& e : scene->entities) caelix_scene_destroy(e.bricks);
+    scene->entities.clear();
+    scene->entity_views.release();
     cx::scene_release(scene->dev);
     if (scene->upload_stream) cudaStreamSynchronize(scene->upload_stream);
     if (scene->stage_keys) cudaFree(scene->stage_keys);
@@ -128,7 +195,12 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
 {
     CAELIX_GUARD_BEGIN
     if (consumed) *consumed = 0;
-    if (!scene || entity != 0 || (count && (!keys || !blocks))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!scene || (count && (!keys || !blocks))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (entity != 0) {
+        CaelixScene* bricks = entity_bricks(scene, entity);
+        return bricks ? caelix_scene_upload_bricks(bricks, 0, count, keys, blocks, consumed)
+                      : CAELIX_ERROR_INVALID_ARGUMENT;
+    }
     for (uint32_t i = 0; i < count; ++i) {
         if (!key_ok(keys[i])) {
             log(CAELIX_LOG_ERROR, "caelix_scene_upload_bricks: key (%d, %d, %d) outside [0, %d)", keys[i].x, keys[i].y,
@@ -248,7 +320,11 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
                                                    const CaelixBrickKey* keys)
 {
     CAELIX_GUARD_BEGIN
-    if (!scene || entity != 0 || (count && !keys)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!scene || (count && !keys)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (entity != 0) {
+        CaelixScene* bricks = entity_bricks(scene, entity);
+        return bricks ? caelix_scene_remove_bricks(bricks, 0, count, keys) : CAELIX_ERROR_INVALID_ARGUMENT;
+    }
     if (count == 0) return CAELIX_OK;
     // Room for the compaction's moves (one per removed key), taken before any state changes.
     CaelixResult r = scene->upload.reserve(8ull * count, "caelix_scene_remove_bricks");
@@ -312,11 +388,89 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
     CAELIX_GUARD_END
 }
 
+CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const CaelixEntityDesc* desc, CaelixEntityId* out_id)
+{
+    CAELIX_GUARD_BEGIN
+    if (out_id) *out_id = CAELIX_INVALID_ENTITY;
+    if (!scene || !desc || !out_id) return CAELIX_ERROR_INVALID_ARGUMENT;
+    float rot[9];
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(desc->position[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!entity_rows(desc->rotation, rot)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    CaelixSceneDesc sd{scene->group_shift, 1, {0, 0}};
+    CaelixScene* bricks = nullptr;
+    CaelixResult r = caelix_scene_create(scene->device, &sd, &bricks);
+    if (r != CAELIX_OK) return r;
+    bricks->light_options.enabled = 0;  // entity bricks do not emit
+    bricks->last_frame = scene->last_frame;
+    uint32_t slot = 0;
+    while (slot < scene->entities.size() && scene->entities[slot].bricks) ++slot;
+    if (slot == scene->entities.size()) scene->entities.emplace_back();
+    CaelixScene::Entity& e = scene->entities[slot];
+    e = CaelixScene::Entity();
+    e.bricks = bricks;
+    std::memcpy(e.guid, desc->guid, sizeof(e.guid));
+    std::memcpy(e.position, desc->position, sizeof(e.position));
+    std::memcpy(e.rotation, desc->rotation, sizeof(e.rotation));
+    std::memcpy(e.rot, rot, sizeof(rot));
+    scene->entity_views_dirty = true;
+    *out_id = slot + 1;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_remove_entity(CaelixScene* scene, CaelixEntityId entity)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || entity == 0 || !entity_bricks(scene, entity)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(scene->device->ordinal);
+    // Renders that read its bricks finish first; the device views drop it before its tables go.
+    CaelixScene* bricks = scene->entities[entity - 1].bricks;
+    scene->entities[entity - 1] = CaelixScene::Entity();
+    CaelixResult r = upload_entity_views(scene, scene->upload_stream);
+    caelix_scene_destroy(bricks);
+    return r;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_set_entity_transform(CaelixScene* scene, CaelixEntityId entity,
+                                                          const float position[3], const float rotation[4])
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || entity == 0 || !entity_bricks(scene, entity) || !position || !rotation)
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    float rot[9];
+    for (int k = 0; k < 3; ++k)
+        if (!std::isfinite(position[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!entity_rows(rotation, rot)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    CaelixScene::Entity& e = scene->entities[entity - 1];
+    std::memcpy(e.position, position, sizeof(e.position));
+    std::memcpy(e.rotation, rotation, sizeof(e.rotation));
+    std::memcpy(e.rot, rot, sizeof(rot));
+    scene->entity_views_dirty = true;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_set_entity_motion(CaelixScene* scene, CaelixEntityId entity, uint32_t motion)
+{
+    if (!scene || entity == 0 || !entity_bricks(scene, entity) ||
+        (motion != CAELIX_ENTITY_STATIC && motion != CAELIX_ENTITY_DYNAMIC))
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    scene->entities[entity - 1].motion = motion;
+    return CAELIX_OK;
+}
+
 CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                      const CaelixBrickKey* keys, const float* power)
 {
     CAELIX_GUARD_BEGIN
-    if (!scene || entity != 0 || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (!scene || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
+    if (entity != 0) {
+        if (!entity_bricks(scene, entity)) return CAELIX_ERROR_INVALID_ARGUMENT;
+        log(CAELIX_LOG_ERROR, "caelix_scene_set_brick_power: entity %u: entity bricks do not emit", entity);
+        return CAELIX_ERROR_UNSUPPORTED;
+    }
     for (uint32_t i = 0; i < count; ++i)
         if (!key_ok(keys[i]) || !std::isfinite(power[i]) || power[i] < 0.0f) return CAELIX_ERROR_INVALID_ARGUMENT;
     for (uint32_t i = 0; i < count; ++i) {
@@ -376,6 +530,19 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         return CAELIX_ERROR_INVALID_ARGUMENT;
     }
     scene->last_frame = desc->frame_number;
+    // The entities' bricks (their own flushes), then their device views when any moved, changed,
+    // came or went.
+    for (auto& ent : scene->entities) {
+        if (!ent.bricks) continue;
+        CaelixResult r = caelix_scene_flush(ent.bricks, desc);
+        if (r != CAELIX_OK) return r;
+        if (ent.bricks->generation != ent.generation) scene->entity_views_dirty = true;
+    }
+    if (scene->entity_views_dirty) {
+        cudaSetDevice(scene->device->ordinal);
+        CaelixResult r = upload_entity_views(scene, reinterpret_cast<cudaStream_t>(desc->command_buffer));
+        if (r != CAELIX_OK) return r;
+    }
     if (!scene->built) scene->full_rebuild = true;
     const bool edits = !scene->dirty_slots.empty();
     if (!scene->full_rebuild && !edits && !scene->light_tree_dirty && !scene->albedo_dirty) return CAELIX_OK;
@@ -620,7 +787,7 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_render");
     if (renderer->trace_mode == CAELIX_TRACE_MEGAKERNEL) {
         cudaEventRecord(renderer->start, stream);
-        e = cx::trace_launch(cx::scene_view(scene->dev), p, reinterpret_cast<float*>(targets->radiance),
+        e = cx::trace_launch(render_view(scene), p, reinterpret_cast<float*>(targets->radiance),
                              renderer->counts, stream);
         cudaEventRecord(renderer->stop, stream);
         renderer->launches = 1;
@@ -629,7 +796,7 @@ CAELIX_API CaelixResult caelix_renderer_render(CaelixRenderer* renderer, const C
         // (or the set capacity), the view and its wave table uploaded ahead of the kernels.
         cx::WaveView view;
         std::memset(&view, 0, sizeof(view));
-        view.scene = cx::scene_view(scene->dev);
+        view.scene = render_view(scene);
         view.params = p;
         view.radiance = reinterpret_cast<float*>(targets->radiance);
         view.ray_counts = renderer->counts;
@@ -680,6 +847,10 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     const CaelixResult r = render_params(renderer, &t, camera, options, "caelix_renderer_backward", &p);
     if (r != CAELIX_OK) return r;
     CaelixScene* scene = renderer->scene;
+    if (scene->entity_view_count) {
+        log(CAELIX_LOG_ERROR, "caelix_renderer_backward: scenes with entities are not differentiated");
+        return CAELIX_ERROR_UNSUPPORTED;
+    }
     cudaSetDevice(renderer->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
     cudaError_t e = cudaMemsetAsync(d_albedo, 0, sizeof(float) * cx::kMaterialSlots * 3, stream);

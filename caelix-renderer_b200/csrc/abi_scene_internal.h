@@ -53,6 +53,23 @@ struct CaelixScene
     cudaEvent_t start = nullptr;
     cudaEvent_t stop = nullptr;
     float flush_ms = 0.0f;
+    // Entities 1, 2, ... (entities[id - 1]; `bricks` null: a free id). Each holds its bricks in a
+    // scene of its own (no lights); the device keeps one EntityView per live entity, in id order
+    // (the index a hit reports), rewritten by the flush after a change and by a removal.
+    struct Entity
+    {
+        CaelixScene* bricks = nullptr;
+        uint8_t guid[16] = {};
+        float position[3] = {0.0f, 0.0f, 0.0f};
+        float rotation[4] = {0.0f, 0.0f, 0.0f, 1.0f};
+        float rot[9] = {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f};
+        uint32_t motion = CAELIX_ENTITY_STATIC;
+        uint64_t generation = ~0ull;  // the generation of `bricks` the device view was made from
+    };
+    std::vector<Entity> entities;
+    cx::GrowBuffer entity_views;  // device EntityView per live entity
+    uint32_t entity_view_count = 0;
+    bool entity_views_dirty = false;
 };
 
 struct CaelixRenderer
@@ -73,6 +90,9 @@ struct CaelixRenderer
     uint32_t launches = 0;          // kernels of the newest render
 };
 
+
+// The scene as the trace kernels see it: the world's tables and the entities' device views.
+cx::SceneView render_view(const CaelixScene* scene);
 
 // The trace parameters of a render call (caelix_renderer_render's checks): INVALID_ARGUMENT for a
 // bad target, camera or options, or a scene that was never flushed.

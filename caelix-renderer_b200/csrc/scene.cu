@@ -793,6 +793,8 @@ SceneView scene_view(const DeviceScene& s)
     v.header = s.tree.header;
     v.light_count = s.light_count;
     v.group_count = s.group_count;
+    v.entities = nullptr;
+    v.entity_count = 0;
     return v;
 }
 

@@ -20,6 +20,8 @@ namespace cx {
 constexpr uint32_t kOpaqueBit = 0x8000u;  // block-ID encoding
 constexpr uint32_t kMaterialSlots = 128;  // albedo table rows (material id = value & 0x7F)
 
+struct EntityView;
+
 // Everything the trace kernels read, passed by value.
 struct SceneView
 {
@@ -42,7 +44,27 @@ struct SceneView
     const LightTreeHeader* header;
     uint32_t light_count;
     uint32_t group_count;
+    // Entities beside the scene's own bricks (the static world): each traversed in its frame
+    // after the world. Their bricks do not emit and hold no light records.
+    const EntityView* entities;  // device, entity_count of them
+    uint32_t entity_count;
 };
+
+// An entity on the device: its bricks' tables (a scene of their own, entity-local block
+// coordinates from 0; no lights, no entities) and its object-to-world transform,
+// world = rot * local + pos (rot row-major). Replaces, for the trace, the reference's TLAS
+// instance of an entity's groups (shaders/render/caelix_scene_trace.hlsl:104-131: the object ray
+// of an instance, the committed object-to-world normal).
+struct EntityView
+{
+    SceneView scene;
+    float rot[9];
+    float pos[3];
+};
+
+// The attribute bit of an entity hit (bits 0..5 face flags, 6..14 cell, 16..31 block: bit 15 is
+// free); the hit's group is then the entity's index and its normal the rotated face normal.
+constexpr uint32_t kEntityHit = 0x8000u;
 
 // Host-side owner of the device scene.
 struct DeviceScene

@@ -17,7 +17,7 @@ __device__ __noinline__ void next_event(const SceneView& s, const float x[3], co
     ShadowRay r;
     if (!nee_prepare(s, x, n, light_rng, r)) return;
     ++rays.shadow;
-    const Hit h = trace_ray(s, x, r.dir, 0.0f, r.t_max);
+    const Hit h = trace_scene(s, x, r.dir, 0.0f, r.t_max);
     if (!h.hit) out[0] = out[1] = out[2] = r.value;
 }
 
@@ -38,7 +38,7 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
 #pragma unroll
     for (int k = 0; k < 3; ++k) d[k] = d[k] * inv_len;
     ++rays.primary;
-    const Hit primary = trace_ray(s, P.position, d, 0.0f, kRayTMax);
+    const Hit primary = trace_scene(s, P.position, d, 0.0f, kRayTMax);
     if (!primary.hit) return;
     uint32_t rng = init_random(px, py, seed);
     uint32_t light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
@@ -59,7 +59,7 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
     uint32_t bounce_index = 1;
     while (bounce_index <= P.bounce_count) {
         ++rays.bounce;
-        const Hit h = trace_ray(s, org, dir, 0.0f, kBounceTMax);
+        const Hit h = trace_scene(s, org, dir, 0.0f, kBounceTMax);
         if (!h.hit) break;
         float al[3], em, o2[3], d2[3];
         shade(s, h, org, dir, rng, al, em, o2, d2);

@@ -313,6 +313,70 @@ __device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], cons
     return trace_ray_body(s, o, d, tmin_ray, tmax_ray);
 }
 
+// The entities after the world's bricks, in order: the ray in each entity's frame
+// (local = rot^T (x - pos)), its bricks' DDA up to the current hit, a strictly nearer hit taken with
+// the entity bit, the entity's index as its group and the rotated face normal (normalised as
+// v * (1 / sqrt(dot(v, v)))).
+__device__ __noinline__ void trace_entities(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
+                                            float tmax_ray, Hit& h)
+{
+    for (uint32_t e = 0; e < s.entity_count; ++e) {
+        const EntityView& E = s.entities[e];
+        float R[9], ol[3], dl[3];
+#pragma unroll
+        for (int i = 0; i < 9; ++i) R[i] = __ldg(&E.rot[i]);
+        const float q[3] = {o[0] - __ldg(&E.pos[0]), o[1] - __ldg(&E.pos[1]), o[2] - __ldg(&E.pos[2])};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            ol[k] = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
+            dl[k] = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
+        }
+        const Hit he = trace_ray_body(E.scene, ol, dl, tmin_ray, h.hit ? h.t : tmax_ray);
+        if (!he.hit) continue;
+        h = he;
+        h.attrib |= kEntityHit;
+        h.group = e;
+        const uint32_t f = (uint32_t)(__ffs(he.attrib & 0x3Fu) - 1);
+        const float sign = (f & 1u) ? -1.0f : 1.0f;
+        float v[3];
+#pragma unroll
+        for (int i = 0; i < 3; ++i) v[i] = R[3 * i + (f >> 1)] * sign;
+        const float inv = 1.0f / sqrtf(dot3(v, v));
+#pragma unroll
+        for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
+    }
+}
+
+// The world normal of an entity hit from its face flags (the wavefront keeps a hit as four words).
+__device__ __forceinline__ void entity_normal(const SceneView& s, uint32_t entity, uint32_t attrib, float n[3])
+{
+    const EntityView& E = s.entities[entity];
+    const uint32_t f = (uint32_t)(__ffs(attrib & 0x3Fu) - 1);
+    const float sign = (f & 1u) ? -1.0f : 1.0f;
+    float v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = __ldg(&E.rot[3 * i + (f >> 1)]) * sign;
+    const float inv = 1.0f / sqrtf(dot3(v, v));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) n[i] = v[i] * inv;
+}
+
+// Closest hit over the world's bricks and the entities'.
+__device__ __forceinline__ Hit trace_scene_body(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
+                                                float tmax_ray)
+{
+    Hit h = trace_ray_body(s, o, d, tmin_ray, tmax_ray);
+    if (s.entity_count) trace_entities(s, o, d, tmin_ray, tmax_ray, h);
+    return h;
+}
+
+__device__ __noinline__ Hit trace_scene(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+{
+    Hit h = trace_ray(s, o, d, tmin_ray, tmax_ray);
+    if (s.entity_count) trace_entities(s, o, d, tmin_ray, tmax_ray, h);
+    return h;
+}
+
 // ---- light tree ----
 __device__ __forceinline__ float power6(const float f[6]) { return f[0] + f[1] + f[2] + f[3] + f[4] + f[5]; }
 
@@ -846,7 +910,7 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
 __device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segment_light, const Hit& h, const float origin[3],
                                  const float dir[3], const float seg_n[3])
 {
-    if (segment_light == 0u || h.t < kNearField) return 1.0f;
+    if (segment_light == 0u || h.t < kNearField || (h.attrib & kEntityHit)) return 1.0f;
     const GroupFrame* fr = s.frames + h.group;
     uint32_t vig[3];
 #pragma unroll
@@ -868,7 +932,7 @@ __device__ __forceinline__ void shade(const SceneView& s, const Hit& h, const fl
                                       uint32_t& rng, float albedo[3], float& emission, float origin[3], float dir[3])
 {
     const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-    emission = (block & kOpaqueBit) ? __ldg(s.power + h.record) : 0.0f;
+    emission = ((block & kOpaqueBit) && !(h.attrib & kEntityHit)) ? __ldg(s.power + h.record) : 0.0f;  // entities do not emit
     const float* a = s.albedo + 3 * (block & (kMaterialSlots - 1));
     albedo[0] = __ldg(a);
     albedo[1] = __ldg(a + 1);

@@ -110,6 +110,9 @@ __global__ void __launch_bounds__(kWaveThreads)
     }
 }
 
+// kEntities: the views' scenes have entities (traversed after the world's bricks); the variant
+// without them keeps the world-only DDA's registers (no out-of-line call).
+template <bool kEntities>
 __global__ void __launch_bounds__(kWaveThreads)
     wave_trace_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
 {
@@ -132,7 +135,9 @@ __global__ void __launch_bounds__(kWaveThreads)
             const float o[3] = {o4.x, o4.y, o4.z};
             const float d[3] = {d4.x, d4.y, d4.z};
             const float t_max = kind == kKindShadow ? d4.w : (kind == kKindPrimary ? kRayTMax : kBounceTMax);
-            const Hit h = trace_ray_body(views[v].scene, o, d, 0.0f, t_max);
+            Hit h;
+            if constexpr (kEntities) h = trace_scene_body(views[v].scene, o, d, 0.0f, t_max);
+            else h = trace_ray_body(views[v].scene, o, d, 0.0f, t_max);
             if (kind == kKindShadow) b.occluded[slot] = h.hit ? 1u : 0u;
             else b.hit[slot] = h.hit ? make_uint4(__float_as_uint(h.t), h.attrib, h.record, h.group) : make_uint4(0, 0, 0, 0);
             key = v * 4u + kind;
@@ -247,6 +252,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                     h.normal[0] = fc == 0 ? 1.0f : (fc == 1 ? -1.0f : 0.0f);
                     h.normal[1] = fc == 2 ? 1.0f : (fc == 3 ? -1.0f : 0.0f);
                     h.normal[2] = fc == 4 ? 1.0f : (fc == 5 ? -1.0f : 0.0f);
+                    if (h.attrib & kEntityHit) entity_normal(S, h.group, h.attrib, h.normal);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) h.object_hit[k] = org[k] + dir[k] * h.t;
                     const uint32_t px = item % P.width, py = item / P.width;
@@ -297,7 +303,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                                 G[k] = (!bad && R[k] <= 65504.0f) ? g[k] * a0[k] : 0.0f;
                                 any |= G[k] != 0.0f;
                             }
-                            if (block0 & kOpaqueBit) atomicAdd(adj.d_power + h.record, g[0] + g[1] + g[2]);
+                            if ((block0 & kOpaqueBit) && !(h.attrib & kEntityHit)) atomicAdd(adj.d_power + h.record, g[0] + g[1] + g[2]);
                             if (!any) nee_now = false, bounce_index = P.bounce_count + 1u;  // nothing flows back
                         }
                     } else {
@@ -317,7 +323,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                         for (int k = 0; k < 3; ++k) rad[k] += em * (tp[k] * ew);
                         if (kMode == kShadeReplay) {
                             const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-                            if (block & kOpaqueBit) atomicAdd(adj.d_power + h.record, gsum3(G, tp, ew));
+                            if ((block & kOpaqueBit) && !(h.attrib & kEntityHit)) atomicAdd(adj.d_power + h.record, gsum3(G, tp, ew));
                             // Everything gathered from here on carries this vertex's albedo.
                             float* ga = s_albedo + 3 * (block & (kMaterialSlots - 1));
 #pragma unroll
@@ -510,15 +516,17 @@ namespace {
 template <int kMode, int kMinBlocks>
 cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b,
                      uint32_t block_width, uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream,
-                     uint32_t* launches)
+                     uint32_t* launches, bool entities = false)
 {
     if (b.capacity == 0) return cudaErrorInvalidValue;
-    static int trace_blocks = 0, shade_blocks = 0;
-    if (trace_blocks == 0) {
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks, wave_trace_kernel, kWaveThreads, 0));
+    static int trace_blocks[2] = {0, 0}, shade_blocks = 0;
+    if (trace_blocks[0] == 0) {
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[0], wave_trace_kernel<false>, kWaveThreads, 0));
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[1], wave_trace_kernel<true>, kWaveThreads, 0));
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel<kMode, kMinBlocks>,
                                                              kWaveThreads, 0));
-        trace_blocks = std::max(trace_blocks, 1);
+        trace_blocks[0] = std::max(trace_blocks[0], 1);
+        trace_blocks[1] = std::max(trace_blocks[1], 1);
         shade_blocks = std::max(shade_blocks, 1);
     }
     uint32_t count = 0;
@@ -536,12 +544,13 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
             wave_generate_kernel<<<(n + kWaveThreads - 1) / kWaveThreads, kWaveThreads, 0, stream>>>(d_views, g, b);
             ++count;
             const uint32_t ray_grid = std::min<uint32_t>((2 * n + kWaveThreads - 1) / kWaveThreads,
-                                                         sm_count * (uint32_t)trace_blocks);
+                                                         sm_count * (uint32_t)trace_blocks[entities ? 1 : 0]);
             const uint32_t shade_grid = std::min<uint32_t>((n + kWaveThreads - 1) / kWaveThreads,
                                                            sm_count * (uint32_t)shade_blocks);
             for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
                 const uint32_t parity = it & 1u;
-                wave_trace_kernel<<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                if (entities) wave_trace_kernel<true><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                else wave_trace_kernel<false><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
                 wave_shade_kernel<kMode, kMinBlocks><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
                 count += 2;
             }
@@ -561,9 +570,13 @@ cudaError_t wave_trace(const WaveView* views, const WaveView* d_views, uint32_t 
                        cudaStream_t stream, uint32_t* launches)
 {
     const WaveAdjoint none{nullptr, nullptr, nullptr, nullptr};
+    bool entities = false;
+    for (uint32_t v = 0; v < view_count; ++v) entities |= views[v].scene.entity_count != 0;
     if (view_count == 1 && wave_resident_scene(views[0].scene))
-        return wave_run<kShadeRender, 5>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
-    return wave_run<kShadeRender, 8>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches);
+        return wave_run<kShadeRender, 5>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches,
+                                         entities);
+    return wave_run<kShadeRender, 8>(d_views, plan, d_table, b, block_width, sm_count, none, stream, launches,
+                                     entities);
 }
 
 cudaError_t wave_adjoint(const SceneView& scene, const WaveView* d_record, const WaveView* d_replay,

@@ -239,10 +239,12 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs_static(uint32_t* keys, uint32_t*
  * Bricks are 8x8x8 blocks of 16-bit values, block-ID encoding (opaque = bit 15 set; a value
  * without bit 15 is transparent, id = value & 0x1FF, id 0 = air), voxel index x + 8y + 64z, as in
  * the reference (include/caelix/caelix.h:240-290). A brick key is the brick coordinate; this
- * version takes keys in [0, 1024) per axis (the world grid is the bounding box of the keys) and
- * one entity with the identity transform. caelix_scene_flush builds, on the device: the brick
- * records (the finalize rules of the reference), the brick hash table, the brick occupancy bitmap,
- * the brick light records and the light tree.
+ * version takes keys in [0, 1024) per axis (the world grid is the bounding box of the keys).
+ * Entity 0 is the scene's static world with the identity transform; caelix_scene_add_entity adds
+ * entities 1, 2, ... with their own bricks (entity-local keys, the same range) under a rigid
+ * transform. caelix_scene_flush builds, on the device: the brick records (the finalize rules of
+ * the reference), the brick hash table, the brick occupancy bitmap, the brick light records and
+ * the light tree of the world, and the same tables (without lights) of every entity.
  * ------------------------------------------------------------------------- */
 
 typedef struct CaelixScene CaelixScene;
@@ -259,6 +261,39 @@ CAELIX_API CaelixResult caelix_scene_create(CaelixDevice* device, const CaelixSc
                                             CaelixScene** out_scene);
 CAELIX_API void caelix_scene_destroy(CaelixScene* scene);
 
+/* Replaces the reference's entities (include/caelix/caelix.h:302-332). Entity ids are small
+   indices; the id of a removed entity is reused by a later add. Entity 0 is the world: it is
+   neither added, moved nor removed. */
+typedef uint32_t CaelixEntityId;
+#define CAELIX_INVALID_ENTITY 0xFFFFFFFFu
+
+typedef struct CaelixEntityDesc
+{
+    uint8_t guid[16];  /* stored for the host; the library does not interpret it */
+    float position[3]; /* world position of the entity origin */
+    float rotation[4]; /* unit quaternion x, y, z, w (normalised by the library) */
+} CaelixEntityDesc;
+
+/* Adds an entity with no bricks: world = R(rotation) * local + position, local = the
+   entity-local block coordinate. Its bricks are traced (closest hit over the world and every
+   entity, ties to the world and then to the lower id) and shaded with the scene's materials; they
+   do not emit and hold no light records (the light tree stays the world's: the reference's second,
+   dynamic light tree is not built). Takes effect at the next flush. */
+CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const CaelixEntityDesc* desc,
+                                                CaelixEntityId* out_id);
+/* Removes the entity and all its bricks at once (waiting for the device first). */
+CAELIX_API CaelixResult caelix_scene_remove_entity(CaelixScene* scene, CaelixEntityId entity);
+/* Moves an entity; takes effect at the next flush. The rotation rows are computed in double from
+   the normalised quaternion and rounded to float. */
+CAELIX_API CaelixResult caelix_scene_set_entity_transform(CaelixScene* scene, CaelixEntityId entity,
+                                                          const float position[3], const float rotation[4]);
+/* Entity motion (the reference uses it only to pick the light tree of an entity's lights; entity
+   lights are not built here, so the value is stored and has no effect). Other values than
+   CAELIX_ENTITY_STATIC / CAELIX_ENTITY_DYNAMIC return CAELIX_ERROR_INVALID_ARGUMENT. */
+#define CAELIX_ENTITY_STATIC 0u
+#define CAELIX_ENTITY_DYNAMIC 1u
+CAELIX_API CaelixResult caelix_scene_set_entity_motion(CaelixScene* scene, CaelixEntityId entity, uint32_t motion);
+
 typedef struct CaelixBrickKey
 {
     int32_t x, y, z;
@@ -266,7 +301,7 @@ typedef struct CaelixBrickKey
 
 /* Replaces caelix_scene_upload_bricks (include/caelix/caelix.h:340-352): count raw bricks of 512
    uint16_t values each (host memory, borrowed for the call); a brick with the same key is
-   replaced. entity must be 0. Every key is checked first: one out of range returns
+   replaced. entity: 0 (the world) or an added entity. Every key is checked first: one out of range returns
    CAELIX_ERROR_INVALID_ARGUMENT and accepts nothing. *consumed (may be NULL) = count. */
 CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                    const CaelixBrickKey* keys, const void* blocks,
@@ -275,7 +310,7 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
 /* Replaces caelix_scene_remove_bricks (include/caelix/caelix.h:353-356): removes the bricks of the
    given keys (host memory, borrowed for the call); keys the scene does not have, including keys
    outside the range an upload accepts, are ignored, and a key repeated in the call is removed
-   once. entity must be 0. The next flush rebuilds the scene's tables from the remaining bricks
+   once. entity: 0 (the world) or an added entity. The next flush rebuilds that entity's tables from the remaining bricks
    (their groups, and a group's light block, go with their last brick). A removed brick's power
    goes with it: a later upload of the same key starts with power 0 unless the host sets it. */
 CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
@@ -285,7 +320,8 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
    brick with power P > 0 emits radiance (P, P, P) and is a light voxel of the light tree (the
    reference derives light voxels from emissive material codes, include/caelix/caelix.h:600-630;
    the benchmark scenes give each emissive brick its own power). Keys without an uploaded brick are
-   kept and apply when it arrives. */
+   kept and apply when it arrives. entity 0 only: an added entity's bricks do not emit
+   (CAELIX_ERROR_UNSUPPORTED). */
 CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                      const CaelixBrickKey* keys, const float* power);
 

@@ -131,6 +131,8 @@ typedef struct oc_scene_desc {
     const float* power;
 } oc_scene_desc;
 
+struct oc_entity;
+
 typedef struct oc_scene {
     uint32_t grid[3];
     uint32_t group_shift;
@@ -154,7 +156,28 @@ typedef struct oc_scene {
     uint32_t* heap;        /* group light blocks (16-byte units) */
     uint32_t* group_rows;  /* [group_count][8] GroupLightRow */
     oc_frame* group_frames;
+    /* Entities beside this scene's bricks (the static world, entity 0): rays also traverse each
+     * entity's own scene under its transform. Entity bricks do not emit and hold no light records. */
+    const struct oc_entity* entities;
+    uint32_t entity_count;
+    uint32_t pad2;
 } oc_scene;
+
+/* An entity: its bricks (a scene of their own, entity-local block coordinates from 0, built with
+ * every power 0) and its object-to-world transform, world = rot * local + pos (rot row-major). */
+typedef struct oc_entity {
+    const oc_scene* scene;
+    float rot[9];
+    float pos[3];
+} oc_entity;
+
+/* An entity hit (oc_hit.attrib bit 15; the hit's group is then the entity index and its normal
+ * the rotated face normal; cell is bits 6..14, the block bits 16..31, so bit 15 is free). */
+#define OC_ENTITY_HIT 0x8000u
+
+/* Rotation rows of a quaternion (x, y, z, w; normalised first), computed in double and rounded:
+ * the same arithmetic as the library's caelix_scene_set_entity_transform. */
+void oc_entity_rows(const float q[4], float rot[9]);
 
 int oc_scene_build(const oc_scene_desc* d, oc_scene* s);
 void oc_scene_free(oc_scene* s);
@@ -200,7 +223,9 @@ typedef struct oc_hit {
     float object_hit[3];
 } oc_hit;
 
-/* Closest hit of a ray (unit direction) over the bricks, t in [tmin, tmax). */
+/* Closest hit of a ray (unit direction) over the bricks, t in [tmin, tmax): the scene's own
+ * bricks, then every entity in order (a ray in the entity's frame, local = rot^T (x - pos); an
+ * entity hit replaces the current one only when strictly nearer). */
 oc_hit oc_trace_ray(const oc_scene* s, const float origin[3], const float dir[3], float tmin, float tmax);
 
 /* Renders the pixel window; radiance[3 * (y * width + x)] (fp32 RGB, averaged over spp);

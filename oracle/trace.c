@@ -218,7 +218,7 @@ static float brick_primitive(const uint32_t* rec, const float o[3], const float 
 
 /* ---- scene traversal: front-to-back DDA over the brick grid ---- */
 
-oc_hit oc_trace_ray(const oc_scene* s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
 {
     oc_hit h;
     memset(&h, 0, sizeof(h));
@@ -278,6 +278,43 @@ oc_hit oc_trace_ray(const oc_scene* s, const float o[3], const float d[3], float
         if (tn[axis] > t_exit) break;
         cell[axis] += step[axis];
         if (cell[axis] < 0 || cell[axis] >= (int)s->grid[axis]) break;
+    }
+    return h;
+}
+
+void oc_entity_rows(const float q[4], float rot[9])
+{
+    const double n = sqrt((double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2] + (double)q[3] * q[3]);
+    const double x = q[0] / n, y = q[1] / n, z = q[2] / n, w = q[3] / n;
+    const double r[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                         2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                         2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
+    for (int i = 0; i < 9; ++i) rot[i] = (float)r[i];
+}
+
+oc_hit oc_trace_ray(const oc_scene* s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+{
+    oc_hit h = trace_grid(s, o, d, tmin_ray, tmax_ray);
+    for (uint32_t e = 0; e < s->entity_count; ++e) {
+        const oc_entity* E = &s->entities[e];
+        const float* R = E->rot;
+        const float q[3] = {o[0] - E->pos[0], o[1] - E->pos[1], o[2] - E->pos[2]};
+        float ol[3], dl[3];
+        for (int k = 0; k < 3; ++k) {
+            ol[k] = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
+            dl[k] = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
+        }
+        const oc_hit he = trace_grid(E->scene, ol, dl, tmin_ray, h.hit ? h.t : tmax_ray);
+        if (!he.hit) continue;
+        h = he;
+        h.attrib |= OC_ENTITY_HIT;
+        h.group = e;
+        const uint32_t f = (uint32_t)__builtin_ctz(he.attrib & 0x3Fu);
+        const float sign = (f & 1u) ? -1.0f : 1.0f;
+        float v[3];
+        for (int i = 0; i < 3; ++i) v[i] = R[3 * i + (f >> 1)] * sign;
+        const float inv = 1.0f / sqrtf(dot3(v, v));
+        for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
     }
     return h;
 }
@@ -806,7 +843,7 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
 static float lamp_hit_weight(ctx* c, uint32_t segment_light, const oc_hit* h, const float origin[3], const float dir[3],
                              const float seg_n[3])
 {
-    if (segment_light == 0u || h->t < NEAR_FIELD) return 1.0f;
+    if (segment_light == 0u || h->t < NEAR_FIELD || (h->attrib & OC_ENTITY_HIT)) return 1.0f;
     int32_t voxel[3];
     for (int k = 0; k < 3; ++k) voxel[k] = (int32_t)floorf(h->object_hit[k] - 0.25f * h->normal[k]);
     const oc_frame* fr = &c->s->group_frames[h->group];
@@ -827,7 +864,7 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
                   float albedo[3], float emission[3], float origin[3], float dir[3])
 {
     const uint32_t block = (h->attrib >> 16) & 0xFFFFu;
-    emission_of(c, h->record, block, emission);
+    emission_of(c, h->record, (h->attrib & OC_ENTITY_HIT) ? 0u : block, emission); /* entities do not emit */
     const float* a = c->albedo + 3 * (block & 0x7Fu); /* the material id of the 128-row table */
     albedo[0] = a[0];
     albedo[1] = a[1];
@@ -906,7 +943,7 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     if (rec) {
         const uint32_t block0 = (primary.attrib >> 16) & 0xFFFFu;
         rec->hit = 1;
-        rec->emits0 = (block0 & OPAQUE) != 0;
+        rec->emits0 = (block0 & OPAQUE) != 0 && !(primary.attrib & OC_ENTITY_HIT);
         rec->material0 = block0 & 0x7Fu;
         rec->record0 = primary.record;
     }
@@ -936,7 +973,7 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
             ew = lamp_hit_weight(c, segment_light, &h, org, dir, seg_n);
         for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
         const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-        if (block & OPAQUE) rec_event(rec, EV_EMIT, h.record, ew);
+        if ((block & OPAQUE) && !(h.attrib & OC_ENTITY_HIT)) rec_event(rec, EV_EMIT, h.record, ew);
         rec_event(rec, EV_ALBEDO, block & 0x7Fu, 0.0f);
         for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
         segment_light = 0u;

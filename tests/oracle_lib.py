@@ -94,7 +94,12 @@ class Scene(C.Structure):
         "hash_max_probe", "bitmap_words", "light_count", "heap_words", "group_count", "groups0", "groups1",
         "groups2", "pad")] + [(n, C.c_void_p) for n in (
         "records", "hash_slots", "bitmap", "light_headers", "light_group", "light_entry", "light_brick",
-        "heap", "group_rows", "group_frames")]
+        "heap", "group_rows", "group_frames")] + [("entities", C.c_void_p), ("entity_count", C.c_uint32),
+                                                   ("pad2", C.c_uint32)]
+
+
+class Entity(C.Structure):
+    _fields_ = [("scene", C.c_void_p), ("rot", C.c_float * 9), ("pos", C.c_float * 3)]
 
 
 class Camera(C.Structure):
@@ -145,6 +150,8 @@ def _bind_scene(lib):
     lib.oc_light_draws.restype = None
     lib.oc_mis_weight.argtypes = [C.c_float, C.c_void_p, C.c_void_p, C.c_float, C.c_float, C.c_int]
     lib.oc_mis_weight.restype = C.c_float
+    lib.oc_entity_rows.argtypes = [C.c_void_p, C.c_void_p]
+    lib.oc_entity_rows.restype = None
     lib.oc_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
     lib.oc_sincos.restype = None
     lib._scene_bound = True
@@ -190,8 +197,26 @@ class OracleScene:
         self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
                             self.tree["header"].ctypes.data)
 
+    def set_entities(self, entities):
+        """Entities beside the scene's bricks: (OracleScene of the entity's bricks, quaternion x y z w,
+        position) each, traversed in order; rotation rows as the library computes them."""
+        self._entity_scenes = [e[0] for e in entities]
+        arr = (Entity * max(len(entities), 1))()
+        for i, (osc, q, pos) in enumerate(entities):
+            qf = np.ascontiguousarray(q, np.float32)
+            rot = np.zeros(9, np.float32)
+            self.lib.oc_entity_rows(qf.ctypes.data, rot.ctypes.data)
+            arr[i].scene = C.cast(C.pointer(osc.s), C.c_void_p)
+            arr[i].rot[:] = [float(v) for v in rot]
+            arr[i].pos[:] = [float(v) for v in np.asarray(pos, np.float32)]
+        self._entities = arr
+        self.s.entities = C.cast(arr, C.c_void_p) if entities else None
+        self.s.entity_count = len(entities)
+
     def close(self):
         if self.s.records:
+            self.s.entities = None
+            self.s.entity_count = 0
             self.lib.oc_scene_free(C.byref(self.s))
 
     def __del__(self):

@@ -1,0 +1,106 @@
+"""Entities through the C ABI against the oracle: a world with two entities (one rotated, one
+translated), rendered with the wavefront and the per-frame kernels; then an entity moved, an
+entity's bricks edited, an entity removed and a new one added in its id. Every state's radiance and
+ray counts equal the oracle's with the same entities (bit-exact expected; the 1e-5 relative bound
+of the trace parity tests)."""
+import numpy as np
+import pytest
+
+import oracle_lib
+from caelix_b200 import workloads
+from test_entities_oracle import entity_bricks
+from test_trace_gpu import assert_radiance_close
+
+pytestmark = pytest.mark.gpu
+
+Q1 = (0.12, -0.31, 0.2, 0.92)
+Q1_MOVED = (-0.4, 0.1, 0.3, 0.86)
+IDENTITY = (0.0, 0.0, 0.0, 1.0)
+
+
+def render_pair(cuda_device, scene, osc, vs, mode=None, spp=2):
+    import torch
+
+    import caelix_b200
+
+    r = caelix_b200.Renderer(cuda_device, scene)
+    if mode is not None:
+        r.set_trace_mode(mode, 0)
+    out = torch.zeros(56 * 72 * 3, dtype=torch.float32, device="cuda")
+    r.render(out, 72, 56, vs.camera, bounces=4, seed=5, spp=spp)
+    st = r.stats()
+    gpu = out.cpu().numpy().reshape(56, 72, 3)
+    ref, rays = osc.render(72, 56, spp=spp, bounces=4, seed=5, threads=8)
+    r.close()
+    assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+    assert_radiance_close(gpu, ref)
+    return gpu
+
+
+def test_entities_parity(cuda_device, oracle):
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(8, 6, 10), brick_occupancy=0.45, emissive_fraction=0.08, seed=3)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    cam = vs.camera
+    ahead = np.asarray(cam["position"], np.float64) + 14.0 * np.asarray(cam["forward"], np.float64)
+    p1 = tuple((ahead - 8.0).astype(np.float32))
+    p2 = tuple((ahead + np.array([10.0, -6.0, 12.0])).astype(np.float32))
+    b1 = entity_bricks(grid=(2, 2, 2), seed=7)
+    b2 = entity_bricks(grid=(1, 2, 1), seed=8, fill=0.8)
+    e1 = scene.add_entity(p1, Q1)
+    e2 = scene.add_entity(p2, IDENTITY)
+    assert (e1, e2) == (1, 2)
+    scene.upload_bricks(b1.keys, b1.voxels, entity=e1)
+    scene.upload_bricks(b2.keys, b2.voxels, entity=e2)
+    scene.set_entity_motion(e2, 1)
+    scene.flush()
+
+    osc = oracle_lib.OracleScene(oracle, vs)
+    o1 = oracle_lib.OracleScene(oracle, b1)
+    o2 = oracle_lib.OracleScene(oracle, b2)
+    osc.set_entities([(o1, Q1, p1), (o2, IDENTITY, p2)])
+    img = render_pair(cuda_device, scene, osc, vs)
+    render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
+    plain = oracle_lib.OracleScene(oracle, vs).render(72, 56, spp=2, bounces=4, seed=5, threads=8)[0]
+    assert not np.array_equal(img, plain)  # the entities are in view
+
+    # Moved; the next flush applies it.
+    scene.set_entity_transform(e1, p1, Q1_MOVED)
+    scene.flush()
+    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)])
+    render_pair(cuda_device, scene, osc, vs)
+
+    # Edited bricks of an entity (no new key: that entity's incremental flush).
+    rng = np.random.default_rng(3)
+    vox2 = b2.voxels.copy()
+    vox2[0] = np.where(rng.random(512) < 0.5, 0x8000 | 17, 0).astype(np.uint16)
+    scene.upload_bricks(b2.keys[:1], vox2[:1], entity=e2)
+    scene.flush()
+    b2e = workloads.VoxelScene(b2.grid, b2.keys, vox2, b2.power, b2.albedo, b2.camera, b2.group_shift)
+    o2 = oracle_lib.OracleScene(oracle, b2e)
+    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)])
+    render_pair(cuda_device, scene, osc, vs)
+
+    # Removed: the remaining entity keeps its order; a new entity takes the free id.
+    scene.remove_entity(e1)
+    osc.set_entities([(o2, IDENTITY, p2)])
+    render_pair(cuda_device, scene, osc, vs)  # the removal applies at once
+    e3 = scene.add_entity(p1, IDENTITY)
+    assert e3 == e1
+    scene.upload_bricks(b1.keys, b1.voxels, entity=e3)
+    scene.flush()
+    osc.set_entities([(o1, IDENTITY, p1), (o2, IDENTITY, p2)])
+    render_pair(cuda_device, scene, osc, vs)
+
+    # Entity bricks do not emit; entity 0 cannot be moved or removed; motion takes two values.
+    with pytest.raises(caelix_b200.CaelixError) as err:
+        scene.set_brick_power(b1.keys[:1], np.ones(1, np.float32), entity=e3)
+    assert err.value.code == caelix_b200.CAELIX_ERROR_UNSUPPORTED
+    with pytest.raises(caelix_b200.CaelixError):
+        scene.remove_entity(0)
+    with pytest.raises(caelix_b200.CaelixError):
+        scene.set_entity_motion(e3, 2)
+    with pytest.raises(caelix_b200.CaelixError):
+        scene.upload_bricks(b1.keys, b1.voxels, entity=7)
+    scene.close()
