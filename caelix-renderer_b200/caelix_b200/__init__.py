@@ -164,9 +164,10 @@ class Library:
                                                  C.POINTER(C.c_uint64)]
         L.caelix_world_upload_entity.argtypes = [vp, C.c_uint32, vp, C.c_uint32, C.POINTER(C.c_int32),
                                                  C.POINTER(C.c_uint64)]
+        L.caelix_world_load.argtypes = [vp, vp, C.c_uint32, C.POINTER(C.c_uint32), C.POINTER(C.c_uint64)]
         for name in (
             "caelix_world_open", "caelix_world_get_info", "caelix_world_get_entity", "caelix_world_get_sector",
-            "caelix_world_decode_sector", "caelix_world_upload_entity",
+            "caelix_world_decode_sector", "caelix_world_upload_entity", "caelix_world_load",
             "caelix_device_create", "caelix_device_check", "caelix_light_bvh_create",
             "caelix_light_bvh_build", "caelix_light_bvh_get_view", "caelix_light_bvh_get_stats",
             "caelix_radix_sort_pairs", "caelix_light_bvh_set_profiling",
@@ -597,6 +598,16 @@ class WorldFile:
         self.L.check(self.L.lib.caelix_world_upload_entity(self.handle, entity, scene.handle, threads, origin,
                                                            C.byref(bricks)), "caelix_world_upload_entity")
         return tuple(origin), bricks.value
+
+    def load(self, scene: "Scene", threads: int = 0):
+        """caelix_world_load: file entity 0 into the scene's world, every other entity as a scene
+        entity; returns (scene entity id of every file entity, bricks uploaded)."""
+        n = self.info().entity_count
+        ids = (C.c_uint32 * max(n, 1))()
+        bricks = C.c_uint64(0)
+        self.L.check(self.L.lib.caelix_world_load(self.handle, scene.handle, threads, ids, C.byref(bricks)),
+                     "caelix_world_load")
+        return list(ids)[:n], bricks.value
 
 
 def camera_struct(cam) -> CaelixCamera:

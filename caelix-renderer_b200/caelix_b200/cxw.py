@@ -174,11 +174,9 @@ def expected_sector(s: Sector):
     return keys, blocks, summaries, voxels
 
 
-def from_voxel_scene(vs, shift=(0, 0, 0), version: int = 8) -> bytes:
-    """A .cxw file holding the bricks of a workloads.VoxelScene as one static entity, the brick
-    keys moved by `shift` bricks (sectors of 16^3 bricks; all-air bricks are written too, the
-    reader drops them)."""
-    keys = np.asarray(vs.keys, np.int64) + np.asarray(shift, np.int64)
+def sectors_of(keys, voxels) -> list:
+    """The sectors (16^3 bricks) holding bricks of the given keys and values, in coordinate order."""
+    keys = np.asarray(keys, np.int64)
     coords = keys // 16
     local = keys - coords * 16
     bi = local[:, 0] + 16 * (local[:, 1] + 16 * local[:, 2])
@@ -186,6 +184,13 @@ def from_voxel_scene(vs, shift=(0, 0, 0), version: int = 8) -> bytes:
     c = coords[order]
     starts = np.flatnonzero(np.r_[True, (c[1:] != c[:-1]).any(axis=1)])
     ends = np.r_[starts[1:], len(order)]
-    voxels = np.asarray(vs.voxels, np.uint16)
-    sectors = [Sector(tuple(int(v) for v in c[a]), (bi[order[a:b]], voxels[order[a:b]])) for a, b in zip(starts, ends)]
-    return build(World(version, [Entity(sectors, flags_byte=2)]))
+    voxels = np.asarray(voxels, np.uint16)
+    return [Sector(tuple(int(v) for v in c[a]), (bi[order[a:b]], voxels[order[a:b]])) for a, b in zip(starts, ends)]
+
+
+def from_voxel_scene(vs, shift=(0, 0, 0), version: int = 8) -> bytes:
+    """A .cxw file holding the bricks of a workloads.VoxelScene as one static entity, the brick
+    keys moved by `shift` bricks (sectors of 16^3 bricks; all-air bricks are written too, the
+    reader drops them)."""
+    keys = np.asarray(vs.keys, np.int64) + np.asarray(shift, np.int64)
+    return build(World(version, [Entity(sectors_of(keys, vs.voxels), flags_byte=2)]))

@@ -10,6 +10,7 @@
 #include <algorithm>
 #include <atomic>
 #include <cinttypes>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -433,17 +434,19 @@ CAELIX_API CaelixResult caelix_world_decode_sector(const CaelixWorldFile* file, 
     CAELIX_GUARD_END
 }
 
-CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, uint32_t entity, CaelixScene* scene,
-                                                   uint32_t threads, int32_t origin[3], uint64_t* bricks)
+}  // extern "C"
+
+namespace {
+
+// Every sector of one file entity decoded on the host threads (each with its own inflate buffer),
+// and the entity's smallest key per axis (its origin in a scene, whose keys start at 0).
+CaelixResult decode_entity(const CaelixWorldFile* file, uint32_t entity, uint32_t threads, const char* what,
+                           std::vector<Decoded>& decoded, int32_t org[3])
 {
-    CAELIX_GUARD_BEGIN
-    if (bricks) *bricks = 0;
-    if (!file || !scene || entity >= file->entities.size()) return CAELIX_ERROR_INVALID_ARGUMENT;
     std::vector<const CaelixWorldSector*> mine;
     for (const CaelixWorldSector& s : file->sectors)
         if (s.entity == entity) mine.push_back(&s);
-    // Every sector decoded on the host threads (each with its own inflate buffer).
-    std::vector<Decoded> decoded(mine.size());
+    decoded.assign(mine.size(), Decoded());
     std::atomic<size_t> next{0};
     std::atomic<bool> failed{false};
     const uint32_t nt = std::max(1u, std::min<uint32_t>(threads ? threads : std::thread::hardware_concurrency(),
@@ -468,7 +471,6 @@ CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, 
     for (std::thread& th : pool) th.join();
     for (uint32_t t = 0; t < nt; ++t)
         if (has_error[t]) return report(first[t]);
-    // The entity's smallest key per axis becomes the scene's origin.
     int64_t lo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, hi[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
     uint64_t total = 0;
     for (const Decoded& d : decoded) {
@@ -481,20 +483,24 @@ CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, 
             }
         }
     }
-    int32_t org[3] = {0, 0, 0};
+    for (int a = 0; a < 3; ++a) org[a] = 0;
     if (total) {
         for (int a = 0; a < 3; ++a) {
             if (hi[a] - lo[a] >= kSceneKeyLimit) {
-                cx::log(CAELIX_LOG_ERROR,
-                        "caelix_world_upload_entity: entity %u spans %" PRId64 " bricks on axis %d (the scene holds %d)",
+                cx::log(CAELIX_LOG_ERROR, "%s: entity %u spans %" PRId64 " bricks on axis %d (the scene holds %d)", what,
                         entity, hi[a] - lo[a] + 1, a, kSceneKeyLimit);
                 return CAELIX_ERROR_UNSUPPORTED;
             }
             org[a] = (int32_t)lo[a];
         }
     }
-    if (origin) std::memcpy(origin, org, sizeof(org));
-    // Uploads in sector order, the keys moved to the origin.
+    return CAELIX_OK;
+}
+
+// Uploads decoded bricks to entity `target` of the scene in sector order, the keys moved to `org`.
+CaelixResult upload_decoded(const std::vector<Decoded>& decoded, const int32_t org[3], CaelixScene* scene,
+                            uint32_t target, uint64_t* bricks)
+{
     std::vector<CaelixBrickKey> keys;
     for (const Decoded& d : decoded) {
         if (d.keys.empty()) continue;
@@ -502,10 +508,109 @@ CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, 
         for (size_t i = 0; i < d.keys.size(); ++i)
             keys[i] = CaelixBrickKey{d.keys[i].x - org[0], d.keys[i].y - org[1], d.keys[i].z - org[2]};
         uint32_t consumed = 0;
-        const CaelixResult r = caelix_scene_upload_bricks(scene, 0, (uint32_t)keys.size(), keys.data(),
+        const CaelixResult r = caelix_scene_upload_bricks(scene, target, (uint32_t)keys.size(), keys.data(),
                                                           d.blocks.data(), &consumed);
         if (r != CAELIX_OK) return r;
         if (bricks) *bricks += consumed;
+    }
+    return CAELIX_OK;
+}
+
+// Rotation rows of a quaternion (x, y, z, w), normalised, in double.
+void quat_rows(const float q[4], double r[9])
+{
+    const double n = std::sqrt((double)q[0] * q[0] + (double)q[1] * q[1] + (double)q[2] * q[2] + (double)q[3] * q[3]);
+    const double x = q[0] / n, y = q[1] / n, z = q[2] / n, w = q[3] / n;
+    const double m[9] = {1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+                         2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+                         2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)};
+    for (int i = 0; i < 9; ++i) r[i] = m[i];
+}
+
+}  // namespace
+
+extern "C" {
+
+CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, uint32_t entity, CaelixScene* scene,
+                                                   uint32_t threads, int32_t origin[3], uint64_t* bricks)
+{
+    CAELIX_GUARD_BEGIN
+    if (bricks) *bricks = 0;
+    if (!file || !scene || entity >= file->entities.size()) return CAELIX_ERROR_INVALID_ARGUMENT;
+    std::vector<Decoded> decoded;
+    int32_t org[3];
+    CaelixResult r = decode_entity(file, entity, threads, "caelix_world_upload_entity", decoded, org);
+    if (r != CAELIX_OK) return r;
+    if (origin) std::memcpy(origin, org, sizeof(org));
+    return upload_decoded(decoded, org, scene, 0, bricks);
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_world_load(const CaelixWorldFile* file, CaelixScene* scene, uint32_t threads,
+                                          CaelixEntityId* ids, uint64_t* bricks)
+{
+    CAELIX_GUARD_BEGIN
+    if (bricks) *bricks = 0;
+    if (!file || !scene || file->entities.empty()) return CAELIX_ERROR_INVALID_ARGUMENT;
+    const uint32_t count = (uint32_t)file->entities.size();
+    if (ids)
+        for (uint32_t i = 0; i < count; ++i) ids[i] = CAELIX_INVALID_ENTITY;
+    // File entity 0 is the world: the scene's frame is its frame, moved by its origin,
+    // x_scene = R0^T (x_file - p0) - 8 org0.
+    std::vector<Decoded> decoded;
+    int32_t org0[3];
+    CaelixResult r = decode_entity(file, 0, threads, "caelix_world_load", decoded, org0);
+    if (r != CAELIX_OK) return r;
+    const CaelixWorldEntity& w = file->entities[0];
+    double r0[9];
+    quat_rows(w.rotation, r0);
+    // Every other entity first decoded and added (a failure removes the ones added), then the
+    // bricks uploaded.
+    std::vector<CaelixEntityId> added;
+    auto undo = [&](CaelixResult res) {
+        for (CaelixEntityId id : added) caelix_scene_remove_entity(scene, id);
+        if (ids)
+            for (uint32_t i = 0; i < count; ++i) ids[i] = CAELIX_INVALID_ENTITY;
+        return res;
+    };
+    r = upload_decoded(decoded, org0, scene, 0, bricks);
+    if (r != CAELIX_OK) return r;
+    if (ids) ids[0] = 0;
+    for (uint32_t i = 1; i < count; ++i) {
+        std::vector<Decoded> dec;
+        int32_t org[3];
+        r = decode_entity(file, i, threads, "caelix_world_load", dec, org);
+        if (r != CAELIX_OK) return undo(r);
+        const CaelixWorldEntity& e = file->entities[i];
+        double ri[9];
+        quat_rows(e.rotation, ri);
+        // Its keys start at its origin: x_file = Ri (local + 8 org) + pi.
+        double v[3];
+        for (int k = 0; k < 3; ++k)
+            v[k] = (ri[3 * k] * (8.0 * org[0]) + ri[3 * k + 1] * (8.0 * org[1]) + ri[3 * k + 2] * (8.0 * org[2])) +
+                   ((double)e.position[k] - (double)w.position[k]);
+        CaelixEntityDesc desc;
+        std::memcpy(desc.guid, e.guid, sizeof(desc.guid));
+        for (int k = 0; k < 3; ++k)
+            desc.position[k] = (float)((r0[k] * v[0] + r0[3 + k] * v[1] + r0[6 + k] * v[2]) - 8.0 * org0[k]);
+        // The rotation R0^T Ri as a quaternion: conj(q0) * qi.
+        const double n0 = std::sqrt((double)w.rotation[0] * w.rotation[0] + (double)w.rotation[1] * w.rotation[1] +
+                                    (double)w.rotation[2] * w.rotation[2] + (double)w.rotation[3] * w.rotation[3]);
+        const double ax = -w.rotation[0] / n0, ay = -w.rotation[1] / n0, az = -w.rotation[2] / n0,
+                     aw = w.rotation[3] / n0;
+        const double bx = e.rotation[0], by = e.rotation[1], bz = e.rotation[2], bw = e.rotation[3];
+        desc.rotation[0] = (float)(aw * bx + ax * bw + ay * bz - az * by);
+        desc.rotation[1] = (float)(aw * by - ax * bz + ay * bw + az * bx);
+        desc.rotation[2] = (float)(aw * bz + ax * by - ay * bx + az * bw);
+        desc.rotation[3] = (float)(aw * bw - ax * bx - ay * by - az * bz);
+        CaelixEntityId id = CAELIX_INVALID_ENTITY;
+        r = caelix_scene_add_entity(scene, &desc, &id);
+        if (r != CAELIX_OK) return undo(r);
+        added.push_back(id);
+        caelix_scene_set_entity_motion(scene, id, (e.flags & 2u) ? CAELIX_ENTITY_STATIC : CAELIX_ENTITY_DYNAMIC);
+        r = upload_decoded(dec, org, scene, id, bricks);
+        if (r != CAELIX_OK) return undo(r);
+        if (ids) ids[i] = id;
     }
     return CAELIX_OK;
     CAELIX_GUARD_END

@@ -734,6 +734,18 @@ CAELIX_API CaelixResult caelix_world_decode_sector(const CaelixWorldFile* file, 
    uploaded. *bricks (may be NULL) = bricks uploaded. */
 CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, uint32_t entity, CaelixScene* scene,
                                                    uint32_t threads, int32_t origin[3], uint64_t* bricks);
+/* Loads every entity of the file, as the reference's WorldLoader::open + upload
+   (host-rs/caelix-app/src/world.rs:93-262): file entity 0 into the scene's world (as
+   caelix_world_upload_entity: keys moved by its origin), every other entity as a scene entity
+   (caelix_scene_add_entity, motion from its Static flag) with its bricks moved by its own origin
+   and its transform expressed in the world's frame: x_scene = R0^T (x_file - p0) - 8 origin0, so
+   the added entity has rotation conj(q0) qi and position
+   R0^T (Ri (8 origin_i) + (pi - p0)) - 8 origin0 (computed in double, rounded to float).
+   ids (may be NULL) receives the scene entity of every file entity (0 for the world). A failure
+   removes the entities added (the world's bricks uploaded before it stay). *bricks (may be NULL)
+   = bricks uploaded. */
+CAELIX_API CaelixResult caelix_world_load(const CaelixWorldFile* file, CaelixScene* scene, uint32_t threads,
+                                          uint32_t* ids, uint64_t* bricks);
 
 #ifdef __cplusplus
 }

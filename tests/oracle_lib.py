@@ -233,8 +233,8 @@ class OracleScene:
         d = np.asarray(direction, np.float32)
         return self.lib.oc_trace_ray(C.byref(self.s), o.ctypes.data, d.ctypes.data, tmin, tmax)
 
-    def render(self, width, height, spp=1, bounces=4, seed=1, light_nee=True, window=None, threads=1):
-        cam = self.src.camera
+    def render(self, width, height, spp=1, bounces=4, seed=1, light_nee=True, window=None, threads=1, camera=None):
+        cam = self.src.camera if camera is None else camera
         c = Camera((C.c_float * 3)(*cam["position"]), (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]),
                    (C.c_float * 3)(*cam["forward"]), float(cam["tan_half_fov_y"]), float(cam["aspect"]))
         x0, y0, x1, y1 = window or (0, 0, width, height)

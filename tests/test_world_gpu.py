@@ -39,3 +39,99 @@ def test_world_file_into_scene(cuda_device, oracle, tmp_path):
     assert_scene_equal(scene, oracle_lib.OracleScene(oracle, exp), exp)
     scene.close()
     f.close()
+
+
+def rows64(q):
+    """Rotation rows of a quaternion in double, as the library computes them."""
+    import math
+
+    q = [float(np.float32(v)) for v in q]
+    n = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    x, y, z, w = q[0] / n, q[1] / n, q[2] / n, q[3] / n
+    return [1.0 - 2.0 * (y * y + z * z), 2.0 * (x * y - z * w), 2.0 * (x * z + y * w),
+            2.0 * (x * y + z * w), 1.0 - 2.0 * (x * x + z * z), 2.0 * (y * z - x * w),
+            2.0 * (x * z - y * w), 2.0 * (y * z + x * w), 1.0 - 2.0 * (x * x + y * y)]
+
+
+def test_world_load_with_entities(cuda_device, oracle, tmp_path):
+    """caelix_world_load: file entity 0 (rotated and moved) becomes the scene's world, entity 1 a
+    scene entity whose transform is expressed in the world's frame; the render equals the oracle's
+    with the same bricks and the transform computed here the library's way (double, then float)."""
+    import math
+
+    import caelix_b200
+    from test_entities_oracle import entity_bricks
+    from test_trace_gpu import assert_radiance_close
+
+    vs = workloads.noise_world(grid_bricks=(10, 8, 9), brick_occupancy=0.4, emissive_fraction=0.06, seed=23)
+    ent = entity_bricks(grid=(2, 2, 2), seed=7)
+    shift0, shift1 = np.array([-37, 5, -16]), np.array([3, -5, 20])
+    q0, p0 = (0.05, -0.1, 0.02, 0.99), (4.0, -2.5, 1.0)
+    q1, p1 = (0.2, 0.3, -0.1, 0.92), (60.0, 40.0, -30.0)
+    world_file = W.World(8, [W.Entity(W.sectors_of(vs.keys + shift0, vs.voxels), position=p0, rotation=q0, flags_byte=2),
+                             W.Entity(W.sectors_of(ent.keys + shift1, ent.voxels), guid=bytes(range(16, 32)),
+                                      position=p1, rotation=q1, flags_byte=0)])
+    path = tmp_path / "entities.cxw"
+    path.write_bytes(W.build(world_file))
+    f = caelix_b200.WorldFile(str(path))
+    scene = caelix_b200.Scene(cuda_device, vs.group_shift)
+    ids, bricks = f.load(scene, threads=4)
+    assert ids == [0, 1]
+    keep0 = (vs.voxels != 0).any(axis=1)
+    keep1 = (ent.voxels != 0).any(axis=1)
+    assert bricks == int(keep0.sum() + keep1.sum())
+    org0 = (vs.keys[keep0] + shift0).min(axis=0)
+    org1 = (ent.keys[keep1] + shift1).min(axis=0)
+
+    def moved(src, keys, voxels, power, shift, org):
+        k = keys + shift - org
+        grid = tuple(int(v) for v in k.max(axis=0) + 1)
+        lin = k[:, 0] + grid[0] * (k[:, 1] + grid[1] * k[:, 2].astype(np.int64))
+        o = np.argsort(lin, kind="stable")
+        return workloads.VoxelScene(grid, k[o].astype(np.int32), voxels[o], power[o], src.albedo, src.camera,
+                                    src.group_shift)
+
+    world = moved(vs, vs.keys[keep0], vs.voxels[keep0], vs.power[keep0], shift0, org0)
+    body = moved(ent, ent.keys[keep1], ent.voxels[keep1], ent.power[keep1], shift1, org1)
+    emissive = world.power > 0
+    scene.set_brick_power(world.keys[emissive], world.power[emissive])
+    scene.set_albedo(world.albedo)
+    scene.flush()
+    assert_scene_equal(scene, oracle_lib.OracleScene(oracle, world), world)
+
+    # The entity's transform in the world's frame, the library's arithmetic.
+    r0, r1 = rows64(q0), rows64(q1)
+    v = [(r1[3 * k] * (8.0 * org1[0]) + r1[3 * k + 1] * (8.0 * org1[1]) + r1[3 * k + 2] * (8.0 * org1[2])) +
+         (float(np.float32(p1[k])) - float(np.float32(p0[k]))) for k in range(3)]
+    pos = tuple(np.float32((r0[k] * v[0] + r0[3 + k] * v[1] + r0[6 + k] * v[2]) - 8.0 * org0[k]) for k in range(3))
+    a = [float(np.float32(c)) for c in q0]
+    n0 = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3])
+    ax, ay, az, aw = -a[0] / n0, -a[1] / n0, -a[2] / n0, a[3] / n0
+    bx, by, bz, bw = (float(np.float32(c)) for c in q1)
+    rot = (np.float32(aw * bx + ax * bw + ay * bz - az * by), np.float32(aw * by - ax * bz + ay * bw + az * bx),
+           np.float32(aw * bz + ax * by - ay * bx + az * bw), np.float32(aw * bw - ax * bx - ay * by - az * bz))
+
+    cam = workloads.look_at(np.array(pos, np.float64) + np.array([-30.0, 20.0, -30.0]), np.array(pos, np.float64))
+    osc = oracle_lib.OracleScene(oracle, world)
+    osc.set_entities([(oracle_lib.OracleScene(oracle, body), rot, pos)])
+    r = caelix_b200.Renderer(cuda_device, scene)
+    import torch
+
+    out = torch.zeros(48 * 64 * 3, dtype=torch.float32, device="cuda")
+    r.render(out, 64, 48, cam, bounces=3, seed=4, spp=2)
+    st = r.stats()
+    gpu = out.cpu().numpy().reshape(48, 64, 3)
+    ref, rays = osc.render(64, 48, spp=2, bounces=3, seed=4, threads=8, camera=cam)
+    assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == tuple(int(x) for x in rays)
+    assert_radiance_close(gpu, ref)
+    hits = 0
+    for py in range(0, 48, 4):
+        for px in range(0, 64, 4):
+            d = np.array(cam["right"]) * ((px + 0.5) / 64 * 2 - 1) * cam["tan_half_fov_y"] * cam["aspect"] + \
+                np.array(cam["up"]) * (1 - (py + 0.5) / 48 * 2) * cam["tan_half_fov_y"] + np.array(cam["forward"])
+            h = osc.trace(np.array(cam["position"], np.float32), (d / np.linalg.norm(d)).astype(np.float32))
+            hits += bool(h.hit and (h.attrib & 0x8000))
+    assert hits > 0  # the entity is in view
+    r.close()
+    scene.close()
+    f.close()
