@@ -132,6 +132,7 @@ typedef struct oc_scene_desc {
 } oc_scene_desc;
 
 struct oc_entity;
+struct oc_light_tree;
 
 typedef struct oc_scene {
     uint32_t grid[3];
@@ -161,6 +162,13 @@ typedef struct oc_scene {
     const struct oc_entity* entities;
     uint32_t entity_count;
     uint32_t pad2;
+    /* The entities' lights (NULL: none): their light blocks, group rows, frames and power merged
+     * into one light set (entity e's groups from its group_base, its bricks' power after the
+     * others', every index entry's leaf word 0x80000000 | leaf of the dynamic tree) and the
+     * dynamic light tree (tree 1) built over them. */
+    const struct oc_scene* dyn;
+    const struct oc_light_tree* dyn_tree;
+    const float* dyn_power;
 } oc_scene;
 
 /* An entity: its bricks (a scene of their own, entity-local block coordinates from 0, built with
@@ -169,10 +177,13 @@ typedef struct oc_entity {
     const oc_scene* scene;
     float rot[9];
     float pos[3];
+    uint32_t group_base; /* its first group in the merged light set */
+    const float* power;  /* its bricks' emitter power */
 } oc_entity;
 
-/* An entity hit (oc_hit.attrib bit 15; the hit's group is then the entity index and its normal
- * the rotated face normal; cell is bits 6..14, the block bits 16..31, so bit 15 is free). */
+/* An entity hit (oc_hit.attrib bit 15; the hit's group is then entity << 24 | the group in the
+ * entity, its normal the rotated face normal and object_hit the entity-local point; cell is
+ * bits 6..14, the block bits 16..31, so bit 15 is free). */
 #define OC_ENTITY_HIT 0x8000u
 
 /* Rotation rows of a quaternion (x, y, z, w; normalised first), computed in double and rounded:
@@ -242,9 +253,10 @@ void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, 
                 const float* d_radiance, double* image, double* d_albedo, double* d_power, int threads);
 
 /* Light tree draw for a point receiver (caelix_light_tree.hlsl:749-767): returns 1 and fills
- * out[0..2] position, out[3..5] normal, out[6] pdf, words[0..4] block, voxel, face, group, entry. */
+ * out[0..2] position, out[3..5] normal, out[6] pdf, words[0..5] block, voxel, face, group, entry,
+ * tree (0: the world's light set, 1: the entities', s->dyn). */
 int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t rng,
-                    float out[7], uint32_t words[5]);
+                    float out[7], uint32_t words[6]);
 /* count draws of oc_light_sample at one receiver (the reference probe's draw mode,
  * tests/light_tree_test.cpp:961 CheckHistogram): per draw out[4 i ..] = group, voxel in group
  * (x | y << 10 | z << 20), face, 1 (all zero for a failed draw). The draws' generator states come
@@ -258,6 +270,10 @@ float oc_mis_weight(float p_area, const float n_r[3], const float w[3], float d,
 /* The light tree pdf of a light face point (caelix_light_tree.hlsl:936-949). */
 float oc_light_point_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
                          uint32_t group, const uint32_t voxel_in_group[3], uint32_t face, uint32_t block);
+/* The same for a light face of either light set (tree 1: group of s->dyn). */
+float oc_light_point_pdf_tree(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
+                              uint32_t tree, uint32_t group, const uint32_t voxel_in_group[3], uint32_t face,
+                              uint32_t block);
 
 #ifdef __cplusplus
 }

@@ -308,7 +308,7 @@ oc_hit oc_trace_ray(const oc_scene* s, const float o[3], const float d[3], float
         if (!he.hit) continue;
         h = he;
         h.attrib |= OC_ENTITY_HIT;
-        h.group = e;
+        h.group = (e << 24) | he.group;
         const uint32_t f = (uint32_t)__builtin_ctz(he.attrib & 0x3Fu);
         const float sign = (f & 1u) ? -1.0f : 1.0f;
         float v[3];
@@ -423,25 +423,34 @@ static uint32_t child_count(const oc_node* node)
            (node->child[3] != OC_NONE);
 }
 
-/* The two trees' root summaries: tree 0 is the built tree, tree 1 (dynamic entities) is empty. */
-static void tree_summary(const oc_light_tree* t, uint32_t k, oc_summary* s, uint32_t* root)
+/* The two trees' root summaries: tree 0 is the world's tree, tree 1 the entities' (empty
+ * without entity lights). */
+static const oc_light_tree* tree_of(const oc_scene* sc, const oc_light_tree* t, uint32_t k)
+{
+    return k == 0 ? t : sc->dyn_tree;
+}
+
+static const oc_scene* lights_of(const oc_scene* sc, uint32_t k) { return k == 0 ? sc : sc->dyn; }
+
+static void tree_summary(const oc_scene* sc, const oc_light_tree* t, uint32_t k, oc_summary* s, uint32_t* root)
 {
     memset(s, 0, sizeof(*s));
     *root = OC_NONE;
-    if (k == 0 && t->header->root != OC_NONE) {
-        *root = t->header->root;
-        *s = t->header->s;
+    const oc_light_tree* tk = k == 0 ? t : (sc->dyn ? sc->dyn_tree : NULL);
+    if (tk && tk->header->root != OC_NONE) {
+        *root = tk->header->root;
+        *s = tk->header->s;
     }
 }
 
-static uint32_t choose_tree(const oc_light_tree* t, const float x[3], const float n[3], uint32_t* rng, float* pdf,
-                            uint32_t* root)
+static uint32_t choose_tree(const oc_scene* sc, const oc_light_tree* t, const float x[3], const float n[3],
+                            uint32_t* rng, float* pdf, uint32_t* root)
 {
     pick p = {0, 0, 0, 0, OC_NONE, OC_NONE};
     uint32_t roots[2];
     for (uint32_t k = 0; k < 2; ++k) {
         oc_summary s;
-        tree_summary(t, k, &s, &roots[k]);
+        tree_summary(sc, t, k, &s, &roots[k]);
         pick_add(&p, oc_importance(x, n, s.lo, s.hi, s.face), power6(s.face), k, lt_random_float(rng));
     }
     float prob;
@@ -451,13 +460,14 @@ static uint32_t choose_tree(const oc_light_tree* t, const float x[3], const floa
     return k;
 }
 
-static float tree_probability(const oc_light_tree* t, const float x[3], const float n[3], uint32_t target)
+static float tree_probability(const oc_scene* sc, const oc_light_tree* t, const float x[3], const float n[3],
+                              uint32_t target)
 {
     float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
     for (uint32_t k = 0; k < 2; ++k) {
         oc_summary s;
         uint32_t root;
-        tree_summary(t, k, &s, &root);
+        tree_summary(sc, t, k, &s, &root);
         const float imp = oc_importance(x, n, s.lo, s.hi, s.face);
         const float pw = power6(s.face);
         sum_i += imp > 0.0f ? imp : 0.0f;
@@ -519,17 +529,21 @@ static float slot_probability(const oc_node* nd, const float x[3], const float n
     return pick_probability(sum_i, sum_p, imp_t, pow_t);
 }
 
-static float leaf_probability(const oc_light_tree* t, uint32_t leaf, const float x[3], const float n[3])
+/* The probability of drawing leaf `leaf` of tree k (T): the slot picks up to its root, times the
+ * pick of tree k among the two (t: the world's tree). */
+static float leaf_probability(const oc_scene* sc, const oc_light_tree* t, const oc_light_tree* T, uint32_t leaf,
+                              const float x[3], const float n[3], uint32_t k)
 {
-    if (t->header->root == OC_NONE) return 0.0f;
-    const uint32_t parent = t->leaves[leaf].parent;
+    const oc_light_tree* t_ = T;
+    if (t_->header->root == OC_NONE) return 0.0f;
+    const uint32_t parent = t_->leaves[leaf].parent;
     if (parent == OC_NONE) return 0.0f;
     uint32_t node = parent >> 2, slot = parent & 3u;
     float probability = 1.0f;
     for (uint32_t depth = 0; depth < 64; ++depth) {
-        const oc_node* nd = &t->nodes[node];
+        const oc_node* nd = &t_->nodes[node];
         probability *= slot_probability(nd, x, n, slot);
-        if (nd->parent == OC_NONE) return probability * tree_probability(t, x, n, 0);
+        if (nd->parent == OC_NONE) return probability * tree_probability(sc, t, x, n, k);
         node = nd->parent;
         slot = nd->parent_slot;
     }
@@ -586,25 +600,28 @@ static float family_weights(const oc_scene* s, uint32_t group, const uint32_t* r
 }
 
 int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t rng,
-                    float out[7], uint32_t words[5])
+                    float out[7], uint32_t words[6])
 {
     memset(out, 0, 7 * sizeof(float));
-    memset(words, 0, 5 * sizeof(uint32_t));
+    memset(words, 0, 6 * sizeof(uint32_t));
     float pdf_brick = 1.0f;
     uint32_t root;
-    const uint32_t k = choose_tree(t, x, n, &rng, &pdf_brick, &root);
+    const uint32_t k = choose_tree(s, t, x, n, &rng, &pdf_brick, &root);
     if (k == OC_NONE) return 0;
-    const uint32_t leaf = choose_leaf(t, root, x, n, &rng, &pdf_brick);
+    const oc_light_tree* T = tree_of(s, t, k);
+    const oc_scene* L = lights_of(s, k);
+    const uint32_t leaf = choose_leaf(T, root, x, n, &rng, &pdf_brick);
     if (leaf == OC_NONE) return 0;
-    const uint32_t group = t->leaves[leaf].group;
-    const uint32_t entry = t->leaves[leaf].entry;
+    const uint32_t group = T->leaves[leaf].group;
+    const uint32_t entry = T->leaves[leaf].entry;
     words[3] = group;
     words[4] = entry;
-    const uint32_t* row = s->group_rows + 8ull * group;
+    words[5] = k;
+    const uint32_t* row = L->group_rows + 8ull * group;
     if (row[1] == 0) return 0;
-    const uint32_t* rec = entry_record(s, group, entry, NULL);
+    const uint32_t* rec = entry_record(L, group, entry, NULL);
     float w[6];
-    const float sum = family_weights(s, group, rec, x, w);
+    const float sum = family_weights(L, group, rec, x, w);
     if (sum <= 0.0f) return 0;
     const float u = lt_random_float(&rng) * sum;
     uint32_t f = OC_NONE, last = 0;
@@ -625,11 +642,11 @@ int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3],
     if (ei > count - 1u) ei = count - 1u;
     const uint32_t ent = rec[12 + first + ei];
     const uint32_t vi = ent & 0x1FFu;
-    const uint32_t gs = s->group_shift, gm = (1u << gs) - 1u;
+    const uint32_t gs = L->group_shift, gm = (1u << gs) - 1u;
     const uint32_t pos = rec[8];
     const uint32_t voxel[3] = {(pos & gm) * 8 + (vi & 7u), ((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u),
                                ((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)};
-    const oc_frame* fr = &s->group_frames[group];
+    const oc_frame* fr = &L->group_frames[group];
     const uint32_t axis = f >> 1;
     float local[3];
     for (int q = 0; q < 3; ++q) local[q] = fr->origin[q] + (float)voxel[q];
@@ -659,11 +676,11 @@ void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3],
     const uint32_t gs = s->group_shift, gm = (1u << gs) - 1u;
     for (uint32_t i = 0; i < count; ++i) {
         float p[7];
-        uint32_t words[5];
+        uint32_t words[6];
         uint32_t* o = out + 4ull * i;
         o[0] = o[1] = o[2] = o[3] = 0;
         if (!oc_light_sample(s, t, x, n, random_u32(&state), p, words)) continue;
-        const uint32_t pos = entry_record(s, words[3], words[4], NULL)[8];
+        const uint32_t pos = entry_record(lights_of(s, words[5]), words[3], words[4], NULL)[8];
         const uint32_t vi = words[1];
         o[0] = words[3];
         o[1] = ((pos & gm) * 8 + (vi & 7u)) | ((((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u)) << 10) |
@@ -733,27 +750,37 @@ static int find_light_face(const oc_scene* s, const oc_light_tree* t, const floa
     return 1;
 }
 
-static float brick_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t group,
-                       uint32_t entry)
+/* The draw probability of entry `entry` of group `group` of light set k (L, its tree T). */
+static float brick_pdf(const oc_scene* sc, const oc_light_tree* t, const oc_scene* L, const oc_light_tree* T,
+                       const float x[3], const float n[3], uint32_t group, uint32_t entry, uint32_t k)
 {
-    const uint32_t* row = s->group_rows + 8ull * group;
+    const uint32_t* row = L->group_rows + 8ull * group;
     if (row[1] == 0) return 0.0f;
-    const uint32_t* block_w = s->heap + 4ull * row[0];
+    const uint32_t* block_w = L->heap + 4ull * row[0];
     if (entry >= block_w[0]) return 0.0f;
     const uint32_t bvh_leaf = block_w[4 + 4 * entry + 3];
     if (bvh_leaf == OC_NONE) return 0.0f;
     const uint32_t leaf = bvh_leaf & 0x7FFFFFFFu;
-    if (t->leaves[leaf].group != group || t->leaves[leaf].entry != entry) return 0.0f;
-    return leaf_probability(t, leaf, x, n);
+    if (T->leaves[leaf].group != group || T->leaves[leaf].entry != entry) return 0.0f;
+    return leaf_probability(sc, t, T, leaf, x, n, k);
+}
+
+float oc_light_point_pdf_tree(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3],
+                              uint32_t tree, uint32_t group, const uint32_t v[3], uint32_t face, uint32_t block)
+{
+    const oc_scene* L = tree > 1 ? NULL : lights_of(s, tree);
+    if (!L) return 0.0f;
+    const oc_light_tree* T = tree_of(s, t, tree);
+    uint32_t entry, leaf;
+    float in_brick;
+    if (!find_light_face(L, T, x, group, v, face, block, &entry, &leaf, &in_brick)) return 0.0f;
+    return brick_pdf(s, t, L, T, x, n, group, entry, tree) * in_brick;
 }
 
 float oc_light_point_pdf(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t group,
                          const uint32_t v[3], uint32_t face, uint32_t block)
 {
-    uint32_t entry, leaf;
-    float in_brick;
-    if (!find_light_face(s, t, x, group, v, face, block, &entry, &leaf, &in_brick)) return 0.0f;
-    return brick_pdf(s, t, x, n, group, entry) * in_brick;
+    return oc_light_point_pdf_tree(s, t, x, n, 0, group, v, face, block);
 }
 
 /* ---- integrator ---- */
@@ -799,7 +826,7 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
     *dvalue = 0.0f;
     const uint32_t point_seed = random_u32(light_rng);
     float p[7];
-    uint32_t words[5];
+    uint32_t words[6];
     if (!oc_light_sample(c->s, c->t, x, n, point_seed, p, words) || !(p[6] > 0.0f)) return;
     float d[3] = {p[0] - x[0], p[1] - x[1], p[2] - x[2]};
     const float d2 = dot3(d, d);
@@ -811,12 +838,19 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
     if (!(cos_r > 0.0f) || !(cos_l > 0.0f)) return;
     float scale = (cos_r * (1.0f / K_PI)) * (cos_l / d2) / p[6];
     scale *= mis_weight(p[6], n, w, dist, cos_l, 1);
-    /* The lamp's emission: the brick of the sampled light voxel. */
-    const uint32_t* row = c->s->group_rows + 8ull * words[3];
-    const uint32_t* block_w = c->s->heap + 4ull * row[0];
+    /* The lamp's emission: the brick of the sampled light voxel (in the world, or in the entities'
+     * merged light set). */
+    const oc_scene* L = lights_of(c->s, words[5]);
+    const uint32_t* row = L->group_rows + 8ull * words[3];
+    const uint32_t* block_w = L->heap + 4ull * row[0];
     const uint32_t brick = block_w[4 + 4 * words[4] + 1];
     float e[3];
-    emission_of(c, brick, words[0], e);
+    if (words[5] == 0) {
+        emission_of(c, brick, words[0], e);
+    } else {
+        const float pw = (words[0] & OPAQUE) ? c->s->dyn_power[brick] : 0.0f;
+        e[0] = e[1] = e[2] = pw;
+    }
     float contribution[3] = {e[0] * scale, e[1] * scale, e[2] * scale};
     const float lum = contribution[0] * 0.2126f + contribution[1] * 0.7152f + contribution[2] * 0.0722f;
     const float w_lamp = lum * hmax(0.05f, 1.0f);
@@ -833,7 +867,7 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
         const float k = w_sum / w_lamp;
         for (int q = 0; q < 3; ++q) out[q] = contribution[q] * k;
         /* For the adjoint: the contribution is the lamp brick's power times scale * k. */
-        if (words[0] & OPAQUE) {
+        if ((words[0] & OPAQUE) && words[5] == 0) {
             *lamp_brick = brick;
             *dvalue = scale * k;
         }
@@ -843,20 +877,35 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
 static float lamp_hit_weight(ctx* c, uint32_t segment_light, const oc_hit* h, const float origin[3], const float dir[3],
                              const float seg_n[3])
 {
-    if (segment_light == 0u || h->t < NEAR_FIELD || (h->attrib & OC_ENTITY_HIT)) return 1.0f;
-    int32_t voxel[3];
-    for (int k = 0; k < 3; ++k) voxel[k] = (int32_t)floorf(h->object_hit[k] - 0.25f * h->normal[k]);
-    const oc_frame* fr = &c->s->group_frames[h->group];
-    uint32_t vig[3];
-    for (int k = 0; k < 3; ++k) vig[k] = (uint32_t)(voxel[k] - (int32_t)fr->origin[k]);
+    if (segment_light == 0u || h->t < NEAR_FIELD) return 1.0f;
+    /* The light set of the hit: the world's, or for an entity hit the entities' (its groups from
+     * the entity's group base; the voxel from the entity-local hit point and face normal). */
+    const oc_scene* L = c->s;
+    const oc_light_tree* T = c->t;
+    uint32_t group = h->group, k = 0;
     const uint32_t face = (uint32_t)__builtin_ctz(h->attrib & 0x3Fu);
+    float nl[3] = {h->normal[0], h->normal[1], h->normal[2]};
+    if (h->attrib & OC_ENTITY_HIT) {
+        if (!c->s->dyn) return 1.0f;
+        L = c->s->dyn;
+        T = c->s->dyn_tree;
+        k = 1;
+        group = c->s->entities[h->group >> 24].group_base + (h->group & 0xFFFFFFu);
+        for (int q = 0; q < 3; ++q) nl[q] = 0.0f;
+        nl[face >> 1] = (face & 1u) ? -1.0f : 1.0f;
+    }
+    int32_t voxel[3];
+    for (int q = 0; q < 3; ++q) voxel[q] = (int32_t)floorf(h->object_hit[q] - 0.25f * nl[q]);
+    const oc_frame* fr = &L->group_frames[group];
+    uint32_t vig[3];
+    for (int q = 0; q < 3; ++q) vig[q] = (uint32_t)(voxel[q] - (int32_t)fr->origin[q]);
     const uint32_t block = (h->attrib >> 16) & 0xFFFFu;
     uint32_t entry, leaf;
     float in_brick;
-    if (!find_light_face(c->s, c->t, origin, h->group, vig, face, block, &entry, &leaf, &in_brick) || leaf == OC_NONE)
+    if (!find_light_face(L, T, origin, group, vig, face, block, &entry, &leaf, &in_brick) || leaf == OC_NONE)
         return 1.0f;
     const float cos_l = -dot3(h->normal, dir);
-    const float p_area = brick_pdf(c->s, c->t, origin, seg_n, h->group, entry) * in_brick;
+    const float p_area = brick_pdf(c->s, c->t, L, T, origin, seg_n, group, entry, k) * in_brick;
     return mis_weight(p_area, seg_n, dir, h->t, cos_l, 0);
 }
 
@@ -864,7 +913,13 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
                   float albedo[3], float emission[3], float origin[3], float dir[3])
 {
     const uint32_t block = (h->attrib >> 16) & 0xFFFFu;
-    emission_of(c, h->record, (h->attrib & OC_ENTITY_HIT) ? 0u : block, emission); /* entities do not emit */
+    if (h->attrib & OC_ENTITY_HIT) { /* an entity brick's power */
+        const float* pw = c->s->entities[h->group >> 24].power;
+        const float p = (pw && (block & OPAQUE)) ? pw[h->record] : 0.0f;
+        emission[0] = emission[1] = emission[2] = p;
+    } else {
+        emission_of(c, h->record, block, emission);
+    }
     const float* a = c->albedo + 3 * (block & 0x7Fu); /* the material id of the 128-row table */
     albedo[0] = a[0];
     albedo[1] = a[1];

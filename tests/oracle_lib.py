@@ -95,11 +95,13 @@ class Scene(C.Structure):
         "groups2", "pad")] + [(n, C.c_void_p) for n in (
         "records", "hash_slots", "bitmap", "light_headers", "light_group", "light_entry", "light_brick",
         "heap", "group_rows", "group_frames")] + [("entities", C.c_void_p), ("entity_count", C.c_uint32),
-                                                   ("pad2", C.c_uint32)]
+                                                   ("pad2", C.c_uint32), ("dyn", C.c_void_p), ("dyn_tree", C.c_void_p),
+                                                   ("dyn_power", C.c_void_p)]
 
 
 class Entity(C.Structure):
-    _fields_ = [("scene", C.c_void_p), ("rot", C.c_float * 9), ("pos", C.c_float * 3)]
+    _fields_ = [("scene", C.c_void_p), ("rot", C.c_float * 9), ("pos", C.c_float * 3), ("group_base", C.c_uint32),
+                ("power", C.c_void_p)]
 
 
 class Camera(C.Structure):
@@ -145,6 +147,9 @@ def _bind_scene(lib):
     lib.oc_light_point_pdf.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
                                        C.c_void_p, C.c_uint32, C.c_uint32]
     lib.oc_light_point_pdf.restype = C.c_float
+    lib.oc_light_point_pdf_tree.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p,
+                                            C.c_uint32, C.c_uint32, C.c_void_p, C.c_uint32, C.c_uint32]
+    lib.oc_light_point_pdf_tree.restype = C.c_float
     lib.oc_light_draws.argtypes = [C.POINTER(Scene), C.POINTER(LightTree), C.c_void_p, C.c_void_p, C.c_uint32,
                                    C.c_uint32, C.c_void_p]
     lib.oc_light_draws.restype = None
@@ -199,9 +204,16 @@ class OracleScene:
 
     def set_entities(self, entities):
         """Entities beside the scene's bricks: (OracleScene of the entity's bricks, quaternion x y z w,
-        position) each, traversed in order; rotation rows as the library computes them."""
+        position) each, traversed in order; rotation rows as the library computes them. The
+        entities' light records (of bricks with power) are merged into one light set in entity
+        order, with its own light tree (tree 1): entity i's groups from the sum of the earlier
+        entities' group counts, its heap units, brick indices and leaves after theirs (the index
+        entries' brick and leaf words moved, the leaf word marked 0x80000000), every group's frame
+        the entity's transform."""
         self._entity_scenes = [e[0] for e in entities]
         arr = (Entity * max(len(entities), 1))()
+        heaps, rows, frames, powers, headers, lgroup, lentry = [], [], [], [], [], [], []
+        group_base = unit_base = record_base = light_base = 0
         for i, (osc, q, pos) in enumerate(entities):
             qf = np.ascontiguousarray(q, np.float32)
             rot = np.zeros(9, np.float32)
@@ -209,14 +221,68 @@ class OracleScene:
             arr[i].scene = C.cast(C.pointer(osc.s), C.c_void_p)
             arr[i].rot[:] = [float(v) for v in rot]
             arr[i].pos[:] = [float(v) for v in np.asarray(pos, np.float32)]
+            arr[i].group_base = group_base
+            arr[i].power = osc.src.power.ctypes.data
+            heap = osc.heap.copy()
+            r = osc.group_rows.copy()
+            for g in np.nonzero(r[:, 1])[0]:
+                block = int(r[g, 0]) * 4
+                for e in range(int(heap[block])):
+                    ie = block + 4 + 4 * e
+                    heap[ie + 1] += record_base
+                    heap[ie + 3] = 0x80000000 | (light_base + (int(heap[ie + 3]) & 0x7FFFFFFF))
+                r[g, 0] += unit_base
+            heaps.append(heap)
+            rows.append(r)
+            fr = osc.group_frames.copy()
+            fr["rotation"] = rot
+            fr["translation"] = np.asarray(pos, np.float32)
+            frames.append(fr)
+            powers.append(osc.src.power)
+            if osc.light_count:
+                headers.append(osc.light_headers)
+                lgroup.append(osc.light_group + group_base)
+                lentry.append(osc.light_entry)
+            group_base += len(r)
+            unit_base += len(heap) // 4
+            record_base += osc.src.brick_count
+            light_base += osc.light_count
         self._entities = arr
         self.s.entities = C.cast(arr, C.c_void_p) if entities else None
         self.s.entity_count = len(entities)
+        self.s.dyn = self.s.dyn_tree = self.s.dyn_power = None
+        if light_base:
+            from caelix_b200 import workloads
+
+            self.dyn_heap = np.ascontiguousarray(np.concatenate(heaps), np.uint32)
+            self.dyn_rows = np.ascontiguousarray(np.concatenate(rows), np.uint32)
+            self.dyn_frames = np.ascontiguousarray(np.concatenate(frames))
+            self.dyn_power = np.ascontiguousarray(np.concatenate(powers), np.float32)
+            self.dyn_headers = np.ascontiguousarray(np.concatenate(headers)).view(workloads.RECORD_DTYPE)
+            self.dyn_group = np.ascontiguousarray(np.concatenate(lgroup), np.uint32)
+            self.dyn_entry = np.ascontiguousarray(np.concatenate(lentry), np.uint32)
+            self.dyn_tree = lt_build(self.lib, self.dyn_headers, record_group=self.dyn_group, record_entry=self.dyn_entry,
+                                     group_frames=self.dyn_frames)
+            self._dyn_lt = LightTree(self.dyn_tree["leaves"].ctypes.data, self.dyn_tree["nodes"].ctypes.data,
+                                     self.dyn_tree["header"].ctypes.data)
+            d = Scene()
+            d.group_shift = self.s.group_shift
+            d.group_count = len(self.dyn_rows)
+            d.light_count = light_base
+            d.heap_words = len(self.dyn_heap)
+            d.heap = self.dyn_heap.ctypes.data
+            d.group_rows = self.dyn_rows.ctypes.data
+            d.group_frames = self.dyn_frames.ctypes.data
+            self._dyn = d
+            self.s.dyn = C.cast(C.pointer(d), C.c_void_p)
+            self.s.dyn_tree = C.cast(C.pointer(self._dyn_lt), C.c_void_p)
+            self.s.dyn_power = self.dyn_power.ctypes.data
 
     def close(self):
         if self.s.records:
             self.s.entities = None
             self.s.entity_count = 0
+            self.s.dyn = self.s.dyn_tree = self.s.dyn_power = None
             self.lib.oc_scene_free(C.byref(self.s))
 
     def __del__(self):

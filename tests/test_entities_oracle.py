@@ -3,7 +3,9 @@ bricks (the reference's TLAS instances, shaders/render/caelix_scene_trace.hlsl:1
 the instance's object space, the committed object-to-world normal). Checked against independent
 restatements: an entity at a translation equals the same bricks merged into the world; a rotated
 solid brick is hit where an exact slab test in double precision says; an entity no ray reaches
-leaves the render bit-identical."""
+leaves the render bit-identical. Entity lights (the reference's dynamic light tree,
+docs/LIGHT_TREE.md:136-176): the pdf over both trees is normalised, draws from the second tree
+match their pdf, and NEE over both trees with entity lamps converges to path tracing."""
 import ctypes as C
 
 import numpy as np
@@ -14,7 +16,7 @@ from caelix_b200 import workloads
 
 
 def entity_bricks(grid=(2, 2, 2), seed=7, fill=0.55):
-    """A small brick set of its own (power 0: entity bricks do not emit)."""
+    """A small brick set of its own, without emitters."""
     vs = workloads.noise_world(grid_bricks=grid, brick_occupancy=1.0, voxel_fill=fill, emissive_fraction=0.0, seed=seed)
     return workloads.VoxelScene(vs.grid, vs.keys, vs.voxels, np.zeros_like(vs.power), vs.albedo, vs.camera,
                                 vs.group_shift)
@@ -129,3 +131,130 @@ def test_entity_in_view_changes_the_render(oracle, world):
     dark, _ = w.render(40, 32, spp=1, bounces=0, seed=2, light_nee=False, threads=4)
     centre = dark[12:20, 16:24]
     assert np.all(centre == 0.0)
+
+
+def light_faces(heap, rows, group_shift):
+    """(group, voxel in group, face, block) of every face entry of a light set's blocks."""
+    faces = []
+    gm = (1 << group_shift) - 1
+    for g, row in enumerate(rows):
+        if row[1] == 0:
+            continue
+        block = int(row[0]) * 4
+        for e in range(int(heap[block])):
+            ie = block + 4 + 4 * e
+            rec = block + 4 * int(heap[ie + 2])
+            pos = int(heap[rec + 8])
+            clo, chi = int(heap[rec + 10]), int(heap[rec + 11])
+            counts = [(clo >> (10 * f)) & 0x3FF for f in range(3)] + [(chi >> (10 * f)) & 0x3FF for f in range(3)]
+            bo = np.array([pos & gm, (pos >> group_shift) & gm, (pos >> (2 * group_shift)) & gm]) * 8
+            first = 0
+            for f in range(6):
+                for q in range(counts[f]):
+                    ent = int(heap[rec + 12 + first + q])
+                    vi = ent & 0x1FF
+                    v = bo + np.array([vi & 7, (vi >> 3) & 7, vi >> 6])
+                    faces.append((g, v.astype(np.uint32), f, ent >> 16))
+                first += counts[f]
+    return faces
+
+
+def lit_entity(grid, seed, fill=0.6, lit=0.5):
+    vs = entity_bricks(grid=grid, seed=seed, fill=fill)
+    rng = np.random.default_rng(seed)
+    power = np.where(rng.random(vs.brick_count) < lit, rng.lognormal(0.0, 1.0, vs.brick_count), 0.0).astype(np.float32)
+    return workloads.VoxelScene(vs.grid, vs.keys, vs.voxels, power, vs.albedo, vs.camera, vs.group_shift)
+
+
+@pytest.fixture(scope="module")
+def lit_scene(oracle, world):
+    w = oracle_lib.OracleScene(oracle, world)
+    e1 = oracle_lib.OracleScene(oracle, lit_entity((2, 2, 2), 31))
+    e2 = oracle_lib.OracleScene(oracle, lit_entity((2, 1, 2), 32))
+    w.set_entities([(e1, (0.2, -0.1, 0.3, 0.93), (60.0, 10.0, 5.0)), (e2, (0.0, 0.0, 0.0, 1.0), (-30.0, 20.0, 12.0))])
+    assert w.s.dyn and w.dyn_tree["header"][0]["root"] != 0xFFFFFFFF
+    return w
+
+
+def test_pdf_normalised_over_both_trees(lit_scene, world):
+    """The light-tree pdf summed over every light face of the world and of the entities (each face
+    of area 1 in its frame) is 1 (1e-4) for every receiver: the tree choice and both trees' walks
+    are consistent (the reference's CheckNormalisation over its two trees)."""
+    w = lit_scene
+    faces0 = light_faces(w.heap, w.group_rows, w.s.group_shift)
+    faces1 = light_faces(w.dyn_heap, w.dyn_rows, w.s.group_shift)
+    assert faces0 and faces1
+    rng = np.random.default_rng(8)
+    span = np.array(world.grid, np.float64) * 8
+    for _ in range(8):
+        x = (rng.uniform(-0.5, 1.5, 3) * span).astype(np.float32)
+        n = rng.normal(size=3)
+        n = (n / np.linalg.norm(n)).astype(np.float32)
+        total = 0.0
+        for tree, faces in ((0, faces0), (1, faces1)):
+            for g, v, f, blk in faces:
+                total += w.lib.oc_light_point_pdf_tree(C.byref(w.s), C.byref(w.lt), x.ctypes.data, n.ctypes.data, tree,
+                                                       g, np.ascontiguousarray(v).ctypes.data, f, blk)
+        assert abs(total - 1.0) <= 1e-4, total
+
+
+def test_entity_light_draws_match_their_pdf(lit_scene, world):
+    """Draws from both trees: a drawn point's pdf equals the pdf evaluated at its face (1e-4), its
+    position lies on the face under the entity's transform, and tree 1 is drawn."""
+    w = lit_scene
+    rng = np.random.default_rng(9)
+    span = np.array(world.grid, np.float64) * 8
+    drawn = [0, 0]
+    for i in range(400):
+        x = (rng.uniform(-0.5, 1.5, 3) * span).astype(np.float32)
+        n = np.zeros(3, np.float32)
+        out = np.zeros(7, np.float32)
+        words = np.zeros(6, np.uint32)
+        if not w.lib.oc_light_sample(C.byref(w.s), C.byref(w.lt), x.ctypes.data, n.ctypes.data, 77 + i,
+                                     out.ctypes.data, words.ctypes.data):
+            continue
+        block, vi, face, group, entry, tree = (int(v) for v in words)
+        drawn[tree] += 1
+        frames = w.dyn_frames if tree else w.group_frames
+        fr = frames[group]
+        R = fr["rotation"].reshape(3, 3).astype(np.float64)
+        local = R.T @ (out[:3].astype(np.float64) - fr["translation"]) - fr["origin"]
+        nl = R.T @ out[3:6].astype(np.float64)
+        v = np.floor(local - 0.25 * nl + 1e-9).astype(np.int64)
+        pdf = w.lib.oc_light_point_pdf_tree(C.byref(w.s), C.byref(w.lt), x.ctypes.data, n.ctypes.data, tree, group,
+                                            np.ascontiguousarray(v.astype(np.uint32)).ctypes.data, face, block)
+        assert abs(pdf - out[6]) <= 1e-4 * max(pdf, out[6]), (tree, pdf, out[6])
+    assert drawn[0] > 20 and drawn[1] > 20, drawn
+
+
+def test_entity_lamps_unbiased(oracle):
+    """NEE with MIS over both trees converges to the plain path tracer when the lamps are entity
+    bricks (rotated lamp panels in a closed room): the emission of entity hits, the second tree's
+    draws and its pdf on BSDF hits agree (mean ratio in [0.97, 1.03], block PSNR above 30 dB)."""
+    import os
+
+    from test_light_nee_oracle import compare_light, lamp_box
+
+    room = lamp_box()
+    walls = room.power == 0
+    world = workloads.VoxelScene(room.grid, room.keys[walls], room.voxels[walls], room.power[walls], room.albedo,
+                                 room.camera, room.group_shift)
+    panel = np.zeros((1, 512), np.uint16)
+    v = np.arange(512)
+    vx, vy, vz = v % 8, (v // 8) % 8, v // 64
+    panel[0] = np.where((vy == 0) & (vx < 6) & (vz < 6), 0x8009, 0)
+    lamp = workloads.VoxelScene((1, 1, 1), np.zeros((1, 3), np.int32), panel, np.full(1, 16.0, np.float32),
+                                room.albedo, room.camera, room.group_shift)
+    w = oracle_lib.OracleScene(oracle, world)
+    lamps = [oracle_lib.OracleScene(oracle, lamp) for _ in range(3)]
+    w.set_entities([(lamps[0], (0.1, 0.0, 0.05, 0.99), (10.0, 37.0, 12.0)),
+                    (lamps[1], (0.0, 0.3, 0.0, 0.95), (28.0, 38.0, 26.0)),
+                    (lamps[2], (-0.08, 0.0, 0.1, 0.99), (14.0, 36.0, 30.0))])
+    threads = max(1, min(8, os.cpu_count() or 1))
+    pt = w.render(32, 32, spp=2048, bounces=4, seed=100000, light_nee=False, threads=threads)[0]
+    nee, rays = w.render(32, 32, spp=512, bounces=4, seed=200000, light_nee=True, threads=threads)
+    assert rays[2] > 0
+    ref_mean, test_mean, psnr = compare_light(pt, nee, direct=8.0)
+    assert ref_mean > 0.01
+    assert 0.97 < test_mean / ref_mean < 1.03, (ref_mean, test_mean)
+    assert psnr > 30.0, psnr

@@ -88,7 +88,7 @@ def test_mis_sides_see_the_same_pdf(lamp_scene):
         for k in range(draws_per_receiver):
             total += 1
             out = np.zeros(7, np.float32)
-            words = np.zeros(5, np.uint32)
+            words = np.zeros(6, np.uint32)
             if not lib.oc_light_sample(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data,
                                        99 + 977 * i + k, out.ctypes.data, words.ctypes.data):
                 continue

@@ -177,12 +177,13 @@ def test_light_sample_pdf_consistency(osc, small_scene):
     checked = 0
     for i, (x, n) in enumerate(zip(xs, ns)):
         out = np.zeros(7, np.float32)
-        words = np.zeros(5, np.uint32)
+        words = np.zeros(6, np.uint32)
         ok = osc.lib.oc_light_sample(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data, 1000 + i,
                                      out.ctypes.data, words.ctypes.data)
         if not ok:
             continue
-        block, vi, face, group, entry = (int(w) for w in words)
+        block, vi, face, group, entry, tree = (int(w) for w in words)
+        assert tree == 0
         fr = osc.group_frames[group]
         v = np.floor(out[:3] - 0.25 * out[3:6] - fr["origin"]).astype(np.int64)
         pdf = osc.lib.oc_light_point_pdf(C.byref(osc.s), C.byref(osc.lt), x.ctypes.data, n.ctypes.data, group,
