@@ -55,26 +55,121 @@ CaelixScene* entity_bricks(CaelixScene* scene, uint32_t entity)
     return scene->entities[entity - 1].bricks;
 }
 
-// Rewrites the device views of the live entities (after waiting for the device: renders may read
-// the old ones) and returns when they are in place. An entity whose bricks were never flushed has
-// no tables yet and joins at the flush that builds them.
+uint64_t align256(uint64_t v) { return (v + 255) & ~255ull; }
+
+// The entities' light set: every live entity's light blocks, group rows, frames, power and light
+// records appended in view order (cx::dyn_append moves their indices), then the dynamic light
+// tree built over them, and the device copy of its SceneView. No entity light: none.
+CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const CaelixScene::Entity*>& live,
+                                 std::vector<cx::EntityView>& views, cudaStream_t stream)
+{
+    scene->dyn_live = false;
+    uint64_t units = 0, groups = 0, bricks = 0, lights = 0;
+    for (size_t i = 0; i < live.size(); ++i) {
+        const cx::DeviceScene& d = live[i]->bricks->dev;
+        views[i].group_base = (uint32_t)groups;
+        units += d.heap_words / 4;
+        groups += d.group_count;
+        bricks += d.brick_count;
+        lights += d.light_count;
+    }
+    if (lights == 0) return CAELIX_OK;
+    if (units * 4 >= (1ull << 32) || groups >= (1ull << 32) || bricks >= (1ull << 32) || lights >= (1ull << 31))
+        return CAELIX_ERROR_OUT_OF_MEMORY;
+    // One allocation, carved: heap, rows, frames, power, records, record groups, record entries.
+    const uint64_t o_rows = align256(16 * units), o_frames = o_rows + align256(32 * groups),
+                   o_power = o_frames + align256(sizeof(cx::GroupFrame) * groups),
+                   o_hdr = o_power + align256(4 * bricks), o_group = o_hdr + align256(sizeof(cx::BrickLightRecord) * lights),
+                   o_entry = o_group + align256(4 * lights), total = o_entry + align256(4 * lights);
+    CaelixResult r = scene->dyn_arrays.reserve_grow(total, "caelix_scene_flush");
+    if (r != CAELIX_OK) return r;
+    uint8_t* base = static_cast<uint8_t*>(scene->dyn_arrays.ptr);
+    uint32_t* heap = reinterpret_cast<uint32_t*>(base);
+    uint32_t* rows = reinterpret_cast<uint32_t*>(base + o_rows);
+    cx::GroupFrame* frames = reinterpret_cast<cx::GroupFrame*>(base + o_frames);
+    float* power = reinterpret_cast<float*>(base + o_power);
+    cx::BrickLightRecord* hdr = reinterpret_cast<cx::BrickLightRecord*>(base + o_hdr);
+    uint32_t* lgroup = reinterpret_cast<uint32_t*>(base + o_group);
+    uint32_t* lentry = reinterpret_cast<uint32_t*>(base + o_entry);
+    if (lights > scene->dyn_tree_capacity) {
+        const uint32_t cap = (uint32_t)std::max<uint64_t>(lights + lights / 8, 64);
+        r = scene->dyn_tree.reserve(cx::lt_buffer_bytes(cap), "caelix_scene_flush");
+        if (r != CAELIX_OK) return r;
+        scene->dyn_tree_capacity = cap;
+    }
+    const cx::LightBvhBuffers tree = cx::lt_carve(scene->dyn_tree.ptr, scene->dyn_tree_capacity);
+    cudaError_t e = cudaSuccess;
+    cx::DynPart part{0, 0, 0, 0, {}, {}};
+    for (size_t i = 0; i < live.size() && e == cudaSuccess; ++i) {
+        const cx::DeviceScene& d = live[i]->bricks->dev;
+        part.group_base = views[i].group_base;
+        std::memcpy(part.rot, live[i]->rot, sizeof(part.rot));
+        std::memcpy(part.pos, live[i]->position, sizeof(part.pos));
+        e = cx::dyn_append(d, part, heap, rows, frames, power, hdr, lgroup, lentry, stream);
+        part.unit_base += d.heap_words / 4;
+        part.record_base += d.brick_count;
+        part.light_base += d.light_count;
+    }
+    cx::LightBvhInput in;
+    in.records = hdr;
+    in.count = (uint32_t)lights;
+    in.record_group = lgroup;
+    in.record_entry = lentry;
+    in.group_frames = frames;
+    in.group_count = (uint32_t)groups;
+    in.sort_keys_per_thread = cx::kSortKeysPerThread;
+    if (e == cudaSuccess) e = cx::lt_build(tree, in, stream, nullptr);
+    cx::SceneView v;
+    std::memset(&v, 0, sizeof(v));
+    v.group_shift = scene->group_shift;
+    v.power = power;
+    v.heap = heap;
+    v.group_rows = rows;
+    v.frames = frames;
+    v.leaves = tree.leaves;
+    v.nodes = tree.nodes;
+    v.header = tree.header;
+    v.light_count = (uint32_t)lights;
+    v.group_count = (uint32_t)groups;
+    if (e == cudaSuccess) {
+        r = scene->dyn_view.reserve_grow(sizeof(v), "caelix_scene_flush");
+        if (r != CAELIX_OK) return r;
+        e = cudaMemcpyAsync(scene->dyn_view.ptr, &v, sizeof(v), cudaMemcpyHostToDevice, stream);
+    }
+    uint32_t status = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &tree.state->status, 4, cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    if (status & ~cx::kStatusNodeOverflow) return cx::status_result(status, "caelix_scene_flush");
+    scene->dyn_live = true;
+    return CAELIX_OK;
+}
+
+// Rewrites the device views of the live entities and their light set (after waiting for the
+// device: renders may read the old ones) and returns when they are in place. An entity whose
+// bricks were never flushed has no tables yet and joins at the flush that builds them.
 CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
 {
     std::vector<cx::EntityView> views;
+    std::vector<const CaelixScene::Entity*> live;
     for (auto& e : scene->entities) {
         if (!e.bricks || !e.bricks->built) continue;
         cx::EntityView v;
         v.scene = cx::scene_view(e.bricks->dev);
         std::memcpy(v.rot, e.rot, sizeof(v.rot));
         std::memcpy(v.pos, e.position, sizeof(v.pos));
+        v.group_base = 0;
         views.push_back(v);
+        live.push_back(&e);
         e.generation = e.bricks->generation;
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     scene->entity_view_count = 0;
+    CaelixResult r = build_entity_lights(scene, live, views, stream);
+    if (r != CAELIX_OK) return r;
     if (!views.empty()) {
-        CaelixResult r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
+        r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
         if (r != CAELIX_OK) return r;
         e = cudaMemcpyAsync(scene->entity_views.ptr, views.data(), sizeof(cx::EntityView) * views.size(),
                             cudaMemcpyHostToDevice, stream);
@@ -94,6 +189,7 @@ cx::SceneView render_view(const CaelixScene* scene)
     if (scene->entity_view_count) {
         v.entities = static_cast<const cx::EntityView*>(scene->entity_views.ptr);
         v.entity_count = scene->entity_view_count;
+        if (scene->dyn_live) v.dyn = static_cast<const cx::SceneView*>(scene->dyn_view.ptr);
     }
     return v;
 }
@@ -175,6 +271,9 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     for (auto& e : scene->entities) caelix_scene_destroy(e.bricks);
     scene->entities.clear();
     scene->entity_views.release();
+    scene->dyn_arrays.release();
+    scene->dyn_tree.release();
+    scene->dyn_view.release();
     cx::scene_release(scene->dev);
     if (scene->upload_stream) cudaStreamSynchronize(scene->upload_stream);
     if (scene->stage_keys) cudaFree(scene->stage_keys);
@@ -401,7 +500,6 @@ CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const Caelix
     CaelixScene* bricks = nullptr;
     CaelixResult r = caelix_scene_create(scene->device, &sd, &bricks);
     if (r != CAELIX_OK) return r;
-    bricks->light_options.enabled = 0;  // entity bricks do not emit
     bricks->last_frame = scene->last_frame;
     uint32_t slot = 0;
     while (slot < scene->entities.size() && scene->entities[slot].bricks) ++slot;
@@ -467,9 +565,8 @@ CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_
     CAELIX_GUARD_BEGIN
     if (!scene || (count && (!keys || !power))) return CAELIX_ERROR_INVALID_ARGUMENT;
     if (entity != 0) {
-        if (!entity_bricks(scene, entity)) return CAELIX_ERROR_INVALID_ARGUMENT;
-        log(CAELIX_LOG_ERROR, "caelix_scene_set_brick_power: entity %u: entity bricks do not emit", entity);
-        return CAELIX_ERROR_UNSUPPORTED;
+        CaelixScene* bricks = entity_bricks(scene, entity);
+        return bricks ? caelix_scene_set_brick_power(bricks, 0, count, keys, power) : CAELIX_ERROR_INVALID_ARGUMENT;
     }
     for (uint32_t i = 0; i < count; ++i)
         if (!key_ok(keys[i]) || !std::isfinite(power[i]) || power[i] < 0.0f) return CAELIX_ERROR_INVALID_ARGUMENT;

@@ -70,6 +70,13 @@ struct CaelixScene
     cx::GrowBuffer entity_views;  // device EntityView per live entity
     uint32_t entity_view_count = 0;
     bool entity_views_dirty = false;
+    // The entities' light set (SceneView::dyn), rebuilt with the views: its arrays, the dynamic
+    // light tree's buffers and the device copy of its SceneView (null: no entity light).
+    cx::GrowBuffer dyn_arrays;
+    cx::GrowBuffer dyn_tree;
+    cx::GrowBuffer dyn_view;
+    uint32_t dyn_tree_capacity = 0;
+    bool dyn_live = false;
 };
 
 struct CaelixRenderer

@@ -795,7 +795,60 @@ SceneView scene_view(const DeviceScene& s)
     v.group_count = s.group_count;
     v.entities = nullptr;
     v.entity_count = 0;
+    v.dyn = nullptr;
     return v;
+}
+
+namespace {
+
+// One thread per group of the entity (its row, its light block, its frame), then one per light
+// record (its group).
+__global__ void dyn_patch_kernel(uint32_t* __restrict__ heap, uint32_t* __restrict__ rows, GroupFrame* __restrict__ frames,
+                                 uint32_t group_count, uint32_t* __restrict__ light_group, uint32_t light_count,
+                                 const DynPart part)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < group_count) {
+        uint32_t* row = rows + 8ull * (part.group_base + i);
+        if (row[1] != 0u) {
+            row[0] += part.unit_base;
+            uint32_t* block = heap + 4ull * row[0];
+            const uint32_t count = block[0];
+            for (uint32_t e = 0; e < count; ++e) {
+                uint32_t* ie = block + 4 + 4ull * e;
+                ie[1] += part.record_base;
+                ie[3] = 0x80000000u | (part.light_base + (ie[3] & 0x7FFFFFFFu));
+            }
+        }
+        GroupFrame& f = frames[part.group_base + i];
+        for (int k = 0; k < 9; ++k) f.rot[k] = part.rot[k];
+        for (int k = 0; k < 3; ++k) f.trans[k] = part.pos[k];
+    }
+    if (i < light_count) light_group[part.light_base + i] += part.group_base;
+}
+
+}  // namespace
+
+cudaError_t dyn_append(const DeviceScene& e, const DynPart& part, uint32_t* dst_heap, uint32_t* dst_rows,
+                       GroupFrame* dst_frames, float* dst_power, BrickLightRecord* dst_headers, uint32_t* dst_group,
+                       uint32_t* dst_entry, cudaStream_t stream)
+{
+    const cudaMemcpyKind d2d = cudaMemcpyDeviceToDevice;
+    if (e.heap_words) CX_TRY(cudaMemcpyAsync(dst_heap + 4ull * part.unit_base, e.heap, 4ull * e.heap_words, d2d, stream));
+    CX_TRY(cudaMemcpyAsync(dst_rows + 8ull * part.group_base, e.group_rows, 32ull * e.group_count, d2d, stream));
+    CX_TRY(cudaMemcpyAsync(dst_frames + part.group_base, e.frames, sizeof(GroupFrame) * e.group_count, d2d, stream));
+    if (e.brick_count)
+        CX_TRY(cudaMemcpyAsync(dst_power + part.record_base, e.power, 4ull * e.brick_count, d2d, stream));
+    if (e.light_count) {
+        CX_TRY(cudaMemcpyAsync(dst_headers + part.light_base, e.light_headers, sizeof(BrickLightRecord) * e.light_count,
+                               d2d, stream));
+        CX_TRY(cudaMemcpyAsync(dst_group + part.light_base, e.light_group, 4ull * e.light_count, d2d, stream));
+        CX_TRY(cudaMemcpyAsync(dst_entry + part.light_base, e.light_entry, 4ull * e.light_count, d2d, stream));
+    }
+    const uint32_t n = std::max(e.group_count, e.light_count);
+    if (n) dyn_patch_kernel<<<(n + 127) / 128, 128, 0, stream>>>(dst_heap, dst_rows, dst_frames, e.group_count, dst_group,
+                                                             e.light_count, part);
+    return cudaGetLastError();
 }
 
 // The build scratch of a scene of s.brick_count bricks (sized by scene_build_device): 8 arrays of

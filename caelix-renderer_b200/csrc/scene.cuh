@@ -48,6 +48,11 @@ struct SceneView
     // after the world. Their bricks do not emit and hold no light records.
     const EntityView* entities;  // device, entity_count of them
     uint32_t entity_count;
+    // The entities' lights (null: none), a light set of its own in device memory (its heap,
+    // group rows, frames, power and the dynamic light tree; the tree of the reference's dynamic
+    // entities): entity e's groups from its group_base, its light blocks' brick words after the
+    // earlier entities' bricks, every index entry's leaf word 0x80000000 | its leaf in that tree.
+    const SceneView* dyn;
 };
 
 // An entity on the device: its bricks' tables (a scene of their own, entity-local block
@@ -60,11 +65,15 @@ struct EntityView
     SceneView scene;
     float rot[9];
     float pos[3];
+    uint32_t group_base;  // its first group in the entities' light set
 };
 
 // The attribute bit of an entity hit (bits 0..5 face flags, 6..14 cell, 16..31 block: bit 15 is
-// free); the hit's group is then the entity's index and its normal the rotated face normal.
+// free); the hit's group is then entity << 24 | the group in the entity, its normal the rotated
+// face normal and its object_hit the entity-local point.
 constexpr uint32_t kEntityHit = 0x8000u;
+constexpr uint32_t kEntityShift = 24;
+constexpr uint32_t kEntityGroupMask = (1u << kEntityShift) - 1u;
 
 // Host-side owner of the device scene.
 struct DeviceScene
@@ -162,6 +171,19 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
 cudaError_t staging_update(const uint16_t* stage_voxels, const uint32_t* slots, const float* power, uint32_t count,
                            const uint32_t* record_of_slot, DeviceScene& s, uint32_t* marks, uint32_t epoch,
                            uint32_t* list, uint32_t* list_count, cudaStream_t stream);
+// The entities' light set (SceneView::dyn): entity e's light blocks, group rows, frames, power
+// and light records copied after the earlier entities' (dst_*: device arrays sized for all) and
+// their indices moved: group rows by unit_base heap units, the index entries' brick words by
+// record_base, their leaf words to 0x80000000 | (light_base + leaf), the frames set to the
+// entity's transform, the light records' groups by group_base.
+struct DynPart
+{
+    uint32_t group_base, unit_base, record_base, light_base;
+    float rot[9], pos[3];
+};
+cudaError_t dyn_append(const DeviceScene& e, const DynPart& part, uint32_t* dst_heap, uint32_t* dst_rows,
+                       GroupFrame* dst_frames, float* dst_power, BrickLightRecord* dst_headers, uint32_t* dst_group,
+                       uint32_t* dst_entry, cudaStream_t stream);
 // Rebuilds the light tree of a built scene from its light records (asynchronous on `stream`, no
 // allocation: the tree buffers were sized by scene_build). The reference's per-flush light BVH
 // rebuild (lib/src/light/light_tree_record.cpp:230-302, RecordTree).

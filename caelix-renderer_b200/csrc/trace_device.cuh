@@ -335,7 +335,7 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
         if (!he.hit) continue;
         h = he;
         h.attrib |= kEntityHit;
-        h.group = e;
+        h.group = (e << kEntityShift) | he.group;
         const uint32_t f = (uint32_t)(__ffs(he.attrib & 0x3Fu) - 1);
         const float sign = (f & 1u) ? -1.0f : 1.0f;
         float v[3];
@@ -344,6 +344,24 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
         const float inv = 1.0f / sqrtf(dot3(v, v));
 #pragma unroll
         for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
+    }
+}
+
+// The entity-local hit point of an entity hit (the wavefront keeps a hit as four words): the ray
+// in the entity's frame as trace_entities computes it, at t.
+__device__ __forceinline__ void entity_local_hit(const SceneView& s, uint32_t entity, const float o[3], const float d[3],
+                                                 float t, float out[3])
+{
+    const EntityView& E = s.entities[entity];
+    float R[9];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) R[i] = __ldg(&E.rot[i]);
+    const float q[3] = {o[0] - __ldg(&E.pos[0]), o[1] - __ldg(&E.pos[1]), o[2] - __ldg(&E.pos[2])};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float ol = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
+        const float dl = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
+        out[k] = ol + dl * t;
     }
 }
 
@@ -493,7 +511,7 @@ __device__ __forceinline__ void node_slot(const LightBvhNode* nd, uint32_t s, Su
     }
 }
 
-// Tree 0 is the built tree; tree 1 (dynamic entities) is empty.
+// Tree 0 is the world's tree; tree 1 the entities' (none without entity lights).
 __device__ __forceinline__ void tree_summary(const SceneView& s, uint32_t k, Summary& out, uint32_t& root)
 {
 #pragma unroll
@@ -501,16 +519,17 @@ __device__ __forceinline__ void tree_summary(const SceneView& s, uint32_t k, Sum
 #pragma unroll
     for (int q = 0; q < 3; ++q) out.lo[q] = out.hi[q] = 0.0f;
     root = kNone;
-    if (k == 0) {
-        const uint32_t r = __ldg(&s.header->root);
+    const LightTreeHeader* h = k == 0 ? s.header : (s.dyn ? s.dyn->header : nullptr);
+    if (h) {
+        const uint32_t r = __ldg(&h->root);
         if (r != kNone) {
             root = r;
 #pragma unroll
-            for (int f = 0; f < 6; ++f) out.face[f] = __ldg(&s.header->summary.face[f]);
+            for (int f = 0; f < 6; ++f) out.face[f] = __ldg(&h->summary.face[f]);
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                out.lo[q] = __ldg(&s.header->summary.lo[q]);
-                out.hi[q] = __ldg(&s.header->summary.hi[q]);
+                out.lo[q] = __ldg(&h->summary.lo[q]);
+                out.hi[q] = __ldg(&h->summary.hi[q]);
             }
         }
     }
@@ -521,19 +540,26 @@ __device__ __forceinline__ uint32_t child_count(const uint4 c)
     return (c.x != kNone) + (c.y != kNone) + (c.z != kNone) + (c.w != kNone);
 }
 
-// The probability of picking tree 0 (LtTreeProbability). Tree 1 (dynamic entities) is empty:
-// its box and faces are zero, so its importance and power are never positive and it adds nothing
-// to either sum.
-__device__ float tree_probability(const SceneView& s, const float x[3], const float n[3])
+// The probability of picking tree `target` (LtTreeProbability). An empty tree's box and faces
+// are zero, so its importance and power are never positive and it adds nothing to either sum.
+__device__ float tree_probability(const SceneView& s, const float x[3], const float n[3], uint32_t target)
 {
-    Summary sm;
-    uint32_t root;
-    tree_summary(s, 0, sm, root);
-    const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
-    const float pw = power6(sm.face);
-    const float sum_i = imp > 0.0f ? imp : 0.0f;
-    const float sum_p = pw > 0.0f ? pw : 0.0f;
-    return pick_probability(sum_i, sum_p, imp, pw);
+    float sum_i = 0.0f, sum_p = 0.0f, imp_t = 0.0f, pow_t = 0.0f;
+    for (uint32_t k = 0; k < 2; ++k) {
+        Summary sm;
+        uint32_t root;
+        tree_summary(s, k, sm, root);
+        if (root == kNone) continue;  // an empty tree adds zero to both sums
+        const float imp = importance(x, n, sm.lo, sm.hi, sm.face);
+        const float pw = power6(sm.face);
+        sum_i += imp > 0.0f ? imp : 0.0f;
+        sum_p += pw > 0.0f ? pw : 0.0f;
+        if (k == target) {
+            imp_t = imp;
+            pow_t = pw;
+        }
+    }
+    return pick_probability(sum_i, sum_p, imp_t, pow_t);
 }
 
 __device__ float slot_probability(const LightBvhNode* nd, const float x[3], const float n[3], uint32_t slot)
@@ -558,18 +584,21 @@ __device__ float slot_probability(const LightBvhNode* nd, const float x[3], cons
     return pick_probability(sum_i, sum_p, imp_t, pow_t);
 }
 
-__device__ __noinline__ float leaf_probability(const SceneView& s, uint32_t leaf, const float x[3], const float n[3])
+// The probability of drawing leaf `leaf` of tree k (its light set L): the slot picks up to the
+// root, times the pick of tree k.
+__device__ __noinline__ float leaf_probability(const SceneView& s, const SceneView& L, uint32_t leaf, const float x[3],
+                                              const float n[3], uint32_t k)
 {
-    if (__ldg(&s.header->root) == kNone) return 0.0f;
-    const uint32_t parent = __ldg(&s.leaves[leaf].parent);
+    if (__ldg(&L.header->root) == kNone) return 0.0f;
+    const uint32_t parent = __ldg(&L.leaves[leaf].parent);
     if (parent == kNone) return 0.0f;
     uint32_t node = parent >> kParentSlotBits, slot = parent & kParentSlotMask;
     float probability = 1.0f;
     for (uint32_t depth = 0; depth < 64; ++depth) {
-        const LightBvhNode* nd = s.nodes + node;
+        const LightBvhNode* nd = L.nodes + node;
         probability *= slot_probability(nd, x, n, slot);
         const uint2 up = __ldg(reinterpret_cast<const uint2*>(&nd->parent));
-        if (up.x == kNone) return probability * tree_probability(s, x, n);
+        if (up.x == kNone) return probability * tree_probability(s, x, n, k);
         node = up.x;
         slot = up.y;
     }
@@ -627,31 +656,42 @@ struct LightPoint
     uint32_t block;
     uint32_t group;
     uint32_t entry;
+    uint32_t tree;  // 0: the world's light set, 1: the entities' (SceneView::dyn)
 };
 
+// kEntities: the scene may have a second (entity) light tree; without it only tree 0 is
+// evaluated and tree 1's draw is consumed (the same results for a scene without entity lights).
+template <bool kEntities = true>
 __device__ __forceinline__ bool light_sample(const SceneView& s, const float x[3], const float n[3], uint32_t rng, LightPoint& p)
 {
     float pdf_brick = 1.0f;
-    // The tree (one draw per tree; tree 1, dynamic entities, is empty: its importance and power
-    // are never positive, so it only consumes its draw).
-    uint32_t root;
+    // The tree (one draw per tree; an empty tree's importance and power are never positive, so
+    // it only consumes its draw).
+    uint32_t root, k;
     {
         Pick pk = {0, 0, 0, 0, kNone, kNone};
-        Summary sm;
-        tree_summary(s, 0, sm, root);
-        pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), 0, lt_random_float(rng));
-        (void)lt_random_float(rng);
+        uint32_t roots[2] = {kNone, kNone};
+#pragma unroll
+        for (uint32_t t = 0; t < 2; ++t) {
+            Summary sm;
+            if (kEntities || t == 0) tree_summary(s, t, sm, roots[t]);
+            const float u = lt_random_float(rng);
+            if (roots[t] != kNone) pick_add(pk, importance(x, n, sm.lo, sm.hi, sm.face), power6(sm.face), t, u);
+        }
         float prob;
-        const uint32_t k = pick_end(pk, prob);
+        k = pick_end(pk, prob);
         if (k == kNone) return false;
         pdf_brick *= prob;
+        root = roots[k];
     }
+    const SceneView& L = (kEntities && k != 0) ? *s.dyn : s;
+    p.tree = k;
     // Down the 4-wide nodes. Every slot's importance is computed by every lane (empty slots
     // hold zero summaries and are skipped by the pick), so the lanes stay converged.
     uint32_t leaf = kNone;
     uint32_t node = root;
     for (uint32_t depth = 0; depth < 64; ++depth) {
-        const LightBvhNode* nd = s.nodes + node;
+        const LightBvhNode* nd = L.nodes + node;
         const uint4 ch = __ldg(reinterpret_cast<const uint4*>(nd->child));
         uint32_t chosen;
         if (child_count(ch) == 1) {
@@ -677,16 +717,16 @@ __device__ __forceinline__ bool light_sample(const SceneView& s, const float x[3
         node = chosen;
     }
     if (leaf == kNone) return false;
-    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&s.leaves[leaf].group));
+    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&L.leaves[leaf].group));
     const uint32_t group = owner.x, entry = owner.y;
     p.group = group;
     p.entry = entry;
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
+    const uint2 row = __ldg(reinterpret_cast<const uint2*>(L.group_rows + 8ull * group));
     if (row.y == 0) return false;
-    const uint32_t* block = s.heap + 4ull * row.x;
+    const uint32_t* block = L.heap + 4ull * row.x;
     const uint32_t* rec = block + 4ull * __ldg(block + 4 + 4 * entry + 2);
     float w[6];
-    const float sum = family_weights(s, group, rec, x, w);
+    const float sum = family_weights(L, group, rec, x, w);
     if (sum <= 0.0f) return false;
     const float u = lt_random_float(rng) * sum;
     uint32_t f = kNone, last = 0;
@@ -718,11 +758,11 @@ __device__ __forceinline__ bool light_sample(const SceneView& s, const float x[3
     ei = ei > count - 1u ? count - 1u : ei;
     const uint32_t ent = __ldg(rec + 12 + first + ei);
     const uint32_t vi = ent & 0x1FFu;
-    const uint32_t gs = s.group_shift, gm = (1u << gs) - 1u;
+    const uint32_t gs = L.group_shift, gm = (1u << gs) - 1u;
     const uint32_t pos = __ldg(rec + 8);
     const uint32_t voxel[3] = {(pos & gm) * 8 + (vi & 7u), ((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u),
                                ((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)};
-    const GroupFrame* fr = s.frames + group;
+    const GroupFrame* fr = L.frames + group;
     const uint32_t axis = f >> 1;
     const float a = lt_random_float(rng);
     const float b = lt_random_float(rng);
@@ -826,18 +866,20 @@ __device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3
     return true;
 }
 
-__device__ float brick_pdf(const SceneView& s, const float x[3], const float n[3], uint32_t group, uint32_t entry)
+// The draw probability of entry `entry` of group `group` of light set k (L).
+__device__ float brick_pdf(const SceneView& s, const SceneView& L, const float x[3], const float n[3], uint32_t group,
+                           uint32_t entry, uint32_t k)
 {
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
+    const uint2 row = __ldg(reinterpret_cast<const uint2*>(L.group_rows + 8ull * group));
     if (row.y == 0) return 0.0f;
-    const uint32_t* block = s.heap + 4ull * row.x;
+    const uint32_t* block = L.heap + 4ull * row.x;
     if (entry >= __ldg(block)) return 0.0f;
     const uint32_t bvh_leaf = __ldg(block + 4 + 4 * entry + 3);
     if (bvh_leaf == kNone) return 0.0f;
     const uint32_t leaf = bvh_leaf & 0x7FFFFFFFu;
-    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&s.leaves[leaf].group));
+    const uint2 owner = __ldg(reinterpret_cast<const uint2*>(&L.leaves[leaf].group));
     if (owner.x != group || owner.y != entry) return 0.0f;
-    return leaf_probability(s, leaf, x, n);
+    return leaf_probability(s, L, leaf, x, n, k);
 }
 
 // ---- integrator ----
@@ -870,12 +912,13 @@ struct ShadowRay
     uint32_t brick;    // the lamp brick (kNone when its emission is not its power)
 };
 
+template <bool kEntities = true>
 __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng,
                                             ShadowRay& r)
 {
     const uint32_t point_seed = random_u32(light_rng);
     LightPoint p;
-    if (!light_sample(s, x, n, point_seed, p) || !(p.pdf > 0.0f)) return false;
+    if (!light_sample<kEntities>(s, x, n, point_seed, p) || !(p.pdf > 0.0f)) return false;
     const float d[3] = {p.position[0] - x[0], p.position[1] - x[1], p.position[2] - x[2]};
     const float d2 = dot3(d, d);
     const float dist = sqrtf(d2);
@@ -886,9 +929,10 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
     if (!(cos_r > 0.0f) || !(cos_l > 0.0f)) return false;
     float scale = (cos_r * (1.0f / kPi)) * (cos_l / d2) / p.pdf;
     scale *= mis_weight(p.pdf, n, w, dist, cos_l, true);
-    const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * p.group));
-    const uint32_t brick = __ldg(s.heap + 4ull * row.x + 4 + 4 * p.entry + 1);
-    const float e = (p.block & kOpaqueBit) ? __ldg(s.power + brick) : 0.0f;
+    const SceneView& L = (kEntities && p.tree != 0) ? *s.dyn : s;
+    const uint2 row = __ldg(reinterpret_cast<const uint2*>(L.group_rows + 8ull * p.group));
+    const uint32_t brick = __ldg(L.heap + 4ull * row.x + 4 + 4 * p.entry + 1);
+    const float e = (p.block & kOpaqueBit) ? __ldg(L.power + brick) : 0.0f;
     const float contribution = e * scale;  // equal on the three channels
     const float lum = contribution * 0.2126f + contribution * 0.7152f + contribution * 0.0722f;
     const float w_lamp = lum * hmax(0.05f, 1.0f);
@@ -903,36 +947,53 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
     const float k = w_sum / w_lamp;
     r.value = contribution * k;
     r.dvalue_de = scale * k;
-    r.brick = (p.block & kOpaqueBit) ? brick : kNone;
+    r.brick = ((p.block & kOpaqueBit) && (!kEntities || p.tree == 0)) ? brick : kNone;  // a world brick's power
     return true;
 }
 
 __device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segment_light, const Hit& h, const float origin[3],
                                  const float dir[3], const float seg_n[3])
 {
-    if (segment_light == 0u || h.t < kNearField || (h.attrib & kEntityHit)) return 1.0f;
-    const GroupFrame* fr = s.frames + h.group;
+    if (segment_light == 0u || h.t < kNearField) return 1.0f;
+    // The light set of the hit: the world's, or for an entity hit the entities' (its groups from
+    // the entity's group base; the voxel from the entity-local hit point and face normal).
+    const uint32_t face = (uint32_t)(__ffs(h.attrib & 0x3Fu) - 1);
+    const bool entity = (h.attrib & kEntityHit) != 0;
+    if (entity && !s.dyn) return 1.0f;
+    const SceneView& L = entity ? *s.dyn : s;
+    const uint32_t group = entity ? __ldg(&s.entities[h.group >> kEntityShift].group_base) + (h.group & kEntityGroupMask)
+                                  : h.group;
+    float nl[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) nl[k] = entity ? ((uint32_t)k == (face >> 1) ? ((face & 1u) ? -1.0f : 1.0f) : 0.0f)
+                                               : h.normal[k];
+    const GroupFrame* fr = L.frames + group;
     uint32_t vig[3];
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
-        const int32_t voxel = (int32_t)floorf(h.object_hit[k] - 0.25f * h.normal[k]);
+        const int32_t voxel = (int32_t)floorf(h.object_hit[k] - 0.25f * nl[k]);
         vig[k] = (uint32_t)(voxel - (int32_t)__ldg(&fr->origin[k]));
     }
-    const uint32_t face = (uint32_t)(__ffs(h.attrib & 0x3Fu) - 1);
     const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
     uint32_t entry, leaf;
     float in_brick;
-    if (!find_light_face(s, origin, h.group, vig, face, block, entry, leaf, in_brick) || leaf == kNone) return 1.0f;
+    if (!find_light_face(L, origin, group, vig, face, block, entry, leaf, in_brick) || leaf == kNone) return 1.0f;
     const float cos_l = -dot3(h.normal, dir);
-    const float p_area = brick_pdf(s, origin, seg_n, h.group, entry) * in_brick;
+    const float p_area = brick_pdf(s, L, origin, seg_n, group, entry, entity ? 1u : 0u) * in_brick;
     return mis_weight(p_area, seg_n, dir, h.t, cos_l, false);
 }
 
+template <bool kEntities = true>
 __device__ __forceinline__ void shade(const SceneView& s, const Hit& h, const float ray_o[3], const float ray_d[3],
                                       uint32_t& rng, float albedo[3], float& emission, float origin[3], float dir[3])
 {
     const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-    emission = ((block & kOpaqueBit) && !(h.attrib & kEntityHit)) ? __ldg(s.power + h.record) : 0.0f;  // entities do not emit
+    if (kEntities && (h.attrib & kEntityHit)) {  // an entity brick's power
+        const float* pw = s.entities[h.group >> kEntityShift].scene.power;
+        emission = ((block & kOpaqueBit) && pw) ? __ldg(pw + h.record) : 0.0f;
+    } else {
+        emission = (block & kOpaqueBit) ? __ldg(s.power + h.record) : 0.0f;
+    }
     const float* a = s.albedo + 3 * (block & (kMaterialSlots - 1));
     albedo[0] = __ldg(a);
     albedo[1] = __ldg(a + 1);

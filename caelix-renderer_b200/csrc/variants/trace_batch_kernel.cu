@@ -216,7 +216,7 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
             light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
         }
         float al[3], em, o2[3], d2[3];
-        shade(S, h, org, dir, rng, al, em, o2, d2);
+        shade<false>(S, h, org, dir, rng, al, em, o2, d2);  // batched scenes have no entities
         bool nee_now;
         if (primary) {
             e0 = em;
@@ -250,7 +250,7 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
         if (nee_now) {
             segment_light = 3u;
             ShadowRay r;
-            shadow = nee_prepare(S, o2, h.normal, light_rng, r);
+            shadow = nee_prepare<false>(S, o2, h.normal, light_rng, r);
             if (shadow) {
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {

@@ -169,7 +169,9 @@ __device__ __forceinline__ float gsum3(const float G[3], const float t[3], float
 // stay in L2, 8 (64 registers) where the descent and the record loads go to HBM and more warps
 // in flight hide them (measured: 5 is the fastest of 3 .. 8 on the 128^3 world; 8 on the
 // 2 M-brick world and the 64-scene batch).
-template <int kMode, int kMinBlocks>
+// kEntities: the views' scenes have entities (their hits, their lights); the variant without
+// them keeps the world-only shading's registers.
+template <int kMode, int kMinBlocks, bool kEntities>
 __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity, const WaveAdjoint adj)
 {
@@ -252,9 +254,14 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                     h.normal[0] = fc == 0 ? 1.0f : (fc == 1 ? -1.0f : 0.0f);
                     h.normal[1] = fc == 2 ? 1.0f : (fc == 3 ? -1.0f : 0.0f);
                     h.normal[2] = fc == 4 ? 1.0f : (fc == 5 ? -1.0f : 0.0f);
-                    if (h.attrib & kEntityHit) entity_normal(S, h.group, h.attrib, h.normal);
 #pragma unroll
                     for (int k = 0; k < 3; ++k) h.object_hit[k] = org[k] + dir[k] * h.t;
+                    if constexpr (kEntities) {
+                        if (h.attrib & kEntityHit) {
+                            entity_normal(S, h.group >> kEntityShift, h.attrib, h.normal);
+                            entity_local_hit(S, h.group >> kEntityShift, org, dir, h.t, h.object_hit);
+                        }
+                    }
                     const uint32_t px = item % P.width, py = item / P.width;
                     const uint32_t seed = P.frame_seed + sp;
                     uint32_t rng, light_rng;
@@ -268,7 +275,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                     float tp[3], seg_n[3];
                     uint32_t bounce_index, seg_light;
                     float al[3], em, o2[3], d2[3];
-                    shade(S, h, org, dir, rng, al, em, o2, d2);
+                    shade<kEntities>(S, h, org, dir, rng, al, em, o2, d2);
                     bool nee_now;
                     if (primary) {
                         e0 = em;
@@ -339,7 +346,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                     float sadd[3] = {0.0f, 0.0f, 0.0f};
                     if (nee_now) {
                         seg_light = 3u;
-                        shadow = nee_prepare(S, o2, h.normal, light_rng, r);
+                        shadow = nee_prepare<kEntities>(S, o2, h.normal, light_rng, r);
                         // Added to the radiance when unoccluded as nee * throughput (this vertex's
                         // throughput, before Russian roulette rescales it).
                         if (shadow) {
@@ -519,15 +526,18 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
                      uint32_t* launches, bool entities = false)
 {
     if (b.capacity == 0) return cudaErrorInvalidValue;
-    static int trace_blocks[2] = {0, 0}, shade_blocks = 0;
+    static int trace_blocks[2] = {0, 0}, shade_blocks[2] = {0, 0};
     if (trace_blocks[0] == 0) {
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[0], wave_trace_kernel<false>, kWaveThreads, 0));
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[1], wave_trace_kernel<true>, kWaveThreads, 0));
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks, wave_shade_kernel<kMode, kMinBlocks>,
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks[0], wave_shade_kernel<kMode, kMinBlocks, false>,
                                                              kWaveThreads, 0));
-        trace_blocks[0] = std::max(trace_blocks[0], 1);
-        trace_blocks[1] = std::max(trace_blocks[1], 1);
-        shade_blocks = std::max(shade_blocks, 1);
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks[1], wave_shade_kernel<kMode, kMinBlocks, true>,
+                                                             kWaveThreads, 0));
+        for (int k = 0; k < 2; ++k) {
+            trace_blocks[k] = std::max(trace_blocks[k], 1);
+            shade_blocks[k] = std::max(shade_blocks[k], 1);
+        }
     }
     uint32_t count = 0;
     for (size_t s = 0; s < plan.items.size(); ++s) {
@@ -546,12 +556,15 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
             const uint32_t ray_grid = std::min<uint32_t>((2 * n + kWaveThreads - 1) / kWaveThreads,
                                                          sm_count * (uint32_t)trace_blocks[entities ? 1 : 0]);
             const uint32_t shade_grid = std::min<uint32_t>((n + kWaveThreads - 1) / kWaveThreads,
-                                                           sm_count * (uint32_t)shade_blocks);
+                                                           sm_count * (uint32_t)shade_blocks[entities ? 1 : 0]);
             for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
                 const uint32_t parity = it & 1u;
                 if (entities) wave_trace_kernel<true><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
                 else wave_trace_kernel<false><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
-                wave_shade_kernel<kMode, kMinBlocks><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
+                if (entities)
+                    wave_shade_kernel<kMode, kMinBlocks, true><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
+                else
+                    wave_shade_kernel<kMode, kMinBlocks, false><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
                 count += 2;
             }
             CX_TRY(cudaGetLastError());

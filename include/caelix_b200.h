@@ -276,9 +276,13 @@ typedef struct CaelixEntityDesc
 
 /* Adds an entity with no bricks: world = R(rotation) * local + position, local = the
    entity-local block coordinate. Its bricks are traced (closest hit over the world and every
-   entity, ties to the world and then to the lower id) and shaded with the scene's materials; they
-   do not emit and hold no light records (the light tree stays the world's: the reference's second,
-   dynamic light tree is not built). Takes effect at the next flush. */
+   entity, ties to the world and then to the lower id) and shaded with the scene's materials. Its
+   emitting bricks (caelix_scene_set_brick_power with its id) are lights of the second light tree
+   (the reference's dynamic tree, docs/LIGHT_TREE.md:136-176): the entities' light records merged
+   in id order under their transforms, rebuilt at a flush after any entity change or move, while
+   the world's tree (tree 0) stays; NEE picks between the two trees by importance. Every added
+   entity's lights go to that tree whatever its motion (the reference puts static entities' lights
+   in tree 0). Takes effect at the next flush. */
 CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const CaelixEntityDesc* desc,
                                                 CaelixEntityId* out_id);
 /* Removes the entity and all its bricks at once (waiting for the device first). */
@@ -287,9 +291,10 @@ CAELIX_API CaelixResult caelix_scene_remove_entity(CaelixScene* scene, CaelixEnt
    the normalised quaternion and rounded to float. */
 CAELIX_API CaelixResult caelix_scene_set_entity_transform(CaelixScene* scene, CaelixEntityId entity,
                                                           const float position[3], const float rotation[4]);
-/* Entity motion (the reference uses it only to pick the light tree of an entity's lights; entity
-   lights are not built here, so the value is stored and has no effect). Other values than
-   CAELIX_ENTITY_STATIC / CAELIX_ENTITY_DYNAMIC return CAELIX_ERROR_INVALID_ARGUMENT. */
+/* Entity motion (the reference uses it only to pick the light tree of an entity's lights; here
+   every added entity's lights are in the dynamic tree, so the value is stored and has no effect).
+   Other values than CAELIX_ENTITY_STATIC / CAELIX_ENTITY_DYNAMIC return
+   CAELIX_ERROR_INVALID_ARGUMENT. */
 #define CAELIX_ENTITY_STATIC 0u
 #define CAELIX_ENTITY_DYNAMIC 1u
 CAELIX_API CaelixResult caelix_scene_set_entity_motion(CaelixScene* scene, CaelixEntityId entity, uint32_t motion);
@@ -320,8 +325,8 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
    brick with power P > 0 emits radiance (P, P, P) and is a light voxel of the light tree (the
    reference derives light voxels from emissive material codes, include/caelix/caelix.h:600-630;
    the benchmark scenes give each emissive brick its own power). Keys without an uploaded brick are
-   kept and apply when it arrives. entity 0 only: an added entity's bricks do not emit
-   (CAELIX_ERROR_UNSUPPORTED). */
+   kept and apply when it arrives. entity: 0 (the world's lights) or an added entity (the
+   entities' light tree). */
 CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                      const CaelixBrickKey* keys, const float* power);
 

@@ -1,8 +1,9 @@
 """Entities through the C ABI against the oracle: a world with two entities (one rotated, one
 translated), rendered with the wavefront and the per-frame kernels; then an entity moved, an
-entity's bricks edited, an entity removed and a new one added in its id. Every state's radiance and
-ray counts equal the oracle's with the same entities (bit-exact expected; the 1e-5 relative bound
-of the trace parity tests)."""
+entity's bricks edited, an entity removed and a new one added in its id, then entity lights (the
+second light tree) and a lit entity moved. Every state's radiance and ray counts equal the
+oracle's with the same entities (bit-exact expected; the 1e-5 relative bound of the trace parity
+tests)."""
 import numpy as np
 import pytest
 
@@ -93,10 +94,28 @@ def test_entities_parity(cuda_device, oracle):
     osc.set_entities([(o1, IDENTITY, p1), (o2, IDENTITY, p2)])
     render_pair(cuda_device, scene, osc, vs)
 
-    # Entity bricks do not emit; entity 0 cannot be moved or removed; motion takes two values.
-    with pytest.raises(caelix_b200.CaelixError) as err:
-        scene.set_brick_power(b1.keys[:1], np.ones(1, np.float32), entity=e3)
-    assert err.value.code == caelix_b200.CAELIX_ERROR_UNSUPPORTED
+    # Entity lights: some bricks of both entities emit (the second light tree), then one moves.
+    rng = np.random.default_rng(4)
+    p_1 = np.where(rng.random(b1.brick_count) < 0.5, rng.lognormal(0.0, 1.0, b1.brick_count), 0.0).astype(np.float32)
+    p_2 = np.where(rng.random(b2.brick_count) < 0.5, rng.lognormal(0.0, 1.0, b2.brick_count), 0.0).astype(np.float32)
+    scene.set_brick_power(b1.keys, p_1, entity=e3)
+    scene.set_brick_power(b2.keys, p_2, entity=e2)
+    scene.flush()
+    l1 = oracle_lib.OracleScene(oracle, workloads.VoxelScene(b1.grid, b1.keys, b1.voxels, p_1, b1.albedo, b1.camera,
+                                                             b1.group_shift))
+    l2 = oracle_lib.OracleScene(oracle, workloads.VoxelScene(b2.grid, b2.keys, vox2, p_2, b2.albedo, b2.camera,
+                                                             b2.group_shift))
+    osc.set_entities([(l1, IDENTITY, p1), (l2, IDENTITY, p2)])
+    assert osc.s.dyn
+    lit = render_pair(cuda_device, scene, osc, vs)
+    render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
+    scene.set_entity_transform(e3, p1, Q1)
+    scene.flush()
+    osc.set_entities([(l1, Q1, p1), (l2, IDENTITY, p2)])
+    moved = render_pair(cuda_device, scene, osc, vs)
+    assert not np.array_equal(lit, moved)
+
+    # Entity 0 cannot be moved or removed; motion takes two values.
     with pytest.raises(caelix_b200.CaelixError):
         scene.remove_entity(0)
     with pytest.raises(caelix_b200.CaelixError):
