@@ -45,7 +45,7 @@ struct SceneView
     uint32_t light_count;
     uint32_t group_count;
     // Entities beside the scene's own bricks (the static world): each traversed in its frame
-    // after the world. Their bricks do not emit and hold no light records.
+    // after the world; their lights are the light set `dyn`.
     const EntityView* entities;  // device, entity_count of them
     uint32_t entity_count;
     // The entities' lights (null: none), a light set of its own in device memory (its heap,

@@ -12,8 +12,8 @@
 //                      caelix_light_nee.hlsl:20-34, caelix_shading.hlsl:267-307,
 //                      caelix_random.hlsl, common/caelix_frame.hlsl:164-171
 // in the configuration of the benchmark scenes: opaque voxels with a Lambertian lobe (metallic 0,
-// smoothness 0), light-tree NEE with MIS, no sun, black sky, no fog, identity entity transform,
-// bounce NEE probability 1. Emission of an opaque voxel = its brick's emitter power on every
+// smoothness 0), light-tree NEE with MIS over the world's and the entities' light trees, no sun,
+// black sky, no fog, bounce NEE probability 1. Emission of an opaque voxel = its brick's emitter power on every
 // channel. Every float operation is one IEEE fp32 operation in the reference's order (the library
 // is built with --fmad=false); sin/cos of the unit-vector draw use this library's Cody-Waite +
 // Taylor polynomials, normalize is v * (1 / sqrt(dot(v, v))).

@@ -158,7 +158,7 @@ typedef struct oc_scene {
     uint32_t* group_rows;  /* [group_count][8] GroupLightRow */
     oc_frame* group_frames;
     /* Entities beside this scene's bricks (the static world, entity 0): rays also traverse each
-     * entity's own scene under its transform. Entity bricks do not emit and hold no light records. */
+     * entity's own scene under its transform; their lights are the light set `dyn`. */
     const struct oc_entity* entities;
     uint32_t entity_count;
     uint32_t pad2;

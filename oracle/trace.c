@@ -14,7 +14,8 @@
  *                      smoothness 0), caelix_random.hlsl (PcgHash, InitRandom, xorshift32,
  *                      RandomUnitVector), common/caelix_frame.hlsl:164-171 (camera ray)
  * in the benchmark scenes' configuration: opaque voxels, light-tree NEE with MIS, no sun, black
- * sky, no fog, one entity with the identity transform, bounce NEE probability 1.
+ * sky, no fog, bounce NEE probability 1; entities under rigid transforms, their lights in the
+ * second light tree (the reference's dynamic tree).
  *
  * Arithmetic: IEEE fp32, no contraction, HLSL operation order. Two definitions are this
  * project's: sin/cos of RandomUnitVector (Cody-Waite reduction by pi/2 and Taylor polynomials to
