@@ -171,8 +171,9 @@ typedef struct oc_scene {
     const float* dyn_power;
 } oc_scene;
 
-/* An entity: its bricks (a scene of their own, entity-local block coordinates from 0, built with
- * every power 0) and its object-to-world transform, world = rot * local + pos (rot row-major). */
+/* An entity: its bricks (a scene of their own, entity-local block coordinates from 0, with its
+ * bricks' power and light records) and its object-to-world transform, world = rot * local + pos
+ * (rot row-major). */
 typedef struct oc_entity {
     const oc_scene* scene;
     float rot[9];
