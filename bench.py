@@ -549,6 +549,65 @@ def measure_trace(args, world, local, dev, stream, flush):
     return result
 
 
+def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64)):
+    """The cost of entities on the plain trace: the 128^3 world with `n` entities of 2 x 2 x 2
+    bricks each (value noise, half of their bricks emitting: the second light tree), at seeded
+    positions inside the world and rotations, the same 512 x 512, 1 spp, 4 bounces frame. The
+    entities are traversed one after another after the world's bricks (the reference traverses
+    its TLAS), so the cost grows with their count. One flush per count (entity bricks, views,
+    their light tree), then frames timed with CUDA events."""
+    import numpy as np
+    import torch
+
+    import caelix_b200
+    from caelix_b200 import workloads
+
+    sptr = stream.cuda_stream
+    vs = workloads.noise_world()
+    out = torch.zeros(TRACE_W * TRACE_H * 3, dtype=torch.float32, device="cuda")
+    rng = np.random.default_rng(17)
+    result = {"workload": "128^3 world + n entities of 2x2x2 bricks (half emitting), 512x512, 1 spp, 4 bounces",
+              "runs": []}
+    for n in counts:
+        scene = caelix_b200.Scene.from_voxel_scene(dev, vs)
+        for i in range(n):
+            ent = workloads.noise_world(grid_bricks=(2, 2, 2), brick_occupancy=1.0, voxel_fill=0.5,
+                                        emissive_fraction=0.0, seed=100 + i)
+            q = rng.normal(size=4)
+            e = scene.add_entity(tuple(rng.uniform(8.0, 112.0, 3)), tuple(q / np.linalg.norm(q)))
+            scene.upload_bricks(ent.keys, ent.voxels, entity=e)
+            power = np.where(rng.random(ent.brick_count) < 0.5, rng.lognormal(0.0, 1.0, ent.brick_count), 0.0)
+            scene.set_brick_power(ent.keys, power.astype(np.float32), entity=e)
+        t0 = time.perf_counter()
+        scene.flush(sptr)
+        flush_s = time.perf_counter() - t0
+        renderer = caelix_b200.Renderer(dev, scene)
+        with torch.cuda.stream(stream):
+            for k in range(max(args.warmup, 1)):
+                renderer.render(out, TRACE_W, TRACE_H, vs.camera, bounces=TRACE_BOUNCES, seed=1000 + k, spp=1,
+                                stream=sptr)
+        stream.synchronize()
+        steps = max(1, min(args.steps, 5))
+        total_ms, rays = 0.0, 0
+        for k in range(steps):
+            with torch.cuda.stream(stream):
+                flush.zero_()
+                a = torch.cuda.Event(enable_timing=True)
+                b = torch.cuda.Event(enable_timing=True)
+                a.record(stream)
+                renderer.render(out, TRACE_W, TRACE_H, vs.camera, bounces=TRACE_BOUNCES, seed=1 + k, spp=1, stream=sptr)
+                b.record(stream)
+            st = renderer.stats()
+            rays += st.primary_rays + st.bounce_rays + st.shadow_rays
+            total_ms += a.elapsed_time(b)
+        ms = max_over_ranks(total_ms, world) / steps
+        result["runs"].append({"entities": n, "ms_per_frame": ms, "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6,
+                               "flush_wall_s": flush_s})
+        renderer.close()
+        scene.close()
+    return result
+
+
 def measure_large(args, world, local, dev, stream, flush):
     """The large scene: 2048 x 2048 x 512 voxels (256 x 256 x 64 bricks), ~2M occupied bricks (12 %
     voxel occupancy overall), ~100k emissive bricks; the flush (records, hash table, light records,
@@ -1033,6 +1092,8 @@ def run_ours(args, world, rank, local):
             line["large"] = measure_large(args, world, local, dev, stream, flush)
         if args.adjoint:
             line["adjoint"] = measure_adjoint(args, world, local, dev, stream, flush, rank)
+        if args.entities:
+            line["entities"] = measure_entities(args, world, local, dev, stream, flush)
         if args.batch:
             line["batch"] = measure_batch(args, world, local, dev, stream)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -1063,6 +1124,8 @@ def main():
     ap.add_argument("--batch-scenes", type=int, default=64)
     ap.add_argument("--adjoint", action=argparse.BooleanOptionalAction, default=True,
                     help="add the differentiation section (forward vs backward time)")
+    ap.add_argument("--entities", action=argparse.BooleanOptionalAction, default=True,
+                    help="add the entities section (the trace with 4, 16 and 64 lit entities)")
     ap.add_argument("--tune-cache", default=TUNE_CACHE, help="the autotuner's JSON cache (read, and written on a miss)")
     ap.add_argument("--tuning", default="", help="fixed batch tuning instead of the autotuner, e.g. "
                     "min_blocks=8,block_width=8,refill_min=4")

@@ -159,6 +159,20 @@ CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
         std::memcpy(v.rot, e.rot, sizeof(v.rot));
         std::memcpy(v.pos, e.position, sizeof(v.pos));
         v.group_base = 0;
+        // The sphere round the entity's brick grid [0, 8 grid) in world space (double, inflated).
+        {
+            double c[3], r2 = 0.0;
+            for (int a = 0; a < 3; ++a) {
+                const double h = 4.0 * e.bricks->dev.grid[a];
+                r2 += h * h;
+            }
+            for (int i = 0; i < 3; ++i) {
+                c[i] = e.position[i];
+                for (int j = 0; j < 3; ++j) c[i] += (double)e.rot[3 * i + j] * 4.0 * e.bricks->dev.grid[j];
+                v.sphere[i] = (float)c[i];
+            }
+            v.sphere[3] = (float)(std::sqrt(r2) * 1.001 + 0.01);
+        }
         views.push_back(v);
         live.push_back(&e);
         e.generation = e.bricks->generation;

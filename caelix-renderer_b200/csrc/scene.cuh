@@ -66,6 +66,7 @@ struct EntityView
     float rot[9];
     float pos[3];
     uint32_t group_base;  // its first group in the entities' light set
+    float sphere[4];      // world centre and radius of a sphere holding its brick grid (inflated)
 };
 
 // The attribute bit of an entity hit (bits 0..5 face flags, 6..14 cell, 16..31 block: bit 15 is

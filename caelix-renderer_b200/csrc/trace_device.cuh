@@ -322,6 +322,20 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
 {
     for (uint32_t e = 0; e < s.entity_count; ++e) {
         const EntityView& E = s.entities[e];
+        // A ray that misses the entity's bounding sphere, or meets it only behind its origin or
+        // beyond the current hit, cannot hit it (the margins cover the rounding: the test only
+        // skips work, it never changes a hit).
+        {
+            const float4 sp = make_float4(__ldg(&E.sphere[0]), __ldg(&E.sphere[1]), __ldg(&E.sphere[2]),
+                                          __ldg(&E.sphere[3]));
+            const float oc[3] = {sp.x - o[0], sp.y - o[1], sp.z - o[2]};
+            const float oc2 = dot3(oc, oc);
+            const float tc = dot3(oc, d);
+            const float t_far = h.hit ? h.t : tmax_ray;
+            if (oc2 - tc * tc > sp.w * sp.w + 1e-5f * (oc2 + 1.0f)) continue;
+            if (tc + sp.w < tmin_ray - 1e-3f * (1.0f + fabsf(tc))) continue;
+            if (tc - sp.w > t_far + 1e-3f * (1.0f + fabsf(tc))) continue;
+        }
         float R[9], ol[3], dl[3];
 #pragma unroll
         for (int i = 0; i < 9; ++i) R[i] = __ldg(&E.rot[i]);
