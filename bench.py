@@ -57,7 +57,7 @@ TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record secto
 # pass at 4,194,304 pairs, scaled per pair; the wavefront frame of the 512 x 512 trace (trace and
 # shade kernels of its 5 bounce iterations).
 SORT_PASS_DRAM_BYTES_PER_PAIR = 34.5e6 / 4194304
-TRACE_FRAME_DRAM_BYTES = 154.3e6
+TRACE_FRAME_DRAM_BYTES = 134.7e6
 
 
 def measured_peaks():
