@@ -260,8 +260,8 @@ int oc_light_sample(const oc_scene* s, const oc_light_tree* t, const float x[3],
                     float out[7], uint32_t words[6]);
 /* count draws of oc_light_sample at one receiver (the reference probe's draw mode,
  * tests/light_tree_test.cpp:961 CheckHistogram): per draw out[4 i ..] = group, voxel in group
- * (x | y << 10 | z << 20), face, 1 (all zero for a failed draw). The draws' generator states come
- * from an xorshift sequence started at seed. */
+ * (x | y << 10 | z << 20), face, 1 | tree << 1 (all zero for a failed draw; tree 1: a group of
+ * s->dyn). The draws' generator states come from an xorshift sequence started at seed. */
 void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3], const float n[3], uint32_t seed,
                     uint32_t count, uint32_t* out);
 /* The balance-heuristic MIS weight of one side (caelix_light_nee.hlsl:20-34): p_area is the

@@ -687,7 +687,7 @@ void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3],
         o[1] = ((pos & gm) * 8 + (vi & 7u)) | ((((pos >> gs) & gm) * 8 + ((vi >> 3) & 7u)) << 10) |
                ((((pos >> (2 * gs)) & gm) * 8 + (vi >> 6)) << 20);
         o[2] = words[2];
-        o[3] = 1;
+        o[3] = 1u | (words[5] << 1);
     }
 }
 

@@ -258,3 +258,36 @@ def test_entity_lamps_unbiased(oracle):
     assert ref_mean > 0.01
     assert 0.97 < test_mean / ref_mean < 1.03, (ref_mean, test_mean)
     assert psnr > 30.0, psnr
+
+
+def test_draw_histogram_over_both_trees(lit_scene, world):
+    """2^21 draws at one receiver land on the light faces of both trees in proportion to their pdf
+    (5 sigma for faces with at least 50 expected draws; no draw on a face of pdf 0), the
+    reference's CheckHistogram over its two trees."""
+    w = lit_scene
+    faces = [(0, f) for f in light_faces(w.heap, w.group_rows, w.s.group_shift)] + \
+            [(1, f) for f in light_faces(w.dyn_heap, w.dyn_rows, w.s.group_shift)]
+    key = {}
+    for i, (tree, (g, v, f, blk)) in enumerate(faces):
+        key[(tree, g, int(v[0]) | (int(v[1]) << 10) | (int(v[2]) << 20), f)] = i
+    x = (np.array(world.grid, np.float32) * 8 * np.float32(0.5)).astype(np.float32)
+    n = np.zeros(3, np.float32)
+    pdfs = np.array([w.lib.oc_light_point_pdf_tree(C.byref(w.s), C.byref(w.lt), x.ctypes.data, n.ctypes.data, tree, g,
+                                                   np.ascontiguousarray(v).ctypes.data, f, blk)
+                     for tree, (g, v, f, blk) in faces], np.float64)
+    draws = 1 << 21
+    out = np.zeros((draws, 4), np.uint32)
+    w.lib.oc_light_draws(C.byref(w.s), C.byref(w.lt), x.ctypes.data, n.ctypes.data, 555, draws, out.ctypes.data)
+    assert np.all(out[:, 3] & 1)
+    rows, per = np.unique(np.column_stack([out[:, 3] >> 1, out[:, :3]]), axis=0, return_counts=True)
+    counts = np.zeros(len(faces), np.int64)
+    for r, c in zip(rows, per):
+        i = key.get((int(r[0]), int(r[1]), int(r[2]), int(r[3])))
+        assert i is not None, r
+        counts[i] += c
+    expected = pdfs * draws
+    assert np.all(counts[pdfs == 0.0] == 0)
+    big = expected >= 50.0
+    in_dyn = np.array([t == 1 for t, _ in faces])
+    assert big[in_dyn].sum() > 0 and big[~in_dyn].sum() > 0
+    assert np.all(np.abs(counts[big] - expected[big]) <= 5.0 * np.sqrt(expected[big]))
