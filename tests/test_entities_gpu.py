@@ -115,6 +115,16 @@ def test_entities_parity(cuda_device, oracle):
     moved = render_pair(cuda_device, scene, osc, vs)
     assert not np.array_equal(lit, moved)
 
+    # A batch takes no scene with entities.
+    import torch
+
+    r = caelix_b200.Renderer(cuda_device, scene)
+    out = torch.zeros(32 * 32 * 3, dtype=torch.float32, device="cuda")
+    with pytest.raises(caelix_b200.CaelixError) as err:
+        caelix_b200.Batch(cuda_device, [(r, out, 32, 32, vs.camera, 2, 1, 1)], rebuild_light_trees=True)
+    assert err.value.code == caelix_b200.CAELIX_ERROR_UNSUPPORTED
+    r.close()
+
     # Entity 0 cannot be moved or removed; motion takes two values.
     with pytest.raises(caelix_b200.CaelixError):
         scene.remove_entity(0)
