@@ -187,17 +187,31 @@ def base_line(args, world, metric, value, unit, ms_per_step, config, higher=True
 TRACE_METRIC = "trace throughput, Mrays/s (primary + bounce + shadow rays counted on the device)"
 BATCH_METRIC = "batched trace throughput, Mrays/s (light-tree rebuild + trace of every scene per step)"
 FLUSH_METRIC = "incremental scene flush time after a 1% edit (ms)"
-TRACE_CONFIG = {
-    "workload": "plain brick-DDA trace: 128^3-voxel world (16^3 bricks, 30% occupied, value noise seed 2), "
-                "512x512 pinhole, 1 spp, 4 bounces, light-tree NEE with MIS, fp32 radiance",
-    "bricks": 1229,
-    "emissive_bricks": 12,
-    "width": TRACE_W,
-    "height": TRACE_H,
-    "spp": 1,
-    "bounces": TRACE_BOUNCES,
-    "l2": "flushed between timed steps (256 MiB write)",
-}
+def trace_config(world: int) -> dict:
+    """The headline workload's config, the same in both arms."""
+    return {
+        "workload": "plain brick-DDA trace: 128^3-voxel world (16^3 bricks, 30% occupied, value noise seed 2), "
+                    "512x512 pinhole, 1 spp, 4 bounces, light-tree NEE with MIS, fp32 radiance",
+        "bricks": 1229,
+        "emissive_bricks": 12,
+        "width": TRACE_W,
+        "height": TRACE_H,
+        "spp": 1,
+        "bounces": TRACE_BOUNCES,
+        "l2": "flushed between timed steps (256 MiB write)",
+        "parallelism": f"replicas x{world}",
+    }
+
+
+def compact(obj, digits: int = 4):
+    """Floats rounded to `digits` significant digits (the detail sections of the line stay short)."""
+    if isinstance(obj, float):
+        return float(f"{obj:.{digits}g}")
+    if isinstance(obj, dict):
+        return {k: compact(v, digits) for k, v in obj.items()}
+    if isinstance(obj, list):
+        return [compact(v, digits) for v in obj]
+    return obj
 
 # ---------------------------------------------------------------------------------------------
 # CPU baseline / reference arm: the oracle (the reference's shader logic restated in C; the
@@ -337,7 +351,8 @@ def run_reference(args, world, rank):
             secs += s
             frames += f
         value = rays / secs / 1e6
-        line = base_line(args, args.gpus, TRACE_METRIC, value, "Mrays/s", 1e3 * secs / frames, TRACE_CONFIG)
+        line = base_line(args, args.gpus, TRACE_METRIC, value, "Mrays/s", 1e3 * secs / frames,
+                         trace_config(args.gpus))
         sample = f"{frames} oracle renders of the whole 512x512 frame on {threads} threads (~2 s per step)"
     line["impl"] = "reference"
     line["cpu_baseline"] = {"value": value, "unit": line["unit"], "cores": threads, "kind": "port", "sample": sample}
@@ -1081,26 +1096,33 @@ def run_ours(args, world, rank, local):
                                     "sample": f"{builds} oracle builds of 1048576 records, 1 thread, {wall:.1f} s"}
     else:
         trace = measure_trace(args, world, local, dev, stream, flush)
-        config = dict(TRACE_CONFIG)
-        config["parallelism"] = f"replicas x{world}"
-        line = base_line(args, world, TRACE_METRIC, trace["value"], "Mrays/s", trace["ms_per_step"], config)
+        line = base_line(args, world, TRACE_METRIC, trace["value"], "Mrays/s", trace["ms_per_step"],
+                         trace_config(world))
         line.update({k: trace[k] for k in ("roofline", "e2e", "gpu_launches", "clocks", "rays_per_step")})
-        if build is not None:
-            line["build"] = {k: build[k] for k in ("workload", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
-                                                   "roofline", "roofline_build", "e2e")}
-        if args.large:
-            line["large"] = measure_large(args, world, local, dev, stream, flush)
-        if args.adjoint:
-            line["adjoint"] = measure_adjoint(args, world, local, dev, stream, flush, rank)
-        if args.entities:
-            line["entities"] = measure_entities(args, world, local, dev, stream, flush)
-        if args.batch:
-            line["batch"] = measure_batch(args, world, local, dev, stream)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             rays, secs, frames = oracle_trace(10.0, 1)
             line["cpu_baseline"] = {"value": rays / secs / 1e6, "unit": "Mrays/s", "cores": 1, "kind": "port",
                                     "sample": f"{frames} oracle renders of the whole 512x512 frame, 1 thread, "
                                               f"{secs:.1f} s"}
+        # The detail sections, rounded; the build goes last, so that the end of the line holds it.
+        if args.large:
+            line["large"] = compact(measure_large(args, world, local, dev, stream, flush))
+        if args.adjoint:
+            line["adjoint"] = compact(measure_adjoint(args, world, local, dev, stream, flush, rank))
+        if args.entities:
+            line["entities"] = compact(measure_entities(args, world, local, dev, stream, flush))
+        if args.batch:
+            line["batch"] = compact(measure_batch(args, world, local, dev, stream))
+        if build is not None:
+            section = {k: build[k] for k in ("records", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
+                                             "roofline", "roofline_build", "e2e")}
+            for k in ("traffic_source", "peak_kind"):
+                section["roofline"].pop(k, None)
+            if rank == 0 and world == 1 and not args.no_cpu_baseline:
+                v, builds, wall = oracle_build_throughput(1 << 18, 8.0, 1)
+                section["cpu_baseline"] = {"value": v, "unit": "Mleaves/s", "cores": 1, "kind": "port",
+                                           "sample": f"{builds} oracle builds of 262144 records, 1 thread"}
+            line["build"] = compact(section)
     if rank == 0:
         print(json.dumps(line), flush=True)
     dev.close()

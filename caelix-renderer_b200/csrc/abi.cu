@@ -12,6 +12,7 @@
 
 #include "../../include/caelix_b200.h"
 #include "abi_internal.h"
+#include "cx_device.cuh"
 #include "lt_build.cuh"
 #include "radix_sort.cuh"
 
@@ -388,6 +389,33 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* 
     cx::onesweep_sort(keys, values, keys_b, values_b, count, identity_values != 0, scratch, device->status, s);
     e = cudaGetLastError();
     return cx::cuda_result(e, "caelix_radix_sort_pairs");
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_radix_sort_pairs_wait_test(CaelixDevice* device, uint32_t* keys, uint32_t* values,
+                                                          uint32_t count, uint32_t silent_tile, uint32_t spin_limit,
+                                                          uint64_t stream)
+{
+    CAELIX_GUARD_BEGIN
+    const uint32_t tiles = cx::sort_tiles(count);
+    if (!device || !keys || !values || count <= cx::kSmallSortKeys || count >= (1u << 30) || silent_tile == 0 ||
+        silent_tile >= tiles || spin_limit == 0 || spin_limit > cx::kSpinLimit)
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    cudaSetDevice(device->ordinal);
+    cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+    const uint64_t words = 2ull * count + cx::sort_scratch_words(count);
+    CaelixResult r = device->sort_scratch.reserve(words * 4, "caelix_radix_sort_pairs_wait_test");
+    if (r != CAELIX_OK) return r;
+    uint32_t* base = static_cast<uint32_t*>(device->sort_scratch.ptr);
+    uint32_t* scratch = base + 2ull * count;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, cx::sort_scratch_words(count) * 4, s);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_radix_sort_pairs_wait_test");
+    const uint32_t grid = std::min<uint32_t>((count + 2047) / 2048, device->sm_count * 4);
+    cx::radix_histogram(keys, count, scratch, grid, s);
+    const cx::SortWaitTest test{silent_tile, spin_limit};
+    cx::onesweep_sort(keys, values, base, base + count, count, false, scratch, device->status, s, nullptr,
+                      cx::kSortKeysPerThread, &test);
+    return cx::cuda_result(cudaGetLastError(), "caelix_radix_sort_pairs_wait_test");
     CAELIX_GUARD_END
 }
 

@@ -462,7 +462,9 @@ CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBa
         CaelixResult r = v.renderer ? CAELIX_OK : CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK && v.renderer->device != device) r = CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK) r = render_params(v.renderer, &v.target, &v.camera, &v.options, "caelix_batch_create", &p);
-        if (r == CAELIX_OK && (v.renderer->scene->entity_view_count || !v.renderer->scene->entities.empty())) {
+        // An entity the trace sees (in the scene's device views) is not batched; the slots of
+        // removed entities, and entities whose bricks were never flushed, are not traced.
+        if (r == CAELIX_OK && v.renderer->scene->entity_view_count) {
             log(CAELIX_LOG_ERROR, "caelix_batch_create: view %u: scenes with entities are not batched", i);
             r = CAELIX_ERROR_UNSUPPORTED;
         }
@@ -523,7 +525,7 @@ CAELIX_API CaelixResult caelix_batch_run(CaelixBatch* batch, const CaelixFrameDe
     CAELIX_GUARD_BEGIN
     if (!batch || !frame) return CAELIX_ERROR_INVALID_ARGUMENT;
     for (const CaelixScene* sc : batch->scenes)
-        if (!sc->entities.empty()) {
+        if (sc->entity_view_count) {
             log(CAELIX_LOG_ERROR, "caelix_batch_run: a scene of the batch has entities (not batched)");
             return CAELIX_ERROR_UNSUPPORTED;
         }

@@ -442,53 +442,75 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
     // Room for the compaction's moves (one per removed key), taken before any state changes.
     CaelixResult r = scene->upload.reserve(8ull * count, "caelix_scene_remove_bricks");
     if (r != CAELIX_OK) return r;
-    // The slots stay dense: the last slot moves into the removed one. `source` maps a slot that
-    // took another brick to the slot that brick had before this call.
+    // The slots stay dense: the last slot moves into the removed one. A dry run over the original
+    // slots first: `source` maps a slot that takes another brick to the slot that brick had
+    // before this call, `moved` a key to its slot after such a move, `gone` the removed keys. The
+    // host state changes only after the moves have been checked.
     const uint32_t old_slots = (uint32_t)scene->slot_power.size();
     uint32_t n = old_slots;
     std::unordered_map<uint32_t, uint32_t> source;
+    std::unordered_map<uint64_t, uint32_t> moved;
+    std::unordered_map<uint64_t, uint32_t> gone;
+    auto original = [&](uint32_t slot) {
+        const auto m = source.find(slot);
+        return m != source.end() ? m->second : slot;
+    };
+    auto key_of = [&](uint32_t slot) {
+        const uint32_t o = original(slot);
+        return pack_key(CaelixBrickKey{scene->keys[3ull * o], scene->keys[3ull * o + 1], scene->keys[3ull * o + 2]});
+    };
     for (uint32_t i = 0; i < count; ++i) {
         if (!key_ok(keys[i])) continue;
-        const auto it = scene->slot_of.find(pack_key(keys[i]));
-        if (it == scene->slot_of.end()) continue;
-        const uint32_t s = it->second;
-        scene->slot_of.erase(it);
+        const uint64_t k = pack_key(keys[i]);
+        if (gone.count(k)) continue;
+        uint32_t slot;
+        if (const auto m = moved.find(k); m != moved.end()) {
+            slot = m->second;
+            moved.erase(m);
+        } else if (const auto it = scene->slot_of.find(k); it != scene->slot_of.end()) {
+            slot = it->second;
+        } else {
+            continue;
+        }
+        gone.emplace(k, slot);
         const uint32_t last = n - 1;
-        if (s != last) {
-            const CaelixBrickKey k{scene->keys[3ull * last], scene->keys[3ull * last + 1], scene->keys[3ull * last + 2]};
-            scene->slot_of[pack_key(k)] = s;
-            for (int a = 0; a < 3; ++a) scene->keys[3ull * s + a] = scene->keys[3ull * last + a];
-            scene->slot_power[s] = scene->slot_power[last];
-            const auto m = source.find(last);
-            const uint32_t from = m != source.end() ? m->second : last;
-            source[s] = from;
+        if (slot != last) {
+            moved[key_of(last)] = slot;
+            source[slot] = original(last);
         }
         source.erase(last);
         n = last;
     }
     if (n == old_slots) return CAELIX_OK;
+    // Every destination is a remaining slot and every source a slot past the end, so the moves
+    // (on the host arrays and on the device) never overlap.
+    std::vector<uint32_t> moves;
+    moves.reserve(2 * source.size());
+    for (const auto& kv : source) {
+        if (kv.first >= n || kv.second < n || kv.second >= old_slots) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_remove_bricks: bad staging move %u <- %u (nothing removed)", kv.first,
+                kv.second);
+            return CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+        moves.push_back(kv.first);
+        moves.push_back(kv.second);
+    }
+    for (const auto& kv : gone) scene->slot_of.erase(kv.first);
+    for (const auto& kv : moved) scene->slot_of[kv.first] = kv.second;
+    for (const auto& kv : source) {
+        for (int a = 0; a < 3; ++a) scene->keys[3ull * kv.first + a] = scene->keys[3ull * kv.second + a];
+        scene->slot_power[kv.first] = scene->slot_power[kv.second];
+    }
     scene->keys.resize(3ull * n);
     scene->slot_power.resize(n);
     scene->slot_dirty.assign(n, 0);
     scene->dirty_slots.clear();
     scene->upload_mark.resize(n, 0);
     for (int a = 0; a < 3; ++a) scene->key_max[a] = 0;
-    for (uint32_t s = 0; s < n; ++s)
-        for (int a = 0; a < 3; ++a) scene->key_max[a] = std::max(scene->key_max[a], scene->keys[3ull * s + a]);
+    for (uint32_t slot = 0; slot < n; ++slot)
+        for (int a = 0; a < 3; ++a) scene->key_max[a] = std::max(scene->key_max[a], scene->keys[3ull * slot + a]);
     // The key set changed: the next flush rebuilds the tables from the remaining slots.
     scene->full_rebuild = true;
-    // Every destination is a remaining slot and every source a slot past the end, so the device
-    // moves never overlap.
-    std::vector<uint32_t> moves;
-    moves.reserve(2 * source.size());
-    for (const auto& kv : source) {
-        if (kv.first >= n || kv.second < n || kv.second >= old_slots) {
-            log(CAELIX_LOG_ERROR, "caelix_scene_remove_bricks: bad staging move %u <- %u", kv.first, kv.second);
-            return CAELIX_ERROR_INVALID_ARGUMENT;
-        }
-        moves.push_back(kv.first);
-        moves.push_back(kv.second);
-    }
     if (moves.empty()) return CAELIX_OK;
     cudaSetDevice(scene->device->ordinal);
     cudaStream_t st = scene->upload_stream;

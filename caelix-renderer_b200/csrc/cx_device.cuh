@@ -78,9 +78,9 @@ __device__ __host__ __forceinline__ float float_unorder(uint32_t u)
 // A bounded spin: returns false once `iteration` reaches the limit (the caller records the
 // failure in its status word and gives up instead of waiting for ever).
 constexpr uint32_t kSpinLimit = 1u << 22;
-__device__ __forceinline__ bool spin_wait(uint32_t& iteration)
+__device__ __forceinline__ bool spin_wait(uint32_t& iteration, uint32_t limit = kSpinLimit)
 {
-    if (++iteration >= kSpinLimit) return false;
+    if (++iteration >= limit) return false;
     if (iteration > 64) __nanosleep(64);
     return true;
 }

@@ -727,7 +727,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     uint32_t* scan_counters = flag_states + scan_tiles_n;
     cudaError_t e = cudaMemsetAsync(b.control, 0, zero_words(n, kpt) * 4, stream);
     if (e != cudaSuccess) return e;
-    const uint32_t sms = 148;
+    const uint32_t sms = current_sm_count();
     if (n > 0) {
         lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
             in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves, b.control);

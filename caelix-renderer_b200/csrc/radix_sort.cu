@@ -1,8 +1,26 @@
 // Kernels of the onesweep radix sort (radix_sort.cuh describes the algorithm).
+#include <atomic>
+
 #include "cx_device.cuh"
 #include "radix_sort.cuh"
 
 namespace cx {
+
+uint32_t current_sm_count()
+{
+    constexpr int kDevices = 64;
+    static std::atomic<uint32_t> cache[kDevices];
+    int device = 0;
+    if (cudaGetDevice(&device) != cudaSuccess) return 1;
+    if (device >= 0 && device < kDevices) {
+        const uint32_t known = cache[device].load(std::memory_order_relaxed);
+        if (known) return known;
+    }
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0) return 1;
+    if (device >= 0 && device < kDevices) cache[device].store((uint32_t)sms, std::memory_order_relaxed);
+    return (uint32_t)sms;
+}
 
 struct SortPass
 {
@@ -20,6 +38,8 @@ struct SortPass
     uint32_t rows_in_stride;
     uint4* rows_out;       // 48-byte rows by destination
     uint32_t* inverse;     // inverse[value] = destination
+    uint32_t silent_tile;  // a tile that publishes no status (SortWaitTest), else 0xFFFFFFFF
+    uint32_t spin_limit;   // polls of a look-back wait before it gives up
 };
 
 namespace {
@@ -136,7 +156,8 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
         total += c;
     }
     uint32_t* state = a.tile_states + (uint64_t)tile * kRadix + d;
-    st_relaxed(state, (tile == 0 ? kTileFlagPrefix : kTileFlagAggregate) | total);
+    const bool publish = tile != a.silent_tile;
+    if (publish) st_relaxed(state, (tile == 0 ? kTileFlagPrefix : kTileFlagAggregate) | total);
     uint32_t tile_total;
     const uint32_t local = block_exclusive_sum<kSortThreads>(total, s_scan, tile_total);
     s_local[d] = local;
@@ -159,7 +180,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
         while (j >= 0) {
             const uint32_t s = ld_relaxed(a.tile_states + (uint64_t)j * kRadix + d);
             if ((s & ~kTileValueMask) == 0) {
-                if (!spin_wait(spins)) {
+                if (!spin_wait(spins, a.spin_limit)) {
                     atomicOr(a.status, kStatusLookbackTimeout);
                     break;
                 }
@@ -169,7 +190,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
             if (s & kTileFlagPrefix) break;
             --j;
         }
-        st_relaxed(state, kTileFlagPrefix | (exclusive + total));
+        if (publish) st_relaxed(state, kTileFlagPrefix | (exclusive + total));
     }
     uint32_t digit_total;
     const uint32_t global_base = block_exclusive_sum<kSortThreads>(a.counts[d], s_scan, digit_total);
@@ -292,7 +313,7 @@ void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t 
 
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
-                   const SortGather* gather, uint32_t keys_per_thread)
+                   const SortGather* gather, uint32_t keys_per_thread, const SortWaitTest* wait_test)
 {
     if (n == 0) return;
     if (n <= kSmallSortKeys) {
@@ -327,6 +348,8 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         p.rows_in_stride = gather ? gather->rows_in_stride : 0;
         p.rows_out = (last && gather) ? gather->rows_out : nullptr;
         p.inverse = (last && gather) ? gather->inverse : nullptr;
+        p.silent_tile = (pass == 0 && wait_test) ? wait_test->silent_tile : 0xFFFFFFFFu;
+        p.spin_limit = wait_test ? wait_test->spin_limit : kSpinLimit;
         if (keys_per_thread == 4) onesweep_pass_kernel<4><<<tiles, kSortThreads, 0, stream>>>(p);
         else if (keys_per_thread == 8) onesweep_pass_kernel<8><<<tiles, kSortThreads, 0, stream>>>(p);
         else onesweep_pass_kernel<16><<<tiles, kSortThreads, 0, stream>>>(p);

@@ -57,6 +57,9 @@ __host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n, uint32_t k
     return 4ull * kRadix + 4ull + 4ull * sort_tiles(n, kpt) * kRadix;
 }
 
+// The number of SMs of the current CUDA device (looked up once per device), for grid sizing.
+uint32_t current_sm_count();
+
 // Accumulates the 256-bin histograms of all four digits of keys[0 .. n) into hist[4][256].
 void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream);
 
@@ -71,6 +74,15 @@ struct SortGather
     uint32_t* inverse;
 };
 
+// A failure injected into the look-back of the first pass, for tests of the bounded waits: tile
+// `silent_tile` never publishes its status words, and every look-back wait gives up after
+// `spin_limit` polls (setting kStatusLookbackTimeout) instead of the default limit.
+struct SortWaitTest
+{
+    uint32_t silent_tile;
+    uint32_t spin_limit;
+};
+
 // Launches the four passes: keys_a/values_a hold the input and, after the even number of passes,
 // the output; keys_b/values_b are the ping-pong buffers. `identity_values`: the input values are
 // 0 .. n-1 and are not read (values_a is still written). `scratch` holds sort_scratch_words(n)
@@ -81,6 +93,7 @@ struct SortGather
 // passes in shared memory (one launch; the same permutation; scratch and histograms unused).
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
-                   const SortGather* gather = nullptr, uint32_t keys_per_thread = kSortKeysPerThread);
+                   const SortGather* gather = nullptr, uint32_t keys_per_thread = kSortKeysPerThread,
+                   const SortWaitTest* wait_test = nullptr);
 
 }  // namespace cx

@@ -954,7 +954,7 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     if (n > 0) {
         hash_home_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, s.hash_capacity, lo, hi, home);
         CX_TRY(cudaMemsetAsync(sortw, 0, sort_words * 4, stream));
-        radix_histogram(home, n, sortw, std::min<uint32_t>(blocks_for(n, 2048), 148 * 4), stream);
+        radix_histogram(home, n, sortw, std::min<uint32_t>(blocks_for(n, 2048), current_sm_count() * 4), stream);
         onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream);
         hash_shift_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(home, n, tmp);
         CX_TRY(run_scan(true, tmp, tmp2, n, small, nullptr, s.status, stream));
@@ -1049,7 +1049,7 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     uint32_t total_units = 0;
     if (m > 0) {
         CX_TRY(cudaMemsetAsync(sortw, 0, sort_scratch_words(m) * 4, stream));
-        radix_histogram(lkeys, m, sortw, std::min<uint32_t>(blocks_for(m, 2048), 148 * 4), stream);
+        radix_histogram(lkeys, m, sortw, std::min<uint32_t>(blocks_for(m, 2048), current_sm_count() * 4), stream);
         onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream);
         uint32_t* units = home;    // m words
         uint32_t* totals = order;  // m words

@@ -20,8 +20,10 @@ namespace {
 
 // Largest count of pairs one call sorts.
 constexpr uint32_t kStaticSortMaxPairs = 1u << 18;  // 262144
-// Scratch layout (u32 words): ping-pong keys [max], ping-pong values [max], a fallback status word
-// block [64], then the onesweep words (histograms, tile counters, look-back tile states).
+// Scratch layout (u32 words): ping-pong keys [max], ping-pong values [max], a status word block
+// [64] that takes the failure bits of calls without a status word of their own (nothing reads it:
+// such a call drops its device-side failures), then the onesweep words (histograms, tile counters,
+// look-back tile states).
 constexpr uint64_t kStaticStatusWords = 64;
 constexpr uint64_t kStaticScratchWords =
     2ull * kStaticSortMaxPairs + kStaticStatusWords + cx::sort_scratch_words(kStaticSortMaxPairs);
@@ -79,12 +81,15 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs_static(uint32_t* keys, uint32_t*
     uint32_t* values_b = base + kStaticSortMaxPairs;
     uint32_t* fallback_status = base + 2ull * kStaticSortMaxPairs;
     uint32_t* scratch = fallback_status + kStaticStatusWords;
-    // The array keeps the previous call's contents: clear the words that must start at zero (the
-    // histograms, tile counters and look-back states of this call's size).
-    cudaError_t e = cudaMemsetAsync(scratch, 0, cx::sort_scratch_words(count) * 4, s);
-    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_radix_sort_pairs_static");
-    const uint32_t grid = std::min<uint32_t>((count + 2047) / 2048, 148 * 4);
-    cx::radix_histogram(keys, count, scratch, grid, s);
+    if (count > cx::kSmallSortKeys) {
+        // The array keeps the previous call's contents: clear the words that must start at zero
+        // (the histograms, tile counters and look-back states of this call's size). A sort of at
+        // most kSmallSortKeys pairs runs in one CTA's shared memory and reads none of them.
+        cudaError_t e = cudaMemsetAsync(scratch, 0, cx::sort_scratch_words(count) * 4, s);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_radix_sort_pairs_static");
+        const uint32_t grid = std::min<uint32_t>((count + 2047) / 2048, cx::current_sm_count() * 4);
+        cx::radix_histogram(keys, count, scratch, grid, s);
+    }
     cx::onesweep_sort(keys, values, keys_b, values_b, count, identity_values != 0, scratch,
                       status ? status : fallback_status, s);
     return cx::cuda_result(cudaGetLastError(), "caelix_radix_sort_pairs_static");

@@ -136,7 +136,7 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
     uint32_t* sortw = scratch + 4ull * n;
     staging_linear_kernel<<<blocks(n), kStageThreads, 0, stream>>>(stage_keys, n, grid[0], grid[1], lin);
     CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n), stream));
-    radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, 148 * 4), stream);
+    radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, current_sm_count() * 4), stream);
     // A stable sort of the linear indices (unique: one slot per key), values = the slots.
     onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream);
     staging_gather_kernel<<<blocks(64ull * n), kStageThreads, 0, stream>>>(

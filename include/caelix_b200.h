@@ -219,6 +219,18 @@ CAELIX_API CaelixResult caelix_light_bvh_get_stats(CaelixLightBvh* bvh, CaelixLi
 CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* keys, uint32_t* values,
                                                 uint32_t count, uint32_t identity_values, uint64_t stream);
 
+/* No counterpart in the reference: a failure-injection hook for tests of the bounded device waits
+   (the reference's look-back has no bound; this library's waits give up and report instead of
+   hanging). Runs the multi-tile sort of caelix_radix_sort_pairs (count > 4096) with tile
+   `silent_tile` (1 .. tiles - 1, tiles of 4096 pairs) of the first pass never publishing its
+   look-back status, and every look-back wait limited to `spin_limit` polls (1 .. 2^22): the tile
+   after it gives up, sets the look-back timeout bit in the device status word and finishes with a
+   wrong prefix (the output is not a valid sort). caelix_device_check then returns
+   CAELIX_ERROR_DEVICE_STATUS with that bit; nothing traps or hangs, and the device stays usable. */
+CAELIX_API CaelixResult caelix_radix_sort_pairs_wait_test(CaelixDevice* device, uint32_t* keys, uint32_t* values,
+                                                          uint32_t count, uint32_t silent_tile, uint32_t spin_limit,
+                                                          uint64_t stream);
+
 /* No counterpart in the reference. The same sort for callers that cannot allocate device memory
    while they record work (an engine render thread that records a frame and must not stall it on
    an allocation, a host whose device memory budget is fixed up front): it allocates nothing. Its scratch is an array
@@ -228,8 +240,8 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* 
    (cudaGetSymbolAddress); make that first call before any stream capture. Every call shares the
    array and clears what must start at zero; calls whose work overlaps on the GPU (other streams,
    other host threads) race on it and must be serialized by the caller. `status` (a device word,
-   may be NULL) receives device-side failures OR-ed in (a look-back that gave up). Asynchronous on
-   `stream`. */
+   may be NULL) receives device-side failures OR-ed in (a look-back that gave up); with NULL such a
+   failure is not reported anywhere. Asynchronous on `stream`. */
 CAELIX_API CaelixResult caelix_radix_sort_pairs_static(uint32_t* keys, uint32_t* values, uint32_t count,
                                                        uint32_t identity_values, uint32_t* status, uint64_t stream);
 

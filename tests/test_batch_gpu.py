@@ -183,3 +183,32 @@ def test_scene_reflush_recaptures(cuda_device):
     batch.close()
     r.close()
     scene.close()
+
+
+def test_batch_after_entity_removed(cuda_device):
+    """A scene whose only entity was added, flushed and removed again has no entity the trace sees:
+    it is batched, and its view equals the plain render."""
+    import torch
+
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(8, 8, 8), seed=23)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    ent = workloads.noise_world(grid_bricks=(2, 2, 2), brick_occupancy=1.0, voxel_fill=0.5, seed=24)
+    e = scene.add_entity((20.0, 20.0, 20.0))
+    scene.upload_bricks(ent.keys, ent.voxels, entity=e)
+    scene.flush()
+    scene.remove_entity(e)
+    scene.flush()
+    r = caelix_b200.Renderer(cuda_device, scene)
+    out = torch.zeros(40 * 40 * 3, device="cuda")
+    batch = caelix_b200.Batch(cuda_device, [(r, out, 40, 40, vs.camera, 3, 1, 1)])
+    batch.run()
+    batch.stats()
+    ref = torch.zeros_like(out)
+    r.render(ref, 40, 40, vs.camera, bounces=3, seed=1, spp=1)
+    torch.cuda.synchronize()
+    assert torch.equal(out, ref)
+    batch.close()
+    r.close()
+    scene.close()

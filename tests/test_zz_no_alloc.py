@@ -56,6 +56,25 @@ def test_static_sort_matches_allocating_sort_twice(cuda_device):
         assert np.array_equal(k2.view(np.uint32), keys[order])
 
 
+def test_static_sort_small_sizes_match_allocating_sort(cuda_device):
+    # 1 and 4096 pairs take the one-CTA path (the whole sort in shared memory, no scratch words);
+    # 4097 is the smallest count of the multi-tile path. Two rounds, so that the second round runs
+    # on what the first left in the shared array.
+    lib = bind(cuda_device.L.lib)
+    rng = np.random.default_rng(12)
+    for round_ in range(2):
+        for n in (1, 4096, 4097):
+            for identity in (False, True):
+                keys = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+                keys[:: 3] = keys[0]
+                vals = rng.integers(0, 1 << 32, size=n, dtype=np.uint64).astype(np.uint32)
+                k1, v1, k2, v2 = sort_both(cuda_device, lib, keys, vals, identity)
+                assert np.array_equal(k1, k2), f"round {round_}, n {n}: keys differ"
+                assert np.array_equal(v1, v2), f"round {round_}, n {n}: values differ"
+                order = np.argsort(keys, kind="stable")
+                assert np.array_equal(k2.view(np.uint32), keys[order])
+
+
 def test_static_sort_rejects_sizes_above_its_scratch(cuda_device):
     import torch
 
