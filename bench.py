@@ -637,12 +637,11 @@ def measure_large(args, world, local, dev, stream, flush):
     t0 = time.perf_counter()
     vs = workloads.noise_world_large()
     gen_s = time.perf_counter() - t0
-    scene = caelix_b200.Scene(dev, vs.group_shift)
+    scene = caelix_b200.Scene.for_voxel_scene(dev, vs)
     t0 = time.perf_counter()
     scene.upload_bricks(vs.keys, vs.voxels)
     em = vs.power > 0
-    scene.set_brick_power(vs.keys[em], vs.power[em])
-    scene.set_albedo(vs.albedo)
+    scene.set_brick_power(vs.keys, vs.power)
     upload_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     scene.flush(stream.cuda_stream)
@@ -671,8 +670,8 @@ def measure_large(args, world, local, dev, stream, flush):
         total_ms += a.elapsed_time(b)
     ms = max_over_ranks(total_ms, world) / steps
     t = renderer.timings()
-    # A light-options change: the next flush rebuilds only the light tree.
-    scene.set_light_options(min_emission=20.0)
+    # A light-options change that keeps the light codes: the next flush rebuilds only the light tree.
+    scene.set_light_options(True, 0.25)
     scene.flush(sptr)
     tree_flush_ms = float(renderer.timings().flush_ms)
     # An edit: 1 % of the bricks uploaded again (to the device staging), then the full flush from
@@ -743,7 +742,7 @@ def measure_flush(args, world, local, dev, stream):
 
     nb = args.flush_bricks
     vs = workloads.noise_world_large(occupied_bricks=nb, emissive_bricks=max(1, nb // 20))
-    scene = caelix_b200.Scene(dev, vs.group_shift)
+    scene = caelix_b200.Scene.for_voxel_scene(dev, vs)
     renderer = caelix_b200.Renderer(dev, scene)
     sptr = stream.cuda_stream
     # The bricks arrive from a .cxw world file: read, decoded on every host thread, uploaded.
@@ -768,8 +767,7 @@ def measure_flush(args, world, local, dev, stream):
     voxels, power = vs.voxels[keep], vs.power[keep]
     threads = os.cpu_count() or 1
     em = power > 0
-    scene.set_brick_power(keys[em], power[em])
-    scene.set_albedo(vs.albedo)
+    scene.set_brick_power(keys, power)
     scene.flush(sptr)
     first_ms = float(renderer.timings().flush_ms)
     rng = np.random.default_rng(5)
@@ -783,7 +781,7 @@ def measure_flush(args, world, local, dev, stream):
         if k >= args.warmup:
             edit_ms.append(float(renderer.timings().flush_ms))
             edit_upload_s.append(up)
-    scene.set_light_options(min_emission=20.0)
+    scene.set_light_options(True, 0.25)
     scene.flush(sptr)
     tree_ms = float(renderer.timings().flush_ms)
     # A brick at the first free cell of the grid: the key set changes, so the flush rebuilds all.
@@ -846,7 +844,7 @@ def measure_adjoint(args, world, local, dev, stream, flush, rank):
     tr = caelix_b200.Renderer(dev, tscene)
     img = torch.zeros(ADJ_W * ADJ_H * 3, device="cuda")
     tgt = torch.zeros_like(img)
-    d_alb = torch.zeros(128 * 3, device="cuda")
+    d_alb = torch.zeros(65536 * 3, device="cuda")
     d_pow = torch.zeros(vs.brick_count, device="cuda")
 
     def forward():

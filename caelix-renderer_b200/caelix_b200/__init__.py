@@ -290,7 +290,14 @@ class CaelixEntityDesc(C.Structure):
 
 
 class CaelixSceneDesc(C.Structure):
-    _fields_ = [("group_shift", C.c_uint32), ("encoding", C.c_uint32), ("reserved", C.c_uint32 * 2)]
+    _fields_ = [("staging_bytes", C.c_uint64), ("records_per_page", C.c_uint32), ("group_shift", C.c_uint32),
+                ("block_bytes", C.c_uint32), ("encoding", C.c_uint32), ("scratch_bytes", C.c_uint64)]
+
+
+assert C.sizeof(CaelixSceneDesc) == 32
+
+ENCODING_PACKED = 0
+ENCODING_BLOCK_ID = 1
 
 
 class CaelixBrickKey(C.Structure):
@@ -308,6 +315,13 @@ class CaelixMaterial(C.Structure):
 
 
 assert C.sizeof(CaelixMaterial) == 112
+
+
+class CaelixMaterialEntry(C.Structure):
+    _fields_ = [("code", C.c_uint32), ("material", CaelixMaterial)]
+
+
+assert C.sizeof(CaelixMaterialEntry) == 116
 
 
 class CaelixLightOptions(C.Structure):
@@ -338,7 +352,8 @@ class CaelixSceneView(C.Structure):
                 ("hash_max_probe", C.c_uint32), ("light_count", C.c_uint32), ("heap_words", C.c_uint32),
                 ("group_count", C.c_uint32)] + [(n, C.c_uint64) for n in (
                     "keys", "records", "hash_slots", "bitmap", "heap", "group_rows", "light_headers", "light_group",
-                    "light_entry", "light_brick", "tree_header", "tree_nodes", "tree_leaves")]
+                    "light_entry", "light_brick", "tree_header", "tree_nodes", "tree_leaves")] + [
+                ("origin", C.c_int32 * 3), ("encoding", C.c_uint32)]
 
 
 class CaelixCamera(C.Structure):
@@ -349,12 +364,16 @@ class CaelixCamera(C.Structure):
 
 
 class CaelixRenderTargets(C.Structure):
-    _fields_ = [("radiance", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32)]
+    _fields_ = [("radiance", C.c_uint64), ("width", C.c_uint32), ("height", C.c_uint32), ("voxel_id", C.c_uint64)]
 
 
 class CaelixRenderOptions(C.Structure):
     _fields_ = [("mode", C.c_uint32), ("bounce_count", C.c_uint32), ("frame_seed", C.c_uint32), ("spp", C.c_uint32),
-                ("reserved", C.c_uint32 * 4)]
+                ("voxel_id_tmax", C.c_float), ("reserved", C.c_uint32 * 3)]
+
+
+def render_options(bounces: int, seed: int, spp: int, voxel_id_tmax: float = 0.0) -> CaelixRenderOptions:
+    return CaelixRenderOptions(1, bounces, seed, spp, float(voxel_id_tmax), (C.c_uint32 * 3)(0, 0, 0))
 
 
 class CaelixLightNeeOptions(C.Structure):
@@ -384,6 +403,8 @@ def _bind_scene(L):
         "caelix_scene_set_entity_transform": [vp, C.c_uint32, vp, vp],
         "caelix_scene_set_entity_motion": [vp, C.c_uint32, C.c_uint32],
         "caelix_scene_set_materials": [vp, vp, C.c_uint32],
+        "caelix_scene_set_material_entries": [vp, vp, C.c_uint32],
+        "caelix_scene_get_material": [vp, C.c_uint32, C.POINTER(CaelixMaterial)],
         "caelix_scene_set_light_options": [vp, C.POINTER(CaelixLightOptions)],
         "caelix_scene_flush": [vp, C.POINTER(CaelixFrameDesc)],
         "caelix_scene_get_view": [vp, C.POINTER(CaelixSceneView)],
@@ -416,12 +437,12 @@ def _bind_scene(L):
 class Scene:
     """caelix_scene_*: bricks, brick power, materials, flush."""
 
-    def __init__(self, device: Device, group_shift: int = 4):
+    def __init__(self, device: Device, group_shift: int = 4, encoding: int = ENCODING_PACKED):
         self.device = device
         self.L = device.L
         _bind_scene(self.L.lib)
         handle = C.c_void_p()
-        desc = CaelixSceneDesc(group_shift, 1, (C.c_uint32 * 2)(0, 0))
+        desc = CaelixSceneDesc(0, 0, group_shift, 0, encoding, 0)
         self.L.check(self.L.lib.caelix_scene_create(device.handle, C.byref(desc), C.byref(handle)), "caelix_scene_create")
         self.handle = handle
         self.frame = 0
@@ -490,23 +511,46 @@ class Scene:
         self.L.check(self.L.lib.caelix_scene_set_brick_power(self.handle, entity, len(keys), keys.ctypes.data,
                                                              power.ctypes.data), "caelix_scene_set_brick_power")
 
-    def set_albedo(self, albedo):
-        """Material table entries 0 .. len(albedo) - 1 with the given albedo (Lambertian)."""
-        entries = (CaelixMaterial * len(albedo))()
-        for i, a in enumerate(albedo):
+    def set_materials(self, materials):
+        """caelix_scene_set_materials: entries [0, len) from (albedo, emission) pairs, the rest built-in."""
+        entries = (CaelixMaterial * max(len(materials), 1))()
+        for i, (a, e) in enumerate(materials):
             entries[i].albedo[:] = [float(v) for v in a]
+            entries[i].emission[:] = [float(v) for v in e]
             entries[i].ior = 1.5
-        self.L.check(self.L.lib.caelix_scene_set_materials(self.handle, entries, len(albedo)),
+        self.L.check(self.L.lib.caelix_scene_set_materials(self.handle, entries, len(materials)),
                      "caelix_scene_set_materials")
+
+    def set_material_entries(self, entries):
+        """caelix_scene_set_material_entries: [(code, albedo rgb, emission rgb)] over the current table."""
+        arr = (CaelixMaterialEntry * max(len(entries), 1))()
+        for i, (code, a, e) in enumerate(entries):
+            arr[i].code = int(code)
+            arr[i].material.albedo[:] = [float(v) for v in a]
+            arr[i].material.emission[:] = [float(v) for v in e]
+            arr[i].material.ior = 1.5
+        self.L.check(self.L.lib.caelix_scene_set_material_entries(self.handle, arr, len(entries)),
+                     "caelix_scene_set_material_entries")
+
+    def material(self, code: int) -> CaelixMaterial:
+        m = CaelixMaterial()
+        self.L.check(self.L.lib.caelix_scene_get_material(self.handle, code, C.byref(m)), "caelix_scene_get_material")
+        return m
+
+    def set_albedo(self, albedo):
+        """The block-ID materials of the benchmark worlds: code 0x8000 | i gets albedo[i] and an emission
+        of 1 on every channel (the brick's power is its voxels' radiance)."""
+        self.set_material_entries([(0x8000 | i, a, (1.0, 1.0, 1.0)) for i, a in enumerate(albedo)])
 
     def flush(self, stream: int = 0):
         self.frame += 1
         fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
         self.L.check(self.L.lib.caelix_scene_flush(self.handle, C.byref(fd)), "caelix_scene_flush")
 
-    def set_light_options(self, enabled: bool = True, min_emission: float = 20.0, heap_bytes: int = 16 << 20):
-        """caelix_scene_set_light_options; with the tree already on, the next flush rebuilds only the
-        light tree."""
+    def set_light_options(self, enabled: bool = True, min_emission: float = 0.5, heap_bytes: int = 16 << 20):
+        """caelix_scene_set_light_options (the library's default min_emission is 20; the benchmark
+        worlds' emission is 1, so 0.5 here); with the tree already on and the light codes unchanged,
+        the next flush rebuilds only the light tree."""
         o = CaelixLightOptions(1 if enabled else 0, float(min_emission), int(heap_bytes))
         self.L.check(self.L.lib.caelix_scene_set_light_options(self.handle, C.byref(o)),
                      "caelix_scene_set_light_options")
@@ -522,14 +566,23 @@ class Scene:
         return s
 
     @classmethod
+    def for_voxel_scene(cls, device: Device, vs):
+        """An empty device scene with a workloads.VoxelScene's encoding, materials and light options."""
+        s = cls(device, vs.group_shift, vs.encoding)
+        entries = vs.material_entries()
+        if entries:
+            s.set_material_entries(entries)
+        s.set_light_options(vs.lights, vs.min_emission)
+        return s
+
+    @classmethod
     def from_voxel_scene(cls, device: Device, vs):
-        """A device scene holding a workloads.VoxelScene (bricks, power, albedo), flushed."""
-        s = cls(device, vs.group_shift)
+        """A device scene holding a workloads.VoxelScene (bricks, every brick's power, materials,
+        light options), flushed."""
+        s = cls.for_voxel_scene(device, vs)
         s.upload_bricks(vs.keys, vs.voxels)
-        emissive = vs.power > 0
-        if emissive.any():
-            s.set_brick_power(vs.keys[emissive], vs.power[emissive])
-        s.set_albedo(vs.albedo)
+        if vs.brick_count:
+            s.set_brick_power(vs.keys, vs.power)
         s.flush()
         return s
 
@@ -660,25 +713,27 @@ class Renderer:
                      "caelix_renderer_set_light_nee_options")
 
     def render(self, radiance, width: int, height: int, camera, bounces: int = 4, seed: int = 1, spp: int = 1,
-               stream: int = 0):
+               stream: int = 0, voxel_id=None, voxel_id_tmax: float = 0.0):
+        """caelix_renderer_render; voxel_id (device, height x width x 2 uint32, optional) receives the
+        voxel id target."""
         self.frame += 1
         fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
-        t = CaelixRenderTargets(_ptr(radiance), width, height)
+        t = CaelixRenderTargets(_ptr(radiance), width, height, _ptr(voxel_id) if voxel_id is not None else 0)
         cam = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
-        o = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+        o = render_options(bounces, seed, spp, voxel_id_tmax)
         self.L.check(self.L.lib.caelix_renderer_render(self.handle, C.byref(fd), C.byref(t), C.byref(cam), C.byref(o)),
                      "caelix_renderer_render")
 
     def backward(self, d_radiance, width: int, height: int, camera, d_albedo, d_power, bounces: int = 4,
                  seed: int = 1, spp: int = 1, image=None, stream: int = 0):
         """caelix_renderer_backward: d_radiance = dL/d(radiance) (device, height x width x 3); writes
-        dL/dalbedo into d_albedo (device, 128 x 3) and dL/dpower into d_power (device, one per brick
+        dL/dalbedo into d_albedo (device, 65536 x 3, by material code) and dL/dpower into d_power (device, one per brick
         in the scene's order); image (device, optional) receives the forward radiance."""
         self.frame += 1
         fd = CaelixFrameDesc(stream, self.frame, self.frame - 1)
-        t = CaelixRenderTargets(_ptr(image) if image is not None else 0, width, height)
+        t = CaelixRenderTargets(_ptr(image) if image is not None else 0, width, height, 0)
         cam = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
-        o = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+        o = render_options(bounces, seed, spp)
         self.L.check(self.L.lib.caelix_renderer_backward(self.handle, C.byref(fd), C.byref(t), C.byref(cam),
                                                          C.byref(o), _ptr(d_radiance), _ptr(d_albedo),
                                                          _ptr(d_power)), "caelix_renderer_backward")
@@ -753,8 +808,8 @@ class Batch:
         for i, (renderer, radiance, width, height, camera, bounces, seed, spp) in enumerate(views):
             arr[i].renderer = renderer.handle
             arr[i].camera = camera if isinstance(camera, CaelixCamera) else camera_struct(camera)
-            arr[i].target = CaelixRenderTargets(_ptr(radiance), width, height)
-            arr[i].options = CaelixRenderOptions(1, bounces, seed, spp, (C.c_uint32 * 4)(0, 0, 0, 0))
+            arr[i].target = CaelixRenderTargets(_ptr(radiance), width, height, 0)
+            arr[i].options = render_options(bounces, seed, spp)
         desc = CaelixBatchDesc(len(views), 1 if rebuild_light_trees else 0, arr, (C.c_uint32 * 4)(0, 0, 0, 0))
         handle = C.c_void_p()
         self.L.check(self.L.lib.caelix_batch_create(device.handle, C.byref(desc), C.byref(handle)),

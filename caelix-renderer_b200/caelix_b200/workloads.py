@@ -128,23 +128,126 @@ def value_noise(p: np.ndarray, seed: int) -> np.ndarray:
     return out
 
 
-class VoxelScene:
-    """A voxel world of 8^3-voxel bricks: brick keys (in increasing linear brick index), raw block
-    values (block-ID encoding: opaque = 0x8000 | material, 0 = air), per-brick emitter power,
-    the albedo table (indexed by the material id) and a camera."""
+ENCODING_PACKED = 0
+ENCODING_BLOCK_ID = 1
+MATERIAL_CODES = 65536
 
-    def __init__(self, grid, keys, voxels, power, albedo, camera, group_shift=4):
+
+def _hash32(v: np.ndarray) -> np.ndarray:
+    v = np.asarray(v, np.uint32).copy()
+    v ^= v >> np.uint32(16)
+    v *= np.uint32(0x7FEB352D)
+    v ^= v >> np.uint32(15)
+    v *= np.uint32(0x846CA68B)
+    v ^= v >> np.uint32(16)
+    return v
+
+
+def _pastel(h: np.ndarray) -> np.ndarray:
+    out = np.empty(h.shape + (3,), np.float32)
+    for c in range(3):
+        b = ((h >> np.uint32(8 * c)) & np.uint32(0xFF)).astype(np.float32)
+        out[..., c] = np.float32(0.35) + np.float32(0.6) * (b / np.float32(255.0))
+    return out
+
+
+def builtin_materials(encoding: int):
+    """The library's built-in material table of an encoding (include/caelix_b200.h, CaelixMaterial):
+    albedo and emission [65536][3] fp32 by code."""
+    code = np.arange(MATERIAL_CODES, dtype=np.uint32)
+    albedo = np.ones((MATERIAL_CODES, 3), np.float32)
+    emission = np.zeros((MATERIAL_CODES, 3), np.float32)
+    if encoding == ENCODING_PACKED:
+        rgb5 = (code & np.uint32(0x8000)) != 0
+        rgb4 = ((code & np.uint32(0xC000)) == np.uint32(0x4000))
+        for c, shift in enumerate((10, 5, 0)):
+            v = ((code >> np.uint32(shift)) & np.uint32(31)).astype(np.float32) / np.float32(31.0)
+            albedo[rgb5, c] = v[rgb5]
+        strength = np.exp2(np.float32(3.0) * (code & np.uint32(3)).astype(np.float32)).astype(np.float32)
+        for c, shift in enumerate((10, 6, 2)):
+            v = ((code >> np.uint32(shift)) & np.uint32(15)).astype(np.float32) / np.float32(15.0)
+            albedo[rgb4, c] = v[rgb4]
+            emission[rgb4, c] = (v * strength)[rgb4]
+    else:
+        opaque = (code & np.uint32(0x8000)) != 0
+        albedo[opaque] = _pastel(_hash32(code[opaque] & np.uint32(0x7FFF)))
+        ids = code & np.uint32(0x1FF)
+        tr = ~opaque & (ids != 0)
+        albedo[tr] = _pastel(_hash32(ids[tr] | np.uint32(0x10000)))
+    return albedo, emission
+
+
+def scene_grid(keys: np.ndarray, group_shift: int):
+    """The box of a set of brick keys as the library's flush computes it: origin = the smallest key
+    per axis rounded down to a multiple of the group edge, grid = the bricks from there to the
+    largest key."""
+    keys = np.asarray(keys, np.int64).reshape(-1, 3)
+    if len(keys) == 0:
+        return (0, 0, 0), (1, 1, 1)
+    edge = 1 << group_shift
+    lo = keys.min(axis=0)
+    origin = (lo // edge) * edge  # floor division rounds toward -inf
+    grid = keys.max(axis=0) - origin + 1
+    return tuple(int(v) for v in origin), tuple(int(v) for v in grid)
+
+
+class VoxelScene:
+    """A voxel world of 8^3-voxel bricks: brick keys (in increasing linear brick index of their
+    box), raw block values, per-brick emitter power, a material table and a camera.
+
+    The material table is the encoding's built-in table with, for the block-ID worlds of the
+    benchmark generators, the entries of codes 0x8000 | i (i < len(albedo)) set to albedo[i] and an
+    emission of 1 on every channel (a brick's power then is its voxels' emitted radiance; bricks
+    of power 0 emit nothing), plus `entries` ({code: (albedo rgb, emission rgb)}) over it. Light
+    voxels: codes whose emission luminance reaches min_emission, in bricks with power above 0."""
+
+    def __init__(self, grid, keys, voxels, power, albedo, camera, group_shift=4, encoding=ENCODING_BLOCK_ID,
+                 entries=None, min_emission=0.5, lights=True):
         self.grid = tuple(int(g) for g in grid)
         self.keys = np.ascontiguousarray(keys, np.int32)
         self.voxels = np.ascontiguousarray(voxels, np.uint16)
         self.power = np.ascontiguousarray(power, np.float32)
-        self.albedo = np.ascontiguousarray(albedo, np.float32)
+        self.albedo = np.ascontiguousarray(albedo if albedo is not None else np.zeros((0, 3)), np.float32)
         self.camera = camera
         self.group_shift = group_shift
+        self.encoding = encoding
+        self.entries = dict(entries or {})
+        self.min_emission = float(min_emission)
+        self.lights = bool(lights)
 
     @property
     def brick_count(self):
         return len(self.keys)
+
+    def material_entries(self):
+        """[(code, albedo rgb, emission rgb)]: the entries the host sets over the built-in table."""
+        out = []
+        if self.encoding == ENCODING_BLOCK_ID:
+            for i, a in enumerate(self.albedo):
+                out.append((0x8000 | i, tuple(float(v) for v in a), (1.0, 1.0, 1.0)))
+        for code, (a, e) in sorted(self.entries.items()):
+            out.append((int(code), tuple(float(v) for v in a), tuple(float(v) for v in e)))
+        return out
+
+    def material_tables(self):
+        """The whole table: albedo and emission [65536][3] fp32 by code."""
+        albedo, emission = builtin_materials(self.encoding)
+        for code, a, e in self.material_entries():
+            albedo[code] = np.asarray(a, np.float32)
+            emission[code] = np.asarray(e, np.float32)
+        return albedo, emission
+
+    def box(self):
+        """(origin, grid) of the keys, as the library's flush computes them."""
+        return scene_grid(self.keys, self.group_shift)
+
+    def like(self, **changes):
+        """A copy with some fields replaced (keys, voxels, power, albedo, ...)."""
+        fields = dict(grid=self.grid, keys=self.keys, voxels=self.voxels, power=self.power, albedo=self.albedo,
+                      camera=self.camera, group_shift=self.group_shift, encoding=self.encoding,
+                      entries=self.entries, min_emission=self.min_emission, lights=self.lights)
+        fields.update(changes)
+        return VoxelScene(**fields)
 
 
 def look_at(position, target, tan_half_fov_y=0.5, aspect=1.0):
@@ -395,4 +498,4 @@ def perturbed(vs: VoxelScene, seed: int = 7, amount: float = 0.10) -> VoxelScene
     up = 2.0 * Pcg32(seed, 22).next_doubles(len(vs.power)) - 1.0
     albedo = (vs.albedo * (1.0 + amount * ua)).astype(np.float32)
     power = (vs.power * (1.0 + amount * up)).astype(np.float32)
-    return VoxelScene(vs.grid, vs.keys, vs.voxels, power, albedo, vs.camera, vs.group_shift)
+    return vs.like(power=power, albedo=albedo)

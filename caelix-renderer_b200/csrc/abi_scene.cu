@@ -13,6 +13,7 @@
 #include "../../include/caelix_b200.h"
 #include "abi_internal.h"
 #include "abi_scene_internal.h"
+#include "materials.h"
 #include "scene.cuh"
 #include "trace.cuh"
 
@@ -20,16 +21,67 @@ using cx::log;
 
 namespace {
 
-constexpr int32_t kMaxKey = 1024;
+// Brick keys per axis in [-2^20, 2^20) (include/caelix/caelix.h:334).
+constexpr int32_t kKeyLimit = 1 << 20;
 
 bool key_ok(const CaelixBrickKey& k)
 {
-    return k.x >= 0 && k.y >= 0 && k.z >= 0 && k.x < kMaxKey && k.y < kMaxKey && k.z < kMaxKey;
+    return k.x >= -kKeyLimit && k.y >= -kKeyLimit && k.z >= -kKeyLimit && k.x < kKeyLimit && k.y < kKeyLimit &&
+           k.z < kKeyLimit;
 }
 
+// 21 bits per axis (the key moved to [0, 2^21)).
 uint64_t pack_key(const CaelixBrickKey& k)
 {
-    return (uint64_t)(uint32_t)k.x | ((uint64_t)(uint32_t)k.y << 20) | ((uint64_t)(uint32_t)k.z << 40);
+    return (uint64_t)(uint32_t)(k.x + kKeyLimit) | ((uint64_t)(uint32_t)(k.y + kKeyLimit) << 21) |
+           ((uint64_t)(uint32_t)(k.z + kKeyLimit) << 42);
+}
+
+// The scene whose material table, light code set and light options a scene uses: its own, or for
+// an entity's bricks the scene that holds the entity.
+const CaelixScene* owner_of(const CaelixScene* scene) { return scene->parent ? scene->parent : scene; }
+
+// The smallest and largest key of the staged bricks, per axis (0 without bricks).
+void key_bounds(CaelixScene* scene)
+{
+    const size_t n = scene->slot_power.size();
+    for (int a = 0; a < 3; ++a) {
+        scene->key_min[a] = n ? scene->keys[a] : 0;
+        scene->key_max[a] = n ? scene->keys[a] : 0;
+    }
+    for (size_t slot = 1; slot < n; ++slot)
+        for (int a = 0; a < 3; ++a) {
+            scene->key_min[a] = std::min(scene->key_min[a], scene->keys[3 * slot + a]);
+            scene->key_max[a] = std::max(scene->key_max[a], scene->keys[3 * slot + a]);
+        }
+}
+
+// The device form of a scene's material table and its light code set, after a change of either
+// (materials or min_emission): uploaded on `stream`; *codes_changed when the light code set is
+// not the one the scene's tables were built with.
+CaelixResult upload_materials(CaelixScene* scene, cudaStream_t stream, bool* codes_changed)
+{
+    *codes_changed = false;
+    if (!scene->materials_dirty) return CAELIX_OK;
+    std::vector<uint32_t> codes;
+    cx::light_code_set(scene->materials, scene->encoding, scene->light_options.min_emission, codes);
+    *codes_changed = codes != scene->light_codes;
+    std::vector<float> table;
+    cx::pack_materials(scene->materials, scene->encoding, table);
+    CaelixResult r = scene->materials_dev.reserve(4ull * table.size(), "caelix_scene_flush");
+    if (r == CAELIX_OK) r = scene->light_codes_dev.reserve(4ull * codes.size(), "caelix_scene_flush");
+    if (r != CAELIX_OK) return r;
+    cudaError_t e = cudaMemcpyAsync(scene->materials_dev.ptr, table.data(), 4ull * table.size(),
+                                    cudaMemcpyHostToDevice, stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(scene->light_codes_dev.ptr, codes.data(), 4ull * codes.size(), cudaMemcpyHostToDevice,
+                            stream);
+    // The host vectors are released on return: the copies finish first.
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    scene->light_codes = std::move(codes);
+    scene->materials_dirty = false;
+    return CAELIX_OK;
 }
 
 // Object-to-world rotation rows of a quaternion (x, y, z, w), normalised, in double, then rounded.
@@ -122,6 +174,9 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     cx::SceneView v;
     std::memset(&v, 0, sizeof(v));
     v.group_shift = scene->group_shift;
+    v.enc = cx::encoding_of(scene->encoding);
+    v.materials = static_cast<const float4*>(scene->materials_dev.ptr);
+    v.light_codes = static_cast<const uint32_t*>(scene->light_codes_dev.ptr);
     v.power = power;
     v.heap = heap;
     v.group_rows = rows;
@@ -152,23 +207,28 @@ CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
 {
     std::vector<cx::EntityView> views;
     std::vector<const CaelixScene::Entity*> live;
-    for (auto& e : scene->entities) {
+    for (size_t id = 0; id < scene->entities.size(); ++id) {
+        CaelixScene::Entity& e = scene->entities[id];
         if (!e.bricks || !e.bricks->built) continue;
         cx::EntityView v;
         v.scene = cx::scene_view(e.bricks->dev);
         std::memcpy(v.rot, e.rot, sizeof(v.rot));
         std::memcpy(v.pos, e.position, sizeof(v.pos));
         v.group_base = 0;
-        // The sphere round the entity's brick grid [0, 8 grid) in world space (double, inflated).
+        v.id = (uint32_t)id + 1;
+        // The sphere round the entity's brick grid [8 origin, 8 (origin + grid)) in world space
+        // (double, inflated).
         {
-            double c[3], r2 = 0.0;
+            const cx::DeviceScene& d = e.bricks->dev;
+            double c[3], r2 = 0.0, mid[3];
             for (int a = 0; a < 3; ++a) {
-                const double h = 4.0 * e.bricks->dev.grid[a];
+                const double h = 4.0 * d.grid[a];
                 r2 += h * h;
+                mid[a] = 8.0 * d.origin[a] + h;
             }
             for (int i = 0; i < 3; ++i) {
                 c[i] = e.position[i];
-                for (int j = 0; j < 3; ++j) c[i] += (double)e.rot[3 * i + j] * 4.0 * e.bricks->dev.grid[j];
+                for (int j = 0; j < 3; ++j) c[i] += (double)e.rot[3 * i + j] * mid[j];
                 v.sphere[i] = (float)c[i];
             }
             v.sphere[3] = (float)(std::sqrt(r2) * 1.001 + 0.01);
@@ -214,7 +274,8 @@ CaelixResult render_params(const CaelixRenderer* renderer, const CaelixRenderTar
 {
     if (!renderer || !targets || !camera || !options || !out) return CAELIX_ERROR_INVALID_ARGUMENT;
     if (!targets->radiance || targets->width == 0 || targets->height == 0 || options->mode != 1 ||
-        options->bounce_count > 14 || camera->jitter[0] != 0.0f || camera->jitter[1] != 0.0f)
+        options->bounce_count > 14 || camera->jitter[0] != 0.0f || camera->jitter[1] != 0.0f ||
+        !std::isfinite(options->voxel_id_tmax) || options->voxel_id_tmax < 0.0f)
         return CAELIX_ERROR_INVALID_ARGUMENT;
     for (uint32_t r : options->reserved)
         if (r) return CAELIX_ERROR_INVALID_ARGUMENT;
@@ -238,6 +299,8 @@ CaelixResult render_params(const CaelixRenderer* renderer, const CaelixRenderTar
     p.bounce_count = options->bounce_count;
     p.frame_seed = options->frame_seed;
     p.light_nee = (renderer->nee.enabled && scene->light_options.enabled && scene->dev.light_count) ? 1u : 0u;
+    p.voxel_id = reinterpret_cast<uint32_t*>(targets->voxel_id);
+    p.voxel_id_tmax = options->voxel_id_tmax;
     return CAELIX_OK;
 }
 
@@ -248,24 +311,30 @@ CAELIX_API CaelixResult caelix_scene_create(CaelixDevice* device, const CaelixSc
     CAELIX_GUARD_BEGIN
     if (!device || !out_scene) return CAELIX_ERROR_INVALID_ARGUMENT;
     *out_scene = nullptr;
-    uint32_t shift = 4;
+    uint32_t shift = 4, encoding = cx::kEncodingPacked;
     if (desc) {
-        if (desc->reserved[0] || desc->reserved[1]) return CAELIX_ERROR_INVALID_ARGUMENT;
-        if (desc->encoding != 1) {
-            log(CAELIX_LOG_ERROR, "caelix_scene_create: only the block-ID encoding (1) is implemented");
-            return desc->encoding == 0 ? CAELIX_ERROR_UNSUPPORTED : CAELIX_ERROR_INVALID_ARGUMENT;
+        // The reference's checks (include/caelix/caelix.h:274-294), then what this version implements.
+        if ((desc->staging_bytes != 0 && desc->staging_bytes < (4ull << 20)) ||
+            (desc->records_per_page & (desc->records_per_page - 1u)) != 0 || desc->group_shift > 8 ||
+            (desc->block_bytes != 0 && desc->block_bytes != 2 && desc->block_bytes != 4) || desc->encoding > 1) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_create: invalid scene description");
+            return CAELIX_ERROR_INVALID_ARGUMENT;
         }
         shift = desc->group_shift ? desc->group_shift : 4;
-        if (shift > 4) {
-            log(CAELIX_LOG_ERROR, "caelix_scene_create: group_shift %u above 4 is not implemented", shift);
+        if (shift > 4 || desc->block_bytes == 4) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_create: group_shift %u above 4 or 4-byte blocks are not implemented",
+                shift);
             return CAELIX_ERROR_UNSUPPORTED;
         }
+        encoding = desc->encoding;
     }
     cudaSetDevice(device->ordinal);
     CaelixScene* s = new CaelixScene();
     s->device = device;
     s->group_shift = shift;
-    for (uint32_t i = 0; i < cx::kMaterialSlots * 3; ++i) s->albedo[i] = 0.5f;
+    s->encoding = encoding;
+    s->materials.resize(cx::kMaterialCodes);
+    for (uint32_t c = 0; c < cx::kMaterialCodes; ++c) s->materials[c] = cx::builtin_material(c, encoding);
     cudaError_t e = cudaEventCreate(&s->start);
     if (e == cudaSuccess) e = cudaEventCreate(&s->stop);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->upload_stream, cudaStreamNonBlocking);
@@ -288,6 +357,8 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     scene->dyn_arrays.release();
     scene->dyn_tree.release();
     scene->dyn_view.release();
+    scene->materials_dev.release();
+    scene->light_codes_dev.release();
     cx::scene_release(scene->dev);
     if (scene->upload_stream) cudaStreamSynchronize(scene->upload_stream);
     if (scene->stage_keys) cudaFree(scene->stage_keys);
@@ -316,8 +387,8 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     }
     for (uint32_t i = 0; i < count; ++i) {
         if (!key_ok(keys[i])) {
-            log(CAELIX_LOG_ERROR, "caelix_scene_upload_bricks: key (%d, %d, %d) outside [0, %d)", keys[i].x, keys[i].y,
-                keys[i].z, kMaxKey);
+            log(CAELIX_LOG_ERROR, "caelix_scene_upload_bricks: key (%d, %d, %d) outside [-%d, %d)", keys[i].x,
+                keys[i].y, keys[i].z, kKeyLimit, kKeyLimit);
             return CAELIX_ERROR_INVALID_ARGUMENT;
         }
     }
@@ -328,6 +399,7 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
     // below gives the new slots back, so the scene stays as it was before the call.
     const uint32_t old_slots = (uint32_t)scene->slot_power.size();
     const int32_t old_max[3] = {scene->key_max[0], scene->key_max[1], scene->key_max[2]};
+    const int32_t old_min[3] = {scene->key_min[0], scene->key_min[1], scene->key_min[2]};
     std::vector<std::pair<uint64_t, float>> taken_power;
     std::vector<uint32_t> slot(count);
     for (uint32_t i = 0; i < count; ++i) {
@@ -335,12 +407,15 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
         const auto ins = scene->slot_of.emplace(packed, (uint32_t)scene->slot_power.size());
         slot[i] = ins.first->second;
         if (ins.second) {
-            scene->keys.insert(scene->keys.end(), {keys[i].x, keys[i].y, keys[i].z});
-            scene->key_max[0] = std::max(scene->key_max[0], keys[i].x);
-            scene->key_max[1] = std::max(scene->key_max[1], keys[i].y);
-            scene->key_max[2] = std::max(scene->key_max[2], keys[i].z);
+            const int32_t k3[3] = {keys[i].x, keys[i].y, keys[i].z};
+            const bool first = scene->slot_power.empty();
+            scene->keys.insert(scene->keys.end(), {k3[0], k3[1], k3[2]});
+            for (int a = 0; a < 3; ++a) {
+                scene->key_max[a] = first ? k3[a] : std::max(scene->key_max[a], k3[a]);
+                scene->key_min[a] = first ? k3[a] : std::min(scene->key_min[a], k3[a]);
+            }
             const auto p = scene->pending_power.find(packed);
-            scene->slot_power.push_back(p != scene->pending_power.end() ? p->second : 0.0f);
+            scene->slot_power.push_back(p != scene->pending_power.end() ? p->second : 1.0f);
             if (p != scene->pending_power.end()) {
                 taken_power.emplace_back(p->first, p->second);
                 scene->pending_power.erase(p);
@@ -355,7 +430,10 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
         }
         scene->keys.resize(3ull * old_slots);
         scene->slot_power.resize(old_slots);
-        for (int a = 0; a < 3; ++a) scene->key_max[a] = old_max[a];
+        for (int a = 0; a < 3; ++a) {
+            scene->key_max[a] = old_max[a];
+            scene->key_min[a] = old_min[a];
+        }
         for (const auto& kv : taken_power) scene->pending_power.insert(kv);
         return r;
     };
@@ -506,9 +584,7 @@ CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t 
     scene->slot_dirty.assign(n, 0);
     scene->dirty_slots.clear();
     scene->upload_mark.resize(n, 0);
-    for (int a = 0; a < 3; ++a) scene->key_max[a] = 0;
-    for (uint32_t slot = 0; slot < n; ++slot)
-        for (int a = 0; a < 3; ++a) scene->key_max[a] = std::max(scene->key_max[a], scene->keys[3ull * slot + a]);
+    key_bounds(scene);
     // The key set changed: the next flush rebuilds the tables from the remaining slots.
     scene->full_rebuild = true;
     if (moves.empty()) return CAELIX_OK;
@@ -532,10 +608,13 @@ CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const Caelix
     for (int k = 0; k < 3; ++k)
         if (!std::isfinite(desc->position[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
     if (!entity_rows(desc->rotation, rot)) return CAELIX_ERROR_INVALID_ARGUMENT;
-    CaelixSceneDesc sd{scene->group_shift, 1, {0, 0}};
+    CaelixSceneDesc sd{0, 0, scene->group_shift, 0, scene->encoding, 0};
     CaelixScene* bricks = nullptr;
     CaelixResult r = caelix_scene_create(scene->device, &sd, &bricks);
     if (r != CAELIX_OK) return r;
+    bricks->parent = scene;
+    bricks->materials.clear();  // the scene's table is used
+    bricks->materials_dirty = false;
     bricks->last_frame = scene->last_frame;
     uint32_t slot = 0;
     while (slot < scene->entities.size() && scene->entities[slot].bricks) ++slot;
@@ -628,27 +707,67 @@ CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_
 CAELIX_API CaelixResult caelix_scene_set_materials(CaelixScene* scene, const CaelixMaterial* entries, uint32_t count)
 {
     CAELIX_GUARD_BEGIN
-    if (!scene || (count && !entries) || count > cx::kMaterialSlots) return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (uint32_t i = 0; i < count; ++i)
-        for (int k = 0; k < 3; ++k)
-            if (!std::isfinite(entries[i].albedo[k])) return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (uint32_t i = 0; i < cx::kMaterialSlots; ++i)
-        for (int k = 0; k < 3; ++k) scene->albedo[3 * i + k] = i < count ? entries[i].albedo[k] : 0.5f;
-    scene->albedo_dirty = true;
+    if (!scene || scene->parent || (count && !entries) || count > cx::kMaterialCodes)
+        return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) {
+        const char* reason = nullptr;
+        if (!cx::material_valid(entries[i], &reason)) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_set_materials: entry %u: %s", i, reason);
+            return CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    for (uint32_t c = 0; c < cx::kMaterialCodes; ++c) {
+        scene->materials[c] = c < count ? entries[c] : cx::builtin_material(c, scene->encoding);
+        scene->materials[c].reserved = 0;
+    }
+    scene->materials_dirty = true;
     return CAELIX_OK;
     CAELIX_GUARD_END
 }
 
+CAELIX_API CaelixResult caelix_scene_set_material_entries(CaelixScene* scene, const CaelixMaterialEntry* entries,
+                                                          uint32_t count)
+{
+    CAELIX_GUARD_BEGIN
+    if (!scene || scene->parent || (count && !entries)) return CAELIX_ERROR_INVALID_ARGUMENT;
+    for (uint32_t i = 0; i < count; ++i) {
+        const char* reason = "code above 0xFFFF";
+        if (entries[i].code > 0xFFFFu || !cx::material_valid(entries[i].material, &reason)) {
+            log(CAELIX_LOG_ERROR, "caelix_scene_set_material_entries: entry %u: %s", i, reason);
+            return CAELIX_ERROR_INVALID_ARGUMENT;
+        }
+    }
+    for (uint32_t i = 0; i < count; ++i) {
+        scene->materials[entries[i].code] = entries[i].material;
+        scene->materials[entries[i].code].reserved = 0;
+    }
+    if (count) scene->materials_dirty = true;
+    return CAELIX_OK;
+    CAELIX_GUARD_END
+}
+
+CAELIX_API CaelixResult caelix_scene_get_material(const CaelixScene* scene, uint32_t code, CaelixMaterial* out)
+{
+    if (!scene || !out || code > 0xFFFFu) return CAELIX_ERROR_INVALID_ARGUMENT;
+    const CaelixScene* o = owner_of(scene);
+    *out = o->materials[cx::canonical_code(code, o->encoding)];
+    return CAELIX_OK;
+}
+
 CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const CaelixLightOptions* options)
 {
-    if (!scene || !options || options->enabled > 1 || !std::isfinite(options->min_emission) ||
+    if (!scene || scene->parent || !options || options->enabled > 1 || !std::isfinite(options->min_emission) ||
         options->min_emission < 0.0f || options->heap_bytes > (16ull << 32))
         return CAELIX_ERROR_INVALID_ARGUMENT;
-    // Toggling the tree changes the light records (the power of every brick); any other change
-    // takes effect as a light-tree rebuild at the next flush, as in the reference.
-    if (options->enabled != scene->light_options.enabled || !scene->built) scene->full_rebuild = true;
+    CaelixLightOptions o = *options;
+    if (o.min_emission == 0.0f) o.min_emission = 20.0f;
+    // Toggling the tree rebuilds the tables (the light records come and go); a new min_emission
+    // may change the light code set (checked at the flush, which then rebuilds the tables); any
+    // other change takes effect as a light-tree rebuild at the next flush, as in the reference.
+    if (o.enabled != scene->light_options.enabled || !scene->built) scene->full_rebuild = true;
     else scene->light_tree_dirty = true;
-    scene->light_options = *options;
+    if (o.min_emission != scene->light_options.min_emission) scene->materials_dirty = true;
+    scene->light_options = o;
     return CAELIX_OK;
 }
 
@@ -663,6 +782,28 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         return CAELIX_ERROR_INVALID_ARGUMENT;
     }
     scene->last_frame = desc->frame_number;
+    cudaSetDevice(scene->device->ordinal);
+    cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
+    const CaelixScene* owner = owner_of(scene);
+    const bool lit = owner->light_options.enabled != 0;
+    // The material table and the light code set first (an entity's bricks use its scene's). The
+    // trace reads the table at draw time; a change of the light code set rebuilds the tables, as the
+    // reference finalizes every resident brick again (include/caelix/caelix.h:625-629).
+    if (!scene->parent) {
+        bool codes_changed = false;
+        CaelixResult r = upload_materials(scene, stream, &codes_changed);
+        if (r != CAELIX_OK) return r;
+        if (codes_changed) {
+            scene->full_rebuild = true;
+            for (auto& ent : scene->entities)
+                if (ent.bricks) ent.bricks->full_rebuild = true;
+        }
+    }
+    if (scene->built && scene->dev.lights != lit) scene->full_rebuild = true;
+    scene->dev.encoding = scene->encoding;
+    scene->dev.materials = static_cast<const float4*>(owner->materials_dev.ptr);
+    scene->dev.light_codes = static_cast<const uint32_t*>(owner->light_codes_dev.ptr);
+    scene->dev.lights = lit;
     // The entities' bricks (their own flushes), then their device views when any moved, changed,
     // came or went.
     for (auto& ent : scene->entities) {
@@ -672,36 +813,30 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         if (ent.bricks->generation != ent.generation) scene->entity_views_dirty = true;
     }
     if (scene->entity_views_dirty) {
-        cudaSetDevice(scene->device->ordinal);
-        CaelixResult r = upload_entity_views(scene, reinterpret_cast<cudaStream_t>(desc->command_buffer));
+        CaelixResult r = upload_entity_views(scene, stream);
         if (r != CAELIX_OK) return r;
     }
     if (!scene->built) scene->full_rebuild = true;
     const bool edits = !scene->dirty_slots.empty();
-    if (!scene->full_rebuild && !edits && !scene->light_tree_dirty && !scene->albedo_dirty) return CAELIX_OK;
-    cudaSetDevice(scene->device->ordinal);
-    cudaStream_t stream = reinterpret_cast<cudaStream_t>(desc->command_buffer);
-    const bool lit = scene->light_options.enabled != 0;
+    if (!scene->full_rebuild && !edits && !scene->light_tree_dirty) return CAELIX_OK;
     uint32_t status = 0;
     cudaError_t e = cudaSuccess;
     if (!scene->full_rebuild) {
         // The brick set is unchanged: the tables stay; the edited bricks are copied into the
         // scene and their records and their neighbours' finalized again, then the light records
         // and the light tree are rebuilt. A light-options change alone rebuilds the light tree.
-        if (edits || scene->albedo_dirty) {
+        if (edits) {
             // Rewritten in place: renders of the scene, on any stream, finish first.
             e = cudaDeviceSynchronize();
             if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
         }
         cudaEventRecord(scene->start, stream);
-        if (scene->albedo_dirty)
-            e = cudaMemcpyAsync(scene->dev.albedo, scene->albedo, sizeof(scene->albedo), cudaMemcpyHostToDevice, stream);
-        if (e == cudaSuccess && edits) {
+        if (edits) {
             const uint32_t c = (uint32_t)scene->dirty_slots.size();
             std::vector<uint32_t> host(2ull * c);
             for (uint32_t i = 0; i < c; ++i) {
                 const uint32_t slot = scene->dirty_slots[i];
-                const float p = lit ? scene->slot_power[slot] : 0.0f;
+                const float p = scene->slot_power[slot];
                 host[i] = slot;
                 std::memcpy(&host[c + i], &p, 4);
             }
@@ -732,7 +867,7 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(&scene->last_update_records, d_count, 4, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        } else if (e == cudaSuccess && scene->light_tree_dirty) {
+        } else if (scene->light_tree_dirty) {
             e = cx::scene_build_light_tree(scene->dev, stream);
             if (e == cudaSuccess) e = cx::scene_read_status(scene->dev, stream, &status);
         }
@@ -742,16 +877,22 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
         cudaEventElapsedTime(&scene->flush_ms, scene->start, scene->stop);
         for (uint32_t slot : scene->dirty_slots) scene->slot_dirty[slot] = 0;
         scene->dirty_slots.clear();
-        scene->albedo_dirty = false;
         scene->light_tree_dirty = false;
         if (edits) scene->generation += 1;
         return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
     }
-    // A full rebuild: the staged bricks in increasing linear brick index of the grid spanned by
-    // the keys, sorted and gathered on the device, then the build.
+    // A full rebuild: the staged bricks in increasing linear brick index of the box spanned by the
+    // keys (rounded to whole groups), sorted and gathered on the device, then the build.
     const uint32_t n = (uint32_t)scene->slot_power.size();
-    const uint32_t grid[3] = {(uint32_t)scene->key_max[0] + 1, (uint32_t)scene->key_max[1] + 1,
-                              (uint32_t)scene->key_max[2] + 1};
+    int32_t origin[3];
+    uint32_t grid[3];
+    if (!cx::scene_grid(scene->key_min, scene->key_max, scene->group_shift, origin, grid)) {
+        log(CAELIX_LOG_ERROR,
+            "caelix_scene_flush: the box of the keys (%d, %d, %d) .. (%d, %d, %d) holds more than 2^32 brick cells",
+            scene->key_min[0], scene->key_min[1], scene->key_min[2], scene->key_max[0], scene->key_max[1],
+            scene->key_max[2]);
+        return CAELIX_ERROR_UNSUPPORTED;
+    }
     CaelixResult r = scene->flush_scratch.reserve_grow(4ull * n + 4 * cx::staging_sort_words(n), "caelix_scene_flush");
     if (r == CAELIX_OK) r = scene->record_of_slot.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
     if (r == CAELIX_OK) r = scene->marks.reserve_grow(4ull * std::max(n, 1u), "caelix_scene_flush");
@@ -766,16 +907,14 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     cudaEventRecord(scene->start, stream);
     e = cx::scene_alloc_inputs(scene->dev, n, stream);
-    if (e == cudaSuccess && lit && n)
+    if (e == cudaSuccess && n)
         e = cudaMemcpyAsync(d_power, scene->slot_power.data(), 4ull * n, cudaMemcpyHostToDevice, stream);
-    if (e == cudaSuccess)
-        e = cudaMemcpyAsync(scene->dev.albedo, scene->albedo, sizeof(scene->albedo), cudaMemcpyHostToDevice, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(scene->marks.ptr, 0, 4ull * std::max(n, 1u), stream);
     if (e == cudaSuccess)
-        e = cx::staging_gather(scene->stage_keys, scene->stage_voxels, lit ? d_power : nullptr, n, grid, sort_scratch,
+        e = cx::staging_gather(scene->stage_keys, scene->stage_voxels, d_power, n, origin, grid, sort_scratch,
                                scene->dev.status, scene->dev.keys, scene->dev.voxels, scene->dev.power,
                                static_cast<uint32_t*>(scene->record_of_slot.ptr), stream);
-    if (e == cudaSuccess) e = cx::scene_build_device(scene->dev, grid, scene->group_shift, n, stream, &status);
+    if (e == cudaSuccess) e = cx::scene_build_device(scene->dev, origin, grid, scene->group_shift, n, stream, &status);
     cudaEventRecord(scene->stop, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     cudaEventSynchronize(scene->stop);
@@ -784,7 +923,6 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     scene->dirty_slots.clear();
     scene->mark_epoch = 0;
     scene->full_rebuild = false;
-    scene->albedo_dirty = false;
     scene->light_tree_dirty = false;
     scene->built = true;
     scene->generation += 1;
@@ -838,7 +976,9 @@ CAELIX_API CaelixResult caelix_scene_get_view(const CaelixScene* scene, CaelixSc
     for (int k = 0; k < 3; ++k) {
         out->grid[k] = d.grid[k];
         out->groups[k] = d.groups[k];
+        out->origin[k] = d.origin[k];
     }
+    out->encoding = d.encoding;
     out->group_shift = d.group_shift;
     out->brick_count = d.brick_count;
     out->hash_capacity = d.hash_capacity;
@@ -986,7 +1126,7 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     }
     cudaSetDevice(renderer->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
-    cudaError_t e = cudaMemsetAsync(d_albedo, 0, sizeof(float) * cx::kMaterialSlots * 3, stream);
+    cudaError_t e = cudaMemsetAsync(d_albedo, 0, sizeof(float) * cx::kMaterialCodes * 3, stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(d_power, 0, sizeof(float) * std::max(scene->dev.brick_count, 1u), stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(renderer->counts, 0, 24, stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_renderer_backward");

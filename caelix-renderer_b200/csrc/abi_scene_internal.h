@@ -15,13 +15,18 @@ struct CaelixScene
 {
     CaelixDevice* device = nullptr;
     uint32_t group_shift = 4;
+    uint32_t encoding = cx::kEncodingPacked;
+    // An entity's bricks are a scene of their own under the scene that holds the entity (`parent`):
+    // they use its material table, light code set and light options.
+    CaelixScene* parent = nullptr;
     // Brick staging. Slot s holds the brick keys[3s .. 3s+2]; its 512 block values stay on the
     // device (stage_voxels[512s ..], copied there by the upload that wrote them), its key in
     // stage_keys[3s ..] and its power in slot_power[s].
     std::unordered_map<uint64_t, uint32_t> slot_of;
     std::vector<int32_t> keys;
     std::vector<float> slot_power;
-    std::unordered_map<uint64_t, float> pending_power;  // power of keys not uploaded yet
+    std::unordered_map<uint64_t, float> pending_power;  // power of keys not uploaded yet (default 1)
+    int32_t key_min[3] = {0, 0, 0};
     int32_t key_max[3] = {0, 0, 0};
     uint32_t stage_capacity = 0;  // slots
     int32_t* stage_keys = nullptr;
@@ -37,14 +42,20 @@ struct CaelixScene
     bool full_rebuild = true;
     std::vector<uint32_t> dirty_slots;
     std::vector<uint8_t> slot_dirty;
-    bool albedo_dirty = false;
+    bool materials_dirty = true;  // the device table and light code set are stale
     cx::GrowBuffer record_of_slot;  // device: the brick index of every slot (the last full build)
     cx::GrowBuffer marks;           // device: one word per brick (staging_update)
     uint32_t mark_epoch = 0;
     cx::GrowBuffer update;          // device: edited slots, their power, the refinalize list
     uint32_t last_update_records = 0;  // records finalized again by the last incremental flush
-    float albedo[cx::kMaterialSlots * 3];
-    CaelixLightOptions light_options{1, 20.0f, 16ull << 20};
+    // The material table (host copy, one entry per 16-bit code), its device form (two float4 per
+    // code: albedo, emission) and the light code set (codes whose emission luminance reaches
+    // min_emission), host and device.
+    std::vector<CaelixMaterial> materials;
+    std::vector<uint32_t> light_codes;
+    cx::GrowBuffer materials_dev;
+    cx::GrowBuffer light_codes_dev;
+    CaelixLightOptions light_options{0, 20.0f, 16ull << 20};
     bool light_tree_dirty = false;  // the light tree is stale (a light-options change)
     uint64_t last_frame = 0;
     cx::DeviceScene dev;

@@ -151,12 +151,13 @@ __global__ void hash_place_kernel(const uint32_t* __restrict__ running_max, cons
     atomicMax(max_probe, pos - home_sorted[k]);
 }
 
-__global__ void bitmap_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t gx, uint32_t gy,
-                              uint32_t* __restrict__ bitmap)
+__global__ void bitmap_kernel(const int32_t* __restrict__ keys, uint32_t n, int32_t ox, int32_t oy, int32_t oz,
+                              uint32_t gx, uint32_t gy, uint32_t* __restrict__ bitmap)
 {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint64_t c = (uint64_t)keys[3 * i] + gx * ((uint64_t)keys[3 * i + 1] + (uint64_t)gy * keys[3 * i + 2]);
+    const uint64_t c = (uint64_t)(uint32_t)(keys[3 * i] - ox) +
+                       gx * ((uint64_t)(uint32_t)(keys[3 * i + 1] - oy) + (uint64_t)gy * (uint32_t)(keys[3 * i + 2] - oz));
     atomicOr(bitmap + (c >> 5), 1u << (c & 31));
 }
 
@@ -196,26 +197,56 @@ __device__ __forceinline__ uint32_t coarse_rows(uint32_t ballot, uint32_t cx)
     return (b & 0xFu) | ((b >> 4) & 0xF0u) | ((b >> 8) & 0xF00u) | ((b >> 12) & 0xF000u);
 }
 
+// Bit 15 of each 16-bit half of a pair of values (one u32): the value is opaque (kEnc: the block
+// encoding; packed values are opaque on bit 14 or 15, block-ID values on bit 15).
+template <uint32_t kEnc>
+__device__ __forceinline__ uint32_t opaque_top(uint32_t w)
+{
+    return kEnc == kEncodingPacked ? (w | (w << 1)) : w;
+}
+
 // Whether a pair of values (one u32) / a value holds a non-opaque value other than air.
+template <uint32_t kEnc>
 __device__ __forceinline__ bool impure(uint32_t w)
 {
-    const uint32_t clear = ~w & 0x80008000u;
+    const uint32_t clear = ~opaque_top<kEnc>(w) & 0x80008000u;
     const uint32_t nonzero = ((w & 0x7FFF7FFFu) + 0x7FFF7FFFu) & 0x80008000u;
     return (clear & nonzero) != 0;
 }
+template <uint32_t kEnc>
 __device__ __forceinline__ bool impure(const uint4& v)
 {
-    return impure(v.x) || impure(v.y) || impure(v.z) || impure(v.w);
+    return impure<kEnc>(v.x) || impure<kEnc>(v.y) || impure<kEnc>(v.z) || impure<kEnc>(v.w);
 }
-__device__ __forceinline__ bool impure16(uint32_t v) { return !(v & kOpaqueBit) && v != 0; }
+template <uint32_t kEnc>
+__device__ __forceinline__ bool impure16(uint32_t v)
+{
+    return !(v & encoding_of(kEnc).opaque_mask) && v != 0;
+}
 
 // The opaque bits of 8 values (bit j = value j).
+template <uint32_t kEnc>
 __device__ __forceinline__ uint32_t opaque_byte(const uint4& v)
 {
-    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    const uint32_t w[4] = {opaque_top<kEnc>(v.x), opaque_top<kEnc>(v.y), opaque_top<kEnc>(v.z), opaque_top<kEnc>(v.w)};
     uint32_t b = 0;
 #pragma unroll
     for (int i = 0; i < 4; ++i) b |= (((w[i] >> 15) & 1u) | ((w[i] >> 30) & 2u)) << (2 * i);
+    return b;
+}
+
+// The light bits of 8 values (bit j = value j's material code is in the light code set).
+template <uint32_t kEnc>
+__device__ __forceinline__ uint32_t light_byte(const uint4& v, const uint32_t* __restrict__ codes)
+{
+    constexpr Encoding E = encoding_of(kEnc);
+    const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+    uint32_t b = 0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t c = material_code((w[i >> 1] >> (16 * (i & 1))) & 0xFFFFu, E);
+        b |= ((__ldg(codes + (c >> 5)) >> (c & 31)) & 1u) << i;
+    }
     return b;
 }
 
@@ -275,22 +306,31 @@ struct OpaqueMasks
     uint32_t o, n[6];
 };
 
-__device__ __forceinline__ OpaqueMasks opaque_masks(const BrickFaces& f, uint32_t lane)
+// The mask words of per-lane bytes (b0: values 8 lane .. 8 lane + 7, b1: 256 + 8 lane ..): lane
+// k < 16 gets word k (bit j = value 32 k + j), the lanes above get the bytes of lanes k - 16 (no use).
+__device__ __forceinline__ uint32_t mask_word(uint32_t b0, uint32_t b1, uint32_t lane)
 {
-    const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
-    const uint32_t o0 = opaque_byte(f.v0), o1 = opaque_byte(f.v1);
     uint32_t o = 0;
 #pragma unroll
     for (uint32_t i = 0; i < 4; ++i) {
         const uint32_t src = (4 * lane + i) & 31u;
-        const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, o0, src), t1 = __shfl_sync(0xFFFFFFFFu, o1, src);
+        const uint32_t t0 = __shfl_sync(0xFFFFFFFFu, b0, src), t1 = __shfl_sync(0xFFFFFFFFu, b1, src);
         o |= (lane < 8 ? t0 : t1) << (8 * i);
     }
-    const uint32_t fxp0 = __ballot_sync(0xFFFFFFFFu, f.xf[0] & kOpaqueBit);
-    const uint32_t fxn0 = __ballot_sync(0xFFFFFFFFu, f.xf[1] & kOpaqueBit);
-    const uint32_t fxp1 = __ballot_sync(0xFFFFFFFFu, f.xf[2] & kOpaqueBit);
-    const uint32_t fxn1 = __ballot_sync(0xFFFFFFFFu, f.xf[3] & kOpaqueBit);
-    const uint32_t fb = opaque_byte(f.fv);
+    return o;
+}
+
+template <uint32_t kEnc>
+__device__ __forceinline__ OpaqueMasks opaque_masks(const BrickFaces& f, uint32_t lane)
+{
+    constexpr uint32_t kOpaque = encoding_of(kEnc).opaque_mask;
+    const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
+    const uint32_t o = mask_word(opaque_byte<kEnc>(f.v0), opaque_byte<kEnc>(f.v1), lane);
+    const uint32_t fxp0 = __ballot_sync(0xFFFFFFFFu, f.xf[0] & kOpaque);
+    const uint32_t fxn0 = __ballot_sync(0xFFFFFFFFu, f.xf[1] & kOpaque);
+    const uint32_t fxp1 = __ballot_sync(0xFFFFFFFFu, f.xf[2] & kOpaque);
+    const uint32_t fxn1 = __ballot_sync(0xFFFFFFFFu, f.xf[3] & kOpaque);
+    const uint32_t fb = opaque_byte<kEnc>(f.fv);
     const uint32_t fyp = __shfl_sync(0xFFFFFFFFu, fb, kz), fyn = __shfl_sync(0xFFFFFFFFu, fb, 8 + kz);
     uint32_t fzp = 0, fzn = 0;
 #pragma unroll
@@ -314,8 +354,10 @@ __device__ __forceinline__ OpaqueMasks opaque_masks(const BrickFaces& f, uint32_
     return m;
 }
 
+template <uint32_t kEnc>
 __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const FinalizeArgs a)
 {
+    constexpr Encoding E = encoding_of(kEnc);
     __shared__ __align__(16) uint32_t s_stage[kFinalizeWarps][kFinalizeStageWords];
     __shared__ __align__(16) uint32_t s_record[kFinalizeWarps][kFinalizeRecordWords];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
@@ -344,14 +386,15 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
         // its raw values as the payload, and a voxel of it is occupied iff it is opaque and not
         // all six of its neighbours are: shifted masks of the opaque voxels. Other bricks take
         // the per-voxel rules.
-        const bool dirty = __any_sync(0xFFFFFFFFu, impure(v0) || impure(v1) || impure(fv) || impure16(xf[0]) ||
-                                                       impure16(xf[1]) || impure16(xf[2]) || impure16(xf[3]));
+        const bool dirty =
+            __any_sync(0xFFFFFFFFu, impure<kEnc>(v0) || impure<kEnc>(v1) || impure<kEnc>(fv) || impure16<kEnc>(xf[0]) ||
+                                        impure16<kEnc>(xf[1]) || impure16<kEnc>(xf[2]) || impure16<kEnc>(xf[3]));
         // Lane k < 16 ends with word k of the occupied voxels: bit x + 8 (y & 3) for the rows
         // y = 4 (k & 1) + (0 .. 3) at z = k >> 1.
         uint32_t my_occ = 0;
         const uint32_t kz = (lane >> 1) & 7u, kyh = lane & 1u;
         if (!dirty) {
-            const OpaqueMasks m = opaque_masks(bf, lane);
+            const OpaqueMasks m = opaque_masks<kEnc>(bf, lane);
             my_occ = m.o & ~(m.n[0] & m.n[1] & m.n[2] & m.n[3] & m.n[4] & m.n[5]);
         } else {
 #pragma unroll 2
@@ -359,7 +402,7 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
                 const uint32_t y = ylo + 4 * (k & 1), z = k >> 1;
                 const uint32_t vi = lane + 32 * k;
                 const uint32_t raw = vox[vi];
-                const uint32_t v = (raw & kOpaqueBit) ? raw : (raw & 0x1FFu);
+                const uint32_t v = material_code(raw, E);
                 uint32_t nb[6];
                 nb[0] = vox[x < 7 ? vi + 1 : 512 + 0 * 64 + y + 8 * z];
                 nb[1] = vox[x > 0 ? vi - 1 : 512 + 1 * 64 + y + 8 * z];
@@ -370,12 +413,12 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
                 uint32_t opaque_count = 0, faces = 0;
 #pragma unroll
                 for (int d = 0; d < 6; ++d) {
-                    const bool nop = (nb[d] & kOpaqueBit) != 0;
+                    const bool nop = (nb[d] & E.opaque_mask) != 0;
                     opaque_count += nop ? 1u : 0u;
-                    if (!nop && (nb[d] & 0x1FFu) != v) faces |= 1u << d;
+                    if (!nop && (nb[d] & E.id_mask) != v) faces |= 1u << d;
                 }
-                const uint32_t result = (v & kOpaqueBit) ? v : (v | (faces << 9));
-                const bool iface = (v & kOpaqueBit) != 0 || faces != 0;
+                const uint32_t result = (v & E.opaque_mask) ? v : (v | (faces << E.face_shift));
+                const bool iface = (v & E.opaque_mask) != 0 || faces != 0;
                 rec16[2 * kRecordPayloadWord + vi] = (uint16_t)result;
                 const uint32_t ballot = __ballot_sync(0xFFFFFFFFu, opaque_count < 6 && result != 0 && iface);
                 if (lane == k) my_occ = ballot;
@@ -429,8 +472,10 @@ __global__ void __launch_bounds__(kFinalizeWarps * 32, 6) finalize_kernel(const 
 }
 
 // ---------------------------------------------------------------------------------------------
-// Light records (caelix_light_tree_build.hlsl:93-285): light voxel = opaque voxel of a brick with
-// emitter power; its open faces are the entries.
+// Light records (caelix_light_tree_build.hlsl:93-285): a light voxel is a voxel whose material code
+// is in the light code set (LtOpenFaces) in a brick with emitter power above 0; its open faces
+// (the neighbour across is not opaque, an absent brick being air) are the entries; a face's
+// weight is the luminance of its voxel's emission times the brick's power.
 
 struct LightArgs
 {
@@ -440,31 +485,55 @@ struct LightArgs
     uint32_t n;
     uint32_t group_shift;
     uint32_t groups[3];
+    int32_t origin[3];
     const uint4* slots;
     uint32_t capacity;
     uint32_t max_probe;
+    const float4* materials;
+    const uint32_t* light_codes;
 };
 
+// Warp per brick: a brick with power above 0 and a voxel whose code is a light code is a light brick.
+template <uint32_t kEnc>
 __global__ void light_collect_kernel(const LightArgs a, uint32_t* counter, uint32_t* lkeys, uint32_t* lbricks)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t lane = threadIdx.x & 31u;
     if (i >= a.n || !(a.power[i] > 0.0f)) return;
+    const uint4* vox = reinterpret_cast<const uint4*>(a.voxels + 512ull * i);
+    const uint32_t bits = light_byte<kEnc>(__ldg(vox + lane), a.light_codes) |
+                          light_byte<kEnc>(__ldg(vox + 32 + lane), a.light_codes);
+    if (!__any_sync(0xFFFFFFFFu, bits != 0u) || lane != 0) return;
     const uint32_t gs = a.group_shift, gm = (1u << gs) - 1u;
-    const uint32_t bx = (uint32_t)a.keys[3 * i], by = (uint32_t)a.keys[3 * i + 1], bz = (uint32_t)a.keys[3 * i + 2];
+    const int32_t kx = a.keys[3 * i], ky = a.keys[3 * i + 1], kz = a.keys[3 * i + 2];
+    const uint32_t bx = (uint32_t)(kx - a.origin[0]), by = (uint32_t)(ky - a.origin[1]), bz = (uint32_t)(kz - a.origin[2]);
     const uint32_t g = (bx >> gs) + a.groups[0] * ((by >> gs) + a.groups[1] * (bz >> gs));
     const uint32_t slot = atomicAdd(counter, 1u);
     lkeys[slot] = (g << (3 * gs)) | morton30(bx & gm, by & gm, bz & gm);
     lbricks[slot] = i;
 }
 
-// The open faces of the light voxels of light brick b (its opaque voxels; a face is open when the
-// neighbour across it is not opaque, an absent brick being air), per family f (+x, -x, +y, -y,
-// +z, -z) in the word layout of opaque_masks: lane k < 16 gets word k of each family.
-__device__ __forceinline__ void light_open_masks(const BrickFaces& f, uint32_t lane, uint32_t open[6])
+// The open faces of the light voxels of light brick b (a face is open when the neighbour across it
+// is not opaque, an absent brick being air), per family f (+x, -x, +y, -y, +z, -z) in the word
+// layout of opaque_masks: lane k < 16 gets word k of each family.
+template <uint32_t kEnc>
+__device__ __forceinline__ void light_open_masks(const BrickFaces& f, const uint32_t* __restrict__ codes, uint32_t lane,
+                                                 uint32_t open[6])
 {
-    const OpaqueMasks m = opaque_masks(f, lane);
+    const OpaqueMasks m = opaque_masks<kEnc>(f, lane);
+    const uint32_t word = mask_word(light_byte<kEnc>(f.v0, codes), light_byte<kEnc>(f.v1, codes), lane);
+    const uint32_t light = lane < 16 ? word : 0u;
 #pragma unroll
-    for (int d = 0; d < 6; ++d) open[d] = m.o & ~m.n[d];
+    for (int d = 0; d < 6; ++d) open[d] = light & ~m.n[d];
+}
+
+// The weight of a light face of value v in a brick of power P: LtLuminance of its material emission
+// times P (each channel times P first).
+template <uint32_t kEnc>
+__device__ __forceinline__ float light_weight(const float4* __restrict__ materials, uint32_t v, float P)
+{
+    const float4 e = __ldg(materials + 2ull * material_code(v, encoding_of(kEnc)) + 1);
+    return (e.x * P) * 0.2126f + (e.y * P) * 0.7152f + (e.z * P) * 0.0722f;
 }
 
 constexpr uint32_t kLightWarps = 4;
@@ -489,6 +558,7 @@ __device__ __forceinline__ uint32_t reused_unit(const LightReuse& r, uint32_t b)
 
 // Warp per light brick (sorted order): the family counts and the record's units (of a reused
 // record, from its header).
+template <uint32_t kEnc>
 __global__ void __launch_bounds__(kLightWarps * 32) light_measure_kernel(const LightArgs a,
                                                                         const uint32_t* __restrict__ lbricks,
                                                                         uint32_t m, uint32_t* __restrict__ counts6,
@@ -510,7 +580,7 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_measure_kernel(const L
     }
     const BrickFaces bf = load_brick_faces(a.keys, a.voxels, a.slots, a.capacity, a.max_probe, lbricks[k], lane);
     uint32_t open[6];
-    light_open_masks(bf, lane, open);
+    light_open_masks<kEnc>(bf, a.light_codes, lane, open);
     uint32_t total = 0;
 #pragma unroll
     for (int f = 0; f < 6; ++f) {
@@ -572,6 +642,7 @@ struct LightWriteArgs
     uint32_t* unit_of_brick;  // out: the first unit of every light brick's record
 };
 
+template <uint32_t kEnc>
 __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const LightWriteArgs w)
 {
     __shared__ __align__(16) uint4 s_vox[kLightWarps][64];
@@ -617,9 +688,8 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
         __syncwarp();
         const uint16_t* vox = reinterpret_cast<const uint16_t*>(s_vox[warp]);
         uint32_t open[6];
-        light_open_masks(bf, lane, open);
+        light_open_masks<kEnc>(bf, a.light_codes, lane, open);
         const float P = a.power[b];
-        const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f;
         // Entries per family in voxel order: lane k writes the voxels of word k (32k + bit) after the
         // family's entries of the lanes before it.
         uint32_t fam_count[6];
@@ -639,12 +709,16 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
                 *out++ = vi | ((uint32_t)vox[vi] << 16);
             }
             written += fam_count[f];
-            // The face sum as sixteen-voxel partial sums (voxels 16l .. 16l + 15 in lane l, the weight
-            // added once per open face), then a tree over the lanes.
+            // The face sum as sixteen-voxel partial sums (voxels 16l .. 16l + 15 in lane l, each open
+            // face's weight added in voxel order), then a tree over the lanes.
             const uint32_t word = __shfl_sync(0xFFFFFFFFu, open[f], lane >> 1);
-            const uint32_t n16 = __popc((word >> (16 * (lane & 1))) & 0xFFFFu);
+            uint32_t half = (word >> (16 * (lane & 1))) & 0xFFFFu;
             float part = 0.0f;
-            for (uint32_t i = 0; i < n16; ++i) part += weight;
+            while (half) {
+                const uint32_t bit = __ffs(half) - 1;
+                half &= half - 1;
+                part += light_weight<kEnc>(a.materials, vox[16 * lane + bit], P);
+            }
             sums[f] = part;
         }
 #pragma unroll
@@ -672,6 +746,8 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
         const uint32_t padded = (w.units[k] - 3) * 4;
         for (uint32_t e = written + lane; e < padded; e += 32) rec[12 + e] = 0u;
         if (lane == 0) {
+            // Group-local positions: the grid origin is a multiple of the group edge, so the low
+            // bits of a key (two's complement for a negative key) are its position in its group.
             const uint32_t gm = (1u << gs) - 1u;
             const int32_t bx = a.keys[3 * b], by = a.keys[3 * b + 1], bz = a.keys[3 * b + 2];
             const uint32_t org[3] = {((uint32_t)bx & gm) * 8, ((uint32_t)by & gm) * 8, ((uint32_t)bz & gm) * 8};
@@ -730,7 +806,7 @@ uint32_t finalize_grid(uint32_t n)
         int dev = 0;
         cudaGetDevice(&dev);
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finalize_kernel, kFinalizeWarps * 32, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, finalize_kernel<kEncodingBlockId>, kFinalizeWarps * 32, 0);
         per_sm = std::max(per_sm, 1);
         sms = std::max(sms, 1);
     }
@@ -769,13 +845,32 @@ cudaError_t run_scan(bool max_op, const uint32_t* in, uint32_t* out, uint32_t co
 
 }  // namespace
 
+bool scene_grid(const int32_t key_min[3], const int32_t key_max[3], uint32_t group_shift, int32_t origin[3],
+                uint32_t grid[3])
+{
+    const int64_t edge = 1ll << group_shift;
+    uint64_t cells = 1;
+    for (int k = 0; k < 3; ++k) {
+        const int64_t lo = key_min[k] >= 0 ? (key_min[k] / edge) * edge : -((-(int64_t)key_min[k] + edge - 1) / edge) * edge;
+        const int64_t extent = (int64_t)key_max[k] - lo + 1;
+        if (extent < 1 || extent > (1ll << 32)) return false;
+        origin[k] = (int32_t)lo;
+        grid[k] = (uint32_t)extent;
+        cells *= (uint64_t)((extent + edge - 1) / edge) * (uint64_t)edge;
+        if (cells > (1ull << 32)) return false;
+    }
+    return true;
+}
+
 SceneView scene_view(const DeviceScene& s)
 {
     SceneView v;
     for (int k = 0; k < 3; ++k) {
         v.grid[k] = s.grid[k];
         v.groups[k] = s.groups[k];
+        v.origin[k] = s.origin[k];
     }
+    v.enc = encoding_of(s.encoding);
     v.group_shift = s.group_shift;
     v.brick_count = s.brick_count;
     v.records = s.records;
@@ -784,7 +879,9 @@ SceneView scene_view(const DeviceScene& s)
     v.hash_max_probe = s.hash_max_probe;
     v.bitmap = s.bitmap;
     v.power = s.power;
-    v.albedo = s.albedo;
+    v.materials = s.materials;
+    v.light_codes = s.light_codes;
+    v.keys = s.keys;
     v.heap = s.heap;
     v.group_rows = s.group_rows;
     v.frames = s.frames;
@@ -886,7 +983,7 @@ static BuildScratch build_scratch(const DeviceScene& s)
 void scene_release(DeviceScene& s)
 {
     void* ptrs[] = {s.keys,          s.voxels,       s.power,        s.records,       s.hash_slots,
-                    s.bitmap,        s.albedo,       s.heap,         s.group_rows,    s.frames,
+                    s.bitmap,        s.heap,         s.group_rows,    s.frames,
                     s.light_headers, s.light_group,  s.light_entry,  s.light_brick,   s.scratch,
                     s.tree_memory,   s.status,       s.heap_prev,    s.unit_of_brick, s.unit_of_brick_prev};
     for (void* p : ptrs)
@@ -901,26 +998,27 @@ cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream)
     CX_TRY(alloc(s.keys, s.capacity.keys, 3ull * n));
     CX_TRY(alloc(s.voxels, s.capacity.voxels, 512ull * n));
     CX_TRY(alloc(s.power, s.capacity.power, n));
-    CX_TRY(alloc(s.albedo, s.capacity.albedo, kMaterialSlots * 3));
     return cudaSuccess;
 }
 
-cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t n, const int32_t* keys,
-                        const uint16_t* voxels, const float* power, const float* albedo, cudaStream_t stream,
-                        uint32_t* device_status_out)
+namespace {
+
+void launch_finalize(const FinalizeArgs& fa, uint32_t encoding, uint32_t items, cudaStream_t stream)
 {
-    CX_TRY(scene_alloc_inputs(s, n, stream));
-    CX_TRY(cudaMemcpyAsync(s.keys, keys, 12ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.voxels, voxels, 1024ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.power, power, 4ull * n, cudaMemcpyHostToDevice, stream));
-    CX_TRY(cudaMemcpyAsync(s.albedo, albedo, 12ull * kMaterialSlots, cudaMemcpyHostToDevice, stream));
-    return scene_build_device(s, grid, group_shift, n, stream, device_status_out);
+    if (encoding == kEncodingPacked)
+        finalize_kernel<kEncodingPacked><<<finalize_grid(items), kFinalizeWarps * 32, 0, stream>>>(fa);
+    else
+        finalize_kernel<kEncodingBlockId><<<finalize_grid(items), kFinalizeWarps * 32, 0, stream>>>(fa);
 }
 
-cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t n,
-                               cudaStream_t stream, uint32_t* device_status_out)
+}  // namespace
+
+cudaError_t scene_build_device(DeviceScene& s, const int32_t origin[3], const uint32_t grid[3], uint32_t group_shift,
+                               uint32_t n, cudaStream_t stream, uint32_t* device_status_out)
 {
+    if (!s.materials || !s.light_codes) return cudaErrorInvalidValue;
     for (int k = 0; k < 3; ++k) s.grid[k] = grid[k];
+    for (int k = 0; k < 3; ++k) s.origin[k] = origin[k];
     s.group_shift = group_shift;
     const uint32_t gm = (1u << group_shift) - 1u;
     for (int k = 0; k < 3; ++k) s.groups[k] = (grid[k] + gm) >> group_shift;
@@ -965,7 +1063,9 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     const uint64_t cells = (uint64_t)grid[0] * grid[1] * grid[2];
     CX_TRY(alloc(s.bitmap, s.capacity.bitmap, (cells + 31) / 32));
     CX_TRY(cudaMemsetAsync(s.bitmap, 0, 4 * ((cells + 31) / 32), stream));
-    if (n > 0) bitmap_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, grid[0], grid[1], s.bitmap);
+    if (n > 0)
+        bitmap_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, origin[0], origin[1], origin[2],
+                                                                         grid[0], grid[1], s.bitmap);
     CX_TRY(cudaMemcpyAsync(&s.hash_max_probe, d_max_probe, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
 
@@ -974,7 +1074,7 @@ cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t 
     if (n > 0) {
         FinalizeArgs fa{s.keys,  s.voxels,          n,         group_shift, s.hash_slots, s.hash_capacity,
                         s.hash_max_probe, s.records, nullptr, nullptr};
-        finalize_kernel<<<finalize_grid(n), kFinalizeWarps * 32, 0, stream>>>(fa);
+        launch_finalize(fa, s.encoding, n, stream);
     }
     return scene_build_lights(s, stream, device_status_out);
 }
@@ -985,7 +1085,7 @@ cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_
     if (max_count == 0) return cudaSuccess;
     FinalizeArgs fa{s.keys,  s.voxels,          s.brick_count, s.group_shift, s.hash_slots, s.hash_capacity,
                     s.hash_max_probe, s.records, list,       list_count};
-    finalize_kernel<<<finalize_grid(max_count), kFinalizeWarps * 32, 0, stream>>>(fa);
+    launch_finalize(fa, s.encoding, max_count, stream);
     return cudaGetLastError();
 }
 
@@ -1015,14 +1115,33 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     uint32_t* small = bs.small;
 
     // Light records.
-    LightArgs la{s.keys, s.voxels, s.power, n, group_shift, {s.groups[0], s.groups[1], s.groups[2]},
-                 s.hash_slots, s.hash_capacity, s.hash_max_probe};
+    if (!s.materials || !s.light_codes) return cudaErrorInvalidValue;
+    const bool packed = s.encoding == kEncodingPacked;
+    LightArgs la{s.keys,
+                 s.voxels,
+                 s.power,
+                 n,
+                 group_shift,
+                 {s.groups[0], s.groups[1], s.groups[2]},
+                 {s.origin[0], s.origin[1], s.origin[2]},
+                 s.hash_slots,
+                 s.hash_capacity,
+                 s.hash_max_probe,
+                 s.materials,
+                 s.light_codes};
     uint32_t* d_light_count = s.status + 5;
     uint32_t* lkeys = bs.lo;  // reuse the hash scratch
     uint32_t* lbricks = bs.hi;
     uint32_t* lkeys_alt = bs.home_alt;
     uint32_t* lbricks_alt = bs.order_alt;
-    if (n > 0) light_collect_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+    if (n > 0 && s.lights) {
+        if (packed)
+            light_collect_kernel<kEncodingPacked>
+                <<<blocks_for(32ull * n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+        else
+            light_collect_kernel<kEncodingBlockId>
+                <<<blocks_for(32ull * n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+    }
     uint32_t m = 0;
     CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
@@ -1038,9 +1157,10 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         const uint32_t gx = g % s.groups[0], gy = (g / s.groups[0]) % s.groups[1], gz = g / (s.groups[0] * s.groups[1]);
         GroupFrame f;
         std::memset(&f, 0, sizeof(f));
-        f.origin[0] = (float)(gx * (8u << group_shift));
-        f.origin[1] = (float)(gy * (8u << group_shift));
-        f.origin[2] = (float)(gz * (8u << group_shift));
+        // The group's voxel origin in the scene: (grid origin + group cell * group edge) * 8.
+        const uint32_t cell[3] = {gx, gy, gz};
+        for (int k = 0; k < 3; ++k)
+            f.origin[k] = (float)(8ll * ((int64_t)s.origin[k] + ((int64_t)cell[k] << group_shift)));
         f.rot[0] = f.rot[4] = f.rot[8] = 1.0f;
         frames[g] = f;
     }
@@ -1055,8 +1175,12 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         uint32_t* totals = order;  // m words
         uint32_t* group_start = tmp;
         uint32_t* offsets = tmp2;
-        light_measure_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(
-            la, lbricks, m, counts6, units, reuse);
+        if (packed)
+            light_measure_kernel<kEncodingPacked><<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(
+                la, lbricks, m, counts6, units, reuse);
+        else
+            light_measure_kernel<kEncodingBlockId><<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(
+                la, lbricks, m, counts6, units, reuse);
         light_group_kernel<<<blocks_for(m, kThreads), kThreads, 0, stream>>>(lkeys, m, group_shift, units, totals,
                                                                              group_start);
         uint32_t* d_total = s.status + 6;
@@ -1070,7 +1194,10 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
                           units,        offsets,       group_start,     total_units, s.heap,
                           s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick,
                           reuse,        s.unit_of_brick};
-        light_write_kernel<<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(wa);
+        if (packed)
+            light_write_kernel<kEncodingPacked><<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(wa);
+        else
+            light_write_kernel<kEncodingBlockId><<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(wa);
     } else {
         s.heap_words = 4;
         CX_TRY(alloc(s.heap, s.capacity.heap, 4));

@@ -17,25 +17,51 @@
 
 namespace cx {
 
-constexpr uint32_t kOpaqueBit = 0x8000u;  // block-ID encoding
-constexpr uint32_t kMaterialSlots = 128;  // albedo table rows (material id = value & 0x7F)
+// Block encodings (caelix_record.hlsl:180-212, include/caelix/caelix.h:243-249): which bits of a
+// 16-bit block value make it opaque, the id of a transparent value and where its face bits go.
+struct Encoding
+{
+    uint32_t opaque_mask;  // opaque when (value & opaque_mask) != 0
+    uint32_t id_mask;      // the id of a transparent value
+    uint32_t face_shift;   // its six face bits start here
+};
+__host__ __device__ constexpr Encoding encoding_of(uint32_t e)
+{
+    return e == kEncodingPacked ? Encoding{0xC000u, 0xFFu, 8u} : Encoding{0x8000u, 0x1FFu, 9u};
+}
+// The material table index of a raw block value (BlockMaterialCode): opaque values as they are,
+// transparent ones without their face bits.
+__host__ __device__ __forceinline__ uint32_t material_code(uint32_t v, const Encoding& e)
+{
+    return (v & e.opaque_mask) ? v : (v & e.id_mask);
+}
+
+// The material table on the device: one entry per 16-bit block code, two float4 (albedo rgb, 0;
+// emission rgb, 0), fp32. The light code set: one bit per code whose emission luminance reaches
+// the scene's min_emission.
+constexpr uint32_t kMaterialCodes = 65536;
+constexpr uint32_t kLightCodeWords = kMaterialCodes / 32;
 
 struct EntityView;
 
 // Everything the trace kernels read, passed by value.
 struct SceneView
 {
-    uint32_t grid[3];
+    uint32_t grid[3];     // bricks of the grid per axis from `origin`
     uint32_t group_shift;
     uint32_t groups[3];
     uint32_t brick_count;
+    int32_t origin[3];    // brick key of grid cell 0 (a multiple of the group edge)
+    Encoding enc;
     const uint32_t* records;  // [brick_count][kRecordWords]
     const uint4* hash_slots;  // key_lo, key_hi, record, 0
     uint32_t hash_capacity;
     uint32_t hash_max_probe;
     const uint32_t* bitmap;  // brick occupancy by linear brick index
-    const float* power;      // per-brick emitter power
-    const float* albedo;     // [kMaterialSlots][3]
+    const float* power;      // per-brick emitter power (a factor of the material emission)
+    const float4* materials;  // [kMaterialCodes][2]: albedo, emission
+    const uint32_t* light_codes;  // [kLightCodeWords]: the light code set
+    const int32_t* keys;          // [brick_count][3]: the key of every record
     const uint32_t* heap;    // group light blocks, 16-byte units
     const uint32_t* group_rows;  // [group_count][8]
     const GroupFrame* frames;    // [group_count]
@@ -67,6 +93,7 @@ struct EntityView
     float pos[3];
     uint32_t group_base;  // its first group in the entities' light set
     float sphere[4];      // world centre and radius of a sphere holding its brick grid (inflated)
+    uint32_t id;          // its entity id (the voxel id target's entity word)
 };
 
 // The attribute bit of an entity hit (bits 0..5 face flags, 6..14 cell, 16..31 block: bit 15 is
@@ -80,6 +107,13 @@ constexpr uint32_t kEntityGroupMask = (1u << kEntityShift) - 1u;
 struct DeviceScene
 {
     uint32_t grid[3] = {0, 0, 0};
+    int32_t origin[3] = {0, 0, 0};
+    uint32_t encoding = kEncodingBlockId;
+    // The material table and the light code set the build reads (device, owned by the scene
+    // object that sets them; an entity's bricks use their scene's).
+    const float4* materials = nullptr;
+    const uint32_t* light_codes = nullptr;
+    bool lights = true;  // build the light records and the light tree (the scene's light tree is enabled)
     uint32_t group_shift = 4;
     uint32_t groups[3] = {0, 0, 0};
     uint32_t group_count = 0;
@@ -97,7 +131,6 @@ struct DeviceScene
     uint32_t* records = nullptr;
     uint4* hash_slots = nullptr;
     uint32_t* bitmap = nullptr;
-    float* albedo = nullptr;
     uint32_t* heap = nullptr;
     uint32_t* group_rows = nullptr;
     GroupFrame* frames = nullptr;
@@ -120,23 +153,23 @@ struct DeviceScene
     // Element capacities of the buffers above: a rebuild reallocates a buffer only to grow it.
     struct
     {
-        uint64_t keys, voxels, power, albedo, scratch, hash_slots, bitmap, records, group_rows, light_headers,
+        uint64_t keys, voxels, power, scratch, hash_slots, bitmap, records, group_rows, light_headers,
             light_group, light_entry, light_brick, frames, heap, heap_prev, unit_of_brick, unit_of_brick_prev;
     } capacity{};
 };
 
-// Builds the device scene from host bricks (keys in increasing linear brick index, every
-// coordinate in [0, grid)), voxels (512 block values per brick), per-brick power and the albedo
-// table (kMaterialSlots x 3). Synchronous on `stream`. Returns the first CUDA error.
-cudaError_t scene_build(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
-                        const int32_t* keys, const uint16_t* voxels, const float* power, const float* albedo,
-                        cudaStream_t stream, uint32_t* device_status_out);
-// The two halves of scene_build for inputs produced on the device: scene_alloc_inputs sizes
-// s.keys, s.voxels, s.power, s.albedo for n bricks (and clears the status words); the caller fills
-// them (keys in increasing linear brick index); scene_build_device builds everything else.
+// The grid of a set of brick keys: `origin` = the smallest key per axis rounded down to a multiple
+// of the group edge, `grid` = the bricks from there to the largest key. False when the grid is
+// larger than the tables allow (more than 2^32 cells once rounded to whole groups).
+bool scene_grid(const int32_t key_min[3], const int32_t key_max[3], uint32_t group_shift, int32_t origin[3],
+                uint32_t grid[3]);
+// Scene build for inputs produced on the device: scene_alloc_inputs sizes s.keys, s.voxels,
+// s.power for n bricks (and clears the status words); the caller fills them (keys in increasing
+// linear brick index of the grid), sets s.encoding, s.materials and s.light_codes;
+// scene_build_device builds everything else.
 cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream);
-cudaError_t scene_build_device(DeviceScene& s, const uint32_t grid[3], uint32_t group_shift, uint32_t brick_count,
-                               cudaStream_t stream, uint32_t* device_status_out);
+cudaError_t scene_build_device(DeviceScene& s, const int32_t origin[3], const uint32_t grid[3], uint32_t group_shift,
+                               uint32_t brick_count, cudaStream_t stream, uint32_t* device_status_out);
 // The parts of a rebuild whose brick set is unchanged (same keys, same order): the records of the
 // bricks list[0 .. *list_count) (device; at most max_count) finalized again from s.voxels, then
 // (scene_build_lights) the light records and the light tree. Synchronous.
@@ -157,13 +190,14 @@ cudaError_t staging_scatter(const uint16_t* src, const uint32_t* src_index, cons
 // block values of slot moves[2j + 1] (moves: device, no destination also a source).
 cudaError_t staging_move(int32_t* stage_keys, uint16_t* stage_voxels, const uint32_t* moves, uint32_t count,
                          cudaStream_t stream);
-// The staging slots in increasing linear brick index of `grid`, gathered into the scene's input
-// arrays (power zero when `power` is null). `scratch`: staging_sort_words(n) words.
+// The staging slots in increasing linear brick index of the grid (origin, grid), gathered into the
+// scene's input arrays (power zero when `power` is null). `scratch`: staging_sort_words(n) words.
 uint64_t staging_sort_words(uint32_t n);
 // Also writes record_of_slot[slot] = the slot's brick index in the scene.
 cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
-                           uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
-                           uint16_t* voxels, float* power, uint32_t* record_of_slot, cudaStream_t stream);
+                           uint32_t n, const int32_t origin[3], const uint32_t grid[3], uint32_t* scratch,
+                           uint32_t* status, int32_t* keys, uint16_t* voxels, float* power, uint32_t* record_of_slot,
+                           cudaStream_t stream);
 // An edit of a built scene that adds no brick: the `count` edited slots (slots[i], with power
 // power[i], both device) copied to their bricks in the scene (values and power), and the list of
 // the bricks whose records depend on them (each edited brick and its six neighbours, each once)

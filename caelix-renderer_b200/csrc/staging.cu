@@ -39,13 +39,16 @@ __global__ void __launch_bounds__(kStageThreads)
     if (w < 3) keys[3ull * dst + w] = keys[3ull * src + w];
 }
 
+// The linear index of a slot's brick in the grid (origin o, extents gx, gy): below 2^32 for every
+// grid the flush accepts.
 __global__ void __launch_bounds__(kStageThreads)
-    staging_linear_kernel(const int32_t* __restrict__ keys, uint32_t n, uint32_t gx, uint32_t gy,
-                          uint32_t* __restrict__ lin)
+    staging_linear_kernel(const int32_t* __restrict__ keys, uint32_t n, int32_t ox, int32_t oy, int32_t oz,
+                          uint32_t gx, uint32_t gy, uint32_t* __restrict__ lin)
 {
     const uint32_t s = blockIdx.x * kStageThreads + threadIdx.x;
     if (s >= n) return;
-    lin[s] = (uint32_t)keys[3 * s] + gx * ((uint32_t)keys[3 * s + 1] + gy * (uint32_t)keys[3 * s + 2]);
+    lin[s] = (uint32_t)(keys[3 * s] - ox) +
+             gx * ((uint32_t)(keys[3 * s + 1] - oy) + gy * (uint32_t)(keys[3 * s + 2] - oz));
 }
 
 __global__ void __launch_bounds__(kStageThreads)
@@ -125,8 +128,9 @@ uint64_t staging_sort_words(uint32_t n)
 }
 
 cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
-                           uint32_t n, const uint32_t grid[3], uint32_t* scratch, uint32_t* status, int32_t* keys,
-                           uint16_t* voxels, float* power, uint32_t* record_of_slot, cudaStream_t stream)
+                           uint32_t n, const int32_t origin[3], const uint32_t grid[3], uint32_t* scratch,
+                           uint32_t* status, int32_t* keys, uint16_t* voxels, float* power, uint32_t* record_of_slot,
+                           cudaStream_t stream)
 {
     if (n == 0) return cudaSuccess;
     uint32_t* lin = scratch;
@@ -134,7 +138,8 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
     uint32_t* lin_alt = scratch + 2ull * n;
     uint32_t* order_alt = scratch + 3ull * n;
     uint32_t* sortw = scratch + 4ull * n;
-    staging_linear_kernel<<<blocks(n), kStageThreads, 0, stream>>>(stage_keys, n, grid[0], grid[1], lin);
+    staging_linear_kernel<<<blocks(n), kStageThreads, 0, stream>>>(stage_keys, n, origin[0], origin[1], origin[2],
+                                                                    grid[0], grid[1], lin);
     CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n), stream));
     radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, current_sm_count() * 4), stream);
     // A stable sort of the linear indices (unique: one slot per key), values = the slots.

@@ -18,7 +18,11 @@ __device__ __noinline__ void next_event(const SceneView& s, const float x[3], co
     if (!nee_prepare(s, x, n, light_rng, r)) return;
     ++rays.shadow;
     const Hit h = trace_scene(s, x, r.dir, 0.0f, r.t_max);
-    if (!h.hit) out[0] = out[1] = out[2] = r.value;
+    if (!h.hit) {
+        out[0] = r.value[0];
+        out[1] = r.value[1];
+        out[2] = r.value[2];
+    }
 }
 
 __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t px, uint32_t py, uint32_t seed,
@@ -39,10 +43,12 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
     for (int k = 0; k < 3; ++k) d[k] = d[k] * inv_len;
     ++rays.primary;
     const Hit primary = trace_scene(s, P.position, d, 0.0f, kRayTMax);
+    if (P.voxel_id && seed == P.frame_seed)
+        write_voxel_id<true>(s, P, py * P.width + px, primary.hit, primary.t, primary.attrib, primary.record, primary.group);
     if (!primary.hit) return;
     uint32_t rng = init_random(px, py, seed);
     uint32_t light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
-    float a0[3], e0, org[3], dir[3];
+    float a0[3], e0[3], org[3], dir[3];
     shade(s, primary, P.position, d, rng, a0, e0, org, dir);
     float seg_n[3] = {primary.normal[0], primary.normal[1], primary.normal[2]};
     float radiance[3] = {0.0f, 0.0f, 0.0f};
@@ -61,13 +67,14 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
         ++rays.bounce;
         const Hit h = trace_scene(s, org, dir, 0.0f, kBounceTMax);
         if (!h.hit) break;
-        float al[3], em, o2[3], d2[3];
+        float al[3], em[3], o2[3], d2[3];
         shade(s, h, org, dir, rng, al, em, o2, d2);
         bounce_index += 1;
         float ew = 1.0f;
-        if (segment_light != 0u && em > 0.0f) ew = lamp_hit_weight(s, segment_light, h, org, dir, seg_n);
+        if (segment_light != 0u && (em[0] > 0.0f || em[1] > 0.0f || em[2] > 0.0f))
+            ew = lamp_hit_weight(s, segment_light, h, org, dir, seg_n);
 #pragma unroll
-        for (int k = 0; k < 3; ++k) radiance[k] += em * (throughput[k] * ew);
+        for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
 #pragma unroll
         for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
         segment_light = 0u;
@@ -94,7 +101,7 @@ __device__ void trace_pixel(const SceneView& s, const TraceParams& P, uint32_t p
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float sr = hmin(bad ? 0.0f : radiance[k], 65504.0f);
-        rgb[k] = e0 + a0[k] * sr;
+        rgb[k] = e0[k] + a0[k] * sr;
     }
 }
 

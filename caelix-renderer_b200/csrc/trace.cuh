@@ -25,6 +25,8 @@ struct TraceParams
     uint32_t bounce_count;  // stochastic bounces after the primary hit
     uint32_t frame_seed;
     uint32_t light_nee;  // 1: light-tree NEE with MIS
+    uint32_t* voxel_id;   // optional: width * height uint2, the camera ray's first hit (first sample)
+    float voxel_id_tmax;  // hits farther than this are misses of the voxel id (0: no limit)
 };
 
 // radiance: width * height fp32 RGB; ray_counts (may be null): u64 primary, bounce, shadow rays,
@@ -33,7 +35,7 @@ cudaError_t trace_launch(const SceneView& s, const TraceParams& p, float* radian
                          cudaStream_t stream);
 
 // The adjoint of a frame (backward.cu): d_radiance = dL/d(radiance), width * height RGB;
-// d_albedo (kMaterialSlots x 3) and d_power (one per brick, the scene's order) are accumulated
+// d_albedo (kMaterialCodes x 3, per material code) and d_power (one per brick, the scene's order) are accumulated
 // into (zero them first); image (may be null) receives the forward radiance; ray_counts (may be
 // null) the rays of the recording pass. `memory`: adjoint_bytes(p, wave_capacity) bytes of device
 // memory, 256-aligned (wave_capacity 0 = one path per pixel).
@@ -74,7 +76,8 @@ struct WaveBuffers
     float4* throughput = nullptr;
     float4* radiance = nullptr;
     float4* seg_n = nullptr;
-    float4* a0e0 = nullptr;  // primary albedo, primary emission
+    float4* a0 = nullptr;    // primary albedo
+    float4* e0 = nullptr;    // primary emission
     float4* sdir = nullptr;  // pending shadow ray: direction, t_max
     float4* sadd = nullptr;  // pending shadow contribution
     uint4* hit = nullptr;    // t bits, attrib (0 = miss), record, group
@@ -96,7 +99,7 @@ struct WaveAdjoint
 {
     const float* d_radiance;
     float* sample_radiance;
-    float* d_albedo;  // [kMaterialSlots][3]
+    float* d_albedo;  // [kMaterialCodes][3]
     float* d_power;   // [brick_count]
 };
 

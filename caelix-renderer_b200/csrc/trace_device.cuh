@@ -13,8 +13,8 @@
 //                      caelix_random.hlsl, common/caelix_frame.hlsl:164-171
 // in the configuration of the benchmark scenes: opaque voxels with a Lambertian lobe (metallic 0,
 // smoothness 0), light-tree NEE with MIS over the world's and the entities' light trees, no sun,
-// black sky, no fog, bounce NEE probability 1. Emission of an opaque voxel = its brick's emitter power on every
-// channel. Every float operation is one IEEE fp32 operation in the reference's order (the library
+// black sky, no fog, bounce NEE probability 1. A voxel's albedo is its material code's table entry;
+// its emission is the entry's emission times its brick's emitter power. Every float operation is one IEEE fp32 operation in the reference's order (the library
 // is built with --fmad=false); sin/cos of the unit-vector draw use this library's Cody-Waite +
 // Taylor polynomials, normalize is v * (1 / sqrt(dot(v, v))).
 #pragma once
@@ -23,6 +23,7 @@
 #include "cx_device.cuh"
 #include "scene.cuh"
 #include "scene_device.cuh"
+#include "trace.cuh"
 
 namespace cx {
 
@@ -116,7 +117,7 @@ __device__ __forceinline__ void vrt_step(int cell[3], const float t_start[3], co
 }
 
 __device__ __forceinline__ float brick_ray(const uint32_t* __restrict__ rec, const float entry[3], const float dir[3],
-                                           float entry_t, uint32_t entry_coarse, uint32_t& attrib)
+                                           float entry_t, uint32_t entry_coarse, const Encoding& enc, uint32_t& attrib)
 {
     float inv[3], t_start[3], origin[3];
     int cell[3], prev[3];
@@ -164,8 +165,8 @@ __device__ __forceinline__ float brick_ray(const uint32_t* __restrict__ rec, con
                 nf = ((dir[0] > 0.0f ? 2u : 1u) & x_use) | ((dir[1] > 0.0f ? 8u : 4u) & y_use) |
                      ((dir[2] > 0.0f ? 32u : 16u) & z_use);
             }
-            bool term = (blk & kOpaqueBit) != 0;
-            if (!term) term = (step == 0 && entry_t == 0.0f) ? false : ((((blk >> 9) & 63u) & nf) != 0);
+            bool term = (blk & enc.opaque_mask) != 0;
+            if (!term) term = (step == 0 && entry_t == 0.0f) ? false : ((((blk >> enc.face_shift) & 63u) & nf) != 0);
             if (term) {
                 attrib = (blk << 16) | (((uint32_t)cell[0] | ((uint32_t)cell[1] << 3) | ((uint32_t)cell[2] << 6)) << 6) | nf;
                 return entry_t + T;
@@ -180,7 +181,8 @@ __device__ __forceinline__ float brick_ray(const uint32_t* __restrict__ rec, con
 }
 
 __device__ __forceinline__ float brick_primitive(const uint32_t* __restrict__ rec, const float o[3], const float d[3],
-                                                 float t_current, const float bo[3], uint32_t& attrib)
+                                                 float t_current, const float bo[3], const Encoding& enc,
+                                                 uint32_t& attrib)
 {
     const uint2 info = __ldg(reinterpret_cast<const uint2*>(rec));
     const uint32_t tb = info.y;
@@ -210,7 +212,7 @@ __device__ __forceinline__ float brick_primitive(const uint32_t* __restrict__ re
     if (largest == tmin[0]) nf = d[0] > 0.0f ? 2u : 1u;
     else if (largest == tmin[1]) nf = d[1] > 0.0f ? 8u : 4u;
     else nf = d[2] > 0.0f ? 32u : 16u;
-    return brick_ray(rec, entry, d, t, (nf << 26) | ((info.x >> 16) & 0xFFu), attrib);
+    return brick_ray(rec, entry, d, t, (nf << 26) | ((info.x >> 16) & 0xFFu), enc, attrib);
 }
 
 struct Hit
@@ -224,7 +226,8 @@ struct Hit
     float object_hit[3];
 };
 
-// Closest hit over the bricks (front-to-back DDA over the brick grid).
+// Closest hit over the bricks (front-to-back DDA over the brick grid). Cell c of axis k is brick
+// key origin[k] + c, voxels [8 (origin[k] + c), 8 (origin[k] + c + 1)).
 __device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
 {
     Hit h;
@@ -233,8 +236,8 @@ __device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         inv[k] = safe_inv_axis(d[k]);
-        const float t0 = (0.0f - o[k]) * inv[k];
-        const float t1 = ((float)(8u * s.grid[k]) - o[k]) * inv[k];
+        const float t0 = ((float)(8 * s.origin[k]) - o[k]) * inv[k];
+        const float t1 = ((float)(8 * (s.origin[k] + (int)s.grid[k])) - o[k]) * inv[k];
         tnear = hmax(tnear, hmin(t0, t1));
         tfar = hmin(tfar, hmax(t0, t1));
     }
@@ -245,7 +248,7 @@ __device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float p = o[k] + d[k] * t_enter;
-        int c = (int)floorf(p * 0.125f);
+        int c = (int)floorf(p * 0.125f) - s.origin[k];
         c = c < 0 ? 0 : c;
         c = c > (int)s.grid[k] - 1 ? (int)s.grid[k] - 1 : c;
         cell[k] = c;
@@ -255,11 +258,13 @@ __device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[
     for (uint32_t it = 0; it < limit; ++it) {
         const uint64_t lin = (uint64_t)cell[0] + s.grid[0] * ((uint64_t)cell[1] + (uint64_t)s.grid[1] * cell[2]);
         if ((__ldg(s.bitmap + (lin >> 5)) >> (lin & 31)) & 1u) {
-            const uint32_t r = hash_lookup(s.hash_slots, s.hash_capacity, s.hash_max_probe, cell[0], cell[1], cell[2]);
+            const int32_t key[3] = {s.origin[0] + cell[0], s.origin[1] + cell[1], s.origin[2] + cell[2]};
+            const uint32_t r = hash_lookup(s.hash_slots, s.hash_capacity, s.hash_max_probe, key[0], key[1], key[2]);
             if (r != 0xFFFFFFFFu) {
-                const float bo[3] = {(float)(cell[0] * 8), (float)(cell[1] * 8), (float)(cell[2] * 8)};
+                const float bo[3] = {(float)(key[0] * 8), (float)(key[1] * 8), (float)(key[2] * 8)};
                 uint32_t attrib;
-                const float t = brick_primitive(s.records + (uint64_t)r * kRecordWords, o, d, tmax_ray, bo, attrib);
+                const float t =
+                    brick_primitive(s.records + (uint64_t)r * kRecordWords, o, d, tmax_ray, bo, s.enc, attrib);
                 if (attrib != 0u && t >= tmin_ray && t < tmax_ray) {
                     h.hit = true;
                     h.t = t;
@@ -280,7 +285,8 @@ __device__ __forceinline__ Hit trace_ray_body(const SceneView& s, const float o[
         }
         float tn[3];
 #pragma unroll
-        for (int k = 0; k < 3; ++k) tn[k] = ((float)((cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
+        for (int k = 0; k < 3; ++k)
+            tn[k] = ((float)((s.origin[k] + cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
         // The axis of the nearest boundary (the first of equals), stepped with selects.
         int axis = 0;
         float t_next = tn[0];
@@ -407,6 +413,55 @@ __device__ __noinline__ Hit trace_scene(const SceneView& s, const float o[3], co
     Hit h = trace_ray(s, o, d, tmin_ray, tmax_ray);
     if (s.entity_count) trace_entities(s, o, d, tmin_ray, tmax_ray, h);
     return h;
+}
+
+// ---- the voxel id target (shaders/render/caelix_scene_trace.hlsl:171-200) ----
+__device__ __forceinline__ uint32_t hash_avalanche(uint32_t v)
+{
+    v ^= v >> 16;
+    v *= 0x7FEB352Du;
+    v ^= v >> 15;
+    v *= 0x846CA68Bu;
+    v ^= v >> 16;
+    return v;
+}
+
+__device__ __forceinline__ uint32_t voxel_id_word(uint32_t seed, uint32_t entity, const int32_t v[3])
+{
+    uint32_t h = hash_avalanche(seed ^ entity);
+    h = hash_avalanche(h ^ (uint32_t)v[0]);
+    h = hash_avalanche(h ^ (uint32_t)v[1]);
+    h = hash_avalanche(h ^ (uint32_t)v[2]);
+    return h == 0xFFFFFFFFu ? 0xFFFFFFFEu : h;
+}
+
+// The voxel id of a hit: two hashes of (entity id, entity-local voxel = 8 brick key + DDA cell).
+template <bool kEntities>
+__device__ __forceinline__ uint2 voxel_id_of(const SceneView& s, uint32_t attrib, uint32_t record, uint32_t group)
+{
+    uint32_t entity = 0;
+    const int32_t* keys = s.keys;
+    if (kEntities && (attrib & kEntityHit)) {
+        const EntityView& E = s.entities[group >> kEntityShift];
+        entity = __ldg(&E.id);
+        keys = E.scene.keys;
+    }
+    const uint32_t cell = (attrib >> 6) & 0x1FFu;
+    int32_t v[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) v[k] = __ldg(keys + 3ull * record + k) * 8 + (int32_t)((cell >> (3 * k)) & 7u);
+    return make_uint2(voxel_id_word(0x9E3779B9u, entity, v), voxel_id_word(0x85EBCA6Bu, entity, v));
+}
+
+// Writes pixel `item`'s voxel id (VoxelIdOrMiss): the hit's, or the miss value for a miss and for a
+// hit farther than the limit.
+template <bool kEntities>
+__device__ __forceinline__ void write_voxel_id(const SceneView& s, const TraceParams& P, uint32_t item, bool hit, float t,
+                                               uint32_t attrib, uint32_t record, uint32_t group)
+{
+    uint2 id = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
+    if (hit && (P.voxel_id_tmax <= 0.0f || t <= P.voxel_id_tmax)) id = voxel_id_of<kEntities>(s, attrib, record, group);
+    reinterpret_cast<uint2*>(P.voxel_id)[item] = id;
 }
 
 // ---- light tree ----
@@ -801,14 +856,16 @@ __device__ __forceinline__ bool light_sample(const SceneView& s, const float x[3
     return true;
 }
 
-// LightTreeFindLightFace: a light voxel is an opaque voxel of a brick with a light record.
+// LightTreeFindLightFace (caelix_light_tree.hlsl:853-935): the face of a voxel whose material code
+// is in the light code set, in a brick with a light record.
 __device__ __noinline__ bool find_light_face(const SceneView& s, const float x[3], uint32_t group, const uint32_t v[3], uint32_t face,
                                 uint32_t block_value, uint32_t& entry_out, uint32_t& leaf_out, float& in_brick)
 {
     entry_out = kNone;
     leaf_out = kNone;
     in_brick = 0.0f;
-    if (!(block_value & kOpaqueBit) || face > 5) return false;
+    const uint32_t code = material_code(block_value, s.enc);
+    if (!((__ldg(s.light_codes + (code >> 5)) >> (code & 31)) & 1u) || face > 5) return false;
     const uint2 row = __ldg(reinterpret_cast<const uint2*>(s.group_rows + 8ull * group));
     if (row.y == 0) return false;
     const uint32_t* block = s.heap + 4ull * row.x;
@@ -921,10 +978,24 @@ struct ShadowRay
 {
     float dir[3];
     float t_max;
-    float value;       // the contribution on every channel if the ray is unoccluded
-    float dvalue_de;   // d value / d (the lamp brick's power), the sampling factors held fixed
-    uint32_t brick;    // the lamp brick (kNone when its emission is not its power)
+    float value[3];      // the contribution if the ray is unoccluded
+    float dvalue_de[3];  // d value / d (the lamp brick's power), the sampling factors held fixed
+    uint32_t brick;      // the lamp brick of the world (kNone for an entity's lamp)
 };
+
+// The material table entry of a block value: albedo and emission (without the brick's power).
+__device__ __forceinline__ void material_of(const SceneView& s, uint32_t block, float albedo[3], float emission[3])
+{
+    const uint32_t code = material_code(block, s.enc);
+    const float4 a = __ldg(s.materials + 2ull * code);
+    const float4 e = __ldg(s.materials + 2ull * code + 1);
+    albedo[0] = a.x;
+    albedo[1] = a.y;
+    albedo[2] = a.z;
+    emission[0] = e.x;
+    emission[1] = e.y;
+    emission[2] = e.z;
+}
 
 template <bool kEntities = true>
 __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3], const float n[3], uint32_t& light_rng,
@@ -946,9 +1017,15 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
     const SceneView& L = (kEntities && p.tree != 0) ? *s.dyn : s;
     const uint2 row = __ldg(reinterpret_cast<const uint2*>(L.group_rows + 8ull * p.group));
     const uint32_t brick = __ldg(L.heap + 4ull * row.x + 4 + 4 * p.entry + 1);
-    const float e = (p.block & kOpaqueBit) ? __ldg(L.power + brick) : 0.0f;
-    const float contribution = e * scale;  // equal on the three channels
-    const float lum = contribution * 0.2126f + contribution * 0.7152f + contribution * 0.0722f;
+    // LampEmission: the table's emission of the lamp voxel's code (the scene's table, shared by its
+    // entities) times its brick's power.
+    float al[3], em[3];
+    material_of(s, p.block, al, em);
+    const float P = __ldg(L.power + brick);
+    float contribution[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) contribution[c] = (em[c] * P) * scale;
+    const float lum = contribution[0] * 0.2126f + contribution[1] * 0.7152f + contribution[2] * 0.0722f;
     const float w_lamp = lum * hmax(0.05f, 1.0f);
     const float w_sum = 0.0f + w_lamp;
     if (!(w_sum > 0.0f)) return false;
@@ -959,9 +1036,12 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
     r.dir[2] = w[2];
     r.t_max = t_max;
     const float k = w_sum / w_lamp;
-    r.value = contribution * k;
-    r.dvalue_de = scale * k;
-    r.brick = ((p.block & kOpaqueBit) && (!kEntities || p.tree == 0)) ? brick : kNone;  // a world brick's power
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        r.value[c] = contribution[c] * k;
+        r.dvalue_de[c] = em[c] * (scale * k);
+    }
+    r.brick = (!kEntities || p.tree == 0) ? brick : kNone;  // a world brick's power
     return true;
 }
 
@@ -997,21 +1077,23 @@ __device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segme
     return mis_weight(p_area, seg_n, dir, h.t, cos_l, false);
 }
 
+// The vertex of a hit: its material (the scene's table; an entity's bricks share it), its emission
+// (the table's times the brick's power) and the Lambertian bounce.
 template <bool kEntities = true>
 __device__ __forceinline__ void shade(const SceneView& s, const Hit& h, const float ray_o[3], const float ray_d[3],
-                                      uint32_t& rng, float albedo[3], float& emission, float origin[3], float dir[3])
+                                      uint32_t& rng, float albedo[3], float emission[3], float origin[3], float dir[3])
 {
     const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
+    material_of(s, block, albedo, emission);
+    float P;
     if (kEntities && (h.attrib & kEntityHit)) {  // an entity brick's power
         const float* pw = s.entities[h.group >> kEntityShift].scene.power;
-        emission = ((block & kOpaqueBit) && pw) ? __ldg(pw + h.record) : 0.0f;
+        P = pw ? __ldg(pw + h.record) : 0.0f;
     } else {
-        emission = (block & kOpaqueBit) ? __ldg(s.power + h.record) : 0.0f;
+        P = __ldg(s.power + h.record);
     }
-    const float* a = s.albedo + 3 * (block & (kMaterialSlots - 1));
-    albedo[0] = __ldg(a);
-    albedo[1] = __ldg(a + 1);
-    albedo[2] = __ldg(a + 2);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) emission[c] *= P;
     (void)random01(rng);  // the lobe draw (specular chance 0)
     float u[3];
     random_unit_vector(rng, u);

@@ -64,7 +64,7 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
     uint32_t bounce_index = 0, segment_light = 0;
     bool alive_after_shadow = false;
     uint32_t rng = 0, light_rng = 0;
-    float acc[3], e0 = 0.0f, a0[3], radiance[3], throughput[3], seg_n[3];
+    float acc[3], e0[3] = {0.0f, 0.0f, 0.0f}, a0[3], radiance[3], throughput[3], seg_n[3];
     float org[3], dir[3], sdir[3], stmax = 0.0f, sadd[3];
     Counters rays = {0, 0, 0};  // of `view`, not yet in s_rays
     bool exhausted = false;     // warp-uniform: the work counter has passed the last item
@@ -103,7 +103,7 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             const float sr = hmin(bad ? 0.0f : radiance[k], 65504.0f);
-            acc[k] += e0 + a0[k] * sr;
+            acc[k] += e0[k] + a0[k] * sr;
         }
         sp += 1;
         if (sp < V->params.spp) {
@@ -190,6 +190,8 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
             ray_d[k] = phase == kPhaseShadow ? sdir[k] : dir[k];
         }
         const Hit h = trace_ray(S, ray_o, ray_d, 0.0f, t_max);
+        if (phase == kPhasePrimary && sp == 0 && P.voxel_id)
+            write_voxel_id<false>(S, P, py * P.width + px, h.hit, h.t, h.attrib, h.record, h.group);
 
         if (phase == kPhaseShadow) {
             if (!h.hit) {
@@ -203,9 +205,8 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
         const bool primary = phase == kPhasePrimary;
         if (!h.hit) {
             if (primary) {  // the sample's value is 0
-                e0 = 0.0f;
 #pragma unroll
-                for (int k = 0; k < 3; ++k) a0[k] = radiance[k] = 0.0f;
+                for (int k = 0; k < 3; ++k) e0[k] = a0[k] = radiance[k] = 0.0f;
             }
             finish_sample();
             continue;
@@ -215,14 +216,14 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
             rng = init_random(px, py, seed);
             light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
         }
-        float al[3], em, o2[3], d2[3];
+        float al[3], em[3], o2[3], d2[3];
         shade<false>(S, h, org, dir, rng, al, em, o2, d2);  // batched scenes have no entities
         bool nee_now;
         if (primary) {
-            e0 = em;
             const float t0 = 1.0f / hmax(0.001f, 1.0f);
 #pragma unroll
             for (int k = 0; k < 3; ++k) {
+                e0[k] = em[k];
                 a0[k] = al[k];
                 radiance[k] = 0.0f;
                 throughput[k] = t0;
@@ -233,14 +234,14 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
         } else {
             bounce_index += 1;
             float ew = 1.0f;
-            if (segment_light != 0u && em > 0.0f) {
+            if (segment_light != 0u && (em[0] > 0.0f || em[1] > 0.0f || em[2] > 0.0f)) {
                 float n_prev[3];
 #pragma unroll
                 for (int k = 0; k < 3; ++k) n_prev[k] = seg_n[k];
                 ew = lamp_hit_weight(S, segment_light, h, ray_o, ray_d, n_prev);
             }
 #pragma unroll
-            for (int k = 0; k < 3; ++k) radiance[k] += em * (throughput[k] * ew);
+            for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
 #pragma unroll
             for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
             segment_light = 0u;
@@ -255,7 +256,7 @@ __global__ void __launch_bounds__(kBatchThreads, CX_BATCH_MIN_BLOCKS) trace_batc
 #pragma unroll
                 for (int k = 0; k < 3; ++k) {
                     sdir[k] = r.dir[k];
-                    sadd[k] = r.value * throughput[k];
+                    sadd[k] = r.value[k] * throughput[k];
                 }
                 stmax = r.t_max;
             }

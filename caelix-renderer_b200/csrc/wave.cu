@@ -160,10 +160,35 @@ enum : int
     kShadeReplay = 2,
 };
 
-__device__ __forceinline__ float gsum3(const float G[3], const float t[3], float s)
+// sum_c G[c] (t[c] s) e[c]: the power gradient of an emission e * P gathered with throughput t and
+// weight s (e the material emission without the power).
+__device__ __forceinline__ float gsum3(const float G[3], const float t[3], float s, const float e[3])
 {
-    return G[0] * (t[0] * s) + G[1] * (t[1] * s) + G[2] * (t[2] * s);
+    return G[0] * ((t[0] * s) * e[0]) + G[1] * ((t[1] * s) * e[1]) + G[2] * ((t[2] * s) * e[2]);
 }
+
+// The replay's albedo gradients per material code: a CTA sums them in shared memory, in a table of
+// kAlbedoCache entries indexed by the code's low bits (the first code to reach an entry owns it; a
+// code whose entry another code owns goes to global memory directly), added to the global
+// gradients once at the end of the CTA.
+constexpr uint32_t kAlbedoCache = 128;
+struct AlbedoCache
+{
+    uint32_t* tag;
+    float* sum;
+    float* global;
+    __device__ __forceinline__ void add(uint32_t code, uint32_t c, float v)
+    {
+        const uint32_t e = code & (kAlbedoCache - 1u);
+        uint32_t owner = tag[e];
+        if (owner == kNone) {
+            const uint32_t old = atomicCAS(tag + e, kNone, code);
+            owner = old == kNone ? code : old;
+        }
+        if (owner == code) atomicAdd(sum + 3 * e + c, v);
+        else atomicAdd(global + 3ull * code + c, v);
+    }
+};
 
 // kMinBlocks CTAs of 128 threads per SM: 5 (96 registers, few spills) for a scene whose records
 // stay in L2, 8 (64 registers) where the descent and the record loads go to HBM and more warps
@@ -175,9 +200,12 @@ template <int kMode, int kMinBlocks, bool kEntities>
 __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     wave_shade_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity, const WaveAdjoint adj)
 {
-    __shared__ float s_albedo[kMode == kShadeReplay ? kMaterialSlots * 3 : 1];
+    __shared__ float s_albedo[kMode == kShadeReplay ? kAlbedoCache * 3 : 1];
+    __shared__ uint32_t s_tag[kMode == kShadeReplay ? kAlbedoCache : 1];
+    AlbedoCache cache{s_tag, s_albedo, adj.d_albedo};
     if (kMode == kShadeReplay) {
-        for (uint32_t i = threadIdx.x; i < kMaterialSlots * 3; i += kWaveThreads) s_albedo[i] = 0.0f;
+        for (uint32_t i = threadIdx.x; i < kAlbedoCache * 3; i += kWaveThreads) s_albedo[i] = 0.0f;
+        for (uint32_t i = threadIdx.x; i < kAlbedoCache; i += kWaveThreads) s_tag[i] = kNone;
         __syncthreads();
     }
     const uint32_t n = *(volatile uint32_t*)&b.counts[2 * parity + 1];
@@ -227,16 +255,21 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                 R[2] = r4.z;
             }
             bool finish = true, zero = false;
-            float e0 = 0.0f, a0[3] = {0.0f, 0.0f, 0.0f};
+            float e0[3] = {0.0f, 0.0f, 0.0f}, a0[3] = {0.0f, 0.0f, 0.0f};
             if (!primary) {
-                const float4 a4 = b.a0e0[slot];
+                const float4 a4 = b.a0[slot];
+                const float4 e4 = b.e0[slot];
                 a0[0] = a4.x;
                 a0[1] = a4.y;
                 a0[2] = a4.z;
-                e0 = a4.w;
+                e0[0] = e4.x;
+                e0[1] = e4.y;
+                e0[2] = e4.z;
             }
             if (f & kFlagExt) {
                 const uint4 hw = b.hit[slot];
+                if (kMode != kShadeReplay && primary && sp == 0 && P.voxel_id)
+                    write_voxel_id<kEntities>(S, P, item, hw.y != 0u, __uint_as_float(hw.x), hw.y, hw.z, hw.w);
                 const float4 o4 = b.org[slot];
                 const float4 d4 = b.dir[slot];
                 const float org[3] = {o4.x, o4.y, o4.z};
@@ -274,14 +307,21 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                     }
                     float tp[3], seg_n[3];
                     uint32_t bounce_index, seg_light;
-                    float al[3], em, o2[3], d2[3];
+                    float al[3], em[3], o2[3], d2[3];
                     shade<kEntities>(S, h, org, dir, rng, al, em, o2, d2);
+                    const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
+                    // The replay's power gradients need the material emission without the power.
+                    float me[3] = {0.0f, 0.0f, 0.0f};
+                    if (kMode == kShadeReplay) {
+                        float ma[3];
+                        material_of(S, block, ma, me);
+                    }
                     bool nee_now;
                     if (primary) {
-                        e0 = em;
                         const float t0 = 1.0f / hmax(0.001f, 1.0f);
 #pragma unroll
                         for (int k = 0; k < 3; ++k) {
+                            e0[k] = em[k];
                             a0[k] = al[k];
                             rad[k] = 0.0f;
                             tp[k] = t0;
@@ -298,19 +338,19 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                                 R[k] = rs[k];
                                 bad |= isnan(R[k]) || isinf(R[k]);
                             }
-                            const uint32_t block0 = (h.attrib >> 16) & 0xFFFFu;
-                            float* ga = s_albedo + 3 * (block0 & (kMaterialSlots - 1));
+                            const uint32_t code0 = material_code(block, S.enc);
                             float g[3];
                             bool any = false;
 #pragma unroll
                             for (int k = 0; k < 3; ++k) {
                                 g[k] = adj.d_radiance[3ull * item + k] / (float)P.spp;
                                 const float sr = hmin(bad ? 0.0f : R[k], 65504.0f);
-                                atomicAdd(ga + k, g[k] * sr);
+                                cache.add(code0, k, g[k] * sr);
                                 G[k] = (!bad && R[k] <= 65504.0f) ? g[k] * a0[k] : 0.0f;
                                 any |= G[k] != 0.0f;
                             }
-                            if ((block0 & kOpaqueBit) && !(h.attrib & kEntityHit)) atomicAdd(adj.d_power + h.record, g[0] + g[1] + g[2]);
+                            if (!(h.attrib & kEntityHit))
+                                atomicAdd(adj.d_power + h.record, g[0] * me[0] + g[1] * me[1] + g[2] * me[2]);
                             if (!any) nee_now = false, bounce_index = P.bounce_count + 1u;  // nothing flows back
                         }
                     } else {
@@ -325,17 +365,17 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                         seg_light = (f & kFlagSegLight) ? 3u : 0u;
                         bounce_index = (f & kFlagBounce) + 1u;
                         float ew = 1.0f;
-                        if (seg_light != 0u && em > 0.0f) ew = lamp_hit_weight(S, seg_light, h, org, dir, seg_n);
+                        if (seg_light != 0u && (em[0] > 0.0f || em[1] > 0.0f || em[2] > 0.0f))
+                            ew = lamp_hit_weight(S, seg_light, h, org, dir, seg_n);
 #pragma unroll
-                        for (int k = 0; k < 3; ++k) rad[k] += em * (tp[k] * ew);
+                        for (int k = 0; k < 3; ++k) rad[k] += em[k] * (tp[k] * ew);
                         if (kMode == kShadeReplay) {
-                            const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-                            if ((block & kOpaqueBit) && !(h.attrib & kEntityHit)) atomicAdd(adj.d_power + h.record, gsum3(G, tp, ew));
+                            if (!(h.attrib & kEntityHit)) atomicAdd(adj.d_power + h.record, gsum3(G, tp, ew, me));
                             // Everything gathered from here on carries this vertex's albedo.
-                            float* ga = s_albedo + 3 * (block & (kMaterialSlots - 1));
+                            const uint32_t code = material_code(block, S.enc);
 #pragma unroll
                             for (int k = 0; k < 3; ++k)
-                                if (al[k] > 0.0f && G[k] != 0.0f) atomicAdd(ga + k, G[k] * (R[k] - rad[k]) / al[k]);
+                                if (al[k] > 0.0f && G[k] != 0.0f) cache.add(code, k, G[k] * (R[k] - rad[k]) / al[k]);
                         }
 #pragma unroll
                         for (int k = 0; k < 3; ++k) tp[k] *= al[k] / hmax(0.001f, 1.0f);
@@ -351,12 +391,15 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                         // throughput, before Russian roulette rescales it).
                         if (shadow) {
 #pragma unroll
-                            for (int k = 0; k < 3; ++k) sadd[k] = r.value * (tp[k] * (1.0f / 1.0f));
+                            for (int k = 0; k < 3; ++k) sadd[k] = r.value[k] * (tp[k] * (1.0f / 1.0f));
                         }
                     }
                     uint2 pending = make_uint2(kNone, 0u);
-                    if (kMode == kShadeReplay && shadow && r.brick != kNone)
-                        pending = make_uint2(r.brick, __float_as_uint(gsum3(G, tp, r.dvalue_de)));
+                    if (kMode == kShadeReplay && shadow && r.brick != kNone) {
+                        const float gp =
+                            G[0] * (tp[0] * r.dvalue_de[0]) + G[1] * (tp[1] * r.dvalue_de[1]) + G[2] * (tp[2] * r.dvalue_de[2]);
+                        pending = make_uint2(r.brick, __float_as_uint(gp));
+                    }
                     bool alive = true;
                     if (!primary) {
                         const float cp = hmax(tp[0], hmax(tp[1], tp[2]));
@@ -386,7 +429,10 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
                             b.sadd[slot] = make_float4(sadd[0], sadd[1], sadd[2], 0.0f);
                         }
                         b.radiance[slot] = make_float4(rad[0], rad[1], rad[2], 0.0f);
-                        if (primary) b.a0e0[slot] = make_float4(a0[0], a0[1], a0[2], e0);
+                        if (primary) {
+                            b.a0[slot] = make_float4(a0[0], a0[1], a0[2], 0.0f);
+                            b.e0[slot] = make_float4(e0[0], e0[1], e0[2], 0.0f);
+                        }
                         if (kMode == kShadeReplay) {
                             if (primary) {
                                 b.adj_g[slot] = make_float4(G[0], G[1], G[2], 0.0f);
@@ -411,7 +457,7 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
 #pragma unroll
                     for (int k = 0; k < 3; ++k) {
                         const float sr = hmin(bad ? 0.0f : rad[k], 65504.0f);
-                        rgb[k] = e0 + a0[k] * sr;
+                        rgb[k] = e0[k] + a0[k] * sr;
                     }
                 }
                 float* o = V.radiance + 3ull * item;
@@ -435,8 +481,10 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     }
     if (kMode == kShadeReplay) {
         __syncthreads();
-        for (uint32_t i = threadIdx.x; i < kMaterialSlots * 3; i += kWaveThreads)
-            if (s_albedo[i] != 0.0f) atomicAdd(adj.d_albedo + i, s_albedo[i]);
+        for (uint32_t i = threadIdx.x; i < kAlbedoCache * 3; i += kWaveThreads) {
+            const uint32_t code = s_tag[i / 3];
+            if (code != kNone && s_albedo[i] != 0.0f) atomicAdd(adj.d_albedo + 3ull * code + i % 3, s_albedo[i]);
+        }
     }
 }
 
@@ -446,7 +494,7 @@ uint64_t wave_buffer_bytes(uint32_t capacity)
 {
     const uint64_t c = std::max<uint32_t>(capacity, 32);
     auto a = [](uint64_t x) { return (x + 255u) & ~uint64_t{255}; };
-    return 5 * a(4 * c) + 8 * a(16 * c) + a(16 * c) + a(4 * c) + 2 * a(8 * c) + 2 * a(4 * c) + a(64) +
+    return 5 * a(4 * c) + 9 * a(16 * c) + a(16 * c) + a(4 * c) + 2 * a(8 * c) + 2 * a(4 * c) + a(64) +
            2 * a(16 * c) + a(8 * c);
 }
 
@@ -471,7 +519,8 @@ WaveBuffers wave_carve(void* base, uint32_t capacity)
     b.throughput = reinterpret_cast<float4*>(take(16 * c));
     b.radiance = reinterpret_cast<float4*>(take(16 * c));
     b.seg_n = reinterpret_cast<float4*>(take(16 * c));
-    b.a0e0 = reinterpret_cast<float4*>(take(16 * c));
+    b.a0 = reinterpret_cast<float4*>(take(16 * c));
+    b.e0 = reinterpret_cast<float4*>(take(16 * c));
     b.sdir = reinterpret_cast<float4*>(take(16 * c));
     b.sadd = reinterpret_cast<float4*>(take(16 * c));
     b.hit = reinterpret_cast<uint4*>(take(16 * c));

@@ -248,24 +248,37 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs_static(uint32_t* keys, uint32_t*
 /* ---------------------------------------------------------------------------
  * Scene: voxel bricks on the device
  *
- * Bricks are 8x8x8 blocks of 16-bit values, block-ID encoding (opaque = bit 15 set; a value
- * without bit 15 is transparent, id = value & 0x1FF, id 0 = air), voxel index x + 8y + 64z, as in
- * the reference (include/caelix/caelix.h:240-290). A brick key is the brick coordinate; this
- * version takes keys in [0, 1024) per axis (the world grid is the bounding box of the keys).
+ * Bricks are 8x8x8 blocks of 16-bit values, voxel index x + 8y + 64z, in one of the reference's
+ * two block encodings (include/caelix/caelix.h:240-249):
+ *   0 packed scene colour (the default): opaque when (value & 0xC000) != 0; transparent id =
+ *     value & 0xFF, face bits at bits 8..13;
+ *   1 block-ID: opaque when (value & 0x8000) != 0; transparent id = value & 0x1FF, face bits at
+ *     bits 9..14.
+ * A brick key is the brick coordinate, each axis in [-2^20, 2^20) as in the reference
+ * (include/caelix/caelix.h:334). The device tables span the box of the keys (rounded to whole
+ * render groups): a flush whose box holds more than 2^32 brick cells returns
+ * CAELIX_ERROR_UNSUPPORTED (the occupancy bitmap is dense over the box).
  * Entity 0 is the scene's static world with the identity transform; caelix_scene_add_entity adds
  * entities 1, 2, ... with their own bricks (entity-local keys, the same range) under a rigid
  * transform. caelix_scene_flush builds, on the device: the brick records (the finalize rules of
  * the reference), the brick hash table, the brick occupancy bitmap, the brick light records and
- * the light tree of the world, and the same tables (without lights) of every entity.
+ * the light tree of the world, and the same tables of every entity.
  * ------------------------------------------------------------------------- */
 
 typedef struct CaelixScene CaelixScene;
 
+/* Replaces CaelixSceneDesc (include/caelix/caelix.h:274-294): the same 32-byte layout. */
 typedef struct CaelixSceneDesc
 {
-    uint32_t group_shift; /* render group edge in bricks = 1 << group_shift; 0 = 4; 1..4 */
-    uint32_t encoding;    /* 1 = block-ID (the only encoding of this version; 0 is rejected) */
-    uint32_t reserved[2]; /* must be 0 */
+    uint64_t staging_bytes;    /* stored (bricks are staged in device memory, grown on demand);
+                                  0 or >= 4 MiB */
+    uint32_t records_per_page; /* 0 or a power of two; stored (records are dense per flush) */
+    uint32_t group_shift;      /* render group edge in bricks = 1 << group_shift; 0 = 4; 1..4
+                                  (5..8: CAELIX_ERROR_UNSUPPORTED) */
+    uint32_t block_bytes;      /* 0 or 2 (4: CAELIX_ERROR_UNSUPPORTED) */
+    uint32_t encoding;         /* 0 = packed scene colour (the default), 1 = block-ID; other values
+                                  return CAELIX_ERROR_INVALID_ARGUMENT */
+    uint64_t scratch_bytes;    /* stored (no acceleration structures: the build sizes its scratch) */
 } CaelixSceneDesc;
 
 /* Replaces caelix_scene_create / caelix_scene_destroy (include/caelix/caelix.h:296-300). */
@@ -289,12 +302,12 @@ typedef struct CaelixEntityDesc
 /* Adds an entity with no bricks: world = R(rotation) * local + position, local = the
    entity-local block coordinate. Its bricks are traced (closest hit over the world and every
    entity, ties to the world and then to the lower id) and shaded with the scene's materials. Its
-   emitting bricks (caelix_scene_set_brick_power with its id) are lights of the second light tree
-   (the reference's dynamic tree, docs/LIGHT_TREE.md:136-176): the entities' light records merged
-   in id order under their transforms, rebuilt at a flush after any entity change or move, while
-   the world's tree (tree 0) stays; NEE picks between the two trees by importance. Every added
-   entity's lights go to that tree whatever its motion (the reference puts static entities' lights
-   in tree 0). Takes effect at the next flush. */
+   light voxels (the scene's light codes, in bricks with power above 0) are lights of the second
+   light tree (the reference's dynamic tree, docs/LIGHT_TREE.md:136-176): the entities' light
+   records merged in id order under their transforms, rebuilt at a flush after any entity change or
+   move, while the world's tree (tree 0) stays; NEE picks between the two trees by importance.
+   Every added entity's lights go to that tree whatever its motion (the reference puts static
+   entities' lights in tree 0). Takes effect at the next flush. */
 CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const CaelixEntityDesc* desc,
                                                 CaelixEntityId* out_id);
 /* Removes the entity and all its bricks at once (waiting for the device first). */
@@ -333,18 +346,29 @@ CAELIX_API CaelixResult caelix_scene_upload_bricks(CaelixScene* scene, uint32_t 
 CAELIX_API CaelixResult caelix_scene_remove_bricks(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                    const CaelixBrickKey* keys);
 
-/* New (no reference counterpart): the emitter power of bricks (host arrays). An opaque voxel of a
-   brick with power P > 0 emits radiance (P, P, P) and is a light voxel of the light tree (the
-   reference derives light voxels from emissive material codes, include/caelix/caelix.h:600-630;
-   the benchmark scenes give each emissive brick its own power). Keys without an uploaded brick are
-   kept and apply when it arrives. entity: 0 (the world's lights) or an added entity (the
-   entities' light tree). */
+/* New (no reference counterpart): the emitter power of bricks (host arrays), a factor of the
+   emission of every voxel of the brick: a voxel emits its material's emission times its brick's
+   power, and a light voxel (its code in the light code set, see caelix_scene_set_light_options)
+   of a brick with power 0 is no light. Every brick's power is 1 until set, so a host that never
+   calls this gets the reference's emission (include/caelix/caelix.h:600-630). The benchmark
+   scenes give each emissive brick its own power. Keys without an uploaded brick are kept and
+   apply when it arrives; a removed brick's power goes with it. power >= 0 and finite. entity: 0
+   (the world's lights) or an added entity (the entities' light tree). */
 CAELIX_API CaelixResult caelix_scene_set_brick_power(CaelixScene* scene, uint32_t entity, uint32_t count,
                                                      const CaelixBrickKey* keys, const float* power);
 
-/* Replaces CaelixMaterial (include/caelix/caelix.h:533-565): the same 112-byte entry. This version
-   shades opaque codes with a Lambertian lobe of `albedo`; the other fields are validated and
-   stored. */
+/* Replaces CaelixMaterial (include/caelix/caelix.h:529-556): the same 112-byte entry. Every scene
+   has a table of 65536 entries, one per 16-bit block code; a transparent code is looked up without
+   its face bits (include/caelix/caelix.h:478-515). This version shades every hit voxel with a
+   Lambertian lobe of `albedo` and its `emission` (times its brick's power, fp32 on the device);
+   the other fields are validated and stored. Built-in content, as in the reference:
+     packed: an opaque code with bit 15 is albedo rgb5 / 31 (r = bits 14..10, g = 9..5, b = 4..0);
+       an emissive code (bits 15..14 = 01) is albedo rgb4 / 15 (r = bits 13..10, g = 9..6,
+       b = 5..2) and emission albedo * 2^(3 * (code & 3)); a transparent code is albedo 1, no
+       emission (the glass palette's tints are not carried: glass is not traced here);
+     block-ID: an opaque code is a pastel hash colour of code & 0x7FFF, a transparent id 1..511 a
+       pastel hash colour of the id, air albedo 1; no emission.
+   Transparent voxels with face bits are hit like opaque ones (no refraction). */
 typedef struct CaelixMaterial
 {
     float albedo[3];
@@ -364,17 +388,46 @@ typedef struct CaelixMaterial
     uint32_t reserved;
 } CaelixMaterial;
 
-/* Replaces caelix_scene_set_materials (include/caelix/caelix.h:567): entries [0, count) are the
-   material table entries of codes 0x8000 | i (the opaque block-ID codes of material id i,
-   i < 128); the rest keep albedo 0.5. Every float must be finite. */
+/* Replaces caelix_scene_set_materials (include/caelix/caelix.h:558-568): entries [0, count) become
+   the table entries of codes [0, count), codes [count, 65536) get the built-in default of the
+   scene's encoding. count <= 65536 (0 restores the default table). The reference's value checks:
+   every float finite with a magnitude <= 65504, ior > 0, extinction >= 0, sss_model <= 255,
+   sss_probability and every sss_albedo in [0, 1], sss_anisotropy in [-1, 1], sss_steps <= 255,
+   texture_set and connect_group <= 0xFFFF; an invalid entry returns CAELIX_ERROR_INVALID_ARGUMENT
+   and changes nothing. Takes effect at the next flush (a change of the light code set rebuilds the
+   scene's records there). */
 CAELIX_API CaelixResult caelix_scene_set_materials(CaelixScene* scene, const CaelixMaterial* entries,
                                                    uint32_t count);
 
-/* Replaces CaelixLightOptions / caelix_scene_set_light_options (include/caelix/caelix.h:632-646). */
+/* Replaces CaelixMaterialEntry (include/caelix/caelix.h:576-581): 116 bytes. */
+typedef struct CaelixMaterialEntry
+{
+    uint32_t code; /* 0 .. 0xFFFF */
+    CaelixMaterial material;
+} CaelixMaterialEntry;
+
+/* Replaces caelix_scene_set_material_entries (include/caelix/caelix.h:583-592): writes
+   entries[i].material at code entries[i].code over the current table; one bad code or entry
+   returns CAELIX_ERROR_INVALID_ARGUMENT and changes nothing; count 0 is a no-op. */
+CAELIX_API CaelixResult caelix_scene_set_material_entries(CaelixScene* scene, const CaelixMaterialEntry* entries,
+                                                          uint32_t count);
+
+/* Replaces caelix_scene_get_material (include/caelix/caelix.h:593-597): the current entry of a raw
+   block code (face bits of a transparent code removed first), the host copy. */
+CAELIX_API CaelixResult caelix_scene_get_material(const CaelixScene* scene, uint32_t code, CaelixMaterial* out);
+
+/* Replaces CaelixLightOptions / caelix_scene_set_light_options (include/caelix/caelix.h:632-646).
+   A light voxel is a voxel whose material emission luminance, 0.2126 r + 0.7152 g + 0.0722 b, is at
+   least min_emission, in a brick with power above 0 (caelix_scene_set_brick_power). Invalid values
+   (enabled not 0 or 1, min_emission negative or not finite, heap_bytes above 2^32 x 16) return
+   CAELIX_ERROR_INVALID_ARGUMENT and change nothing. Takes effect at the next flush: enabling or
+   disabling the tree, or a change of the light code set, rebuilds the scene's tables; any other
+   change rebuilds the light tree alone. With the tree disabled the voxels still emit (their
+   emission is seen by the paths that hit them); there is no light-tree NEE. */
 typedef struct CaelixLightOptions
 {
-    uint32_t enabled;    /* 0 = no light tree, 1 = build it (the default of this version) */
-    float min_emission;  /* stored; light voxels come from the brick power */
+    uint32_t enabled;    /* 0 = no light tree (the default), 1 = build it */
+    float min_emission;  /* light voxel threshold (luminance of the material emission); 0 = 20 */
     uint64_t heap_bytes; /* stored; the heap is sized exactly at every flush */
 } CaelixLightOptions;
 CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const CaelixLightOptions* options);
@@ -423,7 +476,7 @@ CAELIX_API void caelix_scene_get_light_stats(const CaelixScene* scene, CaelixLig
    tests read back). Valid until the next flush that rebuilds or the scene's destruction. */
 typedef struct CaelixSceneView
 {
-    uint32_t grid[3];
+    uint32_t grid[3];       /* brick cells of the box per axis from `origin` */
     uint32_t group_shift;
     uint32_t groups[3];
     uint32_t brick_count;
@@ -446,6 +499,8 @@ typedef struct CaelixSceneView
     uint64_t tree_header;   /* LightTreeHeader + LightTreeState */
     uint64_t tree_nodes;
     uint64_t tree_leaves;
+    int32_t origin[3];      /* brick key of cell 0 of the box (a multiple of the group edge) */
+    uint32_t encoding;
 } CaelixSceneView;
 CAELIX_API CaelixResult caelix_scene_get_view(const CaelixScene* scene, CaelixSceneView* out);
 
@@ -491,6 +546,13 @@ typedef struct CaelixRenderTargets
     uint64_t radiance; /* device float[height][width][3] */
     uint32_t width;
     uint32_t height;
+    /* Optional (0 = none; the reference's voxel id target, include/caelix/caelix.h:1176-1190,
+       R32G32_UINT): device uint32[height][width][2], two independent hashes of (entity id,
+       entity-local integer voxel position) of the camera ray's first hit
+       (shaders/render/caelix_scene_trace.hlsl:171-200): every pixel of one voxel shares the key; a
+       miss, and a hit farther than CaelixRenderOptions::voxel_id_tmax, are 0xFFFFFFFF in both
+       words. Written once per render call, from the camera ray of the first sample. */
+    uint64_t voxel_id;
 } CaelixRenderTargets;
 
 /* Replaces CaelixRenderOptions (include/caelix/caelix.h:1043-1126): the fields of the path-traced
@@ -501,7 +563,9 @@ typedef struct CaelixRenderOptions
     uint32_t bounce_count; /* stochastic bounces after the primary hit, 0 .. 14 */
     uint32_t frame_seed;   /* per-pixel random streams depend on the pixel and this value only */
     uint32_t spp;          /* new: samples per pixel (frame seeds frame_seed .. + spp - 1, averaged); 0 = 1 */
-    uint32_t reserved[4];  /* must be 0 */
+    float voxel_id_tmax;   /* the voxel id target: hits farther than this along the camera ray are
+                              misses; 0 = no limit. Finite and >= 0. */
+    uint32_t reserved[3];  /* must be 0 */
 } CaelixRenderOptions;
 
 /* Replaces caelix_renderer_render (include/caelix/caelix.h:1257): records the trace of one frame
@@ -562,8 +626,8 @@ CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, Cael
 /* New (no reference counterpart): the adjoint of caelix_renderer_render for an image loss L.
    d_radiance: device float[height][width][3], dL/d(radiance) of the frame the same renderer,
    target size, camera and options render. Writes (after zeroing them) the gradients of L with
-   respect to the albedo of every material, d_albedo: device float[128][3] (row = material id,
-   value & 0x7F), and to the emitter power of every brick, d_power: device float[brick_count] in
+   respect to the albedo of every material table entry, d_albedo: device float[65536][3] (row =
+   the material code), and to the emitter power of every brick, d_power: device float[brick_count] in
    the scene's brick order (the keys of caelix_scene_get_view: increasing linear brick index).
    Sampling quantities (pdfs, MIS weights, Russian-roulette probabilities, discrete decisions) are
    held fixed. The frame is traced twice (path replay): once recording each sample's radiance (one

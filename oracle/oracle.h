@@ -117,19 +117,42 @@ float oc_importance(const float x[3], const float n[3], const float lo[3], const
 /* ---- scene (oracle/scene.c) ---- */
 
 #define OC_RECORD_WORDS 274
+#define OC_MATERIAL_CODES 65536
 
-/* A voxel world of bricks: keys[i] = brick coordinate (x, y, z) of brick i (every coordinate in
- * [0, grid)), voxels[512 i + x + 8 y + 64 z] = raw block value (block-ID encoding: opaque =
- * 0x8000 | material, 0 = air), power[i] = the brick's emitter power (0: not emissive). */
+/* Block encodings (include/caelix/caelix.h:243-249): packed (0) is opaque on 0xC000, transparent
+ * id = value & 0xFF, face bits at 8; block-ID (1) is opaque on 0x8000, id = value & 0x1FF, face
+ * bits at 9. */
+#define OC_ENCODING_PACKED 0u
+#define OC_ENCODING_BLOCK_ID 1u
+/* The material table index of a raw value: opaque values as they are, transparent ones without
+ * their face bits (caelix_record.hlsl:205-212 BlockMaterialCode). */
+uint32_t oc_material_code(uint32_t value, uint32_t encoding);
+
+/* A voxel world of bricks: keys[i] = brick coordinate (x, y, z) of brick i, every coordinate in
+ * [origin, origin + grid), in increasing linear index of that box; voxels[512 i + x + 8 y + 64 z]
+ * = raw block value; power[i] = the brick's emitter power (a factor of its voxels' emission).
+ * emission: the material table's emission, [65536][3] by code (a transparent code with face bits
+ * is looked up without them); a light voxel's code has an emission luminance of at least
+ * min_emission (the light code set, oc_light_codes). lights = 0: no light records. */
 typedef struct oc_scene_desc {
     uint32_t grid[3];
     uint32_t group_shift;
     uint32_t brick_count;
+    uint32_t encoding;
+    int32_t origin[3];    /* brick key of grid cell 0, a multiple of the group edge */
+    uint32_t lights;
+    float min_emission;
     uint32_t pad;
     const int32_t* keys;
     const uint16_t* voxels;
     const float* power;
+    const float* emission;
 } oc_scene_desc;
+
+/* The light code set (lib/src/light/light_tree.cpp:186-200 RebuildCodes): bit c of out[c / 32]
+ * for every code whose canonical entry's emission luminance 0.2126 r + 0.7152 g + 0.0722 b is at
+ * least min_emission. out: 2048 words. */
+void oc_light_codes(const float* emission, uint32_t encoding, float min_emission, uint32_t* out);
 
 struct oc_entity;
 struct oc_light_tree;
@@ -137,6 +160,11 @@ struct oc_light_tree;
 typedef struct oc_scene {
     uint32_t grid[3];
     uint32_t group_shift;
+    int32_t origin[3];
+    uint32_t encoding;
+    const float* emission;    /* the material table's emission [65536][3] (the desc's) */
+    uint32_t* light_codes;    /* [2048] */
+    int32_t* keys;            /* [brick_count][3] (a copy of the desc's) */
     uint32_t brick_count;
     uint32_t hash_capacity;   /* home slots (load factor 0.5) */
     uint32_t hash_slot_count; /* slots including the tail */
@@ -179,6 +207,7 @@ typedef struct oc_entity {
     float rot[9];
     float pos[3];
     uint32_t group_base; /* its first group in the merged light set */
+    uint32_t id;         /* its entity id (the voxel id's entity word) */
     const float* power;  /* its bricks' emitter power */
 } oc_entity;
 
@@ -216,6 +245,9 @@ typedef struct oc_render_desc {
     uint32_t frame_seed;
     uint32_t light_nee; /* 1: light-tree NEE with MIS */
     uint32_t x0, y0, x1, y1; /* pixel window rendered (the rest is left untouched) */
+    uint32_t* voxel_id;  /* optional: [height][width][2], the voxel id of the camera ray's first hit */
+    float voxel_id_tmax; /* hits farther than this are voxel id misses (0: no limit) */
+    uint32_t pad;
 } oc_render_desc;
 
 /* A built light tree (the build's output) for the trace. */
@@ -241,14 +273,20 @@ typedef struct oc_hit {
 oc_hit oc_trace_ray(const oc_scene* s, const float origin[3], const float dir[3], float tmin, float tmax);
 
 /* Renders the pixel window; radiance[3 * (y * width + x)] (fp32 RGB, averaged over spp);
- * rays[3]: primary, bounce, shadow rays traced. Threads > 1 splits rows across threads. */
+ * rays[3]: primary, bounce, shadow rays traced. albedo: the material table's albedo [65536][3] by
+ * code; power: per brick. Threads > 1 splits rows across threads. */
 void oc_render(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
                const oc_camera* cam, const oc_render_desc* r, float* radiance, uint64_t* rays, int threads);
+
+/* The voxel id of a hit (shaders/render/caelix_scene_trace.hlsl:171-200): two hashes of (entity
+ * id, entity-local voxel); the world is entity 0, an entity hit takes its oc_entity::id. */
+void oc_voxel_id(const oc_scene* s, const oc_hit* h, uint32_t out[2]);
 
 /* The adjoint reference (double precision): the estimator with the sampling quantities of the
  * fp32 render at (albedo, power) held fixed, evaluated at (A, P) (double; NULL = the fp32
  * parameters). image (may be NULL): the double image. d_radiance (may be NULL): dL/d(pixel);
- * then d_albedo [128][3] and d_power [brick_count] receive dL/dA and dL/dP at (A, P). */
+ * then d_albedo [65536][3] (by material code) and d_power [brick_count] receive dL/dA and dL/dP
+ * at (A, P). */
 void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
                 const oc_camera* cam, const oc_render_desc* r, const double* A, const double* P,
                 const float* d_radiance, double* image, double* d_albedo, double* d_power, int threads);

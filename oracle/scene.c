@@ -1,9 +1,10 @@
 /* Oracle of the scene side of the trace path (TEST INFRASTRUCTURE ONLY; see oracle.h):
  *   - brick records from raw bricks, restating the finalize kernel
  *     (shaders/scene/caelix_finalize.hlsl:110-340; its CPU twin is the reference's
- *     tests/finalize_test.cpp:74): per voxel "alive" (not all six neighbours opaque, an absent
- *     brick is air), occupied = alive && value != 0 && (opaque || a face bit), micro occupancy,
- *     coarse byte, tight bounds; opaque-only payloads are kept as uploaded;
+ *     tests/finalize_test.cpp:74) in either block encoding (caelix_record.hlsl:180-212): per voxel
+ *     "alive" (not all six neighbours opaque, an absent brick is air), occupied = alive && value
+ *     != 0 && (opaque || a face bit), micro occupancy, coarse byte, tight bounds; opaque-only
+ *     payloads are kept as uploaded;
  *   - the brick hash table: the reference's fingerprint (splitmix64 over the key words,
  *     shaders/common/caelix_hash_table.hlsl:102-128) and 16-byte key slots (key_lo, key_hi,
  *     payload, pad: lib/src/rhi/hash_table_layout.h:24-34), linear probing from the home slot.
@@ -11,11 +12,12 @@
  *     first free slot at or after its home (a history-independent layout; no wrap, a tail of
  *     slots follows the table);
  *   - the brick light records and group light blocks, restating the group pass's record build
- *     (shaders/light/records/caelix_light_tree_build.hlsl:93-285): a light voxel is an opaque
- *     voxel of an emissive brick (the per-brick emitter power of the benchmark scenes); its open
- *     faces (neighbour not opaque) are the face entries, sorted per family by voxel index; face
- *     sums = the sum of the luminance of the emission over the entries (per lane of 16 voxels,
- *     then lanes folded 16, 8, 4, 2, 1); box = tight box of the voxels with entries. Index
+ *     (shaders/light/records/caelix_light_tree_build.hlsl:93-285): a light voxel is a voxel whose
+ *     material code is in the light code set (LtOpenFaces), in a brick with emitter power above 0
+ *     (a factor of its voxels' emission); its open faces (neighbour not opaque) are the face
+ *     entries, sorted per family by voxel index; face sums = the sum over the entries of the
+ *     luminance of the emission times the power (per lane of 16 voxels, then lanes folded 16, 8,
+ *     4, 2, 1); box = tight box of the voxels with entries. Index
  *     entries in Morton order of the brick position (caelix_light_tree_layout.hlsl:338-361), the
  *     block layout of light_tree_layout.h:260-323.
  */
@@ -24,7 +26,31 @@
 
 #include "oracle.h"
 
-#define OPAQUE 0x8000u /* block-ID encoding */
+static uint32_t opaque_mask(uint32_t encoding) { return encoding == OC_ENCODING_PACKED ? 0xC000u : 0x8000u; }
+static uint32_t id_mask(uint32_t encoding) { return encoding == OC_ENCODING_PACKED ? 0xFFu : 0x1FFu; }
+static uint32_t face_shift(uint32_t encoding) { return encoding == OC_ENCODING_PACKED ? 8u : 9u; }
+
+uint32_t oc_material_code(uint32_t value, uint32_t encoding)
+{
+    value &= 0xFFFFu;
+    return (value & opaque_mask(encoding)) ? value : (value & id_mask(encoding));
+}
+
+void oc_light_codes(const float* emission, uint32_t encoding, float min_emission, uint32_t* out)
+{
+    memset(out, 0, 4 * (OC_MATERIAL_CODES / 32));
+    for (uint32_t c = 0; c < OC_MATERIAL_CODES; ++c) {
+        const float* e = emission + 3ull * oc_material_code(c, encoding);
+        const float lum = 0.2126f * e[0] + 0.7152f * e[1] + 0.0722f * e[2];
+        if (lum >= min_emission) out[c >> 5] |= 1u << (c & 31);
+    }
+}
+
+static int is_light_code(const oc_scene* s, uint32_t value)
+{
+    const uint32_t c = oc_material_code(value, s->encoding);
+    return (s->light_codes[c >> 5] >> (c & 31)) & 1u;
+}
 
 static uint64_t splitmix64(uint64_t x)
 {
@@ -123,6 +149,7 @@ static void build_records(const oc_scene_desc* d, oc_scene* s)
     const uint32_t n = d->brick_count;
     const uint32_t gshift = d->group_shift;
     const uint32_t gmask = (1u << gshift) - 1u;
+    const uint32_t OPAQUE = opaque_mask(d->encoding), IDS = id_mask(d->encoding), FSHIFT = face_shift(d->encoding);
     s->records = (uint32_t*)calloc((size_t)n * OC_RECORD_WORDS, 4);
     for (uint32_t b = 0; b < n; ++b) {
         const int32_t bx = d->keys[3 * b], by = d->keys[3 * b + 1], bz = d->keys[3 * b + 2];
@@ -134,7 +161,7 @@ static void build_records(const oc_scene_desc* d, oc_scene* s)
             for (int y = 0; y < 8; ++y)
                 for (int x = 0; x < 8; ++x) {
                     const uint32_t v = vox[x + 8 * y + 64 * z];
-                    const uint32_t code = (v & OPAQUE) ? v : (v & 0x1FFu);
+                    const uint32_t code = oc_material_code(v, d->encoding);
                     static const int dx[6] = {1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, 1, -1, 0, 0},
                                      dz[6] = {0, 0, 0, 0, 1, -1};
                     uint32_t opaque_count = 0, faces = 0;
@@ -142,10 +169,10 @@ static void build_records(const oc_scene_desc* d, oc_scene* s)
                         const uint32_t nv = voxel_at(d, s, bx, by, bz, x + dx[f], y + dy[f], z + dz[f]);
                         const int nop = (nv & OPAQUE) != 0;
                         opaque_count += nop;
-                        if (!nop && (nv & 0x1FFu) != code) faces |= 1u << f;
+                        if (!nop && (nv & IDS) != code) faces |= 1u << f;
                     }
                     const int alive = opaque_count < 6;
-                    const uint32_t result = (code & OPAQUE) ? code : (code | (faces << 9));
+                    const uint32_t result = (code & OPAQUE) ? code : (code | (faces << FSHIFT));
                     const int iface = (code & OPAQUE) != 0 || faces != 0;
                     const uint32_t word = 18 + (x >> 1) + 4 * y + 32 * z;
                     rec[word] |= (x & 1) ? (result << 16) : result;
@@ -199,13 +226,13 @@ static uint32_t light_record(const oc_scene_desc* d, const oc_scene* s, uint32_t
     const uint16_t* vox = d->voxels + 512ull * b;
     static const int dx[6] = {1, -1, 0, 0, 0, 0}, dy[6] = {0, 0, 1, -1, 0, 0}, dz[6] = {0, 0, 0, 0, 1, -1};
     const float P = d->power[b];
-    const float weight = P * 0.2126f + P * 0.7152f + P * 0.0722f; /* LtLuminance of (P, P, P) */
+    const uint32_t OPAQUE = opaque_mask(d->encoding);
     uint32_t open[512];
     uint32_t counts[6] = {0};
     for (uint32_t vi = 0; vi < 512; ++vi) {
         const int x = vi & 7, y = (vi >> 3) & 7, z = vi >> 6;
         open[vi] = 0;
-        if (!(vox[vi] & OPAQUE)) continue;
+        if (!is_light_code(s, vox[vi])) continue;
         for (int f = 0; f < 6; ++f) {
             const uint32_t nv = voxel_at(d, s, bx, by, bz, x + dx[f], y + dy[f], z + dz[f]);
             if (!(nv & OPAQUE)) open[vi] |= 1u << f;
@@ -224,6 +251,9 @@ static uint32_t light_record(const oc_scene_desc* d, const oc_scene* s, uint32_t
     for (uint32_t vi = 0; vi < 512; ++vi) {
         if (!open[vi]) continue;
         const uint32_t lane = vi >> 4;
+        /* LtLuminance of the voxel's emission times the brick's power (each channel times P). */
+        const float* e = d->emission + 3ull * oc_material_code(vox[vi], d->encoding);
+        const float weight = (e[0] * P) * 0.2126f + (e[1] * P) * 0.7152f + (e[2] * P) * 0.0722f;
         for (int f = 0; f < 6; ++f) {
             if (!((open[vi] >> f) & 1u)) continue;
             entries[base[f] + cursor[f]] = vi | ((uint32_t)vox[vi] << 16);
@@ -265,9 +295,13 @@ static void build_lights(const oc_scene_desc* d, oc_scene* s)
     s->group_count = s->groups[0] * s->groups[1] * s->groups[2];
     light_brick* lb = (light_brick*)malloc(sizeof(light_brick) * (n ? n : 1));
     uint32_t m = 0;
-    for (uint32_t b = 0; b < n; ++b) {
+    for (uint32_t b = 0; b < n && d->lights; ++b) {
         if (!(d->power[b] > 0.0f)) continue;
-        const uint32_t bx = (uint32_t)d->keys[3 * b], by = (uint32_t)d->keys[3 * b + 1], bz = (uint32_t)d->keys[3 * b + 2];
+        int any = 0;
+        for (uint32_t vi = 0; vi < 512 && !any; ++vi) any = is_light_code(s, d->voxels[512ull * b + vi]);
+        if (!any) continue;
+        const uint32_t bx = (uint32_t)(d->keys[3 * b] - d->origin[0]), by = (uint32_t)(d->keys[3 * b + 1] - d->origin[1]),
+                       bz = (uint32_t)(d->keys[3 * b + 2] - d->origin[2]);
         const uint32_t g = (bx >> gshift) + s->groups[0] * ((by >> gshift) + s->groups[1] * (bz >> gshift));
         lb[m].key = (g << (3 * gshift)) | morton10(bx & gmask, by & gmask, bz & gmask);
         lb[m].brick = b;
@@ -285,9 +319,9 @@ static void build_lights(const oc_scene_desc* d, oc_scene* s)
         const uint32_t gx = g % s->groups[0], gy = (g / s->groups[0]) % s->groups[1],
                        gz = g / (s->groups[0] * s->groups[1]);
         oc_frame* f = &s->group_frames[g];
-        f->origin[0] = (float)(gx * (8u << gshift));
-        f->origin[1] = (float)(gy * (8u << gshift));
-        f->origin[2] = (float)(gz * (8u << gshift));
+        f->origin[0] = (float)(8ll * ((int64_t)d->origin[0] + ((int64_t)gx << gshift)));
+        f->origin[1] = (float)(8ll * ((int64_t)d->origin[1] + ((int64_t)gy << gshift)));
+        f->origin[2] = (float)(8ll * ((int64_t)d->origin[2] + ((int64_t)gz << gshift)));
         f->rot[0] = f->rot[4] = f->rot[8] = 1.0f;
     }
     /* Heap: one block per group with light bricks, in group order. */
@@ -358,20 +392,28 @@ static void build_lights(const oc_scene_desc* d, oc_scene* s)
 int oc_scene_build(const oc_scene_desc* d, oc_scene* s)
 {
     memset(s, 0, sizeof(*s));
-    s->grid[0] = d->grid[0];
-    s->grid[1] = d->grid[1];
-    s->grid[2] = d->grid[2];
+    for (int k = 0; k < 3; ++k) {
+        s->grid[k] = d->grid[k];
+        s->origin[k] = d->origin[k];
+    }
     s->group_shift = d->group_shift;
     s->brick_count = d->brick_count;
+    s->encoding = d->encoding;
+    s->emission = d->emission;
+    s->light_codes = (uint32_t*)malloc(4 * (OC_MATERIAL_CODES / 32));
+    oc_light_codes(d->emission, d->encoding, d->min_emission, s->light_codes);
+    s->keys = (int32_t*)malloc(12ull * (d->brick_count ? d->brick_count : 1));
+    memcpy(s->keys, d->keys, 12ull * d->brick_count);
     build_hash(d, s);
     build_records(d, s);
-    /* Brick occupancy bitmap by linear brick index. */
+    /* Brick occupancy bitmap by linear brick index of the box (origin, grid). */
     const uint64_t cells = (uint64_t)d->grid[0] * d->grid[1] * d->grid[2];
     s->bitmap_words = (uint32_t)((cells + 31) / 32);
     s->bitmap = (uint32_t*)calloc(s->bitmap_words ? s->bitmap_words : 1, 4);
     for (uint32_t b = 0; b < d->brick_count; ++b) {
-        const uint64_t c = (uint64_t)d->keys[3 * b] +
-                           d->grid[0] * ((uint64_t)d->keys[3 * b + 1] + (uint64_t)d->grid[1] * d->keys[3 * b + 2]);
+        const uint64_t c = (uint64_t)(uint32_t)(d->keys[3 * b] - d->origin[0]) +
+                           d->grid[0] * ((uint64_t)(uint32_t)(d->keys[3 * b + 1] - d->origin[1]) +
+                                         (uint64_t)d->grid[1] * (uint32_t)(d->keys[3 * b + 2] - d->origin[2]));
         s->bitmap[c >> 5] |= 1u << (c & 31);
     }
     build_lights(d, s);
@@ -380,6 +422,8 @@ int oc_scene_build(const oc_scene_desc* d, oc_scene* s)
 
 void oc_scene_free(oc_scene* s)
 {
+    free(s->light_codes);
+    free(s->keys);
     free(s->records);
     free(s->hash_slots);
     free(s->bitmap);

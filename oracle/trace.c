@@ -13,9 +13,10 @@
  *                      caelix_shading.hlsl:267-307 (ShadeVoxelHit, opaque Lambertian: metallic 0,
  *                      smoothness 0), caelix_random.hlsl (PcgHash, InitRandom, xorshift32,
  *                      RandomUnitVector), common/caelix_frame.hlsl:164-171 (camera ray)
- * in the benchmark scenes' configuration: opaque voxels, light-tree NEE with MIS, no sun, black
- * sky, no fog, bounce NEE probability 1; entities under rigid transforms, their lights in the
- * second light tree (the reference's dynamic tree).
+ * in the benchmark scenes' configuration: Lambertian voxels (the material table's albedo; the
+ * emission of a voxel = its table emission times its brick's power), light-tree NEE with MIS, no
+ * sun, black sky, no fog, bounce NEE probability 1; entities under rigid transforms, their lights
+ * in the second light tree (the reference's dynamic tree); either block encoding.
  *
  * Arithmetic: IEEE fp32, no contraction, HLSL operation order. Two definitions are this
  * project's: sin/cos of RandomUnitVector (Cody-Waite reduction by pi/2 and Taylor polynomials to
@@ -29,7 +30,6 @@
 
 #include "oracle.h"
 
-#define OPAQUE 0x8000u
 #define RAY_TMAX 1e30f
 #define BOUNCE_TMAX 1e4f
 #define PUSH_OFF 0.002f
@@ -145,8 +145,10 @@ static uint32_t normal_flags(uint32_t index, const int cell[3], const float t_st
 }
 
 static float brick_ray(const uint32_t* rec, const float entry[3], const float dir[3], float entry_t,
-                       uint32_t entry_coarse, uint32_t* attrib)
+                       uint32_t entry_coarse, uint32_t encoding, uint32_t* attrib)
 {
+    const uint32_t opaque = encoding == OC_ENCODING_PACKED ? 0xC000u : 0x8000u;
+    const uint32_t fshift = encoding == OC_ENCODING_PACKED ? 8u : 9u;
     float inv[3], t_start[3], origin[3];
     int cell[3], prev[3];
     for (int k = 0; k < 3; ++k) {
@@ -172,8 +174,8 @@ static float brick_ray(const uint32_t* rec, const float entry[3], const float di
             const uint32_t blk = (w >> ((cell[0] & 1) << 4)) & 0xFFFFu;
             float T;
             const uint32_t nf = normal_flags(step, prev, t_start, dir, inv, entry_coarse >> 26, &T);
-            int term = (blk & OPAQUE) != 0;
-            if (!term) term = (step == 0 && entry_t == 0.0f) ? 0 : ((((blk >> 9) & 63u) & nf) != 0);
+            int term = (blk & opaque) != 0;
+            if (!term) term = (step == 0 && entry_t == 0.0f) ? 0 : ((((blk >> fshift) & 63u) & nf) != 0);
             if (term) {
                 *attrib = (blk << 16) | (((uint32_t)cell[0] | ((uint32_t)cell[1] << 3) | ((uint32_t)cell[2] << 6)) << 6) | nf;
                 return entry_t + T;
@@ -187,7 +189,7 @@ static float brick_ray(const uint32_t* rec, const float entry[3], const float di
 }
 
 static float brick_primitive(const uint32_t* rec, const float o[3], const float d[3], float t_current,
-                             const float brick_origin[3], uint32_t* attrib)
+                             const float brick_origin[3], uint32_t encoding, uint32_t* attrib)
 {
     const uint32_t tb = rec[1];
     const float tmin_v[3] = {(float)(tb & 7u), (float)((tb >> 3) & 7u), (float)((tb >> 6) & 7u)};
@@ -214,10 +216,11 @@ static float brick_primitive(const uint32_t* rec, const float o[3], const float 
     if (largest == tmin[0]) nf = d[0] > 0.0f ? 2u : 1u;
     else if (largest == tmin[1]) nf = d[1] > 0.0f ? 8u : 4u;
     else nf = d[2] > 0.0f ? 32u : 16u;
-    return brick_ray(rec, entry, d, t, (nf << 26) | ((rec[0] >> 16) & 0xFFu), attrib);
+    return brick_ray(rec, entry, d, t, (nf << 26) | ((rec[0] >> 16) & 0xFFu), encoding, attrib);
 }
 
-/* ---- scene traversal: front-to-back DDA over the brick grid ---- */
+/* ---- scene traversal: front-to-back DDA over the brick grid ----
+ * Cell c of axis k is brick key origin[k] + c, voxels [8 (origin[k] + c), 8 (origin[k] + c + 1)). */
 
 static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
 {
@@ -226,8 +229,8 @@ static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], 
     float inv[3], tnear = -3.0e38f, tfar = 3.0e38f;
     for (int k = 0; k < 3; ++k) {
         inv[k] = safe_inv_axis(d[k]);
-        const float t0 = (0.0f - o[k]) * inv[k];
-        const float t1 = ((float)(8u * s->grid[k]) - o[k]) * inv[k];
+        const float t0 = ((float)(8 * s->origin[k]) - o[k]) * inv[k];
+        const float t1 = ((float)(8 * (s->origin[k] + (int)s->grid[k])) - o[k]) * inv[k];
         tnear = hmax(tnear, hmin(t0, t1));
         tfar = hmin(tfar, hmax(t0, t1));
     }
@@ -237,7 +240,7 @@ static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], 
     int cell[3], step[3];
     for (int k = 0; k < 3; ++k) {
         const float p = o[k] + d[k] * t_enter;
-        int c = (int)floorf(p * 0.125f);
+        int c = (int)floorf(p * 0.125f) - s->origin[k];
         if (c < 0) c = 0;
         if (c > (int)s->grid[k] - 1) c = (int)s->grid[k] - 1;
         cell[k] = c;
@@ -247,11 +250,13 @@ static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], 
     for (uint32_t it = 0; it < limit; ++it) {
         const uint64_t lin = (uint64_t)cell[0] + s->grid[0] * ((uint64_t)cell[1] + (uint64_t)s->grid[1] * cell[2]);
         if (s->bitmap[lin >> 5] & (1u << (lin & 31))) {
-            const uint32_t r = oc_hash_lookup(s, cell[0], cell[1], cell[2]);
+            const int32_t key[3] = {s->origin[0] + cell[0], s->origin[1] + cell[1], s->origin[2] + cell[2]};
+            const uint32_t r = oc_hash_lookup(s, key[0], key[1], key[2]);
             if (r != OC_NONE) {
-                const float bo[3] = {(float)(cell[0] * 8), (float)(cell[1] * 8), (float)(cell[2] * 8)};
+                const float bo[3] = {(float)(key[0] * 8), (float)(key[1] * 8), (float)(key[2] * 8)};
                 uint32_t attrib;
-                const float t = brick_primitive(s->records + (size_t)r * OC_RECORD_WORDS, o, d, tmax_ray, bo, &attrib);
+                const float t = brick_primitive(s->records + (size_t)r * OC_RECORD_WORDS, o, d, tmax_ray, bo,
+                                                s->encoding, &attrib);
                 if (attrib != 0u && t >= tmin_ray && t < tmax_ray) {
                     h.hit = 1;
                     h.t = t;
@@ -272,7 +277,7 @@ static oc_hit trace_grid(const oc_scene* s, const float o[3], const float d[3], 
         /* Next cell: the axis whose boundary comes first (ties: x, then y, then z). */
         float tn[3];
         for (int k = 0; k < 3; ++k)
-            tn[k] = ((float)((cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
+            tn[k] = ((float)((s->origin[k] + cell[k] + (step[k] > 0 ? 1 : 0)) * 8) - o[k]) * inv[k];
         int axis = 0;
         if (tn[1] < tn[axis]) axis = 1;
         if (tn[2] < tn[axis]) axis = 2;
@@ -691,8 +696,8 @@ void oc_light_draws(const oc_scene* s, const oc_light_tree* t, const float x[3],
     }
 }
 
-/* LightTreeFindLightFace (caelix_light_tree.hlsl:853-934): with per-brick emitter power, a light
- * voxel is an opaque voxel of a brick that has a brick light record. */
+/* LightTreeFindLightFace (caelix_light_tree.hlsl:853-934): the face of a voxel whose material code
+ * is in the light code set, in a brick that has a brick light record. */
 static int find_light_face(const oc_scene* s, const oc_light_tree* t, const float x[3], uint32_t group,
                            const uint32_t v[3], uint32_t face, uint32_t block, uint32_t* entry_out,
                            uint32_t* leaf_out, float* in_brick)
@@ -700,7 +705,8 @@ static int find_light_face(const oc_scene* s, const oc_light_tree* t, const floa
     *entry_out = OC_NONE;
     *leaf_out = OC_NONE;
     *in_brick = 0.0f;
-    if (!(block & OPAQUE) || face > 5) return 0;
+    const uint32_t code = oc_material_code(block, s->encoding);
+    if (!((s->light_codes[code >> 5] >> (code & 31)) & 1u) || face > 5) return 0;
     const uint32_t* row = s->group_rows + 8ull * group;
     if (row[1] == 0) return 0;
     const uint32_t* block_w = s->heap + 4ull * row[0];
@@ -812,18 +818,56 @@ float oc_mis_weight(float p_area, const float n_r[3], const float w[3], float d,
     return mis_weight(p_area, n_r, w, d, cos_l, nee_side);
 }
 
-static void emission_of(const ctx* c, uint32_t record, uint32_t block, float e[3])
+/* The emission of a voxel: the table's emission of its material code (the scene's table, shared by
+ * its entities) times its brick's power p. */
+static void emission_of(const ctx* c, float p, uint32_t block, float e[3])
 {
-    const float p = (block & OPAQUE) ? c->power[record] : 0.0f;
-    e[0] = e[1] = e[2] = p;
+    const float* m = c->s->emission + 3ull * oc_material_code(block, c->s->encoding);
+    for (int k = 0; k < 3; ++k) e[k] = m[k] * p;
+}
+
+/* ---- the voxel id (shaders/render/caelix_scene_trace.hlsl:171-200) ---- */
+
+static uint32_t hash_avalanche(uint32_t v)
+{
+    v ^= v >> 16;
+    v *= 0x7FEB352Du;
+    v ^= v >> 15;
+    v *= 0x846CA68Bu;
+    v ^= v >> 16;
+    return v;
+}
+
+static uint32_t voxel_id_word(uint32_t seed, uint32_t entity, const int32_t v[3])
+{
+    uint32_t h = hash_avalanche(seed ^ entity);
+    for (int k = 0; k < 3; ++k) h = hash_avalanche(h ^ (uint32_t)v[k]);
+    return h == 0xFFFFFFFFu ? 0xFFFFFFFEu : h;
+}
+
+void oc_voxel_id(const oc_scene* s, const oc_hit* h, uint32_t out[2])
+{
+    uint32_t entity = 0;
+    const oc_scene* b = s;
+    if (h->attrib & OC_ENTITY_HIT) {
+        const uint32_t e = h->group >> 24;
+        entity = s->entities[e].id;
+        b = s->entities[e].scene;
+    }
+    const uint32_t cell = (h->attrib >> 6) & 0x1FFu;
+    int32_t v[3];
+    for (int k = 0; k < 3; ++k) v[k] = b->keys[3ull * h->record + k] * 8 + (int32_t)((cell >> (3 * k)) & 7u);
+    out[0] = voxel_id_word(0x9E3779B9u, entity, v);
+    out[1] = voxel_id_word(0x85EBCA6Bu, entity, v);
 }
 
 /* NextEventAtVertex without the sun: the lamp candidate and its shadow ray. */
 static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* light_rng, float out[3],
-                       uint32_t* lamp_brick, float* dvalue)
+                       uint32_t* lamp_brick, uint32_t* lamp_code, float* dvalue)
 {
     out[0] = out[1] = out[2] = 0.0f;
     *lamp_brick = OC_NONE;
+    *lamp_code = 0;
     *dvalue = 0.0f;
     const uint32_t point_seed = random_u32(light_rng);
     float p[7];
@@ -846,12 +890,7 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
     const uint32_t* block_w = L->heap + 4ull * row[0];
     const uint32_t brick = block_w[4 + 4 * words[4] + 1];
     float e[3];
-    if (words[5] == 0) {
-        emission_of(c, brick, words[0], e);
-    } else {
-        const float pw = (words[0] & OPAQUE) ? c->s->dyn_power[brick] : 0.0f;
-        e[0] = e[1] = e[2] = pw;
-    }
+    emission_of(c, words[5] == 0 ? c->power[brick] : c->s->dyn_power[brick], words[0], e);
     float contribution[3] = {e[0] * scale, e[1] * scale, e[2] * scale};
     const float lum = contribution[0] * 0.2126f + contribution[1] * 0.7152f + contribution[2] * 0.0722f;
     const float w_lamp = lum * hmax(0.05f, 1.0f);
@@ -867,9 +906,11 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
     if (t_max > 0.0f && !occluded) {
         const float k = w_sum / w_lamp;
         for (int q = 0; q < 3; ++q) out[q] = contribution[q] * k;
-        /* For the adjoint: the contribution is the lamp brick's power times scale * k. */
-        if ((words[0] & OPAQUE) && words[5] == 0) {
+        /* For the adjoint: the contribution is the lamp brick's power times the emission of its
+         * code times scale * k. */
+        if (words[5] == 0) {
             *lamp_brick = brick;
+            *lamp_code = oc_material_code(words[0], c->s->encoding);
             *dvalue = scale * k;
         }
     }
@@ -916,12 +957,11 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
     const uint32_t block = (h->attrib >> 16) & 0xFFFFu;
     if (h->attrib & OC_ENTITY_HIT) { /* an entity brick's power */
         const float* pw = c->s->entities[h->group >> 24].power;
-        const float p = (pw && (block & OPAQUE)) ? pw[h->record] : 0.0f;
-        emission[0] = emission[1] = emission[2] = p;
+        emission_of(c, pw ? pw[h->record] : 0.0f, block, emission);
     } else {
-        emission_of(c, h->record, block, emission);
+        emission_of(c, c->power[h->record], block, emission);
     }
-    const float* a = c->albedo + 3 * (block & 0x7Fu); /* the material id of the 128-row table */
+    const float* a = c->albedo + 3ull * oc_material_code(block, c->s->encoding);
     albedo[0] = a[0];
     albedo[1] = a[1];
     albedo[2] = a[2];
@@ -948,14 +988,15 @@ enum { EV_EMIT = 0, EV_ALBEDO = 1, EV_NEE = 2, EV_RR = 3 };
 
 typedef struct path_event {
     uint32_t kind;
-    uint32_t index; /* brick (EMIT, NEE) or material (ALBEDO) */
+    uint32_t index; /* brick (EMIT, NEE) or material code (ALBEDO) */
+    uint32_t code;  /* EMIT, NEE: the material code of the emitting voxel */
     float factor;
 } path_event;
 
 typedef struct path_rec {
     int hit;
-    int emits0;         /* the primary emission is power[record0] */
-    uint32_t material0; /* the primary albedo row */
+    int emits0;         /* the primary emission is power[record0] times the emission of material0 */
+    uint32_t material0; /* the primary material code */
     uint32_t record0;
     int bad;            /* the fp32 radiance was not finite (the sample's radiance part is 0) */
     float radiance[3];  /* the fp32 radiance of the sample */
@@ -963,11 +1004,12 @@ typedef struct path_rec {
     path_event ev[MAX_EVENTS];
 } path_rec;
 
-static void rec_event(path_rec* rec, uint32_t kind, uint32_t index, float factor)
+static void rec_event(path_rec* rec, uint32_t kind, uint32_t index, uint32_t code, float factor)
 {
     if (rec && rec->n < MAX_EVENTS) {
         rec->ev[rec->n].kind = kind;
         rec->ev[rec->n].index = index;
+        rec->ev[rec->n].code = code;
         rec->ev[rec->n].factor = factor;
         rec->n++;
     }
@@ -991,6 +1033,12 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     for (int k = 0; k < 3; ++k) d[k] = d[k] * inv_len;
     c->rays[0]++;
     const oc_hit primary = oc_trace_ray(c->s, cam->position, d, 0.0f, RAY_TMAX);
+    if (r->voxel_id && seed == r->frame_seed) {
+        uint32_t* out = r->voxel_id + 2ull * ((uint64_t)py * r->width + px);
+        out[0] = out[1] = 0xFFFFFFFFu;
+        if (primary.hit && (r->voxel_id_tmax <= 0.0f || primary.t <= r->voxel_id_tmax))
+            oc_voxel_id(c->s, &primary, out);
+    }
     if (!primary.hit) return;
     uint32_t rng = init_random(px, py, seed);
     uint32_t light_rng = init_random(px, py, seed ^ 0x7F4A7C15u);
@@ -999,8 +1047,8 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     if (rec) {
         const uint32_t block0 = (primary.attrib >> 16) & 0xFFFFu;
         rec->hit = 1;
-        rec->emits0 = (block0 & OPAQUE) != 0 && !(primary.attrib & OC_ENTITY_HIT);
-        rec->material0 = block0 & 0x7Fu;
+        rec->emits0 = !(primary.attrib & OC_ENTITY_HIT);
+        rec->material0 = oc_material_code(block0, c->s->encoding);
         rec->record0 = primary.record;
     }
     float seg_n[3];
@@ -1010,10 +1058,10 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     uint32_t segment_light = 0;
     if (r->light_nee && r->bounce_count >= 1) {
         float nee[3], dv;
-        uint32_t lamp;
-        next_event(c, org, primary.normal, &light_rng, nee, &lamp, &dv);
+        uint32_t lamp, lamp_code;
+        next_event(c, org, primary.normal, &light_rng, nee, &lamp, &lamp_code, &dv);
         for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * throughput[k];
-        if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, dv);
+        if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, lamp_code, dv);
         segment_light = 3u; /* lamp NEE with MIS */
     }
     uint32_t bounce_index = 1;
@@ -1028,22 +1076,22 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
         if (segment_light != 0u && (em[0] > 0.0f || em[1] > 0.0f || em[2] > 0.0f))
             ew = lamp_hit_weight(c, segment_light, &h, org, dir, seg_n);
         for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
-        const uint32_t block = (h.attrib >> 16) & 0xFFFFu;
-        if ((block & OPAQUE) && !(h.attrib & OC_ENTITY_HIT)) rec_event(rec, EV_EMIT, h.record, ew);
-        rec_event(rec, EV_ALBEDO, block & 0x7Fu, 0.0f);
+        const uint32_t code = oc_material_code((h.attrib >> 16) & 0xFFFFu, c->s->encoding);
+        if (!(h.attrib & OC_ENTITY_HIT)) rec_event(rec, EV_EMIT, h.record, code, ew);
+        rec_event(rec, EV_ALBEDO, code, 0, 0.0f);
         for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
         segment_light = 0u;
         if (r->light_nee && bounce_index <= r->bounce_count) {
             segment_light = 3u;
             float nee[3], dv;
-            uint32_t lamp;
-            next_event(c, o2, h.normal, &light_rng, nee, &lamp, &dv);
+            uint32_t lamp, lamp_code;
+            next_event(c, o2, h.normal, &light_rng, nee, &lamp, &lamp_code, &dv);
             for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * (throughput[k] * (1.0f / 1.0f));
-            if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, dv);
+            if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, lamp_code, dv);
         }
         const float cp = hmax(throughput[0], hmax(throughput[1], throughput[2]));
         if (cp <= 0.0f || cp < random01(&rng)) break;
-        rec_event(rec, EV_RR, 0, 1.0f / cp);
+        rec_event(rec, EV_RR, 0, 0, 1.0f / cp);
         for (int k = 0; k < 3; ++k) throughput[k] *= 1.0f / cp;
         memcpy(org, o2, sizeof(org));
         memcpy(dir, d2, sizeof(dir));
@@ -1127,16 +1175,17 @@ void oc_render(const oc_scene* s, const oc_light_tree* t, const float* albedo, c
 typedef struct adj_job {
     const ctx* c;
     uint32_t y_begin, y_end;
-    const double* A;        /* evaluation albedo [128][3] */
+    const double* A;        /* evaluation albedo [65536][3] by material code */
     const double* P;        /* evaluation power [brick_count] */
     const float* d_radiance; /* dL/d(pixel) (gradient mode) */
     double* image;          /* evaluation mode: the double image */
-    double* dA;             /* gradient mode: this job's albedo gradient [128][3] */
+    double* dA;             /* gradient mode: this job's albedo gradient [65536][3] */
     double* dP;             /* gradient mode: this job's power gradient [brick_count] */
 } adj_job;
 
-static void eval_sample(const path_rec* rec, const double* A, const double* P, double rgb[3], double T_before[][3],
-                        double R[3])
+/* E: the material table's emission [65536][3] (held fixed). */
+static void eval_sample(const path_rec* rec, const float* E, const double* A, const double* P, double rgb[3],
+                        double T_before[][3], double R[3])
 {
     double T[3] = {1.0, 1.0, 1.0};
     R[0] = R[1] = R[2] = 0.0;
@@ -1144,17 +1193,17 @@ static void eval_sample(const path_rec* rec, const double* A, const double* P, d
         const path_event* e = &rec->ev[i];
         for (int k = 0; k < 3; ++k) T_before[i][k] = T[k];
         if (e->kind == EV_EMIT || e->kind == EV_NEE) {
-            for (int k = 0; k < 3; ++k) R[k] += P[e->index] * (double)e->factor * T[k];
+            for (int k = 0; k < 3; ++k) R[k] += P[e->index] * (double)E[3 * e->code + k] * (double)e->factor * T[k];
         } else if (e->kind == EV_ALBEDO) {
             for (int k = 0; k < 3; ++k) T[k] *= A[3 * e->index + k];
         } else {
             for (int k = 0; k < 3; ++k) T[k] *= (double)e->factor;
         }
     }
-    const double e0 = rec->emits0 ? P[rec->record0] : 0.0;
+    const double p0 = rec->emits0 ? P[rec->record0] : 0.0;
     for (int k = 0; k < 3; ++k) {
         const double sr = rec->bad ? 0.0 : (rec->radiance[k] > 65504.0f ? 65504.0 : R[k]);
-        rgb[k] = e0 + A[3 * rec->material0 + k] * sr;
+        rgb[k] = p0 * (double)E[3 * rec->material0 + k] + A[3 * rec->material0 + k] * sr;
     }
 }
 
@@ -1174,7 +1223,7 @@ static void* run_adjoint_rows(void* arg)
                 trace_pixel(&local, x, y, r->frame_seed + s, rgb32, rec);
                 if (!rec->hit) continue;
                 double rgb[3], R[3];
-                eval_sample(rec, j->A, j->P, rgb, T_before, R);
+                eval_sample(rec, local.s->emission, j->A, j->P, rgb, T_before, R);
                 for (int k = 0; k < 3; ++k) acc[k] += rgb[k];
                 if (!j->dA) continue;
                 double g[3], G[3];
@@ -1186,7 +1235,8 @@ static void* run_adjoint_rows(void* arg)
                     j->dA[3 * rec->material0 + k] += g[k] * sr;
                     G[k] = pass ? g[k] * a0[k] : 0.0;
                 }
-                if (rec->emits0) j->dP[rec->record0] += g[0] + g[1] + g[2];
+                const float* E0 = local.s->emission + 3 * rec->material0;
+                if (rec->emits0) j->dP[rec->record0] += g[0] * E0[0] + g[1] * E0[1] + g[2] * E0[2];
                 /* Backward over the events: lambda = dL/dT after the event. */
                 double lambda[3] = {0, 0, 0};
                 for (int32_t i = (int32_t)rec->n - 1; i >= 0; --i) {
@@ -1194,8 +1244,9 @@ static void* run_adjoint_rows(void* arg)
                     const double* T = T_before[i];
                     if (e->kind == EV_EMIT || e->kind == EV_NEE) {
                         const double f = (double)e->factor;
-                        j->dP[e->index] += (G[0] * T[0] + G[1] * T[1] + G[2] * T[2]) * f;
-                        for (int k = 0; k < 3; ++k) lambda[k] += G[k] * j->P[e->index] * f;
+                        const float* Ee = local.s->emission + 3 * e->code;
+                        j->dP[e->index] += (G[0] * Ee[0] * T[0] + G[1] * Ee[1] * T[1] + G[2] * Ee[2] * T[2]) * f;
+                        for (int k = 0; k < 3; ++k) lambda[k] += G[k] * j->P[e->index] * (double)Ee[k] * f;
                     } else if (e->kind == EV_ALBEDO) {
                         for (int k = 0; k < 3; ++k) {
                             j->dA[3 * e->index + k] += lambda[k] * T[k];
@@ -1217,7 +1268,7 @@ static void* run_adjoint_rows(void* arg)
 /* The frozen estimator (image, double) and/or its gradient. The paths and their sampling
  * quantities are those of the fp32 render at (albedo, power); the estimator is evaluated at
  * (A, P) (double; NULL = the fp32 parameters). d_radiance (may be NULL) = dL/d(pixel): then
- * d_albedo [128][3] and d_power [brick_count] receive dL/dA and dL/dP at (A, P). image (may be
+ * d_albedo [65536][3] and d_power [brick_count] receive dL/dA and dL/dP at (A, P). image (may be
  * NULL) receives the image at (A, P). Per-thread partial gradients are summed in thread order. */
 void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, const float* power,
                 const oc_camera* cam, const oc_render_desc* r, const double* A, const double* P,
@@ -1227,8 +1278,8 @@ void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, 
     double* a_own = NULL;
     double* p_own = NULL;
     if (!A) {
-        a_own = (double*)malloc(sizeof(double) * 128 * 3);
-        for (int i = 0; i < 128 * 3; ++i) a_own[i] = albedo[i];
+        a_own = (double*)malloc(sizeof(double) * OC_MATERIAL_CODES * 3);
+        for (int i = 0; i < OC_MATERIAL_CODES * 3; ++i) a_own[i] = albedo[i];
         A = a_own;
     }
     if (!P) {
@@ -1251,20 +1302,20 @@ void oc_adjoint(const oc_scene* s, const oc_light_tree* t, const float* albedo, 
         jobs[i].d_radiance = d_radiance;
         jobs[i].image = image;
         if (d_radiance) {
-            jobs[i].dA = (double*)calloc(128 * 3, sizeof(double));
+            jobs[i].dA = (double*)calloc(OC_MATERIAL_CODES * 3, sizeof(double));
             jobs[i].dP = (double*)calloc(nb, sizeof(double));
         }
         if (threads == 1) run_adjoint_rows(&jobs[i]);
         else pthread_create(&tids[i], NULL, run_adjoint_rows, &jobs[i]);
     }
     if (d_radiance) {
-        memset(d_albedo, 0, sizeof(double) * 128 * 3);
+        memset(d_albedo, 0, sizeof(double) * OC_MATERIAL_CODES * 3);
         memset(d_power, 0, sizeof(double) * nb);
     }
     for (int i = 0; i < threads; ++i) {
         if (threads > 1) pthread_join(tids[i], NULL);
         if (d_radiance) {
-            for (int q = 0; q < 128 * 3; ++q) d_albedo[q] += jobs[i].dA[q];
+            for (int q = 0; q < OC_MATERIAL_CODES * 3; ++q) d_albedo[q] += jobs[i].dA[q];
             for (size_t q = 0; q < nb; ++q) d_power[q] += jobs[i].dP[q];
             free(jobs[i].dA);
             free(jobs[i].dP);

@@ -85,12 +85,16 @@ def lt_build(lib, records, record_group=None, record_entry=None, group_frames=No
 
 class SceneDesc(C.Structure):
     _fields_ = [("grid", C.c_uint32 * 3), ("group_shift", C.c_uint32), ("brick_count", C.c_uint32),
-                ("pad", C.c_uint32), ("keys", C.c_void_p), ("voxels", C.c_void_p), ("power", C.c_void_p)]
+                ("encoding", C.c_uint32), ("origin", C.c_int32 * 3), ("lights", C.c_uint32),
+                ("min_emission", C.c_float), ("pad", C.c_uint32), ("keys", C.c_void_p), ("voxels", C.c_void_p),
+                ("power", C.c_void_p), ("emission", C.c_void_p)]
 
 
 class Scene(C.Structure):
-    _fields_ = [(n, C.c_uint32) for n in (
-        "grid0", "grid1", "grid2", "group_shift", "brick_count", "hash_capacity", "hash_slot_count",
+    _fields_ = [(n, C.c_uint32) for n in ("grid0", "grid1", "grid2", "group_shift")] + [
+        ("origin", C.c_int32 * 3), ("encoding", C.c_uint32), ("emission", C.c_void_p), ("light_codes", C.c_void_p),
+        ("keys", C.c_void_p)] + [(n, C.c_uint32) for n in (
+        "brick_count", "hash_capacity", "hash_slot_count",
         "hash_max_probe", "bitmap_words", "light_count", "heap_words", "group_count", "groups0", "groups1",
         "groups2", "pad")] + [(n, C.c_void_p) for n in (
         "records", "hash_slots", "bitmap", "light_headers", "light_group", "light_entry", "light_brick",
@@ -101,7 +105,7 @@ class Scene(C.Structure):
 
 class Entity(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("rot", C.c_float * 9), ("pos", C.c_float * 3), ("group_base", C.c_uint32),
-                ("power", C.c_void_p)]
+                ("id", C.c_uint32), ("power", C.c_void_p)]
 
 
 class Camera(C.Structure):
@@ -111,7 +115,8 @@ class Camera(C.Structure):
 
 class RenderDesc(C.Structure):
     _fields_ = [(n, C.c_uint32) for n in (
-        "width", "height", "spp", "bounce_count", "frame_seed", "light_nee", "x0", "y0", "x1", "y1")]
+        "width", "height", "spp", "bounce_count", "frame_seed", "light_nee", "x0", "y0", "x1", "y1")] + [
+        ("voxel_id", C.c_void_p), ("voxel_id_tmax", C.c_float), ("pad", C.c_uint32)]
 
 
 class LightTree(C.Structure):
@@ -169,8 +174,12 @@ class OracleScene:
         _bind_scene(lib)
         self.lib = lib
         self.src = scene
-        self.desc = SceneDesc((C.c_uint32 * 3)(*scene.grid), scene.group_shift, scene.brick_count, 0,
-                              scene.keys.ctypes.data, scene.voxels.ctypes.data, scene.power.ctypes.data)
+        self.origin, self.grid = scene.box()
+        self.albedo_table, self.emission_table = scene.material_tables()
+        self.desc = SceneDesc((C.c_uint32 * 3)(*self.grid), scene.group_shift, scene.brick_count, scene.encoding,
+                              (C.c_int32 * 3)(*self.origin), 1 if scene.lights else 0, scene.min_emission, 0,
+                              scene.keys.ctypes.data, scene.voxels.ctypes.data, scene.power.ctypes.data,
+                              self.emission_table.ctypes.data)
         self.s = Scene()
         lib.oc_scene_build(C.byref(self.desc), C.byref(self.s))
         s = self.s
@@ -202,9 +211,10 @@ class OracleScene:
         self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
                             self.tree["header"].ctypes.data)
 
-    def set_entities(self, entities):
+    def set_entities(self, entities, ids=None):
         """Entities beside the scene's bricks: (OracleScene of the entity's bricks, quaternion x y z w,
-        position) each, traversed in order; rotation rows as the library computes them. The
+        position) each, traversed in order; rotation rows as the library computes them; ids: their
+        entity ids (the voxel id's entity word; default 1, 2, ...). The
         entities' light records (of bricks with power) are merged into one light set in entity
         order, with its own light tree (tree 1): entity i's groups from the sum of the earlier
         entities' group counts, its heap units, brick indices and leaves after theirs (the index
@@ -222,6 +232,7 @@ class OracleScene:
             arr[i].rot[:] = [float(v) for v in rot]
             arr[i].pos[:] = [float(v) for v in np.asarray(pos, np.float32)]
             arr[i].group_base = group_base
+            arr[i].id = int(ids[i]) if ids is not None else i + 1
             arr[i].power = osc.src.power.ctypes.data
             heap = osc.heap.copy()
             r = osc.group_rows.copy()
@@ -267,6 +278,9 @@ class OracleScene:
                                      self.dyn_tree["header"].ctypes.data)
             d = Scene()
             d.group_shift = self.s.group_shift
+            d.encoding = self.s.encoding
+            d.emission = self.s.emission
+            d.light_codes = self.s.light_codes
             d.group_count = len(self.dyn_rows)
             d.light_count = light_base
             d.heap_words = len(self.dyn_heap)
@@ -299,30 +313,39 @@ class OracleScene:
         d = np.asarray(direction, np.float32)
         return self.lib.oc_trace_ray(C.byref(self.s), o.ctypes.data, d.ctypes.data, tmin, tmax)
 
-    def render(self, width, height, spp=1, bounces=4, seed=1, light_nee=True, window=None, threads=1, camera=None):
+    def render(self, width, height, spp=1, bounces=4, seed=1, light_nee=True, window=None, threads=1, camera=None,
+               voxel_ids=False, voxel_id_tmax=0.0):
+        """Radiance [height][width][3] and ray counts; with voxel_ids also the voxel id image
+        [height][width][2] (the first sample's camera rays; outside the window 0)."""
         cam = self.src.camera if camera is None else camera
         c = Camera((C.c_float * 3)(*cam["position"]), (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]),
                    (C.c_float * 3)(*cam["forward"]), float(cam["tan_half_fov_y"]), float(cam["aspect"]))
         x0, y0, x1, y1 = window or (0, 0, width, height)
-        r = RenderDesc(width, height, spp, bounces, seed, 1 if light_nee else 0, x0, y0, x1, y1)
+        ids = np.zeros((height, width, 2), np.uint32) if voxel_ids else None
+        r = RenderDesc(width, height, spp, bounces, seed, 1 if light_nee else 0, x0, y0, x1, y1,
+                       ids.ctypes.data if voxel_ids else None, float(voxel_id_tmax), 0)
         out = np.zeros((height, width, 3), np.float32)
         rays = np.zeros(3, np.uint64)
-        self.lib.oc_render(C.byref(self.s), C.byref(self.lt), self.src.albedo.ctypes.data, self.src.power.ctypes.data,
-                           C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data, threads)
+        self.lib.oc_render(C.byref(self.s), C.byref(self.lt), self.albedo_table.ctypes.data,
+                           self.src.power.ctypes.data, C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data,
+                           threads)
+        if voxel_ids:
+            return out, rays, ids
         return out, rays
 
 
     def adjoint(self, width, height, spp=1, bounces=4, seed=1, d_radiance=None, A=None, P=None, threads=8):
         """The double-precision adjoint reference (oc_adjoint): the frozen estimator's image at
         (A, P) (None: the scene's own fp32 parameters) and, with d_radiance = dL/d(pixel), the
-        gradients dL/dalbedo [128][3] and dL/dpower [brick_count]."""
+        gradients dL/dalbedo [65536][3] (by material code) and dL/dpower [brick_count]. A: the albedo
+        table [65536][3] (None: the scene's)."""
         cam = self.src.camera
         c = Camera((C.c_float * 3)(*cam["position"]), (C.c_float * 3)(*cam["right"]), (C.c_float * 3)(*cam["up"]),
                    (C.c_float * 3)(*cam["forward"]), float(cam["tan_half_fov_y"]), float(cam["aspect"]))
-        r = RenderDesc(width, height, spp, bounces, seed, 1, 0, 0, width, height)
+        r = RenderDesc(width, height, spp, bounces, seed, 1, 0, 0, width, height, None, 0.0, 0)
         nb = max(self.s.brick_count, 1)
         image = np.zeros((height, width, 3), np.float64)
-        dA = np.zeros((128, 3), np.float64)
+        dA = np.zeros((65536, 3), np.float64)
         dP = np.zeros(nb, np.float64)
         a_ptr = p_ptr = None
         if A is not None:
@@ -335,7 +358,7 @@ class OracleScene:
         if d_radiance is not None:
             d_radiance = np.ascontiguousarray(d_radiance, np.float32)
             g_ptr = d_radiance.ctypes.data
-        self.lib.oc_adjoint(C.byref(self.s), C.byref(self.lt), self.src.albedo.ctypes.data, self.src.power.ctypes.data,
+        self.lib.oc_adjoint(C.byref(self.s), C.byref(self.lt), self.albedo_table.ctypes.data, self.src.power.ctypes.data,
                             C.byref(c), C.byref(r), a_ptr, p_ptr, g_ptr, image.ctypes.data, dA.ctypes.data,
                             dP.ctypes.data, threads)
         return image, dA, dP[: self.s.brick_count]

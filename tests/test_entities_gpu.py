@@ -54,6 +54,9 @@ def test_entities_parity(cuda_device, oracle):
     assert (e1, e2) == (1, 2)
     scene.upload_bricks(b1.keys, b1.voxels, entity=e1)
     scene.upload_bricks(b2.keys, b2.voxels, entity=e2)
+    # Entity bricks emit with power 1 until set: these start dark.
+    scene.set_brick_power(b1.keys, b1.power, entity=e1)
+    scene.set_brick_power(b2.keys, b2.power, entity=e2)
     scene.set_entity_motion(e2, 1)
     scene.flush()
 
@@ -90,6 +93,7 @@ def test_entities_parity(cuda_device, oracle):
     e3 = scene.add_entity(p1, IDENTITY)
     assert e3 == e1
     scene.upload_bricks(b1.keys, b1.voxels, entity=e3)
+    scene.set_brick_power(b1.keys, b1.power, entity=e3)
     scene.flush()
     osc.set_entities([(o1, IDENTITY, p1), (o2, IDENTITY, p2)])
     render_pair(cuda_device, scene, osc, vs)

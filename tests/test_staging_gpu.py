@@ -17,10 +17,11 @@ def incremental_scene(cuda_device, vs, rng, pieces=5):
     upload of its brick, half after."""
     import caelix_b200
 
-    s = caelix_b200.Scene(cuda_device, vs.group_shift)
+    s = caelix_b200.Scene.for_voxel_scene(cuda_device, vs)
     n = vs.brick_count
     emissive = np.nonzero(vs.power > 0)[0]
-    early = emissive[: len(emissive) // 2]
+    dark = np.nonzero(vs.power <= 0)[0]
+    early = np.concatenate([emissive[: len(emissive) // 2], dark[: len(dark) // 2]])
     if len(early):
         s.set_brick_power(vs.keys[early], vs.power[early])
     junk = rng.choice(n, size=n // 3, replace=False)
@@ -33,10 +34,9 @@ def incremental_scene(cuda_device, vs, rng, pieces=5):
         keys = np.concatenate([vs.keys[rep], vs.keys[part]])
         vox = np.concatenate([np.full((len(rep), 512), 0x8003, np.uint16), vs.voxels[part]])
         s.upload_bricks(keys, vox)
-    late = emissive[len(emissive) // 2:]
+    late = np.concatenate([emissive[len(emissive) // 2:], dark[len(dark) // 2:]])
     if len(late):
         s.set_brick_power(vs.keys[late], vs.power[late])
-    s.set_albedo(vs.albedo)
     s.flush()
     return s
 
@@ -71,7 +71,7 @@ def test_config2_incremental_then_edit(cuda_device, oracle):
     allvox = np.concatenate([voxels, extra_vox])
     lin = keys[:, 0] + (gx + 2) * (keys[:, 1] + (gy + 1) * keys[:, 2].astype(np.int64))
     o = np.argsort(lin, kind="stable")
-    power = np.concatenate([vs.power, np.zeros(3, np.float32)])
+    power = np.concatenate([vs.power, np.ones(3, np.float32)])  # a new brick's power is 1 until set
     edited = workloads.VoxelScene((gx + 2, gy + 1, gz + 4), keys[o], allvox[o], power[o], vs.albedo, vs.camera,
                                   vs.group_shift)
     scene.upload_bricks(np.concatenate([vs.keys[edit], extra]), np.concatenate([voxels[edit], extra_vox]))
@@ -86,17 +86,15 @@ def test_empty_and_power_only_flushes(cuda_device, oracle):
     import caelix_b200
 
     vs = workloads.noise_world(grid_bricks=(6, 6, 6), brick_occupancy=0.5, emissive_fraction=0.1, seed=4)
-    s = caelix_b200.Scene(cuda_device, vs.group_shift)
+    s = caelix_b200.Scene.for_voxel_scene(cuda_device, vs)
     s.flush()
     assert s.view().brick_count == 0
     s.upload_bricks(vs.keys, vs.voxels)
-    s.set_albedo(vs.albedo)
     s.flush()
-    dark = workloads.VoxelScene(vs.grid, vs.keys, vs.voxels, np.zeros_like(vs.power), vs.albedo, vs.camera,
-                                vs.group_shift)
-    assert_scene_equal(s, oracle_lib.OracleScene(oracle, dark), dark)
-    emissive = vs.power > 0
-    s.set_brick_power(vs.keys[emissive], vs.power[emissive])
+    # Every brick's power is 1 until set: every brick emits.
+    lit = vs.like(power=np.ones_like(vs.power))
+    assert_scene_equal(s, oracle_lib.OracleScene(oracle, lit), lit)
+    s.set_brick_power(vs.keys, vs.power)
     s.flush()
     assert_scene_equal(s, oracle_lib.OracleScene(oracle, vs), vs)
     s.close()
@@ -157,8 +155,8 @@ def test_remove_bricks(cuda_device, oracle):
     """caelix_scene_remove_bricks: a quarter of the bricks removed (every brick of the highest x
     plane among them, so the grid shrinks; emissive bricks; repeated, absent and out-of-range keys
     that are ignored), then some of them uploaded again (one emissive brick without its power: it
-    comes back dark), then every brick removed. Each flushed state equals the oracle's build of the
-    remaining bricks, and so does the render."""
+    comes back with the default power 1), then every brick removed. Each flushed state equals the oracle's build of the
+    remaining bricks, and so does the render. A brick uploaded again has power 1 until set."""
     import caelix_b200
 
     vs = workloads.noise_world(grid_bricks=(9, 7, 8), brick_occupancy=0.5, emissive_fraction=0.08, seed=5)
@@ -168,7 +166,7 @@ def test_remove_bricks(cuda_device, oracle):
     top = np.nonzero(vs.keys[:, 0] == vs.keys[:, 0].max())[0]
     gone = np.unique(np.concatenate([rng.choice(n, size=n // 4, replace=False), top,
                                      np.nonzero(vs.power > 0)[0][:3]]))
-    extra = np.array([[vs.grid[0] + 5, 0, 0], [-1, 2, 2], [0, -3, 1]], np.int32)  # absent, out of range
+    extra = np.array([[vs.grid[0] + 5, 0, 0], [-1, 2, 2], [0, -3, 1], [1 << 21, 0, 0]], np.int32)  # absent, out of range
     scene.remove_bricks(np.concatenate([vs.keys[gone], vs.keys[gone[:10]], extra]))
     scene.flush()
     keep = np.setdiff1d(np.arange(n), gone)
@@ -183,12 +181,13 @@ def test_remove_bricks(cuda_device, oracle):
     back = gone[rng.random(len(gone)) < 0.5]
     lit_back = back[vs.power[back] > 0]
     scene.upload_bricks(vs.keys[back], vs.voxels[back])
-    if len(lit_back) > 1:
-        scene.set_brick_power(vs.keys[lit_back[1:]], vs.power[lit_back[1:]])
+    unset = lit_back[:1]
+    set_back = np.setdiff1d(back, unset)
+    if len(set_back):
+        scene.set_brick_power(vs.keys[set_back], vs.power[set_back])
     scene.flush()
     power = vs.power.copy()
-    if len(lit_back):
-        power[lit_back[0]] = 0.0
+    power[unset] = 1.0
     now = np.union1d(keep, back)
     cur = scene_of(vs.keys[now], vs.voxels[now], power[now], vs)
     osc = oracle_lib.OracleScene(oracle, cur)

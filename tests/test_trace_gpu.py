@@ -30,8 +30,13 @@ def assert_scene_equal(scene, osc, vs):
     v = scene.view()
     n = vs.brick_count
     assert v.brick_count == n
-    assert tuple(v.grid) == tuple(vs.grid)
+    assert tuple(v.grid) == tuple(osc.grid) and tuple(v.origin) == tuple(osc.origin)
+    assert v.encoding == vs.encoding
     assert fetch(v, np.int32, "keys", 3 * n).reshape(n, 3).tobytes() == vs.keys.tobytes()
+    words = int(osc.s.bitmap_words)
+    bitmap = np.ctypeslib.as_array(oracle_lib.C.cast(osc.s.bitmap, oracle_lib.C.POINTER(oracle_lib.C.c_uint32)),
+                                   (max(words, 1),))[:words]
+    assert np.array_equal(fetch(v, np.uint32, "bitmap", words), bitmap)
     rec = fetch(v, np.uint32, "records", 274 * n).reshape(n, 274)
     assert np.array_equal(rec, osc.records)
     assert v.hash_slot_count == osc.hash_slots.shape[0]

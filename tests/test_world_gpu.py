@@ -20,7 +20,7 @@ def test_world_file_into_scene(cuda_device, oracle, tmp_path):
     path = tmp_path / "world.cxw"
     path.write_bytes(W.from_voxel_scene(vs, shift))
     f = caelix_b200.WorldFile(str(path))
-    scene = caelix_b200.Scene(cuda_device, vs.group_shift)
+    scene = caelix_b200.Scene.for_voxel_scene(cuda_device, vs)
     origin, bricks = f.upload_entity(0, scene, threads=4)
     keep = (vs.voxels != 0).any(axis=1)  # the reader drops all-air bricks
     keys = vs.keys[keep]
@@ -32,9 +32,7 @@ def test_world_file_into_scene(cuda_device, oracle, tmp_path):
     o = np.argsort(lin, kind="stable")
     exp = workloads.VoxelScene(grid, moved[o], vs.voxels[keep][o], vs.power[keep][o], vs.albedo, vs.camera,
                                vs.group_shift)
-    emissive = exp.power > 0
-    scene.set_brick_power(exp.keys[emissive], exp.power[emissive])
-    scene.set_albedo(exp.albedo)
+    scene.set_brick_power(exp.keys, exp.power)
     scene.flush()
     assert_scene_equal(scene, oracle_lib.OracleScene(oracle, exp), exp)
     scene.close()
@@ -74,7 +72,7 @@ def test_world_load_with_entities(cuda_device, oracle, tmp_path):
     path = tmp_path / "entities.cxw"
     path.write_bytes(W.build(world_file))
     f = caelix_b200.WorldFile(str(path))
-    scene = caelix_b200.Scene(cuda_device, vs.group_shift)
+    scene = caelix_b200.Scene.for_voxel_scene(cuda_device, vs)
     ids, bricks = f.load(scene, threads=4)
     assert ids == [0, 1]
     keep0 = (vs.voxels != 0).any(axis=1)
@@ -92,10 +90,9 @@ def test_world_load_with_entities(cuda_device, oracle, tmp_path):
                                     src.group_shift)
 
     world = moved(vs, vs.keys[keep0], vs.voxels[keep0], vs.power[keep0], shift0, org0)
-    body = moved(ent, ent.keys[keep1], ent.voxels[keep1], ent.power[keep1], shift1, org1)
-    emissive = world.power > 0
-    scene.set_brick_power(world.keys[emissive], world.power[emissive])
-    scene.set_albedo(world.albedo)
+    # The loader sets no power: the entity's bricks keep the default power 1 (they emit).
+    body = moved(ent, ent.keys[keep1], ent.voxels[keep1], np.ones(int(keep1.sum()), np.float32), shift1, org1)
+    scene.set_brick_power(world.keys, world.power)
     scene.flush()
     assert_scene_equal(scene, oracle_lib.OracleScene(oracle, world), world)
 
