@@ -54,11 +54,12 @@ CaelixResult cuda_result(cudaError_t e, const char* what)
 CaelixResult status_result(uint32_t status, const char* what)
 {
     if (status == 0) return CAELIX_OK;
-    log(CAELIX_LOG_ERROR, "%s: device status 0x%x%s%s%s%s%s", what, status,
+    log(CAELIX_LOG_ERROR, "%s: device status 0x%x%s%s%s%s%s%s%s", what, status,
         (status & kStatusLookbackTimeout) ? " lookback-timeout" : "",
         (status & kStatusDepthGuard) ? " depth-guard" : "", (status & kStatusNodeOverflow) ? " node-overflow" : "",
         (status & kStatusHashProbeLimit) ? " hash-probe-limit" : "",
-        (status & kStatusRecordOverflow) ? " record-overflow" : "");
+        (status & kStatusRecordOverflow) ? " record-overflow" : "", (status & kStatusBadGroup) ? " bad-group" : "",
+        (status & kStatusCopyTimeout) ? " copy-timeout" : "");
     return CAELIX_ERROR_DEVICE_STATUS;
 }
 

@@ -127,5 +127,6 @@ constexpr uint32_t kStatusNodeOverflow = 1u << 2;     // more 4-wide nodes than 
 constexpr uint32_t kStatusHashProbeLimit = 1u << 3;   // a hash probe ran past the table
 constexpr uint32_t kStatusRecordOverflow = 1u << 4;   // a light record did not fit its capacity
 constexpr uint32_t kStatusBadGroup = 1u << 5;         // a record named a group without a frame
+constexpr uint32_t kStatusCopyTimeout = 1u << 6;      // a bulk copy into shared memory did not arrive in time
 
 }  // namespace cx

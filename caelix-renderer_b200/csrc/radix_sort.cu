@@ -1,4 +1,5 @@
 // Kernels of the onesweep radix sort (radix_sort.cuh describes the algorithm).
+#include <algorithm>
 #include <atomic>
 
 #include "cx_device.cuh"
@@ -224,6 +225,214 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
     }
 }
 
+// ---------------------------------------------------------------------------------------------
+// The persistent, software-pipelined pass: a CTA stays resident and takes tile after tile. While
+// it ranks, looks back and writes one tile, the keys and values of its next tile come into shared
+// memory by 1-D bulk copies (cp.async.bulk, completion counted on an mbarrier of the CTA; the
+// source is this GPU's own memory), so the loads of a tile overlap the look-back and the stores of
+// the tile before, and the values are in shared memory before the look-back ends. The ranking, the
+// look-back and the output are the plain pass's (the same stable permutation). Two CTAs per SM.
+constexpr uint32_t kPipeTile = kSortThreads * kSortKeysPerThread;  // 4096
+constexpr uint32_t kPipeMinTiles = 64;
+
+struct PipeShared
+{
+    uint32_t raw_keys[2][kPipeTile];
+    uint32_t raw_values[2][kPipeTile];
+    uint32_t keys[kPipeTile];
+    uint32_t values[kPipeTile];
+    uint32_t warp_counts[kSortWarps][kRadix];
+    uint32_t local[kRadix];
+    uint32_t dest[kRadix];
+    uint32_t base[kRadix];
+    uint32_t scan[kSortWarps];
+    uint32_t tile[2];
+    unsigned long long bar[2];
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, uint32_t arrivals)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(arrivals) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes, unsigned long long* bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// Thread 0: the bulk copies of tile t into stage `stage` (its whole 16-byte units; the tail of a
+// last tile is loaded by plain loads after the wait).
+__device__ __forceinline__ void pipe_issue(const SortPass& a, PipeShared& S, uint32_t t, uint32_t stage)
+{
+    const uint32_t base = t * kPipeTile;
+    const uint32_t count = min(a.n - base, kPipeTile);
+    const uint32_t bytes = (count * 4u) & ~15u;
+    const bool values = a.values_in != nullptr;
+    // Reads of this buffer by the generic proxy (the tile two steps back) come before the copy.
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&S.bar[stage], values ? 2u * bytes : bytes);
+    if (bytes) {
+        bulk_load(S.raw_keys[stage], a.keys_in + base, bytes, &S.bar[stage]);
+        if (values) bulk_load(S.raw_values[stage], a.values_in + base, bytes, &S.bar[stage]);
+    }
+}
+
+__global__ void __launch_bounds__(kSortThreads, 2) onesweep_pipe_kernel(const SortPass a, uint32_t tiles)
+{
+    extern __shared__ __align__(128) unsigned char pipe_smem[];
+    PipeShared& S = *reinterpret_cast<PipeShared*>(pipe_smem);
+    constexpr int KPT = kSortKeysPerThread;
+    const uint32_t tid = threadIdx.x;
+    const uint32_t lane = tid & 31u;
+    const uint32_t warp = tid >> 5;
+    const uint32_t d = tid;  // the digit of this thread in the per-digit phases
+    {
+        uint32_t digit_total;
+        S.base[d] = block_exclusive_sum<kSortThreads>(a.counts[d], S.scan, digit_total);
+    }
+    if (tid == 0) {
+        mbar_init(&S.bar[0], 1);
+        mbar_init(&S.bar[1], 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const uint32_t t = atomicAdd(a.tile_counter, 1u);
+        S.tile[0] = t;
+        if (t < tiles) pipe_issue(a, S, t, 0);
+    }
+    __syncthreads();
+    uint32_t stage = 0, parity = 0;  // parity bit s: the phase of stage s's barrier to wait for
+    for (;;) {
+        const uint32_t tile = S.tile[stage];
+        if (tile >= tiles) break;
+        if (tid == 0) {
+            const uint32_t next = atomicAdd(a.tile_counter, 1u);
+            S.tile[stage ^ 1u] = next;
+            if (next < tiles) pipe_issue(a, S, next, stage ^ 1u);
+        }
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) S.warp_counts[w][tid] = 0;
+        // This tile's copies (a bounded wait: a copy that never lands sets a status bit).
+        {
+            const uint32_t ph = (parity >> stage) & 1u;
+            uint32_t spins = 0;
+            while (!mbar_try_wait(&S.bar[stage], ph)) {
+                if (!spin_wait(spins)) {
+                    if (tid == 0) atomicOr(a.status, kStatusCopyTimeout);
+                    break;
+                }
+            }
+            parity ^= 1u << stage;
+        }
+        const uint32_t base = tile * kPipeTile;
+        const uint32_t count = min(a.n - base, kPipeTile);
+        const uint32_t bulk = ((count * 4u) & ~15u) / 4u;
+        if (tid < count - bulk) {  // the last tile's tail (under 4 elements)
+            S.raw_keys[stage][bulk + tid] = __ldg(a.keys_in + base + bulk + tid);
+            if (a.values_in) S.raw_values[stage][bulk + tid] = __ldg(a.values_in + base + bulk + tid);
+        }
+        __syncthreads();
+        const uint32_t warp_base = base + warp * 32u * KPT;
+        const uint32_t local_base = warp * 32u * KPT;
+        uint32_t key[KPT];
+        TilePositions<KPT> pos;
+#pragma unroll
+        for (int k = 0; k < KPT / 2; ++k) pos.w[k] = 0;
+#pragma unroll
+        for (int k = 0; k < KPT; ++k) {
+            const uint32_t e = local_base + k * 32u + lane;
+            key[k] = e < count ? S.raw_keys[stage][e] : 0u;
+        }
+        warp_rank<KPT>(key, warp_base, a.n, a.shift, S.warp_counts[warp], pos);
+        __syncthreads();
+        uint32_t total = 0;
+#pragma unroll
+        for (int w = 0; w < kSortWarps; ++w) {
+            const uint32_t c = S.warp_counts[w][d];
+            S.warp_counts[w][d] = total;
+            total += c;
+        }
+        uint32_t* state = a.tile_states + (uint64_t)tile * kRadix + d;
+        const bool publish = tile != a.silent_tile;
+        if (publish) st_relaxed(state, (tile == 0 ? kTileFlagPrefix : kTileFlagAggregate) | total);
+        uint32_t tile_total;
+        const uint32_t local = block_exclusive_sum<kSortThreads>(total, S.scan, tile_total);
+        S.local[d] = local;
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < KPT; ++k) {
+            const uint32_t e = local_base + k * 32u + lane;
+            if (e < count) {
+                const uint32_t digit = (key[k] >> a.shift) & 255u;
+                pos.add(k, S.local[digit] + S.warp_counts[warp][digit]);
+                const uint32_t p = pos.get(k);
+                S.keys[p] = key[k];
+                S.values[p] = a.values_in ? S.raw_values[stage][e] : base + e;
+            }
+        }
+        uint32_t exclusive = 0;
+        if (tile != 0) {
+            int64_t j = (int64_t)tile - 1;
+            uint32_t spins = 0;
+            while (j >= 0) {
+                const uint32_t s = ld_relaxed(a.tile_states + (uint64_t)j * kRadix + d);
+                if ((s & ~kTileValueMask) == 0) {
+                    if (!spin_wait(spins, a.spin_limit)) {
+                        atomicOr(a.status, kStatusLookbackTimeout);
+                        break;
+                    }
+                    continue;
+                }
+                exclusive += s & kTileValueMask;
+                if (s & kTileFlagPrefix) break;
+                --j;
+            }
+            if (publish) st_relaxed(state, kTileFlagPrefix | (exclusive + total));
+        }
+        S.dest[d] = S.base[d] + exclusive - local;
+        __syncthreads();
+        for (uint32_t j = tid; j < count; j += kSortThreads) {
+            const uint32_t k = S.keys[j];
+            const uint32_t v = S.values[j];
+            const uint32_t dest = S.dest[(k >> a.shift) & 255u] + j;
+            a.keys_out[dest] = k;
+            a.values_out[dest] = v;
+            if (a.rows_in) {
+                const uint4* src = a.rows_in + (uint64_t)a.rows_in_stride * v;
+                uint4* dst = a.rows_out + 3ull * dest;
+                const uint4 r0 = __ldg(src);
+                const uint4 r1 = __ldg(src + 1);
+                const uint4 r2 = __ldg(src + 2);
+                dst[0] = r0;
+                dst[1] = r1;
+                dst[2] = r2;
+                a.inverse[v] = dest;
+            }
+        }
+        __syncthreads();
+        stage ^= 1u;
+    }
+}
+
 // A whole sort of n <= kSmallSortKeys pairs by one CTA: the four passes of the onesweep ranking
 // over one tile held in shared memory (a stable LSD sort: the same permutation as the onesweep
 // passes), then the output with the optional row gather of the last pass. One launch instead of
@@ -324,6 +533,23 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
     }
     if (!sort_keys_per_thread_ok(keys_per_thread)) keys_per_thread = kSortKeysPerThread;
     const uint32_t tiles = sort_tiles(n, keys_per_thread);
+    // The pipelined pass for sorts of at least kPipeMinTiles tiles of 4096 pairs whose arrays start
+    // on 16-byte boundaries (the bulk copies' rule); the plain pass otherwise.
+    const auto aligned = [](const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+    const bool pipe = keys_per_thread == (uint32_t)kSortKeysPerThread && tiles >= kPipeMinTiles && aligned(keys_a) &&
+                      aligned(keys_b) && aligned(values_a) && aligned(values_b);
+    uint32_t pipe_grid = 0;
+    if (pipe) {
+        static int per_sm = 0;
+        if (per_sm == 0) {
+            cudaFuncSetAttribute(onesweep_pipe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(PipeShared));
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, onesweep_pipe_kernel, kSortThreads,
+                                                          sizeof(PipeShared));
+            per_sm = per_sm > 0 ? per_sm : 1;
+        }
+        pipe_grid = std::min<uint32_t>(tiles, current_sm_count() * (uint32_t)per_sm);
+    }
     uint32_t* hist = scratch;
     uint32_t* counters = scratch + 4 * kRadix;
     uint32_t* states = counters + 4;
@@ -350,7 +576,8 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         p.inverse = (last && gather) ? gather->inverse : nullptr;
         p.silent_tile = (pass == 0 && wait_test) ? wait_test->silent_tile : 0xFFFFFFFFu;
         p.spin_limit = wait_test ? wait_test->spin_limit : kSpinLimit;
-        if (keys_per_thread == 4) onesweep_pass_kernel<4><<<tiles, kSortThreads, 0, stream>>>(p);
+        if (pipe) onesweep_pipe_kernel<<<pipe_grid, kSortThreads, sizeof(PipeShared), stream>>>(p, tiles);
+        else if (keys_per_thread == 4) onesweep_pass_kernel<4><<<tiles, kSortThreads, 0, stream>>>(p);
         else if (keys_per_thread == 8) onesweep_pass_kernel<8><<<tiles, kSortThreads, 0, stream>>>(p);
         else onesweep_pass_kernel<16><<<tiles, kSortThreads, 0, stream>>>(p);
         uint32_t* t = kin;

@@ -368,3 +368,90 @@ def RECORD_DTYPE_LOCAL():
     from caelix_b200 import workloads
 
     return workloads.RECORD_DTYPE
+
+
+def group_frames_of(origin, grid, group_shift):
+    """The frames of a scene's groups (identity rotation, the group's voxel origin), in group order."""
+    from caelix_b200 import workloads
+
+    groups = [(g + (1 << group_shift) - 1) >> group_shift for g in grid]
+    n = groups[0] * groups[1] * groups[2]
+    fr = np.zeros(n, workloads.FRAME_DTYPE)
+    g = np.arange(n)
+    cell = np.stack([g % groups[0], (g // groups[0]) % groups[1], g // (groups[0] * groups[1])], -1)
+    fr["origin"] = (8 * (np.asarray(origin, np.int64) + (cell.astype(np.int64) << group_shift))).astype(np.float32)
+    fr["rotation"][:, [0, 4, 8]] = 1.0
+    return fr, groups
+
+
+class TablesScene(OracleScene):
+    """The oracle's trace over a scene's device-built tables (records, hash table, bitmap, light
+    blocks and light records, as CaelixSceneView hands them out), with the light tree built by the
+    oracle from those light records: for worlds whose full oracle build would take too long, the
+    trace and the light tree are still the oracle's own restatement."""
+
+    def __init__(self, lib, vs, view):
+        import gpu_util
+        from caelix_b200 import workloads
+
+        _bind_scene(lib)
+        lib.oc_light_codes.argtypes = [C.c_void_p, C.c_uint32, C.c_float, C.c_void_p]
+        lib.oc_light_codes.restype = None
+        self.lib = lib
+        self.src = vs
+        v = view
+        self.origin = tuple(int(x) for x in v.origin)
+        self.grid = tuple(int(x) for x in v.grid)
+        self.albedo_table, self.emission_table = vs.material_tables()
+        n = int(v.brick_count)
+        self.records = gpu_util.from_device(v.records, np.uint32, 274 * n)
+        self.hash_slots = gpu_util.from_device(v.hash_slots, np.uint32, 4 * int(v.hash_slot_count))
+        cells = self.grid[0] * self.grid[1] * self.grid[2]
+        self.bitmap = gpu_util.from_device(v.bitmap, np.uint32, (cells + 31) // 32)
+        self.keys_dev = gpu_util.from_device(v.keys, np.int32, 3 * n)
+        m = int(v.light_count)
+        self.light_count = m
+        self.light_headers = gpu_util.from_device(v.light_headers, workloads.RECORD_DTYPE, m)
+        self.light_group = gpu_util.from_device(v.light_group, np.uint32, m)
+        self.light_entry = gpu_util.from_device(v.light_entry, np.uint32, m)
+        self.light_brick = gpu_util.from_device(v.light_brick, np.uint32, m)
+        self.heap = gpu_util.from_device(v.heap, np.uint32, int(v.heap_words))
+        self.group_rows = gpu_util.from_device(v.group_rows, np.uint32, 8 * int(v.group_count)).reshape(-1, 8)
+        self.group_frames, groups = group_frames_of(self.origin, self.grid, int(v.group_shift))
+        self.light_codes = np.zeros(2048, np.uint32)
+        lib.oc_light_codes(self.emission_table.ctypes.data, vs.encoding, vs.min_emission, self.light_codes.ctypes.data)
+        s = Scene()
+        s.grid0, s.grid1, s.grid2 = self.grid
+        s.group_shift = int(v.group_shift)
+        s.origin[:] = self.origin
+        s.encoding = vs.encoding
+        s.emission = self.emission_table.ctypes.data
+        s.light_codes = self.light_codes.ctypes.data
+        s.keys = self.keys_dev.ctypes.data
+        s.brick_count = n
+        s.hash_capacity = int(v.hash_capacity)
+        s.hash_slot_count = int(v.hash_slot_count)
+        s.hash_max_probe = int(v.hash_max_probe)
+        s.bitmap_words = len(self.bitmap)
+        s.light_count = m
+        s.heap_words = int(v.heap_words)
+        s.group_count = int(v.group_count)
+        s.groups0, s.groups1, s.groups2 = groups
+        s.records = self.records.ctypes.data
+        s.hash_slots = self.hash_slots.ctypes.data
+        s.bitmap = self.bitmap.ctypes.data
+        s.light_headers = self.light_headers.ctypes.data
+        s.light_group = self.light_group.ctypes.data
+        s.light_entry = self.light_entry.ctypes.data
+        s.light_brick = self.light_brick.ctypes.data
+        s.heap = self.heap.ctypes.data
+        s.group_rows = self.group_rows.ctypes.data
+        s.group_frames = self.group_frames.ctypes.data
+        self.s = s
+        self.tree = lt_build(lib, self.light_headers, record_group=self.light_group, record_entry=self.light_entry,
+                             group_frames=self.group_frames, leaf_capacity=max(m, 1))
+        self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
+                            self.tree["header"].ctypes.data)
+
+    def close(self):
+        pass  # the arrays are numpy-owned

@@ -212,3 +212,58 @@ def test_batch_after_entity_removed(cuda_device):
     batch.close()
     r.close()
     scene.close()
+
+
+def test_full_batch_plan_views_match_the_oracle(cuda_device, oracle):
+    """The real 64-scene plan of the batched workload (brick counts log-uniform in [1k, 500k],
+    viewports among 256/512/1024, 2 spp, 4 bounces) in one batch run: a pixel window of six views
+    (the three smallest scenes: the oracle's own build; the three largest: the oracle's trace over
+    their flushed tables) equals the oracle within 1e-5 relative; every view's ray counts equal
+    its plain render's."""
+    import torch
+
+    import caelix_b200
+    from test_trace_gpu import assert_radiance_close
+
+    plan = workloads.batch_plan(64)
+    order = sorted(range(len(plan)), key=lambda i: plan[i][0])
+    checked = order[:3] + order[-3:]
+    scenes, renderers, views, worlds = [], [], [], {}
+    for i, (count, side) in enumerate(plan):
+        vs = workloads.batch_scene(count, seed=100 + i)
+        scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+        renderer = caelix_b200.Renderer(cuda_device, scene)
+        out = torch.zeros(side * side * 3, dtype=torch.float32, device="cuda")
+        views.append((renderer, out, side, side, vs.camera, 4, 1 + i, 2))
+        scenes.append(scene)
+        renderers.append(renderer)
+        if i in checked:
+            worlds[i] = vs
+        del vs
+    batch = caelix_b200.Batch(cuda_device, views, rebuild_light_trees=True)
+    batch.set_tuning(min_blocks=8, block_width=8, refill_min=4, order=1, sort_keys_per_thread=16, kernel=1,
+                     wavefront=1 << 22)
+    batch.run()
+    batch.stats()
+    for i in checked:
+        renderer, out, w, h, cam, bounces, seed, spp = views[i]
+        got = out.cpu().numpy().reshape(h, w, 3)
+        vs = worlds[i]
+        small = i in order[:3]
+        osc = oracle_lib.OracleScene(oracle, vs) if small else oracle_lib.TablesScene(oracle, vs, scenes[i].view())
+        x0, y0 = w // 2 - 16, h // 2 - 16
+        ref, _ = osc.render(w, h, spp=spp, bounces=bounces, seed=seed, window=(x0, y0, x0 + 32, y0 + 32), threads=16)
+        assert_radiance_close(got[y0:y0 + 32, x0:x0 + 32], ref[y0:y0 + 32, x0:x0 + 32])
+        assert float(ref[y0:y0 + 32, x0:x0 + 32].max()) > 0.0, i
+        st = batch.view_stats(i)
+        plain = torch.zeros_like(out)
+        renderer.render(plain, w, h, cam, bounces=bounces, seed=seed, spp=spp)
+        ps = renderer.stats()
+        assert (st.primary_rays, st.bounce_rays, st.shadow_rays) == (ps.primary_rays, ps.bounce_rays, ps.shadow_rays)
+        assert torch.equal(plain, out)
+        osc.close()
+    batch.close()
+    for r in renderers:
+        r.close()
+    for s in scenes:
+        s.close()
