@@ -69,6 +69,7 @@ struct CaelixBatch
     bool rebuild = true;
     std::vector<CaelixScene*> scenes;       // distinct scenes, in order of first appearance
     std::vector<uint64_t> generations;      // of the scenes when the graph was captured
+    std::vector<uint64_t> entity_generations;  // of the scenes' entity views then
     CaelixBatchTuning tuning = default_tuning();
     cx::BatchView* d_views = nullptr;
     cx::WaveView* d_wave_views = nullptr;
@@ -94,6 +95,15 @@ struct CaelixBatch
 };
 
 namespace {
+
+// The kernel organisation a run uses: the tuning's, except that views of scenes with entities are
+// traced by the wavefront kernels (the persistent kernel traces world bricks only).
+uint32_t run_kernel(const CaelixBatch* b, const CaelixBatchTuning& t)
+{
+    for (const CaelixScene* s : b->scenes)
+        if (s->entity_view_count) return CAELIX_BATCH_WAVEFRONT;
+    return t.kernel;
+}
 
 void release(CaelixBatch* b)
 {
@@ -138,7 +148,7 @@ cudaError_t upload_views(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t* i
         const CaelixBatchView& v = b->views[i];
         cx::BatchView& h = host[j];
         std::memset(&h, 0, sizeof(h));
-        h.scene = cx::scene_view(v.renderer->scene->dev);
+        h.scene = render_view(v.renderer->scene);
         const CaelixResult r = render_params(v.renderer, &v.target, &v.camera, &v.options, "caelix_batch_run", &h.params);
         if (r != CAELIX_OK) return cudaErrorInvalidValue;
         h.radiance = reinterpret_cast<float*>(v.target.radiance);
@@ -159,7 +169,7 @@ cudaError_t upload_views(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t* i
     }
     *item_count = (uint32_t)items;
     CX_TRY(cudaMemcpy(b->d_views, host.data(), sizeof(cx::BatchView) * n, cudaMemcpyHostToDevice));
-    if (t.kernel != CAELIX_BATCH_WAVEFRONT) return cudaSuccess;
+    if (run_kernel(b, t) != CAELIX_BATCH_WAVEFRONT) return cudaSuccess;
     // The wavefront organisation: its view table, wave plan and path state.
     CX_TRY(cudaMemcpy(b->d_wave_views, b->wave_views.data(), sizeof(cx::WaveView) * n, cudaMemcpyHostToDevice));
     b->plan = cx::wave_plan(b->wave_views.data(), n, bw);
@@ -197,14 +207,23 @@ cudaError_t record(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t item_cou
         CX_TRY(cudaEventRecord(b->fork, s));
         const uint32_t used = std::min<uint32_t>(kMaxBranches, (uint32_t)b->scenes.size());
         for (uint32_t j = 0; j < used; ++j) CX_TRY(cudaStreamWaitEvent(b->branches[j], b->fork, 0));
-        for (size_t i = 0; i < b->scenes.size(); ++i)
-            CX_TRY(cx::scene_build_light_tree(b->scenes[i]->dev, b->branches[i % used], t.sort_keys_per_thread));
+        uint32_t branch = 0;
+        for (size_t i = 0; i < b->scenes.size(); ++i) {
+            CaelixScene* sc = b->scenes[i];
+            CX_TRY(cx::scene_build_light_tree(sc->dev, b->branches[branch++ % used], t.sort_keys_per_thread));
+            if (sc->dyn_live) {  // the entities' light tree
+                cx::LightBvhInput in = sc->dyn_input;
+                in.sort_keys_per_thread = t.sort_keys_per_thread;
+                CX_TRY(cx::lt_build(cx::lt_carve(sc->dyn_tree.ptr, sc->dyn_tree_capacity), in,
+                                    b->branches[branch++ % used], nullptr));
+            }
+        }
         for (uint32_t j = 0; j < used; ++j) {
             CX_TRY(cudaEventRecord(b->joins[j], b->branches[j]));
             CX_TRY(cudaStreamWaitEvent(s, b->joins[j], 0));
         }
     }
-    if (trace && t.kernel == CAELIX_BATCH_WAVEFRONT) {
+    if (trace && run_kernel(b, t) == CAELIX_BATCH_WAVEFRONT) {
         CX_TRY(cudaMemsetAsync(b->d_counts, 0, 24ull * b->views.size(), s));
         const cx::WaveBuffers wb = cx::wave_carve(b->wave_memory.ptr, wave_slots(b, t));
         return cx::wave_trace(b->wave_views.data(), b->d_wave_views, (uint32_t)b->views.size(), b->plan,
@@ -261,7 +280,9 @@ cudaError_t capture_graph(CaelixBatch* b, const CaelixBatchTuning& t, bool build
 bool scenes_moved(const CaelixBatch* b)
 {
     for (size_t i = 0; i < b->scenes.size(); ++i)
-        if (b->scenes[i]->generation != b->generations[i]) return true;
+        if (b->scenes[i]->generation != b->generations[i] ||
+            b->scenes[i]->entity_generation != b->entity_generations[i])
+            return true;
     return false;
 }
 
@@ -281,9 +302,12 @@ cudaError_t ensure_graph(CaelixBatch* b)
     CX_TRY(capture_graph(b, b->tuning, true, true, &b->exec, &kernels));
     b->exec_tuning = b->tuning;
     b->kernel_nodes = kernels;
-    b->wavefront = b->tuning.kernel == CAELIX_BATCH_WAVEFRONT ? wave_slots(b, b->tuning)
+    b->wavefront = run_kernel(b, b->tuning) == CAELIX_BATCH_WAVEFRONT ? wave_slots(b, b->tuning)
                                                                : trace_grid(b, b->tuning) * cx::kBatchThreads;
-    for (size_t i = 0; i < b->scenes.size(); ++i) b->generations[i] = b->scenes[i]->generation;
+    for (size_t i = 0; i < b->scenes.size(); ++i) {
+        b->generations[i] = b->scenes[i]->generation;
+        b->entity_generations[i] = b->scenes[i]->entity_generation;
+    }
     b->captures += 1;
     return cudaSuccess;
 }
@@ -462,12 +486,6 @@ CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBa
         CaelixResult r = v.renderer ? CAELIX_OK : CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK && v.renderer->device != device) r = CAELIX_ERROR_INVALID_ARGUMENT;
         if (r == CAELIX_OK) r = render_params(v.renderer, &v.target, &v.camera, &v.options, "caelix_batch_create", &p);
-        // An entity the trace sees (in the scene's device views) is not batched; the slots of
-        // removed entities, and entities whose bricks were never flushed, are not traced.
-        if (r == CAELIX_OK && v.renderer->scene->entity_view_count) {
-            log(CAELIX_LOG_ERROR, "caelix_batch_create: view %u: scenes with entities are not batched", i);
-            r = CAELIX_ERROR_UNSUPPORTED;
-        }
         if (r == CAELIX_OK) {
             cudaPointerAttributes attr;
             if (cudaPointerGetAttributes(&attr, reinterpret_cast<const void*>(v.target.radiance)) != cudaSuccess ||
@@ -487,6 +505,7 @@ CAELIX_API CaelixResult caelix_batch_create(CaelixDevice* device, const CaelixBa
         if (std::find(b->scenes.begin(), b->scenes.end(), s) == b->scenes.end()) b->scenes.push_back(s);
     }
     b->generations.assign(b->scenes.size(), ~0ull);
+    b->entity_generations.assign(b->scenes.size(), ~0ull);
     const uint32_t n = desc->view_count;
     cudaError_t e = cudaMalloc(&b->d_views, sizeof(cx::BatchView) * n);
     if (e == cudaSuccess) e = cudaMalloc(&b->d_wave_views, sizeof(cx::WaveView) * n);
@@ -524,11 +543,6 @@ CAELIX_API CaelixResult caelix_batch_run(CaelixBatch* batch, const CaelixFrameDe
 {
     CAELIX_GUARD_BEGIN
     if (!batch || !frame) return CAELIX_ERROR_INVALID_ARGUMENT;
-    for (const CaelixScene* sc : batch->scenes)
-        if (sc->entity_view_count) {
-            log(CAELIX_LOG_ERROR, "caelix_batch_run: a scene of the batch has entities (not batched)");
-            return CAELIX_ERROR_UNSUPPORTED;
-        }
     cudaSetDevice(batch->device->ordinal);
     cudaError_t e = ensure_graph(batch);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_batch_run");
@@ -615,6 +629,7 @@ CAELIX_API CaelixResult caelix_batch_autotune(CaelixBatch* batch, const CaelixFr
     float best = INFINITY;
     CaelixBatchTuning best_t = t;
     for (uint32_t kernel : {CAELIX_BATCH_PERSISTENT, CAELIX_BATCH_WAVEFRONT}) {
+        if (run_kernel(batch, CaelixBatchTuning{0, 0, 0, 0, 0, 0, kernel, 0}) != kernel) continue;
         CaelixBatchTuning k = t;
         k.kernel = kernel;
         k.wavefront = 0;

@@ -170,6 +170,7 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     in.group_frames = frames;
     in.group_count = (uint32_t)groups;
     in.sort_keys_per_thread = cx::kSortKeysPerThread;
+    scene->dyn_input = in;
     if (e == cudaSuccess) e = cx::lt_build(tree, in, stream, nullptr);
     cx::SceneView v;
     std::memset(&v, 0, sizeof(v));
@@ -252,6 +253,7 @@ CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
     }
     scene->entity_view_count = (uint32_t)views.size();
     scene->entity_views_dirty = false;
+    scene->entity_generation += 1;
     return CAELIX_OK;
 }
 
@@ -1120,10 +1122,6 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     const CaelixResult r = render_params(renderer, &t, camera, options, "caelix_renderer_backward", &p);
     if (r != CAELIX_OK) return r;
     CaelixScene* scene = renderer->scene;
-    if (scene->entity_view_count) {
-        log(CAELIX_LOG_ERROR, "caelix_renderer_backward: scenes with entities are not differentiated");
-        return CAELIX_ERROR_UNSUPPORTED;
-    }
     cudaSetDevice(renderer->device->ordinal);
     cudaStream_t stream = reinterpret_cast<cudaStream_t>(frame->command_buffer);
     cudaError_t e = cudaMemsetAsync(d_albedo, 0, sizeof(float) * cx::kMaterialCodes * 3, stream);
@@ -1135,7 +1133,7 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
     if (r2 != CAELIX_OK) return r2;
     renderer->launches = 0;
     cudaEventRecord(renderer->start, stream);
-    e = cx::adjoint_launch(cx::scene_view(scene->dev), p, d_radiance, reinterpret_cast<float*>(image), d_albedo,
+    e = cx::adjoint_launch(render_view(scene), p, d_radiance, reinterpret_cast<float*>(image), d_albedo,
                            d_power, renderer->counts, renderer->wave_memory.ptr, renderer->wave_capacity,
                            renderer->device->sm_count, stream, &renderer->launches);
     cudaEventRecord(renderer->stop, stream);

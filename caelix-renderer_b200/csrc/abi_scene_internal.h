@@ -88,6 +88,8 @@ struct CaelixScene
     cx::GrowBuffer dyn_view;
     uint32_t dyn_tree_capacity = 0;
     bool dyn_live = false;
+    cx::LightBvhInput dyn_input{};  // the build input of the entities' light tree (while dyn_live)
+    uint64_t entity_generation = 0;  // uploads of the entity views so far (the device views move)
 };
 
 struct CaelixRenderer

@@ -645,14 +645,17 @@ cudaError_t wave_adjoint(const SceneView& scene, const WaveView* d_record, const
                          const WavePlan& plan, const uint32_t* d_table, const WaveBuffers& b, uint32_t block_width,
                          uint32_t sm_count, const WaveAdjoint& adj, cudaStream_t stream, uint32_t* launches)
 {
+    const bool entities = scene.entity_count != 0;
     if (wave_resident_scene(scene)) {
         CX_TRY((wave_run<kShadeRecord, 5>(d_record, plan, d_table, b, block_width, sm_count, adj, stream,
-                                              launches)));
-        return wave_run<kShadeReplay, 5>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
+                                              launches, entities)));
+        return wave_run<kShadeReplay, 5>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches,
+                                         entities);
     }
     CX_TRY((wave_run<kShadeRecord, 8>(d_record, plan, d_table, b, block_width, sm_count, adj, stream,
-                                          launches)));
-    return wave_run<kShadeReplay, 8>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches);
+                                          launches, entities)));
+    return wave_run<kShadeReplay, 8>(d_replay, plan, d_table, b, block_width, sm_count, adj, stream, launches,
+                                     entities);
 }
 
 }  // namespace cx

@@ -629,7 +629,8 @@ CAELIX_API CaelixResult caelix_renderer_get_stats(CaelixRenderer* renderer, Cael
    respect to the albedo of every material table entry, d_albedo: device float[65536][3] (row =
    the material code), and to the emitter power of every brick, d_power: device float[brick_count] in
    the scene's brick order (the keys of caelix_scene_get_view: increasing linear brick index).
-   Sampling quantities (pdfs, MIS weights, Russian-roulette probabilities, discrete decisions) are
+   A scene's entities are traced and shaded as in the render (their voxels' albedo gradients go to
+   the shared material table); the power of their bricks is not differentiated. Sampling quantities (pdfs, MIS weights, Russian-roulette probabilities, discrete decisions) are
    held fixed. The frame is traced twice (path replay): once recording each sample's radiance (one
    image per sample index, in device memory the renderer keeps), once more gathering the
    gradients; nothing of the paths is stored. When
@@ -650,9 +651,10 @@ CAELIX_API CaelixResult caelix_renderer_backward(CaelixRenderer* renderer, const
  * rebuilt (as caelix_scene_flush does after caelix_scene_set_light_options), the builds of
  * different scenes running as parallel branches, then every view is traced, either by one
  * persistent kernel whose resident threads take pixels of all views from one work counter, or by
- * the wavefront kernels over the paths of all views at once (CaelixBatchTuning::kernel). Each
- * view's radiance is bit-identical to caelix_renderer_render of the same renderer, target, camera
- * and options.
+ * the wavefront kernels over the paths of all views at once (CaelixBatchTuning::kernel; a batch
+ * with a scene that has entities always runs the wavefront kernels, which trace them, and its runs
+ * also rebuild the entities' light tree). Each view's radiance is bit-identical to
+ * caelix_renderer_render of the same renderer, target, camera and options.
  *
  * The scenes must be flushed before the batch is created. A full re-flush of a scene (bricks,
  * powers or materials changed) moves its device tables: the next run notices it and captures

@@ -862,13 +862,17 @@ void oc_voxel_id(const oc_scene* s, const oc_hit* h, uint32_t out[2])
 }
 
 /* NextEventAtVertex without the sun: the lamp candidate and its shadow ray. */
+/* lamp_brick / lamp_code / dvalue: a drawn, unoccluded lamp of the world (its brick, its code and
+ * the factor of its power); lamp_fixed: the power of an unoccluded lamp of the entities' light set
+ * (not differentiated; -1 for none). */
 static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* light_rng, float out[3],
-                       uint32_t* lamp_brick, uint32_t* lamp_code, float* dvalue)
+                       uint32_t* lamp_brick, uint32_t* lamp_code, float* dvalue, float* lamp_fixed)
 {
     out[0] = out[1] = out[2] = 0.0f;
     *lamp_brick = OC_NONE;
     *lamp_code = 0;
     *dvalue = 0.0f;
+    *lamp_fixed = -1.0f;
     const uint32_t point_seed = random_u32(light_rng);
     float p[7];
     uint32_t words[6];
@@ -908,11 +912,10 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
         for (int q = 0; q < 3; ++q) out[q] = contribution[q] * k;
         /* For the adjoint: the contribution is the lamp brick's power times the emission of its
          * code times scale * k. */
-        if (words[5] == 0) {
-            *lamp_brick = brick;
-            *lamp_code = oc_material_code(words[0], c->s->encoding);
-            *dvalue = scale * k;
-        }
+        *lamp_code = oc_material_code(words[0], c->s->encoding);
+        *dvalue = scale * k;
+        if (words[5] == 0) *lamp_brick = brick;
+        else *lamp_fixed = c->s->dyn_power[brick];
     }
 }
 
@@ -983,14 +986,16 @@ static void shade(const ctx* c, const oc_hit* h, const float ray_o[3], const flo
  * bounce vertex multiplies the throughput by the albedo of its material, a Russian-roulette
  * survival by factor (1 / cp). The factors are the sampling quantities of the fp32 forward pass
  * (MIS weights, geometry / pdf terms, RR probabilities), held fixed by the adjoint. */
-enum { EV_EMIT = 0, EV_ALBEDO = 1, EV_NEE = 2, EV_RR = 3 };
+enum { EV_EMIT = 0, EV_ALBEDO = 1, EV_NEE = 2, EV_RR = 3, EV_FIXED = 4 };
 #define MAX_EVENTS 64
 
 typedef struct path_event {
     uint32_t kind;
     uint32_t index; /* brick (EMIT, NEE) or material code (ALBEDO) */
-    uint32_t code;  /* EMIT, NEE: the material code of the emitting voxel */
+    uint32_t code;  /* EMIT, NEE, FIXED: the material code of the emitting voxel */
     float factor;
+    float power;    /* FIXED: the power of an entity's emitting brick (held fixed: an entity's power
+                       is not differentiated) */
 } path_event;
 
 typedef struct path_rec {
@@ -999,20 +1004,34 @@ typedef struct path_rec {
     uint32_t material0; /* the primary material code */
     uint32_t record0;
     int bad;            /* the fp32 radiance was not finite (the sample's radiance part is 0) */
+    float e0_fixed[3];  /* the primary emission of an entity voxel (held fixed) */
     float radiance[3];  /* the fp32 radiance of the sample */
     uint32_t n;
     path_event ev[MAX_EVENTS];
 } path_rec;
 
-static void rec_event(path_rec* rec, uint32_t kind, uint32_t index, uint32_t code, float factor)
+static void rec_event_p(path_rec* rec, uint32_t kind, uint32_t index, uint32_t code, float factor, float power)
 {
     if (rec && rec->n < MAX_EVENTS) {
         rec->ev[rec->n].kind = kind;
         rec->ev[rec->n].index = index;
         rec->ev[rec->n].code = code;
         rec->ev[rec->n].factor = factor;
+        rec->ev[rec->n].power = power;
         rec->n++;
     }
+}
+
+static void rec_event(path_rec* rec, uint32_t kind, uint32_t index, uint32_t code, float factor)
+{
+    rec_event_p(rec, kind, index, code, factor, 0.0f);
+}
+
+/* The NEE events of a vertex: a world lamp's power is a parameter, an entity lamp's is fixed. */
+static void rec_nee(path_rec* rec, uint32_t lamp, uint32_t code, float dv, float fixed)
+{
+    if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, code, dv);
+    else if (fixed >= 0.0f) rec_event_p(rec, EV_FIXED, 0, code, dv, fixed);
 }
 
 static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float rgb[3], path_rec* rec)
@@ -1048,6 +1067,7 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
         const uint32_t block0 = (primary.attrib >> 16) & 0xFFFFu;
         rec->hit = 1;
         rec->emits0 = !(primary.attrib & OC_ENTITY_HIT);
+        if (!rec->emits0) memcpy(rec->e0_fixed, e0, sizeof(rec->e0_fixed));
         rec->material0 = oc_material_code(block0, c->s->encoding);
         rec->record0 = primary.record;
     }
@@ -1057,11 +1077,11 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
     float throughput[3] = {1.0f / hmax(0.001f, 1.0f), 1.0f / hmax(0.001f, 1.0f), 1.0f / hmax(0.001f, 1.0f)};
     uint32_t segment_light = 0;
     if (r->light_nee && r->bounce_count >= 1) {
-        float nee[3], dv;
+        float nee[3], dv, fixed;
         uint32_t lamp, lamp_code;
-        next_event(c, org, primary.normal, &light_rng, nee, &lamp, &lamp_code, &dv);
+        next_event(c, org, primary.normal, &light_rng, nee, &lamp, &lamp_code, &dv, &fixed);
         for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * throughput[k];
-        if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, lamp_code, dv);
+        rec_nee(rec, lamp, lamp_code, dv, fixed);
         segment_light = 3u; /* lamp NEE with MIS */
     }
     uint32_t bounce_index = 1;
@@ -1077,17 +1097,22 @@ static void trace_pixel(ctx* c, uint32_t px, uint32_t py, uint32_t seed, float r
             ew = lamp_hit_weight(c, segment_light, &h, org, dir, seg_n);
         for (int k = 0; k < 3; ++k) radiance[k] += em[k] * (throughput[k] * ew);
         const uint32_t code = oc_material_code((h.attrib >> 16) & 0xFFFFu, c->s->encoding);
-        if (!(h.attrib & OC_ENTITY_HIT)) rec_event(rec, EV_EMIT, h.record, code, ew);
+        if (!(h.attrib & OC_ENTITY_HIT)) {
+            rec_event(rec, EV_EMIT, h.record, code, ew);
+        } else {
+            const float* pw = c->s->entities[h.group >> 24].power;
+            rec_event_p(rec, EV_FIXED, 0, code, ew, pw ? pw[h.record] : 0.0f);
+        }
         rec_event(rec, EV_ALBEDO, code, 0, 0.0f);
         for (int k = 0; k < 3; ++k) throughput[k] *= al[k] / hmax(0.001f, 1.0f);
         segment_light = 0u;
         if (r->light_nee && bounce_index <= r->bounce_count) {
             segment_light = 3u;
-            float nee[3], dv;
+            float nee[3], dv, fixed;
             uint32_t lamp, lamp_code;
-            next_event(c, o2, h.normal, &light_rng, nee, &lamp, &lamp_code, &dv);
+            next_event(c, o2, h.normal, &light_rng, nee, &lamp, &lamp_code, &dv, &fixed);
             for (int k = 0; k < 3; ++k) radiance[k] += nee[k] * (throughput[k] * (1.0f / 1.0f));
-            if (lamp != OC_NONE) rec_event(rec, EV_NEE, lamp, lamp_code, dv);
+            rec_nee(rec, lamp, lamp_code, dv, fixed);
         }
         const float cp = hmax(throughput[0], hmax(throughput[1], throughput[2]));
         if (cp <= 0.0f || cp < random01(&rng)) break;
@@ -1192,8 +1217,9 @@ static void eval_sample(const path_rec* rec, const float* E, const double* A, co
     for (uint32_t i = 0; i < rec->n; ++i) {
         const path_event* e = &rec->ev[i];
         for (int k = 0; k < 3; ++k) T_before[i][k] = T[k];
-        if (e->kind == EV_EMIT || e->kind == EV_NEE) {
-            for (int k = 0; k < 3; ++k) R[k] += P[e->index] * (double)E[3 * e->code + k] * (double)e->factor * T[k];
+        if (e->kind == EV_EMIT || e->kind == EV_NEE || e->kind == EV_FIXED) {
+            const double p = e->kind == EV_FIXED ? (double)e->power : P[e->index];
+            for (int k = 0; k < 3; ++k) R[k] += p * (double)E[3 * e->code + k] * (double)e->factor * T[k];
         } else if (e->kind == EV_ALBEDO) {
             for (int k = 0; k < 3; ++k) T[k] *= A[3 * e->index + k];
         } else {
@@ -1203,7 +1229,7 @@ static void eval_sample(const path_rec* rec, const float* E, const double* A, co
     const double p0 = rec->emits0 ? P[rec->record0] : 0.0;
     for (int k = 0; k < 3; ++k) {
         const double sr = rec->bad ? 0.0 : (rec->radiance[k] > 65504.0f ? 65504.0 : R[k]);
-        rgb[k] = p0 * (double)E[3 * rec->material0 + k] + A[3 * rec->material0 + k] * sr;
+        rgb[k] = p0 * (double)E[3 * rec->material0 + k] + (double)rec->e0_fixed[k] + A[3 * rec->material0 + k] * sr;
     }
 }
 
@@ -1242,7 +1268,11 @@ static void* run_adjoint_rows(void* arg)
                 for (int32_t i = (int32_t)rec->n - 1; i >= 0; --i) {
                     const path_event* e = &rec->ev[i];
                     const double* T = T_before[i];
-                    if (e->kind == EV_EMIT || e->kind == EV_NEE) {
+                    if (e->kind == EV_FIXED) {
+                        const double f = (double)e->factor;
+                        const float* Ee = local.s->emission + 3 * e->code;
+                        for (int k = 0; k < 3; ++k) lambda[k] += G[k] * (double)e->power * (double)Ee[k] * f;
+                    } else if (e->kind == EV_EMIT || e->kind == EV_NEE) {
                         const double f = (double)e->factor;
                         const float* Ee = local.s->emission + 3 * e->code;
                         j->dP[e->index] += (G[0] * Ee[0] * T[0] + G[1] * Ee[1] * T[1] + G[2] * Ee[2] * T[2]) * f;

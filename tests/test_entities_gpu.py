@@ -119,14 +119,33 @@ def test_entities_parity(cuda_device, oracle):
     moved = render_pair(cuda_device, scene, osc, vs)
     assert not np.array_equal(lit, moved)
 
-    # A batch takes no scene with entities.
+    # A batch takes the scene with its entities (the wavefront kernels, both light trees rebuilt):
+    # each view equals the plain render, whatever kernel the tuning names.
     import torch
 
     r = caelix_b200.Renderer(cuda_device, scene)
-    out = torch.zeros(32 * 32 * 3, dtype=torch.float32, device="cuda")
-    with pytest.raises(caelix_b200.CaelixError) as err:
-        caelix_b200.Batch(cuda_device, [(r, out, 32, 32, vs.camera, 2, 1, 1)], rebuild_light_trees=True)
-    assert err.value.code == caelix_b200.CAELIX_ERROR_UNSUPPORTED
+    out = torch.zeros(40 * 32 * 3, dtype=torch.float32, device="cuda")
+    ref = torch.zeros_like(out)
+    r.render(ref, 40, 32, vs.camera, bounces=3, seed=2, spp=2)
+    for kernel in (0, 1):
+        batch = caelix_b200.Batch(cuda_device, [(r, out, 40, 32, vs.camera, 3, 2, 2)], rebuild_light_trees=True)
+        batch.set_tuning(min_blocks=6, block_width=8, refill_min=4, order=1, sort_keys_per_thread=16, kernel=kernel,
+                         wavefront=0)
+        out.fill_(-1.0)
+        batch.run()
+        st = batch.stats()
+        assert st.light_tree_builds >= 1
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+        # An entity moved: the next run captures again and follows it.
+        scene.set_entity_transform(e3, p1, Q1_MOVED if kernel == 0 else Q1)
+        scene.flush()
+        r.render(ref, 40, 32, vs.camera, bounces=3, seed=2, spp=2)
+        batch.run()
+        batch.stats()
+        torch.cuda.synchronize()
+        assert torch.equal(out, ref)
+        batch.close()
     r.close()
 
     # Entity 0 cannot be moved or removed; motion takes two values.
@@ -136,4 +155,54 @@ def test_entities_parity(cuda_device, oracle):
         scene.set_entity_motion(e3, 2)
     with pytest.raises(caelix_b200.CaelixError):
         scene.upload_bricks(b1.keys, b1.voxels, entity=7)
+    scene.close()
+
+
+def test_backward_with_entities(cuda_device, oracle):
+    """caelix_renderer_backward of a scene with a lit, rotated entity: the forward image is the
+    render, and the gradients of the world's bricks' power and of the material table's albedo
+    (entity voxels included) match the double-precision oracle adjoint within 1e-3 relative; the
+    entity's emission and its lamps enter the radiance as fixed terms."""
+    import torch
+
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(8, 6, 10), brick_occupancy=0.45, emissive_fraction=0.1, seed=13)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    cam = vs.camera
+    ahead = np.asarray(cam["position"], np.float64) + 14.0 * np.asarray(cam["forward"], np.float64)
+    p1 = tuple((ahead - 8.0).astype(np.float32))
+    b1 = entity_bricks(grid=(2, 2, 2), seed=7)
+    rng = np.random.default_rng(9)
+    p_1 = np.where(rng.random(b1.brick_count) < 0.5, rng.lognormal(0.0, 1.0, b1.brick_count), 0.0).astype(np.float32)
+    e1 = scene.add_entity(p1, Q1)
+    scene.upload_bricks(b1.keys, b1.voxels, entity=e1)
+    scene.set_brick_power(b1.keys, p_1, entity=e1)
+    scene.flush()
+    osc = oracle_lib.OracleScene(oracle, vs)
+    o1 = oracle_lib.OracleScene(oracle, b1.like(power=p_1))
+    osc.set_entities([(o1, Q1, p1)])
+    w, h, spp, bounces = 64, 48, 2, 3
+    r = caelix_b200.Renderer(cuda_device, scene)
+    img = torch.zeros(h * w * 3, device="cuda")
+    r.render(img, w, h, cam, bounces=bounces, seed=3, spp=spp)
+    target = torch.from_numpy(0.9 * img.cpu().numpy()).cuda()
+    d_rad = 2.0 * (img - target)
+    d_alb = torch.zeros(65536 * 3, device="cuda")
+    d_pow = torch.zeros(vs.brick_count, device="cuda")
+    fwd = torch.zeros_like(img)
+    r.backward(d_rad, w, h, cam, d_alb, d_pow, bounces=bounces, seed=3, spp=spp, image=fwd)
+    torch.cuda.synchronize()
+    assert torch.equal(fwd, img)
+    _, rA, rP = osc.adjoint(w, h, spp=spp, bounces=bounces, seed=3, d_radiance=d_rad.cpu().numpy(), threads=8)
+    gA = d_alb.cpu().numpy().reshape(65536, 3).astype(np.float64)
+    gP = d_pow.cpu().numpy().astype(np.float64)
+    for gpu, ref in ((gA, rA), (gP, rP)):
+        scale = np.abs(ref).max()
+        assert scale > 0
+        big = np.abs(ref) >= 1e-3 * scale
+        assert np.max(np.abs(gpu[big] - ref[big]) / np.abs(ref[big])) <= 1e-3
+        assert np.abs(gpu - ref).max() <= 1e-3 * scale
+    r.close()
+    osc.set_entities([])
     scene.close()
