@@ -109,6 +109,9 @@ CaelixScene* entity_bricks(CaelixScene* scene, uint32_t entity)
 
 uint64_t align256(uint64_t v) { return (v + 255) & ~255ull; }
 
+// Scenes with at least this many entities trace them through the entity BVH.
+constexpr size_t kEntityBvhMin = 4;
+
 // The entities' light set: every live entity's light blocks, group rows, frames, power and light
 // records appended in view order (cx::dyn_append moves their indices), then the dynamic light
 // tree built over them, and the device copy of its SceneView. No entity light: none.
@@ -201,6 +204,48 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     return CAELIX_OK;
 }
 
+// The BVH over the entities' bounding spheres (world space, boxes rounded outwards): binary, one
+// entity per leaf, split at the median of the longest axis of the centres. Node 0 is the root.
+uint32_t entity_bvh_build(std::vector<cx::EntityNode>& nodes, std::vector<uint32_t>& order, size_t first, size_t last,
+                          const std::vector<cx::EntityView>& views)
+{
+    const uint32_t index = (uint32_t)nodes.size();
+    nodes.emplace_back();
+    float lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    double clo[3] = {INFINITY, INFINITY, INFINITY}, chi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (size_t i = first; i < last; ++i) {
+        const float* sp = views[order[i]].sphere;
+        for (int k = 0; k < 3; ++k) {
+            lo[k] = std::min(lo[k], std::nextafter(sp[k] - sp[3], -INFINITY));
+            hi[k] = std::max(hi[k], std::nextafter(sp[k] + sp[3], INFINITY));
+            clo[k] = std::min(clo[k], (double)sp[k]);
+            chi[k] = std::max(chi[k], (double)sp[k]);
+        }
+    }
+    cx::EntityNode n;
+    for (int k = 0; k < 3; ++k) {
+        n.lo[k] = lo[k];
+        n.hi[k] = hi[k];
+    }
+    if (last - first == 1) {
+        n.first = cx::kEntityLeaf | order[first];
+        n.second = 0;
+    } else {
+        int axis = 0;
+        for (int k = 1; k < 3; ++k)
+            if (chi[k] - clo[k] > chi[axis] - clo[axis]) axis = k;
+        const size_t mid = first + (last - first) / 2;
+        std::nth_element(order.begin() + first, order.begin() + mid, order.begin() + last, [&](uint32_t a, uint32_t b) {
+            return views[a].sphere[axis] < views[b].sphere[axis] ||
+                   (views[a].sphere[axis] == views[b].sphere[axis] && a < b);
+        });
+        n.first = entity_bvh_build(nodes, order, first, mid, views);
+        n.second = entity_bvh_build(nodes, order, mid, last, views);
+    }
+    nodes[index] = n;
+    return index;
+}
+
 // Rewrites the device views of the live entities and their light set (after waiting for the
 // device: renders may read the old ones) and returns when they are in place. An entity whose
 // bricks were never flushed has no tables yet and joins at the flush that builds them.
@@ -243,11 +288,25 @@ CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
     scene->entity_view_count = 0;
     CaelixResult r = build_entity_lights(scene, live, views, stream);
     if (r != CAELIX_OK) return r;
+    scene->entity_nodes_used = false;
     if (!views.empty()) {
         r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
         if (r != CAELIX_OK) return r;
         e = cudaMemcpyAsync(scene->entity_views.ptr, views.data(), sizeof(cx::EntityView) * views.size(),
                             cudaMemcpyHostToDevice, stream);
+        // With several entities a ray tests only those whose box it meets (trace_entities).
+        std::vector<cx::EntityNode> nodes;
+        if (e == cudaSuccess && views.size() >= kEntityBvhMin) {
+            std::vector<uint32_t> order(views.size());
+            for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+            nodes.reserve(2 * views.size());
+            entity_bvh_build(nodes, order, 0, order.size(), views);
+            r = scene->entity_nodes.reserve(sizeof(cx::EntityNode) * nodes.size(), "caelix_scene_flush");
+            if (r != CAELIX_OK) return r;
+            e = cudaMemcpyAsync(scene->entity_nodes.ptr, nodes.data(), sizeof(cx::EntityNode) * nodes.size(),
+                                cudaMemcpyHostToDevice, stream);
+            scene->entity_nodes_used = true;
+        }
         if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
         if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     }
@@ -265,6 +324,7 @@ cx::SceneView render_view(const CaelixScene* scene)
     if (scene->entity_view_count) {
         v.entities = static_cast<const cx::EntityView*>(scene->entity_views.ptr);
         v.entity_count = scene->entity_view_count;
+        if (scene->entity_nodes_used) v.entity_nodes = static_cast<const cx::EntityNode*>(scene->entity_nodes.ptr);
         if (scene->dyn_live) v.dyn = static_cast<const cx::SceneView*>(scene->dyn_view.ptr);
     }
     return v;
@@ -356,6 +416,7 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     for (auto& e : scene->entities) caelix_scene_destroy(e.bricks);
     scene->entities.clear();
     scene->entity_views.release();
+    scene->entity_nodes.release();
     scene->dyn_arrays.release();
     scene->dyn_tree.release();
     scene->dyn_view.release();

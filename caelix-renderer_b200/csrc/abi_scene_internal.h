@@ -79,6 +79,8 @@ struct CaelixScene
     };
     std::vector<Entity> entities;
     cx::GrowBuffer entity_views;  // device EntityView per live entity
+    cx::GrowBuffer entity_nodes;  // device EntityNode: the BVH over the live entities
+    bool entity_nodes_used = false;
     uint32_t entity_view_count = 0;
     bool entity_views_dirty = false;
     // The entities' light set (SceneView::dyn), rebuilt with the views: its arrays, the dynamic

@@ -892,6 +892,7 @@ SceneView scene_view(const DeviceScene& s)
     v.group_count = s.group_count;
     v.entities = nullptr;
     v.entity_count = 0;
+    v.entity_nodes = nullptr;
     v.dyn = nullptr;
     return v;
 }

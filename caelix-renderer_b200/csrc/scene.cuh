@@ -44,6 +44,17 @@ constexpr uint32_t kLightCodeWords = kMaterialCodes / 32;
 
 struct EntityView;
 
+// A node of the BVH over a scene's entities (their bounding-sphere boxes, world space): lo, then
+// the left child (or kEntityLeaf | entity index) as a float's bits; hi, then the right child.
+struct EntityNode
+{
+    float lo[3];
+    uint32_t first;
+    float hi[3];
+    uint32_t second;
+};
+constexpr uint32_t kEntityLeaf = 0x80000000u;
+
 // Everything the trace kernels read, passed by value.
 struct SceneView
 {
@@ -74,6 +85,7 @@ struct SceneView
     // after the world; their lights are the light set `dyn`.
     const EntityView* entities;  // device, entity_count of them
     uint32_t entity_count;
+    const EntityNode* entity_nodes;  // the BVH over the entities (root 0), or null: test every entity
     // The entities' lights (null: none), a light set of its own in device memory (its heap,
     // group rows, frames, power and the dynamic light tree; the tree of the reference's dynamic
     // entities): entity e's groups from its group_base, its light blocks' brick words after the

@@ -319,52 +319,112 @@ __device__ __noinline__ Hit trace_ray(const SceneView& s, const float o[3], cons
     return trace_ray_body(s, o, d, tmin_ray, tmax_ray);
 }
 
-// The entities after the world's bricks, in order: the ray in each entity's frame
-// (local = rot^T (x - pos)), its bricks' DDA up to the current hit, a strictly nearer hit taken with
-// the entity bit, the entity's index as its group and the rotated face normal (normalised as
-// v * (1 / sqrt(dot(v, v)))).
+// One entity after the world's bricks: the ray in the entity's frame (local = rot^T (x - pos)),
+// its bricks' DDA up to the current hit, a strictly nearer hit taken with the entity bit, the
+// entity's index as its group and the rotated face normal (normalised as v * (1 / sqrt(dot(v, v)))).
+__device__ __forceinline__ void entity_candidate(const SceneView& s, uint32_t e, const float o[3], const float d[3],
+                                                 float tmin_ray, float tmax_ray, Hit& h)
+{
+    const EntityView& E = s.entities[e];
+    // A ray that misses the entity's bounding sphere, or meets it only behind its origin or beyond
+    // the current hit, cannot hit it (the margins cover the rounding: the test only skips work, it
+    // never changes a hit).
+    {
+        const float4 sp = make_float4(__ldg(&E.sphere[0]), __ldg(&E.sphere[1]), __ldg(&E.sphere[2]),
+                                      __ldg(&E.sphere[3]));
+        const float oc[3] = {sp.x - o[0], sp.y - o[1], sp.z - o[2]};
+        const float oc2 = dot3(oc, oc);
+        const float tc = dot3(oc, d);
+        const float t_far = h.hit ? h.t : tmax_ray;
+        if (oc2 - tc * tc > sp.w * sp.w + 1e-5f * (oc2 + 1.0f)) return;
+        if (tc + sp.w < tmin_ray - 1e-3f * (1.0f + fabsf(tc))) return;
+        if (tc - sp.w > t_far + 1e-3f * (1.0f + fabsf(tc))) return;
+    }
+    float R[9], ol[3], dl[3];
+#pragma unroll
+    for (int i = 0; i < 9; ++i) R[i] = __ldg(&E.rot[i]);
+    const float q[3] = {o[0] - __ldg(&E.pos[0]), o[1] - __ldg(&E.pos[1]), o[2] - __ldg(&E.pos[2])};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ol[k] = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
+        dl[k] = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
+    }
+    const Hit he = trace_ray_body(E.scene, ol, dl, tmin_ray, h.hit ? h.t : tmax_ray);
+    if (!he.hit) return;
+    h = he;
+    h.attrib |= kEntityHit;
+    h.group = (e << kEntityShift) | he.group;
+    const uint32_t f = (uint32_t)(__ffs(he.attrib & 0x3Fu) - 1);
+    const float sign = (f & 1u) ? -1.0f : 1.0f;
+    float v[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) v[i] = R[3 * i + (f >> 1)] * sign;
+    const float inv = 1.0f / sqrtf(dot3(v, v));
+#pragma unroll
+    for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
+}
+
+// The entities after the world's bricks, in index order (entity_candidate): every entity, or with
+// the scene's entity BVH only those whose box the ray meets before the current hit (collected by a
+// traversal of the BVH over the entities' bounding-sphere boxes, then taken in index order, so the
+// hit is the one the loop over every entity finds: the nearest, ties to the world and then to the
+// lower index). More candidates than the list holds: every entity.
+constexpr uint32_t kEntityCandidates = 16;
+constexpr uint32_t kEntityStack = 32;
+
 __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
                                             float tmax_ray, Hit& h)
 {
-    for (uint32_t e = 0; e < s.entity_count; ++e) {
-        const EntityView& E = s.entities[e];
-        // A ray that misses the entity's bounding sphere, or meets it only behind its origin or
-        // beyond the current hit, cannot hit it (the margins cover the rounding: the test only
-        // skips work, it never changes a hit).
-        {
-            const float4 sp = make_float4(__ldg(&E.sphere[0]), __ldg(&E.sphere[1]), __ldg(&E.sphere[2]),
-                                          __ldg(&E.sphere[3]));
-            const float oc[3] = {sp.x - o[0], sp.y - o[1], sp.z - o[2]};
-            const float oc2 = dot3(oc, oc);
-            const float tc = dot3(oc, d);
-            const float t_far = h.hit ? h.t : tmax_ray;
-            if (oc2 - tc * tc > sp.w * sp.w + 1e-5f * (oc2 + 1.0f)) continue;
-            if (tc + sp.w < tmin_ray - 1e-3f * (1.0f + fabsf(tc))) continue;
-            if (tc - sp.w > t_far + 1e-3f * (1.0f + fabsf(tc))) continue;
+    if (s.entity_nodes) {
+        float inv[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) inv[k] = safe_inv_axis(d[k]);
+        const float t_far = h.hit ? h.t : tmax_ray;
+        const float t_lo = tmin_ray - 1e-3f * (1.0f + fabsf(tmin_ray));
+        const float t_hi = t_far + 1e-3f * (1.0f + fabsf(t_far));
+        uint32_t cand[kEntityCandidates];
+        uint32_t stack[kEntityStack];
+        uint32_t n = 0, sp = 0;
+        bool overflow = false;
+        stack[sp++] = 0;
+        while (sp && !overflow) {
+            const EntityNode& N = s.entity_nodes[stack[--sp]];
+            const float4 a = __ldg(reinterpret_cast<const float4*>(&N));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(&N) + 1);
+            const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+            float t0 = t_lo, t1 = t_hi;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float ta = (lo[k] - o[k]) * inv[k];
+                const float tb = (hi[k] - o[k]) * inv[k];
+                t0 = hmax(t0, hmin(ta, tb));
+                t1 = hmin(t1, hmax(ta, tb));
+            }
+            if (!(t0 <= t1)) continue;
+            const uint32_t first = __float_as_uint(a.w), second = __float_as_uint(b.w);
+            if (first & kEntityLeaf) {
+                if (n < kEntityCandidates) cand[n++] = first & ~kEntityLeaf;
+                else overflow = true;
+            } else if (sp + 2 <= kEntityStack) {
+                stack[sp++] = second;
+                stack[sp++] = first;
+            } else {
+                overflow = true;
+            }
         }
-        float R[9], ol[3], dl[3];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) R[i] = __ldg(&E.rot[i]);
-        const float q[3] = {o[0] - __ldg(&E.pos[0]), o[1] - __ldg(&E.pos[1]), o[2] - __ldg(&E.pos[2])};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            ol[k] = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
-            dl[k] = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
+        if (!overflow) {
+            // Index order (an insertion sort of at most kEntityCandidates).
+            for (uint32_t x = 1; x < n; ++x) {
+                const uint32_t v = cand[x];
+                uint32_t y = x;
+                for (; y > 0 && cand[y - 1] > v; --y) cand[y] = cand[y - 1];
+                cand[y] = v;
+            }
+            for (uint32_t x = 0; x < n; ++x) entity_candidate(s, cand[x], o, d, tmin_ray, tmax_ray, h);
+            return;
         }
-        const Hit he = trace_ray_body(E.scene, ol, dl, tmin_ray, h.hit ? h.t : tmax_ray);
-        if (!he.hit) continue;
-        h = he;
-        h.attrib |= kEntityHit;
-        h.group = (e << kEntityShift) | he.group;
-        const uint32_t f = (uint32_t)(__ffs(he.attrib & 0x3Fu) - 1);
-        const float sign = (f & 1u) ? -1.0f : 1.0f;
-        float v[3];
-#pragma unroll
-        for (int i = 0; i < 3; ++i) v[i] = R[3 * i + (f >> 1)] * sign;
-        const float inv = 1.0f / sqrtf(dot3(v, v));
-#pragma unroll
-        for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
     }
+    for (uint32_t e = 0; e < s.entity_count; ++e) entity_candidate(s, e, o, d, tmin_ray, tmax_ray, h);
 }
 
 // The entity-local hit point of an entity hit (the wavefront keeps a hit as four words): the ray

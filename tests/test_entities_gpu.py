@@ -206,3 +206,62 @@ def test_backward_with_entities(cuda_device, oracle):
     r.close()
     osc.set_entities([])
     scene.close()
+
+
+def test_many_entities_parity(cuda_device, oracle):
+    """64 entities (the scene's entity BVH): 40 scattered round the view with random rotations, some
+    lit, and 24 in a row along the camera's axis (more boxes on one ray than the candidate list
+    holds: those rays take every entity in order). The radiance and ray counts equal the oracle's,
+    which loops over every entity, for both kernels; then 40 removed (the BVH rebuilt)."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(8, 6, 10), brick_occupancy=0.3, emissive_fraction=0.08, seed=21)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    cam = vs.camera
+    pos = np.asarray(cam["position"], np.float64)
+    fwd = np.asarray(cam["forward"], np.float64)
+    rng = np.random.default_rng(17)
+    shapes = [entity_bricks(grid=(1, 1, 1), seed=30 + i, fill=0.7) for i in range(4)]
+    placed = []
+    for i in range(64):
+        if i < 40:
+            p = pos + rng.uniform(6.0, 40.0) * fwd + rng.uniform(-14.0, 14.0, 3)
+            q = rng.normal(size=4)
+            q = tuple(float(x) for x in q / np.linalg.norm(q))
+        else:
+            p = pos + (6.0 + 3.0 * (i - 40)) * fwd - 4.0
+            q = IDENTITY
+        shape = shapes[i % 4]
+        power = np.where(rng.random(shape.brick_count) < 0.3, 2.0, 0.0).astype(np.float32)
+        e = scene.add_entity(tuple(p.astype(np.float32)), q)
+        assert e == i + 1
+        scene.upload_bricks(shape.keys, shape.voxels, entity=e)
+        scene.set_brick_power(shape.keys, power, entity=e)
+        placed.append((shape.like(power=power), q, tuple(p.astype(np.float32))))
+    scene.flush()
+    oscs = {}
+
+    def oracle_entities(items):
+        out = []
+        for vsub, q, p in items:
+            key = (id(vsub.voxels), float(vsub.power.sum()), tuple(vsub.power))
+            if key not in oscs:
+                oscs[key] = oracle_lib.OracleScene(oracle, vsub)
+            out.append((oscs[key], q, p))
+        return out
+
+    osc = oracle_lib.OracleScene(oracle, vs)
+    osc.set_entities(oracle_entities(placed))
+    img = render_pair(cuda_device, scene, osc, vs)
+    render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
+    plain = oracle_lib.OracleScene(oracle, vs).render(72, 56, spp=2, bounces=4, seed=5, threads=8)[0]
+    assert not np.array_equal(img, plain)
+
+    for e in range(1, 41):
+        scene.remove_entity(e)
+    osc.set_entities(oracle_entities(placed[40:]))
+    render_pair(cuda_device, scene, osc, vs)
+    scene.flush()
+    render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
+    osc.set_entities([])
+    scene.close()
