@@ -623,7 +623,7 @@ def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64))
     return result
 
 
-def measure_large(args, world, local, dev, stream, flush):
+def measure_large(args, world, local, dev, stream, flush, rank):
     """The large scene: 2048 x 2048 x 512 voxels (256 x 256 x 64 bricks), ~2M occupied bricks (12 %
     voxel occupancy overall), ~100k emissive bricks; the flush (records, hash table, light records,
     a full light-tree rebuild) and 1920 x 1080 frames at 4 spp, 6 bounces, light-tree NEE; then a
@@ -712,6 +712,22 @@ def measure_large(args, world, local, dev, stream, flush):
         "rays_per_frame": rays / steps,
         "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6,
     }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # The oracle's trace over the flushed tables (the light tree its own build), on every host
+        # core, over a centred pixel window of the same frame; rays counted by the oracle.
+        sys.path.insert(0, os.path.join(REPO, "tests"))
+        import oracle_lib
+
+        tab = oracle_lib.TablesScene(oracle_lib.load(), vs, scene.view())
+        threads = os.cpu_count() or 1
+        ww, wh = 96, 64
+        window = ((w - ww) // 2, (h - wh) // 2, (w + ww) // 2, (h + wh) // 2)
+        t0 = time.perf_counter()
+        _, orays = tab.render(w, h, spp=spp, bounces=bounces, seed=1, window=window, threads=threads)
+        cpu_s = time.perf_counter() - t0
+        tab.close()
+        result["cpu_baseline"] = {"value": float(orays.sum()) / cpu_s / 1e6, "unit": "Mrays/s", "cores": threads,
+                                  "kind": "port", "sample": f"oracle trace of a centred {ww}x{wh} window, same frame"}
     renderer.close()
     scene.close()
     return result
@@ -886,7 +902,7 @@ def measure_adjoint(args, world, local, dev, stream, flush, rank):
     result = {
         "workload": f"solid-brick world of the 4096-record build (32^3 bricks), {ADJ_W}x{ADJ_H}, {ADJ_SPP} spp, "
                     f"{ADJ_BOUNCES} bounces, L2 loss vs a target with albedo/power perturbed by up to 10%; "
-                    "gradients w.r.t. 64x3 material albedo and per-brick power (path replay, sampling held fixed)",
+                    "gradients w.r.t. the albedo table (65536 codes x 3) and per-brick power (path replay, sampling held fixed)",
         "bricks": int(vs.brick_count),
         "forward_ms": fwd_ms,
         "backward_ms": bwd_ms,
@@ -1104,7 +1120,7 @@ def run_ours(args, world, rank, local):
                                               f"{secs:.1f} s"}
         # The detail sections, rounded; the build goes last, so that the end of the line holds it.
         if args.large:
-            line["large"] = compact(measure_large(args, world, local, dev, stream, flush))
+            line["large"] = compact(measure_large(args, world, local, dev, stream, flush, rank))
         if args.adjoint:
             line["adjoint"] = compact(measure_adjoint(args, world, local, dev, stream, flush, rank))
         if args.entities:

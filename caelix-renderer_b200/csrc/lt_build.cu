@@ -357,9 +357,17 @@ __global__ void __launch_bounds__(kAggTile)
 {
     __shared__ uint32_t s_count[kAggTile];
     __shared__ LightSummary s_sum[kAggTile];
+    __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
     s_count[threadIdx.x] = 0;
+    {
+        // The tile's own node indices (a node is an end of its leaf range, so every node inside the
+        // tile has its index there), loaded coalesced once; the walks then read them from here.
+        const uint32_t k = lo + threadIdx.x;
+        if (k + 1 < n)
+            s_link[threadIdx.x] = make_uint4(__ldg(left + k), __ldg(right + k), __ldg(parent + k), __ldg(range_end + k));
+    }
     __syncthreads();
     const uint32_t j = lo + threadIdx.x;
     if (j >= n) return;
@@ -368,10 +376,15 @@ __global__ void __launch_bounds__(kAggTile)
     uint32_t node = __ldg(leaf_parent + j);
     uint32_t depth = 0;
     for (; depth < 128 && node != kNone; ++depth) {
-        const uint32_t l = __ldg(left + node);
-        const uint32_t r = __ldg(right + node);
-        const uint32_t up = __ldg(parent + node);
-        const uint32_t end = __ldg(range_end + node);
+        uint4 link;
+        if (node - lo < kAggTile && node + 1 < n)
+            link = s_link[node - lo];
+        else
+            link = make_uint4(__ldg(left + node), __ldg(right + node), __ldg(parent + node), __ldg(range_end + node));
+        const uint32_t l = link.x;
+        const uint32_t r = link.y;
+        const uint32_t up = link.z;
+        const uint32_t end = link.w;
         const uint32_t a = min(node, end);
         const uint32_t b = max(node, end);
         const bool inside = a >= lo && b <= hi;
@@ -511,10 +524,15 @@ __global__ void __launch_bounds__(kScanThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// 4-wide collapse: one thread per binary node at even depth writes its whole node (224 bytes,
-// its own parent link included: the 4-wide parent is the binary grandparent) and the parent words
-// of its leaf slots by sorted position.
-__global__ void __launch_bounds__(kThreads, 4)
+// 4-wide collapse: one thread per binary node at even depth builds its whole node (224 bytes,
+// its own parent link included: the 4-wide parent is the binary grandparent) in shared memory and
+// writes the parent words of its leaf slots by sorted position. The even-depth nodes of a CTA's
+// binary nodes have consecutive 4-wide indices (an exclusive scan of the flags), so the CTA then
+// stores its run of nodes with coalesced 16-byte writes.
+constexpr uint32_t kWideThreads = 128;
+constexpr uint32_t kNodeWords = sizeof(LightBvhNode) / 4;  // 56
+
+__global__ void __launch_bounds__(kWideThreads)
     lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                    const uint32_t* __restrict__ parent, const uint32_t* __restrict__ depth,
@@ -522,82 +540,92 @@ __global__ void __launch_bounds__(kThreads, 4)
                    const AggregateSlot* __restrict__ aggregates, uint32_t* __restrict__ leaf_word,
                    LightBvhNode* __restrict__ nodes)
 {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i + 1 >= n || (__ldg(depth + i) & 1u) != 0) return;
-    const uint32_t w = __ldg(wide + i);
-    if (w >= node_capacity) return;
-    const uint32_t l = __ldg(left + i);
-    const uint32_t r = __ldg(right + i);
-    uint32_t slots[4];
-    uint32_t count;
-    {
-        const bool l_leaf = (l & kChildLeafBit) != 0;
-        const bool r_leaf = (r & kChildLeafBit) != 0;
-        const uint32_t ll = l_leaf ? l : __ldg(left + l);
-        const uint32_t lr = l_leaf ? kNone : __ldg(right + l);
-        const uint32_t rl = r_leaf ? r : __ldg(left + r);
-        const uint32_t rr = r_leaf ? kNone : __ldg(right + r);
-        slots[0] = ll;
-        slots[1] = l_leaf ? rl : lr;
-        slots[2] = l_leaf ? rr : rl;
-        slots[3] = l_leaf ? kNone : rr;
-        count = (l_leaf ? 1u : 2u) + (r_leaf ? 1u : 2u);
-        if (l_leaf && r_leaf) slots[2] = kNone;
-    }
-    // The node's own parent link.
-    uint32_t up_node = kNone, up_slot = 0;
-    if (i != 0) {
-        // An even-depth node below the root has a binary grandparent; the guard keeps a broken
-        // tree (a failed earlier stage) from reading outside the arrays.
-        const uint32_t p = __ldg(parent + i);
-        const uint32_t g = p + 1 < n ? __ldg(parent + p) : kNone;
-        if (g + 1 < n) {
-            const uint32_t gl = __ldg(left + g);
-            const uint32_t base = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
-            up_slot = base + (__ldg(right + p) == i ? 1u : 0u);
-            up_node = __ldg(wide + g);
+    __shared__ __align__(16) float s_node[kWideThreads * kNodeWords];
+    const uint32_t base = blockIdx.x * kWideThreads;
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t binary = n - 1;
+    const bool active = i < binary && (__ldg(depth + i) & 1u) == 0;
+    // The CTA's first 4-wide index: the count of even-depth nodes before `base`.
+    const uint32_t w_base = __ldg(wide + base);
+    const uint32_t count = __syncthreads_count(active);
+    if (active) {
+        const uint32_t w = __ldg(wide + i);
+        float* node = s_node + (w - w_base) * kNodeWords;
+        uint32_t* words = reinterpret_cast<uint32_t*>(node);
+        const uint32_t l = __ldg(left + i);
+        const uint32_t r = __ldg(right + i);
+        uint32_t slots[4];
+        uint32_t used;
+        {
+            const bool l_leaf = (l & kChildLeafBit) != 0;
+            const bool r_leaf = (r & kChildLeafBit) != 0;
+            const uint32_t ll = l_leaf ? l : __ldg(left + l);
+            const uint32_t lr = l_leaf ? kNone : __ldg(right + l);
+            const uint32_t rl = r_leaf ? r : __ldg(left + r);
+            const uint32_t rr = r_leaf ? kNone : __ldg(right + r);
+            slots[0] = ll;
+            slots[1] = l_leaf ? rl : lr;
+            slots[2] = l_leaf ? rr : rl;
+            slots[3] = l_leaf ? kNone : rr;
+            used = (l_leaf ? 1u : 2u) + (r_leaf ? 1u : 2u);
+            if (l_leaf && r_leaf) slots[2] = kNone;
         }
-    }
-    LightSummary sm[4];
-    uint32_t words[4];
-#pragma unroll
-    for (uint32_t s = 0; s < 4; ++s) {
-        words[s] = kNone;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) sm[s].face[f] = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) sm[s].lo[k] = sm[s].hi[k] = 0.0f;
-        if (s < count) {
-            const uint32_t slot = slots[s];
-            if (slot & kChildLeafBit) {
-                const uint32_t p = slot & ~kChildLeafBit;
-                sm[s] = load_summary(sorted + p);
-                words[s] = kChildLeafBit | __ldg(values + p);
-            } else {
-                sm[s] = load_summary(&aggregates[slot].summary);
-                words[s] = __ldg(wide + slot);
+        // The node's own parent link.
+        uint32_t up_node = kNone, up_slot = 0;
+        if (i != 0) {
+            // An even-depth node below the root has a binary grandparent; the guard keeps a broken
+            // tree (a failed earlier stage) from reading outside the arrays.
+            const uint32_t p = __ldg(parent + i);
+            const uint32_t g = p + 1 < n ? __ldg(parent + p) : kNone;
+            if (g + 1 < n) {
+                const uint32_t gl = __ldg(left + g);
+                const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
+                up_slot = b0 + (__ldg(right + p) == i ? 1u : 0u);
+                up_node = __ldg(wide + g);
             }
         }
-    }
 #pragma unroll
-    for (uint32_t s = 0; s < 4; ++s)
-        if (s < count && (slots[s] & kChildLeafBit)) leaf_word[slots[s] & ~kChildLeafBit] = (w << kParentSlotBits) | s;
-    float4* q = reinterpret_cast<float4*>(nodes + w);
-    q[0] = make_float4(sm[0].face[0], sm[0].face[1], sm[0].face[2], sm[0].face[3]);
-    q[1] = make_float4(sm[0].face[4], sm[0].face[5], sm[1].face[0], sm[1].face[1]);
-    q[2] = make_float4(sm[1].face[2], sm[1].face[3], sm[1].face[4], sm[1].face[5]);
-    q[3] = make_float4(sm[2].face[0], sm[2].face[1], sm[2].face[2], sm[2].face[3]);
-    q[4] = make_float4(sm[2].face[4], sm[2].face[5], sm[3].face[0], sm[3].face[1]);
-    q[5] = make_float4(sm[3].face[2], sm[3].face[3], sm[3].face[4], sm[3].face[5]);
-    q[6] = make_float4(sm[0].lo[0], sm[0].lo[1], sm[0].lo[2], sm[1].lo[0]);
-    q[7] = make_float4(sm[1].lo[1], sm[1].lo[2], sm[2].lo[0], sm[2].lo[1]);
-    q[8] = make_float4(sm[2].lo[2], sm[3].lo[0], sm[3].lo[1], sm[3].lo[2]);
-    q[9] = make_float4(sm[0].hi[0], sm[0].hi[1], sm[0].hi[2], sm[1].hi[0]);
-    q[10] = make_float4(sm[1].hi[1], sm[1].hi[2], sm[2].hi[0], sm[2].hi[1]);
-    q[11] = make_float4(sm[2].hi[2], sm[3].hi[0], sm[3].hi[1], sm[3].hi[2]);
-    uint4* u = reinterpret_cast<uint4*>(nodes + w);
-    u[12] = make_uint4(words[0], words[1], words[2], words[3]);
-    u[13] = make_uint4(up_node, up_slot, 0u, 0u);
+        for (uint32_t c = 0; c < 4; ++c) {
+            LightSummary sm;
+#pragma unroll
+            for (int f = 0; f < 6; ++f) sm.face[f] = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) sm.lo[k] = sm.hi[k] = 0.0f;
+            uint32_t word = kNone;
+            if (c < used) {
+                const uint32_t slot = slots[c];
+                if (slot & kChildLeafBit) {
+                    const uint32_t p = slot & ~kChildLeafBit;
+                    sm = load_summary(sorted + p);
+                    word = kChildLeafBit | __ldg(values + p);
+                    leaf_word[p] = (w << kParentSlotBits) | c;
+                } else {
+                    sm = load_summary(&aggregates[slot].summary);
+                    word = __ldg(wide + slot);
+                }
+            }
+#pragma unroll
+            for (int f = 0; f < 6; ++f) node[6 * c + f] = sm.face[f];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                node[24 + 3 * c + k] = sm.lo[k];
+                node[36 + 3 * c + k] = sm.hi[k];
+            }
+            words[48 + c] = word;
+        }
+        words[52] = up_node;
+        words[53] = up_slot;
+        words[54] = 0u;
+        words[55] = 0u;
+    }
+    __syncthreads();
+    // The run [w_base, w_base + count), clipped to the node capacity.
+    const uint32_t last = min(w_base + count, node_capacity);
+    if (w_base >= last) return;
+    const uint32_t quads = (last - w_base) * (kNodeWords / 4);
+    const float4* src = reinterpret_cast<const float4*>(s_node);
+    float4* dst = reinterpret_cast<float4*>(nodes + w_base);
+    for (uint32_t q = threadIdx.x; q < quads; q += kWideThreads) dst[q] = src[q];
 }
 
 // The parent words of the leaves in leaf (record) order: the second 32-byte sector of every leaf
@@ -795,7 +823,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         lt_flags_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.left, b.cover, b.depth, b.wide,
                                                                   flag_states, scan_counters + 1, b.control);
         mark(6);
-        lt_wide_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
+        lt_wide_kernel<<<grid_for(nodes, kWideThreads, 1u << 30), kWideThreads, 0, stream>>>(
             n, b.node_capacity, b.values, b.left, b.right, b.parent, b.depth, b.wide, b.sorted, b.aggregates,
             b.leaf_word, b.nodes);
         lt_leaf_parent_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.inverse, b.leaf_word,
