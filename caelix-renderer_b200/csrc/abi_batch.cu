@@ -210,11 +210,19 @@ cudaError_t record(CaelixBatch* b, const CaelixBatchTuning& t, uint32_t item_cou
         uint32_t branch = 0;
         for (size_t i = 0; i < b->scenes.size(); ++i) {
             CaelixScene* sc = b->scenes[i];
-            CX_TRY(cx::scene_build_light_tree(sc->dev, b->branches[branch++ % used], t.sort_keys_per_thread));
-            if (sc->dyn_live) {  // the entities' light tree
-                cx::LightBvhInput in = sc->dyn_input;
+            // Tree 0: the world's own, or the static set's (world and static entities' lights).
+            if (sc->stat.live && sc->entity_view_count) {
+                cx::LightBvhInput in = sc->stat.input;
                 in.sort_keys_per_thread = t.sort_keys_per_thread;
-                CX_TRY(cx::lt_build(cx::lt_carve(sc->dyn_tree.ptr, sc->dyn_tree_capacity), in,
+                CX_TRY(cx::lt_build(cx::lt_carve(sc->stat.tree.ptr, sc->stat.tree_capacity), in,
+                                    b->branches[branch++ % used], nullptr));
+            } else {
+                CX_TRY(cx::scene_build_light_tree(sc->dev, b->branches[branch++ % used], t.sort_keys_per_thread));
+            }
+            if (sc->dyn.live && sc->entity_view_count) {  // the dynamic entities' light tree
+                cx::LightBvhInput in = sc->dyn.input;
+                in.sort_keys_per_thread = t.sort_keys_per_thread;
+                CX_TRY(cx::lt_build(cx::lt_carve(sc->dyn.tree.ptr, sc->dyn.tree_capacity), in,
                                     b->branches[branch++ % used], nullptr));
             }
         }

@@ -112,17 +112,30 @@ uint64_t align256(uint64_t v) { return (v + 255) & ~255ull; }
 // Scenes with at least this many entities trace them through the entity BVH.
 constexpr size_t kEntityBvhMin = 4;
 
-// The entities' light set: every live entity's light blocks, group rows, frames, power and light
-// records appended in view order (cx::dyn_append moves their indices), then the dynamic light
-// tree built over them, and the device copy of its SceneView. No entity light: none.
-CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const CaelixScene::Entity*>& live,
-                                 std::vector<cx::EntityView>& views, cudaStream_t stream)
+// A merged light set over `parts` (each a built scene's light tables under a transform: rows
+// null for the world part, whose frames are kept), their light blocks, group rows, frames, power
+// and light records appended in order (cx::dyn_append moves their indices; leaf words get
+// `leaf_flag`), then the light tree built over them. group_base[i] receives part i's first group.
+// With no light in any part the set is left not live.
+uint32_t entity_bvh_build(std::vector<cx::EntityNode>& nodes, std::vector<uint32_t>& order, size_t first, size_t last,
+                          const std::vector<cx::EntityView>& views);
+
+struct LightPart
 {
-    scene->dyn_live = false;
+    const cx::DeviceScene* d;
+    const float* rot;  // null: identity, no translation
+    const float* pos;
+};
+
+CaelixResult build_light_set(CaelixScene* scene, LightSet& set, const std::vector<LightPart>& parts,
+                             uint32_t leaf_flag, std::vector<uint32_t>& group_base, cudaStream_t stream)
+{
+    set.live = false;
+    group_base.assign(parts.size(), 0);
     uint64_t units = 0, groups = 0, bricks = 0, lights = 0;
-    for (size_t i = 0; i < live.size(); ++i) {
-        const cx::DeviceScene& d = live[i]->bricks->dev;
-        views[i].group_base = (uint32_t)groups;
+    for (size_t i = 0; i < parts.size(); ++i) {
+        const cx::DeviceScene& d = *parts[i].d;
+        group_base[i] = (uint32_t)groups;
         units += d.heap_words / 4;
         groups += d.group_count;
         bricks += d.brick_count;
@@ -136,9 +149,9 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
                    o_power = o_frames + align256(sizeof(cx::GroupFrame) * groups),
                    o_hdr = o_power + align256(4 * bricks), o_group = o_hdr + align256(sizeof(cx::BrickLightRecord) * lights),
                    o_entry = o_group + align256(4 * lights), total = o_entry + align256(4 * lights);
-    CaelixResult r = scene->dyn_arrays.reserve_grow(total, "caelix_scene_flush");
+    CaelixResult r = set.arrays.reserve_grow(total, "caelix_scene_flush");
     if (r != CAELIX_OK) return r;
-    uint8_t* base = static_cast<uint8_t*>(scene->dyn_arrays.ptr);
+    uint8_t* base = static_cast<uint8_t*>(set.arrays.ptr);
     uint32_t* heap = reinterpret_cast<uint32_t*>(base);
     uint32_t* rows = reinterpret_cast<uint32_t*>(base + o_rows);
     cx::GroupFrame* frames = reinterpret_cast<cx::GroupFrame*>(base + o_frames);
@@ -146,20 +159,22 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     cx::BrickLightRecord* hdr = reinterpret_cast<cx::BrickLightRecord*>(base + o_hdr);
     uint32_t* lgroup = reinterpret_cast<uint32_t*>(base + o_group);
     uint32_t* lentry = reinterpret_cast<uint32_t*>(base + o_entry);
-    if (lights > scene->dyn_tree_capacity) {
+    if (lights > set.tree_capacity) {
         const uint32_t cap = (uint32_t)std::max<uint64_t>(lights + lights / 8, 64);
-        r = scene->dyn_tree.reserve(cx::lt_buffer_bytes(cap), "caelix_scene_flush");
+        r = set.tree.reserve(cx::lt_buffer_bytes(cap), "caelix_scene_flush");
         if (r != CAELIX_OK) return r;
-        scene->dyn_tree_capacity = cap;
+        set.tree_capacity = cap;
     }
-    const cx::LightBvhBuffers tree = cx::lt_carve(scene->dyn_tree.ptr, scene->dyn_tree_capacity);
+    const cx::LightBvhBuffers tree = cx::lt_carve(set.tree.ptr, set.tree_capacity);
     cudaError_t e = cudaSuccess;
-    cx::DynPart part{0, 0, 0, 0, {}, {}};
-    for (size_t i = 0; i < live.size() && e == cudaSuccess; ++i) {
-        const cx::DeviceScene& d = live[i]->bricks->dev;
-        part.group_base = views[i].group_base;
-        std::memcpy(part.rot, live[i]->rot, sizeof(part.rot));
-        std::memcpy(part.pos, live[i]->position, sizeof(part.pos));
+    cx::DynPart part{0, 0, 0, 0, {1.0f, 0.0f, 0.0f, 0.0f, 1.0f, 0.0f, 0.0f, 0.0f, 1.0f}, {0.0f, 0.0f, 0.0f}, leaf_flag};
+    for (size_t i = 0; i < parts.size() && e == cudaSuccess; ++i) {
+        const cx::DeviceScene& d = *parts[i].d;
+        part.group_base = group_base[i];
+        if (parts[i].rot) {
+            std::memcpy(part.rot, parts[i].rot, sizeof(part.rot));
+            std::memcpy(part.pos, parts[i].pos, sizeof(part.pos));
+        }
         e = cx::dyn_append(d, part, heap, rows, frames, power, hdr, lgroup, lentry, stream);
         part.unit_base += d.heap_words / 4;
         part.record_base += d.brick_count;
@@ -173,9 +188,9 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     in.group_frames = frames;
     in.group_count = (uint32_t)groups;
     in.sort_keys_per_thread = cx::kSortKeysPerThread;
-    scene->dyn_input = in;
+    set.input = in;
     if (e == cudaSuccess) e = cx::lt_build(tree, in, stream, nullptr);
-    cx::SceneView v;
+    cx::SceneView& v = set.v;
     std::memset(&v, 0, sizeof(v));
     v.group_shift = scene->group_shift;
     v.enc = cx::encoding_of(scene->encoding);
@@ -191,16 +206,101 @@ CaelixResult build_entity_lights(CaelixScene* scene, const std::vector<const Cae
     v.light_count = (uint32_t)lights;
     v.group_count = (uint32_t)groups;
     if (e == cudaSuccess) {
-        r = scene->dyn_view.reserve_grow(sizeof(v), "caelix_scene_flush");
+        r = set.view.reserve_grow(sizeof(v), "caelix_scene_flush");
         if (r != CAELIX_OK) return r;
-        e = cudaMemcpyAsync(scene->dyn_view.ptr, &v, sizeof(v), cudaMemcpyHostToDevice, stream);
+        e = cudaMemcpyAsync(set.view.ptr, &v, sizeof(v), cudaMemcpyHostToDevice, stream);
     }
     uint32_t status = 0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&status, &tree.state->status, 4, cudaMemcpyDeviceToHost, stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     if (status & ~cx::kStatusNodeOverflow) return cx::status_result(status, "caelix_scene_flush");
-    scene->dyn_live = true;
+    set.live = true;
+    return CAELIX_OK;
+}
+
+// The dynamic entities' light set (SceneView::dyn) over the live dynamic entities, in view order.
+CaelixResult build_dynamic_lights(CaelixScene* scene, cudaStream_t stream)
+{
+    std::vector<LightPart> parts;
+    std::vector<size_t> which;
+    for (size_t i = 0; i < scene->host_views.size(); ++i) {
+        const CaelixScene::Entity& ent = scene->entities[scene->view_entity[i]];
+        if (ent.motion != CAELIX_ENTITY_DYNAMIC) continue;
+        parts.push_back({&ent.bricks->dev, ent.rot, ent.position});
+        which.push_back(i);
+    }
+    std::vector<uint32_t> base;
+    CaelixResult r = build_light_set(scene, scene->dyn, parts, 0x80000000u, base, stream);
+    for (size_t j = 0; j < which.size(); ++j) {
+        scene->host_views[which[j]].group_base = base[j];
+        scene->host_views[which[j]].tree = scene->dyn.live ? 1u : cx::kNone;
+    }
+    return r;
+}
+
+// Tree 0's static set: the world's light tables first (so every world index stays valid), then
+// the live static entities' in view order, with tree 0 built over them. Only while a static
+// entity has lights (and the world's tables exist); otherwise tree 0 is the world's own.
+CaelixResult build_static_lights(CaelixScene* scene, cudaStream_t stream)
+{
+    std::vector<LightPart> parts;
+    std::vector<size_t> which;
+    bool lit = false;
+    if (scene->built) {
+        parts.push_back({&scene->dev, nullptr, nullptr});
+        for (size_t i = 0; i < scene->host_views.size(); ++i) {
+            const CaelixScene::Entity& ent = scene->entities[scene->view_entity[i]];
+            if (ent.motion != CAELIX_ENTITY_STATIC) continue;
+            parts.push_back({&ent.bricks->dev, ent.rot, ent.position});
+            which.push_back(i);
+            lit = lit || ent.bricks->dev.light_count != 0;
+        }
+    }
+    scene->stat_dirty = false;
+    std::vector<uint32_t> base;
+    CaelixResult r = CAELIX_OK;
+    if (lit) {
+        r = build_light_set(scene, scene->stat, parts, 0u, base, stream);
+    } else {
+        scene->stat.live = false;
+        base.assign(parts.size(), 0);
+    }
+    for (size_t j = 0; j < which.size(); ++j) {
+        scene->host_views[which[j]].group_base = base[j + 1];
+        scene->host_views[which[j]].tree = scene->stat.live ? 0u : cx::kNone;
+    }
+    return r;
+}
+
+// The device copies of the entity views (host_views) and the entity BVH.
+CaelixResult write_entity_views(CaelixScene* scene, cudaStream_t stream)
+{
+    const std::vector<cx::EntityView>& views = scene->host_views;
+    scene->entity_nodes_used = false;
+    if (!views.empty()) {
+        CaelixResult r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
+        if (r != CAELIX_OK) return r;
+        cudaError_t e = cudaMemcpyAsync(scene->entity_views.ptr, views.data(), sizeof(cx::EntityView) * views.size(),
+                                        cudaMemcpyHostToDevice, stream);
+        // With several entities a ray tests only those whose box it meets (trace_entities).
+        std::vector<cx::EntityNode> nodes;
+        if (e == cudaSuccess && views.size() >= kEntityBvhMin) {
+            std::vector<uint32_t> order(views.size());
+            for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
+            nodes.reserve(2 * views.size());
+            entity_bvh_build(nodes, order, 0, order.size(), views);
+            r = scene->entity_nodes.reserve(sizeof(cx::EntityNode) * nodes.size(), "caelix_scene_flush");
+            if (r != CAELIX_OK) return r;
+            e = cudaMemcpyAsync(scene->entity_nodes.ptr, nodes.data(), sizeof(cx::EntityNode) * nodes.size(),
+                                cudaMemcpyHostToDevice, stream);
+            scene->entity_nodes_used = true;
+        }
+        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    }
+    scene->entity_view_count = (uint32_t)views.size();
+    scene->entity_generation += 1;
     return CAELIX_OK;
 }
 
@@ -246,22 +346,25 @@ uint32_t entity_bvh_build(std::vector<cx::EntityNode>& nodes, std::vector<uint32
     return index;
 }
 
-// Rewrites the device views of the live entities and their light set (after waiting for the
+// Rewrites the device views of the live entities and their light sets (after waiting for the
 // device: renders may read the old ones) and returns when they are in place. An entity whose
 // bricks were never flushed has no tables yet and joins at the flush that builds them.
 CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
 {
-    std::vector<cx::EntityView> views;
-    std::vector<const CaelixScene::Entity*> live;
+    std::vector<cx::EntityView>& views = scene->host_views;
+    views.clear();
+    scene->view_entity.clear();
     for (size_t id = 0; id < scene->entities.size(); ++id) {
         CaelixScene::Entity& e = scene->entities[id];
         if (!e.bricks || !e.bricks->built) continue;
         cx::EntityView v;
+        std::memset(&v, 0, sizeof(v));
         v.scene = cx::scene_view(e.bricks->dev);
         std::memcpy(v.rot, e.rot, sizeof(v.rot));
         std::memcpy(v.pos, e.position, sizeof(v.pos));
         v.group_base = 0;
         v.id = (uint32_t)id + 1;
+        v.tree = cx::kNone;
         // The sphere round the entity's brick grid [8 origin, 8 (origin + grid)) in world space
         // (double, inflated).
         {
@@ -280,40 +383,35 @@ CaelixResult upload_entity_views(CaelixScene* scene, cudaStream_t stream)
             v.sphere[3] = (float)(std::sqrt(r2) * 1.001 + 0.01);
         }
         views.push_back(v);
-        live.push_back(&e);
+        scene->view_entity.push_back((uint32_t)id);
         e.generation = e.bricks->generation;
     }
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
     scene->entity_view_count = 0;
-    CaelixResult r = build_entity_lights(scene, live, views, stream);
+    CaelixResult r = build_dynamic_lights(scene, stream);
+    if (r == CAELIX_OK) r = build_static_lights(scene, stream);
     if (r != CAELIX_OK) return r;
-    scene->entity_nodes_used = false;
-    if (!views.empty()) {
-        r = scene->entity_views.reserve(sizeof(cx::EntityView) * views.size(), "caelix_scene_flush");
-        if (r != CAELIX_OK) return r;
-        e = cudaMemcpyAsync(scene->entity_views.ptr, views.data(), sizeof(cx::EntityView) * views.size(),
-                            cudaMemcpyHostToDevice, stream);
-        // With several entities a ray tests only those whose box it meets (trace_entities).
-        std::vector<cx::EntityNode> nodes;
-        if (e == cudaSuccess && views.size() >= kEntityBvhMin) {
-            std::vector<uint32_t> order(views.size());
-            for (uint32_t i = 0; i < order.size(); ++i) order[i] = i;
-            nodes.reserve(2 * views.size());
-            entity_bvh_build(nodes, order, 0, order.size(), views);
-            r = scene->entity_nodes.reserve(sizeof(cx::EntityNode) * nodes.size(), "caelix_scene_flush");
-            if (r != CAELIX_OK) return r;
-            e = cudaMemcpyAsync(scene->entity_nodes.ptr, nodes.data(), sizeof(cx::EntityNode) * nodes.size(),
-                                cudaMemcpyHostToDevice, stream);
-            scene->entity_nodes_used = true;
-        }
-        if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-        if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
-    }
-    scene->entity_view_count = (uint32_t)views.size();
+    r = write_entity_views(scene, stream);
+    if (r != CAELIX_OK) return r;
     scene->entity_views_dirty = false;
-    scene->entity_generation += 1;
     return CAELIX_OK;
+}
+
+// After a change of the world's light tables: tree 0's static set again (with the static
+// entities' views, whose group bases follow the world's group count), when static entities exist.
+CaelixResult refresh_static_lights(CaelixScene* scene, cudaStream_t stream)
+{
+    if (!scene->stat_dirty) return CAELIX_OK;
+    scene->stat_dirty = false;
+    bool any = false;
+    for (uint32_t id : scene->view_entity) any = any || scene->entities[id].motion == CAELIX_ENTITY_STATIC;
+    if (!any) return CAELIX_OK;
+    cudaError_t e = cudaDeviceSynchronize();  // renders may read the old set
+    if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+    CaelixResult r = build_static_lights(scene, stream);
+    if (r == CAELIX_OK) r = write_entity_views(scene, stream);
+    return r;
 }
 
 }  // namespace
@@ -325,7 +423,20 @@ cx::SceneView render_view(const CaelixScene* scene)
         v.entities = static_cast<const cx::EntityView*>(scene->entity_views.ptr);
         v.entity_count = scene->entity_view_count;
         if (scene->entity_nodes_used) v.entity_nodes = static_cast<const cx::EntityNode*>(scene->entity_nodes.ptr);
-        if (scene->dyn_live) v.dyn = static_cast<const cx::SceneView*>(scene->dyn_view.ptr);
+        if (scene->dyn.live) v.dyn = static_cast<const cx::SceneView*>(scene->dyn.view.ptr);
+        if (scene->stat.live) {
+            // Tree 0 and its light set: the static set, the world's tables at their own indices.
+            const cx::SceneView& t = scene->stat.v;
+            v.power = t.power;
+            v.heap = t.heap;
+            v.group_rows = t.group_rows;
+            v.frames = t.frames;
+            v.leaves = t.leaves;
+            v.nodes = t.nodes;
+            v.header = t.header;
+            v.light_count = t.light_count;
+            v.group_count = t.group_count;
+        }
     }
     return v;
 }
@@ -417,9 +528,8 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     scene->entities.clear();
     scene->entity_views.release();
     scene->entity_nodes.release();
-    scene->dyn_arrays.release();
-    scene->dyn_tree.release();
-    scene->dyn_view.release();
+    scene->dyn.release();
+    scene->stat.release();
     scene->materials_dev.release();
     scene->light_codes_dev.release();
     cx::scene_release(scene->dev);
@@ -733,7 +843,9 @@ CAELIX_API CaelixResult caelix_scene_set_entity_motion(CaelixScene* scene, Caeli
     if (!scene || entity == 0 || !entity_bricks(scene, entity) ||
         (motion != CAELIX_ENTITY_STATIC && motion != CAELIX_ENTITY_DYNAMIC))
         return CAELIX_ERROR_INVALID_ARGUMENT;
-    scene->entities[entity - 1].motion = motion;
+    CaelixScene::Entity& e = scene->entities[entity - 1];
+    if (e.motion != motion) scene->entity_views_dirty = true;  // its lights change trees at the next flush
+    e.motion = motion;
     return CAELIX_OK;
 }
 
@@ -834,9 +946,8 @@ CAELIX_API CaelixResult caelix_scene_set_light_options(CaelixScene* scene, const
     return CAELIX_OK;
 }
 
-CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrameDesc* desc)
+static CaelixResult scene_flush_body(CaelixScene* scene, const CaelixFrameDesc* desc)
 {
-    CAELIX_GUARD_BEGIN
     if (!scene || !desc) return CAELIX_ERROR_INVALID_ARGUMENT;
     if (desc->frame_number <= scene->last_frame || desc->safe_frame_number >= desc->frame_number) {
         log(CAELIX_LOG_ERROR, "caelix_scene_flush: frame %llu after %llu (safe %llu) breaks the frame contract",
@@ -882,6 +993,7 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     if (!scene->built) scene->full_rebuild = true;
     const bool edits = !scene->dirty_slots.empty();
     if (!scene->full_rebuild && !edits && !scene->light_tree_dirty) return CAELIX_OK;
+    scene->stat_dirty = true;  // the world's light tables change
     uint32_t status = 0;
     cudaError_t e = cudaSuccess;
     if (!scene->full_rebuild) {
@@ -990,6 +1102,15 @@ CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrame
     scene->built = true;
     scene->generation += 1;
     return cx::status_result(status & ~cx::kStatusNodeOverflow, "caelix_scene_flush");
+}
+
+CAELIX_API CaelixResult caelix_scene_flush(CaelixScene* scene, const CaelixFrameDesc* desc)
+{
+    CAELIX_GUARD_BEGIN
+    CaelixResult r = scene_flush_body(scene, desc);
+    // Tree 0's static set follows the world's light tables.
+    if (r == CAELIX_OK) r = refresh_static_lights(scene, reinterpret_cast<cudaStream_t>(desc->command_buffer));
+    return r;
     CAELIX_GUARD_END
 }
 
@@ -1001,7 +1122,10 @@ CAELIX_API void caelix_scene_get_light_stats(const CaelixScene* scene, CaelixLig
     const cx::DeviceScene& d = scene->dev;
     unsigned char host[128];
     cudaSetDevice(scene->device->ordinal);
-    if (cudaMemcpy(host, d.tree.header, 128, cudaMemcpyDeviceToHost) != cudaSuccess) return;
+    // Tree 0: the static set's tree while static entities have lights, else the world's own.
+    const bool stat = scene->stat.live && scene->entity_view_count;
+    const void* tree0 = stat ? static_cast<const void*>(scene->stat.v.header) : static_cast<const void*>(d.tree.header);
+    if (cudaMemcpy(host, tree0, 128, cudaMemcpyDeviceToHost) != cudaSuccess) return;
     cx::LightTreeHeader h;
     cx::LightTreeState st;
     std::memcpy(&h, host, 64);
@@ -1017,6 +1141,15 @@ CAELIX_API void caelix_scene_get_light_stats(const CaelixScene* scene, CaelixLig
     out->tree_nodes[0] = h.node_count;
     out->tree_builds[0] = st.builds;
     out->tree_leaves_dropped[0] = st.leaves_dropped;
+    if (scene->dyn.live && scene->entity_view_count &&
+        cudaMemcpy(host, scene->dyn.v.header, 128, cudaMemcpyDeviceToHost) == cudaSuccess) {
+        std::memcpy(&h, host, 64);
+        std::memcpy(&st, host + 64, 64);
+        out->tree_leaves[1] = h.leaf_count;
+        out->tree_nodes[1] = h.node_count;
+        out->tree_builds[1] = st.builds;
+        out->tree_leaves_dropped[1] = st.leaves_dropped;
+    }
     std::vector<uint32_t> rows(8ull * d.group_count);
     if (d.group_count &&
         cudaMemcpy(rows.data(), d.group_rows, 32ull * d.group_count, cudaMemcpyDeviceToHost) == cudaSuccess) {

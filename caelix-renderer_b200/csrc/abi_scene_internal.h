@@ -11,6 +11,29 @@
 #include "scene.cuh"
 #include "trace.cuh"
 
+// A merged light set on the device (the dynamic entities' lights, or tree 0's static set: the
+// world's lights and the static entities'): its arrays, its light tree, the device copy of its
+// SceneView (the dynamic set's), the tree's build input and the view itself (null pointers when
+// not live).
+struct LightSet
+{
+    cx::GrowBuffer arrays;
+    cx::GrowBuffer tree;
+    cx::GrowBuffer view;
+    uint32_t tree_capacity = 0;
+    bool live = false;
+    cx::LightBvhInput input{};
+    cx::SceneView v{};
+    void release()
+    {
+        arrays.release();
+        tree.release();
+        view.release();
+        tree_capacity = 0;
+        live = false;
+    }
+};
+
 struct CaelixScene
 {
     CaelixDevice* device = nullptr;
@@ -83,14 +106,14 @@ struct CaelixScene
     bool entity_nodes_used = false;
     uint32_t entity_view_count = 0;
     bool entity_views_dirty = false;
-    // The entities' light set (SceneView::dyn), rebuilt with the views: its arrays, the dynamic
-    // light tree's buffers and the device copy of its SceneView (null: no entity light).
-    cx::GrowBuffer dyn_arrays;
-    cx::GrowBuffer dyn_tree;
-    cx::GrowBuffer dyn_view;
-    uint32_t dyn_tree_capacity = 0;
-    bool dyn_live = false;
-    cx::LightBvhInput dyn_input{};  // the build input of the entities' light tree (while dyn_live)
+    // The dynamic entities' light set (SceneView::dyn) and tree 0's static set (the world's lights
+    // then the static entities'; live only while a static entity has lights), rebuilt with the
+    // views; the static set also after every change of the world's lights.
+    LightSet dyn;
+    LightSet stat;
+    bool stat_dirty = false;
+    std::vector<uint32_t> view_entity;     // the entity index of every device view
+    std::vector<cx::EntityView> host_views;  // the host copy of the device views
     uint64_t entity_generation = 0;  // uploads of the entity views so far (the device views move)
 };
 

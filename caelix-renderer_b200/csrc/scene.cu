@@ -915,7 +915,7 @@ __global__ void dyn_patch_kernel(uint32_t* __restrict__ heap, uint32_t* __restri
             for (uint32_t e = 0; e < count; ++e) {
                 uint32_t* ie = block + 4 + 4ull * e;
                 ie[1] += part.record_base;
-                ie[3] = 0x80000000u | (part.light_base + (ie[3] & 0x7FFFFFFFu));
+                if (ie[3] != kNone) ie[3] = part.leaf_flag | (part.light_base + (ie[3] & 0x7FFFFFFFu));
             }
         }
         GroupFrame& f = frames[part.group_base + i];

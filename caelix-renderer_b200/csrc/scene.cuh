@@ -73,6 +73,9 @@ struct SceneView
     const float4* materials;  // [kMaterialCodes][2]: albedo, emission
     const uint32_t* light_codes;  // [kLightCodeWords]: the light code set
     const int32_t* keys;          // [brick_count][3]: the key of every record
+    // The light set of tree 0: the world's own, or, with lights in static entities, the static
+    // light set (the world's light blocks, group rows, frames, power and light records first, at
+    // the same indices, then the static entities' appended as for `dyn`) with tree 0 built over it.
     const uint32_t* heap;    // group light blocks, 16-byte units
     const uint32_t* group_rows;  // [group_count][8]
     const GroupFrame* frames;    // [group_count]
@@ -82,14 +85,15 @@ struct SceneView
     uint32_t light_count;
     uint32_t group_count;
     // Entities beside the scene's own bricks (the static world): each traversed in its frame
-    // after the world; their lights are the light set `dyn`.
+    // after the world; the lights of static entities are in tree 0's light set, those of dynamic
+    // ones in `dyn`.
     const EntityView* entities;  // device, entity_count of them
     uint32_t entity_count;
     const EntityNode* entity_nodes;  // the BVH over the entities (root 0), or null: test every entity
-    // The entities' lights (null: none), a light set of its own in device memory (its heap,
-    // group rows, frames, power and the dynamic light tree; the tree of the reference's dynamic
-    // entities): entity e's groups from its group_base, its light blocks' brick words after the
-    // earlier entities' bricks, every index entry's leaf word 0x80000000 | its leaf in that tree.
+    // The dynamic entities' lights (null: none), a light set of its own in device memory (its
+    // heap, group rows, frames, power and the dynamic light tree; the tree of the reference's
+    // dynamic entities): entity e's groups from its group_base, its light blocks' brick words after
+    // the earlier entities' bricks, every index entry's leaf word 0x80000000 | its leaf in that tree.
     const SceneView* dyn;
 };
 
@@ -103,9 +107,10 @@ struct EntityView
     SceneView scene;
     float rot[9];
     float pos[3];
-    uint32_t group_base;  // its first group in the entities' light set
+    uint32_t group_base;  // its first group in the light set of its tree
     float sphere[4];      // world centre and radius of a sphere holding its brick grid (inflated)
     uint32_t id;          // its entity id (the voxel id target's entity word)
+    uint32_t tree;        // the tree holding its lights: 0 (static), 1 (dynamic), kNone (no light set has it)
 };
 
 // The attribute bit of an entity hit (bits 0..5 face flags, 6..14 cell, 16..31 block: bit 15 is
@@ -218,15 +223,18 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
 cudaError_t staging_update(const uint16_t* stage_voxels, const uint32_t* slots, const float* power, uint32_t count,
                            const uint32_t* record_of_slot, DeviceScene& s, uint32_t* marks, uint32_t epoch,
                            uint32_t* list, uint32_t* list_count, cudaStream_t stream);
-// The entities' light set (SceneView::dyn): entity e's light blocks, group rows, frames, power
-// and light records copied after the earlier entities' (dst_*: device arrays sized for all) and
-// their indices moved: group rows by unit_base heap units, the index entries' brick words by
-// record_base, their leaf words to 0x80000000 | (light_base + leaf), the frames set to the
-// entity's transform, the light records' groups by group_base.
+// A merged light set (SceneView::dyn, or tree 0's static set): a part's light blocks, group rows,
+// frames, power and light records copied after the earlier parts' (dst_*: device arrays sized for
+// all) and their indices moved: group rows by unit_base heap units, the index entries' brick words
+// by record_base, their leaf words to leaf_flag | (light_base + leaf) (0x80000000 in the dynamic
+// tree, 0 in tree 0), the frames set to the part's transform, the light records' groups by
+// group_base. The world as the first part of the static set (bases 0, identity transform) is a
+// plain copy.
 struct DynPart
 {
     uint32_t group_base, unit_base, record_base, light_base;
     float rot[9], pos[3];
+    uint32_t leaf_flag;
 };
 cudaError_t dyn_append(const DeviceScene& e, const DynPart& part, uint32_t* dst_heap, uint32_t* dst_rows,
                        GroupFrame* dst_frames, float* dst_power, BrickLightRecord* dst_headers, uint32_t* dst_group,

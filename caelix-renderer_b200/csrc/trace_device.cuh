@@ -1101,7 +1101,8 @@ __device__ __forceinline__ bool nee_prepare(const SceneView& s, const float x[3]
         r.value[c] = contribution[c] * k;
         r.dvalue_de[c] = em[c] * (scale * k);
     }
-    r.brick = (!kEntities || p.tree == 0) ? brick : kNone;  // a world brick's power
+    // A world brick's power (tree 0 also holds static entities' bricks, after the world's).
+    r.brick = ((!kEntities || p.tree == 0) && brick < s.brick_count) ? brick : kNone;
     return true;
 }
 
@@ -1109,12 +1110,14 @@ __device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segme
                                  const float dir[3], const float seg_n[3])
 {
     if (segment_light == 0u || h.t < kNearField) return 1.0f;
-    // The light set of the hit: the world's, or for an entity hit the entities' (its groups from
-    // the entity's group base; the voxel from the entity-local hit point and face normal).
+    // The light set of the hit: tree 0's for the world and static entities, the dynamic one for
+    // dynamic entities (an entity's groups from its group base; the voxel from the entity-local
+    // hit point and face normal).
     const uint32_t face = (uint32_t)(__ffs(h.attrib & 0x3Fu) - 1);
     const bool entity = (h.attrib & kEntityHit) != 0;
-    if (entity && !s.dyn) return 1.0f;
-    const SceneView& L = entity ? *s.dyn : s;
+    const uint32_t tree = entity ? __ldg(&s.entities[h.group >> kEntityShift].tree) : 0u;
+    if (tree > 1u || (tree == 1u && !s.dyn)) return 1.0f;
+    const SceneView& L = tree == 1u ? *s.dyn : s;
     const uint32_t group = entity ? __ldg(&s.entities[h.group >> kEntityShift].group_base) + (h.group & kEntityGroupMask)
                                   : h.group;
     float nl[3];
@@ -1133,7 +1136,7 @@ __device__ __noinline__ float lamp_hit_weight(const SceneView& s, uint32_t segme
     float in_brick;
     if (!find_light_face(L, origin, group, vig, face, block, entry, leaf, in_brick) || leaf == kNone) return 1.0f;
     const float cos_l = -dot3(h.normal, dir);
-    const float p_area = brick_pdf(s, L, origin, seg_n, group, entry, entity ? 1u : 0u) * in_brick;
+    const float p_area = brick_pdf(s, L, origin, seg_n, group, entry, tree) * in_brick;
     return mis_weight(p_area, seg_n, dir, h.t, cos_l, false);
 }
 

@@ -190,10 +190,12 @@ typedef struct oc_scene {
     const struct oc_entity* entities;
     uint32_t entity_count;
     uint32_t pad2;
-    /* The entities' lights (NULL: none): their light blocks, group rows, frames and power merged
-     * into one light set (entity e's groups from its group_base, its bricks' power after the
-     * others', every index entry's leaf word 0x80000000 | leaf of the dynamic tree) and the
-     * dynamic light tree (tree 1) built over them. */
+    /* The dynamic entities' lights (NULL: none): their light blocks, group rows, frames and power
+     * merged into one light set (entity e's groups from its group_base, its bricks' power after
+     * the others', every index entry's leaf word 0x80000000 | leaf of the dynamic tree) and the
+     * dynamic light tree (tree 1) built over them. Static entities' lights are merged the same
+     * way after the world's own into this scene's light set (heap, group rows, frames; leaf words
+     * without the mark), with tree 0 built over both (the caller passes that tree and power). */
     const struct oc_scene* dyn;
     const struct oc_light_tree* dyn_tree;
     const float* dyn_power;
@@ -206,8 +208,11 @@ typedef struct oc_entity {
     const oc_scene* scene;
     float rot[9];
     float pos[3];
-    uint32_t group_base; /* its first group in the merged light set */
+    uint32_t group_base; /* its first group in the light set of its tree */
     uint32_t id;         /* its entity id (the voxel id's entity word) */
+    uint32_t tree;       /* the tree holding its lights: 0 (a static entity: the scene's own light set,
+                          * which then holds the world's lights first and the static entities' after
+                          * them), 1 (a dynamic entity: `dyn`), OC_NONE (none) */
     const float* power;  /* its bricks' emitter power */
 } oc_entity;
 

@@ -914,8 +914,10 @@ static void next_event(ctx* c, const float x[3], const float n[3], uint32_t* lig
          * code times scale * k. */
         *lamp_code = oc_material_code(words[0], c->s->encoding);
         *dvalue = scale * k;
-        if (words[5] == 0) *lamp_brick = brick;
-        else *lamp_fixed = c->s->dyn_power[brick];
+        /* A world lamp's power is a parameter; a static entity's (tree 0, after the world's
+         * bricks) and a dynamic entity's are held fixed. */
+        if (words[5] == 0 && brick < c->s->brick_count) *lamp_brick = brick;
+        else *lamp_fixed = words[5] == 0 ? c->power[brick] : c->s->dyn_power[brick];
     }
 }
 
@@ -931,11 +933,16 @@ static float lamp_hit_weight(ctx* c, uint32_t segment_light, const oc_hit* h, co
     const uint32_t face = (uint32_t)__builtin_ctz(h->attrib & 0x3Fu);
     float nl[3] = {h->normal[0], h->normal[1], h->normal[2]};
     if (h->attrib & OC_ENTITY_HIT) {
-        if (!c->s->dyn) return 1.0f;
-        L = c->s->dyn;
-        T = c->s->dyn_tree;
-        k = 1;
-        group = c->s->entities[h->group >> 24].group_base + (h->group & 0xFFFFFFu);
+        /* A static entity's lights are in tree 0 (this scene's light set), a dynamic one's in
+         * tree 1. */
+        const oc_entity* E = &c->s->entities[h->group >> 24];
+        if (E->tree > 1u || (E->tree == 1u && !c->s->dyn)) return 1.0f;
+        if (E->tree == 1u) {
+            L = c->s->dyn;
+            T = c->s->dyn_tree;
+            k = 1;
+        }
+        group = E->group_base + (h->group & 0xFFFFFFu);
         for (int q = 0; q < 3; ++q) nl[q] = 0.0f;
         nl[face >> 1] = (face & 1u) ? -1.0f : 1.0f;
     }

@@ -105,7 +105,7 @@ class Scene(C.Structure):
 
 class Entity(C.Structure):
     _fields_ = [("scene", C.c_void_p), ("rot", C.c_float * 9), ("pos", C.c_float * 3), ("group_base", C.c_uint32),
-                ("id", C.c_uint32), ("power", C.c_void_p)]
+                ("id", C.c_uint32), ("tree", C.c_uint32), ("power", C.c_void_p)]
 
 
 class Camera(C.Structure):
@@ -210,30 +210,59 @@ class OracleScene:
             self.tree = lt_build(lib, np.zeros(0, RECORD_DTYPE_LOCAL()), leaf_capacity=1)
         self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
                             self.tree["header"].ctypes.data)
+        self._set_tree0(None)
 
-    def set_entities(self, entities, ids=None):
-        """Entities beside the scene's bricks: (OracleScene of the entity's bricks, quaternion x y z w,
-        position) each, traversed in order; rotation rows as the library computes them; ids: their
-        entity ids (the voxel id's entity word; default 1, 2, ...). The
-        entities' light records (of bricks with power) are merged into one light set in entity
-        order, with its own light tree (tree 1): entity i's groups from the sum of the earlier
-        entities' group counts, its heap units, brick indices and leaves after theirs (the index
-        entries' brick and leaf words moved, the leaf word marked 0x80000000), every group's frame
-        the entity's transform."""
-        self._entity_scenes = [e[0] for e in entities]
-        arr = (Entity * max(len(entities), 1))()
-        heaps, rows, frames, powers, headers, lgroup, lentry = [], [], [], [], [], [], []
+    def _set_tree0(self, merged):
+        """Tree 0 and its light set: the world's own (merged None), or a merged static set (the
+        world's light blocks first at their own indices, then the static entities'): the scene's
+        heap, group rows and frames point at it, `lt` is its tree and `power0` its power."""
+        s = self.s
+        if not hasattr(self, "_own0"):
+            self._own0 = (s.heap, s.heap_words, s.group_rows, s.group_frames, s.group_count, s.light_count, self.lt,
+                          self.tree)
+        own = self._own0
+        if merged is None:
+            s.heap, s.heap_words, s.group_rows, s.group_frames, s.group_count, s.light_count = own[:6]
+            self.lt, self.tree = own[6], own[7]
+            self.heap0, self.rows0, self.frames0 = self.heap, self.group_rows, self.group_frames
+            self.power0 = self.src.power
+            self._merged0 = None
+            return
+        self._merged0 = merged
+        s.heap = merged["heap"].ctypes.data
+        s.heap_words = len(merged["heap"])
+        s.group_rows = merged["rows"].ctypes.data
+        s.group_frames = merged["frames"].ctypes.data
+        s.group_count = len(merged["rows"])
+        s.light_count = merged["lights"]
+        self.tree = merged["tree"]
+        self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
+                            self.tree["header"].ctypes.data)
+        self.heap0, self.rows0, self.frames0 = merged["heap"], merged["rows"], merged["frames"]
+        self.power0 = merged["power"]
+
+    def _merge(self, parts, leaf_flag, world):
+        """A merged light set: with `world` the scene's own light tables first (unchanged), then
+        each part (index, OracleScene, rotation rows, position) with its groups, heap units, brick
+        indices and leaves after the earlier ones' (the index entries' brick and leaf words moved,
+        the leaf word marked with leaf_flag), every group's frame the part's transform. Returns the
+        arrays, the light tree over the records and every part's group base."""
+        from caelix_b200 import workloads
+
+        heaps, rows, frames, powers, headers, lgroup, lentry, bases = [], [], [], [], [], [], [], []
         group_base = unit_base = record_base = light_base = 0
-        for i, (osc, q, pos) in enumerate(entities):
-            qf = np.ascontiguousarray(q, np.float32)
-            rot = np.zeros(9, np.float32)
-            self.lib.oc_entity_rows(qf.ctypes.data, rot.ctypes.data)
-            arr[i].scene = C.cast(C.pointer(osc.s), C.c_void_p)
-            arr[i].rot[:] = [float(v) for v in rot]
-            arr[i].pos[:] = [float(v) for v in np.asarray(pos, np.float32)]
-            arr[i].group_base = group_base
-            arr[i].id = int(ids[i]) if ids is not None else i + 1
-            arr[i].power = osc.src.power.ctypes.data
+        if world:
+            heaps.append(self.heap)
+            rows.append(self.group_rows)
+            frames.append(self.group_frames)
+            powers.append(self.src.power)
+            if self.light_count:
+                headers.append(self.light_headers)
+                lgroup.append(self.light_group)
+                lentry.append(self.light_entry)
+            group_base, unit_base, record_base, light_base = (len(self.group_rows), len(self.heap) // 4,
+                                                              self.src.brick_count, self.light_count)
+        for _, osc, rot, pos in parts:
             heap = osc.heap.copy()
             r = osc.group_rows.copy()
             for g in np.nonzero(r[:, 1])[0]:
@@ -241,7 +270,8 @@ class OracleScene:
                 for e in range(int(heap[block])):
                     ie = block + 4 + 4 * e
                     heap[ie + 1] += record_base
-                    heap[ie + 3] = 0x80000000 | (light_base + (int(heap[ie + 3]) & 0x7FFFFFFF))
+                    if heap[ie + 3] != 0xFFFFFFFF:
+                        heap[ie + 3] = leaf_flag | (light_base + (int(heap[ie + 3]) & 0x7FFFFFFF))
                 r[g, 0] += unit_base
             heaps.append(heap)
             rows.append(r)
@@ -254,26 +284,63 @@ class OracleScene:
                 headers.append(osc.light_headers)
                 lgroup.append(osc.light_group + group_base)
                 lentry.append(osc.light_entry)
+            bases.append(group_base)
             group_base += len(r)
             unit_base += len(heap) // 4
             record_base += osc.src.brick_count
             light_base += osc.light_count
+        if not light_base:
+            return None, bases
+        out = dict(heap=np.ascontiguousarray(np.concatenate(heaps), np.uint32),
+                   rows=np.ascontiguousarray(np.concatenate(rows), np.uint32),
+                   frames=np.ascontiguousarray(np.concatenate(frames)),
+                   power=np.ascontiguousarray(np.concatenate(powers), np.float32),
+                   headers=np.ascontiguousarray(np.concatenate(headers)).view(workloads.RECORD_DTYPE),
+                   group=np.ascontiguousarray(np.concatenate(lgroup), np.uint32),
+                   entry=np.ascontiguousarray(np.concatenate(lentry), np.uint32), lights=light_base)
+        out["tree"] = lt_build(self.lib, out["headers"], record_group=out["group"], record_entry=out["entry"],
+                               group_frames=out["frames"])
+        return out, bases
+
+    def set_entities(self, entities, ids=None, motions=None):
+        """Entities beside the scene's bricks: (OracleScene of the entity's bricks, quaternion x y z w,
+        position) each, traversed in order; rotation rows as the library computes them; ids: their
+        entity ids (the voxel id's entity word; default 1, 2, ...); motions: 0 (static, the
+        library's default) or 1 (dynamic) each. The dynamic entities' light records are merged into
+        one light set in entity order with its own light tree (tree 1; leaf words marked
+        0x80000000); with lights in static entities, the world's light set and the static
+        entities' are merged (the world's first, at its own indices) and tree 0 built over them.
+        In a merged set an entity's groups follow the earlier parts' group counts, its heap units,
+        brick indices and leaves theirs, and every group's frame is the entity's transform."""
+        motions = list(motions) if motions is not None else [0] * len(entities)
+        self._set_tree0(None)
+        self._entity_scenes = [e[0] for e in entities]
+        arr = (Entity * max(len(entities), 1))()
+        dyn_parts, stat_parts = [], []
+        for i, (osc, q, pos) in enumerate(entities):
+            qf = np.ascontiguousarray(q, np.float32)
+            rot = np.zeros(9, np.float32)
+            self.lib.oc_entity_rows(qf.ctypes.data, rot.ctypes.data)
+            arr[i].scene = C.cast(C.pointer(osc.s), C.c_void_p)
+            arr[i].rot[:] = [float(v) for v in rot]
+            arr[i].pos[:] = [float(v) for v in np.asarray(pos, np.float32)]
+            arr[i].group_base = 0
+            arr[i].id = int(ids[i]) if ids is not None else i + 1
+            arr[i].tree = 0xFFFFFFFF
+            arr[i].power = osc.src.power.ctypes.data
+            (dyn_parts if motions[i] == 1 else stat_parts).append((i, osc, rot, pos))
         self._entities = arr
         self.s.entities = C.cast(arr, C.c_void_p) if entities else None
         self.s.entity_count = len(entities)
         self.s.dyn = self.s.dyn_tree = self.s.dyn_power = None
-        if light_base:
-            from caelix_b200 import workloads
-
-            self.dyn_heap = np.ascontiguousarray(np.concatenate(heaps), np.uint32)
-            self.dyn_rows = np.ascontiguousarray(np.concatenate(rows), np.uint32)
-            self.dyn_frames = np.ascontiguousarray(np.concatenate(frames))
-            self.dyn_power = np.ascontiguousarray(np.concatenate(powers), np.float32)
-            self.dyn_headers = np.ascontiguousarray(np.concatenate(headers)).view(workloads.RECORD_DTYPE)
-            self.dyn_group = np.ascontiguousarray(np.concatenate(lgroup), np.uint32)
-            self.dyn_entry = np.ascontiguousarray(np.concatenate(lentry), np.uint32)
-            self.dyn_tree = lt_build(self.lib, self.dyn_headers, record_group=self.dyn_group, record_entry=self.dyn_entry,
-                                     group_frames=self.dyn_frames)
+        dyn, bases = self._merge(dyn_parts, 0x80000000, world=False)
+        if dyn is not None:
+            for (i, _, _, _), b in zip(dyn_parts, bases):
+                arr[i].group_base = b
+                arr[i].tree = 1
+            self.dyn_heap, self.dyn_rows, self.dyn_frames = dyn["heap"], dyn["rows"], dyn["frames"]
+            self.dyn_power, self.dyn_headers = dyn["power"], dyn["headers"]
+            self.dyn_group, self.dyn_entry, self.dyn_tree = dyn["group"], dyn["entry"], dyn["tree"]
             self._dyn_lt = LightTree(self.dyn_tree["leaves"].ctypes.data, self.dyn_tree["nodes"].ctypes.data,
                                      self.dyn_tree["header"].ctypes.data)
             d = Scene()
@@ -282,7 +349,7 @@ class OracleScene:
             d.emission = self.s.emission
             d.light_codes = self.s.light_codes
             d.group_count = len(self.dyn_rows)
-            d.light_count = light_base
+            d.light_count = dyn["lights"]
             d.heap_words = len(self.dyn_heap)
             d.heap = self.dyn_heap.ctypes.data
             d.group_rows = self.dyn_rows.ctypes.data
@@ -291,9 +358,16 @@ class OracleScene:
             self.s.dyn = C.cast(C.pointer(d), C.c_void_p)
             self.s.dyn_tree = C.cast(C.pointer(self._dyn_lt), C.c_void_p)
             self.s.dyn_power = self.dyn_power.ctypes.data
+        if any(osc.light_count for _, osc, _, _ in stat_parts):
+            stat, bases = self._merge(stat_parts, 0, world=True)
+            for (i, _, _, _), b in zip(stat_parts, bases):
+                arr[i].group_base = b
+                arr[i].tree = 0
+            self._set_tree0(stat)
 
     def close(self):
         if self.s.records:
+            self._set_tree0(None)
             self.s.entities = None
             self.s.entity_count = 0
             self.s.dyn = self.s.dyn_tree = self.s.dyn_power = None
@@ -327,7 +401,7 @@ class OracleScene:
         out = np.zeros((height, width, 3), np.float32)
         rays = np.zeros(3, np.uint64)
         self.lib.oc_render(C.byref(self.s), C.byref(self.lt), self.albedo_table.ctypes.data,
-                           self.src.power.ctypes.data, C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data,
+                           self.power0.ctypes.data, C.byref(c), C.byref(r), out.ctypes.data, rays.ctypes.data,
                            threads)
         if voxel_ids:
             return out, rays, ids
@@ -358,7 +432,7 @@ class OracleScene:
         if d_radiance is not None:
             d_radiance = np.ascontiguousarray(d_radiance, np.float32)
             g_ptr = d_radiance.ctypes.data
-        self.lib.oc_adjoint(C.byref(self.s), C.byref(self.lt), self.albedo_table.ctypes.data, self.src.power.ctypes.data,
+        self.lib.oc_adjoint(C.byref(self.s), C.byref(self.lt), self.albedo_table.ctypes.data, self.power0.ctypes.data,
                             C.byref(c), C.byref(r), a_ptr, p_ptr, g_ptr, image.ctypes.data, dA.ctypes.data,
                             dP.ctypes.data, threads)
         return image, dA, dP[: self.s.brick_count]
@@ -452,6 +526,7 @@ class TablesScene(OracleScene):
                              group_frames=self.group_frames, leaf_capacity=max(m, 1))
         self.lt = LightTree(self.tree["leaves"].ctypes.data, self.tree["nodes"].ctypes.data,
                             self.tree["header"].ctypes.data)
+        self._set_tree0(None)
 
     def close(self):
         pass  # the arrays are numpy-owned

@@ -1,7 +1,8 @@
 """Entities through the C ABI against the oracle: a world with two entities (one rotated, one
 translated), rendered with the wavefront and the per-frame kernels; then an entity moved, an
-entity's bricks edited, an entity removed and a new one added in its id, then entity lights (the
-second light tree) and a lit entity moved. Every state's radiance and ray counts equal the
+entity's bricks edited, an entity removed and a new one added in its id, then entity lights (a
+dynamic entity's in the second light tree, a static entity's in tree 0 beside the world's), a lit
+entity moved and a static entity made dynamic. Every state's radiance and ray counts equal the
 oracle's with the same entities (bit-exact expected; the 1e-5 relative bound of the trace parity
 tests)."""
 import numpy as np
@@ -63,7 +64,7 @@ def test_entities_parity(cuda_device, oracle):
     osc = oracle_lib.OracleScene(oracle, vs)
     o1 = oracle_lib.OracleScene(oracle, b1)
     o2 = oracle_lib.OracleScene(oracle, b2)
-    osc.set_entities([(o1, Q1, p1), (o2, IDENTITY, p2)])
+    osc.set_entities([(o1, Q1, p1), (o2, IDENTITY, p2)], motions=[0, 1])
     img = render_pair(cuda_device, scene, osc, vs)
     render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
     plain = oracle_lib.OracleScene(oracle, vs).render(72, 56, spp=2, bounces=4, seed=5, threads=8)[0]
@@ -72,7 +73,7 @@ def test_entities_parity(cuda_device, oracle):
     # Moved; the next flush applies it.
     scene.set_entity_transform(e1, p1, Q1_MOVED)
     scene.flush()
-    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)])
+    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)], motions=[0, 1])
     render_pair(cuda_device, scene, osc, vs)
 
     # Edited bricks of an entity (no new key: that entity's incremental flush).
@@ -83,19 +84,19 @@ def test_entities_parity(cuda_device, oracle):
     scene.flush()
     b2e = workloads.VoxelScene(b2.grid, b2.keys, vox2, b2.power, b2.albedo, b2.camera, b2.group_shift)
     o2 = oracle_lib.OracleScene(oracle, b2e)
-    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)])
+    osc.set_entities([(o1, Q1_MOVED, p1), (o2, IDENTITY, p2)], motions=[0, 1])
     render_pair(cuda_device, scene, osc, vs)
 
     # Removed: the remaining entity keeps its order; a new entity takes the free id.
     scene.remove_entity(e1)
-    osc.set_entities([(o2, IDENTITY, p2)])
+    osc.set_entities([(o2, IDENTITY, p2)], motions=[1])
     render_pair(cuda_device, scene, osc, vs)  # the removal applies at once
     e3 = scene.add_entity(p1, IDENTITY)
     assert e3 == e1
     scene.upload_bricks(b1.keys, b1.voxels, entity=e3)
     scene.set_brick_power(b1.keys, b1.power, entity=e3)
     scene.flush()
-    osc.set_entities([(o1, IDENTITY, p1), (o2, IDENTITY, p2)])
+    osc.set_entities([(o1, IDENTITY, p1), (o2, IDENTITY, p2)], motions=[0, 1])
     render_pair(cuda_device, scene, osc, vs)
 
     # Entity lights: some bricks of both entities emit (the second light tree), then one moves.
@@ -109,13 +110,13 @@ def test_entities_parity(cuda_device, oracle):
                                                              b1.group_shift))
     l2 = oracle_lib.OracleScene(oracle, workloads.VoxelScene(b2.grid, b2.keys, vox2, p_2, b2.albedo, b2.camera,
                                                              b2.group_shift))
-    osc.set_entities([(l1, IDENTITY, p1), (l2, IDENTITY, p2)])
-    assert osc.s.dyn
+    osc.set_entities([(l1, IDENTITY, p1), (l2, IDENTITY, p2)], motions=[0, 1])
+    assert osc.s.dyn and osc._merged0 is not None  # e3's lights in tree 0, e2's in tree 1
     lit = render_pair(cuda_device, scene, osc, vs)
     render_pair(cuda_device, scene, osc, vs, mode=caelix_b200.Renderer.TRACE_MEGAKERNEL, spp=1)
     scene.set_entity_transform(e3, p1, Q1)
     scene.flush()
-    osc.set_entities([(l1, Q1, p1), (l2, IDENTITY, p2)])
+    osc.set_entities([(l1, Q1, p1), (l2, IDENTITY, p2)], motions=[0, 1])
     moved = render_pair(cuda_device, scene, osc, vs)
     assert not np.array_equal(lit, moved)
 
@@ -147,6 +148,13 @@ def test_entities_parity(cuda_device, oracle):
         assert torch.equal(out, ref)
         batch.close()
     r.close()
+
+    # A static entity made dynamic: its lights leave tree 0 for the dynamic tree at the next flush.
+    scene.set_entity_motion(e3, 1)
+    scene.flush()
+    osc.set_entities([(l1, Q1, p1), (l2, IDENTITY, p2)], motions=[1, 1])
+    assert osc._merged0 is None
+    render_pair(cuda_device, scene, osc, vs)
 
     # Entity 0 cannot be moved or removed; motion takes two values.
     with pytest.raises(caelix_b200.CaelixError):

@@ -171,17 +171,22 @@ def lit_scene(oracle, world):
     w = oracle_lib.OracleScene(oracle, world)
     e1 = oracle_lib.OracleScene(oracle, lit_entity((2, 2, 2), 31))
     e2 = oracle_lib.OracleScene(oracle, lit_entity((2, 1, 2), 32))
-    w.set_entities([(e1, (0.2, -0.1, 0.3, 0.93), (60.0, 10.0, 5.0)), (e2, (0.0, 0.0, 0.0, 1.0), (-30.0, 20.0, 12.0))])
+    # e1 static (its lights join the world's in tree 0), e2 dynamic (tree 1).
+    w.set_entities([(e1, (0.2, -0.1, 0.3, 0.93), (60.0, 10.0, 5.0)), (e2, (0.0, 0.0, 0.0, 1.0), (-30.0, 20.0, 12.0))],
+                   motions=[0, 1])
     assert w.s.dyn and w.dyn_tree["header"][0]["root"] != 0xFFFFFFFF
+    assert w._merged0 is not None and w.tree["header"][0]["leaf_count"] == w.light_count + e1.light_count
     return w
 
 
 def test_pdf_normalised_over_both_trees(lit_scene, world):
     """The light-tree pdf summed over every light face of the world and of the entities (each face
     of area 1 in its frame) is 1 (1e-4) for every receiver: the tree choice and both trees' walks
-    are consistent (the reference's CheckNormalisation over its two trees)."""
+    are consistent (the reference's CheckNormalisation over its two trees; tree 0 holds the world's
+    and the static entity's lights)."""
     w = lit_scene
-    faces0 = light_faces(w.heap, w.group_rows, w.s.group_shift)
+    faces0 = light_faces(w.heap0, w.rows0, w.s.group_shift)
+    assert len(faces0) > len(light_faces(w.heap, w.group_rows, w.s.group_shift))
     faces1 = light_faces(w.dyn_heap, w.dyn_rows, w.s.group_shift)
     assert faces0 and faces1
     rng = np.random.default_rng(8)
@@ -215,7 +220,7 @@ def test_entity_light_draws_match_their_pdf(lit_scene, world):
             continue
         block, vi, face, group, entry, tree = (int(v) for v in words)
         drawn[tree] += 1
-        frames = w.dyn_frames if tree else w.group_frames
+        frames = w.dyn_frames if tree else w.frames0
         fr = frames[group]
         R = fr["rotation"].reshape(3, 3).astype(np.float64)
         local = R.T @ (out[:3].astype(np.float64) - fr["translation"]) - fr["origin"]
@@ -265,7 +270,7 @@ def test_draw_histogram_over_both_trees(lit_scene, world):
     (5 sigma for faces with at least 50 expected draws; no draw on a face of pdf 0), the
     reference's CheckHistogram over its two trees."""
     w = lit_scene
-    faces = [(0, f) for f in light_faces(w.heap, w.group_rows, w.s.group_shift)] + \
+    faces = [(0, f) for f in light_faces(w.heap0, w.rows0, w.s.group_shift)] + \
             [(1, f) for f in light_faces(w.dyn_heap, w.dyn_rows, w.s.group_shift)]
     key = {}
     for i, (tree, (g, v, f, blk)) in enumerate(faces):
