@@ -46,7 +46,6 @@ constexpr uint8_t kWorldHasPlayerPose = 1;
 // Version gates of the entity record and the world record.
 constexpr uint16_t kVersionEntityFlags = 3, kVersionVelocity = 4, kVersionProtected = 5, kVersionFlagsV6 = 6,
                    kVersionWorldRecord = 7;
-constexpr int32_t kSceneKeyLimit = 1024;  // caelix_scene_upload_bricks: keys in [0, 1024)
 
 struct ReadError
 {
@@ -438,8 +437,8 @@ CAELIX_API CaelixResult caelix_world_decode_sector(const CaelixWorldFile* file, 
 
 namespace {
 
-// Every sector of one file entity decoded on the host threads (each with its own inflate buffer),
-// and the entity's smallest key per axis (its origin in a scene, whose keys start at 0).
+// Every sector of one file entity decoded on the host threads (each with its own inflate buffer);
+// org (the move applied to its keys) is 0.
 CaelixResult decode_entity(const CaelixWorldFile* file, uint32_t entity, uint32_t threads, const char* what,
                            std::vector<Decoded>& decoded, int32_t org[3])
 {
@@ -471,29 +470,10 @@ CaelixResult decode_entity(const CaelixWorldFile* file, uint32_t entity, uint32_
     for (std::thread& th : pool) th.join();
     for (uint32_t t = 0; t < nt; ++t)
         if (has_error[t]) return report(first[t]);
-    int64_t lo[3] = {INT64_MAX, INT64_MAX, INT64_MAX}, hi[3] = {INT64_MIN, INT64_MIN, INT64_MIN};
-    uint64_t total = 0;
-    for (const Decoded& d : decoded) {
-        total += d.keys.size();
-        for (const CaelixBrickKey& k : d.keys) {
-            const int64_t v[3] = {k.x, k.y, k.z};
-            for (int a = 0; a < 3; ++a) {
-                lo[a] = std::min(lo[a], v[a]);
-                hi[a] = std::max(hi[a], v[a]);
-            }
-        }
-    }
+    // The keys go to the scene as the file holds them (the reference's loader passes the decoder's
+    // keys through): the scene takes [-2^20, 2^20) per axis and its flush checks the box.
+    (void)what;
     for (int a = 0; a < 3; ++a) org[a] = 0;
-    if (total) {
-        for (int a = 0; a < 3; ++a) {
-            if (hi[a] - lo[a] >= kSceneKeyLimit) {
-                cx::log(CAELIX_LOG_ERROR, "%s: entity %u spans %" PRId64 " bricks on axis %d (the scene holds %d)", what,
-                        entity, hi[a] - lo[a] + 1, a, kSceneKeyLimit);
-                return CAELIX_ERROR_UNSUPPORTED;
-            }
-            org[a] = (int32_t)lo[a];
-        }
-    }
     return CAELIX_OK;
 }
 

@@ -811,19 +811,18 @@ CAELIX_API CaelixResult caelix_world_decode_sector(const CaelixWorldFile* file, 
                                                    CaelixBrickKey* keys, uint16_t* blocks, uint32_t* summaries,
                                                    uint32_t* brick_count, uint64_t* voxels);
 /* Decodes every sector of one entity on `threads` host threads (0 = all) and uploads its bricks
-   to the scene (caelix_scene_upload_bricks), keys moved by -origin, origin = the smallest key of
-   the entity per axis (written to `origin`, may be NULL), so that the world's lowest brick sits
-   at 0. Bricks outside the scene's key range after the move: CAELIX_ERROR_UNSUPPORTED, nothing
-   uploaded. *bricks (may be NULL) = bricks uploaded. */
+   to the scene (caelix_scene_upload_bricks) with the file's keys unchanged, as the reference's
+   loader passes the decoder's keys through (host-rs/caelix-app/src/world.rs:212-247); `origin`
+   (may be NULL) receives the move applied to the keys, which is 0. A key outside [-2^20, 2^20):
+   the upload's CAELIX_ERROR_INVALID_ARGUMENT. *bricks (may be NULL) = bricks uploaded. */
 CAELIX_API CaelixResult caelix_world_upload_entity(const CaelixWorldFile* file, uint32_t entity, CaelixScene* scene,
                                                    uint32_t threads, int32_t origin[3], uint64_t* bricks);
 /* Loads every entity of the file, as the reference's WorldLoader::open + upload
    (host-rs/caelix-app/src/world.rs:93-262): file entity 0 into the scene's world (as
-   caelix_world_upload_entity: keys moved by its origin), every other entity as a scene entity
-   (caelix_scene_add_entity, motion from its Static flag) with its bricks moved by its own origin
-   and its transform expressed in the world's frame: x_scene = R0^T (x_file - p0) - 8 origin0, so
-   the added entity has rotation conj(q0) qi and position
-   R0^T (Ri (8 origin_i) + (pi - p0)) - 8 origin0 (computed in double, rounded to float).
+   caelix_world_upload_entity), every other entity as a scene entity (caelix_scene_add_entity,
+   motion from its Static flag) with its transform expressed in the world's frame:
+   x_scene = R0^T (x_file - p0), so the added entity has rotation conj(q0) qi and position
+   R0^T (pi - p0) (computed in double, rounded to float).
    ids (may be NULL) receives the scene entity of every file entity (0 for the world). A failure
    removes the entities added (the world's bricks uploaded before it stay). *bricks (may be NULL)
    = bricks uploaded. */

@@ -231,23 +231,6 @@ def test_large_payload_grows_inflate_buffer(tmp_path):
     assert_decodes(f, 0, s)
 
 
-def test_upload_rejects_a_world_wider_than_the_scene(tmp_path):
-    """caelix_world_upload_entity checks the key span before any device work (no GPU needed to
-    see the refusal: a scene handle is only used when the span fits)."""
-    import ctypes
-
-    import caelix_b200
-
-    w = W.World(8, [W.Entity([simple_sector((0, 0, 0)), simple_sector((64, 0, 0))])])
-    f = open_world(tmp_path, W.build(w))
-    origin = (ctypes.c_int32 * 3)()
-    bricks = ctypes.c_uint64(0)
-    fake_scene = ctypes.c_void_p(1)  # never dereferenced on this path
-    code = f.L.lib.caelix_world_upload_entity(f.handle, 0, fake_scene, 2, origin, ctypes.byref(bricks))
-    assert code == 2 and "spans 1040 bricks on axis 0" in f.L.log[-1]
-    assert bricks.value == 0
-
-
 def test_scene_round_trip(tmp_path):
     """A generated scene written as a world file (caelix_b200.cxw.from_voxel_scene, keys moved to
     negative sectors) decodes back to its non-air bricks, sector by sector."""

@@ -1,6 +1,7 @@
 """A world file into a scene: caelix_world_upload_entity decodes a .cxw world written from a
-generated scene (sectors of 16^3 bricks, moved to negative sector coordinates) and uploads it; the
-flushed scene equals the oracle's build of the same bricks moved to the returned origin."""
+generated scene (sectors of 16^3 bricks, moved to negative sector coordinates, or spread wider than
+1024 bricks) and uploads its keys unchanged, as the reference's loader does; the flushed scene
+equals the oracle's build of the same bricks."""
 import numpy as np
 import pytest
 
@@ -25,13 +26,46 @@ def test_world_file_into_scene(cuda_device, oracle, tmp_path):
     keep = (vs.voxels != 0).any(axis=1)  # the reader drops all-air bricks
     keys = vs.keys[keep]
     assert bricks == int(keep.sum())
-    assert origin == tuple(int(keys[:, a].min()) + shift[a] for a in range(3))
-    moved = keys + np.array(shift, np.int32) - np.array(origin, np.int32)
-    grid = tuple(int(v) for v in moved.max(axis=0) + 1)
-    lin = moved[:, 0] + grid[0] * (moved[:, 1] + grid[1] * moved[:, 2].astype(np.int64))
+    assert origin == (0, 0, 0)  # the keys go in as the file holds them
+    exp = in_box_order(vs, keys + np.array(shift, np.int32), vs.voxels[keep], vs.power[keep])
+    scene.set_brick_power(exp.keys, exp.power)
+    scene.flush()
+    assert_scene_equal(scene, oracle_lib.OracleScene(oracle, exp), exp)
+    scene.close()
+    f.close()
+
+
+def in_box_order(src, keys, voxels, power):
+    """A VoxelScene of the bricks in increasing linear index of the box of their keys (the order of
+    the flushed scene's tables)."""
+    keys = keys.astype(np.int32)
+    origin, grid = workloads.scene_grid(keys, src.group_shift)
+    k = keys.astype(np.int64) - np.array(origin, np.int64)
+    lin = k[:, 0] + grid[0] * (k[:, 1] + grid[1] * k[:, 2])
     o = np.argsort(lin, kind="stable")
-    exp = workloads.VoxelScene(grid, moved[o], vs.voxels[keep][o], vs.power[keep][o], vs.albedo, vs.camera,
-                               vs.group_shift)
+    return workloads.VoxelScene(tuple(int(v) for v in grid), keys[o], voxels[o], power[o], src.albedo, src.camera,
+                                src.group_shift)
+
+
+def test_world_wider_than_1024_bricks(cuda_device, oracle, tmp_path):
+    """A world of two clusters 1,200 bricks apart, one at negative keys: loaded unchanged and
+    flushed, its tables equal the oracle's."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(6, 5, 6), brick_occupancy=0.5, emissive_fraction=0.1, seed=29)
+    half = vs.brick_count // 2
+    keys = vs.keys.copy()
+    keys[:half] += np.array([-600, -3, 2], np.int32)
+    keys[half:] += np.array([600, 1, -40], np.int32)
+    path = tmp_path / "wide.cxw"
+    path.write_bytes(W.build(W.World(8, [W.Entity(W.sectors_of(keys, vs.voxels))])))
+    f = caelix_b200.WorldFile(str(path))
+    scene = caelix_b200.Scene.for_voxel_scene(cuda_device, vs)
+    origin, bricks = f.upload_entity(0, scene, threads=2)
+    keep = (vs.voxels != 0).any(axis=1)
+    assert origin == (0, 0, 0) and bricks == int(keep.sum())
+    exp = in_box_order(vs, keys[keep], vs.voxels[keep], vs.power[keep])
+    assert exp.keys[:, 0].max() - exp.keys[:, 0].min() > 1024
     scene.set_brick_power(exp.keys, exp.power)
     scene.flush()
     assert_scene_equal(scene, oracle_lib.OracleScene(oracle, exp), exp)
@@ -78,29 +112,18 @@ def test_world_load_with_entities(cuda_device, oracle, tmp_path):
     keep0 = (vs.voxels != 0).any(axis=1)
     keep1 = (ent.voxels != 0).any(axis=1)
     assert bricks == int(keep0.sum() + keep1.sum())
-    org0 = (vs.keys[keep0] + shift0).min(axis=0)
-    org1 = (ent.keys[keep1] + shift1).min(axis=0)
-
-    def moved(src, keys, voxels, power, shift, org):
-        k = keys + shift - org
-        grid = tuple(int(v) for v in k.max(axis=0) + 1)
-        lin = k[:, 0] + grid[0] * (k[:, 1] + grid[1] * k[:, 2].astype(np.int64))
-        o = np.argsort(lin, kind="stable")
-        return workloads.VoxelScene(grid, k[o].astype(np.int32), voxels[o], power[o], src.albedo, src.camera,
-                                    src.group_shift)
-
-    world = moved(vs, vs.keys[keep0], vs.voxels[keep0], vs.power[keep0], shift0, org0)
+    # The keys go in unchanged (no origin move).
+    world = in_box_order(vs, vs.keys[keep0] + shift0, vs.voxels[keep0], vs.power[keep0])
     # The loader sets no power: the entity's bricks keep the default power 1 (they emit).
-    body = moved(ent, ent.keys[keep1], ent.voxels[keep1], np.ones(int(keep1.sum()), np.float32), shift1, org1)
+    body = in_box_order(ent, ent.keys[keep1] + shift1, ent.voxels[keep1], np.ones(int(keep1.sum()), np.float32))
     scene.set_brick_power(world.keys, world.power)
     scene.flush()
     assert_scene_equal(scene, oracle_lib.OracleScene(oracle, world), world)
 
     # The entity's transform in the world's frame, the library's arithmetic.
-    r0, r1 = rows64(q0), rows64(q1)
-    v = [(r1[3 * k] * (8.0 * org1[0]) + r1[3 * k + 1] * (8.0 * org1[1]) + r1[3 * k + 2] * (8.0 * org1[2])) +
-         (float(np.float32(p1[k])) - float(np.float32(p0[k]))) for k in range(3)]
-    pos = tuple(np.float32((r0[k] * v[0] + r0[3 + k] * v[1] + r0[6 + k] * v[2]) - 8.0 * org0[k]) for k in range(3))
+    r0 = rows64(q0)
+    v = [(float(np.float32(p1[k])) - float(np.float32(p0[k]))) for k in range(3)]
+    pos = tuple(np.float32(r0[k] * v[0] + r0[3 + k] * v[1] + r0[6 + k] * v[2]) for k in range(3))
     a = [float(np.float32(c)) for c in q0]
     n0 = math.sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2] + a[3] * a[3])
     ax, ay, az, aw = -a[0] / n0, -a[1] / n0, -a[2] / n0, a[3] / n0
@@ -110,7 +133,7 @@ def test_world_load_with_entities(cuda_device, oracle, tmp_path):
 
     cam = workloads.look_at(np.array(pos, np.float64) + np.array([-30.0, 20.0, -30.0]), np.array(pos, np.float64))
     osc = oracle_lib.OracleScene(oracle, world)
-    osc.set_entities([(oracle_lib.OracleScene(oracle, body), rot, pos)])
+    osc.set_entities([(oracle_lib.OracleScene(oracle, body), rot, pos)], motions=[1])  # its Static flag is clear
     r = caelix_b200.Renderer(cuda_device, scene)
     import torch
 
