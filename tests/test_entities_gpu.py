@@ -103,6 +103,7 @@ def test_entities_parity(cuda_device, oracle):
     rng = np.random.default_rng(4)
     p_1 = np.where(rng.random(b1.brick_count) < 0.5, rng.lognormal(0.0, 1.0, b1.brick_count), 0.0).astype(np.float32)
     p_2 = np.where(rng.random(b2.brick_count) < 0.5, rng.lognormal(0.0, 1.0, b2.brick_count), 0.0).astype(np.float32)
+    p_2[0] = 2.0  # both trees hold entity lights
     scene.set_brick_power(b1.keys, p_1, entity=e3)
     scene.set_brick_power(b2.keys, p_2, entity=e2)
     scene.flush()
