@@ -1,0 +1,57 @@
+// The decoupled look-back of the single-pass scans, by one warp: the 32 lanes read the states of
+// 32 predecessor tiles at once, so a tile waits one round trip per 32 predecessors instead of one
+// per predecessor.
+#pragma once
+#include <cstdint>
+
+#include "cx_device.cuh"
+#include "cx_layout.h"
+#include "radix_sort.cuh"
+
+namespace cx {
+
+// Called by every lane of one warp for tile `tile` with its aggregate `agg` (30-bit values; kMax:
+// running maximum, else sum): lane 0 publishes the aggregate, the warp walks back window by window
+// (the nearest tile with an inclusive prefix ends the walk; a window with an unpublished tile
+// before that one is read again, a bounded number of times, after which kStatusLookbackTimeout is
+// set in *status), lane 0 publishes the inclusive prefix. Returns the exclusive prefix in every lane.
+template <bool kMax>
+__device__ __forceinline__ uint32_t warp_lookback(uint32_t* states, uint32_t tile, uint32_t agg, uint32_t* status)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t* state = states + tile;
+    if (tile == 0) {
+        if (lane == 0) st_relaxed(state, kTileFlagPrefix | (agg & kTileValueMask));
+        return 0;
+    }
+    if (lane == 0) st_relaxed(state, kTileFlagAggregate | (agg & kTileValueMask));
+    uint32_t prefix = 0;
+    int64_t j = (int64_t)tile - 1;  // the nearest tile of the window (lane 0's)
+    uint32_t spins = 0;
+    while (j >= 0) {
+        const int64_t t = j - (int64_t)lane;
+        // Before tile 0: an inclusive prefix of 0.
+        const uint32_t s = t >= 0 ? ld_relaxed(states + t) : kTileFlagPrefix;
+        const uint32_t ready = __ballot_sync(0xFFFFFFFFu, (s & ~kTileValueMask) != 0u);
+        const uint32_t found = __ballot_sync(0xFFFFFFFFu, (s & kTileFlagPrefix) != 0u);
+        const uint32_t stop = found ? (uint32_t)(__ffs(found) - 1) : 31u;
+        const uint32_t need = (2u << stop) - 1u;  // lanes 0 .. stop (all 32 when stop is 31)
+        if ((ready & need) != need) {
+            if (!spin_wait(spins)) {
+                if (lane == 0) atomicOr(status, kStatusLookbackTimeout);
+                break;
+            }
+            continue;
+        }
+        const uint32_t v = lane <= stop ? (s & kTileValueMask) : 0u;
+        const uint32_t w = kMax ? __reduce_max_sync(0xFFFFFFFFu, v) : __reduce_add_sync(0xFFFFFFFFu, v);
+        prefix = kMax ? max(prefix, w) : prefix + w;
+        if (found) break;
+        j -= 32;
+    }
+    const uint32_t incl = kMax ? max(prefix, agg) : prefix + agg;
+    if (lane == 0) st_relaxed(state, kTileFlagPrefix | (incl & kTileValueMask));
+    return prefix;
+}
+
+}  // namespace cx

@@ -2,6 +2,7 @@
 #include <cuda/atomic>
 
 #include "cx_device.cuh"
+#include "lookback.cuh"
 #include "lt_build.cuh"
 #include "radix_sort.cuh"
 
@@ -411,39 +412,10 @@ __global__ void __launch_bounds__(kAggTile)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Single-pass exclusive scan (decoupled look-back over tiles of kScanItems per thread). `op`
-// picks the element: the range-count prefix (inclusive, in place) or the even-depth flags.
-constexpr int kScanItems = 4;
+// Single-pass exclusive scans over tiles of kScanItems per thread (decoupled look-back by one warp,
+// warp_lookback).
+constexpr int kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;
-
-__device__ __forceinline__ uint32_t scan_lookback(uint32_t* states, uint32_t tile, uint32_t total,
-                                                  BuildControl* control)
-{
-    uint32_t* state = states + tile;
-    if (tile == 0) {
-        st_relaxed(state, kTileFlagPrefix | total);
-        return 0;
-    }
-    st_relaxed(state, kTileFlagAggregate | total);
-    uint32_t exclusive = 0;
-    int64_t j = (int64_t)tile - 1;
-    uint32_t spins = 0;
-    while (j >= 0) {
-        const uint32_t s = ld_relaxed(states + j);
-        if ((s & ~kTileValueMask) == 0) {
-            if (!spin_wait(spins)) {
-                atomicOr(&control->status, kStatusLookbackTimeout);
-                break;
-            }
-            continue;
-        }
-        exclusive += s & kTileValueMask;
-        if (s & kTileFlagPrefix) break;
-        --j;
-    }
-    st_relaxed(state, kTileFlagPrefix | ((exclusive + total) & kTileValueMask));
-    return exclusive;
-}
 
 // cover[g] for g < count becomes the number of binary nodes over leaf boundary g (inclusive prefix
 // sum of the differences). The u32 differences wrap; the prefix is exact.
@@ -469,7 +441,10 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
     // The look-back values are 30-bit: the range counts (at most the tree depth) never need more,
     // but a tile's sum of differences can be "negative"; carry it as its low 30 bits.
-    if (threadIdx.x == 0) s_prefix = scan_lookback(states, tile, total & kTileValueMask, control);
+    if (threadIdx.x < 32) {
+        const uint32_t p = warp_lookback<false>(states, tile, total & kTileValueMask, &control->status);
+        if (threadIdx.x == 0) s_prefix = p;
+    }
     __syncthreads();
     uint32_t run = s_prefix + local;
 #pragma unroll
@@ -510,9 +485,12 @@ __global__ void __launch_bounds__(kScanThreads)
     }
     uint32_t total;
     const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
-    if (threadIdx.x == 0) {
-        s_prefix = scan_lookback(states, tile, total, control);
-        if (tile == gridDim.x - 1) control->node_count = s_prefix + total;
+    if (threadIdx.x < 32) {
+        const uint32_t p = warp_lookback<false>(states, tile, total, &control->status);
+        if (threadIdx.x == 0) {
+            s_prefix = p;
+            if (tile == gridDim.x - 1) control->node_count = p + total;
+        }
     }
     __syncthreads();
     uint32_t run = s_prefix + local;

@@ -5,6 +5,7 @@
 #include <vector>
 
 #include "cx_device.cuh"
+#include "lookback.cuh"
 #include "radix_sort.cuh"
 #include "scene.cuh"
 #include "scene_device.cuh"
@@ -14,7 +15,7 @@ namespace cx {
 namespace {
 
 constexpr int kThreads = 256;
-constexpr int kScanItems = 4;
+constexpr int kScanItems = 16;
 constexpr uint32_t kScanTile = kThreads * kScanItems;
 
 __host__ __device__ __forceinline__ uint32_t part1by2(uint32_t v)
@@ -73,33 +74,12 @@ __global__ void __launch_bounds__(kThreads)
     uint32_t excl_in_warp = __shfl_up_sync(0xFFFFFFFFu, inc, 1);
     if (lane == 0) excl_in_warp = 0;
     const uint32_t local = kMax ? max(before, excl_in_warp) : before + excl_in_warp;
-    if (threadIdx.x == 0) {
-        uint32_t prefix = 0;
-        uint32_t* state = states + tile;
-        if (tile == 0) {
-            st_relaxed(state, kTileFlagPrefix | (tile_agg & kTileValueMask));
-        } else {
-            st_relaxed(state, kTileFlagAggregate | (tile_agg & kTileValueMask));
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t s = ld_relaxed(states + j);
-                if ((s & ~kTileValueMask) == 0) {
-                    if (!spin_wait(spins)) {
-                        atomicOr(status, kStatusLookbackTimeout);
-                        break;
-                    }
-                    continue;
-                }
-                prefix = kMax ? max(prefix, s & kTileValueMask) : prefix + (s & kTileValueMask);
-                if (s & kTileFlagPrefix) break;
-                --j;
-            }
-            const uint32_t incl = kMax ? max(prefix, tile_agg) : prefix + tile_agg;
-            st_relaxed(state, kTileFlagPrefix | (incl & kTileValueMask));
+    if (threadIdx.x < 32) {
+        const uint32_t prefix = warp_lookback<kMax>(states, tile, tile_agg, status);
+        if (threadIdx.x == 0) {
+            s_prefix = prefix;
+            if (!kMax && tile == gridDim.x - 1 && total) *total = prefix + tile_agg;
         }
-        s_prefix = prefix;
-        if (!kMax && tile == gridDim.x - 1 && total) *total = prefix + tile_agg;
     }
     __syncthreads();
     uint32_t run = kMax ? max(s_prefix, local) : s_prefix + local;
