@@ -111,6 +111,46 @@ __device__ __forceinline__ void warp_rank(const uint32_t (&key)[KPT], uint32_t w
 //   3. decoupled look-back per digit (one thread per digit, bounded spin);
 //   4. values (and, on the gathering pass, the 48-byte rows) are staged by the same positions and
 //      the tile is written out in runs per digit.
+// The exclusive prefix of digit d over the tiles before `tile` (decoupled look-back): the states of
+// kLookbackWindow predecessors are read at once, so a long walk over tiles that have published
+// only their aggregates costs one round trip per window; the walk resumes at the first tile of a
+// window that has published nothing yet (a bounded wait, after which kStatusLookbackTimeout is set).
+constexpr int kLookbackWindow = 8;
+
+__device__ __forceinline__ uint32_t digit_lookback(const SortPass& a, uint32_t tile, uint32_t d)
+{
+    uint32_t exclusive = 0;
+    int64_t j = (int64_t)tile - 1;
+    uint32_t spins = 0;
+    while (j >= 0) {
+        uint32_t st[kLookbackWindow];
+#pragma unroll
+        for (int w = 0; w < kLookbackWindow; ++w)
+            st[w] = j - w >= 0 ? ld_relaxed(a.tile_states + (uint64_t)(j - w) * kRadix + d) : kTileFlagPrefix;
+        bool done = false, stalled = false;
+        int used = 0;
+#pragma unroll
+        for (int w = 0; w < kLookbackWindow; ++w) {
+            if (!done && !stalled) {
+                if ((st[w] & ~kTileValueMask) == 0) {
+                    stalled = true;
+                } else {
+                    exclusive += st[w] & kTileValueMask;
+                    used = w + 1;
+                    done = (st[w] & kTileFlagPrefix) != 0;
+                }
+            }
+        }
+        if (done) break;
+        j -= used;
+        if (stalled && !spin_wait(spins, a.spin_limit)) {
+            atomicOr(a.status, kStatusLookbackTimeout);
+            break;
+        }
+    }
+    return exclusive;
+}
+
 template <int KPT>
 __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const SortPass a)
 {
@@ -176,21 +216,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
     // Phase 3: the exclusive prefix of digit d over the earlier tiles.
     uint32_t exclusive = 0;
     if (tile != 0) {
-        int64_t j = (int64_t)tile - 1;
-        uint32_t spins = 0;
-        while (j >= 0) {
-            const uint32_t s = ld_relaxed(a.tile_states + (uint64_t)j * kRadix + d);
-            if ((s & ~kTileValueMask) == 0) {
-                if (!spin_wait(spins, a.spin_limit)) {
-                    atomicOr(a.status, kStatusLookbackTimeout);
-                    break;
-                }
-                continue;
-            }
-            exclusive += s & kTileValueMask;
-            if (s & kTileFlagPrefix) break;
-            --j;
-        }
+        exclusive = digit_lookback(a, tile, d);
         if (publish) st_relaxed(state, kTileFlagPrefix | (exclusive + total));
     }
     uint32_t digit_total;
@@ -391,21 +417,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_pipe_kernel(const So
         }
         uint32_t exclusive = 0;
         if (tile != 0) {
-            int64_t j = (int64_t)tile - 1;
-            uint32_t spins = 0;
-            while (j >= 0) {
-                const uint32_t s = ld_relaxed(a.tile_states + (uint64_t)j * kRadix + d);
-                if ((s & ~kTileValueMask) == 0) {
-                    if (!spin_wait(spins, a.spin_limit)) {
-                        atomicOr(a.status, kStatusLookbackTimeout);
-                        break;
-                    }
-                    continue;
-                }
-                exclusive += s & kTileValueMask;
-                if (s & kTileFlagPrefix) break;
-                --j;
-            }
+            exclusive = digit_lookback(a, tile, d);
             if (publish) st_relaxed(state, kTileFlagPrefix | (exclusive + total));
         }
         S.dest[d] = S.base[d] + exclusive - local;

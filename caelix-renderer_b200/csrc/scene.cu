@@ -473,22 +473,36 @@ struct LightArgs
     const uint32_t* light_codes;
 };
 
-// Warp per brick: a brick with power above 0 and a voxel whose code is a light code is a light brick.
+// A brick with power above 0 and a voxel whose code is a light code is a light brick. A warp takes
+// 32 consecutive bricks: each lane reads one brick's power, then the warp reads the values of each
+// brick with power (two 16-byte words per lane) and appends the light bricks with one atomic.
 template <uint32_t kEnc>
 __global__ void light_collect_kernel(const LightArgs a, uint32_t* counter, uint32_t* lkeys, uint32_t* lbricks)
 {
-    const uint32_t i = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint32_t first = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32u;
     const uint32_t lane = threadIdx.x & 31u;
-    if (i >= a.n || !(a.power[i] > 0.0f)) return;
-    const uint4* vox = reinterpret_cast<const uint4*>(a.voxels + 512ull * i);
-    const uint32_t bits = light_byte<kEnc>(__ldg(vox + lane), a.light_codes) |
-                          light_byte<kEnc>(__ldg(vox + 32 + lane), a.light_codes);
-    if (!__any_sync(0xFFFFFFFFu, bits != 0u) || lane != 0) return;
+    if (first >= a.n) return;
+    const uint32_t i = first + lane;
+    uint32_t todo = __ballot_sync(0xFFFFFFFFu, i < a.n && a.power[i] > 0.0f);
+    uint32_t found = 0;
+    while (todo) {
+        const uint32_t l = (uint32_t)(__ffs(todo) - 1);
+        todo &= todo - 1u;
+        const uint4* vox = reinterpret_cast<const uint4*>(a.voxels + 512ull * (first + l));
+        const uint32_t bits = light_byte<kEnc>(__ldg(vox + lane), a.light_codes) |
+                              light_byte<kEnc>(__ldg(vox + 32 + lane), a.light_codes);
+        if (__any_sync(0xFFFFFFFFu, bits != 0u)) found |= 1u << l;
+    }
+    if (!found) return;
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, (uint32_t)__popc(found));
+    base = __shfl_sync(0xFFFFFFFFu, base, 0);
+    if (!((found >> lane) & 1u)) return;
     const uint32_t gs = a.group_shift, gm = (1u << gs) - 1u;
     const int32_t kx = a.keys[3 * i], ky = a.keys[3 * i + 1], kz = a.keys[3 * i + 2];
     const uint32_t bx = (uint32_t)(kx - a.origin[0]), by = (uint32_t)(ky - a.origin[1]), bz = (uint32_t)(kz - a.origin[2]);
     const uint32_t g = (bx >> gs) + a.groups[0] * ((by >> gs) + a.groups[1] * (bz >> gs));
-    const uint32_t slot = atomicAdd(counter, 1u);
+    const uint32_t slot = base + (uint32_t)__popc(found & lanemask_lt());
     lkeys[slot] = (g << (3 * gs)) | morton30(bx & gm, by & gm, bz & gm);
     lbricks[slot] = i;
 }
@@ -574,7 +588,7 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_measure_kernel(const L
 // Per light: its block's extra units (header + index entries) when it starts its group.
 __global__ void light_group_kernel(const uint32_t* __restrict__ lkeys, uint32_t m, uint32_t gshift,
                                    const uint32_t* __restrict__ units, uint32_t* __restrict__ total_units,
-                                   uint32_t* __restrict__ group_start)
+                                   uint32_t* __restrict__ group_start, uint32_t* __restrict__ group_end)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= m) return;
@@ -597,6 +611,7 @@ __global__ void light_group_kernel(const uint32_t* __restrict__ lkeys, uint32_t 
             else b = mid;
         }
         extra = 1 + (a - k);
+        group_end[k] = a;  // the end of the group's lights, for the group's first light
     }
     total_units[k] = units[k] + extra;
 }
@@ -611,6 +626,7 @@ struct LightWriteArgs
     const uint32_t* units;
     const uint32_t* offsets;  // exclusive scan of the total units
     const uint32_t* group_start;
+    const uint32_t* group_end;  // at a group's first light: the end of its lights
     uint32_t total;  // all units
     uint32_t* heap;
     uint32_t* group_rows;
@@ -636,16 +652,7 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
     const uint32_t s = w.group_start[k];
     // The group's light count: the next group's start, or the end.
     const uint32_t block = 1 + w.offsets[s];
-    uint32_t count;
-    {
-        uint32_t lo = s, hi = w.m;
-        while (lo < hi) {
-            const uint32_t mid = (lo + hi) >> 1;
-            if ((w.lkeys[mid] >> (3 * gs)) <= g) lo = mid + 1;
-            else hi = mid;
-        }
-        count = lo - s;
-    }
+    const uint32_t count = w.group_end[s] - s;
     const uint32_t rec_unit = 1 + w.offsets[k] + (k == s ? 1 + count : 0);
     uint32_t* rec = w.heap + 4ull * rec_unit;
     BrickLightRecord h;
@@ -1118,10 +1125,10 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     if (n > 0 && s.lights) {
         if (packed)
             light_collect_kernel<kEncodingPacked>
-                <<<blocks_for(32ull * n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+                <<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
         else
             light_collect_kernel<kEncodingBlockId>
-                <<<blocks_for(32ull * n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
+                <<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
     }
     uint32_t m = 0;
     CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
@@ -1162,8 +1169,9 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         else
             light_measure_kernel<kEncodingBlockId><<<blocks_for(32ull * m, kLightWarps * 32), kLightWarps * 32, 0, stream>>>(
                 la, lbricks, m, counts6, units, reuse);
+        uint32_t* group_end = lkeys_alt;  // free once the light sort is done
         light_group_kernel<<<blocks_for(m, kThreads), kThreads, 0, stream>>>(lkeys, m, group_shift, units, totals,
-                                                                             group_start);
+                                                                             group_start, group_end);
         uint32_t* d_total = s.status + 6;
         CX_TRY(run_scan(false, totals, offsets, m, small, d_total, s.status, stream));
         CX_TRY(cudaMemcpyAsync(&total_units, d_total, 4, cudaMemcpyDeviceToHost, stream));
@@ -1172,7 +1180,7 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         CX_TRY(alloc(s.heap, s.capacity.heap, s.heap_words));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
         LightWriteArgs wa{la,           lkeys,         lbricks,         m,           counts6,
-                          units,        offsets,       group_start,     total_units, s.heap,
+                          units,        offsets,       group_start,     group_end,   total_units, s.heap,
                           s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick,
                           reuse,        s.unit_of_brick};
         if (packed)
