@@ -559,9 +559,11 @@ void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t 
 
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
-                   const SortGather* gather, uint32_t keys_per_thread, const SortWaitTest* wait_test)
+                   const SortGather* gather, uint32_t keys_per_thread, const SortWaitTest* wait_test,
+                   uint32_t key_bits)
 {
     if (n == 0) return;
+    const uint32_t passes = key_bits >= 32 ? 4u : std::max(1u, (key_bits + 7u) / 8u);
     if (n <= kSmallSortKeys) {
         const SortGather g = gather ? *gather : SortGather{nullptr, 0, nullptr, nullptr};
         if (identity_values) small_sort_kernel<true><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
@@ -594,7 +596,7 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
     uint32_t* vin = values_a;
     uint32_t* kout = keys_b;
     uint32_t* vout = values_b;
-    for (uint32_t pass = 0; pass < 4; ++pass) {
+    for (uint32_t pass = 0; pass < passes; ++pass) {
         SortPass p;
         p.keys_in = kin;
         p.values_in = (pass == 0 && identity_values) ? nullptr : vin;
@@ -606,7 +608,7 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         p.tile_counter = counters + pass;
         p.tile_states = states + (uint64_t)pass * tiles * kRadix;
         p.status = status;
-        const bool last = pass == 3;
+        const bool last = pass + 1 == passes;
         p.rows_in = (last && gather) ? gather->rows_in : nullptr;
         p.rows_in_stride = gather ? gather->rows_in_stride : 0;
         p.rows_out = (last && gather) ? gather->rows_out : nullptr;
@@ -623,6 +625,10 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
         t = vin;
         vin = vout;
         vout = t;
+    }
+    if (passes & 1u) {  // the result is in keys_b / values_b
+        cudaMemcpyAsync(keys_a, keys_b, 4ull * n, cudaMemcpyDeviceToDevice, stream);
+        cudaMemcpyAsync(values_a, values_b, 4ull * n, cudaMemcpyDeviceToDevice, stream);
     }
 }
 

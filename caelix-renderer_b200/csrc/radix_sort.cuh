@@ -91,9 +91,19 @@ struct SortWaitTest
 // `keys_per_thread` (4, 8 or 16) sets the tile (256 * keys_per_thread keys); `scratch` then holds
 // sort_scratch_words(n, keys_per_thread) words. Up to kSmallSortKeys pairs one CTA does all four
 // passes in shared memory (one launch; the same permutation; scratch and histograms unused).
+// `key_bits`: every key is below 2^key_bits, so only the passes of its low ceil(key_bits / 8) digits
+// run (an odd count of passes ends with a copy of the result back into keys_a / values_a).
 void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint32_t* values_b, uint32_t n,
                    bool identity_values, uint32_t* scratch, uint32_t* status, cudaStream_t stream,
                    const SortGather* gather = nullptr, uint32_t keys_per_thread = kSortKeysPerThread,
-                   const SortWaitTest* wait_test = nullptr);
+                   const SortWaitTest* wait_test = nullptr, uint32_t key_bits = 32);
+
+// The number of bits of the values below `bound` (0 for bound <= 1).
+inline uint32_t bits_below(uint64_t bound)
+{
+    uint32_t b = 0;
+    while (b < 64 && (1ull << b) < bound) ++b;
+    return b;
+}
 
 }  // namespace cx

@@ -1041,7 +1041,8 @@ cudaError_t scene_build_device(DeviceScene& s, const int32_t origin[3], const ui
         hash_home_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, s.hash_capacity, lo, hi, home);
         CX_TRY(cudaMemsetAsync(sortw, 0, sort_words * 4, stream));
         radix_histogram(home, n, sortw, std::min<uint32_t>(blocks_for(n, 2048), current_sm_count() * 4), stream);
-        onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream);
+        onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream, nullptr, kSortKeysPerThread,
+                      nullptr, bits_below(s.hash_capacity));
         hash_shift_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(home, n, tmp);
         CX_TRY(run_scan(true, tmp, tmp2, n, small, nullptr, s.status, stream));
         hash_place_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(tmp2, home, order, lo, hi, n, s.hash_slots,
@@ -1158,7 +1159,9 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     if (m > 0) {
         CX_TRY(cudaMemsetAsync(sortw, 0, sort_scratch_words(m) * 4, stream));
         radix_histogram(lkeys, m, sortw, std::min<uint32_t>(blocks_for(m, 2048), current_sm_count() * 4), stream);
-        onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream);
+        // Keys: the group index above 3 * group_shift bits of position in the group.
+        onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream, nullptr,
+                      kSortKeysPerThread, nullptr, 3 * group_shift + bits_below(s.group_count));
         uint32_t* units = home;    // m words
         uint32_t* totals = order;  // m words
         uint32_t* group_start = tmp;

@@ -143,7 +143,8 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
     CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n), stream));
     radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, current_sm_count() * 4), stream);
     // A stable sort of the linear indices (unique: one slot per key), values = the slots.
-    onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream);
+    onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream, nullptr, kSortKeysPerThread, nullptr,
+                  bits_below((uint64_t)grid[0] * grid[1] * grid[2]));
     staging_gather_kernel<<<blocks(64ull * n), kStageThreads, 0, stream>>>(
         order, n, stage_keys, reinterpret_cast<const uint4*>(stage_voxels), slot_power, keys,
         reinterpret_cast<uint4*>(voxels), power, record_of_slot);
