@@ -1,5 +1,5 @@
 // The decoupled look-back of the single-pass scans, by one warp: the 32 lanes read the states of
-// 32 predecessor tiles at once, so a tile waits one round trip per 32 predecessors instead of one
+// 128 predecessor tiles at once, so a tile waits one round trip per 128 predecessors instead of one
 // per predecessor.
 #pragma once
 #include <cstdint>
@@ -18,6 +18,7 @@ namespace cx {
 template <bool kMax>
 __device__ __forceinline__ uint32_t warp_lookback(uint32_t* states, uint32_t tile, uint32_t agg, uint32_t* status)
 {
+    constexpr int kPerLane = 4;  // a window of 128 predecessors: lane l reads tiles j - l - 32 q
     const uint32_t lane = threadIdx.x & 31u;
     uint32_t* state = states + tile;
     if (tile == 0) {
@@ -26,28 +27,51 @@ __device__ __forceinline__ uint32_t warp_lookback(uint32_t* states, uint32_t til
     }
     if (lane == 0) st_relaxed(state, kTileFlagAggregate | (agg & kTileValueMask));
     uint32_t prefix = 0;
-    int64_t j = (int64_t)tile - 1;  // the nearest tile of the window (lane 0's)
+    int64_t j = (int64_t)tile - 1;  // the nearest tile of the window
     uint32_t spins = 0;
     while (j >= 0) {
-        const int64_t t = j - (int64_t)lane;
-        // Before tile 0: an inclusive prefix of 0.
-        const uint32_t s = t >= 0 ? ld_relaxed(states + t) : kTileFlagPrefix;
-        const uint32_t ready = __ballot_sync(0xFFFFFFFFu, (s & ~kTileValueMask) != 0u);
-        const uint32_t found = __ballot_sync(0xFFFFFFFFu, (s & kTileFlagPrefix) != 0u);
-        const uint32_t stop = found ? (uint32_t)(__ffs(found) - 1) : 31u;
-        const uint32_t need = (2u << stop) - 1u;  // lanes 0 .. stop (all 32 when stop is 31)
-        if ((ready & need) != need) {
+        uint32_t s[kPerLane];
+#pragma unroll
+        for (int q = 0; q < kPerLane; ++q) {
+            const int64_t t = j - (int64_t)lane - 32 * q;
+            s[q] = t >= 0 ? ld_relaxed(states + t) : kTileFlagPrefix;  // before tile 0: a prefix of 0
+        }
+        // The nearest tile with an inclusive prefix (offset `stop` from j), and whether every tile
+        // nearer than it (and it) has published.
+        uint32_t stop = 32u * kPerLane - 1u;
+        bool found = false, ready = true;
+#pragma unroll
+        for (int q = 0; q < kPerLane; ++q) {
+            if (!found) {
+                const uint32_t f = __ballot_sync(0xFFFFFFFFu, (s[q] & kTileFlagPrefix) != 0u);
+                const uint32_t r = __ballot_sync(0xFFFFFFFFu, (s[q] & ~kTileValueMask) != 0u);
+                const uint32_t last = f ? (uint32_t)(__ffs(f) - 1) : 31u;
+                const uint32_t need = (2u << last) - 1u;  // lanes 0 .. last
+                ready = ready && (r & need) == need;
+                if (f) {
+                    found = true;
+                    stop = 32u * q + last;
+                }
+            }
+        }
+        if (!ready) {
             if (!spin_wait(spins)) {
                 if (lane == 0) atomicOr(status, kStatusLookbackTimeout);
                 break;
             }
             continue;
         }
-        const uint32_t v = lane <= stop ? (s & kTileValueMask) : 0u;
+        uint32_t v = 0;
+#pragma unroll
+        for (int q = 0; q < kPerLane; ++q) {
+            const uint32_t off = 32u * q + lane;
+            const uint32_t x = off <= stop ? (s[q] & kTileValueMask) : 0u;
+            v = kMax ? max(v, x) : v + x;
+        }
         const uint32_t w = kMax ? __reduce_max_sync(0xFFFFFFFFu, v) : __reduce_add_sync(0xFFFFFFFFu, v);
         prefix = kMax ? max(prefix, w) : prefix + w;
         if (found) break;
-        j -= 32;
+        j -= 32 * kPerLane;
     }
     const uint32_t incl = kMax ? max(prefix, agg) : prefix + agg;
     if (lane == 0) st_relaxed(state, kTileFlagPrefix | (incl & kTileValueMask));

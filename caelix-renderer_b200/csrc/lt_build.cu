@@ -277,6 +277,25 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
+// The leaf summaries in sorted order: sorted[j] = the first 48 bytes of leaves[values[j]], and
+// inverse[values[j]] = j.
+__global__ void __launch_bounds__(kThreads)
+    lt_gather_kernel(uint32_t n, const uint32_t* __restrict__ values, const LightBvhLeaf* __restrict__ leaves,
+                     LightSummary* __restrict__ sorted, uint32_t* __restrict__ inverse)
+{
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= n) return;
+    const uint32_t v = __ldg(values + j);
+    const uint4* src = reinterpret_cast<const uint4*>(leaves + v);
+    const uint4 r0 = __ldg(src), r1 = __ldg(src + 1), r2 = __ldg(src + 2);
+    uint4* dst = reinterpret_cast<uint4*>(sorted) + 3ull * j;
+    dst[0] = r0;
+    dst[1] = r1;
+    dst[2] = r2;
+    inverse[v] = j;
+}
+
+// ---------------------------------------------------------------------------------------------
 // Karras 2012 binary radix tree over the sorted keys; ties broken by sorted position. Also the
 // range-count differences: node i covers the leaf boundaries [a, b) of its range [a, b], so
 // cover[a] += 1, cover[b] -= 1 (their prefix sum counts the nodes over every boundary).
@@ -773,13 +792,23 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
             b.leaves, n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
         mark(2);
-        SortGather gather;
-        gather.rows_in = reinterpret_cast<const uint4*>(b.leaves);
-        gather.rows_in_stride = sizeof(LightBvhLeaf) / sizeof(uint4);
-        gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
-        gather.inverse = b.inverse;
-        onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
-                      stream, &gather, kpt);
+        if (n <= kSmallSortKeys) {
+            // One CTA sorts and gathers (small_sort_kernel).
+            SortGather gather;
+            gather.rows_in = reinterpret_cast<const uint4*>(b.leaves);
+            gather.rows_in_stride = sizeof(LightBvhLeaf) / sizeof(uint4);
+            gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
+            gather.inverse = b.inverse;
+            onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
+                          stream, &gather, kpt);
+        } else {
+            // The sort, then the summaries gathered in sorted order by a kernel of its own (full
+            // occupancy keeps many of the random row reads in flight).
+            onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
+                          stream, nullptr, kpt);
+            lt_gather_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.values, b.leaves,
+                                                                                        b.sorted, b.inverse);
+        }
         mark(3);
     } else {
         mark(1);
@@ -819,9 +848,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
 
 uint32_t lt_kernel_launches(uint32_t n)
 {
+    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the six tree
+    // kernels from two leaves, finish.
     if (n == 0) return 1;
-    if (n == 1) return 7;
-    return 13;
+    const uint32_t sort = n <= kSmallSortKeys ? 1u : 5u;
+    return 2 + sort + (n >= 2 ? 6u : 0u) + 1;
 }
 
 }  // namespace cx

@@ -422,47 +422,22 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_pipe_kernel(const So
         }
         S.dest[d] = S.base[d] + exclusive - local;
         __syncthreads();
-        if (a.rows_in) {
-            // The row gather of the last pass: the rows of kGatherBatch outputs are loaded before
-            // any of them is stored, so a thread keeps that many random row reads in flight.
-            constexpr uint32_t kGatherBatch = 3;
-            for (uint32_t j0 = tid; j0 < count; j0 += kGatherBatch * kSortThreads) {
-                uint4 row[kGatherBatch][3];
-                uint32_t kk[kGatherBatch], vv[kGatherBatch], dd[kGatherBatch];
-#pragma unroll
-                for (uint32_t q = 0; q < kGatherBatch; ++q) {
-                    const uint32_t j = j0 + q * kSortThreads;
-                    if (j < count) {
-                        kk[q] = S.keys[j];
-                        vv[q] = S.values[j];
-                        dd[q] = S.dest[(kk[q] >> a.shift) & 255u] + j;
-                        const uint4* src = a.rows_in + (uint64_t)a.rows_in_stride * vv[q];
-                        row[q][0] = __ldg(src);
-                        row[q][1] = __ldg(src + 1);
-                        row[q][2] = __ldg(src + 2);
-                    }
-                }
-#pragma unroll
-                for (uint32_t q = 0; q < kGatherBatch; ++q) {
-                    const uint32_t j = j0 + q * kSortThreads;
-                    if (j < count) {
-                        a.keys_out[dd[q]] = kk[q];
-                        a.values_out[dd[q]] = vv[q];
-                        uint4* dst = a.rows_out + 3ull * dd[q];
-                        dst[0] = row[q][0];
-                        dst[1] = row[q][1];
-                        dst[2] = row[q][2];
-                        a.inverse[vv[q]] = dd[q];
-                    }
-                }
-            }
-        } else {
-            for (uint32_t j = tid; j < count; j += kSortThreads) {
-                const uint32_t k = S.keys[j];
-                const uint32_t v = S.values[j];
-                const uint32_t dest = S.dest[(k >> a.shift) & 255u] + j;
-                a.keys_out[dest] = k;
-                a.values_out[dest] = v;
+        for (uint32_t j = tid; j < count; j += kSortThreads) {
+            const uint32_t k = S.keys[j];
+            const uint32_t v = S.values[j];
+            const uint32_t dest = S.dest[(k >> a.shift) & 255u] + j;
+            a.keys_out[dest] = k;
+            a.values_out[dest] = v;
+            if (a.rows_in) {
+                const uint4* src = a.rows_in + (uint64_t)a.rows_in_stride * v;
+                uint4* dst = a.rows_out + 3ull * dest;
+                const uint4 r0 = __ldg(src);
+                const uint4 r1 = __ldg(src + 1);
+                const uint4 r2 = __ldg(src + 2);
+                dst[0] = r0;
+                dst[1] = r1;
+                dst[2] = r2;
+                a.inverse[v] = dest;
             }
         }
         __syncthreads();

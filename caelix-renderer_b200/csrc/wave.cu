@@ -31,6 +31,19 @@ constexpr uint32_t kFlagSegLight = 1u << 8;   // segment_light = 3
 constexpr uint32_t kFlagShadow = 1u << 9;     // a shadow ray of the last vertex was queued
 constexpr uint32_t kFlagExt = 1u << 10;       // an extension ray was queued
 constexpr uint32_t kFlagPrimary = 1u << 11;   // that extension ray is the camera ray
+// Words of WaveBuffers::counts: 0..3 the queue lengths of the two parities (rays, paths), then
+// the trace and shade launches' fetch counters of the two parities.
+constexpr uint32_t kFetchTrace = 4, kFetchShade = 6;
+
+// The next 32-item chunk of a queue for the calling warp, from a fetch counter. A warp that is done
+// with its chunk takes the next one, so the work of a launch whose items' costs differ widely
+// spreads over the warps until its end. Every lane calls.
+__device__ __forceinline__ uint32_t fetch_chunk(uint32_t* counter)
+{
+    uint32_t base = 0;
+    if ((threadIdx.x & 31u) == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xFFFFFFFFu, base, 0);
+}
 
 struct WaveGen
 {
@@ -111,8 +124,11 @@ __global__ void __launch_bounds__(kWaveThreads)
 }
 
 // kEntities: the views' scenes have entities (traversed after the world's bricks); the variant
-// without them keeps the world-only DDA's registers (no out-of-line call).
-template <bool kEntities>
+// without them keeps the world-only DDA's registers (no out-of-line call). kDynamic: warps take
+// chunks of the queue from a fetch counter (fetch_chunk) instead of a fixed grid stride: faster
+// where ray costs spread widely (entities, scenes whose records do not stay in L2), slower on the
+// small resident scene, where the fixed stride is kept.
+template <bool kEntities, bool kDynamic>
 __global__ void __launch_bounds__(kWaveThreads)
     wave_trace_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
 {
@@ -120,10 +136,13 @@ __global__ void __launch_bounds__(kWaveThreads)
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         b.counts[2 * (parity ^ 1u)] = 0;
         b.counts[2 * (parity ^ 1u) + 1] = 0;
+        b.counts[kFetchTrace + (parity ^ 1u)] = 0;  // the next trace launch's fetch counter
     }
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * kWaveThreads;
-    for (uint32_t base = blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n; base += stride) {
+    uint32_t* const fetch = &b.counts[kFetchTrace + parity];
+    for (uint32_t base = kDynamic ? fetch_chunk(fetch) : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
+         base = kDynamic ? fetch_chunk(fetch) : base + stride) {
         const uint32_t i = base + lane;
         uint32_t key = 0xFFFFFFFFu;
         if (i < n) {
@@ -212,7 +231,13 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     const uint32_t out = parity ^ 1u;
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * kWaveThreads;
-    for (uint32_t base = blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n; base += stride) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) b.counts[kFetchShade + out] = 0;  // the next shade launch's
+    // Chunks from a fetch counter (as in wave_trace_kernel) for scenes with entities or records that
+    // do not stay in L2 (the 8-CTA variants); the fixed stride for the resident scene.
+    constexpr bool kDynamic = kEntities || kMinBlocks == 8;
+    uint32_t* const fetch = &b.counts[kFetchShade + parity];
+    for (uint32_t base = kDynamic ? fetch_chunk(fetch) : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
+         base = kDynamic ? fetch_chunk(fetch) : base + stride) {
         const uint32_t i = base + lane;
         uint32_t slot = 0, next_flags = 0;
         bool live = false, shadow = false, ext = false;
@@ -577,8 +602,10 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
     if (b.capacity == 0) return cudaErrorInvalidValue;
     static int trace_blocks[2] = {0, 0}, shade_blocks[2] = {0, 0};
     if (trace_blocks[0] == 0) {
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[0], wave_trace_kernel<false>, kWaveThreads, 0));
-        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[1], wave_trace_kernel<true>, kWaveThreads, 0));
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[0], wave_trace_kernel<false, kMinBlocks == 8>,
+                                                             kWaveThreads, 0));
+        CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&trace_blocks[1], wave_trace_kernel<true, true>, kWaveThreads,
+                                                             0));
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks[0], wave_shade_kernel<kMode, kMinBlocks, false>,
                                                              kWaveThreads, 0));
         CX_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&shade_blocks[1], wave_shade_kernel<kMode, kMinBlocks, true>,
@@ -599,7 +626,7 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
             g.first_item = first;
             g.count = n;
             g.block_width = block_width;
-            CX_TRY(cudaMemsetAsync(b.counts, 0, 16, stream));
+            CX_TRY(cudaMemsetAsync(b.counts, 0, 32, stream));
             wave_generate_kernel<<<(n + kWaveThreads - 1) / kWaveThreads, kWaveThreads, 0, stream>>>(d_views, g, b);
             ++count;
             const uint32_t ray_grid = std::min<uint32_t>((2 * n + kWaveThreads - 1) / kWaveThreads,
@@ -608,8 +635,8 @@ cudaError_t wave_run(const WaveView* d_views, const WavePlan& plan, const uint32
                                                            sm_count * (uint32_t)shade_blocks[entities ? 1 : 0]);
             for (uint32_t it = 0; it <= plan.bounces[s]; ++it) {
                 const uint32_t parity = it & 1u;
-                if (entities) wave_trace_kernel<true><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
-                else wave_trace_kernel<false><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                if (entities) wave_trace_kernel<true, true><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
+                else wave_trace_kernel<false, kMinBlocks == 8><<<ray_grid, kWaveThreads, 0, stream>>>(d_views, b, parity);
                 if (entities)
                     wave_shade_kernel<kMode, kMinBlocks, true><<<shade_grid, kWaveThreads, 0, stream>>>(d_views, b, parity, adj);
                 else
