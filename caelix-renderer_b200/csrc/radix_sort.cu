@@ -445,17 +445,17 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_pipe_kernel(const So
     }
 }
 
-// A whole sort of n <= kSmallSortKeys pairs by one CTA: the four passes of the onesweep ranking
-// over one tile held in shared memory (a stable LSD sort: the same permutation as the onesweep
-// passes), then the output with the optional row gather of the last pass. One launch instead of
-// four for the small sorts of small light trees.
+// A whole sort of n <= kSmallSortKeys pairs by one CTA: the passes of the onesweep ranking that the
+// keys' digits need, over one tile held in shared memory (a stable LSD sort: the same permutation
+// as the onesweep passes), then the output with the optional row gather of the last pass. One
+// launch instead of four for the small sorts of small light trees.
 constexpr int kSmallSortKeysPerThread = 16;
 static_assert(kSmallSortKeys == kSortThreads * kSmallSortKeysPerThread, "one tile");
 
 template <bool kIdentity>
 __global__ void __launch_bounds__(kSortThreads) small_sort_kernel(uint32_t* __restrict__ keys,
                                                                   uint32_t* __restrict__ values, uint32_t n,
-                                                                  const SortGather gather)
+                                                                  uint32_t passes, const SortGather gather)
 {
     constexpr int KPT = kSmallSortKeysPerThread;
     __shared__ uint32_t s_warp_counts[kSortWarps][kRadix];
@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kSortThreads) small_sort_kernel(uint32_t* __re
         s_values[i] = kIdentity ? i : values[i];
     }
     const uint32_t warp_base = warp * 32u * KPT;
-    for (uint32_t pass = 0; pass < 4; ++pass) {
+    for (uint32_t pass = 0; pass < passes; ++pass) {
         const uint32_t shift = 8 * pass;
 #pragma unroll
         for (int w = 0; w < kSortWarps; ++w) s_warp_counts[w][tid] = 0;
@@ -524,6 +524,45 @@ __global__ void __launch_bounds__(kSortThreads) small_sort_kernel(uint32_t* __re
     }
 }
 
+// A whole sort of n <= kRankSortKeys pairs by one CTA without passes: each element's place is the
+// count of smaller keys plus the count of equal keys before it (the stable order), counted over the
+// keys in shared memory; the optional row gather as in small_sort_kernel.
+constexpr uint32_t kRankSortKeys = 512;
+
+template <bool kIdentity>
+__global__ void __launch_bounds__(kSortThreads) rank_sort_kernel(uint32_t* __restrict__ keys,
+                                                                 uint32_t* __restrict__ values, uint32_t n,
+                                                                 const SortGather gather)
+{
+    __shared__ uint32_t s_keys[kRankSortKeys];
+    __shared__ uint32_t s_values[kRankSortKeys];
+    const uint32_t tid = threadIdx.x;
+    for (uint32_t i = tid; i < n; i += kSortThreads) {
+        s_keys[i] = keys[i];
+        s_values[i] = kIdentity ? i : values[i];
+    }
+    __syncthreads();
+    for (uint32_t i = tid; i < n; i += kSortThreads) {
+        const uint32_t k = s_keys[i];
+        uint32_t r = 0;
+        for (uint32_t j = 0; j < n; ++j) {
+            const uint32_t kj = s_keys[j];
+            r += (kj < k || (kj == k && j < i)) ? 1u : 0u;
+        }
+        const uint32_t v = s_values[i];
+        keys[r] = k;
+        values[r] = v;
+        if (gather.rows_in) {
+            const uint4* src = gather.rows_in + (uint64_t)gather.rows_in_stride * v;
+            uint4* dst = gather.rows_out + 3ull * r;
+            dst[0] = __ldg(src);
+            dst[1] = __ldg(src + 1);
+            dst[2] = __ldg(src + 2);
+            gather.inverse[v] = r;
+        }
+    }
+}
+
 }  // namespace
 
 void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream)
@@ -541,8 +580,14 @@ void onesweep_sort(uint32_t* keys_a, uint32_t* values_a, uint32_t* keys_b, uint3
     const uint32_t passes = key_bits >= 32 ? 4u : std::max(1u, (key_bits + 7u) / 8u);
     if (n <= kSmallSortKeys) {
         const SortGather g = gather ? *gather : SortGather{nullptr, 0, nullptr, nullptr};
-        if (identity_values) small_sort_kernel<true><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
-        else small_sort_kernel<false><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
+        if (n <= kRankSortKeys) {
+            if (identity_values) rank_sort_kernel<true><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
+            else rank_sort_kernel<false><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, g);
+        } else if (identity_values) {
+            small_sort_kernel<true><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, passes, g);
+        } else {
+            small_sort_kernel<false><<<1, kSortThreads, 0, stream>>>(keys_a, values_a, n, passes, g);
+        }
         return;
     }
     if (!sort_keys_per_thread_ok(keys_per_thread)) keys_per_thread = kSortKeysPerThread;

@@ -17,7 +17,7 @@ __device__ __noinline__ void next_event(const SceneView& s, const float x[3], co
     ShadowRay r;
     if (!nee_prepare(s, x, n, light_rng, r)) return;
     ++rays.shadow;
-    const Hit h = trace_scene(s, x, r.dir, 0.0f, r.t_max);
+    const Hit h = trace_scene(s, x, r.dir, 0.0f, r.t_max, true);  // occlusion only
     if (!h.hit) {
         out[0] = r.value[0];
         out[1] = r.value[1];

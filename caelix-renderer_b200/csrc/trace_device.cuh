@@ -373,7 +373,7 @@ constexpr uint32_t kEntityCandidates = 16;
 constexpr uint32_t kEntityStack = 32;
 
 __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
-                                            float tmax_ray, Hit& h)
+                                            float tmax_ray, Hit& h, bool any = false)
 {
     if (s.entity_nodes) {
         float inv[3];
@@ -420,11 +420,11 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
                 for (; y > 0 && cand[y - 1] > v; --y) cand[y] = cand[y - 1];
                 cand[y] = v;
             }
-            for (uint32_t x = 0; x < n; ++x) entity_candidate(s, cand[x], o, d, tmin_ray, tmax_ray, h);
+            for (uint32_t x = 0; x < n && !(any && h.hit); ++x) entity_candidate(s, cand[x], o, d, tmin_ray, tmax_ray, h);
             return;
         }
     }
-    for (uint32_t e = 0; e < s.entity_count; ++e) entity_candidate(s, e, o, d, tmin_ray, tmax_ray, h);
+    for (uint32_t e = 0; e < s.entity_count && !(any && h.hit); ++e) entity_candidate(s, e, o, d, tmin_ray, tmax_ray, h);
 }
 
 // The entity-local hit point of an entity hit (the wavefront keeps a hit as four words): the ray
@@ -459,19 +459,22 @@ __device__ __forceinline__ void entity_normal(const SceneView& s, uint32_t entit
     for (int i = 0; i < 3; ++i) n[i] = v[i] * inv;
 }
 
-// Closest hit over the world's bricks and the entities'.
+// Closest hit over the world's bricks and the entities'. `any`: an occlusion test (only h.hit is
+// meaningful): a ray that the world occludes skips the entities, and the entities stop at the
+// first hit.
 __device__ __forceinline__ Hit trace_scene_body(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
-                                                float tmax_ray)
+                                                float tmax_ray, bool any = false)
 {
     Hit h = trace_ray_body(s, o, d, tmin_ray, tmax_ray);
-    if (s.entity_count) trace_entities(s, o, d, tmin_ray, tmax_ray, h);
+    if (s.entity_count && !(any && h.hit)) trace_entities(s, o, d, tmin_ray, tmax_ray, h, any);
     return h;
 }
 
-__device__ __noinline__ Hit trace_scene(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray)
+__device__ __noinline__ Hit trace_scene(const SceneView& s, const float o[3], const float d[3], float tmin_ray, float tmax_ray,
+                                        bool any = false)
 {
     Hit h = trace_ray(s, o, d, tmin_ray, tmax_ray);
-    if (s.entity_count) trace_entities(s, o, d, tmin_ray, tmax_ray, h);
+    if (s.entity_count && !(any && h.hit)) trace_entities(s, o, d, tmin_ray, tmax_ray, h, any);
     return h;
 }
 

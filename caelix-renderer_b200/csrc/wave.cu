@@ -155,7 +155,7 @@ __global__ void __launch_bounds__(kWaveThreads)
             const float d[3] = {d4.x, d4.y, d4.z};
             const float t_max = kind == kKindShadow ? d4.w : (kind == kKindPrimary ? kRayTMax : kBounceTMax);
             Hit h;
-            if constexpr (kEntities) h = trace_scene_body(views[v].scene, o, d, 0.0f, t_max);
+            if constexpr (kEntities) h = trace_scene_body(views[v].scene, o, d, 0.0f, t_max, kind == kKindShadow);
             else h = trace_ray_body(views[v].scene, o, d, 0.0f, t_max);
             if (kind == kKindShadow) b.occluded[slot] = h.hit ? 1u : 0u;
             else b.hit[slot] = h.hit ? make_uint4(__float_as_uint(h.t), h.attrib, h.record, h.group) : make_uint4(0, 0, 0, 0);
