@@ -475,11 +475,12 @@ __global__ void __launch_bounds__(kScanThreads)
 
 // The depth of binary node i is the number of nodes over its split boundary minus one (the nodes
 // over boundary gamma are node i and its ancestors); even depths are flagged and scanned into the
-// 4-wide node index. The last tile writes the node count.
+// 4-wide node index (wide[i]), with even[w] the binary node of 4-wide node w. The last tile writes
+// the node count.
 __global__ void __launch_bounds__(kScanThreads)
     lt_flags_scan_kernel(uint32_t nodes, const uint32_t* __restrict__ left, const uint32_t* __restrict__ cover,
-                         uint32_t* __restrict__ depth_out, uint32_t* __restrict__ wide, uint32_t* states,
-                         uint32_t* tile_counter, BuildControl* control)
+                         uint32_t* __restrict__ depth_out, uint32_t* __restrict__ wide, uint32_t* __restrict__ even,
+                         uint32_t* states, uint32_t* tile_counter, BuildControl* control)
 {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[kScanThreads / 32];
@@ -516,38 +517,35 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         if (base + k < nodes) wide[base + k] = run;
+        if (flag[k]) even[run] = base + k;  // the binary node of every 4-wide node
         run += flag[k];
     }
 }
 
 // ---------------------------------------------------------------------------------------------
-// 4-wide collapse: one thread per binary node at even depth builds its whole node (224 bytes,
-// its own parent link included: the 4-wide parent is the binary grandparent) in shared memory and
-// writes the parent words of its leaf slots by sorted position. The even-depth nodes of a CTA's
-// binary nodes have consecutive 4-wide indices (an exclusive scan of the flags), so the CTA then
-// stores its run of nodes with coalesced 16-byte writes.
+// 4-wide collapse: one thread per 4-wide node w (binary node even[w], at even depth) builds the
+// whole node (224 bytes, its own parent link included: the 4-wide parent is the binary
+// grandparent) in shared memory and writes the parent words of its leaf slots by sorted position;
+// the CTA then stores its run of consecutive nodes with coalesced 16-byte writes.
 constexpr uint32_t kWideThreads = 128;
 constexpr uint32_t kNodeWords = sizeof(LightBvhNode) / 4;  // 56
 
 __global__ void __launch_bounds__(kWideThreads)
     lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                   const uint32_t* __restrict__ parent, const uint32_t* __restrict__ depth,
+                   const uint32_t* __restrict__ parent, const uint32_t* __restrict__ even,
                    const uint32_t* __restrict__ wide, const LightSummary* __restrict__ sorted,
                    const AggregateSlot* __restrict__ aggregates, uint32_t* __restrict__ leaf_word,
-                   LightBvhNode* __restrict__ nodes)
+                   LightBvhNode* __restrict__ nodes, const BuildControl* __restrict__ control)
 {
     __shared__ __align__(16) float s_node[kWideThreads * kNodeWords];
-    const uint32_t base = blockIdx.x * kWideThreads;
-    const uint32_t i = base + threadIdx.x;
-    const uint32_t binary = n - 1;
-    const bool active = i < binary && (__ldg(depth + i) & 1u) == 0;
-    // The CTA's first 4-wide index: the count of even-depth nodes before `base`.
-    const uint32_t w_base = __ldg(wide + base);
-    const uint32_t count = __syncthreads_count(active);
-    if (active) {
-        const uint32_t w = __ldg(wide + i);
-        float* node = s_node + (w - w_base) * kNodeWords;
+    const uint32_t count = min(control->node_count, node_capacity);
+    const uint32_t w_base = blockIdx.x * kWideThreads;
+    if (w_base >= count) return;
+    const uint32_t w = w_base + threadIdx.x;
+    if (w < count) {
+        const uint32_t i = __ldg(even + w);
+        float* node = s_node + threadIdx.x * kNodeWords;
         uint32_t* words = reinterpret_cast<uint32_t*>(node);
         const uint32_t l = __ldg(left + i);
         const uint32_t r = __ldg(right + i);
@@ -616,10 +614,7 @@ __global__ void __launch_bounds__(kWideThreads)
         words[55] = 0u;
     }
     __syncthreads();
-    // The run [w_base, w_base + count), clipped to the node capacity.
-    const uint32_t last = min(w_base + count, node_capacity);
-    if (w_base >= last) return;
-    const uint32_t quads = (last - w_base) * (kNodeWords / 4);
+    const uint32_t quads = (min(w_base + kWideThreads, count) - w_base) * (kNodeWords / 4);
     const float4* src = reinterpret_cast<const float4*>(s_node);
     float4* dst = reinterpret_cast<float4*>(nodes + w_base);
     for (uint32_t q = threadIdx.x; q < quads; q += kWideThreads) dst[q] = src[q];
@@ -827,12 +822,14 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         const uint32_t tiles = (nodes + kScanTile - 1) / kScanTile;
         lt_cover_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.cover, cover_states, scan_counters,
                                                                   b.control);
+        // keys_alt (free after the sort) holds the binary node of every 4-wide node.
         lt_flags_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.left, b.cover, b.depth, b.wide,
-                                                                  flag_states, scan_counters + 1, b.control);
+                                                                  b.keys_alt, flag_states, scan_counters + 1,
+                                                                  b.control);
         mark(6);
         lt_wide_kernel<<<grid_for(nodes, kWideThreads, 1u << 30), kWideThreads, 0, stream>>>(
-            n, b.node_capacity, b.values, b.left, b.right, b.parent, b.depth, b.wide, b.sorted, b.aggregates,
-            b.leaf_word, b.nodes);
+            n, b.node_capacity, b.values, b.left, b.right, b.parent, b.keys_alt, b.wide, b.sorted, b.aggregates,
+            b.leaf_word, b.nodes, b.control);
         lt_leaf_parent_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.inverse, b.leaf_word,
                                                                                         b.leaves);
     } else {
