@@ -86,12 +86,10 @@ __device__ __forceinline__ uint32_t morton30(uint32_t x, uint32_t y, uint32_t z)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Gather emit + centre bounds. A CTA takes tiles of kThreads records: the tile's records (48
-// bytes each) come in as consecutive 16-byte loads into shared memory, every thread computes its
-// record's leaf there, and the tile's leaves (64 bytes each) go out as consecutive 16-byte
-// stores, so every load and store instruction of a warp covers whole 128-byte lines.
-constexpr uint32_t kRecordVecs = sizeof(BrickLightRecord) / 16;  // 3
-constexpr uint32_t kLeafVecs = sizeof(LightBvhLeaf) / 16;        // 4
+// Gather emit + centre bounds: a thread per record (grid-stride), its 48-byte record, group, entry
+// and group frame loaded up front, its 64-byte leaf written as four 16-byte stores (a warp's four
+// store instructions fill whole lines between them); the centre codes max-reduced per warp at the
+// end, one atomic per warp and code.
 static_assert(sizeof(BrickLightRecord) == 48 && sizeof(LightBvhLeaf) == 64, "record and leaf sizes");
 
 __global__ void __launch_bounds__(kThreads)
@@ -100,110 +98,89 @@ __global__ void __launch_bounds__(kThreads)
                    const GroupFrame* __restrict__ frames, uint32_t frame_count, LightBvhLeaf* __restrict__ leaves,
                    BuildControl* __restrict__ control)
 {
-    __shared__ uint4 s_rec[kThreads * kRecordVecs];
-    __shared__ uint4 s_leaf[kThreads * kLeafVecs];
     uint32_t lo_code[3] = {0, 0, 0};  // ~order(centre), max-reduced
     uint32_t hi_code[3] = {0, 0, 0};  // order(centre), max-reduced
-    const uint32_t tiles = (n + kThreads - 1) / kThreads;
     const uint4* rsrc = reinterpret_cast<const uint4*>(records);
     uint4* ldst = reinterpret_cast<uint4*>(leaves);
-    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint32_t first = tile * kThreads;
-        const uint32_t count = min(n - first, kThreads);
-        __syncthreads();  // the previous tile's leaves are out
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const uint4 w0 = __ldg(rsrc + 3ull * i);
+        const uint4 w1 = __ldg(rsrc + 3ull * i + 1);
+        const uint32_t g = record_group ? __ldg(record_group + i) : 0u;
+        const uint32_t e = record_entry ? __ldg(record_entry + i) : i;
+        LightSummary local;
+        local.face[0] = __uint_as_float(w0.x);
+        local.face[1] = __uint_as_float(w0.y);
+        local.face[2] = __uint_as_float(w0.z);
+        local.face[3] = __uint_as_float(w0.w);
+        local.face[4] = __uint_as_float(w1.x);
+        local.face[5] = __uint_as_float(w1.y);
+        const uint32_t box_lo = w1.z;
+        const uint32_t box_hi = w1.w;
+        float origin[3] = {0.0f, 0.0f, 0.0f};
+        float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        float t[3] = {0.0f, 0.0f, 0.0f};
+        if (frames && g >= frame_count) atomicOr(&control->status, kStatusBadGroup);
+        if (frames && g < frame_count) {
+            const GroupFrame* f = frames + g;
 #pragma unroll
-        for (uint32_t k = 0; k < kRecordVecs; ++k) {
-            const uint32_t v = threadIdx.x + k * kThreads;
-            if (v < count * kRecordVecs) s_rec[v] = __ldg(rsrc + (uint64_t)first * kRecordVecs + v);
-        }
-        __syncthreads();
-        const uint32_t i = first + threadIdx.x;
-        if (threadIdx.x < count) {
-            const uint4 w0 = s_rec[kRecordVecs * threadIdx.x];
-            const uint4 w1 = s_rec[kRecordVecs * threadIdx.x + 1];
-            LightSummary local;
-            local.face[0] = __uint_as_float(w0.x);
-            local.face[1] = __uint_as_float(w0.y);
-            local.face[2] = __uint_as_float(w0.z);
-            local.face[3] = __uint_as_float(w0.w);
-            local.face[4] = __uint_as_float(w1.x);
-            local.face[5] = __uint_as_float(w1.y);
-            const uint32_t box_lo = w1.z;
-            const uint32_t box_hi = w1.w;
-            const uint32_t g = record_group ? __ldg(record_group + i) : 0u;
-            float origin[3] = {0.0f, 0.0f, 0.0f};
-            float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-            float t[3] = {0.0f, 0.0f, 0.0f};
-            if (frames && g >= frame_count) atomicOr(&control->status, kStatusBadGroup);
-            if (frames && g < frame_count) {
-                const GroupFrame* f = frames + g;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    origin[k] = __ldg(&f->origin[k]);
-                    t[k] = __ldg(&f->trans[k]);
-                }
-#pragma unroll
-                for (int k = 0; k < 9; ++k) r[k] = __ldg(&f->rot[k]);
+            for (int k = 0; k < 3; ++k) {
+                origin[k] = __ldg(&f->origin[k]);
+                t[k] = __ldg(&f->trans[k]);
             }
-            local.lo[0] = origin[0] + (float)(box_lo & kVoxelMask);
-            local.lo[1] = origin[1] + (float)((box_lo >> kVoxelBits) & kVoxelMask);
-            local.lo[2] = origin[2] + (float)((box_lo >> (2 * kVoxelBits)) & kVoxelMask);
-            local.hi[0] = origin[0] + (float)(box_hi & kVoxelMask);
-            local.hi[1] = origin[1] + (float)((box_hi >> kVoxelBits) & kVoxelMask);
-            local.hi[2] = origin[2] + (float)((box_hi >> (2 * kVoxelBits)) & kVoxelMask);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) r[k] = __ldg(&f->rot[k]);
+        }
+        local.lo[0] = origin[0] + (float)(box_lo & kVoxelMask);
+        local.lo[1] = origin[1] + (float)((box_lo >> kVoxelBits) & kVoxelMask);
+        local.lo[2] = origin[2] + (float)((box_lo >> (2 * kVoxelBits)) & kVoxelMask);
+        local.hi[0] = origin[0] + (float)(box_hi & kVoxelMask);
+        local.hi[1] = origin[1] + (float)((box_hi >> kVoxelBits) & kVoxelMask);
+        local.hi[2] = origin[2] + (float)((box_hi >> (2 * kVoxelBits)) & kVoxelMask);
 
-            // LtWorldSummary (caelix_light_gather_emit.hlsl:11-34).
-            float centre[3], half[3];
+        // LtWorldSummary (caelix_light_gather_emit.hlsl:11-34).
+        float centre[3], half[3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                centre[k] = 0.5f * (local.lo[k] + local.hi[k]);
-                half[k] = 0.5f * (local.hi[k] - local.lo[k]);
-            }
-            LightSummary w;
+        for (int k = 0; k < 3; ++k) {
+            centre[k] = 0.5f * (local.lo[k] + local.hi[k]);
+            half[k] = 0.5f * (local.hi[k] - local.lo[k]);
+        }
+        LightSummary w;
 #pragma unroll
-            for (int row = 0; row < 3; ++row) {
-                const float wc = r[3 * row] * centre[0] + r[3 * row + 1] * centre[1] + r[3 * row + 2] * centre[2] +
-                                 t[row];
-                const float wh = fabsf(r[3 * row]) * half[0] + fabsf(r[3 * row + 1]) * half[1] +
-                                 fabsf(r[3 * row + 2]) * half[2];
-                w.lo[row] = wc - wh;
-                w.hi[row] = wc + wh;
-            }
+        for (int row = 0; row < 3; ++row) {
+            const float wc = r[3 * row] * centre[0] + r[3 * row + 1] * centre[1] + r[3 * row + 2] * centre[2] +
+                             t[row];
+            const float wh = fabsf(r[3 * row]) * half[0] + fabsf(r[3 * row + 1]) * half[1] +
+                             fabsf(r[3 * row + 2]) * half[2];
+            w.lo[row] = wc - wh;
+            w.hi[row] = wc + wh;
+        }
 #pragma unroll
-            for (int f = 0; f < 6; ++f) w.face[f] = 0.0f;
+        for (int f = 0; f < 6; ++f) w.face[f] = 0.0f;
 #pragma unroll
-            for (int f = 0; f < 6; ++f) {
-                const int axis = f >> 1;
-                const float sign = (f & 1) ? -1.0f : 1.0f;
+        for (int f = 0; f < 6; ++f) {
+            const int axis = f >> 1;
+            const float sign = (f & 1) ? -1.0f : 1.0f;
 #pragma unroll
-                for (int b = 0; b < 3; ++b) {
-                    const float d = sign * r[3 * b + axis];
-                    w.face[2 * b] += local.face[f] * hmax(0.0f, d);
-                    w.face[2 * b + 1] += local.face[f] * hmax(0.0f, -d);
-                }
-            }
-            uint4* q = s_leaf + kLeafVecs * threadIdx.x;
-            q[0] = make_uint4(__float_as_uint(w.face[0]), __float_as_uint(w.face[1]), __float_as_uint(w.face[2]),
-                              __float_as_uint(w.face[3]));
-            q[1] = make_uint4(__float_as_uint(w.face[4]), __float_as_uint(w.face[5]), __float_as_uint(w.lo[0]),
-                              __float_as_uint(w.lo[1]));
-            q[2] = make_uint4(__float_as_uint(w.lo[2]), __float_as_uint(w.hi[0]), __float_as_uint(w.hi[1]),
-                              __float_as_uint(w.hi[2]));
-            const uint32_t e = record_entry ? __ldg(record_entry + i) : i;
-            q[3] = make_uint4(g, e, 0u, kNone);
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const float c = 0.5f * (w.lo[k] + w.hi[k]);
-                const uint32_t code = float_order(c);
-                lo_code[k] = max(lo_code[k], ~code);
-                hi_code[k] = max(hi_code[k], code);
+            for (int b = 0; b < 3; ++b) {
+                const float d = sign * r[3 * b + axis];
+                w.face[2 * b] += local.face[f] * hmax(0.0f, d);
+                w.face[2 * b + 1] += local.face[f] * hmax(0.0f, -d);
             }
         }
-        __syncthreads();
+        uint4* q = ldst + 4ull * i;
+        q[0] = make_uint4(__float_as_uint(w.face[0]), __float_as_uint(w.face[1]), __float_as_uint(w.face[2]),
+                          __float_as_uint(w.face[3]));
+        q[1] = make_uint4(__float_as_uint(w.face[4]), __float_as_uint(w.face[5]), __float_as_uint(w.lo[0]),
+                          __float_as_uint(w.lo[1]));
+        q[2] = make_uint4(__float_as_uint(w.lo[2]), __float_as_uint(w.hi[0]), __float_as_uint(w.hi[1]),
+                          __float_as_uint(w.hi[2]));
+        q[3] = make_uint4(g, e, 0u, kNone);
 #pragma unroll
-        for (uint32_t k = 0; k < kLeafVecs; ++k) {
-            const uint32_t v = threadIdx.x + k * kThreads;
-            if (v < count * kLeafVecs) ldst[(uint64_t)first * kLeafVecs + v] = s_leaf[v];
+        for (int k = 0; k < 3; ++k) {
+            const float c = 0.5f * (w.lo[k] + w.hi[k]);
+            const uint32_t code = float_order(c);
+            lo_code[k] = max(lo_code[k], ~code);
+            hi_code[k] = max(hi_code[k], code);
         }
     }
 #pragma unroll
@@ -318,21 +295,23 @@ __global__ void __launch_bounds__(kThreads)
     const uint32_t key_i = __ldg(keys + i);
     const int d = lt_delta(keys, i, i + 1, n, key_i) - lt_delta(keys, i, i - 1, n, key_i) >= 0 ? 1 : -1;
     const int delta_min = lt_delta(keys, i, i - d, n, key_i);
+    // The searches with shifts for the divisions by powers of two (lengths are positive, so the
+    // quotients and the ceilings are those of the divisions).
     int length_max = 2;
-    while (lt_delta(keys, i, i + length_max * d, n, key_i) > delta_min) length_max *= 2;
+    while (lt_delta(keys, i, i + (d > 0 ? length_max : -length_max), n, key_i) > delta_min) length_max <<= 1;
     int length = 0;
-    for (int step = length_max / 2; step >= 1; step /= 2)
-        if (lt_delta(keys, i, i + (length + step) * d, n, key_i) > delta_min) length += step;
-    const int j = i + length * d;
+    for (int step = length_max >> 1; step >= 1; step >>= 1)
+        if (lt_delta(keys, i, i + (d > 0 ? length + step : -(length + step)), n, key_i) > delta_min) length += step;
+    const int j = i + (d > 0 ? length : -length);
     const int delta_node = lt_delta(keys, i, j, n, key_i);
     int split = 0;
-    int divisor = 2;
-    int step2 = (length + divisor - 1) / divisor;
+    uint32_t shift = 1;  // the divisor 2^shift
+    int step2 = (int)(((uint32_t)length + 1u) >> 1);
     for (;;) {
-        if (lt_delta(keys, i, i + (split + step2) * d, n, key_i) > delta_node) split += step2;
+        if (lt_delta(keys, i, i + (d > 0 ? split + step2 : -(split + step2)), n, key_i) > delta_node) split += step2;
         if (step2 == 1) break;
-        divisor *= 2;
-        step2 = (length + divisor - 1) / divisor;
+        ++shift;
+        step2 = (int)(((uint32_t)length + ((1u << shift) - 1u)) >> shift);
     }
     const int gamma = i + split * d + min(d, 0);
     const int a = min(i, j);
