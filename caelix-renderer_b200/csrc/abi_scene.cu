@@ -187,7 +187,7 @@ CaelixResult build_light_set(CaelixScene* scene, LightSet& set, const std::vecto
     in.record_entry = lentry;
     in.group_frames = frames;
     in.group_count = (uint32_t)groups;
-    in.sort_keys_per_thread = cx::kSortKeysPerThread;
+    in.sort_keys_per_thread = 0;  // the tile for the light count (sort_keys_per_thread_for)
     set.input = in;
     if (e == cudaSuccess) e = cx::lt_build(tree, in, stream, nullptr);
     cx::SceneView& v = set.v;

@@ -751,7 +751,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     // Zeroed words of this build: control, the sort scratch sized for n, two scan state arrays and
     // their tile counters.
     const uint32_t kpt = sort_keys_per_thread_ok(in.sort_keys_per_thread) ? in.sort_keys_per_thread
-                                                                             : (uint32_t)kSortKeysPerThread;
+                                                                             : sort_keys_per_thread_for(n);
     const uint32_t scan_tiles_n = (n + kScanTile - 1) / kScanTile;
     uint32_t* cover_states = b.sort_scratch + sort_scratch_words(n, kpt);
     uint32_t* flag_states = cover_states + scan_tiles_n;

@@ -112,7 +112,7 @@ struct LightBvhInput
     const uint32_t* record_entry;
     const GroupFrame* group_frames;
     uint32_t group_count;
-    uint32_t sort_keys_per_thread = kSortKeysPerThread;  // the radix sort's tile: 256 x 4, 8 or 16 keys
+    uint32_t sort_keys_per_thread = kSortKeysPerThread;  // the radix sort's tile: 256 x 4, 8 or 16 keys (0: by size)
 };
 
 constexpr int kScanThreads = 256;

@@ -259,7 +259,6 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
 // the tile before, and the values are in shared memory before the look-back ends. The ranking, the
 // look-back and the output are the plain pass's (the same stable permutation). Two CTAs per SM.
 constexpr uint32_t kPipeTile = kSortThreads * kSortKeysPerThread;  // 4096
-constexpr uint32_t kPipeMinTiles = 64;
 
 struct PipeShared
 {

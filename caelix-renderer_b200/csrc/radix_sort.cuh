@@ -57,6 +57,16 @@ __host__ __device__ constexpr uint64_t sort_scratch_words(uint32_t n, uint32_t k
     return 4ull * kRadix + 4ull + 4ull * sort_tiles(n, kpt) * kRadix;
 }
 
+// The tile for a sort of n pairs chosen by the sort's callers: 4096 keys when that gives at least
+// kPipeMinTiles tiles (the persistent pipelined pass), else 1024 (more tiles for a small sort, and
+// a quarter of the ranking work in each tile's critical path).
+constexpr uint32_t kPipeMinTiles = 64;
+__host__ __device__ constexpr uint32_t sort_keys_per_thread_for(uint32_t n)
+{
+    return sort_tiles(n, kSortKeysPerThread) >= kPipeMinTiles ? (uint32_t)kSortKeysPerThread
+                                                             : (uint32_t)kSortMinKeysPerThread;
+}
+
 // The number of SMs of the current CUDA device (looked up once per device), for grid sizing.
 uint32_t current_sm_count();
 

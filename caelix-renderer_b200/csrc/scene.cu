@@ -945,7 +945,7 @@ struct BuildScratch
 
 static uint64_t build_scratch_words(uint32_t n)
 {
-    return 14ull * std::max(n, 1u) + sort_scratch_words(std::max(n, 1u)) + 2 +
+    return 14ull * std::max(n, 1u) + sort_scratch_words(std::max(n, 1u), kSortMinKeysPerThread) + 2 +
            blocks_for(std::max(n, 1u), kScanTile) + 64;
 }
 
@@ -964,7 +964,7 @@ static BuildScratch build_scratch(const DeviceScene& s)
     b.tmp2 = w + 7 * n;
     b.counts6 = w + 8 * n;
     b.sortw = w + 14 * n;
-    b.small = b.sortw + sort_scratch_words(std::max(s.brick_count, 1u));
+    b.small = b.sortw + sort_scratch_words(std::max(s.brick_count, 1u), kSortMinKeysPerThread);
     return b;
 }
 
@@ -1013,7 +1013,8 @@ cudaError_t scene_build_device(DeviceScene& s, const int32_t origin[3], const ui
     s.group_count = s.groups[0] * s.groups[1] * s.groups[2];
     s.brick_count = n;
 
-    const uint64_t sort_words = sort_scratch_words(std::max(n, 1u));
+    const uint32_t hash_kpt = sort_keys_per_thread_for(n);
+    const uint64_t sort_words = sort_scratch_words(std::max(n, 1u), hash_kpt);
     const uint64_t need = build_scratch_words(n);
     if (need > s.scratch_words) {
         CX_TRY(alloc(s.scratch, s.capacity.scratch, need));
@@ -1041,8 +1042,8 @@ cudaError_t scene_build_device(DeviceScene& s, const int32_t origin[3], const ui
         hash_home_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, s.hash_capacity, lo, hi, home);
         CX_TRY(cudaMemsetAsync(sortw, 0, sort_words * 4, stream));
         radix_histogram(home, n, sortw, std::min<uint32_t>(blocks_for(n, 2048), current_sm_count() * 4), stream);
-        onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream, nullptr, kSortKeysPerThread,
-                      nullptr, bits_below(s.hash_capacity));
+        onesweep_sort(home, order, home_alt, order_alt, n, true, sortw, s.status, stream, nullptr, hash_kpt, nullptr,
+                      bits_below(s.hash_capacity));
         hash_shift_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(home, n, tmp);
         CX_TRY(run_scan(true, tmp, tmp2, n, small, nullptr, s.status, stream));
         hash_place_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(tmp2, home, order, lo, hi, n, s.hash_slots,
@@ -1157,11 +1158,12 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     CX_TRY(cudaMemcpyAsync(s.frames, frames.data(), sizeof(GroupFrame) * s.group_count, cudaMemcpyHostToDevice, stream));
     uint32_t total_units = 0;
     if (m > 0) {
-        CX_TRY(cudaMemsetAsync(sortw, 0, sort_scratch_words(m) * 4, stream));
+        const uint32_t light_kpt = sort_keys_per_thread_for(m);
+        CX_TRY(cudaMemsetAsync(sortw, 0, sort_scratch_words(m, light_kpt) * 4, stream));
         radix_histogram(lkeys, m, sortw, std::min<uint32_t>(blocks_for(m, 2048), current_sm_count() * 4), stream);
         // Keys: the group index above 3 * group_shift bits of position in the group.
-        onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream, nullptr,
-                      kSortKeysPerThread, nullptr, 3 * group_shift + bits_below(s.group_count));
+        onesweep_sort(lkeys, lbricks, lkeys_alt, lbricks_alt, m, false, sortw, s.status, stream, nullptr, light_kpt,
+                      nullptr, 3 * group_shift + bits_below(s.group_count));
         uint32_t* units = home;    // m words
         uint32_t* totals = order;  // m words
         uint32_t* group_start = tmp;

@@ -242,8 +242,7 @@ cudaError_t dyn_append(const DeviceScene& e, const DynPart& part, uint32_t* dst_
 // Rebuilds the light tree of a built scene from its light records (asynchronous on `stream`, no
 // allocation: the tree buffers were sized by scene_build). The reference's per-flush light BVH
 // rebuild (lib/src/light/light_tree_record.cpp:230-302, RecordTree).
-cudaError_t scene_build_light_tree(const DeviceScene& s, cudaStream_t stream,
-                                   uint32_t sort_keys_per_thread = kSortKeysPerThread);
+cudaError_t scene_build_light_tree(const DeviceScene& s, cudaStream_t stream, uint32_t sort_keys_per_thread = 0);
 // Reads the scene's and its light tree's device status words (synchronises `stream`).
 cudaError_t scene_read_status(const DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out);
 void scene_release(DeviceScene& s);

@@ -124,7 +124,7 @@ cudaError_t staging_move(int32_t* stage_keys, uint16_t* stage_voxels, const uint
 uint64_t staging_sort_words(uint32_t n)
 {
     const uint64_t c = std::max(n, 1u);
-    return 4 * c + sort_scratch_words((uint32_t)c);
+    return 4 * c + sort_scratch_words((uint32_t)c, kSortMinKeysPerThread);
 }
 
 cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxels, const float* slot_power,
@@ -140,10 +140,11 @@ cudaError_t staging_gather(const int32_t* stage_keys, const uint16_t* stage_voxe
     uint32_t* sortw = scratch + 4ull * n;
     staging_linear_kernel<<<blocks(n), kStageThreads, 0, stream>>>(stage_keys, n, origin[0], origin[1], origin[2],
                                                                     grid[0], grid[1], lin);
-    CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n), stream));
+    const uint32_t kpt = sort_keys_per_thread_for(n);
+    CX_TRY(cudaMemsetAsync(sortw, 0, 4 * sort_scratch_words(n, kpt), stream));
     radix_histogram(lin, n, sortw, std::min<uint32_t>((n + 2047) / 2048, current_sm_count() * 4), stream);
     // A stable sort of the linear indices (unique: one slot per key), values = the slots.
-    onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream, nullptr, kSortKeysPerThread, nullptr,
+    onesweep_sort(lin, order, lin_alt, order_alt, n, true, sortw, status, stream, nullptr, kpt, nullptr,
                   bits_below((uint64_t)grid[0] * grid[1] * grid[2]));
     staging_gather_kernel<<<blocks(64ull * n), kStageThreads, 0, stream>>>(
         order, n, stage_keys, reinterpret_cast<const uint4*>(stage_voxels), slot_power, keys,
