@@ -330,13 +330,15 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
-// computes its summary from both children and goes on. A CTA owns a tile of kAggTile consecutive
-// sorted leaves: a node whose range lies inside the tile is reached only by the tile's threads,
-// so its arrival counter and summary live in shared memory (block-scope acq_rel); only nodes whose
-// range crosses a tile boundary use device-scope counters. A thread carries the summary of the
-// child it comes from and loads only the sibling. Every node's summary is also stored to its
-// 64-byte global slot (full-sector writes) for the collapse.
+// Bottom-up aggregation. A CTA owns a tile of kAggTile consecutive sorted leaves and the binary
+// nodes with the same indices (a node is an end of its leaf range, so every node whose range lies
+// inside the tile has its index there). In-tile nodes are computed in rounds over shared memory:
+// in each round every in-tile node whose children are done takes the union of their summaries
+// (no atomics: a barrier between rounds makes the results visible). Then the tile's subtree roots
+// (and the leaves whose parent crosses a tile boundary) walk up through the nodes that cross tile
+// boundaries: the second thread to arrive at such a node (a device-scope arrival counter) computes
+// it and goes on. Every node's summary is also stored to its 64-byte global slot (full-sector
+// writes) for the collapse; the union is taken left, right as the tree orders them.
 constexpr uint32_t kAggTile = 256;
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
@@ -354,54 +356,83 @@ __global__ void __launch_bounds__(kAggTile)
                         const uint32_t* __restrict__ leaf_parent, const uint32_t* __restrict__ range_end,
                         uint32_t* counter, AggregateSlot* aggregates, BuildControl* control)
 {
-    __shared__ uint32_t s_count[kAggTile];
-    __shared__ LightSummary s_sum[kAggTile];
+    __shared__ LightSummary s_leaf[kAggTile];
+    __shared__ LightSummary s_node[kAggTile];
     __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
+    __shared__ uint32_t s_done[kAggTile];
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
-    s_count[threadIdx.x] = 0;
-    {
-        // The tile's own node indices (a node is an end of its leaf range, so every node inside the
-        // tile has its index there), loaded coalesced once; the walks then read them from here.
-        const uint32_t k = lo + threadIdx.x;
-        if (k + 1 < n)
-            s_link[threadIdx.x] = make_uint4(__ldg(left + k), __ldg(right + k), __ldg(parent + k), __ldg(range_end + k));
+    const uint32_t k = threadIdx.x;
+    const uint32_t j = lo + k;  // this thread's leaf and node
+    bool mine = false;          // node j lies inside the tile
+    if (j < n) s_leaf[k] = load_summary(sorted + j);
+    if (j + 1 < n) {
+        const uint4 link = make_uint4(__ldg(left + j), __ldg(right + j), __ldg(parent + j), __ldg(range_end + j));
+        s_link[k] = link;
+        mine = min(j, link.w) >= lo && max(j, link.w) <= hi;
     }
-    __syncthreads();
-    const uint32_t j = lo + threadIdx.x;
-    if (j >= n) return;
-    LightSummary cur = load_summary(sorted + j);
-    uint32_t from = kChildLeafBit | j;
-    uint32_t node = __ldg(leaf_parent + j);
+    s_done[k] = 0;
+    const auto inside = [&](uint32_t node) {
+        if (node - lo >= kAggTile || node + 1 >= n) return false;
+        const uint32_t end = s_link[node - lo].w;
+        return min(node, end) >= lo && max(node, end) <= hi;
+    };
+    // The in-tile rounds.
+    bool pending = mine;
+    uint32_t rounds = 0;
+    while (__syncthreads_or(pending)) {
+        bool done_now = false;
+        if (pending) {
+            const uint4 link = s_link[k];
+            const bool l_leaf = (link.x & kChildLeafBit) != 0, r_leaf = (link.y & kChildLeafBit) != 0;
+            const uint32_t l = (link.x & ~kChildLeafBit) - lo, r = (link.y & ~kChildLeafBit) - lo;
+            if ((l_leaf || s_done[l]) && (r_leaf || s_done[r])) {
+                const LightSummary a = l_leaf ? s_leaf[l] : s_node[l];
+                const LightSummary b = r_leaf ? s_leaf[r] : s_node[r];
+                const LightSummary u = lt_union(a, b);
+                s_node[k] = u;
+                store_slot(aggregates + j, u);
+                done_now = true;
+                pending = false;
+            }
+        }
+        __syncthreads();
+        if (done_now) s_done[k] = 1;
+        if (++rounds > kAggTile) {  // a malformed tree: give up (every round completes a node)
+            if (k == 0) atomicOr(&control->status, kStatusDepthGuard);
+            return;
+        }
+    }
+    // The walks up through the nodes that cross tile boundaries: from an in-tile node whose parent
+    // is not in the tile, and from a leaf whose parent is not.
+    LightSummary cur;
+    uint32_t from, node;
+    if (mine) {
+        const uint32_t up = s_link[k].z;
+        if (up == kNone || inside(up)) return;
+        cur = s_node[k];
+        from = j;
+        node = up;
+    } else if (j < n) {
+        const uint32_t up = __ldg(leaf_parent + j);
+        if (up == kNone || inside(up)) return;
+        cur = s_leaf[k];
+        from = kChildLeafBit | j;
+        node = up;
+    } else {
+        return;
+    }
     uint32_t depth = 0;
     for (; depth < 128 && node != kNone; ++depth) {
-        uint4 link;
-        if (node - lo < kAggTile && node + 1 < n)
-            link = s_link[node - lo];
-        else
-            link = make_uint4(__ldg(left + node), __ldg(right + node), __ldg(parent + node), __ldg(range_end + node));
-        const uint32_t l = link.x;
-        const uint32_t r = link.y;
-        const uint32_t up = link.z;
-        const uint32_t end = link.w;
-        const uint32_t a = min(node, end);
-        const uint32_t b = max(node, end);
-        const bool inside = a >= lo && b <= hi;
+        const uint32_t l = __ldg(left + node);
+        const uint32_t r = __ldg(right + node);
+        const uint32_t up = __ldg(parent + node);
         const uint32_t sibling = l == from ? r : l;
-        LightSummary sib;
-        if (inside) {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrival(s_count[node - lo]);
-            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
-            else sib = s_sum[sibling - lo];
-        } else {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
-            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
-            else sib = load_summary_cg(&aggregates[sibling].summary);
-        }
+        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+        if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+        const LightSummary sib = (sibling & kChildLeafBit) ? load_summary(sorted + (sibling & ~kChildLeafBit))
+                                                            : load_summary_cg(&aggregates[sibling].summary);
         cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
-        if (inside) s_sum[node - lo] = cur;
         store_slot(aggregates + node, cur);
         from = node;
         node = up;
