@@ -51,12 +51,15 @@ TRACE_BOUNCES = 4
 L2_FLUSH_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 BUILD_BYTES_PER_LEAF = 492  # emit 112 + Morton 32 + sort 68 + Karras 20 + aggregate 100 + wide 160
-SORT_PASS_BYTES_PER_PAIR = 60.0 / 4  # pass 0 reads keys only (12 B), passes 1-3 read and write pairs (16 B)
+# The sort stage of the build: four onesweep passes (pass 0 reads keys only, 12 B; passes 1-3 read
+# and write pairs, 16 B) and the leaf-summary gather (values 4 B, a 48-byte row read and written,
+# the inverse 4 B).
+SORT_STAGE_BYTES_PER_PAIR = 60.0 + 104.0
 TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record sector per ray
-# DRAM bytes (read + write) measured by ncu (one capture, cold cache; profiles/): a plain onesweep
-# pass at 4,194,304 pairs, scaled per pair; the wavefront frame of the 512 x 512 trace (trace and
-# shade kernels of its 5 bounce iterations).
-SORT_PASS_DRAM_BYTES_PER_PAIR = 34.5e6 / 4194304
+# DRAM bytes (read + write) measured by ncu (one capture per kernel, cold cache; profiles/): the sort
+# stage at 4,194,304 pairs (a pipelined pass times four, plus the gather kernel), scaled per pair;
+# the wavefront frame of the 512 x 512 trace (trace and shade kernels of its 5 bounce iterations).
+SORT_STAGE_DRAM_BYTES_PER_PAIR = (4 * 34.2e6 + 520.2e6 + 205.6e6) / 4194304  # 4 x one pass + the gather
 TRACE_FRAME_DRAM_BYTES = 134.7e6
 
 
@@ -411,7 +414,7 @@ def measure_build(args, world, local, dev, stream, flush, records):
     stage_ms /= reps
     bvh.set_profiling(False)
     peak, peak_kind = measured_peaks()
-    sort_achieved = SORT_PASS_BYTES_PER_PAIR * n / (stage_ms[2] / 4 / 1e3) / 1e9
+    sort_achieved = SORT_STAGE_BYTES_PER_PAIR * n / (stage_ms[2] / 1e3) / 1e9
     build_achieved = BUILD_BYTES_PER_LEAF * n / (ms / 1e3) / 1e9
 
     # The 4,096-record plain build, L2 flushed between builds.
@@ -468,11 +471,11 @@ def measure_build(args, world, local, dev, stream, flush, records):
         "stage_ms": {name: float(v) for name, v in zip(
             ["emit_bounds", "morton_hist", "sort_4_passes", "karras", "aggregate", "depth_scan", "wide_finish"],
             stage_ms)},
-        "roofline": {"kernel": "onesweep_pass_kernel", "bound": "hbm", "achieved": sort_achieved, "peak": peak,
-                     "unit": "GB/s", "frac": sort_achieved / peak, "peak_kind": peak_kind,
-                     "traffic": SORT_PASS_DRAM_BYTES_PER_PAIR * n,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of a 4M-pair pass, per pair",
-                     "algorithmic_bytes_per_launch": SORT_PASS_BYTES_PER_PAIR * n},
+        "roofline": {"kernel": "sort stage: 4 onesweep_pipe_kernel passes + lt_gather_kernel", "bound": "hbm",
+                     "achieved": sort_achieved, "peak": peak, "unit": "GB/s", "frac": sort_achieved / peak,
+                     "peak_kind": peak_kind, "traffic": SORT_STAGE_DRAM_BYTES_PER_PAIR * n,
+                     "traffic_source": "ncu DRAM bytes of one pass (x4) and of the gather at 4M pairs, per pair",
+                     "algorithmic_bytes_per_launch": SORT_STAGE_BYTES_PER_PAIR * n},
         "roofline_build": {"bound": "hbm", "achieved": build_achieved, "peak": peak, "unit": "GB/s",
                            "frac": build_achieved / peak, "bytes_per_leaf": BUILD_BYTES_PER_LEAF},
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mleaves/s",
