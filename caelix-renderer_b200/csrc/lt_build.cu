@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(kThreads)
     lt_emit_kernel(const BrickLightRecord* __restrict__ records, uint32_t n,
                    const uint32_t* __restrict__ record_group, const uint32_t* __restrict__ record_entry,
                    const GroupFrame* __restrict__ frames, uint32_t frame_count, LightBvhLeaf* __restrict__ leaves,
-                   BuildControl* __restrict__ control)
+                   float4* __restrict__ centres, BuildControl* __restrict__ control)
 {
     uint32_t lo_code[3] = {0, 0, 0};  // ~order(centre), max-reduced
     uint32_t hi_code[3] = {0, 0, 0};  // order(centre), max-reduced
@@ -175,13 +175,15 @@ __global__ void __launch_bounds__(kThreads)
         q[2] = make_uint4(__float_as_uint(w.lo[2]), __float_as_uint(w.hi[0]), __float_as_uint(w.hi[1]),
                           __float_as_uint(w.hi[2]));
         q[3] = make_uint4(g, e, 0u, kNone);
+        float c[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float c = 0.5f * (w.lo[k] + w.hi[k]);
-            const uint32_t code = float_order(c);
+            c[k] = 0.5f * (w.lo[k] + w.hi[k]);
+            const uint32_t code = float_order(c[k]);
             lo_code[k] = max(lo_code[k], ~code);
             hi_code[k] = max(hi_code[k], code);
         }
+        centres[i] = make_float4(c[0], c[1], c[2], 0.0f);  // for the Morton codes (16 bytes, not the leaf)
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -211,10 +213,10 @@ __device__ __forceinline__ void decode_bounds(const BuildControl* control, float
 }
 
 // ---------------------------------------------------------------------------------------------
-// Morton codes (value = leaf index) + the four digit histograms + clearing the arrival counters
-// and the range-count differences.
+// Morton codes (value = leaf index) from the box centres the emit wrote + the four digit histograms
+// + clearing the arrival counters and the range-count differences.
 __global__ void __launch_bounds__(kThreads)
-    lt_morton_kernel(const LightBvhLeaf* __restrict__ leaves, uint32_t n, const BuildControl* __restrict__ control,
+    lt_morton_kernel(const float4* __restrict__ centres, uint32_t n, const BuildControl* __restrict__ control,
                      uint32_t* __restrict__ keys, uint32_t* __restrict__ counter, uint32_t* __restrict__ cover,
                      uint32_t* __restrict__ hist)
 {
@@ -227,16 +229,12 @@ __global__ void __launch_bounds__(kThreads)
     for (int k = 0; k < 3; ++k) extent[k] = hmax(hi[k] - lo[k], 1e-6f);
     __syncthreads();
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const float4* lp = reinterpret_cast<const float4*>(leaves + i);
-        const float4 b = __ldg(lp + 1);  // face4, face5, lo.x, lo.y
-        const float4 c = __ldg(lp + 2);  // lo.z, hi.x, hi.y, hi.z
-        const float box_lo[3] = {b.z, b.w, c.x};
-        const float box_hi[3] = {c.y, c.z, c.w};
+        const float4 ctr = __ldg(centres + i);  // the world box centre (emit: 0.5 (lo + hi))
+        const float centre[3] = {ctr.x, ctr.y, ctr.z};
         uint32_t cell[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            const float centre = 0.5f * (box_lo[k] + box_hi[k]);
-            const float q = hmin(hmax((centre - lo[k]) / extent[k] * 1024.0f, 0.0f), 1023.0f);
+            const float q = hmin(hmax((centre[k] - lo[k]) / extent[k] * 1024.0f, 0.0f), 1023.0f);
             cell[k] = (uint32_t)q;
         }
         const uint32_t key = morton30(cell[0], cell[1], cell[2]);
@@ -330,15 +328,13 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Bottom-up aggregation. A CTA owns a tile of kAggTile consecutive sorted leaves and the binary
-// nodes with the same indices (a node is an end of its leaf range, so every node whose range lies
-// inside the tile has its index there). In-tile nodes are computed in rounds over shared memory:
-// in each round every in-tile node whose children are done takes the union of their summaries
-// (no atomics: a barrier between rounds makes the results visible). Then the tile's subtree roots
-// (and the leaves whose parent crosses a tile boundary) walk up through the nodes that cross tile
-// boundaries: the second thread to arrive at such a node (a device-scope arrival counter) computes
-// it and goes on. Every node's summary is also stored to its 64-byte global slot (full-sector
-// writes) for the collapse; the union is taken left, right as the tree orders them.
+// Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
+// computes its summary from both children and goes on. A CTA owns a tile of kAggTile consecutive
+// sorted leaves: a node whose range lies inside the tile is reached only by the tile's threads,
+// so its arrival counter and summary live in shared memory (block-scope acq_rel); only nodes whose
+// range crosses a tile boundary use device-scope counters. A thread carries the summary of the
+// child it comes from and loads only the sibling. Every node's summary is also stored to its
+// 64-byte global slot (full-sector writes) for the collapse.
 constexpr uint32_t kAggTile = 256;
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
@@ -356,83 +352,54 @@ __global__ void __launch_bounds__(kAggTile)
                         const uint32_t* __restrict__ leaf_parent, const uint32_t* __restrict__ range_end,
                         uint32_t* counter, AggregateSlot* aggregates, BuildControl* control)
 {
-    __shared__ LightSummary s_leaf[kAggTile];
-    __shared__ LightSummary s_node[kAggTile];
+    __shared__ uint32_t s_count[kAggTile];
+    __shared__ LightSummary s_sum[kAggTile];
     __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
-    __shared__ uint32_t s_done[kAggTile];
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
-    const uint32_t k = threadIdx.x;
-    const uint32_t j = lo + k;  // this thread's leaf and node
-    bool mine = false;          // node j lies inside the tile
-    if (j < n) s_leaf[k] = load_summary(sorted + j);
-    if (j + 1 < n) {
-        const uint4 link = make_uint4(__ldg(left + j), __ldg(right + j), __ldg(parent + j), __ldg(range_end + j));
-        s_link[k] = link;
-        mine = min(j, link.w) >= lo && max(j, link.w) <= hi;
+    s_count[threadIdx.x] = 0;
+    {
+        // The tile's own node indices (a node is an end of its leaf range, so every node inside the
+        // tile has its index there), loaded coalesced once; the walks then read them from here.
+        const uint32_t k = lo + threadIdx.x;
+        if (k + 1 < n)
+            s_link[threadIdx.x] = make_uint4(__ldg(left + k), __ldg(right + k), __ldg(parent + k), __ldg(range_end + k));
     }
-    s_done[k] = 0;
-    const auto inside = [&](uint32_t node) {
-        if (node - lo >= kAggTile || node + 1 >= n) return false;
-        const uint32_t end = s_link[node - lo].w;
-        return min(node, end) >= lo && max(node, end) <= hi;
-    };
-    // The in-tile rounds.
-    bool pending = mine;
-    uint32_t rounds = 0;
-    while (__syncthreads_or(pending)) {
-        bool done_now = false;
-        if (pending) {
-            const uint4 link = s_link[k];
-            const bool l_leaf = (link.x & kChildLeafBit) != 0, r_leaf = (link.y & kChildLeafBit) != 0;
-            const uint32_t l = (link.x & ~kChildLeafBit) - lo, r = (link.y & ~kChildLeafBit) - lo;
-            if ((l_leaf || s_done[l]) && (r_leaf || s_done[r])) {
-                const LightSummary a = l_leaf ? s_leaf[l] : s_node[l];
-                const LightSummary b = r_leaf ? s_leaf[r] : s_node[r];
-                const LightSummary u = lt_union(a, b);
-                s_node[k] = u;
-                store_slot(aggregates + j, u);
-                done_now = true;
-                pending = false;
-            }
-        }
-        __syncthreads();
-        if (done_now) s_done[k] = 1;
-        if (++rounds > kAggTile) {  // a malformed tree: give up (every round completes a node)
-            if (k == 0) atomicOr(&control->status, kStatusDepthGuard);
-            return;
-        }
-    }
-    // The walks up through the nodes that cross tile boundaries: from an in-tile node whose parent
-    // is not in the tile, and from a leaf whose parent is not.
-    LightSummary cur;
-    uint32_t from, node;
-    if (mine) {
-        const uint32_t up = s_link[k].z;
-        if (up == kNone || inside(up)) return;
-        cur = s_node[k];
-        from = j;
-        node = up;
-    } else if (j < n) {
-        const uint32_t up = __ldg(leaf_parent + j);
-        if (up == kNone || inside(up)) return;
-        cur = s_leaf[k];
-        from = kChildLeafBit | j;
-        node = up;
-    } else {
-        return;
-    }
+    __syncthreads();
+    const uint32_t j = lo + threadIdx.x;
+    if (j >= n) return;
+    LightSummary cur = load_summary(sorted + j);
+    uint32_t from = kChildLeafBit | j;
+    uint32_t node = __ldg(leaf_parent + j);
     uint32_t depth = 0;
     for (; depth < 128 && node != kNone; ++depth) {
-        const uint32_t l = __ldg(left + node);
-        const uint32_t r = __ldg(right + node);
-        const uint32_t up = __ldg(parent + node);
+        uint4 link;
+        if (node - lo < kAggTile && node + 1 < n)
+            link = s_link[node - lo];
+        else
+            link = make_uint4(__ldg(left + node), __ldg(right + node), __ldg(parent + node), __ldg(range_end + node));
+        const uint32_t l = link.x;
+        const uint32_t r = link.y;
+        const uint32_t up = link.z;
+        const uint32_t end = link.w;
+        const uint32_t a = min(node, end);
+        const uint32_t b = max(node, end);
+        const bool inside = a >= lo && b <= hi;
         const uint32_t sibling = l == from ? r : l;
-        cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
-        if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-        const LightSummary sib = (sibling & kChildLeafBit) ? load_summary(sorted + (sibling & ~kChildLeafBit))
-                                                            : load_summary_cg(&aggregates[sibling].summary);
+        LightSummary sib;
+        if (inside) {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrival(s_count[node - lo]);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
+            else sib = s_sum[sibling - lo];
+        } else {
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
+            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
+            else sib = load_summary_cg(&aggregates[sibling].summary);
+        }
         cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
+        if (inside) s_sum[node - lo] = cur;
         store_slot(aggregates + node, cur);
         from = node;
         node = up;
@@ -792,10 +759,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     const uint32_t sms = current_sm_count();
     if (n > 0) {
         lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
-            in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves, b.control);
+            in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves,
+            reinterpret_cast<float4*>(b.aggregates), b.control);  // the slots hold the centres until aggregation
         mark(1);
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
-            b.leaves, n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
+            reinterpret_cast<const float4*>(b.aggregates), n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
         mark(2);
         if (n <= kSmallSortKeys) {
             // One CTA sorts and gathers (small_sort_kernel).
