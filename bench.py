@@ -584,13 +584,13 @@ def measure_trace(args, world, local, dev, stream, flush):
     return result
 
 
-def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64)):
+def measure_entities(args, world, local, dev, stream, flush, counts=(0, 4, 16, 64)):
     """The cost of entities on the plain trace: the 128^3 world with `n` entities of 2 x 2 x 2
-    bricks each (value noise, half of their bricks emitting: the second light tree), at seeded
-    positions inside the world and rotations, the same 512 x 512, 1 spp, 4 bounces frame. The
-    entities are traversed one after another after the world's bricks (the reference traverses
-    its TLAS), so the cost grows with their count. One flush per count (entity bricks, views,
-    their light tree), then frames timed with CUDA events."""
+    bricks each (value noise) at seeded positions inside the world and rotations, the same
+    512 x 512, 1 spp, 4 bounces frame; each count twice: with half of the entities' bricks emitting
+    (their lights join the light trees) and with none emitting (the entities only add geometry).
+    Rays meet the entities through the entity BVH after the world's bricks. One flush per run
+    (entity bricks, views, light sets), then frames timed with CUDA events."""
     import numpy as np
     import torch
 
@@ -600,11 +600,11 @@ def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64))
     sptr = stream.cuda_stream
     vs = workloads.noise_world()
     out = torch.zeros(TRACE_W * TRACE_H * 3, dtype=torch.float32, device="cuda")
-    rng = np.random.default_rng(17)
-    result = {"workload": "128^3 world + n entities of 2x2x2 bricks (half emitting), 512x512, 1 spp, 4 bounces",
-              "runs": []}
-    for n in counts:
+    result = {"workload": "128^3 world + n entities of 2x2x2 bricks (half of their bricks emitting, or none), "
+                          "512x512, 1 spp, 4 bounces", "runs": []}
+    for n, lit in [(c, l) for c in counts for l in ((True,) if c == 0 else (True, False))]:
         scene = caelix_b200.Scene.from_voxel_scene(dev, vs)
+        rng = np.random.default_rng(17)  # the same entities lit and unlit
         for i in range(n):
             ent = workloads.noise_world(grid_bricks=(2, 2, 2), brick_occupancy=1.0, voxel_fill=0.5,
                                         emissive_fraction=0.0, seed=100 + i)
@@ -612,7 +612,7 @@ def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64))
             e = scene.add_entity(tuple(rng.uniform(8.0, 112.0, 3)), tuple(q / np.linalg.norm(q)))
             scene.upload_bricks(ent.keys, ent.voxels, entity=e)
             power = np.where(rng.random(ent.brick_count) < 0.5, rng.lognormal(0.0, 1.0, ent.brick_count), 0.0)
-            scene.set_brick_power(ent.keys, power.astype(np.float32), entity=e)
+            scene.set_brick_power(ent.keys, (power if lit else 0.0 * power).astype(np.float32), entity=e)
         t0 = time.perf_counter()
         scene.flush(sptr)
         flush_s = time.perf_counter() - t0
@@ -636,8 +636,8 @@ def measure_entities(args, world, local, dev, stream, flush, counts=(4, 16, 64))
             rays += st.primary_rays + st.bounce_rays + st.shadow_rays
             total_ms += a.elapsed_time(b)
         ms = max_over_ranks(total_ms, world) / steps
-        result["runs"].append({"entities": n, "ms_per_frame": ms, "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6,
-                               "flush_wall_s": flush_s})
+        result["runs"].append({"entities": n, "lit": lit, "ms_per_frame": ms, "rays_per_frame": rays / steps,
+                               "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6, "flush_wall_s": flush_s})
         renderer.close()
         scene.close()
     return result
@@ -732,6 +732,12 @@ def measure_large(args, world, local, dev, stream, flush, rank):
         "rays_per_frame": rays / steps,
         "mrays_per_s": world * rays / steps / (ms / 1e3) / 1e6,
     }
+    peak, peak_kind = measured_peaks()
+    achieved = TRACE_BYTES_PER_RAY * (rays / steps) / (ms / 1e3) / 1e9
+    result["roofline"] = {"kernel": "wave_trace_kernel + wave_shade_kernel (the frame)", "bound": "hbm",
+                          "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                          "peak_kind": peak_kind, "traffic": None, "bytes_per_ray": TRACE_BYTES_PER_RAY,
+                          "note": "latency-bound ray traversal; the bytes are a per-ray lower bound"}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # The oracle's trace over the flushed tables (the light tree its own build), on every host
         # core, over a centred pixel window of the same frame; rays counted by the oracle.

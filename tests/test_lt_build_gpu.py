@@ -87,7 +87,7 @@ def test_radix_sort_matches_reference_golden(cuda_device, n):
     assert hashlib.sha256(k.tobytes() + v.tobytes()).digest() == GOLDEN[f"n{n}_sha256"].tobytes()
 
 
-@pytest.mark.parametrize("n", [3, 4095, 4096, 4097, 1 << 22])
+@pytest.mark.parametrize("n", [3, 511, 512, 513, 4095, 4096, 4097, 200000, 1 << 22])
 def test_radix_sort_random_is_stable_sort(cuda_device, n):
     import torch
 
