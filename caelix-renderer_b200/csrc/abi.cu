@@ -375,19 +375,21 @@ CAELIX_API CaelixResult caelix_radix_sort_pairs(CaelixDevice* device, uint32_t* 
     if (count == 0) return CAELIX_OK;
     cudaSetDevice(device->ordinal);
     cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
-    // Scratch: ping-pong keys and values, then the onesweep words.
-    const uint64_t words = 2ull * count + cx::sort_scratch_words(count);
+    // Scratch: ping-pong keys and values, then the onesweep words (for the tile chosen by size).
+    const uint32_t kpt = cx::sort_keys_per_thread_for(count);
+    const uint64_t words = 2ull * count + cx::sort_scratch_words(count, kpt);
     CaelixResult r = device->sort_scratch.reserve(words * 4, "caelix_radix_sort_pairs");
     if (r != CAELIX_OK) return r;
     uint32_t* base = static_cast<uint32_t*>(device->sort_scratch.ptr);
     uint32_t* keys_b = base;
     uint32_t* values_b = base + count;
     uint32_t* scratch = base + 2ull * count;
-    cudaError_t e = cudaMemsetAsync(scratch, 0, cx::sort_scratch_words(count) * 4, s);
+    cudaError_t e = cudaMemsetAsync(scratch, 0, cx::sort_scratch_words(count, kpt) * 4, s);
     if (e != cudaSuccess) return cx::cuda_result(e, "caelix_radix_sort_pairs");
     const uint32_t grid = std::min<uint32_t>((count + 2047) / 2048, device->sm_count * 4);
     cx::radix_histogram(keys, count, scratch, grid, s);
-    cx::onesweep_sort(keys, values, keys_b, values_b, count, identity_values != 0, scratch, device->status, s);
+    cx::onesweep_sort(keys, values, keys_b, values_b, count, identity_values != 0, scratch, device->status, s, nullptr,
+                      kpt);
     e = cudaGetLastError();
     return cx::cuda_result(e, "caelix_radix_sort_pairs");
     CAELIX_GUARD_END
