@@ -252,11 +252,10 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// The leaf summaries in sorted order: sorted[j] = the first 48 bytes of leaves[values[j]], and
-// inverse[values[j]] = j.
+// The leaf summaries in sorted order: sorted[j] = the first 48 bytes of leaves[values[j]].
 __global__ void __launch_bounds__(kThreads)
     lt_gather_kernel(uint32_t n, const uint32_t* __restrict__ values, const LightBvhLeaf* __restrict__ leaves,
-                     LightSummary* __restrict__ sorted, uint32_t* __restrict__ inverse)
+                     LightSummary* __restrict__ sorted)
 {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= n) return;
@@ -267,7 +266,6 @@ __global__ void __launch_bounds__(kThreads)
     dst[0] = r0;
     dst[1] = r1;
     dst[2] = r2;
-    inverse[v] = j;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -502,7 +500,7 @@ __global__ void __launch_bounds__(kScanThreads)
 // ---------------------------------------------------------------------------------------------
 // 4-wide collapse: one thread per 4-wide node w (binary node even[w], at even depth) builds the
 // whole node (224 bytes, its own parent link included: the 4-wide parent is the binary
-// grandparent) in shared memory and writes the parent words of its leaf slots by sorted position;
+// grandparent) in shared memory and writes the parent word of each of its leaf slots into the leaf;
 // the CTA then stores its run of consecutive nodes with coalesced 16-byte writes.
 constexpr uint32_t kWideThreads = 128;
 constexpr uint32_t kNodeWords = sizeof(LightBvhNode) / 4;  // 56
@@ -512,7 +510,7 @@ __global__ void __launch_bounds__(kWideThreads)
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                    const uint32_t* __restrict__ parent, const uint32_t* __restrict__ even,
                    const uint32_t* __restrict__ wide, const LightSummary* __restrict__ sorted,
-                   const AggregateSlot* __restrict__ aggregates, uint32_t* __restrict__ leaf_word,
+                   const AggregateSlot* __restrict__ aggregates, LightBvhLeaf* __restrict__ leaves,
                    LightBvhNode* __restrict__ nodes, const BuildControl* __restrict__ control)
 {
     __shared__ __align__(16) float s_node[kWideThreads * kNodeWords];
@@ -569,8 +567,9 @@ __global__ void __launch_bounds__(kWideThreads)
                 if (slot & kChildLeafBit) {
                     const uint32_t p = slot & ~kChildLeafBit;
                     sm = load_summary(sorted + p);
-                    word = kChildLeafBit | __ldg(values + p);
-                    leaf_word[p] = (w << kParentSlotBits) | c;
+                    const uint32_t leaf = __ldg(values + p);
+                    word = kChildLeafBit | leaf;
+                    leaves[leaf].parent = (w << kParentSlotBits) | c;  // the leaf's parent word, in place
                 } else {
                     sm = load_summary(&aggregates[slot].summary);
                     word = __ldg(wide + slot);
@@ -595,23 +594,6 @@ __global__ void __launch_bounds__(kWideThreads)
     const float4* src = reinterpret_cast<const float4*>(s_node);
     float4* dst = reinterpret_cast<float4*>(nodes + w_base);
     for (uint32_t q = threadIdx.x; q < quads; q += kWideThreads) dst[q] = src[q];
-}
-
-// The parent words of the leaves in leaf (record) order: the second 32-byte sector of every leaf
-// is rewritten whole (lo.z, hi, group, entry, pad, parent), so no partial sector is written.
-__global__ void __launch_bounds__(kThreads)
-    lt_leaf_parent_kernel(uint32_t n, const uint32_t* __restrict__ inverse, const uint32_t* __restrict__ leaf_word,
-                          LightBvhLeaf* __restrict__ leaves)
-{
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const uint32_t word = __ldg(leaf_word + __ldg(inverse + i));
-    uint4* sector = reinterpret_cast<uint4*>(leaves + i) + 2;
-    const uint4 a = sector[0];
-    uint4 b = sector[1];
-    b.w = word;
-    sector[0] = a;
-    sector[1] = b;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -780,7 +762,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
             onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
                           stream, nullptr, kpt);
             lt_gather_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.values, b.leaves,
-                                                                                        b.sorted, b.inverse);
+                                                                                        b.sorted);
         }
         mark(3);
     } else {
@@ -807,9 +789,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         mark(6);
         lt_wide_kernel<<<grid_for(nodes, kWideThreads, 1u << 30), kWideThreads, 0, stream>>>(
             n, b.node_capacity, b.values, b.left, b.right, b.parent, b.keys_alt, b.wide, b.sorted, b.aggregates,
-            b.leaf_word, b.nodes, b.control);
-        lt_leaf_parent_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.inverse, b.leaf_word,
-                                                                                        b.leaves);
+            b.leaves, b.nodes, b.control);
     } else {
         mark(4);
         mark(5);
@@ -823,11 +803,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
 
 uint32_t lt_kernel_launches(uint32_t n)
 {
-    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the six tree
+    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the five tree
     // kernels from two leaves, finish.
     if (n == 0) return 1;
     const uint32_t sort = n <= kSmallSortKeys ? 1u : 5u;
-    return 2 + sort + (n >= 2 ? 6u : 0u) + 1;
+    return 2 + sort + (n >= 2 ? 5u : 0u) + 1;
 }
 
 }  // namespace cx
