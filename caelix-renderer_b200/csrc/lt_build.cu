@@ -673,7 +673,7 @@ uint64_t lt_buffer_bytes(uint32_t cap)
     b += align256(c * sizeof(LightBvhLeaf));
     b += align256(c * sizeof(LightBvhNode));  // node capacity = leaf capacity (>= n - 1 nodes)
     b += align256(128);                       // header + state
-    b += 14 * align256(c * 4);                // u32 arrays
+    b += 12 * align256(c * 4);                // u32 arrays
     b += align256(c * sizeof(AggregateSlot));
     b += align256(c * sizeof(LightSummary));
     b += align256(zero_words((uint32_t)c, kSortMinKeysPerThread) * 4);
@@ -710,8 +710,6 @@ LightBvhBuffers lt_carve(void* base, uint32_t cap)
     b.depth = u32();
     b.wide = u32();
     b.cover = u32();
-    b.inverse = u32();
-    b.leaf_word = u32();
     b.aggregates = reinterpret_cast<AggregateSlot*>(take(c * sizeof(AggregateSlot)));
     b.sorted = reinterpret_cast<LightSummary*>(take(c * sizeof(LightSummary)));
     char* z = take(zero_words((uint32_t)c, kSortMinKeysPerThread) * 4);
@@ -753,7 +751,7 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
             gather.rows_in = reinterpret_cast<const uint4*>(b.leaves);
             gather.rows_in_stride = sizeof(LightBvhLeaf) / sizeof(uint4);
             gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
-            gather.inverse = b.inverse;
+            gather.inverse = nullptr;
             onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
                           stream, &gather, kpt);
         } else {

@@ -93,8 +93,6 @@ struct LightBvhBuffers
     uint32_t* depth = nullptr;
     uint32_t* wide = nullptr;
     uint32_t* cover = nullptr;      // range-count differences, then the nodes over each leaf boundary
-    uint32_t* inverse = nullptr;    // sorted position of every leaf
-    uint32_t* leaf_word = nullptr;  // parent word of the leaf at every sorted position
     AggregateSlot* aggregates = nullptr;
     LightSummary* sorted = nullptr;  // leaf summaries in sorted order
     BuildControl* control = nullptr;  // followed by the sort scratch, then the scan states

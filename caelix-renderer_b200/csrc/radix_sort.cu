@@ -38,7 +38,7 @@ struct SortPass
     const uint4* rows_in;  // gathering pass: 48-byte rows by value (stride rows_in_stride uint4), else nullptr
     uint32_t rows_in_stride;
     uint4* rows_out;       // 48-byte rows by destination
-    uint32_t* inverse;     // inverse[value] = destination
+    uint32_t* inverse;     // inverse[value] = destination (null: not written)
     uint32_t silent_tile;  // a tile that publishes no status (SortWaitTest), else 0xFFFFFFFF
     uint32_t spin_limit;   // polls of a look-back wait before it gives up
 };
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(kSortThreads, 4) onesweep_pass_kernel(const So
             dst[0] = r0;
             dst[1] = r1;
             dst[2] = r2;
-            a.inverse[v] = dest;
+            if (a.inverse) a.inverse[v] = dest;
         }
     }
 }
@@ -436,7 +436,7 @@ __global__ void __launch_bounds__(kSortThreads, 2) onesweep_pipe_kernel(const So
                 dst[0] = r0;
                 dst[1] = r1;
                 dst[2] = r2;
-                a.inverse[v] = dest;
+                if (a.inverse) a.inverse[v] = dest;
             }
         }
         __syncthreads();
@@ -518,7 +518,7 @@ __global__ void __launch_bounds__(kSortThreads) small_sort_kernel(uint32_t* __re
             dst[0] = __ldg(src);
             dst[1] = __ldg(src + 1);
             dst[2] = __ldg(src + 2);
-            gather.inverse[v] = i;
+            if (gather.inverse) gather.inverse[v] = i;
         }
     }
 }
@@ -557,7 +557,7 @@ __global__ void __launch_bounds__(kSortThreads) rank_sort_kernel(uint32_t* __res
             dst[0] = __ldg(src);
             dst[1] = __ldg(src + 1);
             dst[2] = __ldg(src + 2);
-            gather.inverse[v] = r;
+            if (gather.inverse) gather.inverse[v] = r;
         }
     }
 }

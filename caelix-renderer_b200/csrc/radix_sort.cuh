@@ -74,8 +74,8 @@ uint32_t current_sm_count();
 void radix_histogram(const uint32_t* keys, uint32_t n, uint32_t* hist, uint32_t grid, cudaStream_t stream);
 
 // An optional gather fused into the last pass: the 48-byte row at rows_in + rows_in_stride * value
-// (in uint4 units) of every element is copied to rows_out[destination] (48-byte rows), and
-// inverse[value] = destination.
+// (in uint4 units) of every element is copied to rows_out[destination] (48-byte rows), and, when
+// inverse is not null, inverse[value] = destination.
 struct SortGather
 {
     const uint4* rows_in;
