@@ -349,7 +349,12 @@ __device__ __forceinline__ void entity_candidate(const SceneView& s, uint32_t e,
         ol[k] = R[k] * q[0] + R[3 + k] * q[1] + R[6 + k] * q[2];
         dl[k] = R[k] * d[0] + R[3 + k] * d[1] + R[6 + k] * d[2];
     }
-    const Hit he = trace_ray_body(E.scene, ol, dl, tmin_ray, h.hit ? h.t : tmax_ray);
+    // A hit must be nearer than the current one; at an equal distance the lower entity index wins
+    // against an entity hit (the world's hit always wins a tie), so the result does not depend on
+    // the order in which the entities are taken.
+    const bool tie_wins = h.hit && (h.attrib & kEntityHit) && e < (h.group >> kEntityShift);
+    const float t_limit = h.hit ? (tie_wins ? nextafterf(h.t, INFINITY) : h.t) : tmax_ray;
+    const Hit he = trace_ray_body(E.scene, ol, dl, tmin_ray, t_limit);
     if (!he.hit) return;
     h = he;
     h.attrib |= kEntityHit;
@@ -364,11 +369,13 @@ __device__ __forceinline__ void entity_candidate(const SceneView& s, uint32_t e,
     for (int i = 0; i < 3; ++i) h.normal[i] = v[i] * inv;
 }
 
-// The entities after the world's bricks, in index order (entity_candidate): every entity, or with
+// The entities after the world's bricks (entity_candidate): every entity in index order, or with
 // the scene's entity BVH only those whose box the ray meets before the current hit (collected by a
-// traversal of the BVH over the entities' bounding-sphere boxes, then taken in index order, so the
-// hit is the one the loop over every entity finds: the nearest, ties to the world and then to the
-// lower index). More candidates than the list holds: every entity.
+// traversal of the BVH over the entities' bounding-sphere boxes, then taken in order of their boxes'
+// entry distance, so that a near hit culls the farther candidates; entity_candidate's tie rule
+// makes the hit the one the loop over every entity finds: the nearest, ties to the world and then to
+// the lower index). More candidates than the list holds: every entity. `any`: an occlusion test,
+// which stops at the first hit (a shadow ray needs only whether something is hit).
 constexpr uint32_t kEntityCandidates = 16;
 constexpr uint32_t kEntityStack = 32;
 
@@ -383,6 +390,7 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
         const float t_lo = tmin_ray - 1e-3f * (1.0f + fabsf(tmin_ray));
         const float t_hi = t_far + 1e-3f * (1.0f + fabsf(t_far));
         uint32_t cand[kEntityCandidates];
+        float cand_t[kEntityCandidates];  // the entry distance of each candidate's box
         uint32_t stack[kEntityStack];
         uint32_t n = 0, sp = 0;
         bool overflow = false;
@@ -403,8 +411,12 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
             if (!(t0 <= t1)) continue;
             const uint32_t first = __float_as_uint(a.w), second = __float_as_uint(b.w);
             if (first & kEntityLeaf) {
-                if (n < kEntityCandidates) cand[n++] = first & ~kEntityLeaf;
-                else overflow = true;
+                if (n < kEntityCandidates) {
+                    cand[n] = first & ~kEntityLeaf;
+                    cand_t[n++] = t0;
+                } else {
+                    overflow = true;
+                }
             } else if (sp + 2 <= kEntityStack) {
                 stack[sp++] = second;
                 stack[sp++] = first;
@@ -413,12 +425,18 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
             }
         }
         if (!overflow) {
-            // Index order (an insertion sort of at most kEntityCandidates).
+            // Nearest box first (an insertion sort of at most kEntityCandidates by entry distance,
+            // then index).
             for (uint32_t x = 1; x < n; ++x) {
                 const uint32_t v = cand[x];
+                const float tv = cand_t[x];
                 uint32_t y = x;
-                for (; y > 0 && cand[y - 1] > v; --y) cand[y] = cand[y - 1];
+                for (; y > 0 && (cand_t[y - 1] > tv || (cand_t[y - 1] == tv && cand[y - 1] > v)); --y) {
+                    cand[y] = cand[y - 1];
+                    cand_t[y] = cand_t[y - 1];
+                }
                 cand[y] = v;
+                cand_t[y] = tv;
             }
             for (uint32_t x = 0; x < n && !(any && h.hit); ++x) entity_candidate(s, cand[x], o, d, tmin_ray, tmax_ray, h);
             return;
