@@ -370,34 +370,14 @@ __device__ __forceinline__ void entity_candidate(const SceneView& s, uint32_t e,
 }
 
 // The entities after the world's bricks (entity_candidate): every entity in index order, or with
-// the scene's entity BVH (boxes round the entities' bounding spheres) a closest-first traversal:
-// at a node both children's boxes are tested against the ray up to the current hit, the nearer is
-// taken and the farther pushed (and tested again when popped, against the hit found meanwhile), a
-// leaf's entity traced at once. entity_candidate's tie rule (the world wins a tie, then the lower
-// entity index) makes the hit the one the loop over every entity finds, whatever the order. `any`:
-// an occlusion test, which stops at the first hit (a shadow ray needs only whether something is hit).
-constexpr uint32_t kEntityStack = 32;  // a median-split BVH of fewer than 2^32 entities is shallower
-
-__device__ __forceinline__ bool entity_box(const SceneView& s, uint32_t node, const float o[3], const float inv[3],
-                                           float t_lo, float t_hi, float& t0, uint32_t& first, uint32_t& second)
-{
-    const EntityNode& N = s.entity_nodes[node];
-    const float4 a = __ldg(reinterpret_cast<const float4*>(&N));
-    const float4 b = __ldg(reinterpret_cast<const float4*>(&N) + 1);
-    const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
-    float t1 = t_hi;
-    t0 = t_lo;
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        const float ta = (lo[k] - o[k]) * inv[k];
-        const float tb = (hi[k] - o[k]) * inv[k];
-        t0 = hmax(t0, hmin(ta, tb));
-        t1 = hmin(t1, hmax(ta, tb));
-    }
-    first = __float_as_uint(a.w);
-    second = __float_as_uint(b.w);
-    return t0 <= t1;
-}
+// the scene's entity BVH only those whose box the ray meets before the current hit (collected by a
+// traversal of the BVH over the entities' bounding-sphere boxes, then taken in order of their boxes'
+// entry distance, so that a near hit culls the farther candidates; entity_candidate's tie rule
+// makes the hit the one the loop over every entity finds: the nearest, ties to the world and then to
+// the lower index). More candidates than the list holds: every entity. `any`: an occlusion test,
+// which stops at the first hit (a shadow ray needs only whether something is hit).
+constexpr uint32_t kEntityCandidates = 16;
+constexpr uint32_t kEntityStack = 32;
 
 __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3], const float d[3], float tmin_ray,
                                             float tmax_ray, Hit& h, bool any = false)
@@ -406,57 +386,61 @@ __device__ __noinline__ void trace_entities(const SceneView& s, const float o[3]
         float inv[3];
 #pragma unroll
         for (int k = 0; k < 3; ++k) inv[k] = safe_inv_axis(d[k]);
-        // The slab margins cover the rounding (the box test only skips work, it never changes a hit).
+        const float t_far = h.hit ? h.t : tmax_ray;
         const float t_lo = tmin_ray - 1e-3f * (1.0f + fabsf(tmin_ray));
-        const auto t_hi = [&]() {
-            const float t_far = h.hit ? h.t : tmax_ray;
-            return t_far + 1e-3f * (1.0f + fabsf(t_far));
-        };
+        const float t_hi = t_far + 1e-3f * (1.0f + fabsf(t_far));
+        uint32_t cand[kEntityCandidates];
+        float cand_t[kEntityCandidates];  // the entry distance of each candidate's box
         uint32_t stack[kEntityStack];
-        uint32_t sp = 0;
-        float t0;
-        uint32_t first, second;
-        bool live = entity_box(s, 0, o, inv, t_lo, t_hi(), t0, first, second);
+        uint32_t n = 0, sp = 0;
         bool overflow = false;
-        while ((live || sp) && !overflow) {
-            if (!live) {
-                live = entity_box(s, stack[--sp], o, inv, t_lo, t_hi(), t0, first, second);
-                continue;
+        stack[sp++] = 0;
+        while (sp && !overflow) {
+            const EntityNode& N = s.entity_nodes[stack[--sp]];
+            const float4 a = __ldg(reinterpret_cast<const float4*>(&N));
+            const float4 b = __ldg(reinterpret_cast<const float4*>(&N) + 1);
+            const float lo[3] = {a.x, a.y, a.z}, hi[3] = {b.x, b.y, b.z};
+            float t0 = t_lo, t1 = t_hi;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const float ta = (lo[k] - o[k]) * inv[k];
+                const float tb = (hi[k] - o[k]) * inv[k];
+                t0 = hmax(t0, hmin(ta, tb));
+                t1 = hmin(t1, hmax(ta, tb));
             }
+            if (!(t0 <= t1)) continue;
+            const uint32_t first = __float_as_uint(a.w), second = __float_as_uint(b.w);
             if (first & kEntityLeaf) {
-                entity_candidate(s, first & ~kEntityLeaf, o, d, tmin_ray, tmax_ray, h);
-                if (any && h.hit) return;
-                live = false;
-                continue;
-            }
-            float ta, tb;
-            uint32_t fa, sa, fb, sb;
-            const float limit = t_hi();
-            const bool ha = entity_box(s, first, o, inv, t_lo, limit, ta, fa, sa);
-            const bool hb = entity_box(s, second, o, inv, t_lo, limit, tb, fb, sb);
-            if (ha && hb) {
-                if (sp == kEntityStack) {
+                if (n < kEntityCandidates) {
+                    cand[n] = first & ~kEntityLeaf;
+                    cand_t[n++] = t0;
+                } else {
                     overflow = true;
-                    break;
                 }
-                const bool a_near = ta <= tb;
-                stack[sp++] = a_near ? second : first;
-                t0 = a_near ? ta : tb;
-                first = a_near ? fa : fb;
-                second = a_near ? sa : sb;
-            } else if (ha) {
-                t0 = ta;
-                first = fa;
-                second = sa;
-            } else if (hb) {
-                t0 = tb;
-                first = fb;
-                second = sb;
+            } else if (sp + 2 <= kEntityStack) {
+                stack[sp++] = second;
+                stack[sp++] = first;
             } else {
-                live = false;
+                overflow = true;
             }
         }
-        if (!overflow) return;
+        if (!overflow) {
+            // Nearest box first (an insertion sort of at most kEntityCandidates by entry distance,
+            // then index).
+            for (uint32_t x = 1; x < n; ++x) {
+                const uint32_t v = cand[x];
+                const float tv = cand_t[x];
+                uint32_t y = x;
+                for (; y > 0 && (cand_t[y - 1] > tv || (cand_t[y - 1] == tv && cand[y - 1] > v)); --y) {
+                    cand[y] = cand[y - 1];
+                    cand_t[y] = cand_t[y - 1];
+                }
+                cand[y] = v;
+                cand_t[y] = tv;
+            }
+            for (uint32_t x = 0; x < n && !(any && h.hit); ++x) entity_candidate(s, cand[x], o, d, tmin_ray, tmax_ray, h);
+            return;
+        }
     }
     for (uint32_t e = 0; e < s.entity_count && !(any && h.hit); ++e) entity_candidate(s, e, o, d, tmin_ray, tmax_ray, h);
 }
