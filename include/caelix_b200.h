@@ -302,12 +302,12 @@ typedef struct CaelixEntityDesc
 /* Adds an entity with no bricks: world = R(rotation) * local + position, local = the
    entity-local block coordinate. Its bricks are traced (closest hit over the world and every
    entity, ties to the world and then to the lower id) and shaded with the scene's materials. Its
-   light voxels (the scene's light codes, in bricks with power above 0) are lights of the second
-   light tree (the reference's dynamic tree, docs/LIGHT_TREE.md:136-176): the entities' light
-   records merged in id order under their transforms, rebuilt at a flush after any entity change or
-   move, while the world's tree (tree 0) stays; NEE picks between the two trees by importance.
-   Every added entity's lights go to that tree whatever its motion (the reference puts static
-   entities' lights in tree 0). Takes effect at the next flush. */
+   light voxels (the scene's light codes, in bricks with power above 0) are lights of one of the two
+   light trees, as in the reference (docs/LIGHT_TREE.md:136-176): a static entity's (the default
+   motion) join the world's in tree 0, a dynamic entity's the second tree, each tree's records
+   merged in id order under the entities' transforms and rebuilt at a flush after any change of
+   its lights or a move; NEE picks between the two trees by importance. Takes effect at the next
+   flush. */
 CAELIX_API CaelixResult caelix_scene_add_entity(CaelixScene* scene, const CaelixEntityDesc* desc,
                                                 CaelixEntityId* out_id);
 /* Removes the entity and all its bricks at once (waiting for the device first). */
@@ -316,10 +316,9 @@ CAELIX_API CaelixResult caelix_scene_remove_entity(CaelixScene* scene, CaelixEnt
    the normalised quaternion and rounded to float. */
 CAELIX_API CaelixResult caelix_scene_set_entity_transform(CaelixScene* scene, CaelixEntityId entity,
                                                           const float position[3], const float rotation[4]);
-/* Entity motion (the reference uses it only to pick the light tree of an entity's lights; here
-   every added entity's lights are in the dynamic tree, so the value is stored and has no effect).
-   Other values than CAELIX_ENTITY_STATIC / CAELIX_ENTITY_DYNAMIC return
-   CAELIX_ERROR_INVALID_ARGUMENT. */
+/* Entity motion (include/caelix/caelix.h:322-332): it picks the light tree of the entity's lights,
+   tree 0 for CAELIX_ENTITY_STATIC (a new entity's), the dynamic tree for CAELIX_ENTITY_DYNAMIC;
+   takes effect at the next flush. Other values return CAELIX_ERROR_INVALID_ARGUMENT. */
 #define CAELIX_ENTITY_STATIC 0u
 #define CAELIX_ENTITY_DYNAMIC 1u
 CAELIX_API CaelixResult caelix_scene_set_entity_motion(CaelixScene* scene, CaelixEntityId entity, uint32_t motion);
