@@ -35,31 +35,15 @@ constexpr uint32_t kFlagPrimary = 1u << 11;   // that extension ray is the camer
 // the trace and shade launches' fetch counters of the two parities.
 constexpr uint32_t kFetchTrace = 4, kFetchShade = 6;
 
-// The 32-item chunks of a queue that the calling warp processes, taken kFetchGroups at a time from
-// a fetch counter: a warp that is done with its chunks takes the next ones, so the work of a launch
-// whose items' costs differ widely spreads over the warps until its end, with one atomic per
-// 32 * kFetchGroups items. Every lane calls; the chunks start below the queue's end until the first
-// that does not (the counter only grows, so no chunk below the end is left out).
-constexpr uint32_t kFetchGroups = 4;
-struct ChunkCursor
+// The next 32-item chunk of a queue for the calling warp, from a fetch counter. A warp that is done
+// with its chunk takes the next one, so the work of a launch whose items' costs differ widely
+// spreads over the warps until its end. Every lane calls.
+__device__ __forceinline__ uint32_t fetch_chunk(uint32_t* counter)
 {
-    uint32_t* counter;
-    uint32_t base;
-    uint32_t left;
-    __device__ __forceinline__ uint32_t fetch()
-    {
-        uint32_t b = 0;
-        if ((threadIdx.x & 31u) == 0) b = atomicAdd(counter, 32u * kFetchGroups);
-        left = kFetchGroups - 1;
-        return base = __shfl_sync(0xFFFFFFFFu, b, 0);
-    }
-    __device__ __forceinline__ uint32_t next()
-    {
-        if (left == 0) return fetch();
-        --left;
-        return base += 32u;
-    }
-};
+    uint32_t base = 0;
+    if ((threadIdx.x & 31u) == 0) base = atomicAdd(counter, 32u);
+    return __shfl_sync(0xFFFFFFFFu, base, 0);
+}
 
 struct WaveGen
 {
@@ -141,7 +125,7 @@ __global__ void __launch_bounds__(kWaveThreads)
 
 // kEntities: the views' scenes have entities (traversed after the world's bricks); the variant
 // without them keeps the world-only DDA's registers (no out-of-line call). kDynamic: warps take
-// chunks of the queue from a fetch counter (ChunkCursor) instead of a fixed grid stride: faster
+// chunks of the queue from a fetch counter (fetch_chunk) instead of a fixed grid stride: faster
 // where ray costs spread widely (entities, scenes whose records do not stay in L2), slower on the
 // small resident scene, where the fixed stride is kept.
 template <bool kEntities, bool kDynamic>
@@ -156,9 +140,9 @@ __global__ void __launch_bounds__(kWaveThreads)
     }
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t stride = gridDim.x * kWaveThreads;
-    ChunkCursor chunks{&b.counts[kFetchTrace + parity], 0, 0};
-    for (uint32_t base = kDynamic ? chunks.fetch() : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
-         base = kDynamic ? chunks.next() : base + stride) {
+    uint32_t* const fetch = &b.counts[kFetchTrace + parity];
+    for (uint32_t base = kDynamic ? fetch_chunk(fetch) : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
+         base = kDynamic ? fetch_chunk(fetch) : base + stride) {
         const uint32_t i = base + lane;
         uint32_t key = 0xFFFFFFFFu;
         if (i < n) {
@@ -251,9 +235,9 @@ __global__ void __launch_bounds__(kWaveThreads, kMinBlocks)
     // Chunks from a fetch counter (as in wave_trace_kernel) for scenes with entities or records that
     // do not stay in L2 (the 8-CTA variants); the fixed stride for the resident scene.
     constexpr bool kDynamic = kEntities || kMinBlocks == 8;
-    ChunkCursor chunks{&b.counts[kFetchShade + parity], 0, 0};
-    for (uint32_t base = kDynamic ? chunks.fetch() : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
-         base = kDynamic ? chunks.next() : base + stride) {
+    uint32_t* const fetch = &b.counts[kFetchShade + parity];
+    for (uint32_t base = kDynamic ? fetch_chunk(fetch) : blockIdx.x * kWaveThreads + (threadIdx.x & ~31u); base < n;
+         base = kDynamic ? fetch_chunk(fetch) : base + stride) {
         const uint32_t i = base + lane;
         uint32_t slot = 0, next_flags = 0;
         bool live = false, shadow = false, ext = false;
