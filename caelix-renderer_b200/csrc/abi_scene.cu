@@ -541,6 +541,7 @@ CAELIX_API void caelix_scene_destroy(CaelixScene* scene)
     scene->record_of_slot.release();
     scene->marks.release();
     scene->update.release();
+    if (scene->edit_host) cudaFreeHost(scene->edit_host);
     if (scene->upload_stream) cudaStreamDestroy(scene->upload_stream);
     if (scene->start) cudaEventDestroy(scene->start);
     if (scene->stop) cudaEventDestroy(scene->stop);
@@ -1008,7 +1009,18 @@ static CaelixResult scene_flush_body(CaelixScene* scene, const CaelixFrameDesc* 
         cudaEventRecord(scene->start, stream);
         if (edits) {
             const uint32_t c = (uint32_t)scene->dirty_slots.size();
-            std::vector<uint32_t> host(2ull * c);
+            // The slots and their power go up from pinned memory (a copy from pageable memory
+            // waits for the stream first); the previous flush has finished with the buffer.
+            if (scene->edit_host_words < 2ull * c) {
+                if (scene->edit_host) cudaFreeHost(scene->edit_host);
+                scene->edit_host = nullptr;
+                scene->edit_host_words = 0;
+                const uint64_t words = 2ull * c + c / 4;
+                e = cudaHostAlloc(reinterpret_cast<void**>(&scene->edit_host), 4ull * words, cudaHostAllocDefault);
+                if (e != cudaSuccess) return cx::cuda_result(e, "caelix_scene_flush");
+                scene->edit_host_words = words;
+            }
+            uint32_t* host = scene->edit_host;
             for (uint32_t i = 0; i < c; ++i) {
                 const uint32_t slot = scene->dirty_slots[i];
                 const float p = scene->slot_power[slot];
@@ -1026,7 +1038,7 @@ static CaelixResult scene_flush_body(CaelixScene* scene, const CaelixFrameDesc* 
                 scene->mark_epoch = 1;
             }
             if (e == cudaSuccess)
-                e = cudaMemcpyAsync(d_slots, host.data(), 8ull * c, cudaMemcpyHostToDevice, stream);
+                e = cudaMemcpyAsync(d_slots, host, 8ull * c, cudaMemcpyHostToDevice, stream);
             if (e == cudaSuccess) e = cudaMemsetAsync(d_count, 0, 4, stream);
             // The build's status words and counters start from zero, as in a full build.
             if (e == cudaSuccess) e = cudaMemsetAsync(scene->dev.status, 0, 64, stream);
@@ -1036,12 +1048,14 @@ static CaelixResult scene_flush_body(CaelixScene* scene, const CaelixFrameDesc* 
                                        static_cast<uint32_t*>(scene->marks.ptr), scene->mark_epoch, d_list, d_count,
                                        stream);
             if (e == cudaSuccess) e = cx::scene_refinalize(scene->dev, d_list, d_count, 7 * c, stream);
+            // The refinalized record count, read back with the build's own reads (which wait for
+            // the stream).
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(scene->dev.pinned + 4, d_count, 4, cudaMemcpyDeviceToHost, stream);
             if (e == cudaSuccess)
                 e = cx::scene_build_lights(scene->dev, stream, &status, static_cast<const uint32_t*>(scene->marks.ptr),
                                            scene->mark_epoch);
-            if (e == cudaSuccess)
-                e = cudaMemcpyAsync(&scene->last_update_records, d_count, 4, cudaMemcpyDeviceToHost, stream);
-            if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+            if (e == cudaSuccess) scene->last_update_records = scene->dev.pinned[4];
         } else if (scene->light_tree_dirty) {
             e = cx::scene_build_light_tree(scene->dev, stream);
             if (e == cudaSuccess) e = cx::scene_read_status(scene->dev, stream, &status);

@@ -70,6 +70,8 @@ struct CaelixScene
     cx::GrowBuffer marks;           // device: one word per brick (staging_update)
     uint32_t mark_epoch = 0;
     cx::GrowBuffer update;          // device: edited slots, their power, the refinalize list
+    uint32_t* edit_host = nullptr;  // pinned host: an edit flush's slots and their power
+    uint64_t edit_host_words = 0;
     uint32_t last_update_records = 0;  // records finalized again by the last incremental flush
     // The material table (host copy, one entry per 16-bit code), its device form (two float4 per
     // code: albedo, emission) and the light code set (codes whose emission luminance reaches

@@ -976,12 +976,14 @@ void scene_release(DeviceScene& s)
                     s.tree_memory,   s.status,       s.heap_prev,    s.unit_of_brick, s.unit_of_brick_prev};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    if (s.pinned) cudaFreeHost(s.pinned);
     s = DeviceScene();
 }
 
 cudaError_t scene_alloc_inputs(DeviceScene& s, uint32_t n, cudaStream_t stream)
 {
     if (!s.status) CX_TRY(cudaMalloc(&s.status, 64));
+    if (!s.pinned) CX_TRY(cudaHostAlloc(reinterpret_cast<void**>(&s.pinned), 32, cudaHostAllocDefault));
     CX_TRY(cudaMemsetAsync(s.status, 0, 64, stream));
     CX_TRY(alloc(s.keys, s.capacity.keys, 3ull * n));
     CX_TRY(alloc(s.voxels, s.capacity.voxels, 512ull * n));
@@ -1132,9 +1134,9 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
             light_collect_kernel<kEncodingBlockId>
                 <<<blocks_for(n, kThreads), kThreads, 0, stream>>>(la, d_light_count, lkeys, lbricks);
     }
-    uint32_t m = 0;
-    CX_TRY(cudaMemcpyAsync(&m, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaMemcpyAsync(s.pinned, d_light_count, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
+    const uint32_t m = s.pinned[0];
     s.light_count = m;
     CX_TRY(alloc(s.group_rows, s.capacity.group_rows, 8ull * s.group_count));
     CX_TRY(cudaMemsetAsync(s.group_rows, 0, 32ull * s.group_count, stream));
@@ -1142,20 +1144,33 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
     CX_TRY(alloc(s.light_group, s.capacity.light_group, m));
     CX_TRY(alloc(s.light_entry, s.capacity.light_entry, m));
     CX_TRY(alloc(s.light_brick, s.capacity.light_brick, m));
-    std::vector<GroupFrame> frames(s.group_count);
-    for (uint32_t g = 0; g < s.group_count; ++g) {
-        const uint32_t gx = g % s.groups[0], gy = (g / s.groups[0]) % s.groups[1], gz = g / (s.groups[0] * s.groups[1]);
-        GroupFrame f;
-        std::memset(&f, 0, sizeof(f));
-        // The group's voxel origin in the scene: (grid origin + group cell * group edge) * 8.
-        const uint32_t cell[3] = {gx, gy, gz};
-        for (int k = 0; k < 3; ++k)
-            f.origin[k] = (float)(8ll * ((int64_t)s.origin[k] + ((int64_t)cell[k] << group_shift)));
-        f.rot[0] = f.rot[4] = f.rot[8] = 1.0f;
-        frames[g] = f;
-    }
+    // The group frames (their origins follow from the grid origin and the group grid; identity
+    // rotations): uploaded when the grid changed or their buffer moved.
+    GroupFrame* const old_frames = s.frames;
     CX_TRY(alloc(s.frames, s.capacity.frames, s.group_count));
-    CX_TRY(cudaMemcpyAsync(s.frames, frames.data(), sizeof(GroupFrame) * s.group_count, cudaMemcpyHostToDevice, stream));
+    const bool same_frames = s.frames == old_frames && s.frames_shift == group_shift &&
+                             std::memcmp(s.frames_origin, s.origin, sizeof(s.frames_origin)) == 0 &&
+                             std::memcmp(s.frames_groups, s.groups, sizeof(s.frames_groups)) == 0;
+    if (!same_frames) {
+        std::vector<GroupFrame> frames(s.group_count);
+        for (uint32_t g = 0; g < s.group_count; ++g) {
+            const uint32_t gx = g % s.groups[0], gy = (g / s.groups[0]) % s.groups[1],
+                           gz = g / (s.groups[0] * s.groups[1]);
+            GroupFrame f;
+            std::memset(&f, 0, sizeof(f));
+            // The group's voxel origin in the scene: (grid origin + group cell * group edge) * 8.
+            const uint32_t cell[3] = {gx, gy, gz};
+            for (int k = 0; k < 3; ++k)
+                f.origin[k] = (float)(8ll * ((int64_t)s.origin[k] + ((int64_t)cell[k] << group_shift)));
+            f.rot[0] = f.rot[4] = f.rot[8] = 1.0f;
+            frames[g] = f;
+        }
+        CX_TRY(cudaMemcpyAsync(s.frames, frames.data(), sizeof(GroupFrame) * s.group_count, cudaMemcpyHostToDevice,
+                               stream));
+        std::memcpy(s.frames_origin, s.origin, sizeof(s.frames_origin));
+        std::memcpy(s.frames_groups, s.groups, sizeof(s.frames_groups));
+        s.frames_shift = group_shift;
+    }
     uint32_t total_units = 0;
     if (m > 0) {
         const uint32_t light_kpt = sort_keys_per_thread_for(m);
@@ -1179,11 +1194,14 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
                                                                              group_start, group_end);
         uint32_t* d_total = s.status + 6;
         CX_TRY(run_scan(false, totals, offsets, m, small, d_total, s.status, stream));
-        CX_TRY(cudaMemcpyAsync(&total_units, d_total, 4, cudaMemcpyDeviceToHost, stream));
+        CX_TRY(cudaMemcpyAsync(s.pinned + 1, d_total, 4, cudaMemcpyDeviceToHost, stream));
         CX_TRY(cudaStreamSynchronize(stream));
+        total_units = s.pinned[1];
         s.heap_words = 4 * (1 + total_units);
         CX_TRY(alloc(s.heap, s.capacity.heap, s.heap_words));
-        CX_TRY(cudaMemsetAsync(s.heap, 0, 4ull * s.heap_words, stream));
+        // Unit 0 is reserved (zero); light_write_kernel writes every other unit (block headers,
+        // index entries, records with their padding).
+        CX_TRY(cudaMemsetAsync(s.heap, 0, 16, stream));
         LightWriteArgs wa{la,           lkeys,         lbricks,         m,           counts6,
                           units,        offsets,       group_start,     group_end,   total_units, s.heap,
                           s.group_rows, s.light_headers, s.light_group, s.light_entry, s.light_brick,
@@ -1236,11 +1254,11 @@ cudaError_t scene_build_light_tree(const DeviceScene& s, cudaStream_t stream, ui
 
 cudaError_t scene_read_status(const DeviceScene& s, cudaStream_t stream, uint32_t* device_status_out)
 {
-    uint32_t status[2] = {0, 0};
-    CX_TRY(cudaMemcpyAsync(status, s.status, 4, cudaMemcpyDeviceToHost, stream));
-    CX_TRY(cudaMemcpyAsync(status + 1, &s.tree.state->status, 4, cudaMemcpyDeviceToHost, stream));
+    if (!s.status || !s.pinned) return cudaErrorInvalidValue;  // never built
+    CX_TRY(cudaMemcpyAsync(s.pinned + 2, s.status, 4, cudaMemcpyDeviceToHost, stream));
+    CX_TRY(cudaMemcpyAsync(s.pinned + 3, &s.tree.state->status, 4, cudaMemcpyDeviceToHost, stream));
     CX_TRY(cudaStreamSynchronize(stream));
-    if (device_status_out) *device_status_out = status[0] | status[1];
+    if (device_status_out) *device_status_out = s.pinned[2] | s.pinned[3];
     return cudaGetLastError();
 }
 

@@ -161,6 +161,13 @@ struct DeviceScene
     LightBvhBuffers tree;
     uint32_t tree_capacity = 0;
     uint32_t* status = nullptr;  // device status word of the build
+    // Pinned host words the build reads back into (a read into pageable memory waits for the
+    // device at every copy): [0] light count, [1] heap units, [2] [3] status words, [4] free.
+    uint32_t* pinned = nullptr;
+    // The group frames on the device were made for this origin, group grid and group edge.
+    int32_t frames_origin[3] = {0, 0, 0};
+    uint32_t frames_groups[3] = {0, 0, 0};
+    uint32_t frames_shift = ~0u;
     // The light records kept for the next rebuild over the same bricks: the first unit of every
     // brick's light record in `heap` (0xFFFFFFFF: none), and the previous heap and map (the
     // buffers a rebuild over the same bricks copies unchanged records from, then swaps).
