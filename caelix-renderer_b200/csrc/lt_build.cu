@@ -328,11 +328,19 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------------------------
 // Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
 // computes its summary from both children and goes on. A CTA owns a tile of kAggTile consecutive
-// sorted leaves: a node whose range lies inside the tile is reached only by the tile's threads,
-// so its arrival counter and summary live in shared memory (block-scope acq_rel); only nodes whose
-// range crosses a tile boundary use device-scope counters. A thread carries the summary of the
-// child it comes from and loads only the sibling. Every node's summary is also stored to its
-// 64-byte global slot (full-sector writes) for the collapse.
+// sorted leaves and the binary nodes with the same indices (a node is an end of its leaf range, so
+// every node whose range lies inside the tile has its index there): the tile's leaf summaries,
+// node links, arrival counters and node summaries all live in shared memory, and a walk inside the
+// tile touches nothing else (block-scope arrivals; no global store before the end, so the arrival
+// fences wait on shared memory only). A walk stops at the first node whose range crosses the tile:
+// it lists the child it comes from (`upper`: an in-tile node, or a leaf with the leaf bit) for
+// lt_aggregate_upper_kernel, which walks the crossing nodes with device-scope arrivals. At the
+// end the CTA stores the summaries of its in-tile nodes to their 64-byte global slots (full-sector
+// writes, coalesced) for the collapse.
+//
+// The upper walks are chains of dependent device-scope atomics and L2 loads; run inside the tile
+// kernel they kept each tile's CTA resident for them, and the tiles then ran in many waves of such
+// tails.
 constexpr uint32_t kAggTile = 256;
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
@@ -348,61 +356,98 @@ __global__ void __launch_bounds__(kAggTile)
     lt_aggregate_kernel(uint32_t n, const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
                         const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
                         const uint32_t* __restrict__ leaf_parent, const uint32_t* __restrict__ range_end,
-                        uint32_t* counter, AggregateSlot* aggregates, BuildControl* control)
+                        AggregateSlot* aggregates, uint32_t* upper, BuildControl* control)
 {
     __shared__ uint32_t s_count[kAggTile];
+    __shared__ LightSummary s_leaf[kAggTile];
     __shared__ LightSummary s_sum[kAggTile];
     __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
-    s_count[threadIdx.x] = 0;
-    {
-        // The tile's own node indices (a node is an end of its leaf range, so every node inside the
-        // tile has its index there), loaded coalesced once; the walks then read them from here.
-        const uint32_t k = lo + threadIdx.x;
-        if (k + 1 < n)
-            s_link[threadIdx.x] = make_uint4(__ldg(left + k), __ldg(right + k), __ldg(parent + k), __ldg(range_end + k));
+    const uint32_t k = threadIdx.x;
+    const uint32_t j = lo + k;  // this thread's leaf, and the node of the same index
+    s_count[k] = 0;
+    uint32_t node = kNone;
+    bool mine = false;  // node j lies inside the tile
+    if (j < n) {
+        s_leaf[k] = load_summary(sorted + j);
+        node = __ldg(leaf_parent + j);
+    }
+    if (j + 1 < n) {
+        const uint4 link = make_uint4(__ldg(left + j), __ldg(right + j), __ldg(parent + j), __ldg(range_end + j));
+        s_link[k] = link;
+        mine = min(j, link.w) >= lo && max(j, link.w) <= hi;
     }
     __syncthreads();
-    const uint32_t j = lo + threadIdx.x;
-    if (j >= n) return;
-    LightSummary cur = load_summary(sorted + j);
-    uint32_t from = kChildLeafBit | j;
-    uint32_t node = __ldg(leaf_parent + j);
-    uint32_t depth = 0;
-    for (; depth < 128 && node != kNone; ++depth) {
-        uint4 link;
-        if (node - lo < kAggTile && node + 1 < n)
-            link = s_link[node - lo];
-        else
-            link = make_uint4(__ldg(left + node), __ldg(right + node), __ldg(parent + node), __ldg(range_end + node));
-        const uint32_t l = link.x;
-        const uint32_t r = link.y;
-        const uint32_t up = link.z;
-        const uint32_t end = link.w;
-        const uint32_t a = min(node, end);
-        const uint32_t b = max(node, end);
-        const bool inside = a >= lo && b <= hi;
-        const uint32_t sibling = l == from ? r : l;
-        LightSummary sib;
-        if (inside) {
+    if (j < n) {
+        LightSummary cur = s_leaf[k];
+        uint32_t from = kChildLeafBit | j;
+        uint32_t depth = 0;
+        for (; depth < 128 && node != kNone; ++depth) {
+            uint4 link = make_uint4(0u, 0u, 0u, 0u);
+            bool inside = node - lo < kAggTile && node + 1 < n;
+            if (inside) {
+                link = s_link[node - lo];
+                inside = min(node, link.w) >= lo && max(node, link.w) <= hi;
+            }
+            if (!inside) {
+                upper[atomicAdd(&control->upper_count, 1u)] = from;  // the upper walks go on from here
+                break;
+            }
             cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrival(s_count[node - lo]);
-            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
-            else sib = s_sum[sibling - lo];
-        } else {
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
-            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) return;
-            if (sibling & kChildLeafBit) sib = load_summary(sorted + (sibling & ~kChildLeafBit));
-            else sib = load_summary_cg(&aggregates[sibling].summary);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) break;
+            const uint32_t l = link.x;
+            const uint32_t sibling = l == from ? link.y : l;
+            const uint32_t sib_at = (sibling & ~kChildLeafBit) - lo;
+            if (sib_at >= kAggTile) {  // a child outside its parent's range: a broken tree
+                atomicOr(&control->status, kStatusDepthGuard);
+                break;
+            }
+            const LightSummary& sib = (sibling & kChildLeafBit) ? s_leaf[sib_at] : s_sum[sib_at];
+            cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
+            s_sum[node - lo] = cur;
+            from = node;
+            node = link.z;
         }
-        cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
-        if (inside) s_sum[node - lo] = cur;
-        store_slot(aggregates + node, cur);
-        from = node;
-        node = up;
+        if (depth == 128) atomicOr(&control->status, kStatusDepthGuard);
     }
-    if (node != kNone) atomicOr(&control->status, kStatusDepthGuard);
+    __syncthreads();
+    if (mine) store_slot(aggregates + j, s_sum[k]);
+}
+
+// The walks up through the nodes whose range crosses a tile, from the children the tiles listed
+// (an in-tile node, its summary in its slot, or a leaf): the second thread to arrive at a node
+// (device-scope counter) computes it and goes on. A persistent grid takes the list (its length is
+// known on the device only).
+__global__ void __launch_bounds__(kThreads)
+    lt_aggregate_upper_kernel(const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
+                              const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
+                              const uint32_t* __restrict__ leaf_parent, uint32_t* counter,
+                              AggregateSlot* aggregates, const uint32_t* __restrict__ upper, BuildControl* control)
+{
+    const uint32_t count = control->upper_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        uint32_t from = upper[i];
+        const bool leaf = (from & kChildLeafBit) != 0;
+        LightSummary cur = leaf ? load_summary(sorted + (from & ~kChildLeafBit)) : load_summary_cg(&aggregates[from].summary);
+        uint32_t node = leaf ? __ldg(leaf_parent + (from & ~kChildLeafBit)) : __ldg(parent + from);
+        uint32_t depth = 0;
+        for (; depth < 128 && node != kNone; ++depth) {
+            const uint32_t l = __ldg(left + node);
+            const uint32_t r = __ldg(right + node);
+            const uint32_t up = __ldg(parent + node);
+            const uint32_t sibling = l == from ? r : l;
+            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+            if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) break;
+            const LightSummary sib = (sibling & kChildLeafBit) ? load_summary(sorted + (sibling & ~kChildLeafBit))
+                                                               : load_summary_cg(&aggregates[sibling].summary);
+            cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
+            store_slot(aggregates + node, cur);
+            from = node;
+            node = up;
+        }
+        if (depth == 128) atomicOr(&control->status, kStatusDepthGuard);
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -774,8 +819,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
             b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover, b.depth);
         mark(4);
         // `depth` holds each node's range end until the flags scan writes the depths.
+        // values_alt (free after the sort) lists the children the tiles hand to the upper walks.
         lt_aggregate_kernel<<<(n + kAggTile - 1) / kAggTile, kAggTile, 0, stream>>>(
-            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.depth, b.counter, b.aggregates, b.control);
+            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.depth, b.aggregates, b.values_alt, b.control);
+        lt_aggregate_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
+            b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.values_alt, b.control);
         mark(5);
         const uint32_t tiles = (nodes + kScanTile - 1) / kScanTile;
         lt_cover_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.cover, cover_states, scan_counters,
@@ -801,11 +849,11 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
 
 uint32_t lt_kernel_launches(uint32_t n)
 {
-    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the five tree
+    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the six tree
     // kernels from two leaves, finish.
     if (n == 0) return 1;
     const uint32_t sort = n <= kSmallSortKeys ? 1u : 5u;
-    return 2 + sort + (n >= 2 ? 5u : 0u) + 1;
+    return 2 + sort + (n >= 2 ? 6u : 0u) + 1;
 }
 
 }  // namespace cx

@@ -58,7 +58,8 @@ struct BuildControl
     uint32_t status;
     uint32_t node_count;         // the scan total of the even-depth flags
     uint32_t scan_tile_counter;  // dynamic tile ids of lt_depth_scan_kernel
-    uint32_t pad[7];
+    uint32_t upper_count;        // nodes the tile aggregation hands to lt_aggregate_upper_kernel
+    uint32_t pad[6];
 };
 static_assert(sizeof(BuildControl) == 64);
 
