@@ -92,98 +92,139 @@ __device__ __forceinline__ uint32_t morton30(uint32_t x, uint32_t y, uint32_t z)
 // end, one atomic per warp and code.
 static_assert(sizeof(BrickLightRecord) == 48 && sizeof(LightBvhLeaf) == 64, "record and leaf sizes");
 
+// One record's leaf (into q: a staging slot) and centre (the loads done by the caller).
+__device__ __forceinline__ void emit_record(uint32_t i, uint4 w0, uint4 w1, uint32_t g, uint32_t e,
+                                            const GroupFrame* __restrict__ frames, uint32_t frame_count,
+                                            uint4* q, float4* __restrict__ centres,
+                                            BuildControl* __restrict__ control, uint32_t lo_code[3],
+                                            uint32_t hi_code[3])
+{
+    LightSummary local;
+    local.face[0] = __uint_as_float(w0.x);
+    local.face[1] = __uint_as_float(w0.y);
+    local.face[2] = __uint_as_float(w0.z);
+    local.face[3] = __uint_as_float(w0.w);
+    local.face[4] = __uint_as_float(w1.x);
+    local.face[5] = __uint_as_float(w1.y);
+    const uint32_t box_lo = w1.z;
+    const uint32_t box_hi = w1.w;
+    float origin[3] = {0.0f, 0.0f, 0.0f};
+    float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    float t[3] = {0.0f, 0.0f, 0.0f};
+    if (frames && g >= frame_count) atomicOr(&control->status, kStatusBadGroup);
+    if (frames && g < frame_count) {
+        const GroupFrame* f = frames + g;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            origin[k] = __ldg(&f->origin[k]);
+            t[k] = __ldg(&f->trans[k]);
+        }
+#pragma unroll
+        for (int k = 0; k < 9; ++k) r[k] = __ldg(&f->rot[k]);
+    }
+    local.lo[0] = origin[0] + (float)(box_lo & kVoxelMask);
+    local.lo[1] = origin[1] + (float)((box_lo >> kVoxelBits) & kVoxelMask);
+    local.lo[2] = origin[2] + (float)((box_lo >> (2 * kVoxelBits)) & kVoxelMask);
+    local.hi[0] = origin[0] + (float)(box_hi & kVoxelMask);
+    local.hi[1] = origin[1] + (float)((box_hi >> kVoxelBits) & kVoxelMask);
+    local.hi[2] = origin[2] + (float)((box_hi >> (2 * kVoxelBits)) & kVoxelMask);
+
+    // LtWorldSummary (caelix_light_gather_emit.hlsl:11-34).
+    float centre[3], half[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        centre[k] = 0.5f * (local.lo[k] + local.hi[k]);
+        half[k] = 0.5f * (local.hi[k] - local.lo[k]);
+    }
+    LightSummary w;
+#pragma unroll
+    for (int row = 0; row < 3; ++row) {
+        const float wc = r[3 * row] * centre[0] + r[3 * row + 1] * centre[1] + r[3 * row + 2] * centre[2] +
+                         t[row];
+        const float wh = fabsf(r[3 * row]) * half[0] + fabsf(r[3 * row + 1]) * half[1] +
+                         fabsf(r[3 * row + 2]) * half[2];
+        w.lo[row] = wc - wh;
+        w.hi[row] = wc + wh;
+    }
+#pragma unroll
+    for (int f = 0; f < 6; ++f) w.face[f] = 0.0f;
+#pragma unroll
+    for (int f = 0; f < 6; ++f) {
+        const int axis = f >> 1;
+        const float sign = (f & 1) ? -1.0f : 1.0f;
+#pragma unroll
+        for (int b = 0; b < 3; ++b) {
+            const float d = sign * r[3 * b + axis];
+            w.face[2 * b] += local.face[f] * hmax(0.0f, d);
+            w.face[2 * b + 1] += local.face[f] * hmax(0.0f, -d);
+        }
+    }
+    q[0] = make_uint4(__float_as_uint(w.face[0]), __float_as_uint(w.face[1]), __float_as_uint(w.face[2]),
+                      __float_as_uint(w.face[3]));
+    q[1] = make_uint4(__float_as_uint(w.face[4]), __float_as_uint(w.face[5]), __float_as_uint(w.lo[0]),
+                      __float_as_uint(w.lo[1]));
+    q[2] = make_uint4(__float_as_uint(w.lo[2]), __float_as_uint(w.hi[0]), __float_as_uint(w.hi[1]),
+                      __float_as_uint(w.hi[2]));
+    q[3] = make_uint4(g, e, 0u, kNone);
+    float c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        c[k] = 0.5f * (w.lo[k] + w.hi[k]);
+        const uint32_t code = float_order(c[k]);
+        lo_code[k] = max(lo_code[k], ~code);
+        hi_code[k] = max(hi_code[k], code);
+    }
+    centres[i] = make_float4(c[0], c[1], c[2], 0.0f);  // for the Morton codes (16 bytes, not the leaf)
+}
+
 __global__ void __launch_bounds__(kThreads)
     lt_emit_kernel(const BrickLightRecord* __restrict__ records, uint32_t n,
                    const uint32_t* __restrict__ record_group, const uint32_t* __restrict__ record_entry,
                    const GroupFrame* __restrict__ frames, uint32_t frame_count, LightBvhLeaf* __restrict__ leaves,
                    float4* __restrict__ centres, BuildControl* __restrict__ control)
 {
+    // A warp's 2 x 32 leaves are staged in shared memory and stored as whole 512-byte rows.
+    __shared__ __align__(16) uint4 s_leaf[kThreads / 32][2][32 * 4];
     uint32_t lo_code[3] = {0, 0, 0};  // ~order(centre), max-reduced
     uint32_t hi_code[3] = {0, 0, 0};  // order(centre), max-reduced
     const uint4* rsrc = reinterpret_cast<const uint4*>(records);
     uint4* ldst = reinterpret_cast<uint4*>(leaves);
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const uint4 w0 = __ldg(rsrc + 3ull * i);
-        const uint4 w1 = __ldg(rsrc + 3ull * i + 1);
-        const uint32_t g = record_group ? __ldg(record_group + i) : 0u;
-        const uint32_t e = record_entry ? __ldg(record_entry + i) : i;
-        LightSummary local;
-        local.face[0] = __uint_as_float(w0.x);
-        local.face[1] = __uint_as_float(w0.y);
-        local.face[2] = __uint_as_float(w0.z);
-        local.face[3] = __uint_as_float(w0.w);
-        local.face[4] = __uint_as_float(w1.x);
-        local.face[5] = __uint_as_float(w1.y);
-        const uint32_t box_lo = w1.z;
-        const uint32_t box_hi = w1.w;
-        float origin[3] = {0.0f, 0.0f, 0.0f};
-        float r[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
-        float t[3] = {0.0f, 0.0f, 0.0f};
-        if (frames && g >= frame_count) atomicOr(&control->status, kStatusBadGroup);
-        if (frames && g < frame_count) {
-            const GroupFrame* f = frames + g;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                origin[k] = __ldg(&f->origin[k]);
-                t[k] = __ldg(&f->trans[k]);
-            }
-#pragma unroll
-            for (int k = 0; k < 9; ++k) r[k] = __ldg(&f->rot[k]);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    uint4* stage0 = s_leaf[warp][0];
+    uint4* stage1 = s_leaf[warp][1];
+    // Two runs of 32 records per warp and step (base and base + stride), both loaded before either
+    // is written (more loads in flight).
+    const uint32_t stride = gridDim.x * blockDim.x;
+    for (uint32_t base = blockIdx.x * blockDim.x + warp * 32u; base < n; base += 2 * stride) {
+        const uint32_t i = base + lane;
+        const uint32_t base2 = base + stride;
+        const uint32_t i2 = base2 + lane;
+        const bool one = i < n, two = i2 < n;
+        uint4 a0 = make_uint4(0u, 0u, 0u, 0u), a1 = a0, b0 = a0, b1 = a0;
+        uint32_t ag = 0, ae = 0, bg = 0, be = 0;
+        if (one) {
+            a0 = __ldg(rsrc + 3ull * i);
+            a1 = __ldg(rsrc + 3ull * i + 1);
+            ag = record_group ? __ldg(record_group + i) : 0u;
+            ae = record_entry ? __ldg(record_entry + i) : i;
         }
-        local.lo[0] = origin[0] + (float)(box_lo & kVoxelMask);
-        local.lo[1] = origin[1] + (float)((box_lo >> kVoxelBits) & kVoxelMask);
-        local.lo[2] = origin[2] + (float)((box_lo >> (2 * kVoxelBits)) & kVoxelMask);
-        local.hi[0] = origin[0] + (float)(box_hi & kVoxelMask);
-        local.hi[1] = origin[1] + (float)((box_hi >> kVoxelBits) & kVoxelMask);
-        local.hi[2] = origin[2] + (float)((box_hi >> (2 * kVoxelBits)) & kVoxelMask);
-
-        // LtWorldSummary (caelix_light_gather_emit.hlsl:11-34).
-        float centre[3], half[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            centre[k] = 0.5f * (local.lo[k] + local.hi[k]);
-            half[k] = 0.5f * (local.hi[k] - local.lo[k]);
+        if (two) {
+            b0 = __ldg(rsrc + 3ull * i2);
+            b1 = __ldg(rsrc + 3ull * i2 + 1);
+            bg = record_group ? __ldg(record_group + i2) : 0u;
+            be = record_entry ? __ldg(record_entry + i2) : i2;
         }
-        LightSummary w;
+        if (one) emit_record(i, a0, a1, ag, ae, frames, frame_count, stage0 + 4 * lane, centres, control, lo_code, hi_code);
+        if (two) emit_record(i2, b0, b1, bg, be, frames, frame_count, stage1 + 4 * lane, centres, control, lo_code, hi_code);
+        __syncwarp();
+        // 16-byte unit u of the run is leaf u / 4's word u % 4.
 #pragma unroll
-        for (int row = 0; row < 3; ++row) {
-            const float wc = r[3 * row] * centre[0] + r[3 * row + 1] * centre[1] + r[3 * row + 2] * centre[2] +
-                             t[row];
-            const float wh = fabsf(r[3 * row]) * half[0] + fabsf(r[3 * row + 1]) * half[1] +
-                             fabsf(r[3 * row + 2]) * half[2];
-            w.lo[row] = wc - wh;
-            w.hi[row] = wc + wh;
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t u = 32u * q + lane;
+            if (base + u / 4 < n) ldst[4ull * base + u] = stage0[u];
+            if (base2 + u / 4 < n) ldst[4ull * base2 + u] = stage1[u];
         }
-#pragma unroll
-        for (int f = 0; f < 6; ++f) w.face[f] = 0.0f;
-#pragma unroll
-        for (int f = 0; f < 6; ++f) {
-            const int axis = f >> 1;
-            const float sign = (f & 1) ? -1.0f : 1.0f;
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-                const float d = sign * r[3 * b + axis];
-                w.face[2 * b] += local.face[f] * hmax(0.0f, d);
-                w.face[2 * b + 1] += local.face[f] * hmax(0.0f, -d);
-            }
-        }
-        uint4* q = ldst + 4ull * i;
-        q[0] = make_uint4(__float_as_uint(w.face[0]), __float_as_uint(w.face[1]), __float_as_uint(w.face[2]),
-                          __float_as_uint(w.face[3]));
-        q[1] = make_uint4(__float_as_uint(w.face[4]), __float_as_uint(w.face[5]), __float_as_uint(w.lo[0]),
-                          __float_as_uint(w.lo[1]));
-        q[2] = make_uint4(__float_as_uint(w.lo[2]), __float_as_uint(w.hi[0]), __float_as_uint(w.hi[1]),
-                          __float_as_uint(w.hi[2]));
-        q[3] = make_uint4(g, e, 0u, kNone);
-        float c[3];
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-            c[k] = 0.5f * (w.lo[k] + w.hi[k]);
-            const uint32_t code = float_order(c[k]);
-            lo_code[k] = max(lo_code[k], ~code);
-            hi_code[k] = max(hi_code[k], code);
-        }
-        centres[i] = make_float4(c[0], c[1], c[2], 0.0f);  // for the Morton codes (16 bytes, not the leaf)
+        __syncwarp();
     }
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
@@ -456,6 +497,39 @@ __global__ void __launch_bounds__(kThreads)
 constexpr int kScanItems = 16;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;
 
+// A thread's kScanItems consecutive words from base (a multiple of kScanItems): four 16-byte loads
+// when all lie below count, else word by word (zero past count).
+__device__ __forceinline__ void load_run(const uint32_t* p, uint32_t base, uint32_t count, uint32_t (&v)[kScanItems])
+{
+    if (base + kScanItems <= count) {
+        const uint4* q = reinterpret_cast<const uint4*>(p + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k) {
+            const uint4 x = q[k];
+            v[4 * k] = x.x;
+            v[4 * k + 1] = x.y;
+            v[4 * k + 2] = x.z;
+            v[4 * k + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = base + k < count ? p[base + k] : 0u;
+    }
+}
+
+__device__ __forceinline__ void store_run(uint32_t* p, uint32_t base, uint32_t count, const uint32_t (&v)[kScanItems])
+{
+    if (base + kScanItems <= count) {
+        uint4* q = reinterpret_cast<uint4*>(p + base);
+#pragma unroll
+        for (int k = 0; k < kScanItems / 4; ++k) q[k] = make_uint4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < count) p[base + k] = v[k];
+    }
+}
+
 // cover[g] for g < count becomes the number of binary nodes over leaf boundary g (inclusive prefix
 // sum of the differences). The u32 differences wrap; the prefix is exact.
 __global__ void __launch_bounds__(kScanThreads)
@@ -470,12 +544,10 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t tile = s_tile;
     const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
+    load_run(cover, base, count, v);
     uint32_t sum = 0;
 #pragma unroll
-    for (int k = 0; k < kScanItems; ++k) {
-        v[k] = base + k < count ? cover[base + k] : 0u;
-        sum += v[k];
-    }
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
     uint32_t total;
     const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
     // The look-back values are 30-bit: the range counts (at most the tree depth) never need more,
@@ -489,8 +561,9 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         run += v[k];
-        if (base + k < count) cover[base + k] = run & kTileValueMask;
+        v[k] = run & kTileValueMask;
     }
+    store_run(cover, base, count, v);
 }
 
 // The depth of binary node i is the number of nodes over its split boundary minus one (the nodes
@@ -510,19 +583,20 @@ __global__ void __launch_bounds__(kScanThreads)
     const uint32_t tile = s_tile;
     const uint32_t base = tile * kScanTile + threadIdx.x * kScanItems;
     uint32_t flag[kScanItems];
+    uint32_t v[kScanItems];
+    load_run(left, base, nodes, v);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) v[k] = base + k < nodes ? __ldg(cover + (v[k] & ~kChildLeafBit)) - 1u : 0u;
+    store_run(depth_out, base, nodes, v);
     uint32_t sum = 0;
+    bool deep = false;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        flag[k] = 0;
-        if (base + k < nodes) {
-            const uint32_t gamma = __ldg(left + base + k) & ~kChildLeafBit;
-            const uint32_t d = __ldg(cover + gamma) - 1u;
-            if (d >= 128u) atomicOr(&control->status, kStatusDepthGuard);
-            depth_out[base + k] = d;
-            flag[k] = (d & 1u) == 0 ? 1u : 0u;
-        }
+        deep = deep || (base + k < nodes && v[k] >= 128u);
+        flag[k] = base + k < nodes && (v[k] & 1u) == 0 ? 1u : 0u;
         sum += flag[k];
     }
+    if (deep) atomicOr(&control->status, kStatusDepthGuard);
     uint32_t total;
     const uint32_t local = block_exclusive_sum<kScanThreads>(sum, s_scan, total);
     if (threadIdx.x < 32) {
@@ -536,10 +610,11 @@ __global__ void __launch_bounds__(kScanThreads)
     uint32_t run = s_prefix + local;
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
-        if (base + k < nodes) wide[base + k] = run;
+        v[k] = run;
         if (flag[k]) even[run] = base + k;  // the binary node of every 4-wide node
         run += flag[k];
     }
+    store_run(wide, base, nodes, v);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -702,6 +777,16 @@ uint32_t grid_for(uint32_t n, uint32_t per_block, uint32_t cap)
 
 uint64_t align256(uint64_t x) { return (x + 255u) & ~uint64_t{255}; }
 
+// Resident CTAs of `kernel` per SM at `threads` threads (at least 1).
+template <typename Kernel>
+uint32_t ctas_per_sm(Kernel kernel, int threads)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess || per_sm < 1)
+        return 1;
+    return (uint32_t)per_sm;
+}
+
 uint64_t zero_words(uint32_t n, uint32_t kpt)
 {
     // control words, the sort scratch of tiles of 256 * kpt keys, then two scan states and their
@@ -783,11 +868,14 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     if (e != cudaSuccess) return e;
     const uint32_t sms = current_sm_count();
     if (n > 0) {
-        lt_emit_kernel<<<grid_for(n, kThreads, sms * 8), kThreads, 0, stream>>>(
+        // The grid-stride kernels run one full wave of resident CTAs.
+        static const uint32_t emit_per_sm = ctas_per_sm(lt_emit_kernel, kThreads);
+        static const uint32_t morton_per_sm = ctas_per_sm(lt_morton_kernel, kThreads);
+        lt_emit_kernel<<<grid_for(n, 2 * kThreads, sms * emit_per_sm), kThreads, 0, stream>>>(
             in.records, n, in.record_group, in.record_entry, in.group_frames, in.group_count, b.leaves,
             reinterpret_cast<float4*>(b.aggregates), b.control);  // the slots hold the centres until aggregation
         mark(1);
-        lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * 4), kThreads, 0, stream>>>(
+        lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * morton_per_sm), kThreads, 0, stream>>>(
             reinterpret_cast<const float4*>(b.aggregates), n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
         mark(2);
         if (n <= kSmallSortKeys) {
