@@ -469,7 +469,7 @@ def measure_build(args, world, local, dev, stream, flush, records):
         "mleaves_per_s": world * n / (ms / 1e3) / 1e6,
         "config1_ms": config1_ms,
         "stage_ms": {name: float(v) for name, v in zip(
-            ["emit_bounds", "morton_hist", "sort_4_passes", "karras", "aggregate", "depth_scan", "wide_finish"],
+            ["emit_bounds", "morton_hist", "sort_4_passes_gather", "karras", "depth_scan", "tile_aggregate_collapse_upper_aggregate", "upper_collapse_finish"],
             stage_ms)},
         "roofline": {"kernel": "sort stage: 4 onesweep_pipe_kernel passes + lt_gather_kernel", "bound": "hbm",
                      "achieved": sort_achieved, "peak": peak, "unit": "GB/s", "frac": sort_achieved / peak,

@@ -367,22 +367,24 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// Bottom-up aggregation, one thread per sorted leaf: the second thread to arrive at a node
-// computes its summary from both children and goes on. A CTA owns a tile of kAggTile consecutive
-// sorted leaves and the binary nodes with the same indices (a node is an end of its leaf range, so
-// every node whose range lies inside the tile has its index there): the tile's leaf summaries,
-// node links, arrival counters and node summaries all live in shared memory, and a walk inside the
-// tile touches nothing else (block-scope arrivals; no global store before the end, so the arrival
-// fences wait on shared memory only). A walk stops at the first node whose range crosses the tile:
-// it lists the child it comes from (`upper`: an in-tile node, or a leaf with the leaf bit) for
-// lt_aggregate_upper_kernel, which walks the crossing nodes with device-scope arrivals. At the
-// end the CTA stores the summaries of its in-tile nodes to their 64-byte global slots (full-sector
-// writes, coalesced) for the collapse.
-//
-// The upper walks are chains of dependent device-scope atomics and L2 loads; run inside the tile
-// kernel they kept each tile's CTA resident for them, and the tiles then ran in many waves of such
-// tails.
+// Bottom-up aggregation and the 4-wide collapse, by tiles. A CTA owns a tile of kAggTile
+// consecutive sorted leaves and the binary nodes with the same indices (a node is an end of its
+// leaf range, so every node whose range lies inside the tile has its index there). The tile's leaf
+// summaries, node links, 4-wide indices, leaf indices, arrival counters and node summaries are
+// loaded into shared memory once; then
+//   1. one walk per leaf: the second thread to arrive at an in-tile node computes its summary from
+//      both children and goes on (block-scope arrivals, nothing but shared memory touched). A walk
+//      stops at the first node whose range crosses the tile and lists the child it comes from
+//      (`upper`: an in-tile node, or a leaf with the leaf bit) for lt_aggregate_upper_kernel;
+//   2. the in-tile summaries go to their 64-byte global slots (coalesced full-sector writes);
+//   3. every in-tile node at even depth becomes its 224-byte 4-wide node, built from shared memory
+//      by half a warp (lane q writes 16-byte unit q: one coalesced row), with the parent words of
+//      its leaf slots written into the leaves. Even-depth nodes that cross the tile are listed
+//      (`crossing`) for lt_wide_upper_kernel.
+// The depths and 4-wide indices come from the scans, which run before this kernel.
 constexpr uint32_t kAggTile = 256;
+constexpr uint32_t kNodeQuads = sizeof(LightBvhNode) / 16;  // 14
+constexpr uint32_t kRowChunk = 48;                           // 4-wide rows staged at a time
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
 {
@@ -393,38 +395,109 @@ __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary&
     q[3] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 }
 
+// The child slots of the 4-wide node over a binary node with children l and r (a child's own
+// children from `link_of`): ll, then lr or (l a leaf) rl, then rl or rr, then rr or nothing; a leaf
+// child stands for itself, an empty slot is kNone.
+template <typename LinkOf>
+__device__ __forceinline__ void wide_slots(uint32_t l, uint32_t r, LinkOf link_of, uint32_t slots[4])
+{
+    const bool l_leaf = (l & kChildLeafBit) != 0;
+    const bool r_leaf = (r & kChildLeafBit) != 0;
+    uint32_t ll = l, lr = kNone, rl = r, rr = kNone;
+    if (!l_leaf) {
+        const uint2 c = link_of(l);
+        ll = c.x;
+        lr = c.y;
+    }
+    if (!r_leaf) {
+        const uint2 c = link_of(r);
+        rl = c.x;
+        rr = c.y;
+    }
+    slots[0] = ll;
+    slots[1] = l_leaf ? rl : lr;
+    slots[2] = l_leaf ? rr : rl;
+    slots[3] = l_leaf ? kNone : rr;
+}
+
+// Summary word `idx` (faces 0..5, lo 6..8, hi 9..11) of row word wd (0..47) of a 4-wide node: the
+// child slot and the word within its summary.
+__device__ __forceinline__ void row_word(uint32_t wd, uint32_t& c, uint32_t& idx)
+{
+    if (wd < 24) {
+        c = wd / 6;
+        idx = wd % 6;
+    } else if (wd < 36) {
+        c = (wd - 24) / 3;
+        idx = 6 + (wd - 24) % 3;
+    } else {
+        c = (wd - 36) / 3;
+        idx = 9 + (wd - 36) % 3;
+    }
+}
+
 __global__ void __launch_bounds__(kAggTile)
-    lt_aggregate_kernel(uint32_t n, const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
-                        const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
-                        const uint32_t* __restrict__ leaf_parent, const uint32_t* __restrict__ range_end,
-                        AggregateSlot* aggregates, uint32_t* upper, BuildControl* control)
+    lt_tile_kernel(uint32_t n, uint32_t node_capacity, const LightSummary* __restrict__ sorted,
+                   const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                   const uint32_t* __restrict__ parent, const uint32_t* __restrict__ leaf_parent,
+                   const uint32_t* __restrict__ range_end, const uint32_t* __restrict__ depth,
+                   const uint32_t* __restrict__ wide, const uint32_t* __restrict__ values,
+                   AggregateSlot* __restrict__ aggregates, uint32_t* __restrict__ upper,
+                   uint32_t* __restrict__ crossing, LightBvhLeaf* __restrict__ leaves,
+                   LightBvhNode* __restrict__ nodes, BuildControl* control)
 {
     __shared__ uint32_t s_count[kAggTile];
     __shared__ LightSummary s_leaf[kAggTile];
     __shared__ LightSummary s_sum[kAggTile];
     __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
+    __shared__ uint32_t s_wide[kAggTile];
+    __shared__ uint32_t s_value[kAggTile];
+    __shared__ uint32_t s_even[kAggTile];   // the tile's in-tile even-depth nodes (offsets from lo), in order
+    __shared__ uint32_t s_scan[kAggTile / 32];
+    __shared__ __align__(16) uint4 s_row[kRowChunk * kNodeQuads];  // rows being built
+    __shared__ uint32_t s_row_w[kRowChunk];
+    __shared__ uint32_t s_upper[kAggTile];  // the tile's upper walks and crossing even-depth nodes,
+    __shared__ uint32_t s_cross[kAggTile];  // copied to the global lists with one atomic each
+    __shared__ uint32_t s_upper_count, s_cross_count, s_upper_base, s_cross_base;
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
     const uint32_t k = threadIdx.x;
     const uint32_t j = lo + k;  // this thread's leaf, and the node of the same index
+    const uint32_t count = min(control->node_count, node_capacity);
+    if (k == 0) {
+        s_upper_count = 0;
+        s_cross_count = 0;
+    }
     s_count[k] = 0;
     uint32_t node = kNone;
     bool mine = false;  // node j lies inside the tile
+    bool even = false;
     if (j < n) {
         s_leaf[k] = load_summary(sorted + j);
+        s_value[k] = __ldg(values + j);
         node = __ldg(leaf_parent + j);
     }
     if (j + 1 < n) {
         const uint4 link = make_uint4(__ldg(left + j), __ldg(right + j), __ldg(parent + j), __ldg(range_end + j));
         s_link[k] = link;
+        s_wide[k] = __ldg(wide + j);
         mine = min(j, link.w) >= lo && max(j, link.w) <= hi;
+        even = (__ldg(depth + j) & 1u) == 0;
     }
-    __syncthreads();
+    // The in-tile even-depth nodes in node order (their 4-wide indices rise with it); the block
+    // scan's barriers also publish the loads above.
+    uint32_t evens;
+    {
+        const uint32_t at = block_exclusive_sum<kAggTile>(even && mine ? 1u : 0u, s_scan, evens);
+        if (even && mine) s_even[at] = k;
+    }
+    if (even && !mine) s_cross[atomicAdd(&s_cross_count, 1u)] = j;
+    // 1. The walks.
     if (j < n) {
         LightSummary cur = s_leaf[k];
         uint32_t from = kChildLeafBit | j;
-        uint32_t depth = 0;
-        for (; depth < 128 && node != kNone; ++depth) {
+        uint32_t steps = 0;
+        for (; steps < 128 && node != kNone; ++steps) {
             uint4 link = make_uint4(0u, 0u, 0u, 0u);
             bool inside = node - lo < kAggTile && node + 1 < n;
             if (inside) {
@@ -432,7 +505,7 @@ __global__ void __launch_bounds__(kAggTile)
                 inside = min(node, link.w) >= lo && max(node, link.w) <= hi;
             }
             if (!inside) {
-                upper[atomicAdd(&control->upper_count, 1u)] = from;  // the upper walks go on from here
+                s_upper[atomicAdd(&s_upper_count, 1u)] = from;  // the upper walks go on from here
                 break;
             }
             cuda::atomic_ref<uint32_t, cuda::thread_scope_block> arrival(s_count[node - lo]);
@@ -450,16 +523,96 @@ __global__ void __launch_bounds__(kAggTile)
             from = node;
             node = link.z;
         }
-        if (depth == 128) atomicOr(&control->status, kStatusDepthGuard);
+        if (steps == 128) atomicOr(&control->status, kStatusDepthGuard);
     }
     __syncthreads();
+    if (k == 0) {
+        s_upper_base = s_upper_count ? atomicAdd(&control->upper_count, s_upper_count) : 0u;
+        s_cross_base = s_cross_count ? atomicAdd(&control->crossing_count, s_cross_count) : 0u;
+    }
+    // 2. The in-tile summaries.
     if (mine) store_slot(aggregates + j, s_sum[k]);
+    __syncthreads();
+    if (k < s_upper_count) upper[s_upper_base + k] = s_upper[k];
+    if (k < s_cross_count) crossing[s_cross_base + k] = s_cross[k];
+    // 3. The in-tile 4-wide nodes, kRowChunk at a time: one thread per node writes its row into
+    // shared memory (the children of an in-tile node are in the tile), then the CTA stores the
+    // rows as 16-byte units (consecutive rows are consecutive 4-wide nodes, except where a node
+    // that crosses the tile takes its place).
+    for (uint32_t first = 0; first < evens; first += kRowChunk) {
+        const uint32_t rows = min(kRowChunk, evens - first);
+        if (k < rows) {
+            const uint32_t i = lo + s_even[first + k];
+            const uint4 link = s_link[i - lo];
+            const uint32_t w = s_wide[i - lo];
+            s_row_w[k] = w < count ? w : kNone;  // past the node capacity: the header reports the overflow
+            uint32_t slots[4];
+            wide_slots(link.x, link.y, [&](uint32_t x) { const uint4 c = s_link[x - lo]; return make_uint2(c.x, c.y); },
+                       slots);
+            float* row = reinterpret_cast<float*>(s_row + k * kNodeQuads);
+            uint32_t word[4];
+#pragma unroll
+            for (uint32_t c = 0; c < 4; ++c) {
+                const uint32_t slot = slots[c];
+                float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b4 = a, c4 = a;
+                word[c] = kNone;
+                if (slot != kNone) {
+                    const uint32_t at = (slot & ~kChildLeafBit) - lo;
+                    const float4* sm = reinterpret_cast<const float4*>((slot & kChildLeafBit) ? &s_leaf[at] : &s_sum[at]);
+                    a = sm[0];
+                    b4 = sm[1];
+                    c4 = sm[2];
+                    word[c] = (slot & kChildLeafBit) ? (kChildLeafBit | s_value[at]) : s_wide[at];
+                    if ((slot & kChildLeafBit) && w < count)
+                        leaves[s_value[at]].parent = (w << kParentSlotBits) | c;  // the leaf's parent word
+                }
+                // faces 6c .. 6c + 5, lo 24 + 3c .., hi 36 + 3c .. (summary: faces, lo, hi)
+                float2* face = reinterpret_cast<float2*>(row + 6 * c);
+                face[0] = make_float2(a.x, a.y);
+                face[1] = make_float2(a.z, a.w);
+                face[2] = make_float2(b4.x, b4.y);
+                row[24 + 3 * c] = b4.z;
+                row[25 + 3 * c] = b4.w;
+                row[26 + 3 * c] = c4.x;
+                row[36 + 3 * c] = c4.y;
+                row[37 + 3 * c] = c4.z;
+                row[38 + 3 * c] = c4.w;
+            }
+            s_row[k * kNodeQuads + 12] = make_uint4(word[0], word[1], word[2], word[3]);
+            // The node's own parent link: the 4-wide parent is the binary grandparent (the guard
+            // keeps a broken tree from reading outside the arrays).
+            uint32_t up_node = kNone, up_slot = 0;
+            if (i != 0) {
+                const auto link_of = [&](uint32_t x) {
+                    return x - lo < kAggTile ? s_link[x - lo] : make_uint4(__ldg(left + x), __ldg(right + x), __ldg(parent + x), 0u);
+                };
+                const uint32_t p = link.z;
+                const uint4 lp = p + 1 < n ? link_of(p) : make_uint4(kNone, kNone, kNone, 0u);
+                const uint32_t g = lp.z;
+                if (g + 1 < n) {
+                    const uint32_t gl = link_of(g).x;
+                    const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
+                    up_slot = b0 + (lp.y == i ? 1u : 0u);
+                    up_node = g - lo < kAggTile ? s_wide[g - lo] : __ldg(wide + g);
+                }
+            }
+            s_row[k * kNodeQuads + 13] = make_uint4(up_node, up_slot, 0u, 0u);
+        }
+        __syncthreads();
+        for (uint32_t t = k; t < rows * kNodeQuads; t += kAggTile) {
+            const uint32_t r = t / kNodeQuads;
+            const uint32_t w = s_row_w[r];
+            if (w != kNone) reinterpret_cast<uint4*>(nodes + w)[t - r * kNodeQuads] = s_row[t];
+        }
+        __syncthreads();
+    }
 }
 
 // The walks up through the nodes whose range crosses a tile, from the children the tiles listed
 // (an in-tile node, its summary in its slot, or a leaf): the second thread to arrive at a node
 // (device-scope counter) computes it and goes on. A persistent grid takes the list (its length is
-// known on the device only).
+// known on the device only). The walks were run inside the tile kernel at first: chains of
+// dependent device-scope atomics and L2 loads that kept each tile's CTA resident for them.
 __global__ void __launch_bounds__(kThreads)
     lt_aggregate_upper_kernel(const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
                               const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
@@ -488,6 +641,76 @@ __global__ void __launch_bounds__(kThreads)
             node = up;
         }
         if (depth == 128) atomicOr(&control->status, kStatusDepthGuard);
+    }
+}
+
+// The 4-wide nodes over the even-depth binary nodes that cross a tile (listed by the tile kernel):
+// one thread per node, children and summaries read from the global arrays and slots, the row
+// written by the thread; the parent words of its leaf slots written into the leaves.
+__global__ void __launch_bounds__(kThreads)
+    lt_wide_upper_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
+                         const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
+                         const uint32_t* __restrict__ parent, const uint32_t* __restrict__ crossing,
+                         const uint32_t* __restrict__ wide, const LightSummary* __restrict__ sorted,
+                         const AggregateSlot* __restrict__ aggregates, LightBvhLeaf* __restrict__ leaves,
+                         LightBvhNode* __restrict__ nodes, const BuildControl* __restrict__ control)
+{
+    const uint32_t count = min(control->node_count, node_capacity);
+    const uint32_t listed = control->crossing_count;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < listed; t += gridDim.x * blockDim.x) {
+        const uint32_t i = crossing[t];
+        const uint32_t w = __ldg(wide + i);
+        if (w >= count) continue;
+        uint32_t slots[4];
+        wide_slots(__ldg(left + i), __ldg(right + i),
+                   [&](uint32_t x) { return make_uint2(__ldg(left + x), __ldg(right + x)); }, slots);
+        uint4* row = reinterpret_cast<uint4*>(nodes + w);
+        LightSummary sm[4];
+        uint32_t word[4];
+#pragma unroll
+        for (uint32_t c = 0; c < 4; ++c) {
+#pragma unroll
+            for (int f = 0; f < 6; ++f) sm[c].face[f] = 0.0f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) sm[c].lo[k] = sm[c].hi[k] = 0.0f;
+            word[c] = kNone;
+            const uint32_t slot = slots[c];
+            if (slot == kNone) continue;
+            if (slot & kChildLeafBit) {
+                const uint32_t p = slot & ~kChildLeafBit;
+                sm[c] = load_summary(sorted + p);
+                const uint32_t leaf = __ldg(values + p);
+                word[c] = kChildLeafBit | leaf;
+                leaves[leaf].parent = (w << kParentSlotBits) | c;  // the leaf's parent word, in place
+            } else {
+                sm[c] = load_summary_cg(&aggregates[slot].summary);
+                word[c] = __ldg(wide + slot);
+            }
+        }
+        float f[48];
+#pragma unroll
+        for (uint32_t wd = 0; wd < 48; ++wd) {
+            uint32_t c, idx;
+            row_word(wd, c, idx);
+            f[wd] = reinterpret_cast<const float*>(&sm[c])[idx];
+        }
+#pragma unroll
+        for (int u = 0; u < 12; ++u) row[u] = make_uint4(__float_as_uint(f[4 * u]), __float_as_uint(f[4 * u + 1]),
+                                                         __float_as_uint(f[4 * u + 2]), __float_as_uint(f[4 * u + 3]));
+        row[12] = make_uint4(word[0], word[1], word[2], word[3]);
+        // The node's own parent link.
+        uint32_t up_node = kNone, up_slot = 0;
+        if (i != 0) {
+            const uint32_t p = __ldg(parent + i);
+            const uint32_t g = p + 1 < n ? __ldg(parent + p) : kNone;
+            if (g + 1 < n) {
+                const uint32_t gl = __ldg(left + g);
+                const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
+                up_slot = b0 + (__ldg(right + p) == i ? 1u : 0u);
+                up_node = __ldg(wide + g);
+            }
+        }
+        row[13] = make_uint4(up_node, up_slot, 0u, 0u);
     }
 }
 
@@ -568,12 +791,11 @@ __global__ void __launch_bounds__(kScanThreads)
 
 // The depth of binary node i is the number of nodes over its split boundary minus one (the nodes
 // over boundary gamma are node i and its ancestors); even depths are flagged and scanned into the
-// 4-wide node index (wide[i]), with even[w] the binary node of 4-wide node w. The last tile writes
-// the node count.
+// 4-wide node index (wide[i]). The last tile writes the node count.
 __global__ void __launch_bounds__(kScanThreads)
     lt_flags_scan_kernel(uint32_t nodes, const uint32_t* __restrict__ left, const uint32_t* __restrict__ cover,
-                         uint32_t* __restrict__ depth_out, uint32_t* __restrict__ wide, uint32_t* __restrict__ even,
-                         uint32_t* states, uint32_t* tile_counter, BuildControl* control)
+                         uint32_t* __restrict__ depth_out, uint32_t* __restrict__ wide, uint32_t* states,
+                         uint32_t* tile_counter, BuildControl* control)
 {
     __shared__ uint32_t s_tile;
     __shared__ uint32_t s_scan[kScanThreads / 32];
@@ -611,109 +833,9 @@ __global__ void __launch_bounds__(kScanThreads)
 #pragma unroll
     for (int k = 0; k < kScanItems; ++k) {
         v[k] = run;
-        if (flag[k]) even[run] = base + k;  // the binary node of every 4-wide node
         run += flag[k];
     }
     store_run(wide, base, nodes, v);
-}
-
-// ---------------------------------------------------------------------------------------------
-// 4-wide collapse: one thread per 4-wide node w (binary node even[w], at even depth) builds the
-// whole node (224 bytes, its own parent link included: the 4-wide parent is the binary
-// grandparent) in shared memory and writes the parent word of each of its leaf slots into the leaf;
-// the CTA then stores its run of consecutive nodes with coalesced 16-byte writes.
-constexpr uint32_t kWideThreads = 128;
-constexpr uint32_t kNodeWords = sizeof(LightBvhNode) / 4;  // 56
-
-__global__ void __launch_bounds__(kWideThreads)
-    lt_wide_kernel(uint32_t n, uint32_t node_capacity, const uint32_t* __restrict__ values,
-                   const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
-                   const uint32_t* __restrict__ parent, const uint32_t* __restrict__ even,
-                   const uint32_t* __restrict__ wide, const LightSummary* __restrict__ sorted,
-                   const AggregateSlot* __restrict__ aggregates, LightBvhLeaf* __restrict__ leaves,
-                   LightBvhNode* __restrict__ nodes, const BuildControl* __restrict__ control)
-{
-    __shared__ __align__(16) float s_node[kWideThreads * kNodeWords];
-    const uint32_t count = min(control->node_count, node_capacity);
-    const uint32_t w_base = blockIdx.x * kWideThreads;
-    if (w_base >= count) return;
-    const uint32_t w = w_base + threadIdx.x;
-    if (w < count) {
-        const uint32_t i = __ldg(even + w);
-        float* node = s_node + threadIdx.x * kNodeWords;
-        uint32_t* words = reinterpret_cast<uint32_t*>(node);
-        const uint32_t l = __ldg(left + i);
-        const uint32_t r = __ldg(right + i);
-        uint32_t slots[4];
-        uint32_t used;
-        {
-            const bool l_leaf = (l & kChildLeafBit) != 0;
-            const bool r_leaf = (r & kChildLeafBit) != 0;
-            const uint32_t ll = l_leaf ? l : __ldg(left + l);
-            const uint32_t lr = l_leaf ? kNone : __ldg(right + l);
-            const uint32_t rl = r_leaf ? r : __ldg(left + r);
-            const uint32_t rr = r_leaf ? kNone : __ldg(right + r);
-            slots[0] = ll;
-            slots[1] = l_leaf ? rl : lr;
-            slots[2] = l_leaf ? rr : rl;
-            slots[3] = l_leaf ? kNone : rr;
-            used = (l_leaf ? 1u : 2u) + (r_leaf ? 1u : 2u);
-            if (l_leaf && r_leaf) slots[2] = kNone;
-        }
-        // The node's own parent link.
-        uint32_t up_node = kNone, up_slot = 0;
-        if (i != 0) {
-            // An even-depth node below the root has a binary grandparent; the guard keeps a broken
-            // tree (a failed earlier stage) from reading outside the arrays.
-            const uint32_t p = __ldg(parent + i);
-            const uint32_t g = p + 1 < n ? __ldg(parent + p) : kNone;
-            if (g + 1 < n) {
-                const uint32_t gl = __ldg(left + g);
-                const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
-                up_slot = b0 + (__ldg(right + p) == i ? 1u : 0u);
-                up_node = __ldg(wide + g);
-            }
-        }
-#pragma unroll
-        for (uint32_t c = 0; c < 4; ++c) {
-            LightSummary sm;
-#pragma unroll
-            for (int f = 0; f < 6; ++f) sm.face[f] = 0.0f;
-#pragma unroll
-            for (int k = 0; k < 3; ++k) sm.lo[k] = sm.hi[k] = 0.0f;
-            uint32_t word = kNone;
-            if (c < used) {
-                const uint32_t slot = slots[c];
-                if (slot & kChildLeafBit) {
-                    const uint32_t p = slot & ~kChildLeafBit;
-                    sm = load_summary(sorted + p);
-                    const uint32_t leaf = __ldg(values + p);
-                    word = kChildLeafBit | leaf;
-                    leaves[leaf].parent = (w << kParentSlotBits) | c;  // the leaf's parent word, in place
-                } else {
-                    sm = load_summary(&aggregates[slot].summary);
-                    word = __ldg(wide + slot);
-                }
-            }
-#pragma unroll
-            for (int f = 0; f < 6; ++f) node[6 * c + f] = sm.face[f];
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                node[24 + 3 * c + k] = sm.lo[k];
-                node[36 + 3 * c + k] = sm.hi[k];
-            }
-            words[48 + c] = word;
-        }
-        words[52] = up_node;
-        words[53] = up_slot;
-        words[54] = 0u;
-        words[55] = 0u;
-    }
-    __syncthreads();
-    const uint32_t quads = (min(w_base + kWideThreads, count) - w_base) * (kNodeWords / 4);
-    const float4* src = reinterpret_cast<const float4*>(s_node);
-    float4* dst = reinterpret_cast<float4*>(nodes + w_base);
-    for (uint32_t q = threadIdx.x; q < quads; q += kWideThreads) dst[q] = src[q];
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -903,25 +1025,25 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
     }
     if (n >= 2) {
         const uint32_t nodes = n - 1;
+        // values_alt (free after the sort) holds each node's range end.
         lt_karras_kernel<<<grid_for(nodes, kThreads, 1u << 30), kThreads, 0, stream>>>(
-            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover, b.depth);
+            b.keys, (int)n, b.left, b.right, b.parent, b.leaf_parent, b.cover, b.values_alt);
         mark(4);
-        // `depth` holds each node's range end until the flags scan writes the depths.
-        // values_alt (free after the sort) lists the children the tiles hand to the upper walks.
-        lt_aggregate_kernel<<<(n + kAggTile - 1) / kAggTile, kAggTile, 0, stream>>>(
-            n, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.depth, b.aggregates, b.values_alt, b.control);
-        lt_aggregate_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
-            b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.values_alt, b.control);
-        mark(5);
         const uint32_t tiles = (nodes + kScanTile - 1) / kScanTile;
         lt_cover_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.cover, cover_states, scan_counters,
                                                                   b.control);
-        // keys_alt (free after the sort) holds the binary node of every 4-wide node.
-        lt_flags_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.left, b.cover, b.depth, b.wide,
-                                                                  b.keys_alt, flag_states, scan_counters + 1,
-                                                                  b.control);
+        lt_flags_scan_kernel<<<tiles, kScanThreads, 0, stream>>>(nodes, b.left, b.cover, b.depth, b.wide, flag_states,
+                                                                  scan_counters + 1, b.control);
+        mark(5);
+        // cover (free after the flags scan) lists the upper walks, keys_alt (free after the sort) the
+        // even-depth nodes that cross a tile.
+        lt_tile_kernel<<<(n + kAggTile - 1) / kAggTile, kAggTile, 0, stream>>>(
+            n, b.node_capacity, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.values_alt, b.depth, b.wide,
+            b.values, b.aggregates, b.cover, b.keys_alt, b.leaves, b.nodes, b.control);
+        lt_aggregate_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
+            b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.cover, b.control);
         mark(6);
-        lt_wide_kernel<<<grid_for(nodes, kWideThreads, 1u << 30), kWideThreads, 0, stream>>>(
+        lt_wide_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
             n, b.node_capacity, b.values, b.left, b.right, b.parent, b.keys_alt, b.wide, b.sorted, b.aggregates,
             b.leaves, b.nodes, b.control);
     } else {

@@ -1,28 +1,29 @@
 // The light BVH build on the GPU: brick light records -> world leaves -> Morton codes -> onesweep
-// radix sort -> Karras binary radix tree -> bottom-up aggregation -> depth parity + scan -> 4-wide
-// collapse -> header.
+// radix sort -> Karras binary radix tree -> depth parity + scan -> bottom-up aggregation with the
+// 4-wide collapse -> header.
 //
 // Replaces the reference's per-tree dispatch sequence LightTree::RecordTree
 // (lib/src/light/light_tree_record.cpp:230-309, about 35 dependent dispatches with a barrier after
-// each) with 13 kernels and one memset, all on one stream (capturable in a CUDA graph):
+// each) with 15 kernels and one memset at 4,097 leaves and more (one small-sort CTA in place of
+// the five sort kernels below that), all on one stream (capturable in a CUDA graph):
 //   lt_emit_kernel        gather emit (caelix_light_gather_emit.hlsl:11-86) fused with the centre
 //                         bounds (caelix_light_bvh_bounds.hlsl:10-53): warp max-reductions of
 //                         order-preserving codes instead of a one-workgroup reduction
 //   lt_morton_kernel      Morton codes (caelix_light_bvh_morton.hlsl:6-28) fused with the digit
 //                         histograms of all four sort passes and the clear of the arrival counters
-//   onesweep_pass_kernel  x4 (radix_sort.cuh); the last pass also gathers the leaf summaries into
-//                         sorted order and the inverse permutation, so every later kernel reads
-//                         leaves by sorted position (coalesced) instead of through the permutation
+//   onesweep_pipe_kernel  x4 (radix_sort.cuh), then lt_gather_kernel: the leaf summaries in sorted
+//                         order, so every later kernel reads leaves by sorted position
 //   lt_karras_kernel      caelix_light_bvh_karras.hlsl:8-96, plus the range-count differences
-//   lt_aggregate_kernel   caelix_light_bvh_aggregate.hlsl:30-55 (acq_rel arrival counters)
 //   lt_cover_scan_kernel  the depths (caelix_light_bvh_depth.hlsl:7-30) without walking to the
 //   lt_flags_scan_kernel  root: depth(i) + 1 = the number of binary nodes whose range spans node i's
 //                         split boundary (node i and its ancestors), a prefix sum of +1/-1 range
 //                         ends; then the even-depth flags scanned into 4-wide indices (single-pass
 //                         decoupled look-back scans instead of the one-workgroup scan)
-//   lt_wide_kernel        caelix_light_bvh_wide.hlsl:10-100; every thread writes its whole node,
-//                         its own parent link included (full 32-byte sectors)
-//   lt_leaf_parent_kernel the leaves' parent words in leaf order (whole-sector rewrites)
+//   lt_tile_kernel        by tiles of 256 sorted leaves in shared memory: the aggregation
+//                         (caelix_light_bvh_aggregate.hlsl:30-55) of the nodes inside the tile and
+//                         the 4-wide nodes over them (caelix_light_bvh_wide.hlsl:10-100)
+//   lt_aggregate_upper_kernel  the aggregation of the nodes that cross tiles (acq_rel arrivals)
+//   lt_wide_upper_kernel  the 4-wide nodes over the nodes that cross tiles
 //   lt_finish_kernel      caelix_light_bvh_finish.hlsl:8-63
 // Every float operation is a single IEEE fp32 operation in the order of the HLSL source (the
 // library is compiled with --fmad=false), so the tree is bit-identical to the oracle's.
@@ -57,9 +58,10 @@ struct BuildControl
     uint32_t bounds_code[6];  // [0..2] ~order(min centre), [3..5] order(max centre): atomicMax from 0
     uint32_t status;
     uint32_t node_count;         // the scan total of the even-depth flags
-    uint32_t scan_tile_counter;  // dynamic tile ids of lt_depth_scan_kernel
-    uint32_t upper_count;        // nodes the tile aggregation hands to lt_aggregate_upper_kernel
-    uint32_t pad[6];
+    uint32_t scan_tile_counter;  // unused
+    uint32_t upper_count;        // walks the tile kernel hands to lt_aggregate_upper_kernel
+    uint32_t crossing_count;     // even-depth nodes the tile kernel hands to lt_wide_upper_kernel
+    uint32_t pad[5];
 };
 static_assert(sizeof(BuildControl) == 64);
 
@@ -121,8 +123,9 @@ uint64_t lt_buffer_bytes(uint32_t leaf_capacity);
 // Carves the arrays of `leaf_capacity` leaves out of `base` (lt_buffer_bytes bytes, 256-aligned).
 LightBvhBuffers lt_carve(void* base, uint32_t leaf_capacity);
 // Stages of a build that lt_build can bracket with events: stage[k] is recorded after stage k - 1
-// (stage[0] before the first command): emit+bounds, morton+histograms, sort (4 passes), karras,
-// aggregate, depth+scan, wide+finish.
+// (stage[0] before the first command): emit+bounds, morton+histograms, sort (4 passes and the
+// gather), karras, depth+scan, tile aggregation and collapse + upper aggregation, upper collapse +
+// finish.
 constexpr int kBuildStages = 7;
 // Records the build into `stream`; `stage` (null, or kBuildStages + 1 events) brackets its stages.
 // Returns the first CUDA launch error.

@@ -190,8 +190,10 @@ typedef struct CaelixLightBvhStats
     float gpu_ms;            /* device time of the newest build (events around it) */
     uint32_t kernel_launches; /* kernels the newest build launched */
     float stage_ms[7];       /* with profiling on (caelix_light_bvh_set_profiling): device time of the
-                                stages emit+bounds, morton+histograms, radix sort (4 passes), karras,
-                                aggregate, depth+scan, wide+finish; 0 otherwise */
+                                stages emit+bounds, morton+histograms, radix sort (4 passes and the
+                                gather), karras, depth+scan, aggregation with the 4-wide nodes inside
+                                tiles + aggregation of the nodes that cross tiles, 4-wide nodes over
+                                those + finish; 0 otherwise */
     uint32_t pad;
 } CaelixLightBvhStats;
 
