@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(kThreads)
 // The depths and 4-wide indices come from the scans, which run before this kernel.
 constexpr uint32_t kAggTile = 256;
 constexpr uint32_t kNodeQuads = sizeof(LightBvhNode) / 16;  // 14
-constexpr uint32_t kRowChunk = 48;                           // 4-wide rows staged at a time
+constexpr uint32_t kRowChunk = kAggTile / 4;                 // 4-wide rows staged at a time (4 threads each)
 
 __device__ __forceinline__ void store_slot(AggregateSlot* p, const LightSummary& s)
 {
@@ -446,18 +446,31 @@ __global__ void __launch_bounds__(kAggTile)
                    uint32_t* __restrict__ crossing, LightBvhLeaf* __restrict__ leaves,
                    LightBvhNode* __restrict__ nodes, BuildControl* control)
 {
-    __shared__ uint32_t s_count[kAggTile];
+    // The arrival counters and the tile's lists are dead once the rows are built: they share
+    // their memory with the row staging.
+    union Scratch
+    {
+        struct
+        {
+            uint32_t count[kAggTile];
+            uint32_t upper[kAggTile];  // the tile's upper walks and crossing even-depth nodes,
+            uint32_t cross[kAggTile];  // copied to the global lists with one atomic each
+        } walk;
+        uint4 row[kRowChunk * kNodeQuads];  // rows being built
+    };
+    __shared__ __align__(16) Scratch s_x;
+    uint32_t* const s_count = s_x.walk.count;
+    uint32_t* const s_upper = s_x.walk.upper;
+    uint32_t* const s_cross = s_x.walk.cross;
+    uint4* const s_row = s_x.row;
     __shared__ LightSummary s_leaf[kAggTile];
     __shared__ LightSummary s_sum[kAggTile];
     __shared__ uint4 s_link[kAggTile];  // left, right, parent, range end of the nodes lo .. lo + kAggTile - 1
     __shared__ uint32_t s_wide[kAggTile];
     __shared__ uint32_t s_value[kAggTile];
-    __shared__ uint32_t s_even[kAggTile];   // the tile's in-tile even-depth nodes (offsets from lo), in order
+    __shared__ uint32_t s_even[kAggTile];  // the tile's in-tile even-depth nodes (offsets from lo), in order
     __shared__ uint32_t s_scan[kAggTile / 32];
-    __shared__ __align__(16) uint4 s_row[kRowChunk * kNodeQuads];  // rows being built
     __shared__ uint32_t s_row_w[kRowChunk];
-    __shared__ uint32_t s_upper[kAggTile];  // the tile's upper walks and crossing even-depth nodes,
-    __shared__ uint32_t s_cross[kAggTile];  // copied to the global lists with one atomic each
     __shared__ uint32_t s_upper_count, s_cross_count, s_upper_base, s_cross_base;
     const uint32_t lo = blockIdx.x * kAggTile;
     const uint32_t hi = min(lo + kAggTile, n) - 1;  // last leaf of the tile
@@ -535,74 +548,76 @@ __global__ void __launch_bounds__(kAggTile)
     __syncthreads();
     if (k < s_upper_count) upper[s_upper_base + k] = s_upper[k];
     if (k < s_cross_count) crossing[s_cross_base + k] = s_cross[k];
-    // 3. The in-tile 4-wide nodes, kRowChunk at a time: one thread per node writes its row into
-    // shared memory (the children of an in-tile node are in the tile), then the CTA stores the
-    // rows as 16-byte units (consecutive rows are consecutive 4-wide nodes, except where a node
-    // that crosses the tile takes its place).
+    // 3. The in-tile 4-wide nodes, kRowChunk at a time: four threads per node (thread c: child
+    // slot c; the children of an in-tile node are in the tile) write its row into shared memory,
+    // then the CTA stores the rows as 16-byte units (consecutive rows are consecutive 4-wide nodes,
+    // except where a node that crosses the tile takes its place).
+    __syncthreads();  // the lists are copied out: their memory takes the rows
+    const uint32_t r = k >> 2;
+    const uint32_t c = k & 3u;
     for (uint32_t first = 0; first < evens; first += kRowChunk) {
         const uint32_t rows = min(kRowChunk, evens - first);
-        if (k < rows) {
-            const uint32_t i = lo + s_even[first + k];
+        if (r < rows) {
+            const uint32_t i = lo + s_even[first + r];
             const uint4 link = s_link[i - lo];
             const uint32_t w = s_wide[i - lo];
-            s_row_w[k] = w < count ? w : kNone;  // past the node capacity: the header reports the overflow
             uint32_t slots[4];
-            wide_slots(link.x, link.y, [&](uint32_t x) { const uint4 c = s_link[x - lo]; return make_uint2(c.x, c.y); },
+            wide_slots(link.x, link.y, [&](uint32_t x) { const uint4 cl = s_link[x - lo]; return make_uint2(cl.x, cl.y); },
                        slots);
-            float* row = reinterpret_cast<float*>(s_row + k * kNodeQuads);
-            uint32_t word[4];
-#pragma unroll
-            for (uint32_t c = 0; c < 4; ++c) {
-                const uint32_t slot = slots[c];
-                float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b4 = a, c4 = a;
-                word[c] = kNone;
-                if (slot != kNone) {
-                    const uint32_t at = (slot & ~kChildLeafBit) - lo;
-                    const float4* sm = reinterpret_cast<const float4*>((slot & kChildLeafBit) ? &s_leaf[at] : &s_sum[at]);
-                    a = sm[0];
-                    b4 = sm[1];
-                    c4 = sm[2];
-                    word[c] = (slot & kChildLeafBit) ? (kChildLeafBit | s_value[at]) : s_wide[at];
-                    if ((slot & kChildLeafBit) && w < count)
-                        leaves[s_value[at]].parent = (w << kParentSlotBits) | c;  // the leaf's parent word
-                }
-                // faces 6c .. 6c + 5, lo 24 + 3c .., hi 36 + 3c .. (summary: faces, lo, hi)
-                float2* face = reinterpret_cast<float2*>(row + 6 * c);
-                face[0] = make_float2(a.x, a.y);
-                face[1] = make_float2(a.z, a.w);
-                face[2] = make_float2(b4.x, b4.y);
-                row[24 + 3 * c] = b4.z;
-                row[25 + 3 * c] = b4.w;
-                row[26 + 3 * c] = c4.x;
-                row[36 + 3 * c] = c4.y;
-                row[37 + 3 * c] = c4.z;
-                row[38 + 3 * c] = c4.w;
+            const uint32_t slot = c == 0 ? slots[0] : c == 1 ? slots[1] : c == 2 ? slots[2] : slots[3];
+            float* row = reinterpret_cast<float*>(s_row + r * kNodeQuads);
+            float4 a = make_float4(0.0f, 0.0f, 0.0f, 0.0f), b4 = a, c4 = a;
+            uint32_t word = kNone;
+            if (slot != kNone) {
+                const uint32_t at = (slot & ~kChildLeafBit) - lo;
+                const float4* sm = reinterpret_cast<const float4*>((slot & kChildLeafBit) ? &s_leaf[at] : &s_sum[at]);
+                a = sm[0];
+                b4 = sm[1];
+                c4 = sm[2];
+                word = (slot & kChildLeafBit) ? (kChildLeafBit | s_value[at]) : s_wide[at];
+                if ((slot & kChildLeafBit) && w < count)
+                    leaves[s_value[at]].parent = (w << kParentSlotBits) | c;  // the leaf's parent word
             }
-            s_row[k * kNodeQuads + 12] = make_uint4(word[0], word[1], word[2], word[3]);
-            // The node's own parent link: the 4-wide parent is the binary grandparent (the guard
-            // keeps a broken tree from reading outside the arrays).
-            uint32_t up_node = kNone, up_slot = 0;
-            if (i != 0) {
-                const auto link_of = [&](uint32_t x) {
-                    return x - lo < kAggTile ? s_link[x - lo] : make_uint4(__ldg(left + x), __ldg(right + x), __ldg(parent + x), 0u);
-                };
-                const uint32_t p = link.z;
-                const uint4 lp = p + 1 < n ? link_of(p) : make_uint4(kNone, kNone, kNone, 0u);
-                const uint32_t g = lp.z;
-                if (g + 1 < n) {
-                    const uint32_t gl = link_of(g).x;
-                    const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
-                    up_slot = b0 + (lp.y == i ? 1u : 0u);
-                    up_node = g - lo < kAggTile ? s_wide[g - lo] : __ldg(wide + g);
+            // faces 6c .. 6c + 5, lo 24 + 3c .., hi 36 + 3c .. (a summary: faces, lo, hi), child c
+            float2* face = reinterpret_cast<float2*>(row + 6 * c);
+            face[0] = make_float2(a.x, a.y);
+            face[1] = make_float2(a.z, a.w);
+            face[2] = make_float2(b4.x, b4.y);
+            row[24 + 3 * c] = b4.z;
+            row[25 + 3 * c] = b4.w;
+            row[26 + 3 * c] = c4.x;
+            row[36 + 3 * c] = c4.y;
+            row[37 + 3 * c] = c4.z;
+            row[38 + 3 * c] = c4.w;
+            reinterpret_cast<uint32_t*>(row)[48 + c] = word;
+            if (c == 0) {
+                s_row_w[r] = w < count ? w : kNone;  // past the node capacity: the header reports the overflow
+                // The node's own parent link: the 4-wide parent is the binary grandparent (the
+                // guard keeps a broken tree from reading outside the arrays).
+                uint32_t up_node = kNone, up_slot = 0;
+                if (i != 0) {
+                    const auto link_of = [&](uint32_t x) {
+                        return x - lo < kAggTile ? s_link[x - lo]
+                                                 : make_uint4(__ldg(left + x), __ldg(right + x), __ldg(parent + x), 0u);
+                    };
+                    const uint32_t p = link.z;
+                    const uint4 lp = p + 1 < n ? link_of(p) : make_uint4(kNone, kNone, kNone, 0u);
+                    const uint32_t g = lp.z;
+                    if (g + 1 < n) {
+                        const uint32_t gl = link_of(g).x;
+                        const uint32_t b0 = p == gl ? 0u : ((gl & kChildLeafBit) ? 1u : 2u);
+                        up_slot = b0 + (lp.y == i ? 1u : 0u);
+                        up_node = g - lo < kAggTile ? s_wide[g - lo] : __ldg(wide + g);
+                    }
                 }
+                s_row[r * kNodeQuads + 13] = make_uint4(up_node, up_slot, 0u, 0u);
             }
-            s_row[k * kNodeQuads + 13] = make_uint4(up_node, up_slot, 0u, 0u);
         }
         __syncthreads();
         for (uint32_t t = k; t < rows * kNodeQuads; t += kAggTile) {
-            const uint32_t r = t / kNodeQuads;
-            const uint32_t w = s_row_w[r];
-            if (w != kNone) reinterpret_cast<uint4*>(nodes + w)[t - r * kNodeQuads] = s_row[t];
+            const uint32_t rr = t / kNodeQuads;
+            const uint32_t w = s_row_w[rr];
+            if (w != kNone) reinterpret_cast<uint4*>(nodes + w)[t - rr * kNodeQuads] = s_row[t];
         }
         __syncthreads();
     }
