@@ -783,6 +783,82 @@ __global__ void __launch_bounds__(kLightWarps * 32) light_write_kernel(const Lig
     }
 }
 
+// ---- group generations ----
+// GroupLightRow::generation (lib/src/light/light_tree_layout.h:217-254, LtNextLife / LtNextVersion
+// in shaders/common/caelix_light_tree_layout.hlsl:126-135): the group's life in the high 16 bits
+// (the next life when the group is released: it had bricks and has none), the version of its
+// light block in the low 16 (the next version when the block is rebuilt). A full build rebuilds
+// every block that has or had light bricks; an edit flush the blocks of the groups holding a
+// refinalized brick that is or was a light brick (the reference's kLtGpuLightChanged: a finalized
+// brick whose old or new light face count is not 0). A new grid (origin, group grid or group edge
+// changed: every group index names another place) starts every group at a life above all earlier
+// ones, version 0. A light brick reference (group, entry, generation) stays valid while the row's
+// generation is unchanged.
+constexpr uint32_t kGroupLitBefore = 1u;       // the previous build's block had light bricks
+constexpr uint32_t kGroupOccupied = 2u;        // this build: the group has bricks
+constexpr uint32_t kGroupOccupiedBefore = 4u;  // the previous full build: the group had bricks
+constexpr uint32_t kGroupTouched = 8u;         // this edit flush: a refinalized brick is or was a light brick
+
+__device__ __forceinline__ uint32_t brick_group(const int32_t* keys, uint32_t i, const int32_t origin[3],
+                                                const uint32_t groups[3], uint32_t gs)
+{
+    const uint32_t bx = (uint32_t)(keys[3 * i] - origin[0]), by = (uint32_t)(keys[3 * i + 1] - origin[1]),
+                   bz = (uint32_t)(keys[3 * i + 2] - origin[2]);
+    return (bx >> gs) + groups[0] * ((by >> gs) + groups[1] * (bz >> gs));
+}
+
+struct GroupGrid
+{
+    int32_t origin[3];
+    uint32_t groups[3];
+    uint32_t shift;
+};
+
+__global__ void group_occupancy_kernel(const int32_t* __restrict__ keys, uint32_t n, const GroupGrid gg,
+                                       uint32_t* __restrict__ flags)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t g = brick_group(keys, i, gg.origin, gg.groups, gg.shift);
+    if (!(flags[g] & kGroupOccupied)) atomicOr(&flags[g], kGroupOccupied);
+}
+
+__global__ void group_touch_kernel(const int32_t* __restrict__ keys, uint32_t n, const uint32_t* __restrict__ marks,
+                                   uint32_t epoch, const uint32_t* __restrict__ unit_now,
+                                   const uint32_t* __restrict__ unit_before, const GroupGrid gg, uint32_t* __restrict__ flags)
+{
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n || marks[i] != epoch) return;
+    if (unit_now[i] == kNone && (!unit_before || unit_before[i] == kNone)) return;
+    atomicOr(&flags[brick_group(keys, i, gg.origin, gg.groups, gg.shift)], kGroupTouched);
+}
+
+// full: a full build (else an edit flush); fresh: a new grid, every group starting at fresh_gen.
+__global__ void group_generation_kernel(uint32_t count, uint32_t* __restrict__ rows, uint32_t* __restrict__ gens,
+                                        uint32_t* __restrict__ flags, uint32_t full, uint32_t fresh, uint32_t fresh_gen)
+{
+    const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= count) return;
+    const uint32_t f = fresh ? 0u : flags[g];
+    uint32_t gen = fresh ? fresh_gen : gens[g];
+    const bool lit = rows[8ull * g + 5] != 0;  // the block's light bricks
+    uint32_t next;
+    if (full) {
+        const bool occupied = (flags[g] & kGroupOccupied) != 0;
+        if ((f & kGroupOccupiedBefore) && !occupied)
+            gen = ((gen >> 16) + 1u) << 16;  // released: the next life
+        else if (lit || (f & kGroupLitBefore))
+            gen = (gen & 0xFFFF0000u) | ((gen + 1u) & 0xFFFFu);  // rebuilt: the next version
+        next = (lit ? kGroupLitBefore : 0u) | (occupied ? kGroupOccupiedBefore : 0u);
+    } else {
+        if (f & kGroupTouched) gen = (gen & 0xFFFF0000u) | ((gen + 1u) & 0xFFFFu);
+        next = (lit ? kGroupLitBefore : 0u) | (f & kGroupOccupiedBefore);
+    }
+    gens[g] = gen;
+    rows[8ull * g + 2] = gen;
+    flags[g] = next;
+}
+
 uint32_t blocks_for(uint64_t n, uint32_t per) { return (uint32_t)std::max<uint64_t>(1, (n + per - 1) / per); }
 
 // Resident CTAs of finalize_kernel on every SM of the current device, at most one warp per brick.
@@ -973,7 +1049,8 @@ void scene_release(DeviceScene& s)
     void* ptrs[] = {s.keys,          s.voxels,       s.power,        s.records,       s.hash_slots,
                     s.bitmap,        s.heap,         s.group_rows,    s.frames,
                     s.light_headers, s.light_group,  s.light_entry,  s.light_brick,   s.scratch,
-                    s.tree_memory,   s.status,       s.heap_prev,    s.unit_of_brick, s.unit_of_brick_prev};
+                    s.tree_memory,   s.status,       s.heap_prev,    s.unit_of_brick, s.unit_of_brick_prev,
+                    s.group_gen,     s.group_flag};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (s.pinned) cudaFreeHost(s.pinned);
@@ -1078,6 +1155,52 @@ cudaError_t scene_refinalize(DeviceScene& s, const uint32_t* list, const uint32_
     FinalizeArgs fa{s.keys,  s.voxels,          s.brick_count, s.group_shift, s.hash_slots, s.hash_capacity,
                     s.hash_max_probe, s.records, list,       list_count};
     launch_finalize(fa, s.encoding, max_count, stream);
+    return cudaGetLastError();
+}
+
+// The generation word of every group row (group_generation_kernel), after the rows are written.
+cudaError_t update_generations(DeviceScene& s, const uint32_t* marks, uint32_t epoch, cudaStream_t stream)
+{
+    const uint32_t count = s.group_count;
+    if (count == 0) return cudaSuccess;
+    const bool same = s.group_gen && s.gen_count == count && s.gen_shift == s.group_shift &&
+                      std::memcmp(s.gen_origin, s.origin, sizeof(s.gen_origin)) == 0 &&
+                      std::memcmp(s.gen_groups, s.groups, sizeof(s.gen_groups)) == 0;
+    uint32_t fresh_gen = 0;
+    if (!same) {
+        // A new grid: every group starts at a life above every earlier one.
+        if (s.group_gen && s.gen_count) {
+            std::vector<uint32_t> old(s.gen_count);
+            CX_TRY(cudaMemcpyAsync(old.data(), s.group_gen, 4ull * s.gen_count, cudaMemcpyDeviceToHost, stream));
+            CX_TRY(cudaStreamSynchronize(stream));
+            uint32_t life = 0;
+            for (uint32_t g : old) life = std::max(life, g >> 16);
+            fresh_gen = ((life + 1u) & 0xFFFFu) << 16;
+        }
+        CX_TRY(alloc(s.group_gen, s.capacity.group_gen, count));
+        CX_TRY(alloc(s.group_flag, s.capacity.group_flag, count));
+        CX_TRY(cudaMemsetAsync(s.group_flag, 0, 4ull * count, stream));
+        s.gen_count = count;
+        s.gen_shift = s.group_shift;
+        std::memcpy(s.gen_origin, s.origin, sizeof(s.gen_origin));
+        std::memcpy(s.gen_groups, s.groups, sizeof(s.gen_groups));
+    }
+    GroupGrid gg;
+    for (int k = 0; k < 3; ++k) {
+        gg.origin[k] = s.origin[k];
+        gg.groups[k] = s.groups[k];
+    }
+    gg.shift = s.group_shift;
+    const uint32_t n = s.brick_count;
+    if (n > 0) {
+        if (!marks)
+            group_occupancy_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(s.keys, n, gg, s.group_flag);
+        else
+            group_touch_kernel<<<blocks_for(n, kThreads), kThreads, 0, stream>>>(
+                s.keys, n, marks, epoch, s.unit_of_brick, s.unit_of_brick_prev, gg, s.group_flag);
+    }
+    group_generation_kernel<<<blocks_for(count, kThreads), kThreads, 0, stream>>>(
+        count, s.group_rows, s.group_gen, s.group_flag, marks ? 0u : 1u, same ? 0u : 1u, fresh_gen);
     return cudaGetLastError();
 }
 
@@ -1215,6 +1338,7 @@ cudaError_t scene_build_lights(DeviceScene& s, cudaStream_t stream, uint32_t* de
         CX_TRY(alloc(s.heap, s.capacity.heap, 4));
         CX_TRY(cudaMemsetAsync(s.heap, 0, 16, stream));
     }
+    CX_TRY(update_generations(s, marks, epoch, stream));
     if (!marks) {
         // The buffers the next rebuild over the same bricks swaps in, sized now (a full build
         // allocates anyway; the edit flushes that follow then allocate nothing while the heap

@@ -174,11 +174,21 @@ struct DeviceScene
     uint32_t* unit_of_brick = nullptr;
     uint32_t* unit_of_brick_prev = nullptr;
     uint32_t* heap_prev = nullptr;
+    // Group generations (GroupLightRow::generation, lib/src/light/light_tree_layout.h:217-254): per
+    // group its generation (life << 16 | version) and the flags the next build compares against,
+    // kept across builds for the grid they were made for (gen_count groups).
+    uint32_t* group_gen = nullptr;
+    uint32_t* group_flag = nullptr;
+    uint32_t gen_count = 0;
+    int32_t gen_origin[3] = {0, 0, 0};
+    uint32_t gen_groups[3] = {0, 0, 0};
+    uint32_t gen_shift = ~0u;
     // Element capacities of the buffers above: a rebuild reallocates a buffer only to grow it.
     struct
     {
         uint64_t keys, voxels, power, scratch, hash_slots, bitmap, records, group_rows, light_headers,
-            light_group, light_entry, light_brick, frames, heap, heap_prev, unit_of_brick, unit_of_brick_prev;
+            light_group, light_entry, light_brick, frames, heap, heap_prev, unit_of_brick, unit_of_brick_prev, group_gen,
+            group_flag;
     } capacity{};
 };
 

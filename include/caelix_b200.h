@@ -492,7 +492,8 @@ typedef struct CaelixSceneView
     uint64_t hash_slots;    /* u32 [hash_slot_count][4]: key_lo, key_hi, record, 0 */
     uint64_t bitmap;        /* u32 brick occupancy by linear brick index */
     uint64_t heap;          /* u32 group light blocks */
-    uint64_t group_rows;    /* u32 [group_count][8] */
+    uint64_t group_rows;    /* u32 [group_count][8]: GroupLightRow (block offset, block units,
+                               generation = life << 16 | version, 0, 0, light bricks, light faces, 0) */
     uint64_t light_headers; /* CaelixBrickLightRecord [light_count], leaf order */
     uint64_t light_group;   /* u32 [light_count] */
     uint64_t light_entry;   /* u32 [light_count] */

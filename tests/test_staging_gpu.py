@@ -199,3 +199,118 @@ def test_remove_bricks(cuda_device, oracle):
     scene.flush()
     assert scene.view().brick_count == 0
     scene.close()
+
+
+def generation_state(scene):
+    """The group generations (row word 2), the brick keys, the keys of the light bricks and the
+    grid (origin, group grid, group edge shift) of a flushed scene."""
+    import gpu_util
+
+    v = scene.view()
+    g, n, m = int(v.group_count), int(v.brick_count), int(v.light_count)
+    rows = gpu_util.from_device(v.group_rows, np.uint32, 8 * g).reshape(-1, 8)
+    keys = gpu_util.from_device(v.keys, np.int32, 3 * n).reshape(-1, 3) if n else np.zeros((0, 3), np.int32)
+    lb = gpu_util.from_device(v.light_brick, np.uint32, m) if m else np.zeros(0, np.uint32)
+    grid = (tuple(int(x) for x in v.origin), tuple(int(x) for x in v.groups), int(v.group_shift))
+    return rows[:, 2].copy(), keys, {tuple(k) for k in keys[lb].tolist()}, grid
+
+
+def groups_of(keys, grid):
+    origin, groups, gs = grid
+    c = (np.asarray(keys, np.int64).reshape(-1, 3) - np.array(origin, np.int64)) >> gs
+    return set((c[:, 0] + groups[0] * (c[:, 1] + groups[1] * c[:, 2])).tolist())
+
+
+def next_version(gen):
+    return (gen & 0xFFFF0000) | ((gen + 1) & 0xFFFF)
+
+
+def test_group_generations(cuda_device):
+    """GroupLightRow::generation (life << 16 | version) over a flush history: the first build gives
+    every group with light bricks version 1; an edit flush bumps the version of exactly the groups
+    holding a refinalized brick (an edited brick or one of its six neighbours) that is or was a
+    light brick; a full rebuild bumps every group that has or had light bricks; a group that loses
+    all its bricks takes the next life (version 0); a new grid starts every group at a life above
+    all earlier ones."""
+    import caelix_b200
+
+    vs = workloads.noise_world(grid_bricks=(12, 10, 12), brick_occupancy=0.5, emissive_fraction=0.06, seed=21)
+    vs = vs.like(group_shift=2)
+    rng = np.random.default_rng(21)
+    scene = caelix_b200.Scene.from_voxel_scene(cuda_device, vs)
+    gen0, keys0, lit0, grid0 = generation_state(scene)
+    lit_groups = groups_of(list(lit0), grid0)
+    assert 1 < len(lit_groups) < len(gen0)
+    assert np.array_equal(gen0, np.array([1 if g in lit_groups else 0 for g in range(len(gen0))], np.uint32))
+
+    # An edit flush: two light bricks emptied, three dark bricks rewritten, one power change.
+    key_set = {tuple(k) for k in keys0.tolist()}
+    lit_list = sorted(lit0)
+    dark = [k for k in map(tuple, keys0.tolist()) if k not in lit0]
+    pick_lit = [lit_list[i] for i in rng.choice(len(lit_list), size=2, replace=False)]
+    pick_dark = [dark[i] for i in rng.choice(len(dark), size=3, replace=False)]
+    edit = np.array(pick_lit + pick_dark, np.int32)
+    vox = np.where(rng.random((len(edit), 512)) < 0.5, 0x8001, 0).astype(np.uint16)
+    vox[:2] = 0
+    scene.upload_bricks(edit, vox)
+    relit = np.array([dark[int(rng.integers(len(dark)))]], np.int32)
+    scene.set_brick_power(relit, np.array([0.0], np.float32))
+    scene.flush()
+    gen1, keys1, lit1, grid1 = generation_state(scene)
+    assert grid1 == grid0 and np.array_equal(keys1, keys0)
+    refin = set()
+    for k in np.concatenate([edit, relit]).tolist():
+        for d in ((0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1)):
+            b = (k[0] + d[0], k[1] + d[1], k[2] + d[2])
+            if b in key_set:
+                refin.add(b)
+    touched = groups_of([b for b in refin if b in lit0 or b in lit1], grid0) if refin else set()
+    expect = gen0.copy()
+    for g in touched:
+        expect[g] = next_version(int(expect[g]))
+    assert touched and len(touched) < len(gen0)
+    assert np.array_equal(gen1, expect)
+
+    # A full rebuild over the same grid: a brick added in an empty cell.
+    cell = next((x, y, z) for z in range(vs.grid[2]) for y in range(vs.grid[1]) for x in range(vs.grid[0])
+                if (x, y, z) not in key_set)
+    scene.upload_bricks(np.array([cell], np.int32), np.full((1, 512), 0x8002, np.uint16))
+    scene.set_brick_power(np.array([cell], np.int32), np.array([0.0], np.float32))
+    scene.flush()
+    gen2, keys2, lit2, grid2 = generation_state(scene)
+    assert grid2 == grid0
+    rebuilt = groups_of(list(lit1 | lit2), grid0)
+    expect = gen1.copy()
+    for g in rebuilt:
+        expect[g] = next_version(int(expect[g]))
+    assert np.array_equal(gen2, expect)
+
+    # Every brick of one inner group removed (the grid stays): that group takes the next life.
+    origin, groups, gs = grid0
+    inner = [g for g in groups_of(keys2, grid0)
+             if 0 < g % groups[0] < groups[0] - 1 and 0 < (g // groups[0]) % groups[1] < groups[1] - 1
+             and 0 < g // (groups[0] * groups[1]) < groups[2] - 1]
+    assert inner
+    gone = inner[0]
+    members = np.array([k for k in keys2.tolist() if groups_of([k], grid0) == {gone}], np.int32)
+    scene.remove_bricks(members)
+    scene.flush()
+    gen3, keys3, lit3, grid3 = generation_state(scene)
+    assert grid3 == grid0
+    expect = gen2.copy()
+    for g in groups_of(list(lit2 | lit3), grid0):
+        expect[g] = next_version(int(expect[g]))
+    expect[gone] = ((int(gen2[gone]) >> 16) + 1) << 16
+    assert np.array_equal(gen3, expect)
+
+    # A brick beyond the grid: a new grid, every group at a new life.
+    far = np.array([[int(keys3[:, 0].max()) + (1 << gs) + 1, 0, 0]], np.int32)
+    scene.upload_bricks(far, np.full((1, 512), 0x8002, np.uint16))
+    scene.flush()
+    gen4, keys4, lit4, grid4 = generation_state(scene)
+    assert grid4 != grid0
+    life = (int(gen3.max() >> 16) if len(gen3) else 0) + 1
+    lit_groups = groups_of(list(lit4), grid4)
+    assert np.array_equal(gen4, np.array([(life << 16) | (1 if g in lit_groups else 0) for g in range(len(gen4))],
+                                         np.uint32))
+    scene.close()

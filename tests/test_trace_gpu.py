@@ -54,7 +54,10 @@ def assert_scene_equal(scene, osc, vs):
     assert v.heap_words == len(osc.heap)
     assert np.array_equal(fetch(v, np.uint32, "heap", v.heap_words), osc.heap)
     rows = fetch(v, np.uint32, "group_rows", 8 * v.group_count).reshape(-1, 8)
-    assert np.array_equal(rows, osc.group_rows)
+    # Word 2 is the group's generation, which follows the scene's flush history (the oracle builds
+    # from scratch): tests/test_staging_gpu.py::test_group_generations checks it.
+    words = [0, 1, 3, 4, 5, 6, 7]
+    assert np.array_equal(rows[:, words], osc.group_rows[:, words])
     # The light tree.
     hdr = fetch(v, oracle_lib.HEADER_DTYPE, "tree_header", 1)
     assert hdr.tobytes() == osc.tree["header"].tobytes()
