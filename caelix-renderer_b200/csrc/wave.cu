@@ -128,11 +128,8 @@ __global__ void __launch_bounds__(kWaveThreads)
 // chunks of the queue from a fetch counter (fetch_chunk) instead of a fixed grid stride: faster
 // where ray costs spread widely (entities, scenes whose records do not stay in L2), slower on the
 // small resident scene, where the fixed stride is kept.
-#ifndef CX_ENTITY_TRACE_MIN_BLOCKS
-#define CX_ENTITY_TRACE_MIN_BLOCKS 1
-#endif
 template <bool kEntities, bool kDynamic>
-__global__ void __launch_bounds__(kWaveThreads, kEntities ? CX_ENTITY_TRACE_MIN_BLOCKS : 1)
+__global__ void __launch_bounds__(kWaveThreads)
     wave_trace_kernel(const WaveView* __restrict__ views, const WaveBuffers b, uint32_t parity)
 {
     const uint32_t n = *(volatile uint32_t*)&b.counts[2 * parity];
