@@ -52,14 +52,18 @@ L2_FLUSH_BYTES = 256 << 20
 FALLBACK_HBM_GBS = 6650.0
 BUILD_BYTES_PER_LEAF = 492  # emit 112 + Morton 32 + sort 68 + Karras 20 + aggregate 100 + wide 160
 # The sort stage of the build: four onesweep passes (pass 0 reads keys only, 12 B; passes 1-3 read
-# and write pairs, 16 B) and the leaf-summary gather (values 4 B, a 48-byte row read and written,
-# the inverse 4 B).
-SORT_STAGE_BYTES_PER_PAIR = 60.0 + 104.0
+# and write pairs, 16 B).
+SORT_STAGE_BYTES_PER_PAIR = 60.0
+# The build's dominant stage: the tile kernel and the upper aggregation (aggregation 52 B read +
+# 48 B written, 4-wide collapse 96 x 1/2 read + 224 x 1/2 written, per leaf).
+TILE_STAGE_BYTES_PER_LEAF = 100.0 + 160.0
 TRACE_BYTES_PER_RAY = 64  # lower bound: one hash slot sector + one record sector per ray
 # DRAM bytes (read + write) measured by ncu (one capture per kernel, cold cache; profiles/): the sort
-# stage at 4,194,304 pairs (a pipelined pass times four, plus the gather kernel), scaled per pair;
-# the wavefront frame of the 512 x 512 trace (trace and shade kernels of its 5 bounce iterations).
-SORT_STAGE_DRAM_BYTES_PER_PAIR = (4 * 34.2e6 + 520.2e6 + 205.6e6) / 4194304  # 4 x one pass + the gather
+# stage at 4,194,304 pairs (a pipelined pass times four), scaled per pair; the tile stage at
+# 2,097,152 leaves (lt_tile_kernel + lt_aggregate_upper_kernel), scaled per leaf; the wavefront
+# frame of the 512 x 512 trace (trace and shade kernels of its 5 bounce iterations).
+SORT_STAGE_DRAM_BYTES_PER_PAIR = 4 * 34.2e6 / 4194304
+TILE_STAGE_DRAM_BYTES_PER_LEAF = (236.7e6 + 378.4e6 + 25.4e6 + 3.1e6) / 2097152
 TRACE_FRAME_DRAM_BYTES = 134.7e6
 
 
@@ -415,6 +419,7 @@ def measure_build(args, world, local, dev, stream, flush, records):
     bvh.set_profiling(False)
     peak, peak_kind = measured_peaks()
     sort_achieved = SORT_STAGE_BYTES_PER_PAIR * n / (stage_ms[2] / 1e3) / 1e9
+    tile_achieved = TILE_STAGE_BYTES_PER_LEAF * n / (stage_ms[5] / 1e3) / 1e9
     build_achieved = BUILD_BYTES_PER_LEAF * n / (ms / 1e3) / 1e9
 
     # The 4,096-record plain build, L2 flushed between builds.
@@ -462,26 +467,31 @@ def measure_build(args, world, local, dev, stream, flush, records):
     e2e_ms = max_over_ranks(e2e_s * 1e3, world) / args.steps
     bvh.close()
     bvh1.close()
+    # The key figures last: the driver keeps the tail of the line.
     return {
         "workload": f"light-tree build, {n} brick light records in a 1024^3-brick grid (16^3-brick groups)",
         "records": n,
-        "build_ms": ms,
-        "mleaves_per_s": world * n / (ms / 1e3) / 1e6,
-        "config1_ms": config1_ms,
         "stage_ms": {name: float(v) for name, v in zip(
-            ["emit_bounds", "morton_hist", "sort_4_passes_gather", "karras", "depth_scan", "tile_aggregate_collapse_upper_aggregate", "upper_collapse_finish"],
+            ["emit_bounds", "morton_hist", "sort_4_passes", "karras", "depth_scan", "tile_aggregate_collapse_upper_aggregate", "upper_collapse_finish"],
             stage_ms)},
-        "roofline": {"kernel": "sort stage: 4 onesweep_pipe_kernel passes + lt_gather_kernel", "bound": "hbm",
-                     "achieved": sort_achieved, "peak": peak, "unit": "GB/s", "frac": sort_achieved / peak,
-                     "peak_kind": peak_kind, "traffic": SORT_STAGE_DRAM_BYTES_PER_PAIR * n,
-                     "traffic_source": "ncu DRAM bytes of one pass (x4) and of the gather at 4M pairs, per pair",
-                     "algorithmic_bytes_per_launch": SORT_STAGE_BYTES_PER_PAIR * n},
-        "roofline_build": {"bound": "hbm", "achieved": build_achieved, "peak": peak, "unit": "GB/s",
-                           "frac": build_achieved / peak, "bytes_per_leaf": BUILD_BYTES_PER_LEAF},
+        "roofline_sort": {"kernel": "sort: 4 onesweep_pipe_kernel passes", "bound": "hbm",
+                          "achieved": sort_achieved, "peak": peak, "unit": "GB/s", "frac": sort_achieved / peak,
+                          "traffic": SORT_STAGE_DRAM_BYTES_PER_PAIR * n,
+                          "algorithmic_bytes_per_launch": SORT_STAGE_BYTES_PER_PAIR * n},
         "e2e": {"value": world * n / (e2e_ms / 1e3) / 1e6, "unit": "Mleaves/s",
                 "h2d_bytes_per_step": rec.nbytes + group.nbytes + frames.nbytes, "d2h_bytes_per_step": 128,
                 "ms_per_step": e2e_ms},
         "gpu_launches": launches,
+        "roofline": {"kernel": "lt_tile_kernel + lt_aggregate_upper_kernel", "bound": "hbm",
+                     "achieved": tile_achieved, "peak": peak, "unit": "GB/s", "frac": tile_achieved / peak,
+                     "peak_kind": peak_kind, "traffic": TILE_STAGE_DRAM_BYTES_PER_LEAF * n,
+                     "traffic_source": "ncu, both kernels at 2M leaves, per leaf",
+                     "algorithmic_bytes_per_launch": TILE_STAGE_BYTES_PER_LEAF * n},
+        "roofline_build": {"bound": "hbm", "achieved": build_achieved, "peak": peak, "unit": "GB/s",
+                           "frac": build_achieved / peak, "bytes_per_leaf": BUILD_BYTES_PER_LEAF},
+        "config1_ms": config1_ms,
+        "mleaves_per_s": world * n / (ms / 1e3) / 1e6,
+        "build_ms": ms,
     }
 
 
@@ -1128,8 +1138,8 @@ def run_ours(args, world, rank, local):
                          build["build_ms"], {"workload": build["workload"], "records": build["records"],
                                              "l2": "flushed between timed steps (256 MiB write)",
                                              "parallelism": f"replicas x{world}"})
-        line.update({k: build[k] for k in ("roofline", "roofline_build", "e2e", "gpu_launches", "stage_ms",
-                                           "config1_ms")})
+        line.update({k: build[k] for k in ("roofline", "roofline_sort", "roofline_build", "e2e", "gpu_launches",
+                                           "stage_ms", "config1_ms")})
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             v, builds, wall = oracle_build_throughput(1 << 20, 10.0, 1)
             line["cpu_baseline"] = {"value": v, "unit": "Mleaves/s", "cores": 1, "kind": "port",
@@ -1154,14 +1164,16 @@ def run_ours(args, world, rank, local):
         if args.batch:
             line["batch"] = compact(measure_batch(args, world, local, dev, stream))
         if build is not None:
-            section = {k: build[k] for k in ("records", "build_ms", "mleaves_per_s", "config1_ms", "stage_ms",
-                                             "roofline", "roofline_build", "e2e")}
-            for k in ("traffic_source", "peak_kind"):
-                section["roofline"].pop(k, None)
+            # The key figures at the very end of the line (the driver keeps its tail).
+            section = {k: build[k] for k in ("records", "stage_ms", "e2e")}
             if rank == 0 and world == 1 and not args.no_cpu_baseline:
                 v, builds, wall = oracle_build_throughput(1 << 18, 8.0, 1)
                 section["cpu_baseline"] = {"value": v, "unit": "Mleaves/s", "cores": 1, "kind": "port",
                                            "sample": f"{builds} oracle builds of 262144 records, 1 thread"}
+            section.update({k: build[k] for k in ("roofline", "roofline_build", "config1_ms", "mleaves_per_s",
+                                                  "build_ms")})
+            for k in ("traffic_source", "peak_kind"):
+                section["roofline"].pop(k, None)
             line["build"] = compact(section)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -293,23 +293,6 @@ __global__ void __launch_bounds__(kThreads)
 }
 
 // ---------------------------------------------------------------------------------------------
-// The leaf summaries in sorted order: sorted[j] = the first 48 bytes of leaves[values[j]].
-__global__ void __launch_bounds__(kThreads)
-    lt_gather_kernel(uint32_t n, const uint32_t* __restrict__ values, const LightBvhLeaf* __restrict__ leaves,
-                     LightSummary* __restrict__ sorted)
-{
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    const uint32_t v = __ldg(values + j);
-    const uint4* src = reinterpret_cast<const uint4*>(leaves + v);
-    const uint4 r0 = __ldg(src), r1 = __ldg(src + 1), r2 = __ldg(src + 2);
-    uint4* dst = reinterpret_cast<uint4*>(sorted) + 3ull * j;
-    dst[0] = r0;
-    dst[1] = r1;
-    dst[2] = r2;
-}
-
-// ---------------------------------------------------------------------------------------------
 // Karras 2012 binary radix tree over the sorted keys; ties broken by sorted position. Also the
 // range-count differences: node i covers the leaf boundaries [a, b) of its range [a, b], so
 // cover[a] += 1, cover[b] -= 1 (their prefix sum counts the nodes over every boundary).
@@ -437,7 +420,7 @@ __device__ __forceinline__ void row_word(uint32_t wd, uint32_t& c, uint32_t& idx
 }
 
 __global__ void __launch_bounds__(kAggTile)
-    lt_tile_kernel(uint32_t n, uint32_t node_capacity, const LightSummary* __restrict__ sorted,
+    lt_tile_kernel(uint32_t n, uint32_t node_capacity, LightSummary* __restrict__ sorted,
                    const uint32_t* __restrict__ left, const uint32_t* __restrict__ right,
                    const uint32_t* __restrict__ parent, const uint32_t* __restrict__ leaf_parent,
                    const uint32_t* __restrict__ range_end, const uint32_t* __restrict__ depth,
@@ -486,8 +469,11 @@ __global__ void __launch_bounds__(kAggTile)
     bool mine = false;  // node j lies inside the tile
     bool even = false;
     if (j < n) {
-        s_leaf[k] = load_summary(sorted + j);
-        s_value[k] = __ldg(values + j);
+        // The sorted leaf's summary, read through the permutation (the leaves' parent words,
+        // written below by other tiles, are other bytes of the rows).
+        const uint32_t v = __ldg(values + j);
+        s_value[k] = v;
+        s_leaf[k] = load_summary(&leaves[v].summary);
         node = __ldg(leaf_parent + j);
     }
     if (j + 1 < n) {
@@ -505,6 +491,19 @@ __global__ void __launch_bounds__(kAggTile)
         if (even && mine) s_even[at] = k;
     }
     if (even && !mine) s_cross[atomicAdd(&s_cross_count, 1u)] = j;
+    // The summaries of the leaves under a node that crosses the tile (a parent or a grandparent
+    // outside it), in sorted order for the upper kernels.
+    if (j < n && node != kNone) {
+        const auto inside_node = [&](uint32_t x) {
+            return x - lo < kAggTile && x + 1 < n && min(x, s_link[x - lo].w) >= lo && max(x, s_link[x - lo].w) <= hi;
+        };
+        bool needed = !inside_node(node);
+        if (!needed) {
+            const uint32_t g = s_link[node - lo].z;
+            needed = g != kNone && !inside_node(g);
+        }
+        if (needed) store_summary(sorted + j, s_leaf[k]);
+    }
     // 1. The walks.
     if (j < n) {
         LightSummary cur = s_leaf[k];
@@ -638,7 +637,7 @@ __global__ void __launch_bounds__(kThreads)
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         uint32_t from = upper[i];
         const bool leaf = (from & kChildLeafBit) != 0;
-        LightSummary cur = leaf ? load_summary(sorted + (from & ~kChildLeafBit)) : load_summary_cg(&aggregates[from].summary);
+        LightSummary cur = leaf ? load_summary_cg(sorted + (from & ~kChildLeafBit)) : load_summary_cg(&aggregates[from].summary);
         uint32_t node = leaf ? __ldg(leaf_parent + (from & ~kChildLeafBit)) : __ldg(parent + from);
         uint32_t depth = 0;
         for (; depth < 128 && node != kNone; ++depth) {
@@ -648,7 +647,7 @@ __global__ void __launch_bounds__(kThreads)
             const uint32_t sibling = l == from ? r : l;
             cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
             if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) break;
-            const LightSummary sib = (sibling & kChildLeafBit) ? load_summary(sorted + (sibling & ~kChildLeafBit))
+            const LightSummary sib = (sibling & kChildLeafBit) ? load_summary_cg(sorted + (sibling & ~kChildLeafBit))
                                                                : load_summary_cg(&aggregates[sibling].summary);
             cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
             store_slot(aggregates + node, cur);
@@ -693,7 +692,7 @@ __global__ void __launch_bounds__(kThreads)
             if (slot == kNone) continue;
             if (slot & kChildLeafBit) {
                 const uint32_t p = slot & ~kChildLeafBit;
-                sm[c] = load_summary(sorted + p);
+                sm[c] = load_summary_cg(sorted + p);
                 const uint32_t leaf = __ldg(values + p);
                 word[c] = kChildLeafBit | leaf;
                 leaves[leaf].parent = (w << kParentSlotBits) | c;  // the leaf's parent word, in place
@@ -1015,23 +1014,10 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         lt_morton_kernel<<<grid_for(n, kThreads * 4, sms * morton_per_sm), kThreads, 0, stream>>>(
             reinterpret_cast<const float4*>(b.aggregates), n, b.control, b.keys, b.counter, b.cover, b.sort_scratch);
         mark(2);
-        if (n <= kSmallSortKeys) {
-            // One CTA sorts and gathers (small_sort_kernel).
-            SortGather gather;
-            gather.rows_in = reinterpret_cast<const uint4*>(b.leaves);
-            gather.rows_in_stride = sizeof(LightBvhLeaf) / sizeof(uint4);
-            gather.rows_out = reinterpret_cast<uint4*>(b.sorted);
-            gather.inverse = nullptr;
-            onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
-                          stream, &gather, kpt);
-        } else {
-            // The sort, then the summaries gathered in sorted order by a kernel of its own (full
-            // occupancy keeps many of the random row reads in flight).
-            onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
-                          stream, nullptr, kpt);
-            lt_gather_kernel<<<grid_for(n, kThreads, 1u << 30), kThreads, 0, stream>>>(n, b.values, b.leaves,
-                                                                                        b.sorted);
-        }
+        // The sort (one small-sort CTA up to kSmallSortKeys pairs); later kernels read a sorted
+        // leaf's summary through the permutation.
+        onesweep_sort(b.keys, b.values, b.keys_alt, b.values_alt, n, true, b.sort_scratch, &b.control->status,
+                      stream, nullptr, kpt);
         mark(3);
     } else {
         mark(1);
@@ -1074,10 +1060,10 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
 
 uint32_t lt_kernel_launches(uint32_t n)
 {
-    // emit, Morton, the sort (one small-sort CTA, or four passes and the gather), the six tree
-    // kernels from two leaves, finish.
+    // emit, Morton, the sort (one small-sort CTA, or four passes), the six tree kernels from two
+    // leaves, finish.
     if (n == 0) return 1;
-    const uint32_t sort = n <= kSmallSortKeys ? 1u : 5u;
+    const uint32_t sort = n <= kSmallSortKeys ? 1u : 4u;
     return 2 + sort + (n >= 2 ? 6u : 0u) + 1;
 }
 
