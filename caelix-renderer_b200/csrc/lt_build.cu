@@ -731,10 +731,10 @@ __global__ void __launch_bounds__(kThreads)
 // ---------------------------------------------------------------------------------------------
 // Single-pass exclusive scans over tiles of kScanItems per thread (decoupled look-back by one warp,
 // warp_lookback).
-constexpr int kScanItems = 16;
+constexpr int kScanItems = 32;
 constexpr uint32_t kScanTile = kScanThreads * kScanItems;
 
-// A thread's kScanItems consecutive words from base (a multiple of kScanItems): four 16-byte loads
+// A thread's kScanItems consecutive words from base (a multiple of kScanItems): 16-byte loads
 // when all lie below count, else word by word (zero past count).
 __device__ __forceinline__ void load_run(const uint32_t* p, uint32_t base, uint32_t count, uint32_t (&v)[kScanItems])
 {
