@@ -624,16 +624,38 @@ __global__ void __launch_bounds__(kAggTile)
 
 // The walks up through the nodes whose range crosses a tile, from the children the tiles listed
 // (an in-tile node, its summary in its slot, or a leaf): the second thread to arrive at a node
-// (device-scope counter) computes it and goes on. A persistent grid takes the list (its length is
-// known on the device only). The walks were run inside the tile kernel at first: chains of
-// dependent device-scope atomics and L2 loads that kept each tile's CTA resident for them.
-__global__ void __launch_bounds__(kThreads)
+// computes it and goes on. The walks were run inside the tile kernel at first: chains of
+// dependent device-scope atomics and L2 loads that kept each tile's CTA resident for them. Up to
+// kUpperOneCtaItems walks (one per thread: builds of up to about 16 k leaves) run in one CTA
+// (kOneCta), whose arrivals are block-scope and whose siblings' summaries come through L1; more
+// run on a persistent grid with device-scope arrivals (the list's length is known on the device
+// only: each variant checks it). With six walks per thread (97 k leaves) the one CTA was slower
+// than the grid (the light-tree flush of the 2 M-brick world 0.22 against 0.18 ms).
+constexpr uint32_t kUpperOneCtaItems = 1024;
+constexpr uint32_t kUpperOneCtaThreads = 1024;
+
+// A summary written earlier by this kernel's CTA (after an acquire: weak loads through L1).
+__device__ __forceinline__ LightSummary load_summary_weak(const LightSummary* p)
+{
+    const float4* q = reinterpret_cast<const float4*>(p);
+    const float4 a = q[0], b = q[1], c = q[2];
+    LightSummary s;
+    s.face[0] = a.x; s.face[1] = a.y; s.face[2] = a.z; s.face[3] = a.w;
+    s.face[4] = b.x; s.face[5] = b.y; s.lo[0] = b.z; s.lo[1] = b.w;
+    s.lo[2] = c.x; s.hi[0] = c.y; s.hi[1] = c.z; s.hi[2] = c.w;
+    return s;
+}
+
+template <bool kOneCta>
+__global__ void __launch_bounds__(kOneCta ? kUpperOneCtaThreads : kThreads)
     lt_aggregate_upper_kernel(const LightSummary* __restrict__ sorted, const uint32_t* __restrict__ left,
                               const uint32_t* __restrict__ right, const uint32_t* __restrict__ parent,
                               const uint32_t* __restrict__ leaf_parent, uint32_t* counter,
                               AggregateSlot* aggregates, const uint32_t* __restrict__ upper, BuildControl* control)
 {
+    constexpr cuda::thread_scope kScope = kOneCta ? cuda::thread_scope_block : cuda::thread_scope_device;
     const uint32_t count = control->upper_count;
+    if (kOneCta ? count > kUpperOneCtaItems : count <= kUpperOneCtaItems) return;
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
         uint32_t from = upper[i];
         const bool leaf = (from & kChildLeafBit) != 0;
@@ -645,10 +667,12 @@ __global__ void __launch_bounds__(kThreads)
             const uint32_t r = __ldg(right + node);
             const uint32_t up = __ldg(parent + node);
             const uint32_t sibling = l == from ? r : l;
-            cuda::atomic_ref<uint32_t, cuda::thread_scope_device> arrival(counter[node]);
+            cuda::atomic_ref<uint32_t, kScope> arrival(counter[node]);
             if (arrival.fetch_add(1u, cuda::memory_order_acq_rel) == 0) break;
-            const LightSummary sib = (sibling & kChildLeafBit) ? load_summary_cg(sorted + (sibling & ~kChildLeafBit))
-                                                               : load_summary_cg(&aggregates[sibling].summary);
+            LightSummary sib;
+            if (sibling & kChildLeafBit) sib = load_summary_cg(sorted + (sibling & ~kChildLeafBit));
+            else if (kOneCta) sib = load_summary_weak(&aggregates[sibling].summary);
+            else sib = load_summary_cg(&aggregates[sibling].summary);
             cur = l == from ? lt_union(cur, sib) : lt_union(sib, cur);
             store_slot(aggregates + node, cur);
             from = node;
@@ -1041,7 +1065,9 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
         lt_tile_kernel<<<(n + kAggTile - 1) / kAggTile, kAggTile, 0, stream>>>(
             n, b.node_capacity, b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.values_alt, b.depth, b.wide,
             b.values, b.aggregates, b.cover, b.keys_alt, b.leaves, b.nodes, b.control);
-        lt_aggregate_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
+        lt_aggregate_upper_kernel<true><<<1, kUpperOneCtaThreads, 0, stream>>>(
+            b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.cover, b.control);
+        lt_aggregate_upper_kernel<false><<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
             b.sorted, b.left, b.right, b.parent, b.leaf_parent, b.counter, b.aggregates, b.cover, b.control);
         mark(6);
         lt_wide_upper_kernel<<<grid_for(nodes, kThreads, sms * 8), kThreads, 0, stream>>>(
@@ -1060,11 +1086,12 @@ cudaError_t lt_build(const LightBvhBuffers& b, const LightBvhInput& in, cudaStre
 
 uint32_t lt_kernel_launches(uint32_t n)
 {
-    // emit, Morton, the sort (one small-sort CTA, or four passes), the six tree kernels from two
-    // leaves, finish.
+    // emit, Morton, the sort (one small-sort CTA, or four passes), the seven tree kernels from two
+    // leaves (the upper aggregation's two variants both launch; one of them returns at once),
+    // finish.
     if (n == 0) return 1;
     const uint32_t sort = n <= kSmallSortKeys ? 1u : 4u;
-    return 2 + sort + (n >= 2 ? 6u : 0u) + 1;
+    return 2 + sort + (n >= 2 ? 7u : 0u) + 1;
 }
 
 }  // namespace cx
