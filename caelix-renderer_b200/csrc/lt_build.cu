@@ -353,17 +353,19 @@ __global__ void __launch_bounds__(kThreads)
 // Bottom-up aggregation and the 4-wide collapse, by tiles. A CTA owns a tile of kAggTile
 // consecutive sorted leaves and the binary nodes with the same indices (a node is an end of its
 // leaf range, so every node whose range lies inside the tile has its index there). The tile's leaf
-// summaries, node links, 4-wide indices, leaf indices, arrival counters and node summaries are
-// loaded into shared memory once; then
+// summaries (each sorted leaf read through the permutation), node links, 4-wide indices, leaf
+// indices, arrival counters and node summaries live in shared memory; then
+//   0. the summaries of the leaves under a node that crosses the tile (a parent or grandparent
+//      outside it) are written in sorted order (`sorted`) for the two upper kernels;
 //   1. one walk per leaf: the second thread to arrive at an in-tile node computes its summary from
 //      both children and goes on (block-scope arrivals, nothing but shared memory touched). A walk
 //      stops at the first node whose range crosses the tile and lists the child it comes from
 //      (`upper`: an in-tile node, or a leaf with the leaf bit) for lt_aggregate_upper_kernel;
 //   2. the in-tile summaries go to their 64-byte global slots (coalesced full-sector writes);
-//   3. every in-tile node at even depth becomes its 224-byte 4-wide node, built from shared memory
-//      by half a warp (lane q writes 16-byte unit q: one coalesced row), with the parent words of
-//      its leaf slots written into the leaves. Even-depth nodes that cross the tile are listed
-//      (`crossing`) for lt_wide_upper_kernel.
+//   3. every in-tile node at even depth becomes its 224-byte 4-wide node: four threads per node
+//      (thread c: child slot c) write its row into a staging buffer of kRowChunk rows, which the
+//      CTA then stores as 16-byte units; the parent words of its leaf slots go into the leaves.
+//      Even-depth nodes that cross the tile are listed (`crossing`) for lt_wide_upper_kernel.
 // The depths and 4-wide indices come from the scans, which run before this kernel.
 constexpr uint32_t kAggTile = 256;
 constexpr uint32_t kNodeQuads = sizeof(LightBvhNode) / 16;  // 14
