@@ -4,15 +4,15 @@
 //
 // Replaces the reference's per-tree dispatch sequence LightTree::RecordTree
 // (lib/src/light/light_tree_record.cpp:230-309, about 35 dependent dispatches with a barrier after
-// each) with 15 kernels and one memset at 4,097 leaves and more (one small-sort CTA in place of
-// the five sort kernels below that), all on one stream (capturable in a CUDA graph):
+// each) with 14 kernels and one memset at 4,097 leaves and more (one small-sort CTA in place of
+// the four sort passes below that), all on one stream (capturable in a CUDA graph):
 //   lt_emit_kernel        gather emit (caelix_light_gather_emit.hlsl:11-86) fused with the centre
 //                         bounds (caelix_light_bvh_bounds.hlsl:10-53): warp max-reductions of
 //                         order-preserving codes instead of a one-workgroup reduction
 //   lt_morton_kernel      Morton codes (caelix_light_bvh_morton.hlsl:6-28) fused with the digit
 //                         histograms of all four sort passes and the clear of the arrival counters
-//   onesweep_pipe_kernel  x4 (radix_sort.cuh), then lt_gather_kernel: the leaf summaries in sorted
-//                         order, so every later kernel reads leaves by sorted position
+//   onesweep_pipe_kernel  x4 (radix_sort.cuh); later kernels read a sorted leaf through the
+//                         permutation
 //   lt_karras_kernel      caelix_light_bvh_karras.hlsl:8-96, plus the range-count differences
 //   lt_cover_scan_kernel  the depths (caelix_light_bvh_depth.hlsl:7-30) without walking to the
 //   lt_flags_scan_kernel  root: depth(i) + 1 = the number of binary nodes whose range spans node i's
@@ -22,7 +22,8 @@
 //   lt_tile_kernel        by tiles of 256 sorted leaves in shared memory: the aggregation
 //                         (caelix_light_bvh_aggregate.hlsl:30-55) of the nodes inside the tile and
 //                         the 4-wide nodes over them (caelix_light_bvh_wide.hlsl:10-100)
-//   lt_aggregate_upper_kernel  the aggregation of the nodes that cross tiles (acq_rel arrivals)
+//   lt_aggregate_upper_kernel  the aggregation of the nodes that cross tiles (acq_rel arrivals; two
+//                         variants, one CTA for up to 1,024 walks or a persistent grid)
 //   lt_wide_upper_kernel  the 4-wide nodes over the nodes that cross tiles
 //   lt_finish_kernel      caelix_light_bvh_finish.hlsl:8-63
 // Every float operation is a single IEEE fp32 operation in the order of the HLSL source (the
